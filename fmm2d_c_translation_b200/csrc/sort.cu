@@ -1,0 +1,117 @@
+// sort.cu -- stable LSD radix sort of (uint32 key, uint32 value) pairs.
+//
+// Used by the tree builder to turn "leaf of every point" into the reference's
+// stable point permutation (isrc / itarg): points are ordered by the
+// depth-first position of their leaf and, inside a leaf, by input index,
+// which is exactly what the reference's repeated stable partition
+// (c_translation/src/pts_tree2d.c:670-765) produces.
+//
+// One pass per 8-bit digit: a per-tile histogram, a scan of the
+// digit-major histogram table, and a scatter in which every tile ranks its
+// items stably (warp match for ties inside a warp, per-warp counts in shared
+// memory across warps, a running per-digit count across rounds).
+#include "common.cuh"
+#include "sort.cuh"
+
+namespace fmm2d {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kRounds = 16;
+constexpr int kTile = kThreads * kRounds;  // 4096 items per block
+constexpr int kRadix = 256;
+
+__global__ void radix_hist_kernel(const uint32_t *__restrict__ keys, int64_t n,
+                                  int shift, int nblocks,
+                                  int *__restrict__ hist) {
+    __shared__ int h[kRadix];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * kTile;
+#pragma unroll 4
+    for (int r = 0; r < kRounds; r++) {
+        int64_t idx = base + (int64_t)r * kThreads + threadIdx.x;
+        if (idx < n) atomicAdd(&h[(keys[idx] >> shift) & 0xff], 1);
+    }
+    __syncthreads();
+    hist[threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+}
+
+__global__ void radix_scatter_kernel(const uint32_t *__restrict__ kin,
+                                     const uint32_t *__restrict__ vin,
+                                     uint32_t *__restrict__ kout,
+                                     uint32_t *__restrict__ vout, int64_t n,
+                                     int shift, int nblocks,
+                                     const int *__restrict__ offs) {
+    __shared__ int run[kRadix];
+    __shared__ int wc[kWarps][kRadix];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    run[tid] = offs[tid * nblocks + blockIdx.x];
+    const unsigned lt_mask = (1u << lane) - 1u;
+    const int64_t base = (int64_t)blockIdx.x * kTile;
+    for (int r = 0; r < kRounds; r++) {
+#pragma unroll
+        for (int w = 0; w < kWarps; w++) wc[w][tid] = 0;
+        __syncthreads();
+        const int64_t idx = base + (int64_t)r * kThreads + tid;
+        const bool valid = idx < n;
+        uint32_t key = 0, val = 0;
+        int d = -1;
+        if (valid) {
+            key = kin[idx];
+            val = vin[idx];
+            d = (int)((key >> shift) & 0xff);
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const int rank = __popc(peers & lt_mask);
+        if (valid && rank == 0) wc[warp][d] = __popc(peers);
+        __syncthreads();
+        if (valid) {
+            int pos = run[d] + rank;
+            for (int w = 0; w < warp; w++) pos += wc[w][d];
+            kout[pos] = key;
+            vout[pos] = val;
+        }
+        __syncthreads();
+        int add = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; w++) add += wc[w][tid];
+        run[tid] += add;
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+void radix_sort_pairs(uint32_t *keys, uint32_t *vals, uint32_t *keys_tmp,
+                      uint32_t *vals_tmp, int64_t n, int key_bits,
+                      cudaStream_t s) {
+    if (n <= 1 || key_bits <= 0) return;
+    const int nblocks = (int)((n + kTile - 1) / kTile);
+    DevBuf<int> hist((size_t)kRadix * nblocks, s);
+    DevBuf<int> offs((size_t)kRadix * nblocks, s);
+    uint32_t *ka = keys, *va = vals, *kb = keys_tmp, *vb = vals_tmp;
+    int passes = 0;
+    for (int shift = 0; shift < key_bits; shift += 8) {
+        radix_hist_kernel<<<nblocks, kThreads, 0, s>>>(ka, n, shift, nblocks,
+                                                       hist.get());
+        FMM_CHECK_LAUNCH();
+        exclusive_scan_i32(hist.get(), offs.get(), (int64_t)kRadix * nblocks,
+                           nullptr, s);
+        radix_scatter_kernel<<<nblocks, kThreads, 0, s>>>(
+            ka, va, kb, vb, n, shift, nblocks, offs.get());
+        FMM_CHECK_LAUNCH();
+        std::swap(ka, kb);
+        std::swap(va, vb);
+        passes++;
+    }
+    if (passes & 1) {
+        FMM_CUDA(cudaMemcpyAsync(keys, ka, n * sizeof(uint32_t),
+                                 cudaMemcpyDeviceToDevice, s));
+        FMM_CUDA(cudaMemcpyAsync(vals, va, n * sizeof(uint32_t),
+                                 cudaMemcpyDeviceToDevice, s));
+    }
+}
+
+}  // namespace fmm2d

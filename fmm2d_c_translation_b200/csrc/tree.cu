@@ -1,0 +1,816 @@
+// tree.cu -- device construction of the reference's adaptive quadtree.
+//
+// The reference builds its tree serially (c_translation/src/pts_tree2d.c,
+// tree_routs2d.c).  Every step it takes is either "for each box of one
+// level, decide something from data of coarser levels" or "append the
+// children of the flagged boxes of a range, in box order".  The first maps
+// to one kernel per level; the second to a prefix sum over the flags (the
+// same role cumsum plays in tree_refine_boxes) followed by one kernel that
+// writes the children at their scanned positions.  With the same FP64
+// operations in the same order (box centers by repeated center +/- bs/2,
+// child choice by `p - c < 0`, the 1.05-scaled distance tests), the box
+// numbering, centers and point permutation come out identical.
+#include "sort.cuh"
+#include "tree.cuh"
+
+#include <algorithm>
+
+namespace fmm2d {
+namespace {
+
+// Child j (0-based) of a box: the reference numbers children 1..4 as
+// (-x,-y), (+x,-y), (-x,+y), (+x,+y) (tree_routs2d.c:77-86).
+__device__ __forceinline__ double2 child_center(double2 c, double bs, int j) {
+    const double hx = ((j & 1) ? bs : -bs) * 0.5;
+    const double hy = ((j & 2) ? bs : -bs) * 0.5;
+    return make_double2(__dadd_rn(c.x, hx), __dadd_rn(c.y, hy));
+}
+
+// Which child of a box with center c holds point p (pts_tree2d.c:697-748):
+// first split on y, then on x, comparing `p - c < 0`.
+__device__ __forceinline__ int child_digit(double2 p, double2 c) {
+    const int right = (__dsub_rn(p.x, c.x) < 0.0) ? 0 : 1;
+    const int upper = (__dsub_rn(p.y, c.y) < 0.0) ? 0 : 2;
+    return right + upper;
+}
+
+__device__ __forceinline__ bool within(double2 a, double2 b, double d) {
+    return fabs(__dsub_rn(a.x, b.x)) <= d && fabs(__dsub_rn(a.y, b.y)) <= d;
+}
+
+struct Builder {
+    Tree &T;
+    cudaStream_t s;
+    DevBuf<int> iflag;
+    DevBuf<int> cnt_s, cnt_t;  // point counts per box (initial build only)
+
+    Builder(Tree &t, cudaStream_t st) : T(t), s(st) {}
+
+    // Grow every per-box array to hold at least `need` boxes.
+    void ensure(int need) {
+        if (need <= T.cap) return;
+        int nc = std::max(need, T.cap + T.cap / 2 + 64);
+        size_t keep = (size_t)T.nboxes;
+        T.centers.grow(nc, keep, s);
+        T.level.grow(nc, keep, s);
+        T.parent.grow(nc, keep, s);
+        T.nchild.grow(nc, keep, s);
+        T.child.grow((size_t)4 * nc, 4 * keep, s);
+        T.nnbors.grow(nc, keep, s);
+        T.nbors.grow((size_t)9 * nc, 9 * keep, s);
+        iflag.grow(nc, keep, s);
+        if (cnt_s.size()) cnt_s.grow(nc, keep, s);
+        if (cnt_t.size()) cnt_t.grow(nc, keep, s);
+        T.cap = nc;
+    }
+
+    // Appends 4 children to every box b in [lo, hi) with sel(b) true, in box
+    // order.  Returns the number of refined boxes.  Mirrors
+    // tree_refine_boxes and, with set_flags, tree_refine_boxes_flag, whose
+    // children get flag 3 under a flag-1 parent and 0 otherwise.  `sel` is
+    // evaluated before any array grows.
+    template <class Sel>
+    int refine_range(int lo, int hi, int newlevel, double bs, Sel sel,
+                     bool set_flags) {
+        const int n = hi - lo;
+        if (n <= 0) return 0;
+        DevBuf<int> f(n, s), off(n, s), tot(1, s);
+        int *fp = f.get();
+        for_each(n, s, [=] __device__(int64_t i) { fp[i] = sel(lo + (int)i) ? 1 : 0; });
+        exclusive_scan_i32(fp, off.get(), n, tot.get(), s);
+        const int nref = read_scalar(tot.get(), s);
+        if (nref == 0) return 0;
+        ensure(T.nboxes + 4 * nref);
+        const int nb0 = T.nboxes;
+        double2 *cen = T.centers.get();
+        int *lev = T.level.get(), *par = T.parent.get(), *nch = T.nchild.get();
+        int *chi = T.child.get(), *flg = iflag.get();
+        int *cs = cnt_s.get(), *ct = cnt_t.get();
+        const int *op = off.get();
+        for_each(n, s, [=] __device__(int64_t i) {
+            if (!fp[i]) return;
+            const int b = lo + (int)i;
+            const int base = nb0 + 4 * op[i];
+            const double2 c = cen[b];
+            const int cf = (set_flags && flg[b] == 1) ? 3 : 0;
+            nch[b] = 4;
+            for (int j = 0; j < 4; j++) {
+                const int kb = base + j;
+                cen[kb] = child_center(c, bs, j);
+                par[kb] = b;
+                nch[kb] = 0;
+                lev[kb] = newlevel;
+                for (int l = 0; l < 4; l++) chi[4 * kb + l] = -1;
+                chi[4 * b + j] = kb;
+                if (set_flags) flg[kb] = cf;
+                if (cs) cs[kb] = 0;
+                if (ct) ct[kb] = 0;
+            }
+        });
+        T.nboxes += 4 * nref;
+        return nref;
+    }
+
+    std::vector<double> host_dist(int kind) const {
+        // 1.05-scaled distance thresholds per level, evaluated exactly as the
+        // reference writes them.
+        std::vector<double> d(T.nlevels + 2, 0.0);
+        const std::vector<double> &bs = T.boxsize;
+        for (int l = 0; l <= T.nlevels; l++) {
+            switch (kind) {
+                case 0: d[l] = 1.05 * bs[l]; break;  // colleagues
+                case 1:  // flag pass (pts_tree2d.c:800)
+                    if (l >= 2) d[l] = 1.05 * (bs[l - 1] + bs[l - 2]) / 2.0;
+                    break;
+                case 2:  // flag+ pass (pts_tree2d.c:829)
+                    if (l >= 1) d[l] = 1.05 * (bs[l] + bs[l - 1]) / 2.0;
+                    break;
+                case 3:  // updateflags / list 1 (tree_routs2d.c:215, 466)
+                    if (l + 1 <= T.nlevels)
+                        d[l] = 1.05 * (bs[l] + bs[l + 1]) / 2.0;
+                    else
+                        d[l] = 1.05 * (bs[l] + bs[l] / 2) / 2.0;
+                    break;
+            }
+        }
+        return d;
+    }
+
+    // computecoll (tree_routs2d.c:140-195) for levels [l0, l1].
+    void computecoll(int l0, int l1) {
+        int *nnb = T.nnbors.get(), *nb = T.nbors.get();
+        const int *par = T.parent.get(), *chi = T.child.get();
+        const double2 *cen = T.centers.get();
+        if (l0 == 0) {
+            for_each(1, s, [=] __device__(int64_t) {
+                nnb[0] = 1;
+                nb[0] = 0;
+                for (int k = 1; k < 9; k++) nb[k] = -1;
+            });
+            l0 = 1;
+        }
+        for (int l = l0; l <= l1; l++) {
+            const int lo = T.lstart[l], n = T.lend[l] - T.lstart[l];
+            const double d = 1.05 * T.boxsize[l];
+            for_each(n, s, [=] __device__(int64_t i) {
+                const int b = lo + (int)i;
+                const int dad = par[b];
+                const double2 cb = cen[b];
+                int cnt = 0;
+                for (int k = 0; k < nnb[dad]; k++) {
+                    const int jb = nb[9 * dad + k];
+                    for (int j = 0; j < 4; j++) {
+                        const int kb = chi[4 * jb + j];
+                        if (kb >= 0 && within(cen[kb], cb, d) && cnt < 9)
+                            nb[9 * b + cnt++] = kb;
+                    }
+                }
+                nnb[b] = cnt;
+                for (int k = cnt; k < 9; k++) nb[9 * b + k] = -1;
+            });
+        }
+    }
+
+    // pts_tree_reorg (pts_tree2d.c:966-1085): on every level >= 2 the boxes
+    // of the level range come first, then the appended ("tail") boxes of
+    // that level, each group in its current order.
+    void reorg(const std::vector<int> &tstart, const std::vector<int> &tend) {
+        const int L = T.nlevels;
+        const int nb = T.nboxes;
+        std::vector<int> h(4 * (L + 1), 0);  // lstart, lend, tstart, nstart
+        int cur = T.lstart[std::min(2, L)];
+        std::vector<int> nstart(L + 1), nend(L + 1);
+        for (int l = 0; l <= L; l++) {
+            if (l < 2) {
+                nstart[l] = T.lstart[l];
+                nend[l] = T.lend[l];
+                continue;
+            }
+            nstart[l] = cur;
+            cur += (T.lend[l] - T.lstart[l]) + (tend[l] - tstart[l]);
+            nend[l] = cur;
+        }
+        for (int l = 0; l <= L; l++) {
+            h[4 * l + 0] = T.lstart[l];
+            h[4 * l + 1] = T.lend[l];
+            h[4 * l + 2] = tstart[l];
+            h[4 * l + 3] = nstart[l];
+        }
+        DevBuf<int> lv(h.size(), s);
+        FMM_CUDA(cudaMemcpyAsync(lv.get(), h.data(), h.size() * sizeof(int),
+                                 cudaMemcpyHostToDevice, s));
+        DevBuf<int> map(nb, s);
+        int *mp = map.get();
+        const int *lvp = lv.get(), *levp = T.level.get();
+        for_each(nb, s, [=] __device__(int64_t i) {
+            const int b = (int)i, l = levp[b];
+            int m;
+            if (l < 2) {
+                m = b;
+            } else {
+                const int ls = lvp[4 * l], le = lvp[4 * l + 1];
+                const int ts = lvp[4 * l + 2], ns0 = lvp[4 * l + 3];
+                m = (b >= ls && b < le) ? ns0 + (b - ls) : ns0 + (le - ls) + (b - ts);
+            }
+            mp[b] = m;
+        });
+        DevBuf<double2> cen2(T.cap, s);
+        DevBuf<int> lev2(T.cap, s), par2(T.cap, s), nch2(T.cap, s),
+            chi2((size_t)4 * T.cap, s), flg2(T.cap, s);
+        const double2 *cen = T.centers.get();
+        const int *par = T.parent.get(), *nch = T.nchild.get(),
+                  *chi = T.child.get(), *flg = iflag.get();
+        double2 *c2 = cen2.get();
+        int *l2 = lev2.get(), *p2 = par2.get(), *n2 = nch2.get(),
+            *h2 = chi2.get(), *f2 = flg2.get();
+        for_each(nb, s, [=] __device__(int64_t i) {
+            const int b = (int)i, m = mp[b];
+            c2[m] = cen[b];
+            l2[m] = levp[b];
+            n2[m] = nch[b];
+            f2[m] = flg[b];
+            p2[m] = par[b] < 0 ? -1 : mp[par[b]];
+            for (int j = 0; j < 4; j++) {
+                const int c = chi[4 * b + j];
+                h2[4 * m + j] = c < 0 ? -1 : mp[c];
+            }
+        });
+        T.centers = std::move(cen2);
+        T.level = std::move(lev2);
+        T.parent = std::move(par2);
+        T.nchild = std::move(nch2);
+        T.child = std::move(chi2);
+        iflag = std::move(flg2);
+        for (int l = 2; l <= L; l++) {
+            T.lstart[l] = nstart[l];
+            T.lend[l] = nend[l];
+        }
+    }
+
+    // pts_tree_fix_lr (pts_tree2d.c:767-964).
+    void fix_lr() {
+        const int L = T.nlevels;
+        int *flg = iflag.get();
+        const int *nch = T.nchild.get(), *par = T.parent.get(),
+                  *lev = T.level.get();
+        const double2 *cen = T.centers.get();
+        iflag.zero(s);
+        const std::vector<double> d1 = host_dist(1), d2 = host_dist(2),
+                                  d3 = host_dist(3);
+        DevBuf<double> dd1(L + 2, s);
+        FMM_CUDA(cudaMemcpyAsync(dd1.get(), d1.data(), d1.size() * sizeof(double),
+                                 cudaMemcpyHostToDevice, s));
+        const double *dp1 = dd1.get();
+        {
+            // flag: leaves among the granddad's colleagues that touch the dad.
+            const int *nnb = T.nnbors.get(), *nb = T.nbors.get();
+            const int lo = T.lstart[2], n = T.lend[L] - T.lstart[2];
+            for_each(n, s, [=] __device__(int64_t i) {
+                const int b = lo + (int)i;
+                const int idad = par[b], igd = par[idad];
+                const double dist = dp1[lev[b]];
+                const double2 cd = cen[idad];
+                for (int k = 0; k < nnb[igd]; k++) {
+                    const int jb = nb[9 * igd + k];
+                    if (nch[jb] == 0 && flg[jb] == 0 && within(cen[jb], cd, dist))
+                        flg[jb] = 1;
+                }
+            });
+        }
+        for (int l = L; l >= 1; l--) {
+            // flag+: leaves among the dad's colleagues that touch a flagged box.
+            const int *nnb = T.nnbors.get(), *nb = T.nbors.get();
+            const int lo = T.lstart[l], n = T.lend[l] - T.lstart[l];
+            const double dist = d2[l];
+            for_each(n, s, [=] __device__(int64_t i) {
+                const int b = lo + (int)i;
+                const int f = flg[b];
+                if (f != 1 && f != 2) return;
+                const int dad = par[b];
+                const double2 cb = cen[b];
+                for (int k = 0; k < nnb[dad]; k++) {
+                    const int jb = nb[9 * dad + k];
+                    if (nch[jb] == 0 && flg[jb] == 0 && within(cen[jb], cb, dist))
+                        flg[jb] = 2;
+                }
+            });
+        }
+        // Subdivide flag and flag+ boxes of the original levels.
+        std::vector<int> ts(L + 1, 0), te(L + 1, 0);
+        for (int l = 1; l <= L - 2; l++) {
+            ts[l + 1] = T.nboxes;
+            int *fl = iflag.get();
+            refine_range(
+                T.lstart[l], T.lend[l], l + 1, T.boxsize[l + 1],
+                [=] __device__(int b) { return fl[b] > 0; }, true);
+            te[l + 1] = T.nboxes;
+        }
+        reorg(ts, te);
+        computecoll(0, L);
+        {
+            int *fl = iflag.get();
+            for_each(T.nboxes, s, [=] __device__(int64_t i) {
+                if (fl[i] != 3) fl[i] = 0;
+            });
+        }
+        std::fill(ts.begin(), ts.end(), 0);
+        std::fill(te.begin(), te.end(), 0);
+        for (int l = 2; l <= L - 2; l++) {
+            // updateflags (tree_routs2d.c:197-252) on the level range and on
+            // this level's tail: a flag++ box is subdivided only when a child
+            // of one of its colleagues has children and touches it.
+            const int *nnb = T.nnbors.get(), *nb = T.nbors.get(),
+                      *chi = T.child.get(), *nchp = T.nchild.get();
+            const double2 *cp = T.centers.get();
+            int *fl = iflag.get();
+            const double dist = d3[l];
+            const int lo = T.lstart[l], n1 = T.lend[l] - T.lstart[l];
+            const int tlo = ts[l], n2 = te[l] - ts[l];
+            for_each(n1 + n2, s, [=] __device__(int64_t i) {
+                const int b = i < n1 ? lo + (int)i : tlo + (int)(i - n1);
+                if (fl[b] != 3) return;
+                int f = 0;
+                const double2 cb = cp[b];
+                for (int k = 0; k < nnb[b] && !f; k++) {
+                    const int jb = nb[9 * b + k];
+                    for (int j = 0; j < 4; j++) {
+                        const int kb = chi[4 * jb + j];
+                        if (kb >= 0 && nchp[kb] > 0 && within(cp[kb], cb, dist)) {
+                            f = 1;
+                            break;
+                        }
+                    }
+                }
+                fl[b] = f;
+            });
+            ts[l + 1] = T.nboxes;
+            refine_range(
+                T.lstart[l], T.lend[l], l + 1, T.boxsize[l + 1],
+                [=] __device__(int b) { return fl[b] > 0; }, true);
+            {
+                int *fl2 = iflag.get();
+                refine_range(
+                    tlo, tlo + n2, l + 1, T.boxsize[l + 1],
+                    [=] __device__(int b) { return fl2[b] > 0; }, true);
+            }
+            te[l + 1] = T.nboxes;
+            // colleagues of the new boxes from their dad's (current) list
+            const int nlo = ts[l + 1], nn = te[l + 1] - ts[l + 1];
+            if (nn > 0) {
+                int *nnbw = T.nnbors.get(), *nbw = T.nbors.get();
+                const int *parp = T.parent.get(), *chip = T.child.get();
+                const double2 *cq = T.centers.get();
+                const double dcol = 1.05 * T.boxsize[l + 1];
+                for_each(nn, s, [=] __device__(int64_t i) {
+                    const int b = nlo + (int)i;
+                    const int dad = parp[b];
+                    const double2 cb = cq[b];
+                    int cnt = 0;
+                    for (int k = 0; k < nnbw[dad]; k++) {
+                        const int jb = nbw[9 * dad + k];
+                        for (int j = 0; j < 4; j++) {
+                            const int kb = chip[4 * jb + j];
+                            if (kb >= 0 && within(cq[kb], cb, dcol) && cnt < 9)
+                                nbw[9 * b + cnt++] = kb;
+                        }
+                    }
+                    nnbw[b] = cnt;
+                    for (int k = cnt; k < 9; k++) nbw[9 * b + k] = -1;
+                });
+            }
+        }
+        reorg(ts, te);
+        computecoll(0, L);
+    }
+
+    // pts_tree_sort (pts_tree2d.c:1087-1119): the permutation and the
+    // per-box point ranges for one point set.
+    void sort_points(const double2 *d_pts, int n, DevBuf<int2> &se,
+                     DevBuf<int> &perm) {
+        const int nb = T.nboxes, L = T.nlevels;
+        se.alloc(nb, s);
+        perm.alloc(std::max(n, 1), s);
+        DevBuf<int> cnt(nb, s), start(nb, s);
+        cnt.zero(s);
+        DevBuf<uint32_t> keys(std::max(n, 1), s), vals(std::max(n, 1), s);
+        int *cp = cnt.get();
+        const int *nch = T.nchild.get(), *chi = T.child.get();
+        const double2 *cen = T.centers.get();
+        uint32_t *kp = keys.get(), *vp = vals.get();
+        // leaf of every point, found by descending from the root
+        for_each(n, s, [=] __device__(int64_t i) {
+            const double2 p = d_pts[i];
+            int b = 0;
+            while (nch[b] > 0) b = chi[4 * b + child_digit(p, cen[b])];
+            kp[i] = (uint32_t)b;
+            atomicAdd(&cp[b], 1);
+        });
+        // subtree counts, deepest level first
+        for (int l = L; l >= 0; l--) {
+            const int lo = T.lstart[l], m = T.lend[l] - T.lstart[l];
+            for_each(m, s, [=] __device__(int64_t i) {
+                const int b = lo + (int)i;
+                if (nch[b] > 0) {
+                    int t = 0;
+                    for (int j = 0; j < 4; j++) t += cp[chi[4 * b + j]];
+                    cp[b] = t;
+                }
+            });
+        }
+        // depth-first starts, root first
+        int *sp = start.get();
+        FMM_CUDA(cudaMemsetAsync(sp, 0, sizeof(int), s));
+        for (int l = 0; l < L; l++) {
+            const int lo = T.lstart[l], m = T.lend[l] - T.lstart[l];
+            for_each(m, s, [=] __device__(int64_t i) {
+                const int b = lo + (int)i;
+                if (nch[b] > 0) {
+                    int st = sp[b];
+                    for (int j = 0; j < 4; j++) {
+                        const int c = chi[4 * b + j];
+                        sp[c] = st;
+                        st += cp[c];
+                    }
+                }
+            });
+        }
+        int2 *sep = se.get();
+        for_each(nb, s, [=] __device__(int64_t i) {
+            sep[i] = make_int2(sp[i], sp[i] + cp[i]);
+        });
+        if (n == 0) return;
+        // stable sort of (leaf start, input index)
+        for_each(n, s, [=] __device__(int64_t i) {
+            kp[i] = (uint32_t)sp[kp[i]];
+            vp[i] = (uint32_t)i;
+        });
+        int bits = 1;
+        while ((1LL << bits) < (long long)n) bits++;
+        DevBuf<uint32_t> kt(n, s), vt(n, s);
+        radix_sort_pairs(kp, vp, kt.get(), vt.get(), n, bits, s);
+        FMM_CUDA(cudaMemcpyAsync(perm.get(), vp, (size_t)n * sizeof(int),
+                                 cudaMemcpyDeviceToDevice, s));
+    }
+};
+
+// Bounding box of sources and targets (pts_tree2d.c:493-513): exact min/max.
+__global__ void bbox_kernel(const double2 *__restrict__ a, int na,
+                            const double2 *__restrict__ b, int nb,
+                            double *__restrict__ out /* 4 per block */) {
+    double xmn = INFINITY, xmx = -INFINITY, ymn = INFINITY, ymx = -INFINITY;
+    const int64_t n = (int64_t)na + nb;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 p = i < na ? a[i] : b[i - na];
+        xmn = fmin(xmn, p.x);
+        xmx = fmax(xmx, p.x);
+        ymn = fmin(ymn, p.y);
+        ymx = fmax(ymx, p.y);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        xmn = fmin(xmn, __shfl_xor_sync(0xffffffffu, xmn, o));
+        xmx = fmax(xmx, __shfl_xor_sync(0xffffffffu, xmx, o));
+        ymn = fmin(ymn, __shfl_xor_sync(0xffffffffu, ymn, o));
+        ymx = fmax(ymx, __shfl_xor_sync(0xffffffffu, ymx, o));
+    }
+    __shared__ double sh[4][32];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        sh[0][w] = xmn;
+        sh[1][w] = xmx;
+        sh[2][w] = ymn;
+        sh[3][w] = ymx;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < (int)(blockDim.x >> 5); k++) {
+            xmn = fmin(xmn, sh[0][k]);
+            xmx = fmax(xmx, sh[1][k]);
+            ymn = fmin(ymn, sh[2][k]);
+            ymx = fmax(ymx, sh[3][k]);
+        }
+        out[4 * blockIdx.x + 0] = xmn;
+        out[4 * blockIdx.x + 1] = xmx;
+        out[4 * blockIdx.x + 2] = ymn;
+        out[4 * blockIdx.x + 3] = ymx;
+    }
+}
+
+}  // namespace
+
+void build_tree(const double2 *d_src, int ns, const double2 *d_targ, int nt,
+                int ndiv, int idivflag, int nlmax, cudaStream_t s, Tree &T) {
+    T = Tree();
+    Builder B(T, s);
+    // ---- root: bounding square of sources and targets ----
+    const int nblk = 2 * kNumSM;
+    DevBuf<double> part(4 * nblk, s);
+    bbox_kernel<<<nblk, 256, 0, s>>>(d_src, ns, d_targ, nt, part.get());
+    FMM_CHECK_LAUNCH();
+    std::vector<double> hp(4 * nblk);
+    FMM_CUDA(cudaMemcpyAsync(hp.data(), part.get(), hp.size() * sizeof(double),
+                             cudaMemcpyDeviceToHost, s));
+    FMM_CUDA(cudaStreamSynchronize(s));
+    double xmin = hp[0], xmax = hp[1], ymin = hp[2], ymax = hp[3];
+    for (int k = 1; k < nblk; k++) {
+        xmin = std::min(xmin, hp[4 * k]);
+        xmax = std::max(xmax, hp[4 * k + 1]);
+        ymin = std::min(ymin, hp[4 * k + 2]);
+        ymax = std::max(ymax, hp[4 * k + 3]);
+    }
+    double bs0 = xmax - xmin;
+    const double sizey = ymax - ymin;
+    if (sizey > bs0) bs0 = sizey;
+    T.boxsize.push_back(bs0);
+    B.cnt_s.alloc(1, s);
+    B.cnt_t.alloc(1, s);
+    B.ensure(1024);
+    T.nboxes = 1;
+    T.lstart.push_back(0);
+    T.lend.push_back(1);
+    {
+        double2 *cen = T.centers.get();
+        int *lev = T.level.get(), *par = T.parent.get(), *nch = T.nchild.get(),
+            *chi = T.child.get(), *cs = B.cnt_s.get(), *ct = B.cnt_t.get();
+        const double cx = (xmin + xmax) / 2, cy = (ymin + ymax) / 2;
+        for_each(1, s, [=] __device__(int64_t) {
+            cen[0] = make_double2(cx, cy);
+            lev[0] = 0;
+            par[0] = -1;
+            nch[0] = 0;
+            for (int j = 0; j < 4; j++) chi[j] = -1;
+            cs[0] = ns;
+            ct[0] = nt;
+        });
+    }
+    // ---- initial levelwise refinement (pts_tree2d.c:541-611) ----
+    DevBuf<int> pbs(std::max(ns, 1), s), pbt(std::max(nt, 1), s);
+    pbs.zero(s);
+    pbt.zero(s);
+    int ilev = 0;
+    for (ilev = 0; ilev <= nlmax - 1; ilev++) {
+        const int lo = T.lstart[ilev], hi = T.lend[ilev];
+        const int *cs = B.cnt_s.get(), *ct = B.cnt_t.get();
+        const int dflag = idivflag, nd = ndiv;
+        auto sel = [=] __device__(int b) {
+            const int nss = cs[b], ntt = ct[b];
+            const int nn = dflag == 0 ? nss : (dflag == 1 ? ntt : (nss > ntt ? nss : ntt));
+            return nn > nd;
+        };
+        T.boxsize.push_back(T.boxsize[ilev] / 2);
+        const int nb0 = T.nboxes;
+        // refine flags are re-derived from the counts inside refine_range;
+        // keep them for the point pass below.
+        DevBuf<int> f(hi - lo, s);
+        int *fp = f.get();
+        for_each(hi - lo, s, [=] __device__(int64_t i) { fp[i] = sel(lo + (int)i) ? 1 : 0; });
+        const int nref = B.refine_range(
+            lo, hi, ilev + 1, T.boxsize[ilev + 1],
+            [=] __device__(int b) { return fp[b - lo] != 0; }, false);
+        if (nref == 0) {
+            T.boxsize.pop_back();
+            break;
+        }
+        T.lstart.push_back(nb0);
+        T.lend.push_back(T.nboxes);
+        const double2 *cen = T.centers.get();
+        const int *chi = T.child.get();
+        int *csw = B.cnt_s.get(), *ctw = B.cnt_t.get();
+        int *ps = pbs.get(), *pt = pbt.get();
+        for_each(ns, s, [=] __device__(int64_t i) {
+            const int b = ps[i];
+            if (b < lo || b >= hi || !fp[b - lo]) return;
+            const int kb = chi[4 * b + child_digit(d_src[i], cen[b])];
+            ps[i] = kb;
+            atomicAdd(&csw[kb], 1);
+        });
+        for_each(nt, s, [=] __device__(int64_t i) {
+            const int b = pt[i];
+            if (b < lo || b >= hi || !fp[b - lo]) return;
+            const int kb = chi[4 * b + child_digit(d_targ[i], cen[b])];
+            pt[i] = kb;
+            atomicAdd(&ctw[kb], 1);
+        });
+    }
+    T.nlevels = ilev;
+    pbs.release();
+    pbt.release();
+    B.cnt_s.release();
+    B.cnt_t.release();
+    // ---- colleagues and level restriction ----
+    B.computecoll(0, T.nlevels);
+    if (T.nlevels >= 2) B.fix_lr();
+    // ---- point permutations ----
+    B.sort_points(d_src, ns, T.srcse, T.isrc);
+    B.sort_points(d_targ, nt, T.trgse, T.itarg);
+    T.d_boxsize.alloc(T.nlevels + 2, s);
+    std::vector<double> bsx(T.boxsize);
+    bsx.push_back(T.boxsize.back() / 2);
+    FMM_CUDA(cudaMemcpyAsync(T.d_boxsize.get(), bsx.data(),
+                             bsx.size() * sizeof(double),
+                             cudaMemcpyHostToDevice, s));
+    FMM_CUDA(cudaStreamSynchronize(s));
+}
+
+void compute_lists(Tree &T, cudaStream_t s) {
+    const int nb = T.nboxes;
+    T.nlist1.alloc(nb, s);
+    T.list1.alloc((size_t)kMaxList1 * nb, s);
+    T.nlist2.alloc(nb, s);
+    T.list2.alloc((size_t)kMaxList2 * nb, s);
+    T.nlist3.alloc(nb, s);
+    T.list3.alloc((size_t)kMaxList3 * nb, s);
+    T.nlist4.alloc(nb, s);
+    T.list4.alloc((size_t)kMaxList4 * nb, s);
+    const int L = T.nlevels;
+    std::vector<double> dcol(L + 2, 0.0), dl1(L + 2, 0.0);
+    for (int l = 0; l <= L; l++) {
+        dcol[l] = 1.05 * T.boxsize[l];
+        const double bsn = l + 1 <= L ? T.boxsize[l + 1] : T.boxsize[l] / 2;
+        dl1[l] = 1.05 * (T.boxsize[l] + bsn) / 2.0;
+    }
+    DevBuf<double> dd(2 * (L + 2), s);
+    std::vector<double> hd(dcol);
+    hd.insert(hd.end(), dl1.begin(), dl1.end());
+    FMM_CUDA(cudaMemcpyAsync(dd.get(), hd.data(), hd.size() * sizeof(double),
+                             cudaMemcpyHostToDevice, s));
+    DevBuf<int> err(1, s);
+    err.zero(s);
+    const double *dc = dd.get(), *d1 = dd.get() + (L + 2);
+    const int *lev = T.level.get(), *par = T.parent.get(),
+              *nch = T.nchild.get(), *chi = T.child.get(),
+              *nnb = T.nnbors.get(), *nbr = T.nbors.get();
+    const double2 *cen = T.centers.get();
+    int *n1 = T.nlist1.get(), *l1 = T.list1.get(), *n2 = T.nlist2.get(),
+        *l2 = T.list2.get(), *n3 = T.nlist3.get(), *l3 = T.list3.get(),
+        *n4 = T.nlist4.get(), *l4 = T.list4.get(), *ep = err.get();
+    for_each(nb, s, [=] __device__(int64_t i) {
+        const int b = (int)i;
+        const int l = lev[b];
+        int c1 = 0, c2 = 0, c3 = 0, c4 = 0;
+        if (l == 0) {
+            if (nch[0] == 0) l1[c1++] = 0;
+            n1[b] = c1;
+            n2[b] = 0;
+            n3[b] = 0;
+            n4[b] = 0;
+            return;
+        }
+        const double2 cb = cen[b];
+        const int dad = par[b];
+        // list 2: children of the dad's colleagues that are not adjacent
+        const double d = dc[l];
+        for (int k = 0; k < nnb[dad]; k++) {
+            const int jb = nbr[9 * dad + k];
+            for (int j = 0; j < nch[jb]; j++) {
+                const int kb = chi[4 * jb + j];
+                const double2 ck = cen[kb];
+                if (fabs(__dsub_rn(ck.x, cb.x)) >= d || fabs(__dsub_rn(ck.y, cb.y)) >= d) {
+                    if (c2 < kMaxList2) l2[kMaxList2 * b + c2] = kb;
+                    c2++;
+                }
+            }
+        }
+        // entries the reference appends while processing the coarser level:
+        // leaves among the dad's colleagues go to list 1 when they touch this
+        // box, else to list 4 (tree_routs2d.c:463-501), in box order.
+        if (l >= 2) {
+            int a1[9], a4[9], m1 = 0, m4 = 0;
+            const double dd2 = d1[l - 1];
+            for (int k = 0; k < nnb[dad]; k++) {
+                const int ib = nbr[9 * dad + k];
+                if (nch[ib] != 0) continue;
+                const double2 ci = cen[ib];
+                const double xd = fabs(__dsub_rn(cb.x, ci.x)), yd = fabs(__dsub_rn(cb.y, ci.y));
+                if (xd < dd2 && yd < dd2)
+                    a1[m1++] = ib;
+                else
+                    a4[m4++] = ib;
+            }
+            for (int x = 1; x < m1; x++)
+                for (int y = x; y > 0 && a1[y - 1] > a1[y]; y--) {
+                    int t = a1[y]; a1[y] = a1[y - 1]; a1[y - 1] = t;
+                }
+            for (int x = 1; x < m4; x++)
+                for (int y = x; y > 0 && a4[y - 1] > a4[y]; y--) {
+                    int t = a4[y]; a4[y] = a4[y - 1]; a4[y - 1] = t;
+                }
+            for (int x = 0; x < m1; x++) {
+                if (c1 < kMaxList1) l1[kMaxList1 * b + c1] = a1[x];
+                c1++;
+            }
+            for (int x = 0; x < m4; x++) {
+                if (c4 < kMaxList4) l4[kMaxList4 * b + c4] = a4[x];
+                c4++;
+            }
+        }
+        // lists 1 and 3 of a leaf
+        if (nch[b] == 0) {
+            const double dd3 = d1[l];
+            for (int k = 0; k < nnb[b]; k++) {
+                const int jb = nbr[9 * b + k];
+                if (nch[jb] == 0) {
+                    if (c1 < kMaxList1) l1[kMaxList1 * b + c1] = jb;
+                    c1++;
+                } else {
+                    for (int j = 0; j < nch[jb]; j++) {
+                        const int kb = chi[4 * jb + j];
+                        const double2 ck = cen[kb];
+                        const double xd = fabs(__dsub_rn(ck.x, cb.x)), yd = fabs(__dsub_rn(ck.y, cb.y));
+                        if (xd < dd3 && yd < dd3) {
+                            if (c1 < kMaxList1) l1[kMaxList1 * b + c1] = kb;
+                            c1++;
+                        } else {
+                            if (c3 < kMaxList3) l3[kMaxList3 * b + c3] = kb;
+                            c3++;
+                        }
+                    }
+                }
+            }
+        }
+        if (c1 > kMaxList1 || c2 > kMaxList2 || c3 > kMaxList3 || c4 > kMaxList4)
+            atomicExch(ep, 1);
+        n1[b] = c1 < kMaxList1 ? c1 : kMaxList1;
+        n2[b] = c2 < kMaxList2 ? c2 : kMaxList2;
+        n3[b] = c3 < kMaxList3 ? c3 : kMaxList3;
+        n4[b] = c4 < kMaxList4 ? c4 : kMaxList4;
+    });
+    if (read_scalar(err.get(), s) != 0)
+        throw FmmError(4, "interaction list exceeds the reference's capacity");
+}
+
+void export_reference_tree(const Tree &T, int ns, int nt, int *itree,
+                           int *iptr, double *centers, double *boxsize,
+                           int *isrc, int *isrcse, int *itarg, int *itargse,
+                           cudaStream_t s) {
+    const int nb = T.nboxes, L = T.nlevels;
+    auto d2h = [&](void *dst, const void *src, size_t bytes) {
+        if (bytes) FMM_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+    };
+    std::vector<int> lev(nb), par(nb), nch(nb), chi(4 * (size_t)nb), nnb(nb),
+        nbr(9 * (size_t)nb);
+    std::vector<int2> sse(nb), tse(nb);
+    std::vector<int> ps(std::max(ns, 0)), pt(std::max(nt, 0));
+    std::vector<double2> cen(nb);
+    d2h(lev.data(), T.level.get(), nb * sizeof(int));
+    d2h(par.data(), T.parent.get(), nb * sizeof(int));
+    d2h(nch.data(), T.nchild.get(), nb * sizeof(int));
+    d2h(chi.data(), T.child.get(), 4 * (size_t)nb * sizeof(int));
+    d2h(nnb.data(), T.nnbors.get(), nb * sizeof(int));
+    d2h(nbr.data(), T.nbors.get(), 9 * (size_t)nb * sizeof(int));
+    d2h(sse.data(), T.srcse.get(), nb * sizeof(int2));
+    d2h(tse.data(), T.trgse.get(), nb * sizeof(int2));
+    d2h(cen.data(), T.centers.get(), nb * sizeof(double2));
+    if (ns > 0) d2h(ps.data(), T.isrc.get(), ns * sizeof(int));
+    if (nt > 0) d2h(pt.data(), T.itarg.get(), nt * sizeof(int));
+    FMM_CUDA(cudaStreamSynchronize(s));
+    int ip[8];
+    ip[0] = 1;
+    ip[1] = 2 * (L + 1) + 1;
+    ip[2] = ip[1] + nb;
+    ip[3] = ip[2] + nb;
+    ip[4] = ip[3] + nb;
+    ip[5] = ip[4] + 4 * nb;
+    ip[6] = ip[5] + nb;
+    ip[7] = ip[6] + 9 * nb;
+    if (iptr)
+        for (int k = 0; k < 8; k++) iptr[k] = ip[k];
+    if (itree) {
+        for (int l = 0; l <= L; l++) {
+            itree[2 * l] = T.lstart[l] + 1;
+            itree[2 * l + 1] = T.lend[l];
+        }
+        auto one = [](int v) { return v < 0 ? -1 : v + 1; };
+        for (int b = 0; b < nb; b++) {
+            itree[ip[1] - 1 + b] = lev[b];
+            itree[ip[2] - 1 + b] = one(par[b]);
+            itree[ip[3] - 1 + b] = nch[b];
+            for (int j = 0; j < 4; j++) itree[ip[4] - 1 + 4 * b + j] = one(chi[4 * b + j]);
+            itree[ip[5] - 1 + b] = nnb[b];
+            for (int j = 0; j < 9; j++) itree[ip[6] - 1 + 9 * b + j] = one(nbr[9 * b + j]);
+        }
+    }
+    if (centers)
+        for (int b = 0; b < nb; b++) {
+            centers[2 * b] = cen[b].x;
+            centers[2 * b + 1] = cen[b].y;
+        }
+    if (boxsize)
+        for (int l = 0; l <= L; l++) boxsize[l] = T.boxsize[l];
+    if (isrc)
+        for (int i = 0; i < ns; i++) isrc[i] = ps[i] + 1;
+    if (itarg)
+        for (int i = 0; i < nt; i++) itarg[i] = pt[i] + 1;
+    if (isrcse)
+        for (int b = 0; b < nb; b++) {
+            isrcse[2 * b] = sse[b].x + 1;
+            isrcse[2 * b + 1] = sse[b].y;
+        }
+    if (itargse)
+        for (int b = 0; b < nb; b++) {
+            itargse[2 * b] = tse[b].x + 1;
+            itargse[2 * b + 1] = tse[b].y;
+        }
+}
+
+}  // namespace fmm2d

@@ -1,0 +1,45 @@
+"""The device-built quadtree is bit-identical to the reference's
+(pts_tree_mem/pts_tree_build/pts_tree_sort/computelists,
+src/common/pts_tree2d.f, src/common/tree_routs2d.f) on the same inputs:
+box arrays, centers, box sizes, point permutations and ranges; the
+interaction lists hold the same boxes in the same order."""
+import numpy as np
+import pytest
+
+import pointsets as ps
+import refimpl
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "uniform_200_100": lambda: (ps.uniform(200, 1), ps.uniform(100, 2), 15, 0),
+    "uniform_20000": lambda: (ps.uniform(20000, 3), None, 15, 0),
+    "blobs_30000_8000": lambda: (ps.blobs(30000, 4), ps.blobs(8000, 5), 10, 0),
+    "starfish_20000": lambda: (ps.starfish(20000, 0)[0],
+                               ps.near_curve_targets(20000, 6), 20, 0),
+    "grid_lines_65": lambda: (ps.grid_lines(64), ps.grid_lines(32), 8, 0),
+    "duplicates_deep": lambda: (ps.with_duplicates(1000, 7, 40), None, 15, 0),
+    "single_box": lambda: (ps.uniform(10, 8), ps.uniform(5, 9), 15, 0),
+    "targets_rule": lambda: (ps.uniform(3000, 10), ps.blobs(6000, 11), 12, 1),
+    "max_rule": lambda: (ps.blobs(3000, 12), ps.uniform(6000, 13), 12, 2),
+}
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_tree_bit_exact(name):
+    import fmm2d_c_translation_b200 as fm
+    src, trg, ndiv, idiv = CASES[name]()
+    got = fm.tree_build(src, trg, ndiv=ndiv, idivflag=idiv)
+    want = refimpl.ref_tree(src, trg, ndiv=ndiv, idivflag=idiv)
+    for k in ("nlevels", "nboxes", "ltree"):
+        assert got[k] == want[k], k
+    for k in ("iptr", "itree", "centers", "boxsize", "isrc", "isrcse",
+              "itarg", "itargse"):
+        np.testing.assert_array_equal(got[k], want[k], err_msg=k)
+    for k in (1, 2, 3, 4):
+        np.testing.assert_array_equal(got[f"nlist{k}"], want[f"nlist{k}"],
+                                      err_msg=f"nlist{k}")
+        m = min(got[f"list{k}"].shape[1], want[f"list{k}"].shape[1])
+        np.testing.assert_array_equal(got[f"list{k}"][:, :m],
+                                      want[f"list{k}"][:, :m],
+                                      err_msg=f"list{k}")
