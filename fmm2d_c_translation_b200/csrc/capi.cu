@@ -1,0 +1,319 @@
+// capi.cu -- the drop-in C ABI: the reference's gfortran-convention entry
+// points (lowercase name + '_', every argument by pointer, integer = int32,
+// complex*16 = interleaved doubles, column-major arrays) plus the one
+// bind(c) Helmholtz entry of include/fmm2d/helmholtz.h.
+//
+//   lfmm2d_{s,t,st}_{c,d,cd}_{p,g,h}_   src/laplace/lfmm2dwrap.f:31-1704
+//   cfmm2d_{s,t,st}_{c,d,cd}_{p,g,h}_   src/laplace/cfmm2dwrap.f:31-1659
+//   hfmm2d_{s,t,st}_{c,d,cd}_{p,g,h}_   src/helmholtz/hfmm2dwrap.f:41-1871
+//   lfmm2d_ / cfmm2d_ / hfmm2d_         guru drivers (lfmm2d.f:29, cfmm2d.f:23,
+//                                       hfmm2d.f:19)
+//   lfmm2d_ndiv_ / cfmm2d_ndiv_ / hfmm2d_ndiv_   MATLAB-path drivers
+//   hfmm2d_s_c_p                        src/helmholtz_c.f03:5-15
+//
+// Each wrapper fixes ifcharge / ifdipole / ifpgh / ifpghtarg with nd = 1,
+// nt = 0 for the sources-only forms and ifpgh = 0 for the targets-only
+// forms, exactly as the Fortran wrappers do, and runs the evaluation on
+// the GPU.  Arrays may be host or device memory (see engine.cuh).
+#include "engine.cuh"
+#include "runtime.cuh"
+
+using namespace fmm2d;
+
+typedef int32_t fint;
+
+namespace {
+
+FmmCall base_call(Kernel k, const double *eps, const double *zk, const fint *ns,
+                  const double *src) {
+    FmmCall c;
+    c.kernel = k;
+    c.eps = *eps;
+    if (zk) {
+        c.zk[0] = zk[0];
+        c.zk[1] = zk[1];
+    }
+    c.ns = *ns;
+    c.sources = src;
+    c.precision = current_precision();
+    return c;
+}
+
+void wrap(Kernel k, const double *eps, const double *zk, const fint *ns,
+          const double *src, const double *chg, const double *dip,
+          const double *dv, int ifc, int ifd, int pgh, double *pot,
+          double *grad, double *hess, int nt, const double *targ, int pght,
+          double *pt, double *gt, double *ht, fint *ier) {
+    FmmCall c = base_call(k, eps, zk, ns, src);
+    c.ifcharge = ifc;
+    c.charge = chg;
+    c.ifdipole = ifd;
+    c.dipstr = dip;
+    c.dipvec = dv;
+    c.ifpgh = pgh;
+    c.pot = pot;
+    c.grad = grad;
+    c.hess = hess;
+    c.nt = nt;
+    c.targ = targ;
+    c.ifpghtarg = pght;
+    c.pottarg = pt;
+    c.gradtarg = gt;
+    c.hesstarg = ht;
+    *ier = run_fmm(c);
+}
+
+}  // namespace
+
+typedef double cplx_t;  // complex*16 arrays are passed as interleaved doubles
+
+// source-strength argument lists: c = charge, d = dipole, cd = both
+#define SRC_c(V) const cplx_t *charge
+#define SRC_d(V) const cplx_t *dipstr V(const double *dipvec)
+#define SRC_cd(V) const cplx_t *charge, const cplx_t *dipstr V(const double *dipvec)
+#define PASS_c charge, nullptr, nullptr, 1, 0
+#define PASS_d nullptr, dipstr, DV(dipvec), 0, 1
+#define PASS_cd charge, dipstr, DV(dipvec), 1, 1
+#define OUT_S_p cplx_t *pot
+#define OUT_S_g cplx_t *pot, cplx_t *grad
+#define OUT_S_h cplx_t *pot, cplx_t *grad, cplx_t *hess
+#define OUT_T_p cplx_t *pottarg
+#define OUT_T_g cplx_t *pottarg, cplx_t *gradtarg
+#define OUT_T_h cplx_t *pottarg, cplx_t *gradtarg, cplx_t *hesstarg
+#define PS_p 1, pot, nullptr, nullptr
+#define PS_g 2, pot, grad, nullptr
+#define PS_h 3, pot, grad, hess
+#define PT_p 1, pottarg, nullptr, nullptr
+#define PT_g 2, pottarg, gradtarg, nullptr
+#define PT_h 3, pottarg, gradtarg, hesstarg
+#define WITH_DV(x) , x
+#define NO_DV(x)
+
+#define DV(x) x
+#define LWRAP(K, P)                                                           \
+    FMM_EXPORT void lfmm2d_s_##K##_##P##_(const double *eps, const fint *ns,  \
+                                          const double *sources,              \
+                                          SRC_##K(WITH_DV), OUT_S_##P,        \
+                                          fint *ier) {                        \
+        wrap(kLaplace, eps, nullptr, ns, sources, PASS_##K, PS_##P, 0,        \
+             nullptr, 0, nullptr, nullptr, nullptr, ier);                     \
+    }                                                                         \
+    FMM_EXPORT void lfmm2d_t_##K##_##P##_(                                    \
+        const double *eps, const fint *ns, const double *sources,             \
+        SRC_##K(WITH_DV), const fint *nt, const double *targ, OUT_T_##P,      \
+        fint *ier) {                                                          \
+        wrap(kLaplace, eps, nullptr, ns, sources, PASS_##K, 0, nullptr,       \
+             nullptr, nullptr, *nt, targ, PT_##P, ier);                       \
+    }                                                                         \
+    FMM_EXPORT void lfmm2d_st_##K##_##P##_(                                   \
+        const double *eps, const fint *ns, const double *sources,             \
+        SRC_##K(WITH_DV), OUT_S_##P, const fint *nt, const double *targ,      \
+        OUT_T_##P, fint *ier) {                                               \
+        wrap(kLaplace, eps, nullptr, ns, sources, PASS_##K, PS_##P, *nt,      \
+             targ, PT_##P, ier);                                              \
+    }
+
+#define HWRAP(K, P)                                                           \
+    FMM_EXPORT void hfmm2d_s_##K##_##P##_(                                    \
+        const double *eps, const cplx_t *zk, const fint *ns,                  \
+        const double *sources, SRC_##K(WITH_DV), OUT_S_##P, fint *ier) {      \
+        wrap(kHelmholtz, eps, zk, ns, sources, PASS_##K, PS_##P, 0, nullptr,  \
+             0, nullptr, nullptr, nullptr, ier);                              \
+    }                                                                         \
+    FMM_EXPORT void hfmm2d_t_##K##_##P##_(                                    \
+        const double *eps, const cplx_t *zk, const fint *ns,                  \
+        const double *sources, SRC_##K(WITH_DV), const fint *nt,              \
+        const double *targ, OUT_T_##P, fint *ier) {                           \
+        wrap(kHelmholtz, eps, zk, ns, sources, PASS_##K, 0, nullptr, nullptr, \
+             nullptr, *nt, targ, PT_##P, ier);                                \
+    }                                                                         \
+    FMM_EXPORT void hfmm2d_st_##K##_##P##_(                                   \
+        const double *eps, const cplx_t *zk, const fint *ns,                  \
+        const double *sources, SRC_##K(WITH_DV), OUT_S_##P, const fint *nt,   \
+        const double *targ, OUT_T_##P, fint *ier) {                           \
+        wrap(kHelmholtz, eps, zk, ns, sources, PASS_##K, PS_##P, *nt, targ,   \
+             PT_##P, ier);                                                    \
+    }
+
+LWRAP(c, p) LWRAP(c, g) LWRAP(c, h)
+LWRAP(d, p) LWRAP(d, g) LWRAP(d, h)
+LWRAP(cd, p) LWRAP(cd, g) LWRAP(cd, h)
+HWRAP(c, p) HWRAP(c, g) HWRAP(c, h)
+HWRAP(d, p) HWRAP(d, g) HWRAP(d, h)
+HWRAP(cd, p) HWRAP(cd, g) HWRAP(cd, h)
+#undef DV
+
+#define DV(x) nullptr
+#define CWRAP(K, P)                                                           \
+    FMM_EXPORT void cfmm2d_s_##K##_##P##_(const double *eps, const fint *ns,  \
+                                          const double *sources,              \
+                                          SRC_##K(NO_DV), OUT_S_##P,          \
+                                          fint *ier) {                        \
+        wrap(kCauchy, eps, nullptr, ns, sources, PASS_##K, PS_##P, 0,         \
+             nullptr, 0, nullptr, nullptr, nullptr, ier);                     \
+    }                                                                         \
+    FMM_EXPORT void cfmm2d_t_##K##_##P##_(                                    \
+        const double *eps, const fint *ns, const double *sources,             \
+        SRC_##K(NO_DV), const fint *nt, const double *targ, OUT_T_##P,        \
+        fint *ier) {                                                          \
+        wrap(kCauchy, eps, nullptr, ns, sources, PASS_##K, 0, nullptr,        \
+             nullptr, nullptr, *nt, targ, PT_##P, ier);                       \
+    }                                                                         \
+    FMM_EXPORT void cfmm2d_st_##K##_##P##_(                                   \
+        const double *eps, const fint *ns, const double *sources,             \
+        SRC_##K(NO_DV), OUT_S_##P, const fint *nt, const double *targ,        \
+        OUT_T_##P, fint *ier) {                                               \
+        wrap(kCauchy, eps, nullptr, ns, sources, PASS_##K, PS_##P, *nt, targ, \
+             PT_##P, ier);                                                    \
+    }
+
+CWRAP(c, p) CWRAP(c, g) CWRAP(c, h)
+CWRAP(d, p) CWRAP(d, g) CWRAP(d, h)
+CWRAP(cd, p) CWRAP(cd, g) CWRAP(cd, h)
+#undef DV
+
+// ---------------------------------------------------------------------------
+// Guru drivers.  `iper` is accepted and ignored (set to 0), as in the
+// reference (src/laplace/cfmm2d.f:150).
+// ---------------------------------------------------------------------------
+namespace {
+void guru(Kernel k, const fint *nd, const double *eps, const double *zk,
+          const fint *ns, const double *sources, const fint *ifcharge,
+          const double *charge, const fint *ifdipole, const double *dipstr,
+          const double *dipvec, fint *iper, const fint *ifpgh, double *pot,
+          double *grad, double *hess, const fint *nt, const double *targ,
+          const fint *ifpghtarg, double *pottarg, double *gradtarg,
+          double *hesstarg, const fint *ndiv, const fint *idivflag,
+          const fint *ifnear, double *timeinfo, fint *ier) {
+    FmmCall c = base_call(k, eps, zk, ns, sources);
+    c.nd = *nd;
+    c.ifcharge = *ifcharge;
+    c.charge = charge;
+    c.ifdipole = *ifdipole;
+    c.dipstr = dipstr;
+    c.dipvec = dipvec;
+    c.ifpgh = *ifpgh;
+    c.pot = pot;
+    c.grad = grad;
+    c.hess = hess;
+    c.nt = *nt;
+    c.targ = targ;
+    c.ifpghtarg = *ifpghtarg;
+    c.pottarg = pottarg;
+    c.gradtarg = gradtarg;
+    c.hesstarg = hesstarg;
+    if (ndiv) {
+        c.ndiv = *ndiv;
+        c.idivflag = *idivflag;
+    }
+    if (ifnear) c.ifnear = *ifnear;
+    c.timeinfo = timeinfo;
+    if (iper) *iper = 0;
+    *ier = run_fmm(c);
+}
+}  // namespace
+
+FMM_EXPORT void lfmm2d_(const fint *nd, const double *eps, const fint *ns,
+                        const double *sources, const fint *ifcharge,
+                        const cplx_t *charge, const fint *ifdipole,
+                        const cplx_t *dipstr, const double *dipvec, fint *iper,
+                        const fint *ifpgh, cplx_t *pot, cplx_t *grad,
+                        cplx_t *hess, const fint *nt, const double *targ,
+                        const fint *ifpghtarg, cplx_t *pottarg,
+                        cplx_t *gradtarg, cplx_t *hesstarg, fint *ier) {
+    guru(kLaplace, nd, eps, nullptr, ns, sources, ifcharge, charge, ifdipole,
+         dipstr, dipvec, iper, ifpgh, pot, grad, hess, nt, targ, ifpghtarg,
+         pottarg, gradtarg, hesstarg, nullptr, nullptr, nullptr, nullptr, ier);
+}
+
+FMM_EXPORT void cfmm2d_(const fint *nd, const double *eps, const fint *ns,
+                        const double *sources, const fint *ifcharge,
+                        const cplx_t *charge, const fint *ifdipole,
+                        const cplx_t *dipstr, fint *iper, const fint *ifpgh,
+                        cplx_t *pot, cplx_t *grad, cplx_t *hess, const fint *nt,
+                        const double *targ, const fint *ifpghtarg,
+                        cplx_t *pottarg, cplx_t *gradtarg, cplx_t *hesstarg,
+                        fint *ier) {
+    guru(kCauchy, nd, eps, nullptr, ns, sources, ifcharge, charge, ifdipole,
+         dipstr, nullptr, iper, ifpgh, pot, grad, hess, nt, targ, ifpghtarg,
+         pottarg, gradtarg, hesstarg, nullptr, nullptr, nullptr, nullptr, ier);
+}
+
+FMM_EXPORT void hfmm2d_(const fint *nd, const double *eps, const cplx_t *zk,
+                        const fint *ns, const double *sources,
+                        const fint *ifcharge, const cplx_t *charge,
+                        const fint *ifdipole, const cplx_t *dipstr,
+                        const double *dipvec, fint *iper, const fint *ifpgh,
+                        cplx_t *pot, cplx_t *grad, cplx_t *hess, const fint *nt,
+                        const double *targ, const fint *ifpghtarg,
+                        cplx_t *pottarg, cplx_t *gradtarg, cplx_t *hesstarg,
+                        fint *ier) {
+    guru(kHelmholtz, nd, eps, zk, ns, sources, ifcharge, charge, ifdipole,
+         dipstr, dipvec, iper, ifpgh, pot, grad, hess, nt, targ, ifpghtarg,
+         pottarg, gradtarg, hesstarg, nullptr, nullptr, nullptr, nullptr, ier);
+}
+
+FMM_EXPORT void lfmm2d_ndiv_(const fint *nd, const double *eps, const fint *ns,
+                             const double *sources, const fint *ifcharge,
+                             const cplx_t *charge, const fint *ifdipole,
+                             const cplx_t *dipstr, const double *dipvec,
+                             fint *iper, const fint *ifpgh, cplx_t *pot,
+                             cplx_t *grad, cplx_t *hess, const fint *nt,
+                             const double *targ, const fint *ifpghtarg,
+                             cplx_t *pottarg, cplx_t *gradtarg,
+                             cplx_t *hesstarg, const fint *ndiv,
+                             const fint *idivflag, const fint *ifnear,
+                             double *timeinfo, fint *ier) {
+    guru(kLaplace, nd, eps, nullptr, ns, sources, ifcharge, charge, ifdipole,
+         dipstr, dipvec, iper, ifpgh, pot, grad, hess, nt, targ, ifpghtarg,
+         pottarg, gradtarg, hesstarg, ndiv, idivflag, ifnear, timeinfo, ier);
+}
+
+FMM_EXPORT void cfmm2d_ndiv_(const fint *nd, const double *eps, const fint *ns,
+                             const double *sources, const fint *ifcharge,
+                             const cplx_t *charge, const fint *ifdipole,
+                             const cplx_t *dipstr, fint *iper,
+                             const fint *ifpgh, cplx_t *pot, cplx_t *grad,
+                             cplx_t *hess, const fint *nt, const double *targ,
+                             const fint *ifpghtarg, cplx_t *pottarg,
+                             cplx_t *gradtarg, cplx_t *hesstarg,
+                             const fint *ndiv, const fint *idivflag,
+                             const fint *ifnear, double *timeinfo, fint *ier) {
+    guru(kCauchy, nd, eps, nullptr, ns, sources, ifcharge, charge, ifdipole,
+         dipstr, nullptr, iper, ifpgh, pot, grad, hess, nt, targ, ifpghtarg,
+         pottarg, gradtarg, hesstarg, ndiv, idivflag, ifnear, timeinfo, ier);
+}
+
+FMM_EXPORT void hfmm2d_ndiv_(const fint *nd, const double *eps,
+                             const cplx_t *zk, const fint *ns,
+                             const double *sources, const fint *ifcharge,
+                             const cplx_t *charge, const fint *ifdipole,
+                             const cplx_t *dipstr, const double *dipvec,
+                             fint *iper, const fint *ifpgh, cplx_t *pot,
+                             cplx_t *grad, cplx_t *hess, const fint *nt,
+                             const double *targ, const fint *ifpghtarg,
+                             cplx_t *pottarg, cplx_t *gradtarg,
+                             cplx_t *hesstarg, const fint *ndiv,
+                             const fint *idivflag, const fint *ifnear,
+                             double *timeinfo, fint *ier) {
+    guru(kHelmholtz, nd, eps, zk, ns, sources, ifcharge, charge, ifdipole,
+         dipstr, dipvec, iper, ifpgh, pot, grad, hess, nt, targ, ifpghtarg,
+         pottarg, gradtarg, hesstarg, ndiv, idivflag, ifnear, timeinfo, ier);
+}
+
+// ---------------------------------------------------------------------------
+// Library knobs with no counterpart in the reference.
+// ---------------------------------------------------------------------------
+// Precision policy: 0 auto (mixed for eps >= 1e-6), 1 all-FP64, 2 mixed.
+FMM_EXPORT int fmm2d_b200_set_precision(int mode) {
+    if (mode < 0 || mode > 2) return 4;
+    set_precision(mode);
+    return 0;
+}
+
+// Host-only helpers (no device needed): the eps -> order and eps -> leaf
+// capacity rules the drivers use.
+FMM_EXPORT int fmm2d_b200_laplace_nterms(double eps) { return laplace_nterms(eps); }
+FMM_EXPORT int fmm2d_b200_leaf_capacity(double eps, int ns, int nt) {
+    return leaf_capacity(eps, ns, nt);
+}

@@ -1,0 +1,321 @@
+// engine.cu -- the driver layer of one evaluation (the reference's
+// lfmm2d / cfmm2d drivers, src/laplace/lfmm2d.f:29-225 and
+// c_translation/src/cfmm2d.c:1053-1401): inputs to the device, tree and
+// lists, gather into tree order (with the complex-Laplace two-channel
+// split), the FMM passes, scatter back to input order (with the channel
+// recombination), outputs to the caller.
+#include "engine.cuh"
+#include "laplace.cuh"
+#include "runtime.cuh"
+#include "tree.cuh"
+
+#include <atomic>
+#include <cmath>
+#include <stdlib.h>
+#include <string.h>
+
+namespace fmm2d {
+
+namespace {
+
+std::atomic<int> g_precision{-1};
+
+bool is_device_ptr(const void *p) {
+    if (!p) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Inputs of one call on the device: either the caller's own device arrays
+// or copies of its host arrays.
+template <class T>
+struct InBuf {
+    DevBuf<T> own;
+    const T *ptr = nullptr;
+    void set(const void *user, size_t n, bool on_dev, cudaStream_t s) {
+        if (!user || n == 0) {
+            ptr = nullptr;
+            return;
+        }
+        if (on_dev) {
+            ptr = static_cast<const T *>(user);
+            return;
+        }
+        own.alloc(n, s);
+        FMM_CUDA(cudaMemcpyAsync(own.get(), user, n * sizeof(T),
+                                 cudaMemcpyHostToDevice, s));
+        ptr = own.get();
+    }
+};
+
+// Outputs in the caller's layout on the device.
+struct OutBuf {
+    DevBuf<double2> own;
+    double2 *ptr = nullptr;
+    void *user = nullptr;
+    size_t n = 0;
+    bool on_dev = false;
+    void set(void *u, size_t count, bool dev, cudaStream_t s) {
+        user = u;
+        n = count;
+        on_dev = dev;
+        if (!u || !count) {
+            ptr = nullptr;
+            return;
+        }
+        if (dev) {
+            ptr = static_cast<double2 *>(u);
+        } else {
+            own.alloc(count, s);
+            ptr = own.get();
+        }
+    }
+    void flush(cudaStream_t s) {
+        if (ptr && !on_dev)
+            FMM_CUDA(cudaMemcpyAsync(user, ptr, n * sizeof(double2),
+                                     cudaMemcpyDeviceToHost, s));
+    }
+};
+
+}  // namespace
+
+int current_precision() {
+    int p = g_precision.load();
+    if (p < 0) {
+        const char *e = getenv("FMM2D_B200_PRECISION");
+        p = kPrecAuto;
+        if (e && !strcmp(e, "fp64")) p = kPrecFP64;
+        if (e && !strcmp(e, "mixed")) p = kPrecMixed;
+        g_precision.store(p);
+    }
+    return p;
+}
+
+void set_precision(int p) { g_precision.store(p); }
+
+// c_translation/src/l2dterms.c:26-67: the first j >= 2 with
+// |(sqrt(2)/2)^j / 1.5^(j+1)| < eps (j <= 100), else 1.
+int laplace_nterms(double eps) {
+    const double z2 = std::sqrt(2.0) / 2.0;
+    for (int j = 2; j <= 100; j++) {
+        const double t = std::pow(z2, (double)j) * (1.0 / std::pow(1.5, (double)(j + 1)));
+        if (t < eps) return j;
+    }
+    return 1;
+}
+
+// src/laplace/lndiv2d.f:1-39 (identical table in hndiv2d.c:15-48).
+int leaf_capacity(double eps, int ns, int nt) {
+    if (eps >= 0.5e0) return 3;
+    if (eps >= 0.5e-1) return 5;
+    if (eps >= 0.5e-2) return 8;
+    if (eps >= 0.5e-3) return 10;
+    if (eps >= 0.5e-6) return 15;
+    if (eps >= 0.5e-9) return 20;
+    if (eps >= 0.5e-12) return 25;
+    if (eps >= 0.5e-15) return 45;
+    return ns + nt;
+}
+
+namespace {
+
+void run_laplace_family(const FmmCall &c, CallCtx &ctx) {
+    cudaStream_t s = ctx.stream();
+    const bool lap = c.kernel == kLaplace;
+    const int nd = c.nd, ndc = lap ? 2 * nd : nd;
+    const int ns = c.ns, nt = c.nt;
+    const bool on_dev = is_device_ptr(c.sources);
+    // ---- inputs ----
+    InBuf<double2> src_in, trg_in, chg_in, dip_in;
+    InBuf<double> dv_in;
+    src_in.set(c.sources, ns, on_dev, s);
+    trg_in.set(nt > 0 ? c.targ : nullptr, nt, on_dev, s);
+    if (c.ifcharge) chg_in.set(c.charge, (size_t)nd * ns, on_dev, s);
+    if (c.ifdipole) {
+        dip_in.set(c.dipstr, (size_t)nd * ns, on_dev, s);
+        if (lap) dv_in.set(c.dipvec, (size_t)2 * nd * ns, on_dev, s);
+    }
+    // ---- tree ----
+    const int ndiv = c.ndiv >= 0 ? c.ndiv : leaf_capacity(c.eps, ns, nt);
+    const int idivflag = c.ndiv >= 0 ? c.idivflag : 0;
+    Tree T;
+    build_tree(src_in.ptr, ns, trg_in.ptr, nt, ndiv, idivflag, kMaxLevels, s, T);
+    compute_lists(T, s);
+    // ---- gather into tree order ----
+    DevBuf<double2> src_s(ns, s), trg_s(std::max(nt, 1), s);
+    DevBuf<double2> chg_s, dip_s;
+    {
+        const int *perm = T.isrc.get();
+        const double2 *sp = src_in.ptr;
+        double2 *so = src_s.get();
+        for_each(ns, s, [=] __device__(int64_t k) { so[k] = sp[perm[k]]; });
+        if (nt > 0) {
+            const int *pt = T.itarg.get();
+            const double2 *tp = trg_in.ptr;
+            double2 *to = trg_s.get();
+            for_each(nt, s, [=] __device__(int64_t k) { to[k] = tp[pt[k]]; });
+        }
+        if (c.ifcharge) {
+            chg_s.alloc((size_t)ns * ndc, s);
+            const double2 *q = chg_in.ptr;
+            double2 *qo = chg_s.get();
+            for_each(ns, s, [=] __device__(int64_t k) {
+                const int i = perm[k];
+                for (int j = 0; j < nd; j++) {
+                    const double2 v = q[(size_t)i * nd + j];
+                    if (lap) {
+                        // charge1(1:2, j, i) = (Re q, Im q)  (lfmm2d.f:141-147)
+                        qo[(size_t)k * ndc + 2 * j] = make_double2(v.x, 0.0);
+                        qo[(size_t)k * ndc + 2 * j + 1] = make_double2(v.y, 0.0);
+                    } else {
+                        qo[(size_t)k * ndc + j] = v;
+                    }
+                }
+            });
+        }
+        if (c.ifdipole) {
+            dip_s.alloc((size_t)ns * ndc, s);
+            const double2 *d = dip_in.ptr;
+            const double *dv = dv_in.ptr;
+            double2 *dout = dip_s.get();
+            for_each(ns, s, [=] __device__(int64_t k) {
+                const int i = perm[k];
+                for (int j = 0; j < nd; j++) {
+                    const double2 v = d[(size_t)i * nd + j];
+                    if (lap) {
+                        // dipstr1 = (Re d, Im d) * (-(v1 + i v2))  (lfmm2d.f:149-157)
+                        const double v1 = dv[((size_t)i * 2 + 0) * nd + j];
+                        const double v2 = dv[((size_t)i * 2 + 1) * nd + j];
+                        dout[(size_t)k * ndc + 2 * j] = make_double2(-v.x * v1, -v.x * v2);
+                        dout[(size_t)k * ndc + 2 * j + 1] = make_double2(-v.y * v1, -v.y * v2);
+                    } else {
+                        dout[(size_t)k * ndc + j] = v;
+                    }
+                }
+            });
+        }
+    }
+    src_in.own.release();
+    chg_in.own.release();
+    dip_in.own.release();
+    dv_in.own.release();
+    // ---- outputs in tree order ----
+    const int spgh = c.ifpgh, tpgh = nt > 0 ? c.ifpghtarg : 0;
+    DevBuf<double2> spot, sgrad, shess, tpot, tgrad, thess;
+    auto mk = [&](DevBuf<double2> &b, int n, bool need) {
+        if (need && n > 0) {
+            b.alloc((size_t)n * ndc, s);
+            b.zero(s);
+        }
+    };
+    mk(spot, ns, spgh >= 1);
+    mk(sgrad, ns, spgh >= 2);
+    mk(shess, ns, spgh >= 3);
+    mk(tpot, nt, tpgh >= 1);
+    mk(tgrad, nt, tpgh >= 2);
+    mk(thess, nt, tpgh >= 3);
+    CauchyProblem P;
+    P.ndc = ndc;
+    P.p = laplace_nterms(c.eps);
+    P.ifcharge = c.ifcharge;
+    P.ifdipole = c.ifdipole;
+    P.src = src_s.get();
+    P.charge = chg_s.get();
+    P.dipstr = dip_s.get();
+    P.sset.pos = src_s.get();
+    P.sset.se = T.srcse.get();
+    P.sset.n = ns;
+    P.sset.pgh = spgh;
+    P.sset.pot = spot.get();
+    P.sset.grad = sgrad.get();
+    P.sset.hess = shess.get();
+    P.tset.pos = trg_s.get();
+    P.tset.se = T.trgse.get();
+    P.tset.n = nt;
+    P.tset.pgh = tpgh;
+    P.tset.pot = tpot.get();
+    P.tset.grad = tgrad.get();
+    P.tset.hess = thess.get();
+    // thresh = boxsize(0) * 2^-51 (c_translation/src/cfmm2d.c:994)
+    P.thresh = T.boxsize[0] * std::ldexp(1.0, -51);
+    P.ifnear = c.ifnear;
+    cauchy_fmm(T, P, s);
+    // ---- back to input order, in the caller's layout ----
+    auto unsort = [&](int n, const int *perm, int pgh, const DevBuf<double2> &po,
+                      const DevBuf<double2> &gr, const DevBuf<double2> &he,
+                      double *upot, double *ugrad, double *uhess) {
+        if (pgh <= 0 || n <= 0) return;
+        const int gcomp = lap ? 2 : 1, hcomp = lap ? 3 : 1;
+        OutBuf op, og, oh;
+        op.set(upot, (size_t)nd * n, on_dev, s);
+        if (pgh >= 2) og.set(ugrad, (size_t)nd * gcomp * n, on_dev, s);
+        if (pgh >= 3) oh.set(uhess, (size_t)nd * hcomp * n, on_dev, s);
+        const double2 *P0 = po.get(), *G0 = gr.get(), *H0 = he.get();
+        double2 *up = op.ptr, *ug = og.ptr, *uh = oh.ptr;
+        for_each(n, s, [=] __device__(int64_t k) {
+            const int i = perm[k];
+            for (int j = 0; j < nd; j++) {
+                if (lap) {
+                    // lfmm2d.f:168-225: pot = Re pot1(1) + i Re pot1(2),
+                    // grad(1) = Re g1 + i Re g2, grad(2) = -Im g1 - i Im g2,
+                    // hess likewise with hess(3) = -hess(1).
+                    const size_t a = (size_t)k * ndc + 2 * j;
+                    const double2 p1 = P0[a], p2 = P0[a + 1];
+                    up[(size_t)i * nd + j] = make_double2(p1.x, p2.x);
+                    if (pgh >= 2) {
+                        const double2 g1 = G0[a], g2 = G0[a + 1];
+                        ug[((size_t)i * 2 + 0) * nd + j] = make_double2(g1.x, g2.x);
+                        ug[((size_t)i * 2 + 1) * nd + j] = make_double2(-g1.y, -g2.y);
+                    }
+                    if (pgh >= 3) {
+                        const double2 h1 = H0[a], h2 = H0[a + 1];
+                        uh[((size_t)i * 3 + 0) * nd + j] = make_double2(h1.x, h2.x);
+                        uh[((size_t)i * 3 + 1) * nd + j] = make_double2(-h1.y, -h2.y);
+                        uh[((size_t)i * 3 + 2) * nd + j] = make_double2(-h1.x, -h2.x);
+                    }
+                } else {
+                    const size_t a = (size_t)k * ndc + j, o = (size_t)i * nd + j;
+                    up[o] = P0[a];
+                    if (pgh >= 2) ug[o] = G0[a];
+                    if (pgh >= 3) uh[o] = H0[a];
+                }
+            }
+        });
+        op.flush(s);
+        og.flush(s);
+        oh.flush(s);
+        FMM_CUDA(cudaStreamSynchronize(s));
+    };
+    unsort(ns, T.isrc.get(), spgh, spot, sgrad, shess, c.pot, c.grad, c.hess);
+    unsort(nt, T.itarg.get(), tpgh, tpot, tgrad, thess, c.pottarg, c.gradtarg,
+           c.hesstarg);
+    if (c.timeinfo)
+        for (int k = 0; k < 8; k++) c.timeinfo[k] = 0.0;
+}
+
+}  // namespace
+
+int run_fmm(const FmmCall &c) {
+    return guarded([&] {
+        if (c.ns < 1) throw FmmError(4, "ns must be at least 1");
+        if (c.nt < 0) throw FmmError(4, "nt must be non-negative");
+        if (c.nd < 1) throw FmmError(4, "nd must be at least 1");
+        if (!c.ifcharge && !c.ifdipole)
+            throw FmmError(4, "at least one of ifcharge / ifdipole must be 1");
+        CallCtx ctx;
+        switch (c.kernel) {
+            case kLaplace:
+            case kCauchy:
+                run_laplace_family(c, ctx);
+                break;
+            default:
+                throw FmmError(4, "Helmholtz evaluation is not available yet");
+        }
+    });
+}
+
+}  // namespace fmm2d

@@ -1,0 +1,55 @@
+// engine.cuh -- one FMM evaluation from user arrays to user arrays.
+#pragma once
+
+#include "common.cuh"
+
+namespace fmm2d {
+
+enum Kernel { kLaplace = 0, kCauchy = 1, kHelmholtz = 2 };
+enum Precision { kPrecAuto = 0, kPrecFP64 = 1, kPrecMixed = 2 };
+
+// Arguments of the reference's guru drivers (lfmm2d / cfmm2d / hfmm2d and
+// their _ndiv forms).  Complex arrays are interleaved (re, im) doubles in
+// the reference's column-major layouts.  Pointers may be host memory
+// (pageable or pinned) or device memory of the current device; all
+// pointers of one call must be of the same kind.
+struct FmmCall {
+    Kernel kernel = kLaplace;
+    int nd = 1;
+    double eps = 1e-6;
+    double zk[2] = {0, 0};
+    int ns = 0;
+    const double *sources = nullptr;
+    int ifcharge = 0;
+    const double *charge = nullptr;
+    int ifdipole = 0;
+    const double *dipstr = nullptr;
+    const double *dipvec = nullptr;  // Laplace / Helmholtz only
+    int ifpgh = 0;
+    double *pot = nullptr, *grad = nullptr, *hess = nullptr;
+    int nt = 0;
+    const double *targ = nullptr;
+    int ifpghtarg = 0;
+    double *pottarg = nullptr, *gradtarg = nullptr, *hesstarg = nullptr;
+    int ndiv = -1;       // < 0: from eps (lndiv2d / hndiv2d)
+    int idivflag = 0;
+    int ifnear = 1;
+    double *timeinfo = nullptr;  // 8 entries, optional
+    int precision = kPrecAuto;
+};
+
+// Runs the evaluation on the calling thread's current device; returns the
+// reference's ier (0 ok, 4 failure) after recording any error message.
+int run_fmm(const FmmCall &c);
+
+// Expansion order of the Laplace FMM (l2dterms, c_translation/src/l2dterms.c).
+int laplace_nterms(double eps);
+// Leaf capacity (lndiv2d.f / hndiv2d.c).
+int leaf_capacity(double eps, int ns, int nt);
+
+// Process-wide precision policy (env FMM2D_B200_PRECISION=auto|fp64|mixed,
+// or fmm2d_b200_set_precision).
+int current_precision();
+void set_precision(int p);
+
+}  // namespace fmm2d

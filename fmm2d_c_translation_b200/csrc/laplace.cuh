@@ -1,0 +1,50 @@
+// laplace.cuh -- the Cauchy-kernel FMM passes over a device tree.
+//
+// Expansions are stored box-major: coefficient k of channel c of box b sits
+// at [b * stride + k * ndc + c] (double2), stride = (p + 1) * ndc, the
+// reference's mpole(nd, 0:nterms) per box (c_translation/src/laprouts2d.c:31).
+#pragma once
+
+#include "common.cuh"
+#include "tree.cuh"
+
+namespace fmm2d {
+
+// Sorted-order point data and outputs of one evaluation.
+struct PointSet {
+    const double2 *pos = nullptr;  // (x, y), sorted
+    const int2 *se = nullptr;      // per-box [start, end)
+    int n = 0;
+    int pgh = 0;                   // 0 none, 1 pot, 2 +grad, 3 +hess
+    double2 *pot = nullptr, *grad = nullptr, *hess = nullptr;  // [i*ndc + c]
+};
+
+struct CauchyProblem {
+    int ndc = 1;        // Cauchy channels
+    int p = 0;          // expansion order (nterms), same on every level
+    int ifcharge = 0, ifdipole = 0;
+    const double2 *src = nullptr;     // sorted sources
+    const double2 *charge = nullptr;  // [i*ndc + c], sorted
+    const double2 *dipstr = nullptr;  // [i*ndc + c], sorted
+    PointSet sset;                    // sources as targets
+    PointSet tset;                    // targets
+    double thresh = 0;                // near-field exclusion radius
+    int ifnear = 1;
+    double *timeinfo = nullptr;       // 8 phase times (s), optional
+};
+
+// Runs steps 1-8 of cfmm2dmain (src/laplace/cfmm2d.f:442-1340) on the
+// device.  Outputs in sset / tset must be zeroed by the caller.
+void cauchy_fmm(const Tree &T, const CauchyProblem &P, cudaStream_t s);
+
+// Direct sums over all sources for every point of `set` (the reference's
+// c2d_direct* kernels, src/laplace/cauchykernels2d.f).
+void cauchy_direct(const CauchyProblem &P, int ns, PointSet set,
+                   cudaStream_t s);
+
+// Binomial table C(l, m), l, m <= kLdc, built with the reference's Pascal
+// recurrence (init_carray, src/common/fmmcommon2d.f).
+constexpr int kLdc = 127;
+const double *device_binomials(cudaStream_t s);
+
+}  // namespace fmm2d
