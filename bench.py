@@ -1,0 +1,437 @@
+"""Benchmark of the B200 fmm2d evaluation path.
+
+Workload (default): Laplace ``lfmm2d_st_cd_g`` on 10^7 sources + 10^7
+targets uniform in [0,1]^2, complex charges and dipole strengths N(0,1),
+unit dipole vectors at angle U[0, 2pi), eps = 1e-6 -- seeded synthetic
+inputs of the shapes the reference's Laplace FMM is quoted on.
+
+One step = one full evaluation (tree, lists, all FMM passes, near field,
+outputs in input order) through the library's C ABI.
+  value  : points/s with inputs and outputs resident in HBM (the C ABI is
+           called with device pointers).
+  e2e    : points/s through the same C-ABI call with pinned HOST buffers;
+           host->device and device->host copies are inside the call.
+Timing: CUDA events on the stream the library runs on (set with
+fmm2d_b200_set_stream), W untimed warm-up steps, K timed steps bracketed
+by a barrier and cuda synchronize; inputs (0.8 GB) exceed the 126 MB L2.
+
+``--impl reference`` times the reference's own C translation (compiled
+from the reference sources into oracle/_ref/ by oracle/Makefile) on the
+host cores: each step runs one bounded sample of the same workload per
+host thread, concurrently.
+
+Multi-GPU (``torchrun --nproc-per-node N``): independent replicas, one
+full problem per GPU (the evaluation path does not shard), value = all
+points of all ranks / max step time over ranks.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "points/s Laplace FMM eps 1e-6 mixed vs FP64 plain, 1 B200; serving p50/p99 ms"
+P = ctypes.c_void_p
+NS_DEFAULT = 10_000_000
+NT_DEFAULT = 10_000_000
+
+
+def make_inputs(ns, nt, seed):
+    rng = np.random.default_rng(seed)
+    src = rng.random((ns, 2))
+    trg = rng.random((nt, 2))
+    q = rng.standard_normal(ns) + 1j * rng.standard_normal(ns)
+    d = rng.standard_normal(ns) + 1j * rng.standard_normal(ns)
+    th = rng.uniform(0.0, 2 * np.pi, ns)
+    v = np.stack([np.cos(th), np.sin(th)], axis=1)
+    return src, trg, q, d, v
+
+
+def read_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.out = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def parse_profile(s):
+    out = {}
+    for kv in s.split(";"):
+        if "=" in kv:
+            k, v = kv.split("=", 1)
+            out[k] = float(v)
+    return out
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def run_reference(args):
+    """The reference's C translation on the host cores."""
+    ws, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(REPO, "tests"))
+    import refimpl
+    if not refimpl.have_ref():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/libfmm2d_ref.so not built (reference sources absent at build time)"}))
+        return 0
+    R = refimpl.ref()
+    threads = args.cpu_threads or (os.cpu_count() or 1)
+    ns, nt = args.cpu_sample, args.cpu_sample
+    inputs = [make_inputs(ns, nt, 1000 + t) for t in range(threads)]
+    eps = ctypes.c_double(args.eps)
+
+    def one(t):
+        src, trg, q, d, v = inputs[t]
+        pot = np.zeros(ns, complex)
+        grad = np.zeros((ns, 2), complex)
+        pt = np.zeros(nt, complex)
+        gt = np.zeros((nt, 2), complex)
+        ier = ctypes.c_int(0)
+        R.lfmm2d_st_cd_g_(ctypes.byref(eps), ctypes.byref(ctypes.c_int(ns)),
+                          src.ctypes.data_as(P), q.ctypes.data_as(P),
+                          d.ctypes.data_as(P), v.ctypes.data_as(P),
+                          pot.ctypes.data_as(P), grad.ctypes.data_as(P),
+                          ctypes.byref(ctypes.c_int(nt)), trg.ctypes.data_as(P),
+                          pt.ctypes.data_as(P), gt.ctypes.data_as(P),
+                          ctypes.byref(ier))
+
+    def step():
+        ths = [threading.Thread(target=one, args=(t,)) for t in range(threads)]
+        t0 = time.perf_counter()
+        for th in ths:
+            th.start()
+        for th in ths:
+            th.join()
+        return time.perf_counter() - t0
+
+    for _ in range(args.warmup):
+        step()
+    times = [step() for _ in range(args.steps)]
+    tm = sum(times) / len(times)
+    value = threads * (ns + nt) / tm
+    sample = (f"{threads} concurrent lfmm2d_st_cd_g calls of {ns}+{nt} points "
+              f"(same distributions, eps={args.eps:g}) per step")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "points/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": tm * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "lfmm2d_st_cd_g uniform 1e7+1e7 eps 1e-6 (bounded CPU sample)",
+                   "precision": "fp64", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": "points/s", "cores": threads,
+                         "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def cpu_baseline_sample(args):
+    """A bounded run of the reference C translation (1 core per call, all
+    host threads concurrently) for the cpu_baseline field."""
+    sys.path.insert(0, os.path.join(REPO, "tests"))
+    import refimpl
+    if not refimpl.have_ref():
+        return None
+    R = refimpl.ref()
+    threads = args.cpu_threads or (os.cpu_count() or 1)
+    ns = nt = args.cpu_sample
+    inputs = [make_inputs(ns, nt, 2000 + t) for t in range(threads)]
+    eps = ctypes.c_double(args.eps)
+
+    def one(t):
+        src, trg, q, d, v = inputs[t]
+        outs = [np.zeros(ns, complex), np.zeros((ns, 2), complex),
+                np.zeros(nt, complex), np.zeros((nt, 2), complex)]
+        ier = ctypes.c_int(0)
+        R.lfmm2d_st_cd_g_(ctypes.byref(eps), ctypes.byref(ctypes.c_int(ns)),
+                          src.ctypes.data_as(P), q.ctypes.data_as(P),
+                          d.ctypes.data_as(P), v.ctypes.data_as(P),
+                          outs[0].ctypes.data_as(P), outs[1].ctypes.data_as(P),
+                          ctypes.byref(ctypes.c_int(nt)), trg.ctypes.data_as(P),
+                          outs[2].ctypes.data_as(P), outs[3].ctypes.data_as(P),
+                          ctypes.byref(ier))
+
+    ths = [threading.Thread(target=one, args=(t,)) for t in range(threads)]
+    t0 = time.perf_counter()
+    for th in ths:
+        th.start()
+    for th in ths:
+        th.join()
+    dt = time.perf_counter() - t0
+    sample = (f"{threads} concurrent reference lfmm2d_st_cd_g calls of "
+              f"{ns}+{nt} points, eps={args.eps:g}, {dt:.1f} s wall")
+    return {"value": threads * (ns + nt) / dt, "unit": "points/s",
+            "cores": threads, "kind": "reference", "sample": sample}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["auto", "fp64", "mixed"])
+    ap.add_argument("--ns", type=int, default=NS_DEFAULT)
+    ap.add_argument("--nt", type=int, default=NT_DEFAULT)
+    ap.add_argument("--eps", type=float, default=1e-6)
+    ap.add_argument("--cpu-sample", type=int, default=100_000)
+    ap.add_argument("--cpu-threads", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+    import fmm2d_c_translation_b200 as fm
+
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+
+    L = fm.lib()
+    L.fmm2d_b200_launch_count.restype = ctypes.c_ulonglong
+    L.fmm2d_b200_set_precision({"auto": 0, "fp64": 1, "mixed": 2}[args.precision])
+    stream = torch.cuda.current_stream()
+    L.fmm2d_b200_set_stream(ctypes.c_void_p(stream.cuda_stream))
+
+    ns, nt = args.ns, args.nt
+    src, trg, q, d, v = make_inputs(ns, nt, 7 + rank)
+    dev = torch.device("cuda", local)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a))
+    d_src, d_trg = t(src).to(dev), t(trg).to(dev)
+    d_q = t(q.view(np.float64)).to(dev)
+    d_d = t(d.view(np.float64)).to(dev)
+    d_v = t(v).to(dev)
+    d_pot = torch.zeros(2 * ns, dtype=torch.float64, device=dev)
+    d_grad = torch.zeros(4 * ns, dtype=torch.float64, device=dev)
+    d_pt = torch.zeros(2 * nt, dtype=torch.float64, device=dev)
+    d_gt = torch.zeros(4 * nt, dtype=torch.float64, device=dev)
+    eps = ctypes.c_double(args.eps)
+    c_ns, c_nt = ctypes.c_int(ns), ctypes.c_int(nt)
+    ier = ctypes.c_int(0)
+
+    def ptr(x):
+        return ctypes.c_void_p(x.data_ptr())
+
+    def call(a):
+        L.lfmm2d_st_cd_g_(ctypes.byref(eps), ctypes.byref(c_ns), ptr(a[0]),
+                          ptr(a[2]), ptr(a[3]), ptr(a[4]), ptr(a[5]),
+                          ptr(a[6]), ctypes.byref(c_nt), ptr(a[1]), ptr(a[7]),
+                          ptr(a[8]), ctypes.byref(ier))
+        if ier.value != 0:
+            raise RuntimeError("lfmm2d_st_cd_g_ failed: " + fm.last_error())
+
+    dev_args = (d_src, d_trg, d_q, d_d, d_v, d_pot, d_grad, d_pt, d_gt)
+
+    def timed(a, steps, profile=False):
+        L.fmm2d_b200_set_profiling(1 if profile else 0)
+        evs = []
+        prof = []
+        buf = ctypes.create_string_buffer(4096)
+        for _ in range(steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            call(a)
+            e1.record(stream)
+            evs.append((e0, e1))
+            if profile:
+                L.fmm2d_b200_last_profile(buf, len(buf))
+                prof.append(parse_profile(buf.value.decode()))
+        torch.cuda.synchronize()
+        L.fmm2d_b200_set_profiling(0)
+        return [a_.elapsed_time(b_) for a_, b_ in evs], prof
+
+    # ---- device-resident ----
+    for _ in range(args.warmup):
+        call(dev_args)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    torch.cuda.synchronize()
+    barrier()
+    n0 = L.fmm2d_b200_launch_count()
+    ms, prof = timed(dev_args, args.steps, profile=True)
+    n1 = L.fmm2d_b200_launch_count()
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    t_step = sum(ms) / len(ms)
+    if ws > 1:
+        tt = torch.tensor([t_step], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_step = float(tt.item())
+    value = ws * (ns + nt) / (t_step * 1e-3)
+
+    # ---- end to end through the C ABI with pinned host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        pin = lambda x: x.cpu().pin_memory()
+        h_args = tuple(pin(x) for x in dev_args)
+        for _ in range(max(1, args.warmup - 1)):
+            call(h_args)
+        torch.cuda.synchronize()
+        barrier()
+        ms_e2e, _ = timed(h_args, args.steps)
+        barrier()
+        te = sum(ms_e2e) / len(ms_e2e)
+        if ws > 1:
+            tt = torch.tensor([te], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            te = float(tt.item())
+        h2d = sum(x.numel() * 8 for x in h_args[:5])
+        d2h = sum(x.numel() * 8 for x in h_args[5:])
+        e2e = {"value": ws * (ns + nt) / (te * 1e-3), "unit": "points/s",
+               "ms_per_step": te, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h}
+
+    if ws > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+
+    # ---- roofline of the dominant phase ----
+    phases = {}
+    for p_ in prof:
+        for k, v_ in p_.items():
+            phases.setdefault(k, []).append(v_)
+    avg = {k: sum(v_) / len(v_) for k, v_ in phases.items()}
+    counts = {k[1:]: v_ for k, v_ in avg.items() if k.startswith("#")}
+    times = {k: v_ for k, v_ in avg.items() if not k.startswith("#")}
+    dom = max(times, key=times.get) if times else None
+    peaks, peak_kind = read_peaks()
+    ndc = counts.get("ndc", 2)
+    pterm = counts.get("nterms", 18)
+    roof = None
+    if dom == "m2l":
+        flops = 8.0 * counts.get("m2l_pairs", 0) * (pterm + 1) ** 2 * ndc
+        ach = flops / (times[dom] * 1e-3) / 1e12
+        pk = measure_fp64_peak(L)
+        roof = {"kernel": "m2l", "bound": "fp64", "achieved": ach, "peak": pk,
+                "unit": "TFLOP/s", "frac": ach / pk if pk else None, "traffic": None,
+                "peak_source": "FP64 FMA microbenchmark on this GPU (no tensor-core path in FP64 mode)"}
+    elif dom == "p2p":
+        pairs = counts.get("p2p_pairs_src", 0) + counts.get("p2p_pairs_targ", 0)
+        flops = pairs * (10 + ndc * 20)
+        ach = flops / (times[dom] * 1e-3) / 1e12
+        pk = measure_fp64_peak(L)
+        roof = {"kernel": "p2p", "bound": "fp64", "achieved": ach, "peak": pk,
+                "unit": "TFLOP/s", "frac": ach / pk if pk else None, "traffic": None,
+                "peak_source": "FP64 FMA microbenchmark on this GPU"}
+    elif dom is not None:
+        # memory-bound phases: compulsory bytes of the whole evaluation
+        byts = (ns * (16 + 16 * ndc * 2 + 16) + nt * 16 +
+                (ns + nt) * 16 * ndc * 3)
+        ach = byts / (times[dom] * 1e-3) / 1e9
+        pk = peaks.get("hbm_gbs")
+        roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": pk,
+                "unit": "GB/s", "frac": ach / pk if pk else None, "traffic": None}
+    if roof is not None:
+        roof["peak_file"] = peak_kind
+        roof["phase_ms"] = {k: round(v_, 4) for k, v_ in times.items()}
+        roof["counts"] = counts
+
+    cpu = None
+    if not args.no_cpu_baseline and ws == 1:
+        cpu = cpu_baseline_sample(args)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"lfmm2d_st_cd_g uniform {ns}+{nt} points eps {args.eps:g}",
+                   "precision": args.precision, "ns": ns, "nt": nt,
+                   "eps": args.eps, "parallelism": f"replicas{ws}",
+                   "l2": "inputs 0.8 GB > L2; no flush"},
+        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+        "gpu_launches": int(n1 - n0), "clocks": clk,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def measure_fp64_peak(L):
+    L.fmm2d_b200_fp64_peak_tflops.restype = ctypes.c_double
+    return L.fmm2d_b200_fp64_peak_tflops()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

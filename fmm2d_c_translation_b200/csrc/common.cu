@@ -1,6 +1,7 @@
 // common.cu -- device-wide exclusive scan and the library's last-error slot.
 #include "common.cuh"
 
+#include <atomic>
 #include <mutex>
 
 namespace fmm2d {
@@ -94,6 +95,79 @@ void scan_rec(const int *in, int *out, int64_t n, int *d_total,
     FMM_CHECK_LAUNCH();
 }
 }  // namespace
+
+namespace {
+std::atomic<unsigned long long> g_launches{0};
+std::atomic<int> g_profiling{0};
+
+struct ProfState {
+    std::vector<cudaEvent_t> pool;
+    std::vector<std::pair<std::string, int>> marks;  // phase name, event index
+    std::vector<std::pair<std::string, double>> result;  // phase, ms
+    std::vector<std::pair<std::string, double>> counts;
+    bool active = false;
+    cudaEvent_t ev(int i) {
+        while ((int)pool.size() <= i) {
+            cudaEvent_t e;
+            FMM_CUDA(cudaEventCreate(&e));
+            pool.push_back(e);
+        }
+        return pool[i];
+    }
+};
+thread_local ProfState g_prof;
+}  // namespace
+
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+unsigned long long launch_count() { return g_launches.load(); }
+void set_profiling(int on) { g_profiling.store(on); }
+bool profiling_enabled() { return g_profiling.load() != 0; }
+
+void prof_begin(cudaStream_t s) {
+    g_prof.marks.clear();
+    g_prof.counts.clear();
+    g_prof.active = profiling_enabled();
+    if (!g_prof.active) return;
+    g_prof.marks.push_back({"", 0});
+    FMM_CUDA(cudaEventRecord(g_prof.ev(0), s));
+}
+
+void prof_mark(const char *phase, cudaStream_t s) {
+    if (!g_prof.active) return;
+    const int i = (int)g_prof.marks.size();
+    g_prof.marks.push_back({phase, i});
+    FMM_CUDA(cudaEventRecord(g_prof.ev(i), s));
+}
+
+void prof_end(cudaStream_t s) {
+    if (!g_prof.active) return;
+    FMM_CUDA(cudaStreamSynchronize(s));
+    g_prof.result.clear();
+    for (size_t i = 1; i < g_prof.marks.size(); i++) {
+        float ms = 0;
+        FMM_CUDA(cudaEventElapsedTime(&ms, g_prof.ev((int)i - 1), g_prof.ev((int)i)));
+        bool merged = false;
+        for (auto &r : g_prof.result)
+            if (r.first == g_prof.marks[i].first) {
+                r.second += ms;
+                merged = true;
+            }
+        if (!merged) g_prof.result.push_back({g_prof.marks[i].first, (double)ms});
+    }
+    for (auto &c : g_prof.counts) g_prof.result.push_back({"#" + c.first, c.second});
+    g_prof.active = false;
+}
+
+void prof_set_count(const char *name, double value) {
+    if (g_prof.active) g_prof.counts.push_back({name, value});
+}
+
+// "name=value;" pairs of the last profiled call on this thread.
+std::string prof_report() {
+    std::string out;
+    for (auto &r : g_prof.result) out += r.first + "=" + std::to_string(r.second) + ";";
+    return out;
+}
 
 void set_last_error(const std::string &msg) {
     std::lock_guard<std::mutex> g(g_err_mu);

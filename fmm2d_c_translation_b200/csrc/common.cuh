@@ -43,7 +43,26 @@ void set_last_error(const std::string &msg);
         }                                                                     \
     } while (0)
 
-#define FMM_CHECK_LAUNCH() FMM_CUDA(cudaGetLastError())
+// Every kernel launch of the library is followed by FMM_CHECK_LAUNCH, which
+// also counts it (fmm2d_b200_launch_count).
+void note_launch();
+#define FMM_CHECK_LAUNCH()                 \
+    do {                                   \
+        FMM_CUDA(cudaGetLastError());      \
+        ::fmm2d::note_launch();            \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// Phase profiling: when enabled, entry points record a CUDA event on their
+// stream at every phase boundary; the per-phase device times and the work
+// counts of the last profiled call on this thread are kept for
+// fmm2d_b200_last_profile().
+// ---------------------------------------------------------------------------
+bool profiling_enabled();
+void prof_begin(cudaStream_t s);
+void prof_mark(const char *phase, cudaStream_t s);
+void prof_end(cudaStream_t s);
+void prof_set_count(const char *name, double value);
 
 // ---------------------------------------------------------------------------
 // Device buffers: stream-ordered allocations from the device's default pool.

@@ -129,6 +129,7 @@ void run_laplace_family(const FmmCall &c, CallCtx &ctx) {
     const int nd = c.nd, ndc = lap ? 2 * nd : nd;
     const int ns = c.ns, nt = c.nt;
     const bool on_dev = is_device_ptr(c.sources);
+    prof_begin(s);
     // ---- inputs ----
     InBuf<double2> src_in, trg_in, chg_in, dip_in;
     InBuf<double> dv_in;
@@ -139,12 +140,15 @@ void run_laplace_family(const FmmCall &c, CallCtx &ctx) {
         dip_in.set(c.dipstr, (size_t)nd * ns, on_dev, s);
         if (lap) dv_in.set(c.dipvec, (size_t)2 * nd * ns, on_dev, s);
     }
+    prof_mark("h2d", s);
     // ---- tree ----
     const int ndiv = c.ndiv >= 0 ? c.ndiv : leaf_capacity(c.eps, ns, nt);
     const int idivflag = c.ndiv >= 0 ? c.idivflag : 0;
     Tree T;
     build_tree(src_in.ptr, ns, trg_in.ptr, nt, ndiv, idivflag, kMaxLevels, s, T);
+    prof_mark("tree", s);
     compute_lists(T, s);
+    prof_mark("lists", s);
     // ---- gather into tree order ----
     DevBuf<double2> src_s(ns, s), trg_s(std::max(nt, 1), s);
     DevBuf<double2> chg_s, dip_s;
@@ -199,6 +203,7 @@ void run_laplace_family(const FmmCall &c, CallCtx &ctx) {
             });
         }
     }
+    prof_mark("gather", s);
     src_in.own.release();
     chg_in.own.release();
     dip_in.own.release();
@@ -293,6 +298,8 @@ void run_laplace_family(const FmmCall &c, CallCtx &ctx) {
     unsort(ns, T.isrc.get(), spgh, spot, sgrad, shess, c.pot, c.grad, c.hess);
     unsort(nt, T.itarg.get(), tpgh, tpot, tgrad, thess, c.pottarg, c.gradtarg,
            c.hesstarg);
+    prof_mark("scatter_d2h", s);
+    prof_end(s);
     if (c.timeinfo)
         for (int k = 0; k < 8; k++) c.timeinfo[k] = 0.0;
 }

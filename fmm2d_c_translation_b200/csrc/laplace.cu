@@ -704,6 +704,7 @@ void cauchy_fmm_chunk(const Tree &T, const CauchyProblem &P, int c0,
             P.ifdipole, P.ndc, c0, p, loc);
         FMM_CHECK_LAUNCH();
     }
+    prof_mark("p2m_p2l", s);
     // step 3: M2M, finest parents first
     for (int l = L - 1; l >= 1; l--) {
         const int lo = T.lstart[l], hi = T.lend[l];
@@ -713,6 +714,7 @@ void cauchy_fmm_chunk(const Tree &T, const CauchyProblem &P, int c0,
             binom, mp);
         FMM_CHECK_LAUNCH();
     }
+    prof_mark("m2m", s);
     // step 4: M2L over list 2, per level
     const size_t sh_m2l = (size_t)(((p + 1) * (p + 1) + 1) & ~1) * sizeof(double) + sh_exp;
     FMM_CUDA(cudaFuncSetAttribute(m2l_kernel<CH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -724,6 +726,7 @@ void cauchy_fmm_chunk(const Tree &T, const CauchyProblem &P, int c0,
             T.boxsize[l], P.ndc, c0, p, binom, mp, loc);
         FMM_CHECK_LAUNCH();
     }
+    prof_mark("m2l", s);
     // step 5: L2L, coarsest parents first
     for (int l = 1; l <= L - 1; l++) {
         const int lo = T.lstart[l + 1], hi = T.lend[l + 1];
@@ -732,6 +735,7 @@ void cauchy_fmm_chunk(const Tree &T, const CauchyProblem &P, int c0,
             T.boxsize[l + 1], P.ndc, c0, p, binom, loc);
         FMM_CHECK_LAUNCH();
     }
+    prof_mark("l2l", s);
     // steps 6-7: list-3 multipoles and local expansions at the points
     for (const PointSet *set : {&P.tset, &P.sset}) {
         if (set->pgh <= 0 || set->n <= 0) continue;
@@ -740,6 +744,7 @@ void cauchy_fmm_chunk(const Tree &T, const CauchyProblem &P, int c0,
             T.nlist3.get(), T.list3.get(), *set, P.ndc, c0, p, L, mp, loc);
         FMM_CHECK_LAUNCH();
     }
+    prof_mark("m2p_l2p", s);
     // step 8: near field over list 1 (leaves, then any non-leaf box that
     // holds list-1 entries, so that no two warps write the same point)
     if (P.ifnear) {
@@ -750,6 +755,41 @@ void cauchy_fmm_chunk(const Tree &T, const CauchyProblem &P, int c0,
             launch_p2p<CH>(T, P, *set, c0, th2, 0, nb, 0, s);
         }
     }
+    prof_mark("p2p", s);
+}
+
+// Work counts of one evaluation for the roofline: list-2 pairs translated
+// (boxes passing the step-4 test) and near-field point pairs.
+void count_work(const Tree &T, const CauchyProblem &P, cudaStream_t s) {
+    DevBuf<unsigned long long> cnt(3, s);
+    cnt.zero(s);
+    unsigned long long *c = cnt.get();
+    const EvalCounts ec{T.srcse.get(), T.trgse.get(), P.sset.pgh, P.tset.pgh};
+    const int *lev = T.level.get(), *n1 = T.nlist1.get(), *l1 = T.list1.get(),
+              *n2 = T.nlist2.get();
+    const int2 *sse = T.srcse.get(), *tse = T.trgse.get();
+    const int spgh = P.sset.pgh, tpgh = P.tset.pgh;
+    for_each(T.nboxes, s, [=] __device__(int64_t i) {
+        const int b = (int)i;
+        if (lev[b] >= 2 && ec.npts(b) > 0 && n2[b] > 0)
+            atomicAdd(&c[0], (unsigned long long)n2[b]);
+        if (n1[b] > 0) {
+            unsigned long long ns_ = 0;
+            for (int e = 0; e < n1[b]; e++) ns_ += count(sse, l1[kMaxList1 * b + e]);
+            if (spgh > 0) atomicAdd(&c[1], ns_ * (unsigned long long)count(sse, b));
+            if (tpgh > 0) atomicAdd(&c[2], ns_ * (unsigned long long)count(tse, b));
+        }
+    });
+    unsigned long long h[3];
+    FMM_CUDA(cudaMemcpyAsync(h, c, sizeof(h), cudaMemcpyDeviceToHost, s));
+    FMM_CUDA(cudaStreamSynchronize(s));
+    prof_set_count("m2l_pairs", (double)h[0]);
+    prof_set_count("p2p_pairs_src", (double)h[1]);
+    prof_set_count("p2p_pairs_targ", (double)h[2]);
+    prof_set_count("nterms", (double)P.p);
+    prof_set_count("nboxes", (double)T.nboxes);
+    prof_set_count("nlevels", (double)T.nlevels);
+    prof_set_count("ndc", (double)P.ndc);
 }
 
 }  // namespace
@@ -781,6 +821,7 @@ const double *device_binomials(cudaStream_t s) {
 }
 
 void cauchy_fmm(const Tree &T, const CauchyProblem &P, cudaStream_t s) {
+    if (profiling_enabled()) count_work(T, P, s);
     if (2 * P.p > kLdc)
         throw FmmError(4, "expansion order above the supported maximum (64)");
     const double *binom = device_binomials(s);
@@ -788,6 +829,7 @@ void cauchy_fmm(const Tree &T, const CauchyProblem &P, cudaStream_t s) {
     DevBuf<double2> mp(nexp, s), loc(nexp, s);
     mp.zero(s);
     loc.zero(s);
+    prof_mark("fmm_setup", s);
     for (int c0 = 0; c0 < P.ndc; c0 += 2) {
         if (P.ndc - c0 >= 2)
             cauchy_fmm_chunk<2>(T, P, c0, binom, mp.get(), loc.get(), s);

@@ -27,14 +27,28 @@ void ensure_pool(int dev) {
 // One non-blocking stream per (host thread, device), created on first use and
 // kept for the life of the thread, so that buffers owned by long-lived
 // objects (tree handles) always free on a live stream.
+namespace {
+thread_local cudaStream_t g_user_stream = nullptr;
+thread_local bool g_user_stream_set = false;
+}  // namespace
+
 CallCtx::CallCtx() : dev_(0), s_(nullptr) {
     static thread_local cudaStream_t streams[64];
     FMM_CUDA(cudaGetDevice(&dev_));
     if (dev_ < 0 || dev_ >= 64) throw FmmError(4, "device index out of range");
     ensure_pool(dev_);
+    if (g_user_stream_set) {
+        s_ = g_user_stream;
+        return;
+    }
     if (!streams[dev_])
         FMM_CUDA(cudaStreamCreateWithFlags(&streams[dev_], cudaStreamNonBlocking));
     s_ = streams[dev_];
+}
+
+void set_user_stream(cudaStream_t s, bool on) {
+    g_user_stream = s;
+    g_user_stream_set = on;
 }
 
 CallCtx::~CallCtx() {
@@ -53,6 +67,39 @@ FMM_EXPORT const char *fmm2d_b200_version(void) { return "fmm2d-b200 0.1"; }
 // Copies the message of the last failed call (any thread) into buf.
 FMM_EXPORT int fmm2d_b200_last_error(char *buf, int len) {
     std::string m = get_last_error();
+    if (buf && len > 0) {
+        strncpy(buf, m.c_str(), (size_t)len - 1);
+        buf[len - 1] = 0;
+    }
+    return (int)m.size();
+}
+
+// Makes the calling thread's subsequent calls run on `stream` (a
+// cudaStream_t of the current device; 0 = legacy default stream).  Calls
+// still return only after their work on that stream has completed.
+FMM_EXPORT int fmm2d_b200_set_stream(void *stream) {
+    set_user_stream((cudaStream_t)stream, true);
+    return 0;
+}
+
+// Back to the library's own per-thread stream.
+FMM_EXPORT int fmm2d_b200_reset_stream(void) {
+    set_user_stream(nullptr, false);
+    return 0;
+}
+
+// Number of kernels the library has launched in this process.
+FMM_EXPORT unsigned long long fmm2d_b200_launch_count(void) { return launch_count(); }
+
+// Phase profiling of subsequent calls (CUDA events on the call's stream).
+FMM_EXPORT int fmm2d_b200_set_profiling(int on) {
+    set_profiling(on);
+    return 0;
+}
+
+// "phase=ms;...;#count=value;" of the last profiled call on this thread.
+FMM_EXPORT int fmm2d_b200_last_profile(char *buf, int len) {
+    std::string m = prof_report();
     if (buf && len > 0) {
         strncpy(buf, m.c_str(), (size_t)len - 1);
         buf[len - 1] = 0;

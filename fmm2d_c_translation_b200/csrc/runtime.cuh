@@ -15,6 +15,10 @@
 namespace fmm2d {
 
 std::string get_last_error();
+std::string prof_report();
+unsigned long long launch_count();
+void set_profiling(int on);
+void set_user_stream(cudaStream_t s, bool on);
 
 class CallCtx {
   public:
