@@ -1,0 +1,694 @@
+/*
+ * fmm2d_b200.h -- C ABI of libfmm2d_b200.so, the B200 evaluation path of
+ * fmm2d (complex-Laplace, Cauchy and Helmholtz FMMs in two dimensions).
+ *
+ * The first group of entry points replaces the reference library's own
+ * symbols one for one: same names (gfortran convention: lowercase + '_'),
+ * same arguments in the same order, every argument by pointer, Fortran
+ * integer = int32_t, complex*16 = double _Complex (interleaved re, im),
+ * arrays column-major exactly as the reference documents them.  A program
+ * linked against the reference library links against this one unchanged.
+ * Each declaration cites the reference interface it replaces.
+ *
+ * Semantics follow the reference: outputs are overwritten (not
+ * accumulated) in input order; ier = 0 on success, 4 on failure (the only
+ * code the reference reports, src/helmholtz/hfmm2d.f:374-381); the message
+ * of a failure is available from fmm2d_b200_last_error().  Arrays may be
+ * host memory (pageable or pinned) or device memory of the calling
+ * thread's current CUDA device; all arrays of one call must be of the same
+ * kind.  Calls are synchronous and may be made concurrently from several
+ * host threads.
+ *
+ * The second group (fmm2d_b200_*) has no counterpart in the reference:
+ * library-specific controls, inspection and measurement helpers.
+ */
+#ifndef FMM2D_B200_H
+#define FMM2D_B200_H
+
+#include <stdint.h>
+#ifdef __cplusplus
+/* C++ callers pass complex arrays as double * (interleaved re, im) */
+#define _Complex
+extern "C" {
+#endif
+
+/* ===================================================================== */
+/* Flag wrappers: {l,c,h}fmm2d_{s,t,st}_{c,d,cd}_{p,g,h}_                 */
+/*   s / t / st : evaluate at sources, at targets, at both               */
+/*   c / d / cd : charges, dipoles, both                                 */
+/*   p / g / h  : potential, + gradient, + Hessian                       */
+/* lfmm2d: grad(2,n), hess(3,n); cfmm2d: grad(n), hess(n) (d/dz, d2/dz2);  */
+/* hfmm2d: grad(2,n), hess(3,n) and the Helmholtz parameter zk.          */
+/* ===================================================================== */
+/* src/laplace/lfmm2dwrap.f:31 */
+void lfmm2d_s_c_p_(const double *eps, const int32_t *ns,
+                   const double *sources, const double _Complex *charge,
+                   double _Complex *pot, int32_t *ier);
+/* src/laplace/lfmm2dwrap.f:93 */
+void lfmm2d_s_c_g_(const double *eps, const int32_t *ns,
+                   const double *sources, const double _Complex *charge,
+                   double _Complex *pot, double _Complex *grad, int32_t *ier);
+/* src/laplace/lfmm2dwrap.f:156 */
+void lfmm2d_s_c_h_(const double *eps, const int32_t *ns,
+                   const double *sources, const double _Complex *charge,
+                   double _Complex *pot, double _Complex *grad,
+                   double _Complex *hess, int32_t *ier);
+/* src/laplace/lfmm2dwrap.f:217 */
+void lfmm2d_s_d_p_(const double *eps, const int32_t *ns,
+                   const double *sources, const double _Complex *dipstr,
+                   const double *dipvec, double _Complex *pot, int32_t *ier);
+/* src/laplace/lfmm2dwrap.f:280 */
+void lfmm2d_s_d_g_(const double *eps, const int32_t *ns,
+                   const double *sources, const double _Complex *dipstr,
+                   const double *dipvec, double _Complex *pot,
+                   double _Complex *grad, int32_t *ier);
+/* src/laplace/lfmm2dwrap.f:344 */
+void lfmm2d_s_d_h_(const double *eps, const int32_t *ns,
+                   const double *sources, const double _Complex *dipstr,
+                   const double *dipvec, double _Complex *pot,
+                   double _Complex *grad, double _Complex *hess,
+                   int32_t *ier);
+/* src/laplace/lfmm2dwrap.f:406 */
+void lfmm2d_s_cd_p_(const double *eps, const int32_t *ns,
+                    const double *sources, const double _Complex *charge,
+                    const double _Complex *dipstr, const double *dipvec,
+                    double _Complex *pot, int32_t *ier);
+/* src/laplace/lfmm2dwrap.f:468 */
+void lfmm2d_s_cd_g_(const double *eps, const int32_t *ns,
+                    const double *sources, const double _Complex *charge,
+                    const double _Complex *dipstr, const double *dipvec,
+                    double _Complex *pot, double _Complex *grad,
+                    int32_t *ier);
+/* src/laplace/lfmm2dwrap.f:531 */
+void lfmm2d_s_cd_h_(const double *eps, const int32_t *ns,
+                    const double *sources, const double _Complex *charge,
+                    const double _Complex *dipstr, const double *dipvec,
+                    double _Complex *pot, double _Complex *grad,
+                    double _Complex *hess, int32_t *ier);
+/* src/laplace/lfmm2dwrap.f:594 */
+void lfmm2d_t_c_p_(const double *eps, const int32_t *ns,
+                   const double *sources, const double _Complex *charge,
+                   const int32_t *nt, const double *targ,
+                   double _Complex *pottarg, int32_t *ier);
+/* src/laplace/lfmm2dwrap.f:654 */
+void lfmm2d_t_c_g_(const double *eps, const int32_t *ns,
+                   const double *sources, const double _Complex *charge,
+                   const int32_t *nt, const double *targ,
+                   double _Complex *pottarg, double _Complex *gradtarg,
+                   int32_t *ier);
+/* src/laplace/lfmm2dwrap.f:715 */
+void lfmm2d_t_c_h_(const double *eps, const int32_t *ns,
+                   const double *sources, const double _Complex *charge,
+                   const int32_t *nt, const double *targ,
+                   double _Complex *pottarg, double _Complex *gradtarg,
+                   double _Complex *hesstarg, int32_t *ier);
+/* src/laplace/lfmm2dwrap.f:775 */
+void lfmm2d_t_d_p_(const double *eps, const int32_t *ns,
+                   const double *sources, const double _Complex *dipstr,
+                   const double *dipvec, const int32_t *nt,
+                   const double *targ, double _Complex *pottarg,
+                   int32_t *ier);
+/* src/laplace/lfmm2dwrap.f:836 */
+void lfmm2d_t_d_g_(const double *eps, const int32_t *ns,
+                   const double *sources, const double _Complex *dipstr,
+                   const double *dipvec, const int32_t *nt,
+                   const double *targ, double _Complex *pottarg,
+                   double _Complex *gradtarg, int32_t *ier);
+/* src/laplace/lfmm2dwrap.f:898 */
+void lfmm2d_t_d_h_(const double *eps, const int32_t *ns,
+                   const double *sources, const double _Complex *dipstr,
+                   const double *dipvec, const int32_t *nt,
+                   const double *targ, double _Complex *pottarg,
+                   double _Complex *gradtarg, double _Complex *hesstarg,
+                   int32_t *ier);
+/* src/laplace/lfmm2dwrap.f:959 */
+void lfmm2d_t_cd_p_(const double *eps, const int32_t *ns,
+                    const double *sources, const double _Complex *charge,
+                    const double _Complex *dipstr, const double *dipvec,
+                    const int32_t *nt, const double *targ,
+                    double _Complex *pottarg, int32_t *ier);
+/* src/laplace/lfmm2dwrap.f:1019 */
+void lfmm2d_t_cd_g_(const double *eps, const int32_t *ns,
+                    const double *sources, const double _Complex *charge,
+                    const double _Complex *dipstr, const double *dipvec,
+                    const int32_t *nt, const double *targ,
+                    double _Complex *pottarg, double _Complex *gradtarg,
+                    int32_t *ier);
+/* src/laplace/lfmm2dwrap.f:1080 */
+void lfmm2d_t_cd_h_(const double *eps, const int32_t *ns,
+                    const double *sources, const double _Complex *charge,
+                    const double _Complex *dipstr, const double *dipvec,
+                    const int32_t *nt, const double *targ,
+                    double _Complex *pottarg, double _Complex *gradtarg,
+                    double _Complex *hesstarg, int32_t *ier);
+/* src/laplace/lfmm2dwrap.f:1143 */
+void lfmm2d_st_c_p_(const double *eps, const int32_t *ns,
+                    const double *sources, const double _Complex *charge,
+                    double _Complex *pot, const int32_t *nt,
+                    const double *targ, double _Complex *pottarg,
+                    int32_t *ier);
+/* src/laplace/lfmm2dwrap.f:1204 */
+void lfmm2d_st_c_g_(const double *eps, const int32_t *ns,
+                    const double *sources, const double _Complex *charge,
+                    double _Complex *pot, double _Complex *grad,
+                    const int32_t *nt, const double *targ,
+                    double _Complex *pottarg, double _Complex *gradtarg,
+                    int32_t *ier);
+/* src/laplace/lfmm2dwrap.f:1267 */
+void lfmm2d_st_c_h_(const double *eps, const int32_t *ns,
+                    const double *sources, const double _Complex *charge,
+                    double _Complex *pot, double _Complex *grad,
+                    double _Complex *hess, const int32_t *nt,
+                    const double *targ, double _Complex *pottarg,
+                    double _Complex *gradtarg, double _Complex *hesstarg,
+                    int32_t *ier);
+/* src/laplace/lfmm2dwrap.f:1330 */
+void lfmm2d_st_d_p_(const double *eps, const int32_t *ns,
+                    const double *sources, const double _Complex *dipstr,
+                    const double *dipvec, double _Complex *pot,
+                    const int32_t *nt, const double *targ,
+                    double _Complex *pottarg, int32_t *ier);
+/* src/laplace/lfmm2dwrap.f:1392 */
+void lfmm2d_st_d_g_(const double *eps, const int32_t *ns,
+                    const double *sources, const double _Complex *dipstr,
+                    const double *dipvec, double _Complex *pot,
+                    double _Complex *grad, const int32_t *nt,
+                    const double *targ, double _Complex *pottarg,
+                    double _Complex *gradtarg, int32_t *ier);
+/* src/laplace/lfmm2dwrap.f:1456 */
+void lfmm2d_st_d_h_(const double *eps, const int32_t *ns,
+                    const double *sources, const double _Complex *dipstr,
+                    const double *dipvec, double _Complex *pot,
+                    double _Complex *grad, double _Complex *hess,
+                    const int32_t *nt, const double *targ,
+                    double _Complex *pottarg, double _Complex *gradtarg,
+                    double _Complex *hesstarg, int32_t *ier);
+/* src/laplace/lfmm2dwrap.f:1520 */
+void lfmm2d_st_cd_p_(const double *eps, const int32_t *ns,
+                     const double *sources, const double _Complex *charge,
+                     const double _Complex *dipstr, const double *dipvec,
+                     double _Complex *pot, const int32_t *nt,
+                     const double *targ, double _Complex *pottarg,
+                     int32_t *ier);
+/* src/laplace/lfmm2dwrap.f:1581 */
+void lfmm2d_st_cd_g_(const double *eps, const int32_t *ns,
+                     const double *sources, const double _Complex *charge,
+                     const double _Complex *dipstr, const double *dipvec,
+                     double _Complex *pot, double _Complex *grad,
+                     const int32_t *nt, const double *targ,
+                     double _Complex *pottarg, double _Complex *gradtarg,
+                     int32_t *ier);
+/* src/laplace/lfmm2dwrap.f:1644 */
+void lfmm2d_st_cd_h_(const double *eps, const int32_t *ns,
+                     const double *sources, const double _Complex *charge,
+                     const double _Complex *dipstr, const double *dipvec,
+                     double _Complex *pot, double _Complex *grad,
+                     double _Complex *hess, const int32_t *nt,
+                     const double *targ, double _Complex *pottarg,
+                     double _Complex *gradtarg, double _Complex *hesstarg,
+                     int32_t *ier);
+/* src/laplace/cfmm2dwrap.f:31 */
+void cfmm2d_s_c_p_(const double *eps, const int32_t *ns,
+                   const double *sources, const double _Complex *charge,
+                   double _Complex *pot, int32_t *ier);
+/* src/laplace/cfmm2dwrap.f:92 */
+void cfmm2d_s_c_g_(const double *eps, const int32_t *ns,
+                   const double *sources, const double _Complex *charge,
+                   double _Complex *pot, double _Complex *grad, int32_t *ier);
+/* src/laplace/cfmm2dwrap.f:154 */
+void cfmm2d_s_c_h_(const double *eps, const int32_t *ns,
+                   const double *sources, const double _Complex *charge,
+                   double _Complex *pot, double _Complex *grad,
+                   double _Complex *hess, int32_t *ier);
+/* src/laplace/cfmm2dwrap.f:214 */
+void cfmm2d_s_d_p_(const double *eps, const int32_t *ns,
+                   const double *sources, const double _Complex *dipstr,
+                   double _Complex *pot, int32_t *ier);
+/* src/laplace/cfmm2dwrap.f:275 */
+void cfmm2d_s_d_g_(const double *eps, const int32_t *ns,
+                   const double *sources, const double _Complex *dipstr,
+                   double _Complex *pot, double _Complex *grad, int32_t *ier);
+/* src/laplace/cfmm2dwrap.f:337 */
+void cfmm2d_s_d_h_(const double *eps, const int32_t *ns,
+                   const double *sources, const double _Complex *dipstr,
+                   double _Complex *pot, double _Complex *grad,
+                   double _Complex *hess, int32_t *ier);
+/* src/laplace/cfmm2dwrap.f:397 */
+void cfmm2d_s_cd_p_(const double *eps, const int32_t *ns,
+                    const double *sources, const double _Complex *charge,
+                    const double _Complex *dipstr, double _Complex *pot,
+                    int32_t *ier);
+/* src/laplace/cfmm2dwrap.f:457 */
+void cfmm2d_s_cd_g_(const double *eps, const int32_t *ns,
+                    const double *sources, const double _Complex *charge,
+                    const double _Complex *dipstr, double _Complex *pot,
+                    double _Complex *grad, int32_t *ier);
+/* src/laplace/cfmm2dwrap.f:518 */
+void cfmm2d_s_cd_h_(const double *eps, const int32_t *ns,
+                    const double *sources, const double _Complex *charge,
+                    const double _Complex *dipstr, double _Complex *pot,
+                    double _Complex *grad, double _Complex *hess,
+                    int32_t *ier);
+/* src/laplace/cfmm2dwrap.f:579 */
+void cfmm2d_t_c_p_(const double *eps, const int32_t *ns,
+                   const double *sources, const double _Complex *charge,
+                   const int32_t *nt, const double *targ,
+                   double _Complex *pottarg, int32_t *ier);
+/* src/laplace/cfmm2dwrap.f:638 */
+void cfmm2d_t_c_g_(const double *eps, const int32_t *ns,
+                   const double *sources, const double _Complex *charge,
+                   const int32_t *nt, const double *targ,
+                   double _Complex *pottarg, double _Complex *gradtarg,
+                   int32_t *ier);
+/* src/laplace/cfmm2dwrap.f:698 */
+void cfmm2d_t_c_h_(const double *eps, const int32_t *ns,
+                   const double *sources, const double _Complex *charge,
+                   const int32_t *nt, const double *targ,
+                   double _Complex *pottarg, double _Complex *gradtarg,
+                   double _Complex *hesstarg, int32_t *ier);
+/* src/laplace/cfmm2dwrap.f:757 */
+void cfmm2d_t_d_p_(const double *eps, const int32_t *ns,
+                   const double *sources, const double _Complex *dipstr,
+                   const int32_t *nt, const double *targ,
+                   double _Complex *pottarg, int32_t *ier);
+/* src/laplace/cfmm2dwrap.f:816 */
+void cfmm2d_t_d_g_(const double *eps, const int32_t *ns,
+                   const double *sources, const double _Complex *dipstr,
+                   const int32_t *nt, const double *targ,
+                   double _Complex *pottarg, double _Complex *gradtarg,
+                   int32_t *ier);
+/* src/laplace/cfmm2dwrap.f:876 */
+void cfmm2d_t_d_h_(const double *eps, const int32_t *ns,
+                   const double *sources, const double _Complex *dipstr,
+                   const int32_t *nt, const double *targ,
+                   double _Complex *pottarg, double _Complex *gradtarg,
+                   double _Complex *hesstarg, int32_t *ier);
+/* src/laplace/cfmm2dwrap.f:935 */
+void cfmm2d_t_cd_p_(const double *eps, const int32_t *ns,
+                    const double *sources, const double _Complex *charge,
+                    const double _Complex *dipstr, const int32_t *nt,
+                    const double *targ, double _Complex *pottarg,
+                    int32_t *ier);
+/* src/laplace/cfmm2dwrap.f:993 */
+void cfmm2d_t_cd_g_(const double *eps, const int32_t *ns,
+                    const double *sources, const double _Complex *charge,
+                    const double _Complex *dipstr, const int32_t *nt,
+                    const double *targ, double _Complex *pottarg,
+                    double _Complex *gradtarg, int32_t *ier);
+/* src/laplace/cfmm2dwrap.f:1052 */
+void cfmm2d_t_cd_h_(const double *eps, const int32_t *ns,
+                    const double *sources, const double _Complex *charge,
+                    const double _Complex *dipstr, const int32_t *nt,
+                    const double *targ, double _Complex *pottarg,
+                    double _Complex *gradtarg, double _Complex *hesstarg,
+                    int32_t *ier);
+/* src/laplace/cfmm2dwrap.f:1113 */
+void cfmm2d_st_c_p_(const double *eps, const int32_t *ns,
+                    const double *sources, const double _Complex *charge,
+                    double _Complex *pot, const int32_t *nt,
+                    const double *targ, double _Complex *pottarg,
+                    int32_t *ier);
+/* src/laplace/cfmm2dwrap.f:1173 */
+void cfmm2d_st_c_g_(const double *eps, const int32_t *ns,
+                    const double *sources, const double _Complex *charge,
+                    double _Complex *pot, double _Complex *grad,
+                    const int32_t *nt, const double *targ,
+                    double _Complex *pottarg, double _Complex *gradtarg,
+                    int32_t *ier);
+/* src/laplace/cfmm2dwrap.f:1235 */
+void cfmm2d_st_c_h_(const double *eps, const int32_t *ns,
+                    const double *sources, const double _Complex *charge,
+                    double _Complex *pot, double _Complex *grad,
+                    double _Complex *hess, const int32_t *nt,
+                    const double *targ, double _Complex *pottarg,
+                    double _Complex *gradtarg, double _Complex *hesstarg,
+                    int32_t *ier);
+/* src/laplace/cfmm2dwrap.f:1297 */
+void cfmm2d_st_d_p_(const double *eps, const int32_t *ns,
+                    const double *sources, const double _Complex *dipstr,
+                    double _Complex *pot, const int32_t *nt,
+                    const double *targ, double _Complex *pottarg,
+                    int32_t *ier);
+/* src/laplace/cfmm2dwrap.f:1357 */
+void cfmm2d_st_d_g_(const double *eps, const int32_t *ns,
+                    const double *sources, const double _Complex *dipstr,
+                    double _Complex *pot, double _Complex *grad,
+                    const int32_t *nt, const double *targ,
+                    double _Complex *pottarg, double _Complex *gradtarg,
+                    int32_t *ier);
+/* src/laplace/cfmm2dwrap.f:1419 */
+void cfmm2d_st_d_h_(const double *eps, const int32_t *ns,
+                    const double *sources, const double _Complex *dipstr,
+                    double _Complex *pot, double _Complex *grad,
+                    double _Complex *hess, const int32_t *nt,
+                    const double *targ, double _Complex *pottarg,
+                    double _Complex *gradtarg, double _Complex *hesstarg,
+                    int32_t *ier);
+/* src/laplace/cfmm2dwrap.f:1481 */
+void cfmm2d_st_cd_p_(const double *eps, const int32_t *ns,
+                     const double *sources, const double _Complex *charge,
+                     const double _Complex *dipstr, double _Complex *pot,
+                     const int32_t *nt, const double *targ,
+                     double _Complex *pottarg, int32_t *ier);
+/* src/laplace/cfmm2dwrap.f:1540 */
+void cfmm2d_st_cd_g_(const double *eps, const int32_t *ns,
+                     const double *sources, const double _Complex *charge,
+                     const double _Complex *dipstr, double _Complex *pot,
+                     double _Complex *grad, const int32_t *nt,
+                     const double *targ, double _Complex *pottarg,
+                     double _Complex *gradtarg, int32_t *ier);
+/* src/laplace/cfmm2dwrap.f:1601 */
+void cfmm2d_st_cd_h_(const double *eps, const int32_t *ns,
+                     const double *sources, const double _Complex *charge,
+                     const double _Complex *dipstr, double _Complex *pot,
+                     double _Complex *grad, double _Complex *hess,
+                     const int32_t *nt, const double *targ,
+                     double _Complex *pottarg, double _Complex *gradtarg,
+                     double _Complex *hesstarg, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap.f:41 */
+void hfmm2d_s_c_p_(const double *eps, const double _Complex *zk,
+                   const int32_t *ns, const double *sources,
+                   const double _Complex *charge, double _Complex *pot,
+                   int32_t *ier);
+/* src/helmholtz/hfmm2dwrap.f:108 */
+void hfmm2d_s_c_g_(const double *eps, const double _Complex *zk,
+                   const int32_t *ns, const double *sources,
+                   const double _Complex *charge, double _Complex *pot,
+                   double _Complex *grad, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap.f:177 */
+void hfmm2d_s_c_h_(const double *eps, const double _Complex *zk,
+                   const int32_t *ns, const double *sources,
+                   const double _Complex *charge, double _Complex *pot,
+                   double _Complex *grad, double _Complex *hess,
+                   int32_t *ier);
+/* src/helmholtz/hfmm2dwrap.f:245 */
+void hfmm2d_s_d_p_(const double *eps, const double _Complex *zk,
+                   const int32_t *ns, const double *sources,
+                   const double _Complex *dipstr, const double *dipvec,
+                   double _Complex *pot, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap.f:312 */
+void hfmm2d_s_d_g_(const double *eps, const double _Complex *zk,
+                   const int32_t *ns, const double *sources,
+                   const double _Complex *dipstr, const double *dipvec,
+                   double _Complex *pot, double _Complex *grad, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap.f:382 */
+void hfmm2d_s_d_h_(const double *eps, const double _Complex *zk,
+                   const int32_t *ns, const double *sources,
+                   const double _Complex *dipstr, const double *dipvec,
+                   double _Complex *pot, double _Complex *grad,
+                   double _Complex *hess, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap.f:451 */
+void hfmm2d_s_cd_p_(const double *eps, const double _Complex *zk,
+                    const int32_t *ns, const double *sources,
+                    const double _Complex *charge,
+                    const double _Complex *dipstr, const double *dipvec,
+                    double _Complex *pot, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap.f:521 */
+void hfmm2d_s_cd_g_(const double *eps, const double _Complex *zk,
+                    const int32_t *ns, const double *sources,
+                    const double _Complex *charge,
+                    const double _Complex *dipstr, const double *dipvec,
+                    double _Complex *pot, double _Complex *grad,
+                    int32_t *ier);
+/* src/helmholtz/hfmm2dwrap.f:590 */
+void hfmm2d_s_cd_h_(const double *eps, const double _Complex *zk,
+                    const int32_t *ns, const double *sources,
+                    const double _Complex *charge,
+                    const double _Complex *dipstr, const double *dipvec,
+                    double _Complex *pot, double _Complex *grad,
+                    double _Complex *hess, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap.f:657 */
+void hfmm2d_t_c_p_(const double *eps, const double _Complex *zk,
+                   const int32_t *ns, const double *sources,
+                   const double _Complex *charge, const int32_t *nt,
+                   const double *targ, double _Complex *pottarg,
+                   int32_t *ier);
+/* src/helmholtz/hfmm2dwrap.f:721 */
+void hfmm2d_t_c_g_(const double *eps, const double _Complex *zk,
+                   const int32_t *ns, const double *sources,
+                   const double _Complex *charge, const int32_t *nt,
+                   const double *targ, double _Complex *pottarg,
+                   double _Complex *gradtarg, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap.f:788 */
+void hfmm2d_t_c_h_(const double *eps, const double _Complex *zk,
+                   const int32_t *ns, const double *sources,
+                   const double _Complex *charge, const int32_t *nt,
+                   const double *targ, double _Complex *pottarg,
+                   double _Complex *gradtarg, double _Complex *hesstarg,
+                   int32_t *ier);
+/* src/helmholtz/hfmm2dwrap.f:855 */
+void hfmm2d_t_d_p_(const double *eps, const double _Complex *zk,
+                   const int32_t *ns, const double *sources,
+                   const double _Complex *dipstr, const double *dipvec,
+                   const int32_t *nt, const double *targ,
+                   double _Complex *pottarg, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap.f:920 */
+void hfmm2d_t_d_g_(const double *eps, const double _Complex *zk,
+                   const int32_t *ns, const double *sources,
+                   const double _Complex *dipstr, const double *dipvec,
+                   const int32_t *nt, const double *targ,
+                   double _Complex *pottarg, double _Complex *gradtarg,
+                   int32_t *ier);
+/* src/helmholtz/hfmm2dwrap.f:988 */
+void hfmm2d_t_d_h_(const double *eps, const double _Complex *zk,
+                   const int32_t *ns, const double *sources,
+                   const double _Complex *dipstr, const double *dipvec,
+                   const int32_t *nt, const double *targ,
+                   double _Complex *pottarg, double _Complex *gradtarg,
+                   double _Complex *hesstarg, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap.f:1056 */
+void hfmm2d_t_cd_p_(const double *eps, const double _Complex *zk,
+                    const int32_t *ns, const double *sources,
+                    const double _Complex *charge,
+                    const double _Complex *dipstr, const double *dipvec,
+                    const int32_t *nt, const double *targ,
+                    double _Complex *pottarg, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap.f:1124 */
+void hfmm2d_t_cd_g_(const double *eps, const double _Complex *zk,
+                    const int32_t *ns, const double *sources,
+                    const double _Complex *charge,
+                    const double _Complex *dipstr, const double *dipvec,
+                    const int32_t *nt, const double *targ,
+                    double _Complex *pottarg, double _Complex *gradtarg,
+                    int32_t *ier);
+/* src/helmholtz/hfmm2dwrap.f:1191 */
+void hfmm2d_t_cd_h_(const double *eps, const double _Complex *zk,
+                    const int32_t *ns, const double *sources,
+                    const double _Complex *charge,
+                    const double _Complex *dipstr, const double *dipvec,
+                    const int32_t *nt, const double *targ,
+                    double _Complex *pottarg, double _Complex *gradtarg,
+                    double _Complex *hesstarg, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap.f:1264 */
+void hfmm2d_st_c_p_(const double *eps, const double _Complex *zk,
+                    const int32_t *ns, const double *sources,
+                    const double _Complex *charge, double _Complex *pot,
+                    const int32_t *nt, const double *targ,
+                    double _Complex *pottarg, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap.f:1329 */
+void hfmm2d_st_c_g_(const double *eps, const double _Complex *zk,
+                    const int32_t *ns, const double *sources,
+                    const double _Complex *charge, double _Complex *pot,
+                    double _Complex *grad, const int32_t *nt,
+                    const double *targ, double _Complex *pottarg,
+                    double _Complex *gradtarg, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap.f:1397 */
+void hfmm2d_st_c_h_(const double *eps, const double _Complex *zk,
+                    const int32_t *ns, const double *sources,
+                    const double _Complex *charge, double _Complex *pot,
+                    double _Complex *grad, double _Complex *hess,
+                    const int32_t *nt, const double *targ,
+                    double _Complex *pottarg, double _Complex *gradtarg,
+                    double _Complex *hesstarg, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap.f:1465 */
+void hfmm2d_st_d_p_(const double *eps, const double _Complex *zk,
+                    const int32_t *ns, const double *sources,
+                    const double _Complex *dipstr, const double *dipvec,
+                    double _Complex *pot, const int32_t *nt,
+                    const double *targ, double _Complex *pottarg,
+                    int32_t *ier);
+/* src/helmholtz/hfmm2dwrap.f:1531 */
+void hfmm2d_st_d_g_(const double *eps, const double _Complex *zk,
+                    const int32_t *ns, const double *sources,
+                    const double _Complex *dipstr, const double *dipvec,
+                    double _Complex *pot, double _Complex *grad,
+                    const int32_t *nt, const double *targ,
+                    double _Complex *pottarg, double _Complex *gradtarg,
+                    int32_t *ier);
+/* src/helmholtz/hfmm2dwrap.f:1600 */
+void hfmm2d_st_d_h_(const double *eps, const double _Complex *zk,
+                    const int32_t *ns, const double *sources,
+                    const double _Complex *dipstr, const double *dipvec,
+                    double _Complex *pot, double _Complex *grad,
+                    double _Complex *hess, const int32_t *nt,
+                    const double *targ, double _Complex *pottarg,
+                    double _Complex *gradtarg, double _Complex *hesstarg,
+                    int32_t *ier);
+/* src/helmholtz/hfmm2dwrap.f:1669 */
+void hfmm2d_st_cd_p_(const double *eps, const double _Complex *zk,
+                     const int32_t *ns, const double *sources,
+                     const double _Complex *charge,
+                     const double _Complex *dipstr, const double *dipvec,
+                     double _Complex *pot, const int32_t *nt,
+                     const double *targ, double _Complex *pottarg,
+                     int32_t *ier);
+/* src/helmholtz/hfmm2dwrap.f:1738 */
+void hfmm2d_st_cd_g_(const double *eps, const double _Complex *zk,
+                     const int32_t *ns, const double *sources,
+                     const double _Complex *charge,
+                     const double _Complex *dipstr, const double *dipvec,
+                     double _Complex *pot, double _Complex *grad,
+                     const int32_t *nt, const double *targ,
+                     double _Complex *pottarg, double _Complex *gradtarg,
+                     int32_t *ier);
+/* src/helmholtz/hfmm2dwrap.f:1806 */
+void hfmm2d_st_cd_h_(const double *eps, const double _Complex *zk,
+                     const int32_t *ns, const double *sources,
+                     const double _Complex *charge,
+                     const double _Complex *dipstr, const double *dipvec,
+                     double _Complex *pot, double _Complex *grad,
+                     double _Complex *hess, const int32_t *nt,
+                     const double *targ, double _Complex *pottarg,
+                     double _Complex *gradtarg, double _Complex *hesstarg,
+                     int32_t *ier);
+
+/* ===================================================================== */
+/* Guru drivers (full flag sets, nd densities).  iper is ignored and set */
+/* to 0, as in the reference (src/laplace/cfmm2d.f:150).                 */
+/* ===================================================================== */
+/* src/laplace/lfmm2d.f:29 */
+void lfmm2d_(const int32_t *nd, const double *eps, const int32_t *ns,
+             const double *sources, const int32_t *ifcharge,
+             const double _Complex *charge, const int32_t *ifdipole,
+             const double _Complex *dipstr, const double *dipvec,
+             int32_t *iper, const int32_t *ifpgh, double _Complex *pot,
+             double _Complex *grad, double _Complex *hess, const int32_t *nt,
+             const double *targ, const int32_t *ifpghtarg,
+             double _Complex *pottarg, double _Complex *gradtarg,
+             double _Complex *hesstarg, int32_t *ier);
+/* src/laplace/cfmm2d.f:23, c_translation/src/cfmm2d.c:1053 */
+void cfmm2d_(const int32_t *nd, const double *eps, const int32_t *ns,
+             const double *sources, const int32_t *ifcharge,
+             const double _Complex *charge, const int32_t *ifdipole,
+             const double _Complex *dipstr, int32_t *iper,
+             const int32_t *ifpgh, double _Complex *pot, double _Complex *grad,
+             double _Complex *hess, const int32_t *nt, const double *targ,
+             const int32_t *ifpghtarg, double _Complex *pottarg,
+             double _Complex *gradtarg, double _Complex *hesstarg,
+             int32_t *ier);
+/* src/helmholtz/hfmm2d.f:19, c_translation/src/hfmm2d.c:1529 */
+void hfmm2d_(const int32_t *nd, const double *eps, const double _Complex *zk,
+             const int32_t *ns, const double *sources,
+             const int32_t *ifcharge, const double _Complex *charge,
+             const int32_t *ifdipole, const double _Complex *dipstr,
+             const double *dipvec, int32_t *iper, const int32_t *ifpgh,
+             double _Complex *pot, double _Complex *grad,
+             double _Complex *hess, const int32_t *nt, const double *targ,
+             const int32_t *ifpghtarg, double _Complex *pottarg,
+             double _Complex *gradtarg, double _Complex *hesstarg,
+             int32_t *ier);
+
+/* Drivers with caller-chosen leaf capacity ndiv, subdivision rule idivflag
+ * (0 sources, 1 targets, 2 both), near-field switch ifnear and per-step
+ * timings timeinfo(8) (MATLAB path, matlab/fmm2d.c:1256-1286). */
+/* src/laplace/lfmm2d_ndiv.f:29, c_translation/src/lfmm2d_ndiv.c:57 */
+void lfmm2d_ndiv_(const int32_t *nd, const double *eps, const int32_t *ns,
+                  const double *sources, const int32_t *ifcharge,
+                  const double _Complex *charge, const int32_t *ifdipole,
+                  const double _Complex *dipstr, const double *dipvec,
+                  int32_t *iper, const int32_t *ifpgh, double _Complex *pot,
+                  double _Complex *grad, double _Complex *hess,
+                  const int32_t *nt, const double *targ,
+                  const int32_t *ifpghtarg, double _Complex *pottarg,
+                  double _Complex *gradtarg, double _Complex *hesstarg,
+                  const int32_t *ndiv, const int32_t *idivflag,
+                  const int32_t *ifnear, double *timeinfo, int32_t *ier);
+/* src/laplace/cfmm2d_ndiv.f:23, c_translation/src/cfmm2d_ndiv.c:94 */
+void cfmm2d_ndiv_(const int32_t *nd, const double *eps, const int32_t *ns,
+                  const double *sources, const int32_t *ifcharge,
+                  const double _Complex *charge, const int32_t *ifdipole,
+                  const double _Complex *dipstr, int32_t *iper,
+                  const int32_t *ifpgh, double _Complex *pot,
+                  double _Complex *grad, double _Complex *hess,
+                  const int32_t *nt, const double *targ,
+                  const int32_t *ifpghtarg, double _Complex *pottarg,
+                  double _Complex *gradtarg, double _Complex *hesstarg,
+                  const int32_t *ndiv, const int32_t *idivflag,
+                  const int32_t *ifnear, double *timeinfo, int32_t *ier);
+/* src/helmholtz/hfmm2d_ndiv.f:19, c_translation/src/hfmm2d_ndiv.c:68 */
+void hfmm2d_ndiv_(const int32_t *nd, const double *eps,
+                  const double _Complex *zk, const int32_t *ns,
+                  const double *sources, const int32_t *ifcharge,
+                  const double _Complex *charge, const int32_t *ifdipole,
+                  const double _Complex *dipstr, const double *dipvec,
+                  int32_t *iper, const int32_t *ifpgh, double _Complex *pot,
+                  double _Complex *grad, double _Complex *hess,
+                  const int32_t *nt, const double *targ,
+                  const int32_t *ifpghtarg, double _Complex *pottarg,
+                  double _Complex *gradtarg, double _Complex *hesstarg,
+                  const int32_t *ndiv, const int32_t *idivflag,
+                  const int32_t *ifnear, double *timeinfo, int32_t *ier);
+
+/* ===================================================================== */
+/* Library entry points with no counterpart in the reference.           */
+/* ===================================================================== */
+const char *fmm2d_b200_version(void);
+/* Message of the last failed call (any thread); returns its length. */
+int fmm2d_b200_last_error(char *buf, int len);
+/* Precision policy of later calls: 0 auto (mixed when eps >= 1e-6),
+ * 1 all-FP64, 2 mixed.  Also FMM2D_B200_PRECISION=auto|fp64|mixed. */
+int fmm2d_b200_set_precision(int mode);
+/* Run the calling thread's later calls on a caller-owned cudaStream_t. */
+int fmm2d_b200_set_stream(void *stream);
+int fmm2d_b200_reset_stream(void);
+/* Return cached device workspace of the current device to the driver. */
+int fmm2d_b200_release_memory(void);
+/* Host-only rules: expansion order (l2dterms, c_translation/src/l2dterms.c:26)
+ * and leaf capacity (src/laplace/lndiv2d.f:1) for a precision. */
+int fmm2d_b200_laplace_nterms(double eps);
+int fmm2d_b200_leaf_capacity(double eps, int ns, int nt);
+
+/* Direct sums on the GPU, incrementing the outputs (the reference's
+ * l2d_direct* / c2d_direct* kernels, src/laplace/lapkernels2d.f,
+ * src/laplace/cauchykernels2d.f): every target against every source. */
+int fmm2d_b200_l2d_direct(int nd, int ns, const double *sources,
+                          int ifcharge, const double _Complex *charge,
+                          int ifdipole, const double _Complex *dipstr,
+                          const double *dipvec, int nt, const double *targ,
+                          int ifpgh, double _Complex *pot,
+                          double _Complex *grad, double _Complex *hess,
+                          double thresh);
+int fmm2d_b200_c2d_direct(int nd, int ns, const double *sources,
+                          int ifcharge, const double _Complex *charge,
+                          int ifdipole, const double _Complex *dipstr, int nt,
+                          const double *targ, int ifpgh, double _Complex *pot,
+                          double _Complex *grad, double _Complex *hess,
+                          double thresh);
+
+/* Quadtree inspection in the reference's layout (pts_tree_mem/build/sort,
+ * src/common/pts_tree2d.f:34,406,1222; computelists,
+ * src/common/tree_routs2d.f:486). */
+int fmm2d_b200_tree_build(const double *sources, int ns, const double *targ,
+                          int nt, int ndiv, int idivflag, void **handle);
+int fmm2d_b200_tree_sizes(void *handle, int *nlevels, int *nboxes,
+                          int *ltree);
+int fmm2d_b200_tree_export(void *handle, int *itree, int *iptr,
+                           double *centers, double *boxsize, int *isrc,
+                           int *isrcse, int *itarg, int *itargse);
+int fmm2d_b200_tree_lists(void *handle, int *nlist1, int *list1,
+                          int *nlist2, int *list2, int *nlist3, int *list3,
+                          int *nlist4, int *list4);
+void fmm2d_b200_tree_free(void *handle);
+
+/* Measurement helpers. */
+int fmm2d_b200_set_profiling(int on);
+int fmm2d_b200_last_profile(char *buf, int len);
+unsigned long long fmm2d_b200_launch_count(void);
+double fmm2d_b200_fp64_peak_tflops(void);
+double fmm2d_b200_fp32_peak_tflops(void);
+
+#ifdef __cplusplus
+}
+#undef _Complex
+#endif
+#endif /* FMM2D_B200_H */

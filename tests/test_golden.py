@@ -1,0 +1,77 @@
+"""Golden fixtures (tests/golden/, generated from the reference's C
+translation by tests/golden/make_golden.py) against the oracle: the FMM
+outputs the reference produced agree with the oracle's FP64 direct sums to
+the requested precision, and the reference build, where present,
+reproduces them."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import refimpl
+import wrappers as W
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+FILES = sorted(glob.glob(os.path.join(GOLD, "fmm_*.npz")))
+
+
+def oracle_outputs(fam, variant, g):
+    _, cd, p = variant.split("_")
+    pgh = {"p": 1, "g": 2, "h": 3}[p]
+    src = np.ascontiguousarray(g["src"].T)
+    trg = np.ascontiguousarray(g["trg"].T)
+    ns, nt = src.shape[0], trg.shape[0]
+    q, d = g["charge"], g["dipstr"]
+    v = np.ascontiguousarray(g["dipvec"].T)
+    res = {}
+    for key, pts, n in (("", src, ns), ("targ", trg, nt)):
+        gc = 2 if fam == "l" else 1
+        hc = 3 if fam == "l" else 1
+        pot = np.zeros(n, complex)
+        grad = np.zeros((n, gc), complex)
+        hess = np.zeros((n, hc), complex)
+        if fam == "l":
+            refimpl.orc().oracle_l2d_direct(
+                ns, W._p(src), int("c" in cd), W._p(q), int("d" in cd), W._p(d),
+                W._p(v), 0, n, W._p(pts), pgh, W._p(pot), W._p(grad), W._p(hess), 1e-300)
+        else:
+            refimpl.orc().oracle_c2d_direct(
+                ns, W._p(src), int("c" in cd), W._p(q), int("d" in cd), W._p(d),
+                0, n, W._p(pts), pgh, W._p(pot), W._p(grad), W._p(hess), 1e-300)
+        res["pot" + key] = pot
+        if pgh >= 2:
+            res["grad" + key] = grad if gc > 1 else grad[:, 0]
+        if pgh >= 3:
+            res["hess" + key] = hess if hc > 1 else hess[:, 0]
+    return res
+
+
+@pytest.mark.parametrize("path", FILES, ids=[os.path.basename(f) for f in FILES])
+def test_golden_against_oracle(path):
+    name = os.path.basename(path)[4:-4]
+    fam, variant = name.split("_", 1)
+    g = np.load(path)
+    ref = oracle_outputs(fam, variant, g)
+    eps = float(g["eps"])
+    for k, v in ref.items():
+        # Cauchy potentials of complex strengths are defined only up to the
+        # far-field branch term (the FMM's q log z vs the direct q log|z|);
+        # the derivatives are exact.  The real parts of Laplace potentials
+        # and every gradient/Hessian must match to eps.
+        if fam == "c" and k.startswith("pot"):
+            continue
+        assert W.rel_err(g[k], v) < 20 * eps, (name, k)
+
+
+@pytest.mark.skipif(not refimpl.have_ref(), reason="reference build absent")
+@pytest.mark.parametrize("path", FILES, ids=[os.path.basename(f) for f in FILES])
+def test_reference_reproduces_golden(path):
+    name = os.path.basename(path)[4:-4]
+    fam, variant = name.split("_", 1)
+    g = np.load(path)
+    out, ier = W.call(refimpl.ref(), fam, variant, float(g["eps"]), g["src"],
+                      g["charge"], g["dipstr"], g["dipvec"], g["trg"])
+    assert ier == 0
+    for k in out:
+        assert W.rel_err(out[k], g[k]) < 1e-13
