@@ -665,6 +665,24 @@ int fmm2d_b200_c2d_direct(int nd, int ns, const double *sources,
                           double _Complex *grad, double _Complex *hess,
                           double thresh);
 
+/* No counterpart in the reference.  fmm2d_b200_l2d_direct for callers
+ * that cannot have device memory allocated for them (GPU memory owned by
+ * another allocator or a fixed budget; callers that cannot accept an
+ * allocation call's possible device synchronization).  Same arguments plus
+ * a stream; device arrays only; scratch is a fixed 4 MiB device array
+ * (nd * nt * outputs <= 262144, outputs = 1, 3 or 6), held by every GPU
+ * that loads the library.  The first call on a device sets the array up
+ * and should come before any stream capture; calls that overlap on the GPU
+ * race on the shared array.  Returns after `stream` has finished the call. */
+int fmm2d_b200_l2d_direct_noalloc(int nd, int ns, const double *sources,
+                                  int ifcharge, const double _Complex *charge,
+                                  int ifdipole, const double _Complex *dipstr,
+                                  const double *dipvec, int nt,
+                                  const double *targ, int ifpgh,
+                                  double _Complex *pot, double _Complex *grad,
+                                  double _Complex *hess, double thresh,
+                                  void *stream);
+
 /* Quadtree inspection in the reference's layout (pts_tree_mem/build/sort,
  * src/common/pts_tree2d.f:34,406,1222; computelists,
  * src/common/tree_routs2d.f:486). */
