@@ -146,7 +146,6 @@ void run_laplace_family(const FmmCall &c, CallCtx &ctx) {
     const int idivflag = c.ndiv >= 0 ? c.idivflag : 0;
     Tree T;
     build_tree(src_in.ptr, ns, trg_in.ptr, nt, ndiv, idivflag, kMaxLevels, s, T);
-    prof_mark("tree", s);
     compute_lists(T, s);
     prof_mark("lists", s);
     // ---- gather into tree order ----

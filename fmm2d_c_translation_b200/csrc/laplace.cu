@@ -11,6 +11,8 @@
 #include "laplace.cuh"
 
 #include <mutex>
+#include <stdlib.h>
+#include <string.h>
 
 namespace fmm2d {
 
@@ -301,7 +303,7 @@ __global__ void __launch_bounds__(kBlock) m2l_kernel(
     const int stride = (p + 1) * ndc;
     for (int b = lo + warp_global(); b < hi; b += warp_count()) {
         const int n2 = nlist2[b];
-        if (n2 == 0 || ec.npts(b) <= 0) continue;
+        if (ec.npts(b) <= 0) continue;
         const double2 c2 = centers[b];
         for (int kb = 0; kb <= p; kb += 32) {
             const int i = kb + lane;
@@ -310,6 +312,7 @@ __global__ void __launch_bounds__(kBlock) m2l_kernel(
             for (int q = 0; q < CH; q++) acc[q] = make_double2(0.0, 0.0);
             for (int e = 0; e < n2; e++) {
                 const int sb = list2[kMaxList2 * b + e];
+                if (count(ec.sse, sb) <= 0) continue;  // no multipole
                 const double2 c1 = centers[sb];
                 const double2 z0 = make_double2(c1.x - c2.x, c1.y - c2.y);
                 const double2 zi = cinv(z0);
@@ -349,12 +352,11 @@ __global__ void __launch_bounds__(kBlock) m2l_kernel(
                 }
                 __syncwarp();
             }
+            // first writer of this box's local expansion
             if (i <= p) {
 #pragma unroll
-                for (int q = 0; q < CH; q++) {
-                    double2 &o = loc[(size_t)b * stride + (size_t)i * ndc + c0 + q];
-                    o = cadd(o, acc[q]);
-                }
+                for (int q = 0; q < CH; q++)
+                    loc[(size_t)b * stride + (size_t)i * ndc + c0 + q] = acc[q];
             }
         }
     }
@@ -425,8 +427,8 @@ __global__ void __launch_bounds__(kBlock) eval_far_kernel(
     int lo, int hi, const int *__restrict__ nchild,
     const int *__restrict__ level, const double2 *__restrict__ centers,
     const double *__restrict__ bs, const int *__restrict__ nlist3,
-    const int *__restrict__ list3, PointSet set, int ndc, int c0, int p,
-    int nlevels, const double2 *__restrict__ mp,
+    const int *__restrict__ list3, const int2 *__restrict__ sse, PointSet set,
+    int ndc, int c0, int p, int nlevels, const double2 *__restrict__ mp,
     const double2 *__restrict__ loc) {
     const int lane = lane_id();
     const int stride = (p + 1) * ndc;
@@ -450,6 +452,7 @@ __global__ void __launch_bounds__(kBlock) eval_far_kernel(
             // list 3: multipoles of the finer separated boxes
             for (int e = 0; e < n3; e++) {
                 const int jb = list3[kMaxList3 * b + e];
+                if (sse[jb].y <= sse[jb].x) continue;  // no multipole
                 const double2 cj = centers[jb];
                 const double r = bs[level[jb]];
                 double2 z = make_double2(x.x - cj.x, x.y - cj.y);
@@ -681,15 +684,14 @@ void launch_p2p(const Tree &T, const CauchyProblem &P, const PointSet &set,
     }
 }
 
+// Upward pass for channels [c0, c0 + CH): P2M at the leaves of levels >= 2,
+// then M2M from the finest parents up.
 template <int CH>
-void cauchy_fmm_chunk(const Tree &T, const CauchyProblem &P, int c0,
-                      const double *binom, double2 *mp, double2 *loc,
-                      cudaStream_t s) {
+void upward_chunk(const Tree &T, const CauchyProblem &P, int c0,
+                  const double *binom, double2 *mp, cudaStream_t s) {
     const int L = T.nlevels, p = P.p, nb = T.nboxes;
     const double *bs = T.d_boxsize.get();
-    const EvalCounts ec{T.srcse.get(), T.trgse.get(), P.sset.pgh, P.tset.pgh};
     const size_t sh_exp = (size_t)kWarpsPerBlock * (p + 1) * CH * sizeof(double2);
-    // step 1: P2M at leaves of levels >= 2
     if (L >= 2) {
         const int lo = T.lstart[2];
         p2m_kernel<CH><<<grid_for(nb - lo), kBlock, 0, s>>>(
@@ -697,15 +699,8 @@ void cauchy_fmm_chunk(const Tree &T, const CauchyProblem &P, int c0,
             T.srcse.get(), P.src, P.charge, P.dipstr, P.ifcharge, P.ifdipole,
             P.ndc, c0, p, mp);
         FMM_CHECK_LAUNCH();
-        // step 2: P2L from list 4
-        p2l_kernel<CH><<<grid_for(nb - lo), kBlock, 0, s>>>(
-            lo, nb, ec, T.nlist4.get(), T.list4.get(), T.centers.get(),
-            T.level.get(), bs, P.src, P.charge, P.dipstr, P.ifcharge,
-            P.ifdipole, P.ndc, c0, p, loc);
-        FMM_CHECK_LAUNCH();
     }
-    prof_mark("p2m_p2l", s);
-    // step 3: M2M, finest parents first
+    prof_mark("p2m", s);
     for (int l = L - 1; l >= 1; l--) {
         const int lo = T.lstart[l], hi = T.lend[l];
         m2m_kernel<CH><<<grid_for(hi - lo), kBlock, sh_exp, s>>>(
@@ -715,7 +710,16 @@ void cauchy_fmm_chunk(const Tree &T, const CauchyProblem &P, int c0,
         FMM_CHECK_LAUNCH();
     }
     prof_mark("m2m", s);
-    // step 4: M2L over list 2, per level
+}
+
+// M2L with the per-box kernel, levels 2..L, channels [c0, c0 + CH).
+template <int CH>
+void m2l_chunk(const Tree &T, const CauchyProblem &P, int c0,
+               const double *binom, const double2 *mp, double2 *loc,
+               cudaStream_t s) {
+    const int L = T.nlevels, p = P.p;
+    const EvalCounts ec{T.srcse.get(), T.trgse.get(), P.sset.pgh, P.tset.pgh};
+    const size_t sh_exp = (size_t)kWarpsPerBlock * (p + 1) * CH * sizeof(double2);
     const size_t sh_m2l = (size_t)(((p + 1) * (p + 1) + 1) & ~1) * sizeof(double) + sh_exp;
     FMM_CUDA(cudaFuncSetAttribute(m2l_kernel<CH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)sh_m2l));
@@ -726,7 +730,28 @@ void cauchy_fmm_chunk(const Tree &T, const CauchyProblem &P, int c0,
             T.boxsize[l], P.ndc, c0, p, binom, mp, loc);
         FMM_CHECK_LAUNCH();
     }
-    prof_mark("m2l", s);
+}
+
+// Downward pass and evaluation for channels [c0, c0 + CH): P2L, L2L, M2P +
+// L2P, P2P.
+template <int CH>
+void downward_chunk(const Tree &T, const CauchyProblem &P, int c0,
+                    const double *binom, const double2 *mp, double2 *loc,
+                    cudaStream_t s) {
+    const int L = T.nlevels, p = P.p, nb = T.nboxes;
+    const double *bs = T.d_boxsize.get();
+    const EvalCounts ec{T.srcse.get(), T.trgse.get(), P.sset.pgh, P.tset.pgh};
+    const size_t sh_exp = (size_t)kWarpsPerBlock * (p + 1) * CH * sizeof(double2);
+    // step 2: P2L from list 4 (after M2L, which initialises the locals)
+    if (L >= 2) {
+        const int lo = T.lstart[2];
+        p2l_kernel<CH><<<grid_for(nb - lo), kBlock, 0, s>>>(
+            lo, nb, ec, T.nlist4.get(), T.list4.get(), T.centers.get(),
+            T.level.get(), bs, P.src, P.charge, P.dipstr, P.ifcharge,
+            P.ifdipole, P.ndc, c0, p, loc);
+        FMM_CHECK_LAUNCH();
+    }
+    prof_mark("p2l", s);
     // step 5: L2L, coarsest parents first
     for (int l = 1; l <= L - 1; l++) {
         const int lo = T.lstart[l + 1], hi = T.lend[l + 1];
@@ -741,7 +766,8 @@ void cauchy_fmm_chunk(const Tree &T, const CauchyProblem &P, int c0,
         if (set->pgh <= 0 || set->n <= 0) continue;
         eval_far_kernel<CH><<<grid_for(nb), kBlock, 0, s>>>(
             0, nb, T.nchild.get(), T.level.get(), T.centers.get(), bs,
-            T.nlist3.get(), T.list3.get(), *set, P.ndc, c0, p, L, mp, loc);
+            T.nlist3.get(), T.list3.get(), T.srcse.get(), *set, P.ndc, c0, p,
+            L, mp, loc);
         FMM_CHECK_LAUNCH();
     }
     prof_mark("m2p_l2p", s);
@@ -827,15 +853,32 @@ void cauchy_fmm(const Tree &T, const CauchyProblem &P, cudaStream_t s) {
     const double *binom = device_binomials(s);
     const size_t nexp = (size_t)T.nboxes * (P.p + 1) * P.ndc;
     DevBuf<double2> mp(nexp, s), loc(nexp, s);
-    mp.zero(s);
-    loc.zero(s);
+    // Expansions are written before they are read (P2M / M2M store the
+    // multipoles of every box that has sources, M2L stores the locals of
+    // every box of level >= 2 with points), except the locals of levels 0
+    // and 1, which receive no M2L and start at zero.
+    const int nlow = T.nlevels >= 1 ? T.lend[1] : T.lend[0];
+    FMM_CUDA(cudaMemsetAsync(loc.get(), 0,
+                             (size_t)nlow * (P.p + 1) * P.ndc * sizeof(double2), s));
     prof_mark("fmm_setup", s);
-    for (int c0 = 0; c0 < P.ndc; c0 += 2) {
-        if (P.ndc - c0 >= 2)
-            cauchy_fmm_chunk<2>(T, P, c0, binom, mp.get(), loc.get(), s);
-        else
-            cauchy_fmm_chunk<1>(T, P, c0, binom, mp.get(), loc.get(), s);
-    }
+    auto per_chunk = [&](auto f2, auto f1) {
+        for (int c0 = 0; c0 < P.ndc; c0 += 2) {
+            if (P.ndc - c0 >= 2)
+                f2(c0);
+            else
+                f1(c0);
+        }
+    };
+    per_chunk([&](int c0) { upward_chunk<2>(T, P, c0, binom, mp.get(), s); },
+              [&](int c0) { upward_chunk<1>(T, P, c0, binom, mp.get(), s); });
+    const char *mode = getenv("FMM2D_B200_M2L");
+    const bool simple = mode && !strcmp(mode, "simple");
+    if (simple || !m2l_tensor_fp64(T, P, mp.get(), loc.get(), s))
+        per_chunk([&](int c0) { m2l_chunk<2>(T, P, c0, binom, mp.get(), loc.get(), s); },
+                  [&](int c0) { m2l_chunk<1>(T, P, c0, binom, mp.get(), loc.get(), s); });
+    prof_mark("m2l", s);
+    per_chunk([&](int c0) { downward_chunk<2>(T, P, c0, binom, mp.get(), loc.get(), s); },
+              [&](int c0) { downward_chunk<1>(T, P, c0, binom, mp.get(), loc.get(), s); });
 }
 
 void cauchy_direct(const CauchyProblem &P, int ns, PointSet set,

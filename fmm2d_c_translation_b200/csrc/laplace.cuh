@@ -42,6 +42,12 @@ void cauchy_fmm(const Tree &T, const CauchyProblem &P, cudaStream_t s);
 void cauchy_direct(const CauchyProblem &P, int ns, PointSet set,
                    cudaStream_t s);
 
+// M2L over list 2 on the FP64 tensor cores for all channels and levels
+// (m2l.cu); false when the tree does not fit its tiling (the caller then
+// uses the per-box kernel).
+bool m2l_tensor_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp,
+                     double2 *loc, cudaStream_t s);
+
 // Binomial table C(l, m), l, m <= kLdc, built with the reference's Pascal
 // recurrence (init_carray, src/common/fmmcommon2d.f).
 constexpr int kLdc = 127;

@@ -496,6 +496,49 @@ __global__ void bbox_kernel(const double2 *__restrict__ a, int na,
     }
 }
 
+// Moves every point of a refined box of the current level into its child
+// and counts the points per child.  The counts are aggregated before they
+// reach global memory: in a shared-memory histogram when the new level has
+// at most kHistChildren boxes (the shallow levels, where every point would
+// otherwise hit the same few counters), by warp-level grouping otherwise.
+constexpr int kHistChildren = 8192;
+
+template <bool HIST>
+__global__ void __launch_bounds__(256) assign_children_kernel(
+    int n, const double2 *__restrict__ pts, int *__restrict__ pbox, int lo,
+    int hi, const int *__restrict__ flag, const double2 *__restrict__ cen,
+    const int *__restrict__ chi, int clo, int nchildren, int *__restrict__ cnt) {
+    extern __shared__ int hist[];
+    if (HIST) {
+        for (int k = threadIdx.x; k < nchildren; k += blockDim.x) hist[k] = 0;
+        __syncthreads();
+    }
+    const int lane = threadIdx.x & 31;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n;
+         base += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = base + threadIdx.x;
+        int key = -1;
+        if (i < n) {
+            const int b = pbox[i];
+            if (b >= lo && b < hi && flag[b - lo]) {
+                key = chi[4 * b + child_digit(pts[i], cen[b])];
+                pbox[i] = key;
+            }
+        }
+        if (HIST) {
+            if (key >= 0) atomicAdd(&hist[key - clo], 1);
+        } else {
+            const unsigned peers = __match_any_sync(0xffffffffu, key);
+            if (key >= 0 && lane == __ffs(peers) - 1) atomicAdd(&cnt[key], __popc(peers));
+        }
+    }
+    if (HIST) {
+        __syncthreads();
+        for (int k = threadIdx.x; k < nchildren; k += blockDim.x)
+            if (hist[k]) atomicAdd(&cnt[clo + k], hist[k]);
+    }
+}
+
 }  // namespace
 
 void build_tree(const double2 *d_src, int ns, const double2 *d_targ, int nt,
@@ -504,6 +547,7 @@ void build_tree(const double2 *d_src, int ns, const double2 *d_targ, int nt,
     Builder B(T, s);
     // ---- root: bounding square of sources and targets ----
     const int nblk = 2 * kNumSM;
+    prof_mark("tree_start", s);
     DevBuf<double> part(4 * nblk, s);
     bbox_kernel<<<nblk, 256, 0, s>>>(d_src, ns, d_targ, nt, part.get());
     FMM_CHECK_LAUNCH();
@@ -575,24 +619,25 @@ void build_tree(const double2 *d_src, int ns, const double2 *d_targ, int nt,
         T.lend.push_back(T.nboxes);
         const double2 *cen = T.centers.get();
         const int *chi = T.child.get();
-        int *csw = B.cnt_s.get(), *ctw = B.cnt_t.get();
-        int *ps = pbs.get(), *pt = pbt.get();
-        for_each(ns, s, [=] __device__(int64_t i) {
-            const int b = ps[i];
-            if (b < lo || b >= hi || !fp[b - lo]) return;
-            const int kb = chi[4 * b + child_digit(d_src[i], cen[b])];
-            ps[i] = kb;
-            atomicAdd(&csw[kb], 1);
-        });
-        for_each(nt, s, [=] __device__(int64_t i) {
-            const int b = pt[i];
-            if (b < lo || b >= hi || !fp[b - lo]) return;
-            const int kb = chi[4 * b + child_digit(d_targ[i], cen[b])];
-            pt[i] = kb;
-            atomicAdd(&ctw[kb], 1);
-        });
+        const int nch = T.nboxes - nb0;
+        for (int set = 0; set < 2; set++) {
+            const int n = set == 0 ? ns : nt;
+            if (n <= 0) continue;
+            const double2 *pts = set == 0 ? d_src : d_targ;
+            int *pb = set == 0 ? pbs.get() : pbt.get();
+            int *cnt = set == 0 ? B.cnt_s.get() : B.cnt_t.get();
+            const int blocks = (int)std::min<int64_t>(((int64_t)n + 255) / 256, kNumSM * 4);
+            if (nch <= kHistChildren)
+                assign_children_kernel<true><<<blocks, 256, nch * sizeof(int), s>>>(
+                    n, pts, pb, lo, hi, fp, cen, chi, nb0, nch, cnt);
+            else
+                assign_children_kernel<false><<<blocks, 256, 0, s>>>(
+                    n, pts, pb, lo, hi, fp, cen, chi, nb0, nch, cnt);
+            FMM_CHECK_LAUNCH();
+        }
     }
     T.nlevels = ilev;
+    prof_mark("tree_refine", s);
     pbs.release();
     pbt.release();
     B.cnt_s.release();
@@ -600,9 +645,11 @@ void build_tree(const double2 *d_src, int ns, const double2 *d_targ, int nt,
     // ---- colleagues and level restriction ----
     B.computecoll(0, T.nlevels);
     if (T.nlevels >= 2) B.fix_lr();
+    prof_mark("tree_fixlr", s);
     // ---- point permutations ----
     B.sort_points(d_src, ns, T.srcse, T.isrc);
     B.sort_points(d_targ, nt, T.trgse, T.itarg);
+    prof_mark("tree_sort", s);
     T.d_boxsize.alloc(T.nlevels + 2, s);
     std::vector<double> bsx(T.boxsize);
     bsx.push_back(T.boxsize.back() / 2);
