@@ -239,7 +239,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["auto", "fp64", "mixed"])
+    ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed"])
+    ap.add_argument("--no-fp64-compare", action="store_true")
+    ap.add_argument("--accuracy-sample", type=int, default=10000)
     ap.add_argument("--ns", type=int, default=NS_DEFAULT)
     ap.add_argument("--nt", type=int, default=NT_DEFAULT)
     ap.add_argument("--eps", type=float, default=1e-6)
@@ -319,26 +321,74 @@ def main():
         return [a_.elapsed_time(b_) for a_, b_ in evs], prof
 
     # ---- device-resident ----
-    for _ in range(args.warmup):
+    prec_code = {"auto": 0, "fp64": 1, "mixed": 2}
+
+    def measure(precision):
+        L.fmm2d_b200_set_precision(prec_code[precision])
+        for _ in range(args.warmup):
+            call(dev_args)
+        torch.cuda.synchronize()
+        barrier()
+        clocks = ClockSampler(local)
+        clocks.start()
+        torch.cuda.synchronize()
+        barrier()
+        n0 = L.fmm2d_b200_launch_count()
+        ms, prof = timed(dev_args, args.steps, profile=True)
+        n1 = L.fmm2d_b200_launch_count()
+        torch.cuda.synchronize()
+        barrier()
+        clk = clocks.stop()
+        t = sum(ms) / len(ms)
+        if ws > 1:
+            tt = torch.tensor([t], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+        return t, prof, clk, int(n1 - n0)
+
+    def accuracy(precision):
+        """relative l2 errors at sampled targets vs the GPU FP64 direct sum"""
+        L.fmm2d_b200_set_precision(prec_code[precision])
         call(dev_args)
-    torch.cuda.synchronize()
-    barrier()
-    clocks = ClockSampler(local)
-    clocks.start()
-    torch.cuda.synchronize()
-    barrier()
-    n0 = L.fmm2d_b200_launch_count()
-    ms, prof = timed(dev_args, args.steps, profile=True)
-    n1 = L.fmm2d_b200_launch_count()
-    torch.cuda.synchronize()
-    barrier()
-    clk = clocks.stop()
-    t_step = sum(ms) / len(ms)
-    if ws > 1:
-        tt = torch.tensor([t_step], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_step = float(tt.item())
+        torch.cuda.synchronize()
+        m = min(args.accuracy_sample, nt)
+        idx = np.random.default_rng(99).choice(nt, m, replace=False)
+        sub = torch.from_numpy(np.ascontiguousarray(trg[idx])).to(dev)
+        pot = torch.zeros(2 * m, dtype=torch.float64, device=dev)
+        grad = torch.zeros(4 * m, dtype=torch.float64, device=dev)
+        ierd = L.fmm2d_b200_l2d_direct(1, ns, ptr(d_src), 1, ptr(d_q), 1, ptr(d_d),
+                                       ptr(d_v), m, ptr(sub), 2, ptr(pot), ptr(grad),
+                                       None, ctypes.c_double(1e-300))
+        if ierd != 0:
+            raise RuntimeError(fm.last_error())
+        torch.cuda.synchronize()
+        ix = torch.from_numpy(idx).to(dev)
+        got_p = d_pt.view(-1, 2)[ix]
+        got_g = d_gt.view(-1, 4)[ix]
+        rel = lambda a, b: float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
+        return {"pottarg_rel_l2": rel(got_p, pot.view(-1, 2)),
+                "gradtarg_rel_l2": rel(got_g, grad.view(-1, 4)), "targets": m}
+
+    t_step, prof, clk, nlaunch = measure(args.precision)
     value = ws * (ns + nt) / (t_step * 1e-3)
+    fp64 = None
+    if args.precision != "fp64" and not args.no_fp64_compare:
+        t64, prof64, clk64, _ = measure("fp64")
+        ph64 = {}
+        for p_ in prof64:
+            for k, v_ in p_.items():
+                if not k.startswith("#"):
+                    ph64.setdefault(k, []).append(v_)
+        fp64 = {"value": ws * (ns + nt) / (t64 * 1e-3), "unit": "points/s",
+                "ms_per_step": t64, "speedup_of_headline": t64 / t_step,
+                "phase_ms": {k: round(sum(v_) / len(v_), 4) for k, v_ in ph64.items()}}
+    acc = None
+    if rank == 0 and args.accuracy_sample > 0 and nt > 0:
+        acc = {"sample": f"{min(args.accuracy_sample, nt)} random targets vs GPU FP64 direct sum over all sources",
+               args.precision: accuracy(args.precision)}
+        if fp64 is not None:
+            acc["fp64"] = accuracy("fp64")
+    L.fmm2d_b200_set_precision(prec_code[args.precision])
 
     # ---- end to end through the C ABI with pinned host buffers ----
     e2e = None
@@ -416,13 +466,14 @@ def main():
         "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic",
+        "dtype": "f32+f64" if args.precision != "fp64" else "f64", "data": "synthetic",
         "config": {"workload": f"lfmm2d_st_cd_g uniform {ns}+{nt} points eps {args.eps:g}",
                    "precision": args.precision, "ns": ns, "nt": nt,
                    "eps": args.eps, "parallelism": f"replicas{ws}",
                    "l2": "inputs 0.8 GB > L2; no flush"},
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
-        "gpu_launches": int(n1 - n0), "clocks": clk,
+        "gpu_launches": nlaunch, "clocks": clk, "fp64_plain": fp64,
+        "accuracy": acc,
     }
     print(json.dumps(line))
     return 0

@@ -210,11 +210,9 @@ void run_laplace_family(const FmmCall &c, CallCtx &ctx) {
     // ---- outputs in tree order ----
     const int spgh = c.ifpgh, tpgh = nt > 0 ? c.ifpghtarg : 0;
     DevBuf<double2> spot, sgrad, shess, tpot, tgrad, thess;
+    // (the far-field pass is the first writer of every output)
     auto mk = [&](DevBuf<double2> &b, int n, bool need) {
-        if (need && n > 0) {
-            b.alloc((size_t)n * ndc, s);
-            b.zero(s);
-        }
+        if (need && n > 0) b.alloc((size_t)n * ndc, s);
     };
     mk(spot, ns, spgh >= 1);
     mk(sgrad, ns, spgh >= 2);
@@ -247,6 +245,9 @@ void run_laplace_family(const FmmCall &c, CallCtx &ctx) {
     // thresh = boxsize(0) * 2^-51 (c_translation/src/cfmm2d.c:994)
     P.thresh = T.boxsize[0] * std::ldexp(1.0, -51);
     P.ifnear = c.ifnear;
+    // mixed precision for eps >= 1e-6 unless all-FP64 is requested
+    const int prec = c.precision;
+    P.mixed = prec == kPrecMixed || (prec == kPrecAuto && c.eps >= 0.5e-6);
     cauchy_fmm(T, P, s);
     // ---- back to input order, in the caller's layout ----
     auto unsort = [&](int n, const int *perm, int pgh, const DevBuf<double2> &po,

@@ -10,6 +10,7 @@
 // c_translation/src/laprouts2d.c and cauchykernels2d.c term by term.
 #include "laplace.cuh"
 
+#include <algorithm>
 #include <mutex>
 #include <stdlib.h>
 #include <string.h>
@@ -418,102 +419,155 @@ __global__ void __launch_bounds__(kBlock) l2l_kernel(
 }
 
 // ---------------------------------------------------------------------------
-// Steps 6 and 7 for one point set: M2P over list 3 (l2dmpevalp/g/h,
-// laprouts2d.c:193-356) and L2P at leaves (l2dtaevalp/g/h, :508-664).
-// Lanes run over the box's points; series by Horner's rule.
+// Precision of the evaluation passes: FP64 throughout (plain), or FP32
+// series and pair arithmetic with FP64 point differences and FP64 output
+// accumulation (mixed).
 // ---------------------------------------------------------------------------
-template <int CH>
-__global__ void __launch_bounds__(kBlock) eval_far_kernel(
-    int lo, int hi, const int *__restrict__ nchild,
-    const int *__restrict__ level, const double2 *__restrict__ centers,
-    const double *__restrict__ bs, const int *__restrict__ nlist3,
-    const int *__restrict__ list3, const int2 *__restrict__ sse, PointSet set,
-    int ndc, int c0, int p, int nlevels, const double2 *__restrict__ mp,
-    const double2 *__restrict__ loc) {
-    const int lane = lane_id();
-    const int stride = (p + 1) * ndc;
-    const int pgh = set.pgh;
-    for (int b = lo + warp_global(); b < hi; b += warp_count()) {
+template <bool MIXED> struct Real;
+template <> struct Real<false> {
+    typedef double T;
+    typedef double2 T2;
+    static __device__ __forceinline__ T log_(T x) { return log(x); }
+    static __device__ __forceinline__ T rcp(T x) { return 1.0 / x; }
+};
+template <> struct Real<true> {
+    typedef float T;
+    typedef float2 T2;
+    static __device__ __forceinline__ T log_(T x) { return __logf(x); }
+    static __device__ __forceinline__ T rcp(T x) { return __fdividef(1.0f, x); }
+};
+
+template <class T2> __device__ __forceinline__ T2 mk2(double a, double b);
+template <> __device__ __forceinline__ double2 mk2<double2>(double a, double b) { return make_double2(a, b); }
+template <> __device__ __forceinline__ float2 mk2<float2>(double a, double b) { return make_float2((float)a, (float)b); }
+template <class T2> __device__ __forceinline__ T2 cv2(double2 v) { return mk2<T2>(v.x, v.y); }
+
+template <class T2> __device__ __forceinline__ T2 zmul(T2 a, T2 b) {
+    T2 r;
+    r.x = a.x * b.x - a.y * b.y;
+    r.y = a.x * b.y + a.y * b.x;
+    return r;
+}
+template <class T2> __device__ __forceinline__ void zfma(T2 &acc, T2 a, T2 b) {
+    acc.x = fma(a.x, b.x, fma(-a.y, b.y, acc.x));
+    acc.y = fma(a.x, b.y, fma(a.y, b.x, acc.y));
+}
+template <class T2, class T> __device__ __forceinline__ T2 zscal(T2 a, T s) {
+    T2 r;
+    r.x = a.x * s;
+    r.y = a.y * s;
+    return r;
+}
+template <class T2> __device__ __forceinline__ T2 zadd(T2 a, T2 b) {
+    T2 r;
+    r.x = a.x + b.x;
+    r.y = a.y + b.y;
+    return r;
+}
+template <class T2> __device__ __forceinline__ void add_out(double2 &o, T2 v) {
+    o.x += (double)v.x;
+    o.y += (double)v.y;
+}
+
+// Leaf of every point of a set, in tree order.
+__global__ void leaf_of_kernel(int nb, const int *__restrict__ nchild,
+                               const int2 *__restrict__ se, int *__restrict__ leaf) {
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
         if (nchild[b] != 0) continue;
-        const int2 rg = set.se[b];
-        if (rg.y <= rg.x) continue;
+        const int2 r = se[b];
+        for (int k = r.x; k < r.y; k++) leaf[k] = b;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Steps 6 and 7 for one point set, one thread per point: M2P over the
+// leaf's list 3 (l2dmpevalp/g/h, laprouts2d.c:193-356) and L2P of the
+// leaf's local expansion (l2dtaevalp/g/h, :508-664), both by Horner's rule
+// with the first and second derivatives carried along as requested.
+// This pass stores the outputs (it is their first writer); P2P adds.
+// ---------------------------------------------------------------------------
+template <int CH, int PGH, bool MIXED>
+__global__ void __launch_bounds__(256) eval_far_points_kernel(
+    int n, const int *__restrict__ leaf, const int *__restrict__ level,
+    const double2 *__restrict__ centers, const double *__restrict__ bs,
+    const int *__restrict__ nlist3, const int *__restrict__ list3,
+    const int2 *__restrict__ sse, PointSet set, int ndc, int c0, int p,
+    int nlevels, const double2 *__restrict__ mp,
+    const double2 *__restrict__ loc) {
+    typedef typename Real<MIXED>::T R;
+    typedef typename Real<MIXED>::T2 R2;
+    const int stride = (p + 1) * ndc;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int b = leaf[k];
         const int lb = level[b];
-        const double2 cb = centers[b];
-        const double rb = bs[lb];
+        const double2 x = set.pos[k];
+        R2 po[CH], gr[CH], he[CH];
+#pragma unroll
+        for (int q = 0; q < CH; q++) po[q] = gr[q] = he[q] = mk2<R2>(0.0, 0.0);
         const int n3 = (lb >= 1 && lb <= nlevels - 1) ? nlist3[b] : 0;
-        for (int t0 = rg.x; t0 < rg.y; t0 += 32) {
-            const int t = t0 + lane;
-            const bool act = t < rg.y;
-            const double2 x = act ? set.pos[t] : cb;
-            double2 po[CH], gr[CH], he[CH];
+        for (int e = 0; e < n3; e++) {
+            const int jb = list3[kMaxList3 * b + e];
+            if (sse[jb].y <= sse[jb].x) continue;  // no multipole
+            const double2 cj = centers[jb];
+            const double r = bs[level[jb]];
+            const double zx = x.x - cj.x, zy = x.y - cj.y;
+            const double zz = zx * zx + zy * zy;
+            const R2 zi = mk2<R2>(zx / zz, -zy / zz);                 // 1/z
+            const R2 w = mk2<R2>(r * zx / zz, -r * zy / zz);          // r/z
+            const R lz = (R)0.5 * Real<MIXED>::log_((R)zz);
+            const R rinv = (R)(1.0 / r);
 #pragma unroll
-            for (int q = 0; q < CH; q++)
-                po[q] = gr[q] = he[q] = make_double2(0.0, 0.0);
-            // list 3: multipoles of the finer separated boxes
-            for (int e = 0; e < n3; e++) {
-                const int jb = list3[kMaxList3 * b + e];
-                if (sse[jb].y <= sse[jb].x) continue;  // no multipole
-                const double2 cj = centers[jb];
-                const double r = bs[level[jb]];
-                double2 z = make_double2(x.x - cj.x, x.y - cj.y);
-                if (!act) z = make_double2(r, 0.0);
-                const double2 zi = cinv(z);
-                const double2 w = cscal(zi, r);
-                const double lz = 0.5 * log(z.x * z.x + z.y * z.y);
-#pragma unroll
-                for (int q = 0; q < CH; q++) {
-                    const double2 *M = mp + (size_t)jb * stride + c0 + q;
-                    double2 q0 = M[(size_t)p * ndc], q1 = make_double2(0.0, 0.0),
-                            q2 = make_double2(0.0, 0.0);
-                    for (int n = p - 1; n >= 0; n--) {
-                        const double2 Mn = n >= 1 ? M[(size_t)n * ndc] : make_double2(0.0, 0.0);
-                        q2 = cadd(cmul(q2, w), q1);
-                        q1 = cadd(cmul(q1, w), q0);
-                        q0 = cadd(cmul(q0, w), Mn);
-                    }
-                    const double2 M0 = M[0];
-                    po[q] = cadd(po[q], cadd(cscal(M0, lz), q0));
-                    if (pgh >= 2) {
-                        const double2 w2 = cmul(w, w);
-                        const double2 g = csub(cmul(M0, zi), cscal(cmul(q1, w2), 1.0 / r));
-                        gr[q] = cadd(gr[q], g);
-                        if (pgh >= 3) {
-                            const double2 w3 = cmul(w2, w), w4 = cmul(w2, w2);
-                            double2 h = cscal(cmul(M0, cmul(zi, zi)), -1.0);
-                            h = cadd(h, cscal(cmul(q2, w4), 2.0 / (r * r)));
-                            h = cadd(h, cscal(cmul(q1, w3), 2.0 / (r * r)));
-                            he[q] = cadd(he[q], h);
-                        }
+            for (int q = 0; q < CH; q++) {
+                const double2 *M = mp + (size_t)jb * stride + c0 + q;
+                R2 q0 = cv2<R2>(M[(size_t)p * ndc]), q1 = mk2<R2>(0.0, 0.0), q2 = mk2<R2>(0.0, 0.0);
+                for (int m = p - 1; m >= 1; m--) {
+                    if (PGH >= 3) q2 = zadd(zmul(q2, w), q1);
+                    if (PGH >= 2) q1 = zadd(zmul(q1, w), q0);
+                    q0 = zadd(zmul(q0, w), cv2<R2>(M[(size_t)m * ndc]));
+                }
+                if (PGH >= 3) q2 = zadd(zmul(q2, w), q1);
+                if (PGH >= 2) q1 = zadd(zmul(q1, w), q0);
+                q0 = zmul(q0, w);
+                const R2 M0 = cv2<R2>(M[0]);
+                po[q] = zadd(po[q], zadd(zscal(M0, lz), q0));
+                if (PGH >= 2) {
+                    const R2 w2 = zmul(w, w);
+                    gr[q] = zadd(gr[q], zadd(zmul(M0, zi), zscal(zmul(q1, w2), -rinv)));
+                    if (PGH >= 3) {
+                        const R2 w3 = zmul(w2, w), w4 = zmul(w2, w2);
+                        R2 h = zscal(zmul(M0, zmul(zi, zi)), (R)-1);
+                        h = zadd(h, zscal(zmul(q2, w4), (R)2 * rinv * rinv));
+                        h = zadd(h, zscal(zmul(q1, w3), (R)2 * rinv * rinv));
+                        he[q] = zadd(he[q], h);
                     }
                 }
             }
-            // local expansion of the leaf
-            {
-                const double2 z = make_double2((x.x - cb.x) / rb, (x.y - cb.y) / rb);
+        }
+        {
+            const double2 cb = centers[b];
+            const double rb = bs[lb];
+            const R2 z = mk2<R2>((x.x - cb.x) / rb, (x.y - cb.y) / rb);
+            const R rinv = (R)(1.0 / rb);
 #pragma unroll
-                for (int q = 0; q < CH; q++) {
-                    const double2 *Lc = loc + (size_t)b * stride + c0 + q;
-                    double2 q0 = Lc[(size_t)p * ndc], q1 = make_double2(0.0, 0.0),
-                            q2 = make_double2(0.0, 0.0);
-                    for (int n = p - 1; n >= 0; n--) {
-                        q2 = cadd(cmul(q2, z), q1);
-                        q1 = cadd(cmul(q1, z), q0);
-                        q0 = cadd(cmul(q0, z), Lc[(size_t)n * ndc]);
-                    }
-                    po[q] = cadd(po[q], q0);
-                    if (pgh >= 2) gr[q] = cadd(gr[q], cscal(q1, 1.0 / rb));
-                    if (pgh >= 3) he[q] = cadd(he[q], cscal(q2, 2.0 / (rb * rb)));
+            for (int q = 0; q < CH; q++) {
+                const double2 *Lc = loc + (size_t)b * stride + c0 + q;
+                R2 q0 = cv2<R2>(Lc[(size_t)p * ndc]), q1 = mk2<R2>(0.0, 0.0), q2 = mk2<R2>(0.0, 0.0);
+                for (int m = p - 1; m >= 0; m--) {
+                    if (PGH >= 3) q2 = zadd(zmul(q2, z), q1);
+                    if (PGH >= 2) q1 = zadd(zmul(q1, z), q0);
+                    q0 = zadd(zmul(q0, z), cv2<R2>(Lc[(size_t)m * ndc]));
                 }
+                po[q] = zadd(po[q], q0);
+                if (PGH >= 2) gr[q] = zadd(gr[q], zscal(q1, rinv));
+                if (PGH >= 3) he[q] = zadd(he[q], zscal(q2, (R)2 * rinv * rinv));
             }
-            if (act) {
+        }
 #pragma unroll
-                for (int q = 0; q < CH; q++) {
-                    const size_t o = (size_t)t * ndc + c0 + q;
-                    set.pot[o] = cadd(set.pot[o], po[q]);
-                    if (pgh >= 2) set.grad[o] = cadd(set.grad[o], gr[q]);
-                    if (pgh >= 3) set.hess[o] = cadd(set.hess[o], he[q]);
-                }
-            }
+        for (int q = 0; q < CH; q++) {
+            const size_t o = (size_t)k * ndc + c0 + q;
+            set.pot[o] = make_double2((double)po[q].x, (double)po[q].y);
+            if (PGH >= 2) set.grad[o] = make_double2((double)gr[q].x, (double)gr[q].y);
+            if (PGH >= 3) set.hess[o] = make_double2((double)he[q].x, (double)he[q].y);
         }
     }
 }
@@ -523,127 +577,233 @@ __global__ void __launch_bounds__(kBlock) eval_far_kernel(
 //   pot += q log|z| + d/z,  grad += q/z - d/z^2,  hess += -q/z^2 + 2d/z^3,
 // z = t - s; pairs with |z|^2 <= thresh^2 (pot only) or < thresh^2 skipped.
 // A warp takes up to 32 targets of one box; when the box has fewer, lane
-// groups split the sources and are summed at the end.
+// groups split the sources and are summed at the end.  Point differences
+// are formed in FP64 in both precisions.
 // ---------------------------------------------------------------------------
-constexpr int kP2PStage = 64;
+// One warp per box takes the box's targets of both point sets (targets
+// first, then sources as targets).  The sources of all list-1 boxes are
+// staged once into shared memory (FP64 positions, strengths in the pass's
+// precision), in chunks of kP2PStage; the targets are split into chunks of
+// T <= 32 chosen to keep as many lanes busy as possible, each chunk's
+// lanes forming G = 32 / T groups that split the staged sources and are
+// summed at the end.  Point differences are formed in FP64 in both
+// precisions.
+constexpr int kP2PStage = 128;
+constexpr int kP2PWarps = 4;
 
-template <int CH, int PGH, bool IFC, bool IFD>
-__device__ __forceinline__ void p2p_pair(double2 x, double2 s, const double2 *qv,
-                                         const double2 *dv, double th2,
-                                         double2 *po, double2 *gr, double2 *he) {
-    const double dx = x.x - s.x, dy = x.y - s.y;
-    const double rr = dx * dx + dy * dy;
-    if (PGH == 1 ? (rr <= th2) : (rr < th2)) return;
-    const double rinv2 = 1.0 / rr;
-    const double2 zi = make_double2(dx * rinv2, -dy * rinv2);
-    double rl = 0.0;
-    if (IFC) rl = 0.5 * log(rr);
-    double2 zi2 = make_double2(0.0, 0.0), zi3 = make_double2(0.0, 0.0);
-    if (PGH >= 2 || IFD) zi2 = cmul(zi, zi);
-    if (PGH >= 3 && IFD) zi3 = cmul(zi2, zi);
-#pragma unroll
-    for (int q = 0; q < CH; q++) {
-        if (IFC) {
-            po[q].x = fma(rl, qv[q].x, po[q].x);
-            po[q].y = fma(rl, qv[q].y, po[q].y);
-            if (PGH >= 2) cfma(gr[q], zi, qv[q]);
-            if (PGH >= 3) cfma(he[q], cscal(zi2, -1.0), qv[q]);
-        }
-        if (IFD) {
-            cfma(po[q], zi, dv[q]);
-            if (PGH >= 2) cfma(gr[q], cscal(zi2, -1.0), dv[q]);
-            if (PGH >= 3) cfma(he[q], cscal(zi3, 2.0), dv[q]);
-        }
-    }
+// Point positions as the near field reads them: FP64 (x, y), or for the
+// mixed pass a float4 (x_hi, x_lo, y_hi, y_lo) with x = x_hi + x_lo, whose
+// FP32 difference (x_hi - x'_hi) + (x_lo - x'_lo) carries the FP64
+// difference to FP32 accuracy without FP64 instructions.
+template <bool MIXED> struct PosT { typedef double2 T; };
+template <> struct PosT<true> { typedef float4 T; };
+
+__device__ __forceinline__ float4 split_pos(double2 p) {
+    const float xh = (float)p.x, yh = (float)p.y;
+    return make_float4(xh, (float)(p.x - (double)xh), yh, (float)(p.y - (double)yh));
 }
 
-template <int CH, int PGH, bool IFC, bool IFD>
-__global__ void __launch_bounds__(kBlock) p2p_kernel(
+__device__ __forceinline__ void pos_diff(double2 a, double2 b, double &dx, double &dy) {
+    dx = a.x - b.x;
+    dy = a.y - b.y;
+}
+__device__ __forceinline__ void pos_diff(float4 a, float4 b, float &dx, float &dy) {
+    dx = (a.x - b.x) + (a.y - b.y);
+    dy = (a.z - b.z) + (a.w - b.w);
+}
+
+__device__ __forceinline__ float rcp_fast(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float half_ln_fast(float x) {  // 0.5 * ln(x)
+    float r;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r * 0.34657359027997264f;  // ln(2) / 2
+}
+__device__ __forceinline__ double rcp_pair(double x) { return 1.0 / x; }
+__device__ __forceinline__ float rcp_pair(float x) { return rcp_fast(x); }
+__device__ __forceinline__ double half_ln_pair(double x) { return 0.5 * log(x); }
+__device__ __forceinline__ float half_ln_pair(float x) { return half_ln_fast(x); }
+
+template <int CH, int PGH, bool IFC, bool IFD, bool MIXED>
+__global__ void __launch_bounds__(kP2PWarps * 32) p2p_kernel(
     int lo, int hi, const int *__restrict__ nlist1,
     const int *__restrict__ list1, const int *__restrict__ nchild,
-    int leaves, const int2 *__restrict__ sse, const double2 *__restrict__ src,
-    const double2 *__restrict__ chg, const double2 *__restrict__ dip,
-    PointSet set, int ndc, int c0, double th2) {
-    // per-warp buffer: staged sources during the sweep, partial sums after
-    constexpr int kStage = kP2PStage * (1 + (IFC ? CH : 0) + (IFD ? CH : 0));
-    constexpr int kRed = 32 * 3 * CH;
-    constexpr int kBuf = kStage > kRed ? kStage : kRed;
-    __shared__ double2 s_buf[kWarpsPerBlock][kBuf];
+    int leaves, const int2 *__restrict__ sse,
+    const typename PosT<MIXED>::T *__restrict__ src,
+    const typename Real<MIXED>::T2 *__restrict__ chg,
+    const typename Real<MIXED>::T2 *__restrict__ dip, PointSet sset,
+    PointSet tset, const typename PosT<MIXED>::T *__restrict__ spos,
+    const typename PosT<MIXED>::T *__restrict__ tpos, int ndc, int c0,
+    double th2d) {
+    typedef typename Real<MIXED>::T R;
+    typedef typename Real<MIXED>::T2 R2;
+    typedef typename PosT<MIXED>::T PT;
+    constexpr int kStr = (IFC ? CH : 0) + (IFD ? CH : 0);
+    constexpr int kRed = 3 * CH;
+    constexpr int kWarpBytes = kP2PStage * (16 + kStr * (int)sizeof(R2));
+    extern __shared__ __align__(16) unsigned char p2p_smem[];
     const int lane = lane_id(), wib = threadIdx.x >> 5;
-    double2 *s_pos = s_buf[wib];
-    double2 *s_q = s_pos + kP2PStage;
-    double2 *s_d = s_q + (IFC ? kP2PStage * CH : 0);
+    PT *s_pos = reinterpret_cast<PT *>(p2p_smem + (size_t)wib * kWarpBytes);
+    R2 *s_str = reinterpret_cast<R2 *>(s_pos + kP2PStage);
+    R2 *red = s_str;  // reused for the group sums
+    // (the FP32 threshold is kept above zero so that coincident points are
+    // skipped even when thresh^2 underflows)
+    const R th2 = MIXED ? (R)fmax(th2d, 1.1754943508222875e-38) : (R)th2d;
     for (int b = lo + warp_global(); b < hi; b += warp_count()) {
         const int n1 = nlist1[b];
         if (n1 == 0) continue;
         if ((nchild[b] == 0) != (leaves != 0)) continue;
-        const int2 rg = set.se[b];
-        if (rg.y <= rg.x) continue;
-        for (int t0 = rg.x; t0 < rg.y; t0 += 32) {
-            const int T = min(32, rg.y - t0);
+        const int2 tr = tset.pgh > 0 ? tset.se[b] : make_int2(0, 0);
+        const int2 sr0 = sset.pgh > 0 ? sset.se[b] : make_int2(0, 0);
+        const int ntb = tr.y - tr.x, nsb = sr0.y - sr0.x, ntot = ntb + nsb;
+        if (ntot == 0) continue;
+        // list-1 source ranges and their running offsets
+        int jstart = 0, jcount = 0;  // lane e < n1 holds entry e
+        if (lane < n1) {
+            const int2 r = sse[list1[kMaxList1 * b + lane]];
+            jstart = r.x;
+            jcount = r.y - r.x;
+        }
+        int jofs = jcount;  // inclusive prefix over entries
+#pragma unroll
+        for (int d = 1; d < 16; d <<= 1) {
+            const int o = __shfl_up_sync(0xffffffffu, jofs, d);
+            if (lane >= d) jofs += o;
+        }
+        const int nsrc = __shfl_sync(0xffffffffu, jofs, n1 - 1);
+        jofs -= jcount;  // exclusive
+        if (nsrc == 0) continue;
+        // target chunking: c chunks of T = ceil(ntot / c) minimising the
+        // lane sweeps c * ceil(min(nsrc, stage) / (32 / T))
+        int best_c = (ntot + 31) / 32, best_cost = 1 << 30;
+        const int ns_eff = min(nsrc, kP2PStage);
+        for (int c = (ntot + 31) / 32; c <= (ntot + 31) / 32 + 3 && c <= ntot; c++) {
+            const int Tc = (ntot + c - 1) / c;
+            const int cost = c * ((ns_eff + 32 / Tc - 1) / (32 / Tc));
+            if (cost < best_cost) {
+                best_cost = cost;
+                best_c = c;
+            }
+        }
+        const int Tch = (ntot + best_c - 1) / best_c;
+        for (int t0 = 0; t0 < ntot; t0 += Tch) {
+            const int T = min(Tch, ntot - t0);
             const int G = 32 / T;
             const int g = lane / T, tl = lane - g * T;
             const bool act = g < G;
-            const double2 x = act ? set.pos[t0 + tl] : make_double2(0.0, 0.0);
-            double2 po[CH], gr[CH], he[CH];
+            const int it = t0 + tl;
+            const bool is_t = it < ntb;
+            PT x;
+            if (act)
+                x = is_t ? tpos[tr.x + it] : spos[sr0.x + it - ntb];
+            else
+                x = spos[sr0.x];  // any valid point; results discarded
+            R2 po[CH], gr[CH], he[CH];
 #pragma unroll
-            for (int q = 0; q < CH; q++)
-                po[q] = gr[q] = he[q] = make_double2(0.0, 0.0);
-            for (int e = 0; e < n1; e++) {
-                const int jb = list1[kMaxList1 * b + e];
-                const int2 sr = sse[jb];
-                for (int s0 = sr.x; s0 < sr.y; s0 += kP2PStage) {
-                    const int ns = min(kP2PStage, sr.y - s0);
-                    for (int k = lane; k < ns; k += 32) {
-                        s_pos[k] = src[s0 + k];
+            for (int q = 0; q < CH; q++) po[q] = gr[q] = he[q] = mk2<R2>(0.0, 0.0);
+            for (int s0 = 0; s0 < nsrc; s0 += kP2PStage) {
+                const int nst = min(kP2PStage, nsrc - s0);
+                __syncwarp();
+                for (int i0 = 0; i0 < nst; i0 += 32) {  // warp-uniform trip count
+                    // source i of the concatenated list-1 ranges
+                    const int i = i0 + lane;
+                    const int gi = s0 + i;
+                    int e = 0;
+                    for (int u = 1; u < n1; u++)
+                        if (__shfl_sync(0xffffffffu, jofs, u) <= gi) e = u;
+                    const int k = __shfl_sync(0xffffffffu, jstart, e) + gi -
+                                  __shfl_sync(0xffffffffu, jofs, e);
+                    if (i >= nst) continue;
+                    s_pos[i] = src[k];
+#pragma unroll
+                    for (int q = 0; q < CH; q++) {
+                        if (IFC) s_str[i * kStr + q] = chg[(size_t)k * ndc + c0 + q];
+                        if (IFD) s_str[i * kStr + (IFC ? CH : 0) + q] = dip[(size_t)k * ndc + c0 + q];
+                    }
+                }
+                __syncwarp();
+                if (act) {
+#pragma unroll 4
+                    for (int kk = g; kk < nst; kk += G) {
+                        R dx, dy;
+                        pos_diff(x, s_pos[kk], dx, dy);
+                        const R rr = dx * dx + dy * dy;
+                        // skipped pairs contribute exactly zero, without a branch
+                        const bool skip = PGH == 1 ? (rr <= th2) : (rr < th2);
+                        const R rrs = skip ? (R)1 : rr;
+                        const R ri = skip ? (R)0 : rcp_pair(rrs);
+                        R2 zi;
+                        zi.x = dx * ri;
+                        zi.y = -dy * ri;
+                        R2 zi2 = mk2<R2>(0.0, 0.0), zi3 = mk2<R2>(0.0, 0.0);
+                        if (PGH >= 2 || IFD) zi2 = zmul(zi, zi);
+                        if (PGH >= 3 && IFD) zi3 = zmul(zi2, zi);
+                        R rl = 0;
+                        if (IFC) rl = skip ? (R)0 : half_ln_pair(rrs);
 #pragma unroll
                         for (int q = 0; q < CH; q++) {
-                            if (IFC) s_q[k * CH + q] = chg[(size_t)(s0 + k) * ndc + c0 + q];
-                            if (IFD) s_d[k * CH + q] = dip[(size_t)(s0 + k) * ndc + c0 + q];
+                            if (IFC) {
+                                const R2 qv = s_str[kk * kStr + q];
+                                po[q].x = fma(rl, qv.x, po[q].x);
+                                po[q].y = fma(rl, qv.y, po[q].y);
+                                if (PGH >= 2) zfma(gr[q], zi, qv);
+                                if (PGH >= 3) zfma(he[q], zscal(zi2, (R)-1), qv);
+                            }
+                            if (IFD) {
+                                const R2 dv = s_str[kk * kStr + (IFC ? CH : 0) + q];
+                                zfma(po[q], zi, dv);
+                                if (PGH >= 2) zfma(gr[q], zscal(zi2, (R)-1), dv);
+                                if (PGH >= 3) zfma(he[q], zscal(zi3, (R)2), dv);
+                            }
                         }
                     }
-                    __syncwarp();
-                    if (act) {
-                        for (int k = g; k < ns; k += G) {
-                            p2p_pair<CH, PGH, IFC, IFD>(
-                                x, s_pos[k], IFC ? &s_q[k * CH] : nullptr,
-                                IFD ? &s_d[k * CH] : nullptr, th2, po, gr, he);
-                        }
-                    }
-                    __syncwarp();
                 }
             }
             // sum the lane groups
-            double2 *red = s_buf[wib];
+            if (G > 1) {
+                __syncwarp();
 #pragma unroll
-            for (int q = 0; q < CH; q++) {
-                red[(lane * 3 + 0) * CH + q] = po[q];
-                red[(lane * 3 + 1) * CH + q] = gr[q];
-                red[(lane * 3 + 2) * CH + q] = he[q];
-            }
-            __syncwarp();
-            if (act && g == 0) {
-                for (int gg = 1; gg < G; gg++) {
-                    const int ol = gg * T + tl;
+                for (int q = 0; q < CH; q++) {
+                    red[lane * kRed + q] = po[q];
+                    if (PGH >= 2) red[lane * kRed + CH + q] = gr[q];
+                    if (PGH >= 3) red[lane * kRed + 2 * CH + q] = he[q];
+                }
+                __syncwarp();
+                if (act && g == 0) {
+                    for (int gg = 1; gg < G; gg++) {
+                        const int ol = gg * T + tl;
 #pragma unroll
-                    for (int q = 0; q < CH; q++) {
-                        po[q] = cadd(po[q], red[(ol * 3 + 0) * CH + q]);
-                        gr[q] = cadd(gr[q], red[(ol * 3 + 1) * CH + q]);
-                        he[q] = cadd(he[q], red[(ol * 3 + 2) * CH + q]);
+                        for (int q = 0; q < CH; q++) {
+                            po[q] = zadd(po[q], red[ol * kRed + q]);
+                            if (PGH >= 2) gr[q] = zadd(gr[q], red[ol * kRed + CH + q]);
+                            if (PGH >= 3) he[q] = zadd(he[q], red[ol * kRed + 2 * CH + q]);
+                        }
                     }
                 }
-                const int t = t0 + tl;
+            }
+            if (act && g == 0) {
+                const PointSet &S = is_t ? tset : sset;
+                const int t = is_t ? tr.x + it : sr0.x + it - ntb;
+                const int pg = S.pgh;
 #pragma unroll
                 for (int q = 0; q < CH; q++) {
                     const size_t o = (size_t)t * ndc + c0 + q;
-                    set.pot[o] = cadd(set.pot[o], po[q]);
-                    if (PGH >= 2) set.grad[o] = cadd(set.grad[o], gr[q]);
-                    if (PGH >= 3) set.hess[o] = cadd(set.hess[o], he[q]);
+                    add_out(S.pot[o], po[q]);
+                    if (PGH >= 2 && pg >= 2) add_out(S.grad[o], gr[q]);
+                    if (PGH >= 3 && pg >= 3) add_out(S.hess[o], he[q]);
                 }
             }
-            __syncwarp();
         }
     }
+}
+
+template <int CH, bool IFC, bool IFD, bool MIXED>
+constexpr size_t p2p_smem_bytes() {
+    return (size_t)kP2PWarps * kP2PStage *
+           (16 + ((IFC ? CH : 0) + (IFD ? CH : 0)) * sizeof(typename Real<MIXED>::T2));
 }
 
 int grid_for(int nwarps) {
@@ -652,17 +812,27 @@ int grid_for(int nwarps) {
     return blocks < 1 ? 1 : blocks;
 }
 
-template <int CH, int PGH>
-void launch_p2p_t(const Tree &T, const CauchyProblem &P, const PointSet &set,
-                  int c0, double th2, int lo, int hi, int leaves,
-                  cudaStream_t s) {
-    const int g = grid_for(hi - lo);
+template <int CH, int PGH, bool MIXED>
+void launch_p2p_t(const Tree &T, const CauchyProblem &P, int c0, double th2,
+                  int lo, int hi, int leaves, cudaStream_t s) {
+    typedef typename Real<MIXED>::T2 R2;
+    const int g = std::max(1, std::min((hi - lo + kP2PWarps - 1) / kP2PWarps, kNumSM * 16));
     const int *n1 = T.nlist1.get(), *l1 = T.list1.get(), *nc = T.nchild.get();
     const int2 *sse = T.srcse.get();
+    typedef typename PosT<MIXED>::T PT;
+    const R2 *chg = MIXED ? (const R2 *)P.charge32 : (const R2 *)P.charge;
+    const R2 *dip = MIXED ? (const R2 *)P.dipstr32 : (const R2 *)P.dipstr;
+    const PT *spos = MIXED ? (const PT *)P.src_hl : (const PT *)P.src;
+    const PT *tpos = MIXED ? (const PT *)P.trg_hl : (const PT *)P.tset.pos;
 #define FMM_P2P_CASE(IFC, IFD)                                                  \
-    p2p_kernel<CH, PGH, IFC, IFD><<<g, kBlock, 0, s>>>(                         \
-        lo, hi, n1, l1, nc, leaves, sse, P.src, P.charge, P.dipstr, set,       \
-        P.ndc, c0, th2)
+    do {                                                                        \
+        constexpr size_t sm = p2p_smem_bytes<CH, IFC, IFD, MIXED>();            \
+        auto kern = p2p_kernel<CH, PGH, IFC, IFD, MIXED>;                       \
+        FMM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); \
+        kern<<<g, kP2PWarps * 32, sm, s>>>(lo, hi, n1, l1, nc, leaves, sse,     \
+                                          spos, chg, dip, P.sset, P.tset, spos, \
+                                          tpos, P.ndc, c0, th2);                \
+    } while (0)
     if (P.ifcharge && P.ifdipole)
         FMM_P2P_CASE(true, true);
     else if (P.ifcharge)
@@ -673,15 +843,48 @@ void launch_p2p_t(const Tree &T, const CauchyProblem &P, const PointSet &set,
     FMM_CHECK_LAUNCH();
 }
 
+// P2P for both point sets over boxes [lo, hi): leaves, or the non-leaf
+// boxes that hold list-1 entries (a second launch, so that no two warps
+// write the same point).
 template <int CH>
-void launch_p2p(const Tree &T, const CauchyProblem &P, const PointSet &set,
-                int c0, double th2, int lo, int hi, int leaves, cudaStream_t s) {
-    switch (set.pgh) {
-        case 1: launch_p2p_t<CH, 1>(T, P, set, c0, th2, lo, hi, leaves, s); break;
-        case 2: launch_p2p_t<CH, 2>(T, P, set, c0, th2, lo, hi, leaves, s); break;
-        case 3: launch_p2p_t<CH, 3>(T, P, set, c0, th2, lo, hi, leaves, s); break;
+void launch_p2p(const Tree &T, const CauchyProblem &P, int c0, double th2,
+                int lo, int hi, int leaves, cudaStream_t s) {
+    const int pgh = std::max(P.sset.n > 0 ? P.sset.pgh : 0, P.tset.n > 0 ? P.tset.pgh : 0);
+#define FMM_P2P_PGH(PG)                                                         \
+    if (P.mixed)                                                                \
+        launch_p2p_t<CH, PG, true>(T, P, c0, th2, lo, hi, leaves, s);           \
+    else                                                                        \
+        launch_p2p_t<CH, PG, false>(T, P, c0, th2, lo, hi, leaves, s);
+    switch (pgh) {
+        case 1: FMM_P2P_PGH(1) break;
+        case 2: FMM_P2P_PGH(2) break;
+        case 3: FMM_P2P_PGH(3) break;
         default: break;
     }
+#undef FMM_P2P_PGH
+}
+
+template <int CH>
+void launch_eval_far(const Tree &T, const CauchyProblem &P, const PointSet &set,
+                     const int *leaf, int c0, const double2 *mp,
+                     const double2 *loc, cudaStream_t s) {
+    const int blocks = std::max(1, std::min((set.n + 255) / 256, kNumSM * 8));
+#define FMM_EVAL_CASE(PG, MX)                                                   \
+    eval_far_points_kernel<CH, PG, MX><<<blocks, 256, 0, s>>>(                  \
+        set.n, leaf, T.level.get(), T.centers.get(), T.d_boxsize.get(),         \
+        T.nlist3.get(), T.list3.get(), T.srcse.get(), set, P.ndc, c0, P.p,      \
+        T.nlevels, mp, loc)
+    if (P.mixed) {
+        if (set.pgh == 1) FMM_EVAL_CASE(1, true);
+        if (set.pgh == 2) FMM_EVAL_CASE(2, true);
+        if (set.pgh == 3) FMM_EVAL_CASE(3, true);
+    } else {
+        if (set.pgh == 1) FMM_EVAL_CASE(1, false);
+        if (set.pgh == 2) FMM_EVAL_CASE(2, false);
+        if (set.pgh == 3) FMM_EVAL_CASE(3, false);
+    }
+#undef FMM_EVAL_CASE
+    FMM_CHECK_LAUNCH();
 }
 
 // Upward pass for channels [c0, c0 + CH): P2M at the leaves of levels >= 2,
@@ -764,50 +967,57 @@ void downward_chunk(const Tree &T, const CauchyProblem &P, int c0,
     // steps 6-7: list-3 multipoles and local expansions at the points
     for (const PointSet *set : {&P.tset, &P.sset}) {
         if (set->pgh <= 0 || set->n <= 0) continue;
-        eval_far_kernel<CH><<<grid_for(nb), kBlock, 0, s>>>(
-            0, nb, T.nchild.get(), T.level.get(), T.centers.get(), bs,
-            T.nlist3.get(), T.list3.get(), T.srcse.get(), *set, P.ndc, c0, p,
-            L, mp, loc);
-        FMM_CHECK_LAUNCH();
+        launch_eval_far<CH>(T, P, *set, set == &P.tset ? P.tleaf : P.sleaf, c0,
+                            mp, loc, s);
     }
     prof_mark("m2p_l2p", s);
     // step 8: near field over list 1 (leaves, then any non-leaf box that
     // holds list-1 entries, so that no two warps write the same point)
     if (P.ifnear) {
-        for (const PointSet *set : {&P.tset, &P.sset}) {
-            if (set->pgh <= 0 || set->n <= 0) continue;
-            const double th2 = P.thresh * P.thresh;
-            launch_p2p<CH>(T, P, *set, c0, th2, 0, nb, 1, s);
-            launch_p2p<CH>(T, P, *set, c0, th2, 0, nb, 0, s);
-        }
+        const double th2 = P.thresh * P.thresh;
+        launch_p2p<CH>(T, P, c0, th2, 0, nb, 1, s);
+        launch_p2p<CH>(T, P, c0, th2, 0, nb, 0, s);
     }
     prof_mark("p2p", s);
 }
 
 // Work counts of one evaluation for the roofline: list-2 pairs translated
 // (boxes passing the step-4 test) and near-field point pairs.
+__global__ void count_work_kernel(int nb, EvalCounts ec, const int *__restrict__ lev,
+                                  const int *__restrict__ n1, const int *__restrict__ l1,
+                                  const int *__restrict__ n2,
+                                  unsigned long long *__restrict__ c) {
+    unsigned long long a0 = 0, a1 = 0, a2 = 0;
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+        if (lev[b] >= 2 && ec.npts(b) > 0) a0 += (unsigned long long)n2[b];
+        if (n1[b] > 0) {
+            unsigned long long ns_ = 0;
+            for (int e = 0; e < n1[b]; e++) ns_ += count(ec.sse, l1[kMaxList1 * b + e]);
+            if (ec.spgh > 0) a1 += ns_ * (unsigned long long)count(ec.sse, b);
+            if (ec.tpgh > 0) a2 += ns_ * (unsigned long long)count(ec.tse, b);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&c[0], a0);
+        atomicAdd(&c[1], a1);
+        atomicAdd(&c[2], a2);
+    }
+}
+
 void count_work(const Tree &T, const CauchyProblem &P, cudaStream_t s) {
     DevBuf<unsigned long long> cnt(3, s);
     cnt.zero(s);
-    unsigned long long *c = cnt.get();
     const EvalCounts ec{T.srcse.get(), T.trgse.get(), P.sset.pgh, P.tset.pgh};
-    const int *lev = T.level.get(), *n1 = T.nlist1.get(), *l1 = T.list1.get(),
-              *n2 = T.nlist2.get();
-    const int2 *sse = T.srcse.get(), *tse = T.trgse.get();
-    const int spgh = P.sset.pgh, tpgh = P.tset.pgh;
-    for_each(T.nboxes, s, [=] __device__(int64_t i) {
-        const int b = (int)i;
-        if (lev[b] >= 2 && ec.npts(b) > 0 && n2[b] > 0)
-            atomicAdd(&c[0], (unsigned long long)n2[b]);
-        if (n1[b] > 0) {
-            unsigned long long ns_ = 0;
-            for (int e = 0; e < n1[b]; e++) ns_ += count(sse, l1[kMaxList1 * b + e]);
-            if (spgh > 0) atomicAdd(&c[1], ns_ * (unsigned long long)count(sse, b));
-            if (tpgh > 0) atomicAdd(&c[2], ns_ * (unsigned long long)count(tse, b));
-        }
-    });
+    count_work_kernel<<<kNumSM * 2, 256, 0, s>>>(T.nboxes, ec, T.level.get(), T.nlist1.get(),
+                                                 T.list1.get(), T.nlist2.get(), cnt.get());
+    FMM_CHECK_LAUNCH();
     unsigned long long h[3];
-    FMM_CUDA(cudaMemcpyAsync(h, c, sizeof(h), cudaMemcpyDeviceToHost, s));
+    FMM_CUDA(cudaMemcpyAsync(h, cnt.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
     FMM_CUDA(cudaStreamSynchronize(s));
     prof_set_count("m2l_pairs", (double)h[0]);
     prof_set_count("p2p_pairs_src", (double)h[1]);
@@ -846,8 +1056,54 @@ const double *device_binomials(cudaStream_t s) {
     return tab[dev];
 }
 
-void cauchy_fmm(const Tree &T, const CauchyProblem &P, cudaStream_t s) {
-    if (profiling_enabled()) count_work(T, P, s);
+void cauchy_fmm(const Tree &T, const CauchyProblem &P0, cudaStream_t s) {
+    if (profiling_enabled()) count_work(T, P0, s);
+    CauchyProblem P = P0;
+    // leaf of every sorted point, for the per-point far-field evaluation
+    DevBuf<int> sleaf(std::max(P.sset.n, 1), s), tleaf(std::max(P.tset.n, 1), s);
+    {
+        const int blocks = std::max(1, std::min((T.nboxes + 255) / 256, kNumSM * 8));
+        if (P.sset.pgh > 0 && P.sset.n > 0) {
+            leaf_of_kernel<<<blocks, 256, 0, s>>>(T.nboxes, T.nchild.get(), T.srcse.get(), sleaf.get());
+            FMM_CHECK_LAUNCH();
+        }
+        if (P.tset.pgh > 0 && P.tset.n > 0) {
+            leaf_of_kernel<<<blocks, 256, 0, s>>>(T.nboxes, T.nchild.get(), T.trgse.get(), tleaf.get());
+            FMM_CHECK_LAUNCH();
+        }
+        P.sleaf = sleaf.get();
+        P.tleaf = tleaf.get();
+    }
+    // FP32 copies of the strengths for the mixed-precision near field
+    DevBuf<float2> chg32, dip32;
+    if (P.mixed) {
+        const size_t nv = (size_t)P.sset.n * P.ndc;
+        auto conv = [&](const double2 *in, DevBuf<float2> &out) {
+            if (!in || !nv) return;
+            out.alloc(nv, s);
+            float2 *o = out.get();
+            for_each((int64_t)nv, s, [=] __device__(int64_t i) {
+                o[i] = make_float2((float)in[i].x, (float)in[i].y);
+            });
+        };
+        conv(P.charge, chg32);
+        conv(P.dipstr, dip32);
+        P.charge32 = chg32.get();
+        P.dipstr32 = dip32.get();
+    }
+    // hi/lo FP32 positions for the mixed near field
+    DevBuf<float4> shl, thl;
+    if (P.mixed) {
+        auto split = [&](const double2 *in, int n, DevBuf<float4> &out) {
+            out.alloc(std::max(n, 1), s);
+            float4 *o = out.get();
+            for_each(n, s, [=] __device__(int64_t i) { o[i] = split_pos(in[i]); });
+        };
+        split(P.src, P.sset.n, shl);
+        split(P.tset.pos, P.tset.n, thl);
+        P.src_hl = shl.get();
+        P.trg_hl = thl.get();
+    }
     if (2 * P.p > kLdc)
         throw FmmError(4, "expansion order above the supported maximum (64)");
     const double *binom = device_binomials(s);

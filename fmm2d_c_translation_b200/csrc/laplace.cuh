@@ -14,7 +14,7 @@ namespace fmm2d {
 struct PointSet {
     const double2 *pos = nullptr;  // (x, y), sorted
     const int2 *se = nullptr;      // per-box [start, end)
-    int n = 0;
+    int n = 0;                     // (the sources' n is also the source count)
     int pgh = 0;                   // 0 none, 1 pot, 2 +grad, 3 +hess
     double2 *pot = nullptr, *grad = nullptr, *hess = nullptr;  // [i*ndc + c]
 };
@@ -30,11 +30,18 @@ struct CauchyProblem {
     PointSet tset;                    // targets
     double thresh = 0;                // near-field exclusion radius
     int ifnear = 1;
+    bool mixed = false;               // FP32 series / pair arithmetic
+    const int *sleaf = nullptr;       // leaf of every sorted source (set by cauchy_fmm)
+    const int *tleaf = nullptr;       // leaf of every sorted target
+    const float2 *charge32 = nullptr; // FP32 strengths (mixed near field)
+    const float2 *dipstr32 = nullptr;
+    const float4 *src_hl = nullptr;   // hi/lo FP32 positions (mixed near field)
+    const float4 *trg_hl = nullptr;
     double *timeinfo = nullptr;       // 8 phase times (s), optional
 };
 
 // Runs steps 1-8 of cfmm2dmain (src/laplace/cfmm2d.f:442-1340) on the
-// device.  Outputs in sset / tset must be zeroed by the caller.
+// device.  The outputs in sset / tset are overwritten.
 void cauchy_fmm(const Tree &T, const CauchyProblem &P, cudaStream_t s);
 
 // Direct sums over all sources for every point of `set` (the reference's

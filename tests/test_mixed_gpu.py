@@ -1,0 +1,80 @@
+"""Mixed-precision mode (FP32 series and pair arithmetic, FP64 geometry and
+output accumulation): for eps >= 1e-6 every result stays within the
+requested eps of the FP64 direct sum and of the reference FMM at the same
+eps (relative l2 over sampled points)."""
+import numpy as np
+import pytest
+
+import pointsets as ps
+import refimpl
+import wrappers as W
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def mlib():
+    import fmm2d_c_translation_b200 as fm
+    L = fm.lib()
+    L.fmm2d_b200_set_precision(2)
+    yield L
+    L.fmm2d_b200_set_precision(0)
+
+
+def inputs(ns, nt, seed, dist):
+    rng = np.random.default_rng(seed)
+    if dist == "uniform":
+        src, trg = ps.uniform(ns, seed), ps.uniform(nt, seed + 1)
+    elif dist == "blobs":
+        src, trg = ps.blobs(ns, seed), ps.blobs(nt, seed + 1)
+    else:
+        src = ps.starfish(ns, seed)[0]
+        trg = ps.near_curve_targets(nt, seed + 1)
+    q = rng.standard_normal(ns) + 1j * rng.standard_normal(ns)
+    d = rng.standard_normal(ns) + 1j * rng.standard_normal(ns)
+    th = rng.uniform(0, 2 * np.pi, ns)
+    v = np.stack([np.cos(th), np.sin(th)])
+    return src, trg, q, d, v
+
+
+def direct(src, q, d, v, pts, m, pgh):
+    ns = src.shape[1]
+    pot = np.zeros(m, complex)
+    grad = np.zeros((m, 2), complex)
+    hess = np.zeros((m, 3), complex)
+    s = np.ascontiguousarray(src.T)
+    refimpl.orc().oracle_l2d_direct(
+        ns, W._p(s), 1, W._p(q), 1, W._p(d), W._p(np.ascontiguousarray(v.T)), 0, m,
+        W._p(np.ascontiguousarray(pts[:, :m].T)), pgh, W._p(pot), W._p(grad),
+        W._p(hess), 1e-300)
+    return pot, grad, hess
+
+
+@pytest.mark.parametrize("eps", [1e-3, 1e-6])
+@pytest.mark.parametrize("dist", ["uniform", "blobs", "starfish"])
+def test_mixed_within_eps(mlib, eps, dist):
+    src, trg, q, d, v = inputs(40000, 20000, 7, dist)
+    got, ier = W.call(mlib, "l", "st_cd_h", eps, src, q, d, v, trg)
+    assert ier == 0
+    m = 400
+    dp, dg, dh = direct(src, q, d, v, trg, m, 3)
+    assert W.rel_err(got["pottarg"][:m], dp) <= eps
+    assert W.rel_err(got["gradtarg"][:m], dg) <= eps
+    assert W.rel_err(got["hesstarg"][:m], dh) <= 10 * eps
+    sp, sg, _ = direct(src, q, d, v, src, m, 2)
+    assert W.rel_err(got["pot"][:m], sp) <= eps
+    assert W.rel_err(got["grad"][:m], sg) <= eps
+    want, ier = W.call(refimpl.ref(), "l", "st_cd_h", eps, src, q, d, v, trg)
+    for k in ("pot", "grad", "pottarg", "gradtarg"):
+        assert W.rel_err(got[k], want[k]) <= eps, k
+
+
+@pytest.mark.parametrize("variant", ["s_c_p", "t_d_g", "st_cd_g"])
+@pytest.mark.parametrize("family", ["l", "c"])
+def test_mixed_variants_match_reference(mlib, family, variant):
+    src, trg, q, d, v = inputs(20000, 5000, 9, "blobs")
+    got, ier = W.call(mlib, family, variant, 1e-6, src, q, d, v, trg)
+    want, ier2 = W.call(refimpl.ref(), family, variant, 1e-6, src, q, d, v, trg)
+    assert ier == 0 and ier2 == 0
+    for k in want:
+        assert W.rel_err(got[k], want[k]) <= 1e-6, k
