@@ -11,6 +11,7 @@
 #include "laplace.cuh"
 
 #include <algorithm>
+#include <complex>
 #include <mutex>
 #include <stdlib.h>
 #include <string.h>
@@ -218,6 +219,11 @@ __global__ void __launch_bounds__(kBlock) m2m_kernel(
     const int lane = lane_id();
     const int wib = threadIdx.x >> 5;
     double2 *ht = sh_m2m + (size_t)wib * (p + 1) * CH;
+    // binomials C(l, m), 0 <= m <= l < p, row stride p (after the warp buffers)
+    double *bsh = reinterpret_cast<double *>(sh_m2m + (size_t)kWarpsPerBlock * (p + 1) * CH);
+    for (int e = threadIdx.x; e < p * p; e += blockDim.x)
+        bsh[e] = binom[(size_t)(e / p) * (kLdc + 1) + (e % p)];
+    __syncthreads();
     const int stride = (p + 1) * ndc;
     for (int b = lo + warp_global(); b < hi; b += warp_count()) {
         if (nchild[b] == 0) continue;
@@ -253,7 +259,7 @@ __global__ void __launch_bounds__(kBlock) m2m_kernel(
                             t = ht[q];
                         } else {
                             t = cscal(ht[q], -1.0 / i);
-                            const double *brow = binom + (size_t)(i - 1) * (kLdc + 1);
+                            const double *brow = bsh + (size_t)(i - 1) * p;
                             for (int j = 1; j <= i; j++) {
                                 const double cb_ = brow[j - 1];
                                 t.x = fma(cb_, ht[j * CH + q].x, t.x);
@@ -378,6 +384,11 @@ __global__ void __launch_bounds__(kBlock) l2l_kernel(
     const int lane = lane_id();
     const int wib = threadIdx.x >> 5;
     double2 *jt = sh_l2l + (size_t)wib * (p + 1) * CH;
+    // binomials C(j, i), 0 <= i, j <= p, as bsh[j * (p + 1) + i]
+    double *bsh = reinterpret_cast<double *>(sh_l2l + (size_t)kWarpsPerBlock * (p + 1) * CH);
+    for (int e = threadIdx.x; e < (p + 1) * (p + 1); e += blockDim.x)
+        bsh[e] = binom[(size_t)(e / (p + 1)) * (kLdc + 1) + (e % (p + 1))];
+    __syncthreads();
     const int stride = (p + 1) * ndc;
     for (int b = lo + warp_global(); b < hi; b += warp_count()) {
         const int pb = parent[b];
@@ -405,7 +416,7 @@ __global__ void __launch_bounds__(kBlock) l2l_kernel(
                 for (int q = 0; q < CH; q++) {
                     double2 t = make_double2(0.0, 0.0);
                     for (int j = i; j <= p; j++) {
-                        const double cb_ = binom[(size_t)j * (kLdc + 1) + i];
+                        const double cb_ = bsh[(size_t)j * (p + 1) + i];
                         t.x = fma(cb_, jt[j * CH + q].x, t.x);
                         t.y = fma(cb_, jt[j * CH + q].y, t.y);
                     }
@@ -887,29 +898,269 @@ void launch_eval_far(const Tree &T, const CauchyProblem &P, const PointSet &set,
     FMM_CHECK_LAUNCH();
 }
 
+// ---------------------------------------------------------------------------
+// Expansion operators with one thread per (box, coefficient): every thread
+// owns one coefficient of one box for the chunk's channels, so lanes are
+// never idle on short expansions and no warp shuffles are needed.
+// ---------------------------------------------------------------------------
+
+// Step 1, P2M (l2dformmpc/d/cd, laprouts2d.c:41-190) at the leaves of levels
+// >= 2 with sources:  M_0 += q,  M_k += -q z^k / k,  M_k += d z^(k-1) / r,
+// z = (x - c) / r.
+template <int CH>
+__global__ void __launch_bounds__(256) p2m_coef_kernel(
+    int lo, int hi, int p, const int *__restrict__ nchild,
+    const double2 *__restrict__ centers, const int *__restrict__ level,
+    const double *__restrict__ bs, const int2 *__restrict__ sse,
+    const double2 *__restrict__ src, const double2 *__restrict__ chg,
+    const double2 *__restrict__ dip, int ifc, int ifd, int ndc, int c0,
+    double2 *__restrict__ mp) {
+    const int np1 = p + 1, stride = np1 * ndc;
+    const int64_t n = (int64_t)(hi - lo) * np1;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int b = lo + (int)(t / np1), k = (int)(t % np1);
+        if (nchild[b] != 0) continue;
+        const int2 rg = sse[b];
+        if (rg.y <= rg.x) continue;
+        const double2 c = centers[b];
+        const double r = bs[level[b]], rinv = 1.0 / r;
+        double2 acc[CH];
+#pragma unroll
+        for (int q = 0; q < CH; q++) acc[q] = make_double2(0.0, 0.0);
+        const double ck = k > 0 ? -1.0 / k : 0.0;
+        for (int j = rg.x; j < rg.y; j++) {
+            const double2 x = src[j];
+            const double2 z = make_double2((x.x - c.x) / r, (x.y - c.y) / r);
+            const double2 zk1 = k > 0 ? zpow_int(z, k - 1) : make_double2(0.0, 0.0);
+            const double2 zk = k > 0 ? cmul(zk1, z) : make_double2(1.0, 0.0);
+#pragma unroll
+            for (int q = 0; q < CH; q++) {
+                if (ifc) {
+                    const double2 qq = chg[(size_t)j * ndc + c0 + q];
+                    if (k == 0)
+                        acc[q] = cadd(acc[q], qq);
+                    else
+                        cfma(acc[q], qq, cscal(zk, ck));
+                }
+                if (ifd && k > 0) cfma(acc[q], dip[(size_t)j * ndc + c0 + q], cscal(zk1, rinv));
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < CH; q++) mp[(size_t)b * stride + (size_t)k * ndc + c0 + q] = acc[q];
+    }
+}
+
+// Step 2, P2L from list 4 (l2dformtac/d/cd, laprouts2d.c:358-505):
+//   L_0 += q log|z|,  L_k += -q (r/z)^k / k,  L_k += -d (r/z)^k / z.
+template <int CH>
+__global__ void __launch_bounds__(256) p2l_coef_kernel(
+    int lo, int hi, int p, EvalCounts ec, const int *__restrict__ nlist4,
+    const int *__restrict__ list4, const double2 *__restrict__ centers,
+    const int *__restrict__ level, const double *__restrict__ bs,
+    const double2 *__restrict__ src, const double2 *__restrict__ chg,
+    const double2 *__restrict__ dip, int ifc, int ifd, int ndc, int c0,
+    double2 *__restrict__ loc) {
+    const int np1 = p + 1, stride = np1 * ndc;
+    const int64_t n = (int64_t)(hi - lo) * np1;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int b = lo + (int)(t / np1), k = (int)(t % np1);
+        const int n4 = nlist4[b];
+        if (n4 == 0 || ec.npts(b) <= 0) continue;
+        const double2 c = centers[b];
+        const double r = bs[level[b]];
+        const double ck = k > 0 ? -1.0 / k : 0.0;
+        double2 acc[CH];
+#pragma unroll
+        for (int q = 0; q < CH; q++) acc[q] = make_double2(0.0, 0.0);
+        for (int e = 0; e < n4; e++) {
+            const int2 rg = ec.sse[list4[kMaxList4 * b + e]];
+            for (int j = rg.x; j < rg.y; j++) {
+                const double2 x = src[j];
+                const double2 z0 = make_double2(x.x - c.x, x.y - c.y);
+                const double2 zi = cinv(z0);
+                const double2 wk = zpow_int(cscal(zi, r), k);  // (r/z)^k
+                const double lz = k == 0 ? 0.5 * log(z0.x * z0.x + z0.y * z0.y) : 0.0;
+#pragma unroll
+                for (int q = 0; q < CH; q++) {
+                    if (ifc) {
+                        const double2 qq = chg[(size_t)j * ndc + c0 + q];
+                        if (k == 0)
+                            cfma(acc[q], qq, make_double2(lz, 0.0));
+                        else
+                            cfma(acc[q], qq, cscal(wk, ck));
+                    }
+                    if (ifd) cfma(acc[q], dip[(size_t)j * ndc + c0 + q], cscal(cmul(wk, zi), -1.0));
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < CH; q++) {
+            double2 &o = loc[(size_t)b * stride + (size_t)k * ndc + c0 + q];
+            o = cadd(o, acc[q]);
+        }
+    }
+}
+
+// Child position (0..3) of box b in its parent.
+__device__ __forceinline__ int child_pos(const int *__restrict__ child, int pb, int b) {
+    int c = 0;
+#pragma unroll
+    for (int j = 1; j < 4; j++)
+        if (child[4 * pb + j] == b) c = j;
+    return c;
+}
+
+// Step 3, M2M (l2dmpmp, laprouts2d.c:666-775) for the parents of one level:
+//   H_i = sum over children with sources of sum_j A[cpos][i][j] M_j,
+// with the fixed shift matrices A of the four child positions.
+template <int CH>
+__global__ void __launch_bounds__(256) m2m_coef_kernel(
+    int lo, int hi, int p, const int *__restrict__ nchild,
+    const int *__restrict__ child, const int2 *__restrict__ sse,
+    const double2 *__restrict__ A, int ndc, int c0, double2 *__restrict__ mp) {
+    const int np1 = p + 1, stride = np1 * ndc;
+    const int64_t n = (int64_t)(hi - lo) * np1;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int b = lo + (int)(t / np1), i = (int)(t % np1);
+        if (nchild[b] == 0) continue;
+        double2 acc[CH];
+#pragma unroll
+        for (int q = 0; q < CH; q++) acc[q] = make_double2(0.0, 0.0);
+        for (int cp = 0; cp < 4; cp++) {
+            const int cb = child[4 * b + cp];
+            if (count(sse, cb) <= 0) continue;
+            const double2 *Arow = A + ((size_t)cp * np1 + i) * np1;
+            const double2 *M = mp + (size_t)cb * stride + c0;
+            for (int j = 0; j <= i; j++) {
+                const double2 a = Arow[j];
+#pragma unroll
+                for (int q = 0; q < CH; q++) cfma(acc[q], a, M[(size_t)j * ndc + q]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < CH; q++) mp[(size_t)b * stride + (size_t)i * ndc + c0 + q] = acc[q];
+    }
+}
+
+// Step 5, L2L (l2dlocloc, laprouts2d.c:777-884) for the children of one
+// level whose parent holds points:  L_i += sum_{j>=i} A[cpos][i][j] Lp_j.
+template <int CH>
+__global__ void __launch_bounds__(256) l2l_coef_kernel(
+    int lo, int hi, int p, EvalCounts ec, const int *__restrict__ parent,
+    const int *__restrict__ child, const double2 *__restrict__ A, int ndc,
+    int c0, double2 *__restrict__ loc) {
+    const int np1 = p + 1, stride = np1 * ndc;
+    const int64_t n = (int64_t)(hi - lo) * np1;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int b = lo + (int)(t / np1), i = (int)(t % np1);
+        const int pb = parent[b];
+        if (ec.npts(pb) <= 0) continue;
+        const int cp = child_pos(child, pb, b);
+        const double2 *Arow = A + ((size_t)cp * np1 + i) * np1;
+        const double2 *Lp = loc + (size_t)pb * stride + c0;
+        double2 acc[CH];
+#pragma unroll
+        for (int q = 0; q < CH; q++) acc[q] = make_double2(0.0, 0.0);
+        for (int j = i; j <= p; j++) {
+            const double2 a = Arow[j];
+#pragma unroll
+            for (int q = 0; q < CH; q++) cfma(acc[q], a, Lp[(size_t)j * ndc + q]);
+        }
+#pragma unroll
+        for (int q = 0; q < CH; q++) {
+            double2 &o = loc[(size_t)b * stride + (size_t)i * ndc + c0 + q];
+            o = cadd(o, acc[q]);
+        }
+    }
+}
+
+// Fixed M2M / L2L shift matrices of the four child positions, in scaled
+// form (level independent): a child's center is its parent's +/- r_c / 2
+// in x and y (r_c the child's box size), so with s = sx + i sy, sx, sy = +-1,
+//   M2M: z0/r_child = s/2, z0/r_parent = s/4;  L2L: z0/r_parent = s/4,
+//   r_child/z0 = 2/s,
+// all exact in binary.  Layout [cpos][i][j], (p+1)^2 per position.
+const double2 *shift_tables(int p, bool m2m, cudaStream_t s) {
+    static std::mutex mu;
+    static std::vector<std::pair<long, const double2 *>> cache;
+    int dev;
+    FMM_CUDA(cudaGetDevice(&dev));
+    const long key = ((long)dev << 20) | ((long)p << 1) | (m2m ? 1 : 0);
+    std::lock_guard<std::mutex> g(mu);
+    for (auto &e : cache)
+        if (e.first == key) return e.second;
+    const int n = p + 1;
+    // exact binomials by the Pascal recurrence
+    std::vector<double> C((size_t)(2 * n + 1) * (2 * n + 1), 0.0);
+    const int nc = 2 * n + 1;
+    for (int l = 0; l < nc; l++) {
+        C[(size_t)l * nc] = 1.0;
+        C[(size_t)l * nc + l] = 1.0;
+        for (int m = 1; m < l; m++)
+            C[(size_t)l * nc + m] = C[(size_t)(l - 1) * nc + m - 1] + C[(size_t)(l - 1) * nc + m];
+    }
+    auto binom = [&](int l, int m) { return (m < 0 || m > l) ? 0.0 : C[(size_t)l * nc + m]; };
+    typedef std::complex<double> cd;
+    std::vector<double2> h((size_t)4 * n * n, make_double2(0.0, 0.0));
+    for (int cp = 0; cp < 4; cp++) {
+        const cd sgn((cp & 1) ? 1.0 : -1.0, (cp & 2) ? 1.0 : -1.0);
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                cd v(0.0, 0.0);
+                if (m2m) {
+                    const cd z_par = sgn / 4.0, rz_ch = 2.0 / sgn;  // z0/r2, r1/z0
+                    if (i == 0)
+                        v = (j == 0) ? cd(1.0, 0.0) : cd(0.0, 0.0);
+                    else if (j == 0)
+                        v = std::pow(z_par, i) * (-1.0 / i);
+                    else if (j <= i)
+                        v = std::pow(z_par, i) * binom(i - 1, j - 1) * std::pow(rz_ch, j);
+                } else {
+                    const cd z_par = sgn / 4.0, rz_ch = 2.0 / sgn;  // z0/r1, r2/z0
+                    if (j >= i) v = std::pow(rz_ch, i) * binom(j, i) * std::pow(z_par, j);
+                }
+                h[((size_t)cp * n + i) * n + j] = make_double2(v.real(), v.imag());
+            }
+    }
+    double2 *d = nullptr;
+    FMM_CUDA(cudaMalloc(&d, h.size() * sizeof(double2)));
+    FMM_CUDA(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
+    FMM_CUDA(cudaStreamSynchronize(s));
+    cache.push_back({key, d});
+    return d;
+}
+
 // Upward pass for channels [c0, c0 + CH): P2M at the leaves of levels >= 2,
 // then M2M from the finest parents up.
 template <int CH>
 void upward_chunk(const Tree &T, const CauchyProblem &P, int c0,
                   const double *binom, double2 *mp, cudaStream_t s) {
+    (void)binom;
     const int L = T.nlevels, p = P.p, nb = T.nboxes;
     const double *bs = T.d_boxsize.get();
-    const size_t sh_exp = (size_t)kWarpsPerBlock * (p + 1) * CH * sizeof(double2);
+    auto blocks = [&](int nbox) {
+        const int64_t n = (int64_t)nbox * (p + 1);
+        return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, kNumSM * 8));
+    };
     if (L >= 2) {
         const int lo = T.lstart[2];
-        p2m_kernel<CH><<<grid_for(nb - lo), kBlock, 0, s>>>(
-            lo, nb, T.nchild.get(), T.centers.get(), T.level.get(), bs,
+        p2m_coef_kernel<CH><<<blocks(nb - lo), 256, 0, s>>>(
+            lo, nb, p, T.nchild.get(), T.centers.get(), T.level.get(), bs,
             T.srcse.get(), P.src, P.charge, P.dipstr, P.ifcharge, P.ifdipole,
-            P.ndc, c0, p, mp);
+            P.ndc, c0, mp);
         FMM_CHECK_LAUNCH();
     }
     prof_mark("p2m", s);
+    const double2 *A = shift_tables(p, true, s);
     for (int l = L - 1; l >= 1; l--) {
         const int lo = T.lstart[l], hi = T.lend[l];
-        m2m_kernel<CH><<<grid_for(hi - lo), kBlock, sh_exp, s>>>(
-            lo, hi, T.nchild.get(), T.child.get(), T.centers.get(),
-            T.boxsize[l + 1], T.boxsize[l], T.srcse.get(), P.ndc, c0, p,
-            binom, mp);
+        m2m_coef_kernel<CH><<<blocks(hi - lo), 256, 0, s>>>(
+            lo, hi, p, T.nchild.get(), T.child.get(), T.srcse.get(), A, P.ndc,
+            c0, mp);
         FMM_CHECK_LAUNCH();
     }
     prof_mark("m2m", s);
@@ -945,22 +1196,28 @@ void downward_chunk(const Tree &T, const CauchyProblem &P, int c0,
     const double *bs = T.d_boxsize.get();
     const EvalCounts ec{T.srcse.get(), T.trgse.get(), P.sset.pgh, P.tset.pgh};
     const size_t sh_exp = (size_t)kWarpsPerBlock * (p + 1) * CH * sizeof(double2);
+    (void)sh_exp;
+    (void)binom;
+    auto blocks = [&](int nbox) {
+        const int64_t n = (int64_t)nbox * (p + 1);
+        return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, kNumSM * 8));
+    };
     // step 2: P2L from list 4 (after M2L, which initialises the locals)
     if (L >= 2) {
         const int lo = T.lstart[2];
-        p2l_kernel<CH><<<grid_for(nb - lo), kBlock, 0, s>>>(
-            lo, nb, ec, T.nlist4.get(), T.list4.get(), T.centers.get(),
+        p2l_coef_kernel<CH><<<blocks(nb - lo), 256, 0, s>>>(
+            lo, nb, p, ec, T.nlist4.get(), T.list4.get(), T.centers.get(),
             T.level.get(), bs, P.src, P.charge, P.dipstr, P.ifcharge,
-            P.ifdipole, P.ndc, c0, p, loc);
+            P.ifdipole, P.ndc, c0, loc);
         FMM_CHECK_LAUNCH();
     }
     prof_mark("p2l", s);
     // step 5: L2L, coarsest parents first
+    const double2 *A = shift_tables(p, false, s);
     for (int l = 1; l <= L - 1; l++) {
         const int lo = T.lstart[l + 1], hi = T.lend[l + 1];
-        l2l_kernel<CH><<<grid_for(hi - lo), kBlock, sh_exp, s>>>(
-            lo, hi, ec, T.parent.get(), T.centers.get(), T.boxsize[l],
-            T.boxsize[l + 1], P.ndc, c0, p, binom, loc);
+        l2l_coef_kernel<CH><<<blocks(hi - lo), 256, 0, s>>>(
+            lo, hi, p, ec, T.parent.get(), T.child.get(), A, P.ndc, c0, loc);
         FMM_CHECK_LAUNCH();
     }
     prof_mark("l2l", s);

@@ -24,6 +24,7 @@
 #include "sort.cuh"
 
 #include <algorithm>
+#include <stdlib.h>
 #include <vector>
 
 namespace fmm2d {
@@ -81,7 +82,7 @@ struct SegTable {
 };
 
 template <int MT, int KS, int CH>
-__global__ void __launch_bounds__(128) m2l_dmma_kernel(
+__global__ void __launch_bounds__(128, 4) m2l_dmma_kernel(
     SegTable seg, const int *__restrict__ boxes, const int *__restrict__ slots,
     const double *__restrict__ bs, int ndc, int c0, int p,
     const double *__restrict__ binom, const double2 *__restrict__ mp,
@@ -223,8 +224,10 @@ void launch_dmma(const SegTable &sg, const int *boxes, const int *slots,
                  const double *bs, int ndc, int p, const double *binom,
                  const double2 *mp, double2 *loc, int ntiles, cudaStream_t s) {
     const int blocks = std::max(1, std::min((ntiles + 3) / 4, kNumSM * 16));
+    const char *e = getenv("FMM2D_B200_M2L_CH2");
+    const bool ch2 = e && e[0] == '1';
     for (int c0 = 0; c0 < ndc;) {
-        if (ndc - c0 >= 2 && MT <= 5) {
+        if (ch2 && ndc - c0 >= 2 && MT <= 5) {
             m2l_dmma_kernel<MT, KS, 2><<<blocks, 128, 0, s>>>(
                 sg, boxes, slots, bs, ndc, c0, p, binom, mp, loc, ntiles);
             c0 += 2;
