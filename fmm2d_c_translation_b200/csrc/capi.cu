@@ -15,7 +15,11 @@
 // nt = 0 for the sources-only forms and ifpgh = 0 for the targets-only
 // forms, exactly as the Fortran wrappers do, and runs the evaluation on
 // the GPU.  Arrays may be host or device memory (see engine.cuh).
+#include <stdint.h>
+
 #include "engine.cuh"
+#include "hankel.cuh"
+#include "helmholtz.cuh"
 #include "runtime.cuh"
 
 using namespace fmm2d;
@@ -316,4 +320,65 @@ FMM_EXPORT int fmm2d_b200_set_precision(int mode) {
 FMM_EXPORT int fmm2d_b200_laplace_nterms(double eps) { return laplace_nterms(eps); }
 FMM_EXPORT int fmm2d_b200_leaf_capacity(double eps, int ns, int nt) {
     return leaf_capacity(eps, ns, nt);
+}
+
+// ---------------------------------------------------------------------------
+// bind(c) Helmholtz entry, src/helmholtz_c.f03:5-15: eps, zk and ns by
+// value, ns and ier 64-bit.  A complex double passed by value has the
+// calling convention of a struct of two doubles.
+// ---------------------------------------------------------------------------
+struct cplx_by_value {
+    double re, im;
+};
+
+FMM_EXPORT void hfmm2d_s_c_p(double eps, cplx_by_value zk, int64_t ns, const double *sources,
+                             const cplx_t *charge, cplx_t *pot, int64_t *ier) {
+    if (ns < 1 || ns > INT32_MAX) {
+        set_last_error("ns out of range for the 32-bit drivers");
+        *ier = 4;
+        return;
+    }
+    const double zkv[2] = {zk.re, zk.im};
+    const fint ns32 = (fint)ns;
+    fint ier32 = 0;
+    wrap(kHelmholtz, &eps, zkv, &ns32, sources, charge, nullptr, nullptr, 1, 0, 1, pot, nullptr,
+         nullptr, 0, nullptr, 0, nullptr, nullptr, nullptr, &ier32);
+    *ier = ier32;
+}
+
+// Helmholtz direct sum (h2d_direct*, c_translation/src/helmkernels2d.c):
+// increments pot(nd,nt), grad(nd,2,nt), hess(nd,3,nt); zk = (re, im).
+FMM_EXPORT int fmm2d_b200_h2d_direct(int nd, const double *zk, int ns, const double *sources,
+                                     int ifcharge, const double *charge, int ifdipole,
+                                     const double *dipstr, const double *dipvec, int nt,
+                                     const double *targ, int ifpgh, double *pot, double *grad,
+                                     double *hess, double thresh) {
+    return run_helm_direct(nd, zk, ns, sources, ifcharge, charge, ifdipole, dipstr, dipvec, nt,
+                           targ, ifpgh, pot, grad, hess, thresh);
+}
+
+// Host-only: the Helmholtz expansion order of h2dterms for a box size, and
+// H0, H1 of the library's own Hankel routine at n complex points
+// (z[2k], z[2k+1]) -> out[4k .. 4k+3] = (H0 re, im, H1 re, im).
+FMM_EXPORT int fmm2d_b200_helm_nterms(double bsize, double zk_re, double zk_im, double eps) {
+    return helm_nterms(bsize, make_double2(zk_re, zk_im), eps);
+}
+FMM_EXPORT void fmm2d_b200_hankel01(int n, const double *z, double *out) {
+    for (int k = 0; k < n; k++) {
+        double2 h0, h1;
+        hk::hankel01(make_double2(z[2 * k], z[2 * k + 1]), h0, h1);
+        out[4 * k] = h0.x;
+        out[4 * k + 1] = h0.y;
+        out[4 * k + 2] = h1.x;
+        out[4 * k + 3] = h1.y;
+    }
+}
+// Host-only: the scaled sequences the Helmholtz translations are built
+// from, out[0..n] complex (interleaved): H_k(z) rscale^k (h2dall) and
+// J_k(z) / rscale^k (jbessel2d).
+FMM_EXPORT void fmm2d_b200_helm_hvec(int n, double z_re, double z_im, double rscale, double *out) {
+    helm_hvec(n, make_double2(z_re, z_im), rscale, reinterpret_cast<double2 *>(out));
+}
+FMM_EXPORT void fmm2d_b200_helm_jvec(int n, double z_re, double z_im, double rscale, double *out) {
+    helm_jvec(n, make_double2(z_re, z_im), rscale, reinterpret_cast<double2 *>(out));
 }

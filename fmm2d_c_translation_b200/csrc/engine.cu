@@ -1,10 +1,11 @@
 // engine.cu -- the driver layer of one evaluation (the reference's
-// lfmm2d / cfmm2d drivers, src/laplace/lfmm2d.f:29-225 and
-// c_translation/src/cfmm2d.c:1053-1401): inputs to the device, tree and
-// lists, gather into tree order (with the complex-Laplace two-channel
-// split), the FMM passes, scatter back to input order (with the channel
-// recombination), outputs to the caller.
+// lfmm2d / cfmm2d / hfmm2d drivers, src/laplace/lfmm2d.f:29-225,
+// c_translation/src/cfmm2d.c:1053-1401 and hfmm2d.c:1529-1907): inputs to
+// the device, tree and lists, gather into tree order (with the
+// complex-Laplace two-channel split), the FMM passes, scatter back to input
+// order (with the channel recombination), outputs to the caller.
 #include "engine.cuh"
+#include "helmholtz.cuh"
 #include "laplace.cuh"
 #include "runtime.cuh"
 #include "tree.cuh"
@@ -304,7 +305,198 @@ void run_laplace_family(const FmmCall &c, CallCtx &ctx) {
         for (int k = 0; k < 8; k++) c.timeinfo[k] = 0.0;
 }
 
+
+// Gathers the Helmholtz inputs into tree order: charges and dipole
+// strengths (nd, ns) complex, dipole vectors (nd, 2, ns) as (v1, v2) pairs.
+struct HelmInputs {
+    DevBuf<double2> src, trg, chg, dip, dv;
+};
+
+void gather_helm(const FmmCall &c, const Tree &T, const double2 *src, const double2 *trg,
+                 const double2 *q, const double2 *d, const double *dv, HelmInputs &o,
+                 cudaStream_t s) {
+    const int nd = c.nd, ns = c.ns, nt = c.nt;
+    o.src.alloc(ns, s);
+    o.trg.alloc(std::max(nt, 1), s);
+    const int *perm = T.isrc.get();
+    {
+        double2 *so = o.src.get();
+        for_each(ns, s, [=] __device__(int64_t k) { so[k] = src[perm[k]]; });
+    }
+    if (nt > 0) {
+        const int *pt = T.itarg.get();
+        double2 *to = o.trg.get();
+        for_each(nt, s, [=] __device__(int64_t k) { to[k] = trg[pt[k]]; });
+    }
+    if (c.ifcharge) {
+        o.chg.alloc((size_t)ns * nd, s);
+        double2 *qo = o.chg.get();
+        for_each((int64_t)ns * nd, s, [=] __device__(int64_t t) {
+            const int64_t k = t / nd, j = t % nd;
+            qo[t] = q[(int64_t)perm[k] * nd + j];
+        });
+    }
+    if (c.ifdipole) {
+        o.dip.alloc((size_t)ns * nd, s);
+        o.dv.alloc((size_t)ns * nd, s);
+        double2 *dout = o.dip.get(), *vout = o.dv.get();
+        for_each((int64_t)ns * nd, s, [=] __device__(int64_t t) {
+            const int64_t k = t / nd, j = t % nd, i = perm[k];
+            dout[t] = d[i * nd + j];
+            vout[t] = make_double2(dv[(i * 2 + 0) * nd + j], dv[(i * 2 + 1) * nd + j]);
+        });
+    }
+}
+
+void run_helmholtz(const FmmCall &c, CallCtx &ctx) {
+    cudaStream_t s = ctx.stream();
+    const int nd = c.nd, ns = c.ns, nt = c.nt;
+    if (c.zk[0] == 0.0 && c.zk[1] == 0.0) throw FmmError(4, "zk must be nonzero");
+    const bool on_dev = is_device_ptr(c.sources);
+    prof_begin(s);
+    InBuf<double2> src_in, trg_in, chg_in, dip_in;
+    InBuf<double> dv_in;
+    src_in.set(c.sources, ns, on_dev, s);
+    trg_in.set(nt > 0 ? c.targ : nullptr, nt, on_dev, s);
+    if (c.ifcharge) chg_in.set(c.charge, (size_t)nd * ns, on_dev, s);
+    if (c.ifdipole) {
+        dip_in.set(c.dipstr, (size_t)nd * ns, on_dev, s);
+        dv_in.set(c.dipvec, (size_t)2 * nd * ns, on_dev, s);
+    }
+    prof_mark("h2d", s);
+    // hndiv2d (c_translation/src/hndiv2d.c) has the lndiv2d table
+    const int ndiv = c.ndiv >= 0 ? c.ndiv : leaf_capacity(c.eps, ns, nt);
+    const int idivflag = c.ndiv >= 0 ? c.idivflag : 0;
+    Tree T;
+    build_tree(src_in.ptr, ns, trg_in.ptr, nt, ndiv, idivflag, kMaxLevels, s, T);
+    compute_lists(T, s);
+    prof_mark("lists", s);
+    HelmInputs in;
+    gather_helm(c, T, src_in.ptr, trg_in.ptr, chg_in.ptr, dip_in.ptr, dv_in.ptr, in, s);
+    prof_mark("gather", s);
+    src_in.own.release();
+    chg_in.own.release();
+    dip_in.own.release();
+    dv_in.own.release();
+    const int spgh = c.ifpgh, tpgh = nt > 0 ? c.ifpghtarg : 0;
+    DevBuf<double2> spot, sgrad, shess, tpot, tgrad, thess;
+    auto mk = [&](DevBuf<double2> &b, int n, int comps, bool need) {
+        if (need && n > 0) b.alloc((size_t)n * nd * comps, s);
+    };
+    mk(spot, ns, 1, spgh >= 1);
+    mk(sgrad, ns, 2, spgh >= 2);
+    mk(shess, ns, 3, spgh >= 3);
+    mk(tpot, nt, 1, tpgh >= 1);
+    mk(tgrad, nt, 2, tpgh >= 2);
+    mk(thess, nt, 3, tpgh >= 3);
+    HelmProblem P;
+    P.nd = nd;
+    P.zk = make_double2(c.zk[0], c.zk[1]);
+    P.eps = c.eps;
+    P.ifcharge = c.ifcharge;
+    P.ifdipole = c.ifdipole;
+    P.src = in.src.get();
+    P.charge = in.chg.get();
+    P.dipstr = in.dip.get();
+    P.dipvec = in.dv.get();
+    P.sset = HPointSet{in.src.get(), T.srcse.get(), ns, spgh, spot.get(), sgrad.get(), shess.get()};
+    P.tset = HPointSet{in.trg.get(), T.trgse.get(), nt, tpgh, tpot.get(), tgrad.get(), thess.get()};
+    P.ifnear = c.ifnear;
+    helmholtz_fmm(T, P, s);
+    // back to input order: per point, nd * comps consecutive values
+    auto unsort = [&](int n, const int *perm, int pgh, const DevBuf<double2> &po,
+                      const DevBuf<double2> &gr, const DevBuf<double2> &he, double *upot,
+                      double *ugrad, double *uhess) {
+        if (pgh <= 0 || n <= 0) return;
+        auto one = [&](const DevBuf<double2> &b, double *user, int comps) {
+            OutBuf ob;
+            ob.set(user, (size_t)n * nd * comps, on_dev, s);
+            const int w = nd * comps;
+            const double2 *src = b.get();
+            double2 *dst = ob.ptr;
+            for_each((int64_t)n * w, s, [=] __device__(int64_t t) {
+                const int64_t k = t / w, j = t % w;
+                dst[(int64_t)perm[k] * w + j] = src[t];
+            });
+            ob.flush(s);
+            FMM_CUDA(cudaStreamSynchronize(s));
+        };
+        one(po, upot, 1);
+        if (pgh >= 2) one(gr, ugrad, 2);
+        if (pgh >= 3) one(he, uhess, 3);
+    };
+    unsort(ns, T.isrc.get(), spgh, spot, sgrad, shess, c.pot, c.grad, c.hess);
+    unsort(nt, T.itarg.get(), tpgh, tpot, tgrad, thess, c.pottarg, c.gradtarg, c.hesstarg);
+    prof_mark("scatter_d2h", s);
+    prof_end(s);
+    if (c.timeinfo)
+        for (int k = 0; k < 8; k++) c.timeinfo[k] = 0.0;
+}
+
 }  // namespace
+
+// Helmholtz direct sum over all sources at nt targets (h2d_direct*,
+// c_translation/src/helmkernels2d.c); increments pot(nd,nt), grad(nd,2,nt),
+// hess(nd,3,nt).  Host or device arrays.
+int run_helm_direct(int nd, const double *zk, int ns, const double *sources, int ifcharge,
+                    const double *charge, int ifdipole, const double *dipstr,
+                    const double *dipvec, int nt, const double *targ, int ifpgh, double *pot,
+                    double *grad, double *hess, double thresh) {
+    return guarded([&] {
+        if (nd < 1 || ns < 0 || nt < 0 || ifpgh < 1 || ifpgh > 3 || (!ifcharge && !ifdipole))
+            throw FmmError(4, "invalid direct-sum arguments");
+        if (nt == 0 || ns == 0) return;
+        CallCtx ctx;
+        cudaStream_t s = ctx.stream();
+        const bool od = is_device_ptr(sources);
+        InBuf<double2> S, Tg, Q, D;
+        InBuf<double> V;
+        S.set(sources, ns, od, s);
+        Tg.set(targ, nt, od, s);
+        if (ifcharge) Q.set(charge, (size_t)nd * ns, od, s);
+        DevBuf<double2> dv;
+        if (ifdipole) {
+            D.set(dipstr, (size_t)nd * ns, od, s);
+            V.set(dipvec, (size_t)2 * nd * ns, od, s);
+            dv.alloc((size_t)nd * ns, s);
+            const double *vp = V.ptr;
+            double2 *vo = dv.get();
+            const int ndd = nd;
+            for_each((int64_t)ns * nd, s, [=] __device__(int64_t t) {
+                const int64_t k = t / ndd, j = t % ndd;
+                vo[t] = make_double2(vp[(k * 2 + 0) * ndd + j], vp[(k * 2 + 1) * ndd + j]);
+            });
+        }
+        // outputs are incremented: bring the caller's values in
+        OutBuf Po, G, H;
+        Po.set(pot, (size_t)nd * nt, od, s);
+        if (ifpgh >= 2) G.set(grad, (size_t)nd * 2 * nt, od, s);
+        if (ifpgh >= 3) H.set(hess, (size_t)nd * 3 * nt, od, s);
+        auto load = [&](OutBuf &b, const double *u, size_t n) {
+            if (b.ptr && !od)
+                FMM_CUDA(cudaMemcpyAsync(b.ptr, u, n * sizeof(double2), cudaMemcpyHostToDevice, s));
+        };
+        load(Po, pot, (size_t)nd * nt);
+        if (ifpgh >= 2) load(G, grad, (size_t)nd * 2 * nt);
+        if (ifpgh >= 3) load(H, hess, (size_t)nd * 3 * nt);
+        HelmProblem P;
+        P.nd = nd;
+        P.zk = make_double2(zk[0], zk[1]);
+        P.ifcharge = ifcharge;
+        P.ifdipole = ifdipole;
+        P.src = S.ptr;
+        P.charge = Q.ptr;
+        P.dipstr = D.ptr;
+        P.dipvec = dv.get();
+        HPointSet X{Tg.ptr, nullptr, nt, ifpgh, Po.ptr, G.ptr, H.ptr};
+        helmholtz_direct(P, ns, X, thresh, s);
+        Po.flush(s);
+        G.flush(s);
+        H.flush(s);
+        FMM_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
 
 int run_fmm(const FmmCall &c) {
     return guarded([&] {
@@ -319,8 +511,11 @@ int run_fmm(const FmmCall &c) {
             case kCauchy:
                 run_laplace_family(c, ctx);
                 break;
+            case kHelmholtz:
+                run_helmholtz(c, ctx);
+                break;
             default:
-                throw FmmError(4, "Helmholtz evaluation is not available yet");
+                throw FmmError(4, "unknown kernel");
         }
     });
 }

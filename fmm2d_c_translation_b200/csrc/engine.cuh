@@ -42,6 +42,13 @@ struct FmmCall {
 // reference's ier (0 ok, 4 failure) after recording any error message.
 int run_fmm(const FmmCall &c);
 
+// Helmholtz direct sum (h2d_direct*), incrementing the outputs; host or
+// device arrays of one kind.  Returns 0 or 4.
+int run_helm_direct(int nd, const double *zk, int ns, const double *sources, int ifcharge,
+                    const double *charge, int ifdipole, const double *dipstr,
+                    const double *dipvec, int nt, const double *targ, int ifpgh, double *pot,
+                    double *grad, double *hess, double thresh);
+
 // Expansion order of the Laplace FMM (l2dterms, c_translation/src/l2dterms.c).
 int laplace_nterms(double eps);
 // Leaf capacity (lndiv2d.f / hndiv2d.c).

@@ -1,0 +1,60 @@
+// helmholtz.cuh -- the Helmholtz FMM passes over a device tree.
+//
+// Expansions follow the reference's scaled Graf form (c_translation/src/
+// helmrouts2d.c): a box at level l of order p_l and scale r_l holds
+// coefficients n = -p_l..p_l per channel, stored box-major as
+// [box][n + p_l][channel] (double2), the reference's mpole(nd, -nterms:nterms).
+// Boxes of one level are contiguous, so a box's block is found from a
+// per-level offset.
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+#include "tree.cuh"
+
+namespace fmm2d {
+
+// Sorted-order point data and outputs of one Helmholtz evaluation.
+// Outputs: pot [k*nd + c], grad [(k*2 + d)*nd + c], hess [(k*3 + d)*nd + c].
+struct HPointSet {
+    const double2 *pos = nullptr;
+    const int2 *se = nullptr;
+    int n = 0;
+    int pgh = 0;
+    double2 *pot = nullptr, *grad = nullptr, *hess = nullptr;
+};
+
+struct HelmProblem {
+    int nd = 1;
+    double2 zk = {0.0, 0.0};
+    double eps = 1e-6;
+    int ifcharge = 0, ifdipole = 0;
+    const double2 *src = nullptr;     // sorted sources
+    const double2 *charge = nullptr;  // [k*nd + c]
+    const double2 *dipstr = nullptr;  // [k*nd + c]
+    const double2 *dipvec = nullptr;  // [k*nd + c] = (v1, v2)
+    HPointSet sset, tset;
+    int ifnear = 1;
+};
+
+// Runs the steps of hfmm2dmain (c_translation/src/hfmm2d.c:619-1528) on the
+// device; the outputs in sset / tset are overwritten.
+void helmholtz_fmm(const Tree &T, const HelmProblem &P, cudaStream_t s);
+
+// Direct sums over all sources for every point of `set` (the reference's
+// h2d_direct* kernels, c_translation/src/helmkernels2d.c), adding to the
+// outputs; pairs with |zk r| below thresh are skipped.
+void helmholtz_direct(const HelmProblem &P, int ns, HPointSet set, double thresh,
+                      cudaStream_t s);
+
+// Host restatements of the reference's scalar routines.
+// h2dterms (c_translation/src/h2dterms.c:19-69): expansion order for a box
+// of size bsize; -1 when no order up to 50000 reaches eps.
+int helm_nterms(double bsize, double2 zk, double eps);
+// h2dall (h2dcommon.c:35-90): hvec[0..n] = H_k(z) rscale^k.
+void helm_hvec(int n, double2 z, double rscale, double2 *hvec);
+// jbessel2d (cdjseval2d.c:11-160): fjs[0..n] = J_k(z) / rscale^k.
+void helm_jvec(int n, double2 z, double rscale, double2 *fjs);
+
+}  // namespace fmm2d

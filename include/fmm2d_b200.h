@@ -629,6 +629,20 @@ void hfmm2d_ndiv_(const int32_t *nd, const double *eps,
                   const int32_t *ndiv, const int32_t *idivflag,
                   const int32_t *ifnear, double *timeinfo, int32_t *ier);
 
+/* bind(c) entry, src/helmholtz_c.f03:5-15: eps, zk and ns by value, ns
+ * and ier 64-bit (c_int64_t).  C++ callers pass zk as a struct of two
+ * doubles, which has the calling convention of double _Complex. */
+#ifdef __cplusplus
+typedef struct { double re, im; } fmm2d_b200_zk_t;
+void hfmm2d_s_c_p(double eps, fmm2d_b200_zk_t zk, int64_t ns,
+                  const double *sources, const double *charge, double *pot,
+                  int64_t *ier);
+#else
+void hfmm2d_s_c_p(double eps, double _Complex zk, int64_t ns,
+                  const double *sources, const double _Complex *charge,
+                  double _Complex *pot, int64_t *ier);
+#endif
+
 /* ===================================================================== */
 /* Library entry points with no counterpart in the reference.           */
 /* ===================================================================== */
@@ -664,6 +678,31 @@ int fmm2d_b200_c2d_direct(int nd, int ns, const double *sources,
                           const double *targ, int ifpgh, double _Complex *pot,
                           double _Complex *grad, double _Complex *hess,
                           double thresh);
+
+/* Helmholtz direct sum (h2d_direct*, c_translation/src/helmkernels2d.c),
+ * zk = {re, im}: increments pot(nd,nt), grad(nd,2,nt), hess(nd,3,nt);
+ * pairs with |zk r| below thresh are skipped (<= for charge-only
+ * potentials, < otherwise, as the reference kernels do). */
+int fmm2d_b200_h2d_direct(int nd, const double *zk, int ns,
+                          const double *sources, int ifcharge,
+                          const double _Complex *charge, int ifdipole,
+                          const double _Complex *dipstr, const double *dipvec,
+                          int nt, const double *targ, int ifpgh,
+                          double _Complex *pot, double _Complex *grad,
+                          double _Complex *hess, double thresh);
+
+/* Host-only Helmholtz helpers: the expansion order of a box
+ * (h2dterms, c_translation/src/h2dterms.c:19; -1 when above 50000),
+ * H0 and H1 at n points (z[2k], z[2k+1]) -> out[4k..4k+3], and the scaled
+ * sequences H_k(z) rscale^k (h2dall, h2dcommon.c:35) and J_k(z) / rscale^k
+ * (jbessel2d, cdjseval2d.c:11), k = 0..n, as interleaved complex. */
+int fmm2d_b200_helm_nterms(double bsize, double zk_re, double zk_im,
+                           double eps);
+void fmm2d_b200_hankel01(int n, const double *z, double *out);
+void fmm2d_b200_helm_hvec(int n, double z_re, double z_im, double rscale,
+                          double *out);
+void fmm2d_b200_helm_jvec(int n, double z_re, double z_im, double rscale,
+                          double *out);
 
 /* No counterpart in the reference.  fmm2d_b200_l2d_direct for callers
  * that cannot have device memory allocated for them (GPU memory owned by

@@ -8,6 +8,9 @@ Fixtures (seeded inputs, the reference's test sizes ns = 200, nt = 100,
 eps = 1e-6, as in c_translation/test/test_lfmm2d_ndiv.f:25,49):
   tree_200_100.npz      pts_tree_build / pts_tree_sort / computelists output
   fmm_<fam>_<variant>.npz  inputs and outputs of lfmm2d_st_* and cfmm2d_st_*
+  fmm_h1_<variant>.npz, fmm_h2_<variant>.npz  hfmm2d_st_* with zk = 10 and
+      zk = 0.5 + 0.1i (the values of test/helmholtz/test_hfmm2d.f:48-49),
+      eps = 0.51e-8 (:51)
 """
 import os
 import sys
@@ -45,6 +48,15 @@ def main():
                 np.savez_compressed(os.path.join(HERE, f"fmm_{fam}_{var}.npz"),
                                     src=src, trg=trg, charge=q, dipstr=d,
                                     dipvec=v, eps=1e-6, **out)
+    for tag, zk in (("h1", 10.0 + 0j), ("h2", 0.5 + 0.1j)):
+        for cd in ("c", "d", "cd"):
+            for p in "pgh":
+                var = f"st_{cd}_{p}"
+                out, ier = W.call(refimpl.ref(), "h", var, 0.51e-8, src, q, d, v, trg, zk=zk)
+                assert ier == 0
+                np.savez_compressed(os.path.join(HERE, f"fmm_{tag}_{var}.npz"),
+                                    src=src, trg=trg, charge=q, dipstr=d, dipvec=v,
+                                    eps=0.51e-8, zk=zk, family="h", **out)
     print("golden fixtures written to", HERE)
 
 

@@ -1,0 +1,227 @@
+"""Helmholtz parity on the GPU (hfmm2d_*, src/helmholtz/hfmm2dwrap.f):
+
+* all 27 flag wrappers against the reference build on the same inputs, at
+  the reference test's sizes (ns = 1000, nt = 1001, eps = 0.51e-8,
+  test/helmholtz/test_hfmm2d.f:19-51) for zk = 10 and zk = 0.5 + 0.1i;
+* the same wrappers against the direct sum at the first 20 points with the
+  reference test's own criterion (relative l2 error < eps);
+* zk = 500 (test_hfmm2d_hf.f:50), where the reference switches its coarse
+  levels to the diagonal (FFT) translations and this library keeps the
+  coefficient-space Graf translations (the same truncated operators);
+* the guru driver with nd = 2, the ndiv driver, the bind(c) entry, and the
+  GPU direct sum against the reference's h2d_direct kernels.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import refimpl
+import wrappers as W
+
+pytestmark = pytest.mark.gpu
+_P = ctypes.c_void_p
+EPS = 0.51e-8
+ZKS = [10.0 + 0j, 0.5 + 0.1j]
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_P)
+
+
+def inputs(ns=1000, nt=1001, seed=7):
+    rng = np.random.default_rng(seed)
+    src = rng.random((2, ns))
+    trg = rng.random((2, nt))
+    q = rng.random(ns) + 1j * rng.random(ns)
+    d = rng.random(ns) + 1j * rng.random(ns)
+    v = rng.random((2, ns))
+    return src, trg, q, d, v
+
+
+@pytest.fixture(scope="module")
+def glib():
+    import fmm2d_c_translation_b200 as fm
+    return fm.lib()
+
+
+def h_direct(lib, zk, src, q, d, v, trg, pgh, ifc, ifd, nd=1):
+    """GPU direct sum at trg (2, n): pot (n,), grad (n, 2), hess (n, 3)."""
+    n = trg.shape[1]
+    pot = np.zeros(n * nd, np.complex128)
+    grad = np.zeros(n * nd * 2, np.complex128)
+    hess = np.zeros(n * nd * 3, np.complex128)
+    zka = np.array([zk.real, zk.imag])
+    srcf = np.asfortranarray(src)
+    trgf = np.asfortranarray(trg)
+    qq = np.ascontiguousarray(q, np.complex128) if ifc else None
+    dd = np.ascontiguousarray(d, np.complex128) if ifd else None
+    vv = np.asfortranarray(v, np.float64) if ifd else None
+    thresh = abs(zk) * 2.0 ** -51
+    ier = lib.fmm2d_b200_h2d_direct(
+        ctypes.c_int(nd), _p(zka), ctypes.c_int(src.shape[1]), _p(srcf), ctypes.c_int(ifc),
+        _p(qq), ctypes.c_int(ifd), _p(dd), _p(vv), ctypes.c_int(n), _p(trgf),
+        ctypes.c_int(pgh), _p(pot), _p(grad), _p(hess), ctypes.c_double(thresh))
+    assert ier == 0
+    return pot, grad.reshape(n, 2), hess.reshape(n, 3)
+
+
+def _check_direct(lib, zk, variant, out, src, trg, q, d, v, ntest=20):
+    st, cd, p = variant.split("_")
+    pgh = {"p": 1, "g": 2, "h": 3}[p]
+    ifc, ifd = int("c" in cd), int("d" in cd)
+    for where, pts in (("", src), ("targ", trg)):
+        if f"pot{where}" not in out:
+            continue
+        sub = pts[:, :ntest]
+        pot, grad, hess = h_direct(lib, zk, src, q, d, v, sub, pgh, ifc, ifd)
+        num = np.linalg.norm(out[f"pot{where}"][:ntest] - pot) ** 2
+        den = np.linalg.norm(pot) ** 2
+        if pgh >= 2:
+            num += np.linalg.norm(out[f"grad{where}"][:ntest] - grad) ** 2
+            den += np.linalg.norm(grad) ** 2
+        if pgh >= 3:
+            num += np.linalg.norm(out[f"hess{where}"][:ntest] - hess) ** 2
+            den += np.linalg.norm(hess) ** 2
+        err = np.sqrt(num / den)
+        assert err < EPS, (variant, where, err)
+
+
+@pytest.mark.parametrize("zk", ZKS, ids=["zk10", "zk0.5+0.1i"])
+@pytest.mark.parametrize("variant", W.VARIANTS)
+def test_hfmm2d_wrappers(glib, zk, variant):
+    src, trg, q, d, v = inputs()
+    out, ier = W.call(glib, "h", variant, EPS, src, q, d, v, trg, zk=zk)
+    assert ier == 0
+    _check_direct(glib, zk, variant, out, src, trg, q, d, v)
+    if refimpl.have_ref():
+        ro, rier = W.call(refimpl.ref(), "h", variant, EPS, src, q, d, v, trg, zk=zk)
+        assert rier == 0
+        for k in out:
+            assert W.rel_err(out[k], ro[k]) < 1e-10, (variant, k, W.rel_err(out[k], ro[k]))
+
+
+@pytest.mark.parametrize("variant", ["st_cd_h", "s_c_p", "t_d_g", "st_c_g"])
+def test_hfmm2d_high_frequency(glib, variant):
+    zk = 500.0 + 0j
+    src, trg, q, d, v = inputs()
+    out, ier = W.call(glib, "h", variant, EPS, src, q, d, v, trg, zk=zk)
+    assert ier == 0
+    _check_direct(glib, zk, variant, out, src, trg, q, d, v)
+    if refimpl.have_ref():
+        ro, _ = W.call(refimpl.ref(), "h", variant, EPS, src, q, d, v, trg, zk=zk)
+        for k in out:
+            assert W.rel_err(out[k], ro[k]) < 1e-8, (variant, k, W.rel_err(out[k], ro[k]))
+
+
+@pytest.mark.parametrize("eps", [1e-3, 1e-6, 1e-12])
+@pytest.mark.parametrize("zk", [30.0 + 0j, 2.0 + 3.0j, 1e-2 + 0j])
+def test_hfmm2d_eps_and_zk(glib, eps, zk):
+    src, trg, q, d, v = inputs(ns=3000, nt=500, seed=11)
+    out, ier = W.call(glib, "h", "st_cd_g", eps, src, q, d, v, trg, zk=zk)
+    assert ier == 0
+    if refimpl.have_ref():
+        ro, _ = W.call(refimpl.ref(), "h", "st_cd_g", eps, src, q, d, v, trg, zk=zk)
+        for k in out:
+            assert W.rel_err(out[k], ro[k]) < max(1e-10, 10 * eps * 1e-2), (k, W.rel_err(out[k], ro[k]))
+    pot, grad, _ = h_direct(glib, zk, src, q, d, v, trg[:, :50], 2, 1, 1)
+    assert W.rel_err(out["pottarg"][:50], pot) < 10 * eps
+    assert W.rel_err(out["gradtarg"][:50], grad) < 100 * eps
+
+
+def _guru(lib, fn_name, nd, zk, src, q, d, v, trg, ndiv=None):
+    ns, nt = src.shape[1], trg.shape[1]
+    pot = np.zeros((ns, nd), np.complex128)
+    grad = np.zeros((ns, 2, nd), np.complex128)
+    hess = np.zeros((ns, 3, nd), np.complex128)
+    pt = np.zeros((nt, nd), np.complex128)
+    gt = np.zeros((nt, 2, nd), np.complex128)
+    ht = np.zeros((nt, 3, nd), np.complex128)
+    zka = np.array([zk], np.complex128)
+    ier = ctypes.c_int(-1)
+    iper = ctypes.c_int(0)
+    ci = lambda x: ctypes.byref(ctypes.c_int(x))  # noqa: E731
+    args = [ci(nd), ctypes.byref(ctypes.c_double(1e-10)), _p(zka), ci(ns),
+            _p(np.asfortranarray(src)), ci(1), _p(q), ci(1), _p(d), _p(v),
+            ctypes.byref(iper), ci(3), _p(pot), _p(grad), _p(hess), ci(nt),
+            _p(np.asfortranarray(trg)), ci(3), _p(pt), _p(gt), _p(ht)]
+    if ndiv is not None:
+        timeinfo = np.zeros(8)
+        args += [ci(ndiv), ci(0), ci(1), _p(timeinfo)]
+    args.append(ctypes.byref(ier))
+    getattr(lib, fn_name)(*args)
+    return ier.value, [pot, grad, hess, pt, gt, ht]
+
+
+@pytest.mark.parametrize("fn", ["hfmm2d_", "hfmm2d_ndiv_"])
+def test_hfmm2d_guru_nd2(glib, fn):
+    if not refimpl.have_ref():
+        pytest.skip("reference build absent")
+    rng = np.random.default_rng(3)
+    ns, nt, nd = 800, 300, 2
+    src = rng.random((2, ns))
+    trg = rng.random((2, nt))
+    q = np.ascontiguousarray(rng.standard_normal((ns, nd)) + 1j * rng.standard_normal((ns, nd)))
+    d = np.ascontiguousarray(rng.standard_normal((ns, nd)) + 1j * rng.standard_normal((ns, nd)))
+    v = np.ascontiguousarray(rng.standard_normal((ns, 2, nd)))
+    zk = 7.0 + 0.3j
+    ndiv = 12 if fn == "hfmm2d_ndiv_" else None
+    ier, out = _guru(glib, fn, nd, zk, src, q, d, v, trg, ndiv)
+    rier, ro = _guru(refimpl.ref(), fn, nd, zk, src, q, d, v, trg, ndiv)
+    assert ier == 0 and rier == 0
+    for a, b in zip(out, ro):
+        assert W.rel_err(a, b) < 1e-10
+
+
+def test_bind_c_entry(glib):
+    src, trg, q, d, v = inputs(ns=500)
+    zk = 10.0 + 0j
+    pot = np.zeros(500, np.complex128)
+    ier = ctypes.c_int64(-1)
+
+    class Z(ctypes.Structure):
+        _fields_ = [("re", ctypes.c_double), ("im", ctypes.c_double)]
+
+    f = glib.hfmm2d_s_c_p
+    f.argtypes = [ctypes.c_double, Z, ctypes.c_int64, _P, _P, _P, ctypes.POINTER(ctypes.c_int64)]
+    f(EPS, Z(zk.real, zk.imag), 500, _p(np.asfortranarray(src)), _p(q), _p(pot), ctypes.byref(ier))
+    assert ier.value == 0
+    out, _ = W.call(glib, "h", "s_c_p", EPS, src, q, d, v, trg, zk=zk)
+    np.testing.assert_allclose(pot, out["pot"], rtol=0, atol=0)
+
+
+@pytest.mark.parametrize("zk", [10.0 + 0j, 0.5 + 0.1j, 80 + 0j])
+@pytest.mark.parametrize("ifc,ifd", [(1, 0), (0, 1), (1, 1)])
+@pytest.mark.parametrize("pgh", [1, 2, 3])
+def test_h2d_direct_vs_reference(glib, zk, ifc, ifd, pgh):
+    if not refimpl.have_ref():
+        pytest.skip("reference build absent")
+    src, trg, q, d, v = inputs(ns=300, nt=200, seed=5)
+    trg[:, :3] = src[:, :3]  # coincident points exercise the threshold
+    pot, grad, hess = h_direct(glib, zk, src, q, d, v, trg, pgh, ifc, ifd)
+    R = refimpl.ref()
+    nt = trg.shape[1]
+    rp = np.zeros(nt, np.complex128)
+    rg = np.zeros((nt, 2), np.complex128)
+    rh = np.zeros((nt, 3), np.complex128)
+    kind = {(1, 0): "c", (0, 1): "d", (1, 1): "cd"}[(ifc, ifd)] + "pgh"[pgh - 1]
+    zka = np.array([zk], np.complex128)
+    thresh = ctypes.byref(ctypes.c_double(abs(zk) * 2.0 ** -51))
+    ci = lambda x: ctypes.byref(ctypes.c_int(x))  # noqa: E731
+    args = [ci(1), _p(zka), _p(np.asfortranarray(src)), ci(src.shape[1])]
+    if ifc:
+        args.append(_p(q))
+    if ifd:
+        args += [_p(d), _p(np.asfortranarray(v))]
+    args += [_p(np.asfortranarray(trg)), ci(nt), _p(rp)]
+    if pgh >= 2:
+        args.append(_p(rg))
+    if pgh >= 3:
+        args.append(_p(rh))
+    args.append(thresh)
+    getattr(R, f"h2d_direct{kind}_")(*args)
+    assert W.rel_err(pot, rp) < 1e-13
+    if pgh >= 2:
+        assert W.rel_err(grad, rg) < 1e-13
+    if pgh >= 3:
+        assert W.rel_err(hess, rh) < 1e-13
