@@ -134,3 +134,118 @@ def tree_build(sources, targets=None, ndiv=15, idivflag=0, lists=True):
         return out
     finally:
         L.fmm2d_b200_tree_free(h)
+
+
+# ---------------------------------------------------------------------------
+# fmm2dpy-compatible front end (python/fmm2dpy/fmm2d.py:20 hfmm2d, :459
+# lfmm2d, :715 cfmm2d): same keyword arguments, array shapes and Output
+# fields.  Every call goes through the guru drivers of the C ABI.
+# ---------------------------------------------------------------------------
+def _as_f(a, dtype):
+    return np.asfortranarray(np.asarray(a, dtype=dtype))
+
+
+def _run(kernel, *, eps, zk, sources, charges, dipstr, dipvec, targets, pg, pgt, nd):
+    out = Output()
+    sources = np.asarray(sources, dtype=np.float64)
+    assert sources.shape[0] == 2, "The first dimension of sources must be 2"
+    ns = sources.shape[1] if sources.ndim == 2 else 1
+    src = _as_f(sources.reshape(2, ns), np.float64)
+    if pg == 0 and pgt == 0:
+        print("Nothing to compute, set either pg or pgt to non-zero")
+        return out
+    ifcharge = int(charges is not None)
+    ifdipole = int(dipstr is not None or dipvec is not None)
+    if ifcharge:
+        q = _as_f(charges, np.complex128)
+        assert q.size == nd * ns, "Charges must be of shape [nd,ns] (or [ns] for nd = 1)"
+    else:
+        q = np.zeros(nd * ns, np.complex128)
+    if ifdipole:
+        d = _as_f(dipstr, np.complex128)
+        assert d.size == nd * ns, "Dipole strengths must be of shape [nd,ns] (or [ns])"
+        if kernel != "c":
+            v = _as_f(dipvec, np.float64)
+            assert v.size == nd * 2 * ns, "Dipole vectors must be of shape [nd,2,ns] (or [2,ns])"
+        else:
+            v = np.zeros(1)
+    else:
+        d = np.zeros(nd * ns, np.complex128)
+        v = np.zeros(nd * 2 * ns)
+    if targets is not None:
+        targets = np.asarray(targets, dtype=np.float64)
+        assert targets.shape[0] == 2, "The first dimension of targets must be 2"
+        nt = targets.shape[1] if targets.ndim == 2 else 1
+        trg = _as_f(targets.reshape(2, nt), np.float64)
+    else:
+        nt, trg, pgt = 0, np.zeros((2, 1), order="F"), 0
+    gc, hc = (1, 1) if kernel == "c" else (2, 3)
+
+    def alloc(n, comps):
+        shape = (nd, n) if comps == 1 else (nd, comps, n)
+        return np.zeros(shape, np.complex128, order="F")
+
+    pot, grad, hess = alloc(ns, 1), alloc(ns, gc), alloc(ns, hc)
+    pt, gt, ht = alloc(max(nt, 1), 1), alloc(max(nt, 1), gc), alloc(max(nt, 1), hc)
+    ier = _I(0)
+    iper = _I(0)
+    args = [ctypes.byref(_I(nd)), ctypes.byref(ctypes.c_double(eps))]
+    if kernel == "h":
+        zka = np.array([complex(zk)], np.complex128)
+        args.append(_ptr(zka))
+    args += [ctypes.byref(_I(ns)), _ptr(src), ctypes.byref(_I(ifcharge)), _ptr(q),
+             ctypes.byref(_I(ifdipole)), _ptr(d)]
+    if kernel != "c":
+        args.append(_ptr(v))
+    args += [ctypes.byref(iper), ctypes.byref(_I(pg)), _ptr(pot), _ptr(grad), _ptr(hess),
+             ctypes.byref(_I(nt)), _ptr(trg), ctypes.byref(_I(pgt)), _ptr(pt), _ptr(gt),
+             _ptr(ht), ctypes.byref(ier)]
+    getattr(lib(), f"{kernel}fmm2d_")(*args)
+    out.ier = ier.value
+    _check(out.ier, f"{kernel}fmm2d")
+
+    def shaped(a):
+        return a[0] if nd == 1 else a
+
+    if pg >= 1:
+        out.pot = shaped(pot)
+    if pg >= 2:
+        out.grad = shaped(grad)
+    if pg >= 3:
+        out.hess = shaped(hess)
+    if pgt >= 1:
+        out.pottarg = shaped(pt[..., :nt])
+    if pgt >= 2:
+        out.gradtarg = shaped(gt[..., :nt])
+    if pgt >= 3:
+        out.hesstarg = shaped(ht[..., :nt])
+    return out
+
+
+def hfmm2d(*, eps, zk, sources, charges=None, dipstr=None, dipvec=None, targets=None, pg=0,
+           pgt=0, nd=1):
+    """Helmholtz FMM, u(x) = (i/4) sum_j [c_j H0(k|x - x_j|) + k d_j
+    (v_j . (x - x_j)) / |x - x_j| H1(k|x - x_j|)] (fmm2dpy.hfmm2d).
+    pg / pgt: 1 potential, 2 + gradient, 3 + Hessian at sources / targets.
+    Returns Output with pot (n) or (nd, n), grad (2, n) or (nd, 2, n), hess
+    (3, n) or (nd, 3, n) and the same for targets."""
+    return _run("h", eps=eps, zk=zk, sources=sources, charges=charges, dipstr=dipstr,
+                dipvec=dipvec, targets=targets, pg=pg, pgt=pgt, nd=nd)
+
+
+def lfmm2d(*, eps, sources, charges=None, dipstr=None, dipvec=None, targets=None, pg=0,
+           pgt=0, nd=1):
+    """Complex-Laplace FMM with the kernels the reference computes,
+    u(x) = sum_j [c_j log|x - x_j| - d_j (v_j . (x - x_j)) / |x - x_j|^2]
+    (fmm2dpy.lfmm2d); arguments and outputs as for hfmm2d."""
+    return _run("l", eps=eps, zk=None, sources=sources, charges=charges, dipstr=dipstr,
+                dipvec=dipvec, targets=targets, pg=pg, pgt=pgt, nd=nd)
+
+
+def cfmm2d(*, eps, sources, charges=None, dipstr=None, targets=None, pg=0, pgt=0, nd=1):
+    """Cauchy-kernel FMM with the reference's conventions (fmm2dpy.cfmm2d):
+    u(z) = sum_j [c_j log(z - xi_j) + d_j / (z - xi_j)], the near field
+    taking log|z - xi_j| for the logarithm as the reference's direct kernels
+    do; grad = du/dz and hess = d2u/dz2, shape (n) or (nd, n)."""
+    return _run("c", eps=eps, zk=None, sources=sources, charges=charges, dipstr=dipstr,
+                dipvec=None, targets=targets, pg=pg, pgt=pgt, nd=nd)

@@ -24,6 +24,7 @@
 #include "sort.cuh"
 
 #include <algorithm>
+#include <mutex>
 #include <stdlib.h>
 #include <vector>
 
@@ -246,9 +247,11 @@ bool m2l_tensor_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp,
                      double2 *loc, cudaStream_t s) {
     const int L = T.nlevels, p = P.p;
     if (L < 2 || p > 63) return false;
+    static std::mutex tables_mu;
     static bool tables_ready[64] = {false};
     int dev = 0;
     FMM_CUDA(cudaGetDevice(&dev));
+    std::unique_lock<std::mutex> tables_lock(tables_mu);
     if (!tables_ready[dev]) {
         const SlotTables st = make_slot_tables();
         FMM_CUDA(cudaMemcpyToSymbolAsync(c_slot_dx, st.dx, sizeof(st.dx), 0, cudaMemcpyHostToDevice, s));
@@ -257,6 +260,7 @@ bool m2l_tensor_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp,
         FMM_CUDA(cudaStreamSynchronize(s));
         tables_ready[dev] = true;
     }
+    tables_lock.unlock();
     const int lo = T.lstart[2], n = T.nboxes - lo;
     const int nseg = 4 * (L - 1);
     const int2 *sse = T.srcse.get(), *tse = T.trgse.get();

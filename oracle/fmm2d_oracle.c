@@ -15,7 +15,9 @@
  *        pot  += q log|z| + d / z,  grad += q / z - d / z^2,
  *        hess += -q / z^2 + 2 d / z^3;
  *   - the eps -> leaf capacity table (src/laplace/lndiv2d.f:1-39) and the
- *     eps -> expansion order rule (c_translation/src/l2dterms.c:26-67).
+ *     eps -> expansion order rule (c_translation/src/l2dterms.c:26-67);
+ *   - the Helmholtz direct sums (helmkernels2d.c:21-520) with H0 and H1
+ *     from textbook methods (end of this file).
  * Pairs closer than `thresh` are skipped, as the reference kernels do.
  *
  * Outputs are INCREMENTED (like the reference kernels).  Complex arrays are
@@ -162,6 +164,222 @@ void oracle_c2d_direct(int ns, const double *src, int ifcharge,
                 if (ifpgh >= 3)
                     cacc(&hess[2 * j], cscale(cmul(d, cmul(zi2, zi)), 2.0));
             }
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------
+ * Helmholtz direct sums (c_translation/src/helmkernels2d.c:21-520), nd = 1:
+ *   pot  += (i/4) [q H0(k r) + d k H1(k r) (v . r) / r]
+ *   grad, hess: its x / y derivatives, in the reference's closed forms.
+ * Pairs with |k r| below thresh are skipped (<= for charge-only
+ * potentials, < otherwise).  H0 and H1 come from the textbook methods
+ * below (not from the reference's hank103 tables):
+ *   |z| small: ascending series (Abramowitz & Stegun 9.1.10, 9.1.11);
+ *   Im z >= 0 otherwise: H_nu(z) = (2/pi) i^-(nu+1) K_nu(-iz) with K0, K1
+ *     by Temme's continued fraction (Steed's algorithm);
+ *   Im z < 0, moderate |z|: Miller's recurrence for J and the Neumann
+ *     series for Y;  large |z|: Hankel's asymptotic expansion.
+ * ------------------------------------------------------------------------ */
+#include <complex.h>
+
+static const double kPiO = 3.14159265358979323846;
+static const double kGammaO = 0.57721566490153286061;
+
+static void o_hank_series(double complex z, double complex *h0, double complex *h1)
+{
+    double complex w = -z * z / 4.0, t0 = 1.0, t1 = 1.0, j0 = 1.0, j1s = 1.0;
+    double complex s0 = 0.0, s1 = (1.0 - 2.0 * kGammaO);
+    double hk = 0.0, mag = 1.0, aw = cabs(w);
+    for (int k = 1; k < 40; k++) {
+        t0 *= w / ((double)k * k);
+        t1 *= w / ((double)k * (k + 1));
+        hk += 1.0 / k;
+        j0 += t0;
+        j1s += t1;
+        s0 += t0 * hk;
+        s1 += t1 * (2.0 * hk + 1.0 / (k + 1) - 2.0 * kGammaO);
+        mag *= aw / ((double)k * k);
+        if (mag * (1.0 + hk) < 1e-18) break;
+    }
+    double complex lz = clog(z / 2.0), j1 = z / 2.0 * j1s;
+    double complex y0 = 2.0 / kPiO * ((lz + kGammaO) * j0 - s0);
+    double complex y1 = -2.0 / (kPiO * z) + 2.0 / kPiO * lz * j1 - z / 2.0 * s1 / kPiO;
+    *h0 = j0 + I * y0;
+    *h1 = j1 + I * y1;
+}
+
+static void o_hank_cf2(double complex z, double complex *h0, double complex *h1)
+{
+    double complex w = -I * z, b = 2.0 * (1.0 + w), d = 1.0 / b, h = d, delh = d;
+    double complex q1 = 0.0, q2 = 1.0, q = 0.25, s = 1.0 + 0.25 * delh;
+    double a = -0.25, c = 0.25;
+    for (int i = 2; i < 2000; i++) {
+        a -= 2.0 * (i - 1);
+        c = -a * c / i;
+        double complex qn = (q1 - b * q2) / a;
+        q1 = q2;
+        q2 = qn;
+        q += c * qn;
+        b += 2.0;
+        d = 1.0 / (b + a * d);
+        delh = (b * d - 1.0) * delh;
+        h += delh;
+        double complex dels = q * delh;
+        s += dels;
+        if (cabs(dels) < 1e-17 * cabs(s)) break;
+    }
+    double complex k0 = csqrt(kPiO / (2.0 * w)) * cexp(-w) / s;
+    double complex k1 = k0 * (w + 0.5 - 0.25 * h) / w;
+    *h0 = -2.0 * I / kPiO * k0;
+    *h1 = -2.0 / kPiO * k1;
+}
+
+static void o_hank_neumann(double complex z, double complex *h0, double complex *h1)
+{
+    double az = cabs(z);
+    int n = 2 * (int)((az + 40.0 + 6.0 * sqrt(az)) * 0.5) + 2;
+    double complex zm = cimag(z) >= 0 ? -I : I, f = 1e-300, fp1 = 0.0;
+    double complex psi = 0.0, sy0 = 0.0, sy1 = 0.0, zmk = cpow(zm, n % 4);
+    for (int k = n; k >= 1; k--) {
+        psi += zmk * f;
+        zmk /= zm;
+        if ((k & 1) == 0) {
+            int m = k / 2;
+            sy0 += f * ((m & 1) ? -1.0 : 1.0) / m;
+        } else {
+            int mlo = (k + 1) / 2, mhi = (k - 1) / 2;
+            sy1 += f * ((mlo & 1) ? -1.0 : 1.0) / mlo;
+            if (mhi >= 1) sy1 -= f * ((mhi & 1) ? -1.0 : 1.0) / mhi;
+        }
+        double complex fm1 = 2.0 * k / z * f - fp1;
+        fp1 = f;
+        f = fm1;
+        if (cabs(f) > 1e250) {
+            f *= 1e-250;
+            fp1 *= 1e-250;
+            psi *= 1e-250;
+            sy0 *= 1e-250;
+            sy1 *= 1e-250;
+        }
+    }
+    double complex sc = (cimag(z) >= 0 ? cexp(-I * z) : cexp(I * z)) / (f + 2.0 * psi);
+    double complex j0 = f * sc, j1 = fp1 * sc, lg = clog(z / 2.0) + kGammaO;
+    double complex y0 = 2.0 / kPiO * lg * j0 - 4.0 / kPiO * sy0 * sc;
+    double complex y1 = 2.0 / kPiO * lg * j1 - 2.0 / kPiO * j0 / z + 2.0 / kPiO * sy1 * sc;
+    *h0 = j0 + I * y0;
+    *h1 = j1 + I * y1;
+}
+
+static void o_hank_asym(double complex z, double complex *h0, double complex *h1)
+{
+    double complex izi = I / z, p0 = 1.0, p1 = 1.0, t0 = 1.0, t1 = 1.0;
+    double az = cabs(z);
+    for (int k = 1; k < 200; k++) {
+        double o = 2.0 * k - 1.0;
+        if (o * o > 8.0 * k * az) break;
+        t0 *= izi * (-o * o / (8.0 * k));
+        t1 *= izi * ((4.0 - o * o) / (8.0 * k));
+        p0 += t0;
+        p1 += t1;
+        if (cabs(t0) + cabs(t1) < 1e-18) break;
+    }
+    double complex pre = csqrt(2.0 / (kPiO * z)) * cexp(I * z);
+    *h0 = pre * cexp(-I * kPiO / 4.0) * p0;
+    *h1 = pre * cexp(-3.0 * I * kPiO / 4.0) * p1;
+}
+
+static void o_hankel01(double complex z, double complex *h0, double complex *h1)
+{
+    double az = cabs(z);
+    if (cimag(z) >= 0) {
+        if (az <= 1.5 || (az <= 4.0 && cimag(z) < 1.5)) o_hank_series(z, h0, h1);
+        else o_hank_cf2(z, h0, h1);
+    } else if (az <= 4.0) {
+        o_hank_series(z, h0, h1);
+    } else if (az < 20.0) {
+        o_hank_neumann(z, h0, h1);
+    } else {
+        o_hank_asym(z, h0, h1);
+    }
+}
+
+void oracle_hankel01(int n, const double *z, double *out)
+{
+    for (int k = 0; k < n; k++) {
+        double complex h0, h1;
+        o_hankel01(z[2 * k] + I * z[2 * k + 1], &h0, &h1);
+        out[4 * k] = creal(h0);
+        out[4 * k + 1] = cimag(h0);
+        out[4 * k + 2] = creal(h1);
+        out[4 * k + 3] = cimag(h1);
+    }
+}
+
+void oracle_h2d_direct(double zk_re, double zk_im, int ns, const double *src, int ifcharge,
+                       const double *charge, int ifdipole, const double *dipstr,
+                       const double *dipvec, int nt, const double *targ, int ifpgh,
+                       double *pot, double *grad, double *hess, double thresh)
+{
+    const double complex zk = zk_re + I * zk_im, i4 = I / 4.0;
+    const int le = ifcharge && !ifdipole && ifpgh == 1;
+    for (int t = 0; t < nt; t++) {
+        double complex p = 0, gx = 0, gy = 0, hxx = 0, hxy = 0, hyy = 0;
+        for (int s = 0; s < ns; s++) {
+            const double dx = targ[2 * t] - src[2 * s], dy = targ[2 * t + 1] - src[2 * s + 1];
+            const double rr = dx * dx + dy * dy, r = sqrt(rr);
+            const double complex z = zk * r;
+            const double az = cabs(z);
+            if (le ? (az <= thresh) : (az < thresh)) continue;
+            double complex h0, h1;
+            o_hankel01(z, &h0, &h1);
+            if (ifcharge) {
+                const double complex q = charge[2 * s] + I * charge[2 * s + 1];
+                p += h0 * q * i4;
+                const double complex cd = -h1 * (zk * i4 / r) * q;
+                gx += cd * dx;
+                gy += cd * dy;
+                const double complex c2 = (zk * i4 / r) / rr * q, h2z = -z * h0 + 2.0 * h1;
+                hxx += c2 * (h2z * dx * dx - rr * h1);
+                hxy += c2 * (h2z * dx * dy);
+                hyy += c2 * (h2z * dy * dy - rr * h1);
+            }
+            if (ifdipole) {
+                const double complex d = dipstr[2 * s] + I * dipstr[2 * s + 1];
+                const double v1 = dipvec[2 * s], v2 = dipvec[2 * s + 1];
+                const double ct = dx / r, st = dy / r;
+                const double complex h2 = 2.0 * h1 / z - h0, h3 = 4.0 * h2 / z - h1;
+                p += h1 / r * zk * i4 * d * (dx * v1 + dy * v2);
+                const double complex c2 = -zk * zk * i4 * d;
+                const double complex f1 = h2 * (ct * ct - 0.5) - h0 / 2.0, f2 = h2 * ct * st;
+                const double complex f3 = h2 * (st * st - 0.5) - h0 / 2.0;
+                gx += c2 * (f1 * v1 + f2 * v2);
+                gy += c2 * (f2 * v1 + f3 * v2);
+                const double complex a1 = (h1 * 0.75 - h3 / 2.0 * (ct * ct - 0.5 - st * st)) * ct;
+                const double complex a2 = (h1 * 0.25 - h3 / 2.0 * (1.5 * ct * ct - 0.5 * st * st)) * st;
+                const double complex a3 = (h1 * 0.25 - h3 / 2.0 * (1.5 * st * st - 0.5 * ct * ct)) * ct;
+                const double complex a4 = (h1 * 0.75 - h3 / 2.0 * (st * st - 0.5 - ct * ct)) * st;
+                const double complex c3 = -zk * zk * zk * d * i4;
+                hxx += c3 * (a1 * v1 + a2 * v2);
+                hxy += c3 * (a2 * v1 + a3 * v2);
+                hyy += c3 * (a3 * v1 + a4 * v2);
+            }
+        }
+        pot[2 * t] += creal(p);
+        pot[2 * t + 1] += cimag(p);
+        if (ifpgh >= 2) {
+            grad[4 * t] += creal(gx);
+            grad[4 * t + 1] += cimag(gx);
+            grad[4 * t + 2] += creal(gy);
+            grad[4 * t + 3] += cimag(gy);
+        }
+        if (ifpgh >= 3) {
+            hess[6 * t] += creal(hxx);
+            hess[6 * t + 1] += cimag(hxx);
+            hess[6 * t + 2] += creal(hxy);
+            hess[6 * t + 3] += cimag(hxy);
+            hess[6 * t + 4] += creal(hyy);
+            hess[6 * t + 5] += cimag(hyy);
         }
     }
 }

@@ -3,6 +3,7 @@ translation by tests/golden/make_golden.py) against the oracle: the FMM
 outputs the reference produced agree with the oracle's FP64 direct sums to
 the requested precision, and the reference build, where present,
 reproduces them."""
+import ctypes
 import glob
 import os
 
@@ -16,7 +17,15 @@ GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 FILES = sorted(glob.glob(os.path.join(GOLD, "fmm_*.npz")))
 
 
-def oracle_outputs(fam, variant, g):
+def _family(name, g):
+    """(family, variant, zk) of a fixture; Helmholtz ones carry zk."""
+    fam, variant = name.split("_", 1)
+    if "family" in g.files:
+        return str(g["family"]), variant, complex(g["zk"])
+    return fam, variant, None
+
+
+def oracle_outputs(fam, variant, g, zk=None):
     _, cd, p = variant.split("_")
     pgh = {"p": 1, "g": 2, "h": 3}[p]
     src = np.ascontiguousarray(g["src"].T)
@@ -26,12 +35,23 @@ def oracle_outputs(fam, variant, g):
     v = np.ascontiguousarray(g["dipvec"].T)
     res = {}
     for key, pts, n in (("", src, ns), ("targ", trg, nt)):
-        gc = 2 if fam == "l" else 1
-        hc = 3 if fam == "l" else 1
+        gc = 1 if fam == "c" else 2
+        hc = 1 if fam == "c" else 3
         pot = np.zeros(n, complex)
         grad = np.zeros((n, gc), complex)
         hess = np.zeros((n, hc), complex)
-        if fam == "l":
+        if fam == "h":
+            O = refimpl.orc()
+            O.oracle_h2d_direct.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                            ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                            ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                            ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_void_p, ctypes.c_double]
+            O.oracle_h2d_direct(zk.real, zk.imag, ns, W._p(src), int("c" in cd), W._p(q),
+                                int("d" in cd), W._p(d), W._p(v), n, W._p(pts), pgh,
+                                W._p(pot), W._p(grad), W._p(hess), abs(zk) * 2.0 ** -51)
+        elif fam == "l":
             refimpl.orc().oracle_l2d_direct(
                 ns, W._p(src), int("c" in cd), W._p(q), int("d" in cd), W._p(d),
                 W._p(v), 0, n, W._p(pts), pgh, W._p(pot), W._p(grad), W._p(hess), 1e-300)
@@ -50,9 +70,9 @@ def oracle_outputs(fam, variant, g):
 @pytest.mark.parametrize("path", FILES, ids=[os.path.basename(f) for f in FILES])
 def test_golden_against_oracle(path):
     name = os.path.basename(path)[4:-4]
-    fam, variant = name.split("_", 1)
     g = np.load(path)
-    ref = oracle_outputs(fam, variant, g)
+    fam, variant, zk = _family(name, g)
+    ref = oracle_outputs(fam, variant, g, zk)
     eps = float(g["eps"])
     for k, v in ref.items():
         # Cauchy potentials of complex strengths are defined only up to the
@@ -68,10 +88,10 @@ def test_golden_against_oracle(path):
 @pytest.mark.parametrize("path", FILES, ids=[os.path.basename(f) for f in FILES])
 def test_reference_reproduces_golden(path):
     name = os.path.basename(path)[4:-4]
-    fam, variant = name.split("_", 1)
     g = np.load(path)
+    fam, variant, zk = _family(name, g)
     out, ier = W.call(refimpl.ref(), fam, variant, float(g["eps"]), g["src"],
-                      g["charge"], g["dipstr"], g["dipvec"], g["trg"])
+                      g["charge"], g["dipstr"], g["dipvec"], g["trg"], zk=zk)
     assert ier == 0
     for k in out:
         assert W.rel_err(out[k], g[k]) < 1e-13

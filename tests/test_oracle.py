@@ -85,3 +85,57 @@ def test_rules_match_reference():
         R.hndiv2d_(D(eps), I(10), I(5), I(1), I(0), I(1), I(0),
                    ctypes.byref(nd), ctypes.byref(idf))
         assert O.oracle_lndiv2d(eps, 10, 5) == nd.value
+
+
+@pytest.mark.parametrize("zk", [10.0 + 0j, 0.5 + 0.1j, 80.0 + 0j, 3.0 + 6.0j])
+@pytest.mark.parametrize("cd", ["c", "d", "cd"])
+@pytest.mark.parametrize("pgh", [1, 2, 3])
+def test_h2d_direct_matches_reference(zk, cd, pgh):
+    ns, nt = 200, 90
+    src, trg, q, d, v = data(ns, nt, 2)
+    thr = abs(zk) * 2.0 ** -51
+    ifc, ifd = int("c" in cd), int("d" in cd)
+    O = refimpl.orc()
+    O.oracle_h2d_direct.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                    ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                    ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                    ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                    ctypes.c_double]
+    mine = [np.zeros(nt, complex), np.zeros((nt, 2), complex), np.zeros((nt, 3), complex)]
+    O.oracle_h2d_direct(zk.real, zk.imag, ns, W._p(np.asfortranarray(src)), ifc, W._p(q), ifd,
+                        W._p(d), W._p(np.asfortranarray(v)), nt, W._p(np.asfortranarray(trg)),
+                        pgh, W._p(mine[0]), W._p(mine[1]), W._p(mine[2]), thr)
+    outs = [np.zeros(nt, complex), np.zeros((nt, 2), complex), np.zeros((nt, 3), complex)]
+    zka = np.array([zk])
+    args = [I(1), W._p(zka), W._p(np.asfortranarray(src)), I(ns)]
+    if ifc:
+        args.append(W._p(q))
+    if ifd:
+        args += [W._p(d), W._p(np.asfortranarray(v))]
+    args += [W._p(np.asfortranarray(trg)), I(nt)] + [W._p(o) for o in outs[:pgh]] + [D(thr)]
+    getattr(refimpl.ref(), f"h2d_direct{cd}{'pgh'[pgh - 1]}_")(*args)
+    for k in range(pgh):
+        assert W.rel_err(mine[k], outs[k]) < 1e-13, (k, W.rel_err(mine[k], outs[k]))
+
+
+def test_oracle_hankel_matches_hank103():
+    rng = np.random.default_rng(5)
+    r = np.exp(rng.uniform(np.log(1e-6), np.log(1e3), 3000))
+    a = rng.uniform(-np.pi / 2, np.pi, 3000)
+    z = np.ascontiguousarray(r * np.exp(1j * a))
+    out = np.zeros(4 * len(z))
+    O = refimpl.orc()
+    O.oracle_hankel01.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    O.oracle_hankel01(len(z), W._p(z), W._p(out))
+    h0 = out[0::4] + 1j * out[1::4]
+    one = ctypes.c_int(1)
+    worst = 0.0
+    for k in range(len(z)):
+        zz = np.array([z[k]])
+        a0 = np.zeros(1, complex)
+        a1 = np.zeros(1, complex)
+        refimpl.ref().hank103_(W._p(zz), W._p(a0), W._p(a1), ctypes.byref(one))
+        if np.isfinite(a0[0]) and 1e-290 < abs(a0[0]) < 1e290:
+            worst = max(worst, abs(h0[k] - a0[0]) / abs(a0[0]))
+    assert worst < 2e-14
