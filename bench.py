@@ -23,6 +23,19 @@ host thread, concurrently.
 Multi-GPU (``torchrun --nproc-per-node N``): independent replicas, one
 full problem per GPU (the evaluation path does not shard), value = all
 points of all ranks / max step time over ranks.
+
+Serving (``serving`` key, rank 0): the stream of the serving configuration
+-- requests with N log-uniform in [1e3, 1e6] points, uniform or Gaussian
+blobs (sigma 0.01) in [0,1]^2, 70 % Laplace lfmm2d_s_c_g at eps in
+{1e-3, 1e-6, 1e-9}, 30 % Helmholtz hfmm2d_s_c_g with zk ~ U[1, 50] at eps
+1e-6, complex charges N(0,1) -- through the library's request loop
+(fmm2d_b200_server_*) with an HBM budget of 120 GB.  Arrivals are Poisson
+at 70 % of the throughput measured on a saturating burst of the same
+stream; latency = submission to completion (host arrays, copies
+included); p50 / p99 over all requests.  Beside it, the same requests one
+at a time in all-FP64 mode (one slot).  ``--serve-requests`` sets the
+stream length (the configuration names 20,000; the default run uses 2,000
+to stay within minutes).
 """
 import argparse
 import ctypes
@@ -249,6 +262,9 @@ def main():
     ap.add_argument("--cpu-threads", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=2000)
+    ap.add_argument("--serve-slots", type=int, default=6)
+    ap.add_argument("--serve-budget-gb", type=float, default=120.0)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -458,6 +474,11 @@ def main():
         roof["phase_ms"] = {k: round(v_, 4) for k, v_ in times.items()}
         roof["counts"] = counts
 
+    serving = None
+    if args.serve_requests > 0:
+        L.fmm2d_b200_reset_stream()
+        serving = measure_serving(fm, args)
+
     cpu = None
     if not args.no_cpu_baseline and ws == 1:
         cpu = cpu_baseline_sample(args)
@@ -473,10 +494,100 @@ def main():
                    "l2": "inputs 0.8 GB > L2; no flush"},
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": nlaunch, "clocks": clk, "fp64_plain": fp64,
-        "accuracy": acc,
+        "accuracy": acc, "serving": serving,
     }
     print(json.dumps(line))
     return 0
+
+
+def serving_stream(n_req, seed=2025):
+    """The serving configuration's request mix: list of dicts."""
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for _ in range(n_req):
+        n = int(round(10 ** rng.uniform(3.0, 6.0)))
+        helm = rng.random() < 0.3
+        reqs.append(dict(kernel="h" if helm else "l", n=n,
+                         eps=1e-6 if helm else float(rng.choice([1e-3, 1e-6, 1e-9])),
+                         zk=float(rng.uniform(1.0, 50.0)) if helm else 0.0,
+                         blobs=bool(rng.random() < 0.5), off=int(rng.integers(0, 1 << 30))))
+    return reqs
+
+
+def measure_serving(fm, args):
+    nmax = 1_000_000
+    rng = np.random.default_rng(77)
+    uni = np.asfortranarray(rng.random((2, nmax)))
+    centers = rng.random((2, 32))
+    blob = centers[:, rng.integers(0, 32, nmax)] + 0.01 * rng.standard_normal((2, nmax))
+    blob = np.asfortranarray(np.clip(blob, 0.0, 1.0))
+    chg = rng.standard_normal(nmax) + 1j * rng.standard_normal(nmax)
+    reqs = serving_stream(args.serve_requests)
+
+    def build(r, precision=0):
+        n = r["n"]
+        o = r["off"] % (nmax - n + 1)
+        pts = (blob if r["blobs"] else uni)[:, o:o + n]
+        return fm.make_request(r["kernel"], eps=r["eps"], sources=pts, charges=chg[o:o + n],
+                               pg=2, zk=r["zk"], precision=precision)
+
+    def run(stream, slots, precision, rate=None):
+        """Submits `stream` (Poisson at `rate` req/s, or all at once);
+        returns (wall s, latencies ms, points)."""
+        srv = fm.Server(slots=slots, hbm_budget=args.serve_budget_gb * 1e9)
+        lat = [None] * len(stream)
+        tickets = [None] * len(stream)
+        done = threading.Semaphore(0)
+
+        def waiter():
+            for i in range(len(stream)):
+                done.acquire()
+                ier, tms = srv.wait(tickets[i])
+                if ier != 0:
+                    raise RuntimeError("serving request failed: " + fm.last_error())
+                lat[i] = tms[2]
+
+        th = threading.Thread(target=waiter)
+        th.start()
+        arr = np.cumsum(np.random.default_rng(5).exponential(1.0 / rate, len(stream))) \
+            if rate else np.zeros(len(stream))
+        t0 = time.perf_counter()
+        for i, r in enumerate(stream):
+            dt = arr[i] - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            req, keep = build(r, precision)
+            tickets[i] = srv.submit(req, keep)
+            done.release()
+        th.join()
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
+        return wall, lat, sum(r["n"] for r in stream), st
+
+    # warm the pool and the code paths
+    run(reqs[:20], args.serve_slots, 0)
+    burst = reqs[: min(len(reqs), 300)]
+    wall_b, _, pts_b, _ = run(burst, args.serve_slots, 0)
+    cap = len(burst) / wall_b
+    rate = 0.7 * cap
+    wall, lat, pts, st = run(reqs, args.serve_slots, 0, rate=rate)
+    lat = np.array(lat)
+    base = reqs[: min(len(reqs), 200)]
+    wall1, lat1, pts1, _ = run(base, 1, 1)
+    return {
+        "requests": len(reqs), "slots": args.serve_slots,
+        "hbm_budget_gb": args.serve_budget_gb,
+        "arrival": f"Poisson at {rate:.1f} req/s (70% of the {cap:.1f} req/s burst capacity)",
+        "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+        "mean_ms": float(lat.mean()), "throughput_req_s": len(reqs) / wall,
+        "throughput_points_s": pts / wall, "burst_points_s": pts_b / wall_b,
+        "peak_running": st["peak_running"], "peak_budget_gb": st["peak_bytes"] / 1e9,
+        "one_at_a_time_fp64": {"requests": len(base), "points_s": pts1 / wall1,
+                               "req_s": len(base) / wall1,
+                               "p50_ms": float(np.percentile(lat1, 50))},
+        "points": "N log-uniform [1e3, 1e6], uniform or Gaussian blobs, host arrays",
+    }
 
 
 def measure_fp64_peak(L):

@@ -18,7 +18,8 @@ import os
 import numpy as np
 
 __all__ = ["Output", "lfmm2d", "cfmm2d", "hfmm2d", "lib", "lib_path",
-           "last_error", "tree_build", "FmmError"]
+           "last_error", "tree_build", "FmmError", "Server", "Request",
+           "make_request"]
 
 _PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 lib_path = os.path.join(_PKG_DIR, "libfmm2d_b200.so")
@@ -249,3 +250,124 @@ def cfmm2d(*, eps, sources, charges=None, dipstr=None, targets=None, pg=0, pgt=0
     do; grad = du/dz and hess = d2u/dz2, shape (n) or (nd, n)."""
     return _run("c", eps=eps, zk=None, sources=sources, charges=charges, dipstr=dipstr,
                 dipvec=None, targets=targets, pg=pg, pgt=pgt, nd=nd)
+
+
+# ---------------------------------------------------------------------------
+# Request loop (serve.cu): continuous admission of independent evaluations.
+# ---------------------------------------------------------------------------
+class Request(ctypes.Structure):
+    """fmm2d_b200_request: the guru drivers' arguments of one evaluation."""
+    _fields_ = [("kernel", _I), ("nd", _I), ("eps", ctypes.c_double),
+                ("zk", ctypes.c_double * 2), ("ns", _I), ("sources", _P),
+                ("ifcharge", _I), ("charge", _P), ("ifdipole", _I), ("dipstr", _P),
+                ("dipvec", _P), ("ifpgh", _I), ("pot", _P), ("grad", _P), ("hess", _P),
+                ("nt", _I), ("targ", _P), ("ifpghtarg", _I), ("pottarg", _P),
+                ("gradtarg", _P), ("hesstarg", _P), ("precision", _I)]
+
+
+class Server:
+    """A request loop on the current device: `slots` concurrent
+    evaluations within `hbm_budget` bytes of estimated footprint.  submit()
+    keeps the request's arrays alive until wait() returns its ticket."""
+
+    def __init__(self, slots=4, hbm_budget=120e9):
+        L = lib()
+        L.fmm2d_b200_server_create.restype = _P
+        L.fmm2d_b200_server_create.argtypes = [_I, ctypes.c_double]
+        L.fmm2d_b200_server_submit.restype = ctypes.c_longlong
+        L.fmm2d_b200_server_submit.argtypes = [_P, ctypes.POINTER(Request)]
+        L.fmm2d_b200_server_wait.argtypes = [_P, ctypes.c_longlong, _P]
+        L.fmm2d_b200_server_stats.argtypes = [_P, _P]
+        L.fmm2d_b200_server_stats.restype = None
+        L.fmm2d_b200_server_destroy.argtypes = [_P]
+        L.fmm2d_b200_server_destroy.restype = None
+        L.fmm2d_b200_request_bytes.restype = ctypes.c_double
+        L.fmm2d_b200_request_bytes.argtypes = [ctypes.POINTER(Request)]
+        self._L = L
+        self._h = L.fmm2d_b200_server_create(int(slots), float(hbm_budget))
+        if not self._h:
+            raise FmmError("server_create failed")
+        self._keep = {}
+
+    def submit(self, req, keep=()):
+        t = self._L.fmm2d_b200_server_submit(self._h, ctypes.byref(req))
+        if t < 0:
+            raise FmmError("invalid request")
+        self._keep[t] = (req, keep)
+        return t
+
+    def wait(self, ticket):
+        """(ier, (queue_ms, run_ms, total_ms))."""
+        times = np.zeros(3)
+        ier = self._L.fmm2d_b200_server_wait(self._h, ticket, _ptr(times))
+        self._keep.pop(ticket, None)
+        return ier, tuple(times)
+
+    def stats(self):
+        out = np.zeros(6)
+        self._L.fmm2d_b200_server_stats(self._h, _ptr(out))
+        return dict(bytes_in_use=out[0], peak_bytes=out[1], queued=int(out[2]),
+                    running=int(out[3]), rejected=int(out[4]), peak_running=int(out[5]))
+
+    def request_bytes(self, req):
+        return self._L.fmm2d_b200_request_bytes(ctypes.byref(req))
+
+    def close(self):
+        if self._h:
+            self._L.fmm2d_b200_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def make_request(kernel, *, eps, sources, charges=None, dipstr=None, dipvec=None,
+                 targets=None, pg=1, pgt=0, zk=0.0, precision=0):
+    """A Request for nd = 1 with freshly allocated outputs.  Returns
+    (Request, arrays) where arrays holds every buffer the request points to
+    (pass it to Server.submit as `keep`); outputs are arrays["pot"], ...,
+    grad as (n, 2) rows and hess as (n, 3) rows for lfmm2d / hfmm2d."""
+    kid = {"l": 0, "c": 1, "h": 2}[kernel]
+    src = _as_f(sources, np.float64)
+    ns = src.shape[1]
+    arrs = {"src": src}
+    r = Request()
+    r.kernel, r.nd, r.eps = kid, 1, float(eps)
+    zk = complex(zk)
+    r.zk[0], r.zk[1] = zk.real, zk.imag
+    r.ns, r.sources = ns, src.ctypes.data
+    r.precision = int(precision)
+    if charges is not None:
+        arrs["q"] = np.ascontiguousarray(charges, np.complex128)
+        r.ifcharge, r.charge = 1, arrs["q"].ctypes.data
+    if dipstr is not None:
+        arrs["d"] = np.ascontiguousarray(dipstr, np.complex128)
+        r.ifdipole, r.dipstr = 1, arrs["d"].ctypes.data
+        if kernel != "c":
+            arrs["v"] = _as_f(dipvec, np.float64)
+            r.dipvec = arrs["v"].ctypes.data
+    gc, hc = (1, 1) if kernel == "c" else (2, 3)
+
+    def outs(prefix, n, flag):
+        arrs["pot" + prefix] = np.zeros(n, np.complex128)
+        ptrs = [arrs["pot" + prefix].ctypes.data, None, None]
+        if flag >= 2:
+            arrs["grad" + prefix] = np.zeros((n, gc) if gc > 1 else n, np.complex128)
+            ptrs[1] = arrs["grad" + prefix].ctypes.data
+        if flag >= 3:
+            arrs["hess" + prefix] = np.zeros((n, hc) if hc > 1 else n, np.complex128)
+            ptrs[2] = arrs["hess" + prefix].ctypes.data
+        return ptrs
+
+    if pg:
+        r.ifpgh = pg
+        r.pot, r.grad, r.hess = outs("", ns, pg)
+    if targets is not None and pgt:
+        trg = _as_f(targets, np.float64)
+        arrs["trg"] = trg
+        r.nt, r.targ, r.ifpghtarg = trg.shape[1], trg.ctypes.data, pgt
+        r.pottarg, r.gradtarg, r.hesstarg = outs("targ", trg.shape[1], pgt)
+    return r, arrs

@@ -722,6 +722,47 @@ int fmm2d_b200_l2d_direct_noalloc(int nd, int ns, const double *sources,
                                   double _Complex *hess, double thresh,
                                   void *stream);
 
+/* Request loop for many independent evaluations on one GPU (no
+ * counterpart in the reference).  `slots` worker threads, each on its own
+ * stream, take queued requests whose estimated device footprint fits into
+ * the HBM budget left (bytes), so requests that arrive while others run
+ * are admitted as slots and memory free up and their work overlaps on the
+ * device.  A request larger than the whole budget finishes at once with
+ * ier = 4.  Arrays follow the guru drivers (host or device memory) and must
+ * stay valid until fmm2d_b200_server_wait returns for the ticket. */
+typedef struct {
+    int kernel; /* 0 lfmm2d, 1 cfmm2d, 2 hfmm2d */
+    int nd;
+    double eps;
+    double zk[2];
+    int ns;
+    const double *sources;
+    int ifcharge;
+    const double *charge;
+    int ifdipole;
+    const double *dipstr;
+    const double *dipvec; /* lfmm2d / hfmm2d only */
+    int ifpgh;
+    double *pot, *grad, *hess;
+    int nt;
+    const double *targ;
+    int ifpghtarg;
+    double *pottarg, *gradtarg, *hesstarg;
+    int precision; /* 0 auto (mixed when eps >= 1e-6), 1 all-FP64, 2 mixed */
+} fmm2d_b200_request;
+void *fmm2d_b200_server_create(int slots, double hbm_budget_bytes);
+/* Returns a ticket (>= 0), or -1 for an invalid request. */
+long long fmm2d_b200_server_submit(void *server, const fmm2d_b200_request *req);
+/* Waits for a ticket; returns its ier and, if times_ms is not null, the
+ * milliseconds spent queued, running and in total. */
+int fmm2d_b200_server_wait(void *server, long long ticket, double *times_ms);
+/* bytes in use, peak bytes in use, queued, running, rejected, peak running */
+void fmm2d_b200_server_stats(void *server, double *out6);
+/* The footprint estimate the server admits a request by (bytes). */
+double fmm2d_b200_request_bytes(const fmm2d_b200_request *req);
+/* Finishes the queued requests, then stops the workers. */
+void fmm2d_b200_server_destroy(void *server);
+
 /* Quadtree inspection in the reference's layout (pts_tree_mem/build/sort,
  * src/common/pts_tree2d.f:34,406,1222; computelists,
  * src/common/tree_routs2d.f:486). */

@@ -1,0 +1,77 @@
+"""The request loop (csrc/serve.cu): admission by the HBM budget, tickets,
+and -- on a GPU -- that every result in a mixed stream equals the same
+request run alone."""
+import numpy as np
+import pytest
+
+import wrappers as W
+
+
+@pytest.fixture(scope="module")
+def fm():
+    import fmm2d_c_translation_b200 as m
+    return m
+
+
+def _req(fm, kernel, n, seed, eps=1e-6, zk=5.0, pgt=0, precision=0):
+    rng = np.random.default_rng(seed)
+    src = rng.random((2, n))
+    q = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    trg = rng.random((2, n // 2)) if pgt else None
+    return fm.make_request(kernel, eps=eps, sources=src, charges=q, targets=trg, pg=2,
+                           pgt=pgt, zk=zk, precision=precision)
+
+
+def test_oversize_request_is_rejected(fm):
+    srv = fm.Server(slots=2, hbm_budget=1e6)
+    r, keep = _req(fm, "l", 100000, 1)
+    assert srv.request_bytes(r) > 1e6
+    t = srv.submit(r, keep)
+    ier, times = srv.wait(t)
+    assert ier == 4 and times[2] == 0.0
+    assert srv.stats()["rejected"] == 1
+    srv.close()
+
+
+def test_footprint_grows_with_size(fm):
+    srv = fm.Server(slots=1, hbm_budget=1e12)
+    small, _ = _req(fm, "l", 1000, 2)
+    big, _ = _req(fm, "l", 100000, 2)
+    helm, _ = _req(fm, "h", 100000, 2, zk=50.0)
+    assert srv.request_bytes(small) < srv.request_bytes(big) < srv.request_bytes(helm)
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_mixed_stream_matches_alone(fm):
+    specs = [("l", 20000, 1e-6, 0), ("h", 8000, 1e-6, 1), ("c", 15000, 1e-9, 0),
+             ("l", 3000, 1e-3, 1), ("h", 30000, 1e-9, 0), ("l", 60000, 1e-9, 1),
+             ("c", 1000, 1e-3, 1), ("h", 2000, 1e-6, 1)] * 3
+    # alone: one request at a time through a single-slot server
+    alone = []
+    srv1 = fm.Server(slots=1, hbm_budget=100e9)
+    for i, (k, n, eps, pgt) in enumerate(specs):
+        r, keep = _req(fm, k, n, 100 + i, eps=eps, zk=3.0 + i, pgt=pgt)
+        t = srv1.submit(r, keep)
+        ier, _ = srv1.wait(t)
+        assert ier == 0
+        alone.append(keep)
+    srv1.close()
+    # mixed: everything submitted at once into 6 slots and a budget that
+    # admits only part of the stream at a time
+    budget = 3e9
+    srv = fm.Server(slots=6, hbm_budget=budget)
+    tickets = []
+    for i, (k, n, eps, pgt) in enumerate(specs):
+        r, keep = _req(fm, k, n, 100 + i, eps=eps, zk=3.0 + i, pgt=pgt)
+        tickets.append((srv.submit(r, keep), keep))
+    for (t, keep), ref in zip(tickets, alone):
+        ier, _ = srv.wait(t)
+        assert ier == 0
+        for key in ref:
+            if key.startswith(("pot", "grad")):
+                assert W.rel_err(keep[key], ref[key]) <= 1e-14, key
+    st = srv.stats()
+    assert st["peak_bytes"] <= budget
+    assert st["peak_running"] >= 2
+    srv.close()
