@@ -382,3 +382,14 @@ FMM_EXPORT void fmm2d_b200_helm_hvec(int n, double z_re, double z_im, double rsc
 FMM_EXPORT void fmm2d_b200_helm_jvec(int n, double z_re, double z_im, double rscale, double *out) {
     helm_jvec(n, make_double2(z_re, z_im), rscale, reinterpret_cast<double2 *>(out));
 }
+
+// Leaf capacity of the mixed-precision Laplace / Cauchy mode for order
+// nterms (ndiv <= 0: back to the reference's rule); the current choice.
+FMM_EXPORT int fmm2d_b200_set_leaf_capacity(int nterms, int ndiv) {
+    if (nterms < 0 || nterms >= 128) return 4;
+    set_mixed_leaf_capacity(nterms, ndiv);
+    return 0;
+}
+FMM_EXPORT int fmm2d_b200_mixed_leaf_capacity(double eps, int ns, int nt) {
+    return mixed_leaf_capacity(laplace_nterms(eps), leaf_capacity(eps, ns, nt));
+}

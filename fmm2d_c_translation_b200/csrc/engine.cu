@@ -11,6 +11,7 @@
 #include "tree.cuh"
 
 #include <atomic>
+#include <mutex>
 #include <cmath>
 #include <stdlib.h>
 #include <string.h>
@@ -122,6 +123,29 @@ int leaf_capacity(double eps, int ns, int nt) {
     return ns + nt;
 }
 
+// Leaf capacity of the mixed-precision Laplace / Cauchy evaluation.  That
+// mode is held to eps against the direct sum, not to the reference's tree,
+// so its leaf capacity is chosen for speed: FMM2D_B200_MIXED_NDIV, else the
+// tuned value for the order (fmm2d_b200_set_leaf_capacity), else the
+// reference's rule.
+namespace {
+std::mutex g_ndiv_mu;
+int g_mixed_ndiv[128] = {0};
+}  // namespace
+
+int mixed_leaf_capacity(int p, int fallback) {
+    const char *e = getenv("FMM2D_B200_MIXED_NDIV");
+    if (e && atoi(e) > 0) return atoi(e);
+    std::lock_guard<std::mutex> g(g_ndiv_mu);
+    if (p >= 0 && p < 128 && g_mixed_ndiv[p] > 0) return g_mixed_ndiv[p];
+    return fallback;
+}
+
+void set_mixed_leaf_capacity(int p, int ndiv) {
+    std::lock_guard<std::mutex> g(g_ndiv_mu);
+    if (p >= 0 && p < 128) g_mixed_ndiv[p] = ndiv > 0 ? ndiv : 0;
+}
+
 namespace {
 
 void run_laplace_family(const FmmCall &c, CallCtx &ctx) {
@@ -143,7 +167,11 @@ void run_laplace_family(const FmmCall &c, CallCtx &ctx) {
     }
     prof_mark("h2d", s);
     // ---- tree ----
-    const int ndiv = c.ndiv >= 0 ? c.ndiv : leaf_capacity(c.eps, ns, nt);
+    // mixed precision for eps >= 1e-6 unless all-FP64 is requested
+    const int prec = c.precision;
+    const bool mixed = prec == kPrecMixed || (prec == kPrecAuto && c.eps >= 0.5e-6);
+    int ndiv = c.ndiv >= 0 ? c.ndiv : leaf_capacity(c.eps, ns, nt);
+    if (c.ndiv < 0 && mixed) ndiv = mixed_leaf_capacity(laplace_nterms(c.eps), ndiv);
     const int idivflag = c.ndiv >= 0 ? c.idivflag : 0;
     Tree T;
     build_tree(src_in.ptr, ns, trg_in.ptr, nt, ndiv, idivflag, kMaxLevels, s, T);
@@ -246,9 +274,7 @@ void run_laplace_family(const FmmCall &c, CallCtx &ctx) {
     // thresh = boxsize(0) * 2^-51 (c_translation/src/cfmm2d.c:994)
     P.thresh = T.boxsize[0] * std::ldexp(1.0, -51);
     P.ifnear = c.ifnear;
-    // mixed precision for eps >= 1e-6 unless all-FP64 is requested
-    const int prec = c.precision;
-    P.mixed = prec == kPrecMixed || (prec == kPrecAuto && c.eps >= 0.5e-6);
+    P.mixed = mixed;
     cauchy_fmm(T, P, s);
     // ---- back to input order, in the caller's layout ----
     auto unsort = [&](int n, const int *perm, int pgh, const DevBuf<double2> &po,

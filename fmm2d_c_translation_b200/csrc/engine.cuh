@@ -54,6 +54,11 @@ int laplace_nterms(double eps);
 // Leaf capacity (lndiv2d.f / hndiv2d.c).
 int leaf_capacity(double eps, int ns, int nt);
 
+// Leaf capacity of the mixed-precision Laplace / Cauchy mode for order p
+// (falls back to `fallback`), and its setter (ndiv <= 0 clears).
+int mixed_leaf_capacity(int p, int fallback);
+void set_mixed_leaf_capacity(int p, int ndiv);
+
 // Process-wide precision policy (env FMM2D_B200_PRECISION=auto|fp64|mixed,
 // or fmm2d_b200_set_precision).
 int current_precision();

@@ -1386,7 +1386,9 @@ void cauchy_fmm(const Tree &T, const CauchyProblem &P0, cudaStream_t s) {
               [&](int c0) { upward_chunk<1>(T, P, c0, binom, mp.get(), s); });
     const char *mode = getenv("FMM2D_B200_M2L");
     const bool simple = mode && !strcmp(mode, "simple");
-    if (simple || !m2l_tensor_fp64(T, P, mp.get(), loc.get(), s))
+    const bool fp32 = P.mixed && !(mode && !strcmp(mode, "fp64"));
+    if (simple || !((fp32 && m2l_fp32(T, P, mp.get(), loc.get(), s)) ||
+                    m2l_tensor_fp64(T, P, mp.get(), loc.get(), s)))
         per_chunk([&](int c0) { m2l_chunk<2>(T, P, c0, binom, mp.get(), loc.get(), s); },
                   [&](int c0) { m2l_chunk<1>(T, P, c0, binom, mp.get(), loc.get(), s); });
     prof_mark("m2l", s);

@@ -55,6 +55,12 @@ void cauchy_direct(const CauchyProblem &P, int ns, PointSet set,
 bool m2l_tensor_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp,
                      double2 *loc, cudaStream_t s);
 
+// FP32 M2L of the mixed-precision mode (m2l.cu): one complex matrix per
+// (child position, slot) applied to FP32 copies of the multipoles; false
+// when the order or the tree does not fit (the caller then uses FP64).
+bool m2l_fp32(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 *loc,
+              cudaStream_t s);
+
 // Binomial table C(l, m), l, m <= kLdc, built with the reference's Pascal
 // recurrence (init_carray, src/common/fmmcommon2d.f).
 constexpr int kLdc = 127;

@@ -241,17 +241,27 @@ void launch_dmma(const SegTable &sg, const int *boxes, const int *slots,
     }
 }
 
-}  // namespace
 
-bool m2l_tensor_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp,
-                     double2 *loc, cudaStream_t s) {
-    const int L = T.nlevels, p = P.p;
-    if (L < 2 || p > 63) return false;
+// The tiles of one M2L evaluation: target boxes of levels >= 2 that hold
+// points, sorted by (level, child position) = segment, and the source box of
+// every (target, slot).
+struct M2LWork {
+    DevBuf<uint32_t> keys, vals, kt, vt;
+    DevBuf<int> segd, slots;
+    int nseg = 0, ntarg = 0, ntiles = 0;
+    SegTable seg() const {
+        const int *h = segd.get();
+        return SegTable{h, h + nseg + 1, h + 2 * nseg + 1, h + 3 * nseg + 1, h + 4 * nseg + 1,
+                        nseg};
+    }
+};
+
+void ensure_slot_tables(cudaStream_t s) {
     static std::mutex tables_mu;
     static bool tables_ready[64] = {false};
     int dev = 0;
     FMM_CUDA(cudaGetDevice(&dev));
-    std::unique_lock<std::mutex> tables_lock(tables_mu);
+    std::lock_guard<std::mutex> tables_lock(tables_mu);
     if (!tables_ready[dev]) {
         const SlotTables st = make_slot_tables();
         FMM_CUDA(cudaMemcpyToSymbolAsync(c_slot_dx, st.dx, sizeof(st.dx), 0, cudaMemcpyHostToDevice, s));
@@ -260,17 +270,28 @@ bool m2l_tensor_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp,
         FMM_CUDA(cudaStreamSynchronize(s));
         tables_ready[dev] = true;
     }
-    tables_lock.unlock();
+}
+
+// Builds the segments (tiles of `tile` boxes) and the slot table; false
+// when a list-2 entry falls outside the 27 slots or there are too many
+// segments.
+bool m2l_work(const Tree &T, const CauchyProblem &P, int tile, cudaStream_t s, M2LWork &w) {
+    const int L = T.nlevels;
+    ensure_slot_tables(s);
     const int lo = T.lstart[2], n = T.nboxes - lo;
     const int nseg = 4 * (L - 1);
+    w.nseg = nseg;
     const int2 *sse = T.srcse.get(), *tse = T.trgse.get();
     const int spgh = P.sset.pgh, tpgh = P.tset.pgh;
     const int *lev = T.level.get(), *par = T.parent.get(), *chi = T.child.get();
     // ---- keys: (level - 2) * 4 + child position, or nseg when not a target
-    DevBuf<uint32_t> keys(n, s), vals(n, s), kt(n, s), vt(n, s);
+    w.keys.alloc(n, s);
+    w.vals.alloc(n, s);
+    w.kt.alloc(n, s);
+    w.vt.alloc(n, s);
     DevBuf<int> cnt(nseg + 1, s);
     cnt.zero(s);
-    uint32_t *kp = keys.get(), *vp = vals.get();
+    uint32_t *kp = w.keys.get(), *vp = w.vals.get();
     int *cp = cnt.get();
     for_each(n, s, [=] __device__(int64_t i) {
         const int b = lo + (int)i;
@@ -291,7 +312,7 @@ bool m2l_tensor_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp,
     });
     int bits = 1;
     while ((1 << bits) <= nseg) bits++;
-    radix_sort_pairs(kp, vp, kt.get(), vt.get(), n, bits, s);
+    radix_sort_pairs(kp, vp, w.kt.get(), w.vt.get(), n, bits, s);
     std::vector<int> hc(nseg + 1);
     FMM_CUDA(cudaMemcpyAsync(hc.data(), cp, (nseg + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
     FMM_CUDA(cudaStreamSynchronize(s));
@@ -304,21 +325,24 @@ bool m2l_tensor_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp,
         ct[k] = hc[k];
         lv[k] = 2 + k / 4;
         cpv[k] = k % 4;
-        run += (hc[k] + 7) / 8;
+        run += (hc[k] + tile - 1) / tile;
         start += hc[k];
     }
     tb[nseg] = run;
-    const int ntiles = run, ntarg = start;
-    if (ntiles == 0) return true;
+    w.ntiles = run;
+    w.ntarg = start;
+    if (w.ntiles == 0) return true;
     if (nseg + 1 > 257) return false;
-    DevBuf<int> segd(h.size(), s);
-    FMM_CUDA(cudaMemcpyAsync(segd.get(), h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+    w.segd.alloc(h.size(), s);
+    FMM_CUDA(cudaMemcpyAsync(w.segd.get(), h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice, s));
     // ---- the source box of every (target, slot), from list 2
-    DevBuf<int> slots((size_t)ntarg * kSlots, s), err(1, s);
-    FMM_CUDA(cudaMemsetAsync(slots.get(), 0xff, (size_t)ntarg * kSlots * sizeof(int), s));
+    const int ntarg = w.ntarg;
+    w.slots.alloc((size_t)ntarg * kSlots, s);
+    DevBuf<int> err(1, s);
+    FMM_CUDA(cudaMemsetAsync(w.slots.get(), 0xff, (size_t)ntarg * kSlots * sizeof(int), s));
     err.zero(s);
     {
-        int *sl = slots.get(), *ep = err.get();
+        int *sl = w.slots.get(), *ep = err.get();
         const int *n2 = T.nlist2.get(), *l2 = T.list2.get();
         const double2 *cen = T.centers.get();
         const double *bsd = T.d_boxsize.get();
@@ -346,17 +370,196 @@ bool m2l_tensor_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp,
             }
         });
     }
-    if (read_scalar(err.get(), s) != 0) return false;
-    SegTable sg{segd.get(), segd.get() + nseg + 1, segd.get() + 2 * nseg + 1,
-                segd.get() + 3 * nseg + 1, segd.get() + 4 * nseg + 1, nseg};
-    const int *boxes = (const int *)vp;
+    return read_scalar(err.get(), s) == 0;
+}
+
+// ---------------------------------------------------------------------------
+// FP32 M2L of the mixed-precision mode.  With t the slot offset in box
+// units, the whole shift is one complex matrix per (child position, slot),
+// level independent in the scaled form:
+//     T_ij = w2^i B_ij w1^j  (T_00 = log|t|),
+// and L_i += sum_slots sum_j T_ij M_j, plus log(r) M_0 in L_0.  One thread
+// per target box, 128 boxes of one segment per block; the block stages
+// each slot's matrix in shared memory (read as broadcasts) and every thread
+// streams its source multipole (an FP32 copy) through the j loop, keeping
+// the P1 x CH accumulators in registers (FP32 arithmetic, FP32
+// accumulation over the 27 slots, stored as FP64).
+// ---------------------------------------------------------------------------
+constexpr int kFp32Tile = 128;
+
+template <int P1, int CH>
+__global__ void __launch_bounds__(kFp32Tile) m2l_fp32_kernel(
+    SegTable seg, const int *__restrict__ boxes, const int *__restrict__ slots,
+    const double *__restrict__ bs, int ndc, int c0, int p, const float2 *__restrict__ Tall,
+    const float2 *__restrict__ mp32, double2 *__restrict__ loc, int ntiles) {
+    __shared__ float2 sT[P1 * P1];
+    __shared__ int s_tb[257];
+    for (int e = threadIdx.x; e <= seg.nseg && e < 257; e += blockDim.x) s_tb[e] = seg.tile_base[e];
+    __syncthreads();
+    const int stride = (p + 1) * ndc;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        int lo = 0, hi = seg.nseg;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (s_tb[mid] <= tile) lo = mid; else hi = mid;
+        }
+        const int sg = lo;
+        const int q = seg.start[sg] + (tile - s_tb[sg]) * kFp32Tile + threadIdx.x;
+        const bool valid = q < seg.start[sg] + seg.count[sg];
+        const int cp = seg.cpos[sg];
+        const float lr = (float)log(bs[seg.level[sg]]);
+        float2 acc[CH][P1];
+        float2 s0[CH];
+#pragma unroll
+        for (int c = 0; c < CH; c++) {
+            s0[c] = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int i = 0; i < P1; i++) acc[c][i] = make_float2(0.f, 0.f);
+        }
+        for (int k = 0; k < kSlots; k++) {
+            __syncthreads();  // the previous slot's matrix is no longer read
+            const float2 *Tk = Tall + ((size_t)cp * kSlots + k) * P1 * P1;
+            for (int e = threadIdx.x; e < P1 * P1; e += blockDim.x) sT[e] = Tk[e];
+            __syncthreads();
+            const int sb = valid ? slots[(size_t)q * kSlots + k] : -1;
+            if (sb < 0) continue;
+            const float2 *M = mp32 + (size_t)sb * stride + c0;
+#pragma unroll
+            for (int j = 0; j < P1; j++) {
+                float2 m[CH];
+#pragma unroll
+                for (int c = 0; c < CH; c++)
+                    m[c] = j <= p ? M[(size_t)j * ndc + c] : make_float2(0.f, 0.f);
+                if (j == 0) {
+#pragma unroll
+                    for (int c = 0; c < CH; c++) {
+                        s0[c].x += m[c].x;
+                        s0[c].y += m[c].y;
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < P1; i++) {
+                    const float2 t = sT[i * P1 + j];
+#pragma unroll
+                    for (int c = 0; c < CH; c++) {
+                        acc[c][i].x = fmaf(t.x, m[c].x, fmaf(-t.y, m[c].y, acc[c][i].x));
+                        acc[c][i].y = fmaf(t.x, m[c].y, fmaf(t.y, m[c].x, acc[c][i].y));
+                    }
+                }
+            }
+        }
+        if (valid) {
+            const int b = boxes[q];
+#pragma unroll
+            for (int c = 0; c < CH; c++) {
+                acc[c][0].x += lr * s0[c].x;
+                acc[c][0].y += lr * s0[c].y;
+            }
+#pragma unroll
+            for (int i = 0; i < P1; i++) {
+                if (i > p) break;
+#pragma unroll
+                for (int c = 0; c < CH; c++)
+                    loc[(size_t)b * stride + (size_t)i * ndc + c0 + c] =
+                        make_double2((double)acc[c][i].x, (double)acc[c][i].y);
+            }
+        }
+    }
+}
+
+// T_ij = w2^i B_ij w1^j per (child position, slot), FP64 built, FP32
+// stored, padded to P1 x P1; cached per device and order.
+const float2 *fp32_tables(int p, int P1, cudaStream_t s) {
+    static std::mutex mu;
+    static std::vector<std::pair<long, const float2 *>> cache;
+    int dev;
+    FMM_CUDA(cudaGetDevice(&dev));
+    const long key = ((long)dev << 20) | ((long)p << 8) | P1;
+    std::lock_guard<std::mutex> g(mu);
+    for (auto &e : cache)
+        if (e.first == key) return e.second;
+    const SlotTables st = make_slot_tables();
+    // binomials C(l, m) for l <= 2 P1
+    const int nc = 2 * P1 + 2;
+    std::vector<double> C((size_t)nc * nc, 0.0);
+    for (int l = 0; l < nc; l++) {
+        C[(size_t)l * nc] = 1.0;
+        for (int m = 1; m <= l; m++)
+            C[(size_t)l * nc + m] = C[(size_t)(l - 1) * nc + m - 1] + (m < l ? C[(size_t)(l - 1) * nc + m] : 0.0);
+    }
+    std::vector<float2> h((size_t)4 * kSlots * P1 * P1, make_float2(0.f, 0.f));
+    for (int c = 0; c < 4; c++)
+        for (int k = 0; k < kSlots; k++) {
+            const double tx = st.dx[c][k], ty = st.dy[c][k];
+            const double tn = 1.0 / (tx * tx + ty * ty);
+            const double2 w2 = make_double2(tx * tn, -ty * tn), w1 = make_double2(-w2.x, -w2.y);
+            float2 *Tk = h.data() + ((size_t)c * kSlots + k) * P1 * P1;
+            double2 w2i = make_double2(1.0, 0.0);
+            for (int i = 0; i <= p; i++) {
+                double2 w1j = make_double2(1.0, 0.0);
+                for (int j = 0; j <= p; j++) {
+                    double b;
+                    if (i == 0)
+                        b = j == 0 ? 0.0 : 1.0;
+                    else
+                        b = j == 0 ? -1.0 / i : C[(size_t)(i + j - 1) * nc + (j - 1)];
+                    double2 v = cscal(cmul(w2i, w1j), b);
+                    if (i == 0 && j == 0) v = make_double2(0.5 * std::log(tx * tx + ty * ty), 0.0);
+                    Tk[i * P1 + j] = make_float2((float)v.x, (float)v.y);
+                    w1j = cmul(w1j, w1);
+                }
+                w2i = cmul(w2i, w2);
+            }
+        }
+    float2 *d = nullptr;
+    FMM_CUDA(cudaMalloc(&d, h.size() * sizeof(float2)));
+    FMM_CUDA(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(float2), cudaMemcpyHostToDevice, s));
+    FMM_CUDA(cudaStreamSynchronize(s));
+    cache.push_back({key, d});
+    return d;
+}
+
+template <int P1>
+void launch_fp32(const M2LWork &w, const Tree &T, const CauchyProblem &P, const float2 *Tab,
+                 const float2 *mp32, double2 *loc, cudaStream_t s) {
+    const int blocks = std::max(1, std::min(w.ntiles, kNumSM * 16));
+    const SegTable sg = w.seg();
+    const int *boxes = (const int *)w.vals.get();
+    for (int c0 = 0; c0 < P.ndc;) {
+        if (P.ndc - c0 >= 2) {
+            m2l_fp32_kernel<P1, 2><<<blocks, kFp32Tile, 0, s>>>(
+                sg, boxes, w.slots.get(), T.d_boxsize.get(), P.ndc, c0, P.p, Tab, mp32, loc,
+                w.ntiles);
+            c0 += 2;
+        } else {
+            m2l_fp32_kernel<P1, 1><<<blocks, kFp32Tile, 0, s>>>(
+                sg, boxes, w.slots.get(), T.d_boxsize.get(), P.ndc, c0, P.p, Tab, mp32, loc,
+                w.ntiles);
+            c0 += 1;
+        }
+        FMM_CHECK_LAUNCH();
+    }
+}
+
+}  // namespace
+
+bool m2l_tensor_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp,
+                     double2 *loc, cudaStream_t s) {
+    const int L = T.nlevels, p = P.p;
+    if (L < 2 || p > 63) return false;
+    M2LWork w;
+    if (!m2l_work(T, P, 8, s, w)) return false;
+    if (w.ntiles == 0) return true;
+    const SegTable sg = w.seg();
+    const int *boxes = (const int *)w.vals.get();
     const double *bs = T.d_boxsize.get();
     const double *binom = device_binomials(s);
+    const int ntiles = w.ntiles;
     const int ks = (p + 1 + 3) / 4;
     const int mt = (p + 1 + 7) / 8;
 #define FMM_M2L_CASE(MT_, KS_)                                                   \
     if (mt <= MT_ && ks <= KS_) {                                                \
-        launch_dmma<MT_, KS_>(sg, boxes, slots.get(), bs, P.ndc, p, binom, mp,   \
+        launch_dmma<MT_, KS_>(sg, boxes, w.slots.get(), bs, P.ndc, p, binom, mp, \
                               loc, ntiles, s);                                   \
         return true;                                                             \
     }
@@ -369,6 +572,32 @@ bool m2l_tensor_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp,
     FMM_M2L_CASE(8, 16)
 #undef FMM_M2L_CASE
     return false;
+}
+
+bool m2l_fp32(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 *loc,
+              cudaStream_t s) {
+    const int L = T.nlevels, p = P.p;
+    if (L < 2 || p + 1 > 20) return false;
+    M2LWork w;
+    if (!m2l_work(T, P, kFp32Tile, s, w)) return false;
+    if (w.ntiles == 0) return true;
+    // FP32 copy of the multipoles of levels >= 2
+    const int lo = T.lstart[2];
+    const size_t stride = (size_t)(p + 1) * P.ndc;
+    const size_t nv = (size_t)(T.nboxes - lo) * stride;
+    DevBuf<float2> mp32((size_t)T.nboxes * stride, s);
+    {
+        const double2 *src = mp + (size_t)lo * stride;
+        float2 *dst = mp32.get() + (size_t)lo * stride;
+        for_each((int64_t)nv, s, [=] __device__(int64_t i) {
+            dst[i] = make_float2((float)src[i].x, (float)src[i].y);
+        });
+    }
+    if (p + 1 <= 12)
+        launch_fp32<12>(w, T, P, fp32_tables(p, 12, s), mp32.get(), loc, s);
+    else
+        launch_fp32<20>(w, T, P, fp32_tables(p, 20, s), mp32.get(), loc, s);
+    return true;
 }
 
 }  // namespace fmm2d
