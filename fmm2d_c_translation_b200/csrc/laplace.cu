@@ -1134,6 +1134,239 @@ const double2 *shift_tables(int p, bool m2m, cudaStream_t s) {
     return d;
 }
 
+// ---------------------------------------------------------------------------
+// Box-thread forms of P2M, P2L, M2M and L2L for orders p < P1 (P1 <= 20):
+// one thread per box keeps all p + 1 coefficients of CH channels in
+// registers, so each source's powers are built once by recurrence and each
+// child / parent coefficient is loaded once.  Same formulas as the
+// coefficient-thread kernels above; FP64 throughout.
+// ---------------------------------------------------------------------------
+template <int P1, int CH>
+__global__ void __launch_bounds__(128) p2m_box_kernel(
+    int lo, int hi, int p, const int *__restrict__ nchild, const double2 *__restrict__ centers,
+    const int *__restrict__ level, const double *__restrict__ bs, const int2 *__restrict__ sse,
+    const double2 *__restrict__ src, const double2 *__restrict__ chg,
+    const double2 *__restrict__ dip, int ifc, int ifd, int ndc, int c0,
+    double2 *__restrict__ mp) {
+    const int stride = (p + 1) * ndc;
+    for (int b = lo + blockIdx.x * blockDim.x + threadIdx.x; b < hi;
+         b += gridDim.x * blockDim.x) {
+        if (nchild[b] != 0) continue;
+        const int2 rg = sse[b];
+        if (rg.y <= rg.x) continue;
+        const double2 c = centers[b];
+        const double r = bs[level[b]], rinv = 1.0 / r;
+        double2 acc[CH][P1];
+#pragma unroll
+        for (int q = 0; q < CH; q++)
+#pragma unroll
+            for (int k = 0; k < P1; k++) acc[q][k] = make_double2(0.0, 0.0);
+        for (int j = rg.x; j < rg.y; j++) {
+            const double2 x = src[j];
+            const double2 z = make_double2((x.x - c.x) / r, (x.y - c.y) / r);
+            double2 qv[CH], dv[CH];
+#pragma unroll
+            for (int q = 0; q < CH; q++) {
+                qv[q] = ifc ? chg[(size_t)j * ndc + c0 + q] : make_double2(0.0, 0.0);
+                dv[q] = ifd ? cscal(dip[(size_t)j * ndc + c0 + q], rinv) : make_double2(0.0, 0.0);
+            }
+#pragma unroll
+            for (int q = 0; q < CH; q++) acc[q][0] = cadd(acc[q][0], qv[q]);
+            double2 zk1 = make_double2(1.0, 0.0);  // z^(k-1)
+#pragma unroll
+            for (int k = 1; k < P1; k++) {
+                if (k > p) break;
+                const double2 zk = cmul(zk1, z);
+                const double2 cz = cscal(zk, -1.0 / k);
+#pragma unroll
+                for (int q = 0; q < CH; q++) {
+                    cfma(acc[q][k], qv[q], cz);
+                    cfma(acc[q][k], dv[q], zk1);
+                }
+                zk1 = zk;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < P1; k++) {
+            if (k > p) break;
+#pragma unroll
+            for (int q = 0; q < CH; q++) mp[(size_t)b * stride + (size_t)k * ndc + c0 + q] = acc[q][k];
+        }
+    }
+}
+
+template <int P1, int CH>
+__global__ void __launch_bounds__(128) p2l_box_kernel(
+    int lo, int hi, int p, EvalCounts ec, const int *__restrict__ nlist4,
+    const int *__restrict__ list4, const double2 *__restrict__ centers,
+    const int *__restrict__ level, const double *__restrict__ bs,
+    const double2 *__restrict__ src, const double2 *__restrict__ chg,
+    const double2 *__restrict__ dip, int ifc, int ifd, int ndc, int c0,
+    double2 *__restrict__ loc) {
+    const int stride = (p + 1) * ndc;
+    for (int b = lo + blockIdx.x * blockDim.x + threadIdx.x; b < hi;
+         b += gridDim.x * blockDim.x) {
+        const int n4 = nlist4[b];
+        if (n4 == 0 || ec.npts(b) <= 0) continue;
+        const double2 c = centers[b];
+        const double r = bs[level[b]];
+        double2 acc[CH][P1];
+#pragma unroll
+        for (int q = 0; q < CH; q++)
+#pragma unroll
+            for (int k = 0; k < P1; k++) acc[q][k] = make_double2(0.0, 0.0);
+        for (int e = 0; e < n4; e++) {
+            const int2 rg = ec.sse[list4[kMaxList4 * b + e]];
+            for (int j = rg.x; j < rg.y; j++) {
+                const double2 x = src[j];
+                const double2 z0 = make_double2(x.x - c.x, x.y - c.y);
+                const double2 zi = cinv(z0);
+                const double2 w = cscal(zi, r);  // r / z0
+                const double lz = 0.5 * log(z0.x * z0.x + z0.y * z0.y);
+                double2 qv[CH], dv[CH];
+#pragma unroll
+                for (int q = 0; q < CH; q++) {
+                    qv[q] = ifc ? chg[(size_t)j * ndc + c0 + q] : make_double2(0.0, 0.0);
+                    // -d / z0
+                    dv[q] = ifd ? cscal(cmul(dip[(size_t)j * ndc + c0 + q], zi), -1.0)
+                                : make_double2(0.0, 0.0);
+                }
+                double2 wk = make_double2(1.0, 0.0);
+#pragma unroll
+                for (int k = 0; k < P1; k++) {
+                    if (k > p) break;
+#pragma unroll
+                    for (int q = 0; q < CH; q++) {
+                        if (k == 0)
+                            cfma(acc[q][0], qv[q], make_double2(lz, 0.0));
+                        else
+                            cfma(acc[q][k], qv[q], cscal(wk, -1.0 / k));
+                        cfma(acc[q][k], dv[q], wk);
+                    }
+                    wk = cmul(wk, w);
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < P1; k++) {
+            if (k > p) break;
+#pragma unroll
+            for (int q = 0; q < CH; q++) {
+                double2 &o = loc[(size_t)b * stride + (size_t)k * ndc + c0 + q];
+                o = cadd(o, acc[q][k]);
+            }
+        }
+    }
+}
+
+// M2M: parent i = sum over children with sources of sum_{j <= i}
+// A[cpos][i][j] M_j (A staged in shared memory, read as broadcasts).
+template <int P1, int CH>
+__global__ void __launch_bounds__(128) m2m_box_kernel(
+    int lo, int hi, int p, const int *__restrict__ nchild, const int *__restrict__ child,
+    const int2 *__restrict__ sse, const double2 *__restrict__ A, int ndc, int c0,
+    double2 *__restrict__ mp) {
+    __shared__ double2 sA[4 * P1 * P1];
+    const int np1 = p + 1;
+    for (int e = threadIdx.x; e < 4 * P1 * P1; e += blockDim.x) {
+        const int cp = e / (P1 * P1), i = (e / P1) % P1, j = e % P1;
+        sA[e] = (i <= p && j <= p) ? A[((size_t)cp * np1 + i) * np1 + j] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    const int stride = np1 * ndc;
+    for (int b = lo + blockIdx.x * blockDim.x + threadIdx.x; b < hi;
+         b += gridDim.x * blockDim.x) {
+        if (nchild[b] == 0) continue;
+        double2 acc[CH][P1];
+#pragma unroll
+        for (int q = 0; q < CH; q++)
+#pragma unroll
+            for (int i = 0; i < P1; i++) acc[q][i] = make_double2(0.0, 0.0);
+        for (int cs = 0; cs < 4; cs++) {
+            const int cb = child[4 * b + cs];
+            if (count(sse, cb) <= 0) continue;
+            const double2 *M = mp + (size_t)cb * stride + c0;
+            const double2 *Ac = sA + cs * P1 * P1;
+#pragma unroll
+            for (int j = 0; j < P1; j++) {
+                if (j > p) break;
+                double2 m[CH];
+#pragma unroll
+                for (int q = 0; q < CH; q++) m[q] = M[(size_t)j * ndc + q];
+#pragma unroll
+                for (int i = j; i < P1; i++) {
+                    const double2 a = Ac[i * P1 + j];
+#pragma unroll
+                    for (int q = 0; q < CH; q++) cfma(acc[q][i], a, m[q]);
+                }
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < P1; i++) {
+            if (i > p) break;
+#pragma unroll
+            for (int q = 0; q < CH; q++) mp[(size_t)b * stride + (size_t)i * ndc + c0 + q] = acc[q][i];
+        }
+    }
+}
+
+// L2L: child i += sum_{j >= i} A[cpos][i][j] Lp_j for the children of
+// parents that hold points.
+template <int P1, int CH>
+__global__ void __launch_bounds__(128) l2l_box_kernel(
+    int lo, int hi, int p, EvalCounts ec, const int *__restrict__ parent,
+    const int *__restrict__ child, const double2 *__restrict__ A, int ndc, int c0,
+    double2 *__restrict__ loc) {
+    __shared__ double2 sA[4 * P1 * P1];
+    const int np1 = p + 1;
+    for (int e = threadIdx.x; e < 4 * P1 * P1; e += blockDim.x) {
+        const int cp = e / (P1 * P1), i = (e / P1) % P1, j = e % P1;
+        sA[e] = (i <= p && j <= p) ? A[((size_t)cp * np1 + i) * np1 + j] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    const int stride = np1 * ndc;
+    for (int b = lo + blockIdx.x * blockDim.x + threadIdx.x; b < hi;
+         b += gridDim.x * blockDim.x) {
+        const int pb = parent[b];
+        if (ec.npts(pb) <= 0) continue;
+        const int cs = child_pos(child, pb, b);
+        const double2 *Lp = loc + (size_t)pb * stride + c0;
+        const double2 *Ac = sA + cs * P1 * P1;
+        double2 acc[CH][P1];
+#pragma unroll
+        for (int q = 0; q < CH; q++)
+#pragma unroll
+            for (int i = 0; i < P1; i++) acc[q][i] = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int j = 0; j < P1; j++) {
+            if (j > p) break;
+            double2 l[CH];
+#pragma unroll
+            for (int q = 0; q < CH; q++) l[q] = Lp[(size_t)j * ndc + q];
+#pragma unroll
+            for (int i = 0; i <= j; i++) {
+                const double2 a = Ac[i * P1 + j];
+#pragma unroll
+                for (int q = 0; q < CH; q++) cfma(acc[q][i], a, l[q]);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < P1; i++) {
+            if (i > p) break;
+#pragma unroll
+            for (int q = 0; q < CH; q++) {
+                double2 &o = loc[(size_t)b * stride + (size_t)i * ndc + c0 + q];
+                o = cadd(o, acc[q][i]);
+            }
+        }
+    }
+}
+
+
+inline int box_blocks(int nbox) {
+    return std::max(1, std::min((nbox + 127) / 128, kNumSM * 16));
+}
+
 // Upward pass for channels [c0, c0 + CH): P2M at the leaves of levels >= 2,
 // then M2M from the finest parents up.
 template <int CH>
@@ -1146,21 +1379,32 @@ void upward_chunk(const Tree &T, const CauchyProblem &P, int c0,
         const int64_t n = (int64_t)nbox * (p + 1);
         return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, kNumSM * 8));
     };
+    const bool boxk = p + 1 <= 20;
     if (L >= 2) {
         const int lo = T.lstart[2];
-        p2m_coef_kernel<CH><<<blocks(nb - lo), 256, 0, s>>>(
-            lo, nb, p, T.nchild.get(), T.centers.get(), T.level.get(), bs,
-            T.srcse.get(), P.src, P.charge, P.dipstr, P.ifcharge, P.ifdipole,
-            P.ndc, c0, mp);
+        if (boxk)
+            p2m_box_kernel<20, CH><<<box_blocks(nb - lo), 128, 0, s>>>(
+                lo, nb, p, T.nchild.get(), T.centers.get(), T.level.get(), bs,
+                T.srcse.get(), P.src, P.charge, P.dipstr, P.ifcharge, P.ifdipole,
+                P.ndc, c0, mp);
+        else
+            p2m_coef_kernel<CH><<<blocks(nb - lo), 256, 0, s>>>(
+                lo, nb, p, T.nchild.get(), T.centers.get(), T.level.get(), bs,
+                T.srcse.get(), P.src, P.charge, P.dipstr, P.ifcharge, P.ifdipole,
+                P.ndc, c0, mp);
         FMM_CHECK_LAUNCH();
     }
     prof_mark("p2m", s);
     const double2 *A = shift_tables(p, true, s);
     for (int l = L - 1; l >= 1; l--) {
         const int lo = T.lstart[l], hi = T.lend[l];
-        m2m_coef_kernel<CH><<<blocks(hi - lo), 256, 0, s>>>(
-            lo, hi, p, T.nchild.get(), T.child.get(), T.srcse.get(), A, P.ndc,
-            c0, mp);
+        if (boxk)
+            m2m_box_kernel<20, CH><<<box_blocks(hi - lo), 128, 0, s>>>(
+                lo, hi, p, T.nchild.get(), T.child.get(), T.srcse.get(), A, P.ndc, c0, mp);
+        else
+            m2m_coef_kernel<CH><<<blocks(hi - lo), 256, 0, s>>>(
+                lo, hi, p, T.nchild.get(), T.child.get(), T.srcse.get(), A, P.ndc,
+                c0, mp);
         FMM_CHECK_LAUNCH();
     }
     prof_mark("m2m", s);
@@ -1203,12 +1447,19 @@ void downward_chunk(const Tree &T, const CauchyProblem &P, int c0,
         return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, kNumSM * 8));
     };
     // step 2: P2L from list 4 (after M2L, which initialises the locals)
+    const bool boxk = p + 1 <= 20;
     if (L >= 2) {
         const int lo = T.lstart[2];
-        p2l_coef_kernel<CH><<<blocks(nb - lo), 256, 0, s>>>(
-            lo, nb, p, ec, T.nlist4.get(), T.list4.get(), T.centers.get(),
-            T.level.get(), bs, P.src, P.charge, P.dipstr, P.ifcharge,
-            P.ifdipole, P.ndc, c0, loc);
+        if (boxk)
+            p2l_box_kernel<20, CH><<<box_blocks(nb - lo), 128, 0, s>>>(
+                lo, nb, p, ec, T.nlist4.get(), T.list4.get(), T.centers.get(),
+                T.level.get(), bs, P.src, P.charge, P.dipstr, P.ifcharge,
+                P.ifdipole, P.ndc, c0, loc);
+        else
+            p2l_coef_kernel<CH><<<blocks(nb - lo), 256, 0, s>>>(
+                lo, nb, p, ec, T.nlist4.get(), T.list4.get(), T.centers.get(),
+                T.level.get(), bs, P.src, P.charge, P.dipstr, P.ifcharge,
+                P.ifdipole, P.ndc, c0, loc);
         FMM_CHECK_LAUNCH();
     }
     prof_mark("p2l", s);
@@ -1216,8 +1467,12 @@ void downward_chunk(const Tree &T, const CauchyProblem &P, int c0,
     const double2 *A = shift_tables(p, false, s);
     for (int l = 1; l <= L - 1; l++) {
         const int lo = T.lstart[l + 1], hi = T.lend[l + 1];
-        l2l_coef_kernel<CH><<<blocks(hi - lo), 256, 0, s>>>(
-            lo, hi, p, ec, T.parent.get(), T.child.get(), A, P.ndc, c0, loc);
+        if (boxk)
+            l2l_box_kernel<20, CH><<<box_blocks(hi - lo), 128, 0, s>>>(
+                lo, hi, p, ec, T.parent.get(), T.child.get(), A, P.ndc, c0, loc);
+        else
+            l2l_coef_kernel<CH><<<blocks(hi - lo), 256, 0, s>>>(
+                lo, hi, p, ec, T.parent.get(), T.child.get(), A, P.ndc, c0, loc);
         FMM_CHECK_LAUNCH();
     }
     prof_mark("l2l", s);
