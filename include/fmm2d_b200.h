@@ -661,6 +661,13 @@ int fmm2d_b200_release_memory(void);
  * and leaf capacity (src/laplace/lndiv2d.f:1) for a precision. */
 int fmm2d_b200_laplace_nterms(double eps);
 int fmm2d_b200_leaf_capacity(double eps, int ns, int nt);
+/* Leaf capacity of the mixed-precision Laplace / Cauchy mode (held to eps
+ * against the direct sum, not to the reference's tree) for expansion order
+ * nterms; ndiv <= 0 restores the reference's rule.  The environment
+ * variable FMM2D_B200_MIXED_NDIV overrides both.  The second function
+ * returns the capacity a mixed call at eps would use. */
+int fmm2d_b200_set_leaf_capacity(int nterms, int ndiv);
+int fmm2d_b200_mixed_leaf_capacity(double eps, int ns, int nt);
 
 /* Direct sums on the GPU, incrementing the outputs (the reference's
  * l2d_direct* / c2d_direct* kernels, src/laplace/lapkernels2d.f,
