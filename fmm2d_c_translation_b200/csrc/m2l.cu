@@ -24,8 +24,10 @@
 #include "sort.cuh"
 
 #include <algorithm>
+#include <cmath>
 #include <mutex>
 #include <stdlib.h>
+#include <string.h>
 #include <vector>
 
 namespace fmm2d {
@@ -541,6 +543,418 @@ void launch_fp32(const M2LWork &w, const Tree &T, const CauchyProblem &P, const 
     }
 }
 
+// ---------------------------------------------------------------------------
+// M2L of the mixed mode on the 5th-generation tensor cores (tcgen05, kind
+// tf32, operands in shared memory, accumulator in tensor memory).
+//
+// In real form the slot operator is the 2P x 2P block matrix
+// [[Re T, -Im T], [Im T, Re T]] (P = p + 1) acting on [Re M; Im M].  A tile
+// is 128 rows = 128 / CH target boxes x CH channels of one segment; for each
+// of the 27 slots the block gathers the rows' source multipoles (A, 128 x
+// KP, KP = 2P rounded up to 8) and copies the slot's matrix (B, KP x KP,
+// stored N-rows x K as the MMA's K-major B) into shared memory, and one
+// thread issues D += A_hi B_hi + A_hi B_lo + A_lo B_hi (3 x TF32 split:
+// x = hi + lo, both TF32-rounded; about 22 significant bits) accumulating
+// all slots in the same tensor-memory tile.  The rows are read back with
+// tcgen05.ld and stored as FP64.  Waits on the MMA-completion barrier are
+// bounded; a wait that runs out sets *err and the kernel returns after
+// releasing its tensor memory.
+//
+// Shared-memory operands use the no-swizzle K-major layout: 8-row x 16-byte
+// core matrices, contiguous 128 bytes each; core matrix (row group g, K
+// chunk c) at ((c * G + g) * 128) bytes, G = rows / 8.  So SBO (between row
+// groups) = 128 bytes and LBO (between K chunks) = G * 128 bytes.
+// ---------------------------------------------------------------------------
+constexpr int kTcRows = 128;
+constexpr int kTcMaxKP = 40;
+constexpr long kTcWaitLimit = 1L << 26;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *ptr) {
+    return (uint32_t)__cvta_generic_to_shared(ptr);
+}
+
+// Shared-memory matrix descriptor: start, LBO, SBO (bytes, 16-byte units),
+// descriptor version 1 (bits 46-47), no swizzle.
+__device__ __forceinline__ uint64_t tc_sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = (uint64_t)((addr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+
+__device__ __forceinline__ float tc_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc,
+                                       uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        :
+        : "r"(d), "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 :
+                 : "r"(mbar)
+                 : "memory");
+}
+
+// Bounded wait for the barrier phase with the given parity.
+__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity) {
+    for (long it = 0; it < kTcWaitLimit; it++) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(ok)
+            : "r"(mbar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tc_ld8(uint32_t taddr, float (&v)[8]) {
+    uint32_t r[8];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7])
+        : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 8; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// byte offset of element (row, k) in a K-major no-swizzle operand of
+// `rows` rows
+__host__ __device__ __forceinline__ int tc_off(int row, int k, int rows) {
+    return (((k >> 2) * (rows >> 3) + (row >> 3)) << 7) + ((row & 7) << 4) + ((k & 3) << 2);
+}
+
+template <int CH, int HALF>
+__global__ void __launch_bounds__(kTcRows, 1) m2l_tc_kernel(
+    SegTable seg, const int *__restrict__ boxes, const int *__restrict__ slots,
+    const double *__restrict__ bs, int ndc, int c0, int p,
+    const float *__restrict__ Bimg, const float2 *__restrict__ T0,
+    const float2 *__restrict__ mp32, double2 *__restrict__ loc, int ntiles,
+    int *__restrict__ err) {
+    constexpr int KP = 2 * HALF;  // [Re 0..HALF-1 | Im 0..HALF-1]
+    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    float *sAhi = reinterpret_cast<float *>(tc_smem);
+    float *sAlo = sAhi + kTcRows * KP;
+    float *sBhi = sAlo + kTcRows * KP;  // followed by the lo image
+    __shared__ __align__(8) uint64_t s_mbar;
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_tb[257];
+    __shared__ unsigned s_mask;
+    __shared__ float2 s_t0[kSlots * (kTcMaxKP / 2)];
+    const int tid = threadIdx.x, warp = tid >> 5;
+    for (int e = tid; e <= seg.nseg && e < 257; e += blockDim.x) s_tb[e] = seg.tile_base[e];
+    if (tid == 0) s_mask = 0u;
+    const uint32_t mbar = smem_u32(&s_mbar);
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(1) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&s_tmem)),
+                     "r"(64)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    const int TPT = kTcRows / CH;
+    const int P = p + 1, stride = P * ndc;
+    const int nB4 = (2 * KP * KP) / 4;  // float4s of the two B images
+    const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(KP >> 3) << 17) |
+                           (8u << 24);
+    const uint32_t aLBO = (kTcRows / 8) * 128, bLBO = (KP / 8) * 128, SBO = 128;
+    const uint32_t aHi = smem_u32(sAhi), aLo = smem_u32(sAlo);
+    const uint32_t bHi = smem_u32(sBhi), bLo = bHi + KP * KP * 4;
+    uint32_t ncommit = 0;
+    bool failed = false;
+    int cp_loaded = -1;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        int lo = 0, hi = seg.nseg;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (s_tb[mid] <= tile) lo = mid; else hi = mid;
+        }
+        const int sg = lo;
+        const int qend = seg.start[sg] + seg.count[sg];
+        const int q = seg.start[sg] + (tile - s_tb[sg]) * TPT + tid / CH;
+        const int c = c0 + tid % CH;
+        const bool valid = q < qend;
+        const int cp = seg.cpos[sg];
+        // the source of every slot for this row, and the tile's slot mask
+        const int *qslots = slots + (size_t)(valid ? q : 0) * kSlots;
+        unsigned mymask = 0u;
+#pragma unroll
+        for (int k = 0; k < kSlots; k++)
+            if (valid && qslots[k] >= 0) mymask |= 1u << k;
+        if (mymask) atomicOr(&s_mask, mymask);
+        if (cp != cp_loaded) {  // row 0 of this position's 27 matrices
+            for (int e = tid; e < kSlots * P; e += blockDim.x)
+                s_t0[(e / P) * (kTcMaxKP / 2) + e % P] = T0[((size_t)cp * kSlots + e / P) * P + e % P];
+        }
+        cp_loaded = cp;
+        __syncthreads();
+        unsigned mask = s_mask;
+        __syncthreads();  // all have read the mask; it is cleared for the next tile
+        if (tid == 0) s_mask = 0u;
+        float l0x = 0.f, l0y = 0.f;  // row 0 (L_0) on the CUDA cores
+        float s0x = 0.f, s0y = 0.f;
+        // registers holding the next slot's row and matrix part
+        float2 mrow[HALF];
+        float4 breg[(2 * KP * KP / 4 + kTcRows - 1) / kTcRows];
+        auto prefetch = [&](int k) {
+            const int sb = valid ? qslots[k] : -1;
+            const float2 *M = mp32 + (size_t)(sb >= 0 ? sb : 0) * stride + c;
+#pragma unroll
+            for (int j = 0; j < HALF; j++)
+                mrow[j] = (sb >= 0 && j < P) ? M[(size_t)j * ndc] : make_float2(0.f, 0.f);
+            const float4 *src = reinterpret_cast<const float4 *>(
+                Bimg + ((size_t)cp * kSlots + k) * 2 * KP * KP);
+#pragma unroll
+            for (int u = 0; u < (int)(sizeof(breg) / sizeof(float4)); u++) {
+                const int e = tid + u * kTcRows;
+                breg[u] = e < nB4 ? src[e] : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        };
+        bool issued = false;
+        if (mask) prefetch(__ffs(mask) - 1);
+        while (mask) {
+            const int k = __ffs(mask) - 1;
+            mask &= mask - 1;
+            // the previous slot's MMAs read the operand buffers
+            if (ncommit > 0 && !tc_wait(mbar, (ncommit - 1) & 1)) failed = true;
+            if (__syncthreads_or(failed)) {
+                failed = true;
+                break;
+            }
+            // A row `tid`: [Re M_0..HALF-1 | Im M_0..HALF-1] (zero beyond p),
+            // split into TF32 hi / lo
+#pragma unroll
+            for (int kc = 0; kc < KP; kc += 4) {
+                float4 vh, vl;
+                float *ph = &vh.x, *pl = &vl.x;
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int kk = kc + u;
+                    const float v = kk < HALF ? mrow[kk].x : mrow[kk - HALF].y;
+                    const float h = tc_tf32(v);
+                    ph[u] = h;
+                    pl[u] = tc_tf32(v - h);
+                }
+                const int off = tc_off(tid, kc, kTcRows) >> 2;
+                *reinterpret_cast<float4 *>(sAhi + off) = vh;
+                *reinterpret_cast<float4 *>(sAlo + off) = vl;
+            }
+            {
+                float4 *dst = reinterpret_cast<float4 *>(sBhi);
+#pragma unroll
+                for (int u = 0; u < (int)(sizeof(breg) / sizeof(float4)); u++) {
+                    const int e = tid + u * kTcRows;
+                    if (e < nB4) dst[e] = breg[u];
+                }
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncthreads();
+            if (tid == 0) {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                for (int ks = 0; ks < KP / 8; ks++) {
+                    const uint32_t ao = 2 * ks * aLBO, bo = 2 * ks * bLBO;
+                    tc_mma(tmem, tc_sdesc(aHi + ao, aLBO, SBO), tc_sdesc(bHi + bo, bLBO, SBO),
+                           idesc, (issued || ks > 0) ? 1u : 0u);
+                    tc_mma(tmem, tc_sdesc(aHi + ao, aLBO, SBO), tc_sdesc(bLo + bo, bLBO, SBO),
+                           idesc, 1u);
+                    tc_mma(tmem, tc_sdesc(aLo + ao, aLBO, SBO), tc_sdesc(bHi + bo, bLBO, SBO),
+                           idesc, 1u);
+                }
+                tc_commit(mbar);
+            }
+            ncommit++;
+            issued = true;
+            // row 0 on the CUDA cores while the MMAs run, then the next slot
+            if (valid && qslots[k] >= 0) {
+                const float2 *t0 = s_t0 + k * (kTcMaxKP / 2);
+#pragma unroll
+                for (int j = 0; j < HALF; j++) {
+                    if (j < P) {
+                        const float2 t = t0[j], m = mrow[j];
+                        l0x = fmaf(t.x, m.x, fmaf(-t.y, m.y, l0x));
+                        l0y = fmaf(t.x, m.y, fmaf(t.y, m.x, l0y));
+                    }
+                }
+                s0x += mrow[0].x;
+                s0y += mrow[0].y;
+            }
+            if (mask) prefetch(__ffs(mask) - 1);
+        }
+        if (failed) break;
+        float d[KP];
+#pragma unroll
+        for (int i = 0; i < KP; i++) d[i] = 0.f;
+        if (issued) {
+            if (!tc_wait(mbar, (ncommit - 1) & 1)) failed = true;
+            if (__syncthreads_or(failed)) {
+                failed = true;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll
+            for (int c8 = 0; c8 < KP / 8; c8++) {
+                float v[8];
+                tc_ld8(taddr + c8 * 8, v);
+#pragma unroll
+                for (int u = 0; u < 8; u++) d[c8 * 8 + u] = v[u];
+            }
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        }
+        if (valid) {
+            const int b = boxes[q];
+            const double lr = log(bs[seg.level[sg]]);
+#pragma unroll
+            for (int i = 0; i < HALF; i++) {
+                if (i < P) {
+                    double re, im;
+                    if (i == 0) {
+                        re = (double)l0x + lr * s0x;
+                        im = (double)l0y + lr * s0y;
+                    } else {
+                        re = d[i];
+                        im = d[HALF + i];
+                    }
+                    loc[(size_t)b * stride + (size_t)i * ndc + c] = make_double2(re, im);
+                }
+            }
+        }
+        // the next tile's MMAs overwrite the accumulator
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+    }
+    if (failed) {
+        if (tid == 0) atomicExch(err, 1);
+        // let MMAs still in flight finish before the memory is released
+        if (ncommit > 0) tc_wait(mbar, (ncommit - 1) & 1);
+    }
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64)
+                     : "memory");
+    }
+}
+
+// B images per (child position, slot): the real form of T (rows = outputs
+// i, K = inputs j), TF32 hi and lo, in the operand layout; cached per
+// device and order.
+float tf32_round_host(float x) {
+    uint32_t u;
+    memcpy(&u, &x, 4);
+    if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x1000u) & 0xffffe000u;
+    float r;
+    memcpy(&r, &u, 4);
+    return r;
+}
+
+// Also returns (t0) row 0 of each matrix, P complex FP32 values per
+// (child position, slot), for the CUDA-core L_0 sum.
+const float *tc_tables(int p, int KP, cudaStream_t s, const float2 **t0out) {
+    static std::mutex mu;
+    static std::vector<std::pair<long, const float *>> cache;
+    static std::vector<std::pair<long, const float2 *>> cache0;
+    int dev;
+    FMM_CUDA(cudaGetDevice(&dev));
+    const long key = ((long)dev << 20) | ((long)p << 8) | KP;
+    std::lock_guard<std::mutex> g(mu);
+    for (size_t e = 0; e < cache.size(); e++)
+        if (cache[e].first == key) {
+            *t0out = cache0[e].second;
+            return cache[e].second;
+        }
+    const int P = p + 1;
+    const SlotTables st = make_slot_tables();
+    std::vector<float2> t0h((size_t)4 * kSlots * P);
+    const int nc = 2 * P + 2;
+    std::vector<double> C((size_t)nc * nc, 0.0);
+    for (int l = 0; l < nc; l++) {
+        C[(size_t)l * nc] = 1.0;
+        for (int m = 1; m <= l; m++)
+            C[(size_t)l * nc + m] =
+                C[(size_t)(l - 1) * nc + m - 1] + (m < l ? C[(size_t)(l - 1) * nc + m] : 0.0);
+    }
+    std::vector<float> h((size_t)4 * kSlots * 2 * KP * KP, 0.f);
+    std::vector<double2> T((size_t)P * P);
+    for (int cp = 0; cp < 4; cp++)
+        for (int k = 0; k < kSlots; k++) {
+            const double tx = st.dx[cp][k], ty = st.dy[cp][k];
+            const double tn = 1.0 / (tx * tx + ty * ty);
+            const double2 w2 = make_double2(tx * tn, -ty * tn), w1 = make_double2(-w2.x, -w2.y);
+            double2 w2i = make_double2(1.0, 0.0);
+            for (int i = 0; i < P; i++) {
+                double2 w1j = make_double2(1.0, 0.0);
+                for (int j = 0; j < P; j++) {
+                    double b;
+                    if (i == 0)
+                        b = j == 0 ? 0.0 : 1.0;
+                    else
+                        b = j == 0 ? -1.0 / i : C[(size_t)(i + j - 1) * nc + (j - 1)];
+                    double2 v = cscal(cmul(w2i, w1j), b);
+                    if (i == 0 && j == 0) v = make_double2(0.5 * std::log(tx * tx + ty * ty), 0.0);
+                    T[(size_t)i * P + j] = v;
+                    w1j = cmul(w1j, w1);
+                }
+                w2i = cmul(w2i, w2);
+            }
+            float *hi = h.data() + ((size_t)cp * kSlots + k) * 2 * KP * KP;
+            float *lo = hi + KP * KP;
+            float2 *t0 = t0h.data() + ((size_t)cp * kSlots + k) * P;
+            for (int j = 0; j < P; j++)
+                t0[j] = make_float2((float)T[j].x, (float)T[j].y);
+            // rows / columns [Re 0..HALF-1 | Im 0..HALF-1], zero beyond p;
+            // row 0 (L_0) is summed on the CUDA cores: rows 0 and HALF stay zero
+            const int HALF = KP / 2;
+            for (int n = 0; n < KP; n++)
+                for (int kk = 0; kk < KP; kk++) {
+                    const int i = n < HALF ? n : n - HALF, j = kk < HALF ? kk : kk - HALF;
+                    if (i == 0 || i >= P || j >= P) continue;
+                    const double2 t = T[(size_t)i * P + j];
+                    double v;
+                    if (n < HALF) v = kk < HALF ? t.x : -t.y;
+                    else v = kk < HALF ? t.y : t.x;
+                    const float f = (float)v;
+                    const float fh = tf32_round_host(f);
+                    const int off = tc_off(n, kk, KP) >> 2;
+                    hi[off] = fh;
+                    lo[off] = tf32_round_host(f - fh);
+                }
+        }
+    float *d = nullptr;
+    float2 *d0 = nullptr;
+    FMM_CUDA(cudaMalloc(&d, h.size() * sizeof(float)));
+    FMM_CUDA(cudaMalloc(&d0, t0h.size() * sizeof(float2)));
+    FMM_CUDA(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+    FMM_CUDA(cudaMemcpyAsync(d0, t0h.data(), t0h.size() * sizeof(float2), cudaMemcpyHostToDevice, s));
+    FMM_CUDA(cudaStreamSynchronize(s));
+    cache.push_back({key, d});
+    cache0.push_back({key, d0});
+    *t0out = d0;
+    return d;
+}
+
 }  // namespace
 
 bool m2l_tensor_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp,
@@ -578,8 +992,11 @@ bool m2l_fp32(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 
               cudaStream_t s) {
     const int L = T.nlevels, p = P.p;
     if (L < 2 || p + 1 > 20) return false;
+    const char *mode = getenv("FMM2D_B200_M2L");
+    const bool simt = mode && !strcmp(mode, "simt");
+    const int CH = P.ndc >= 2 ? 2 : 1;
     M2LWork w;
-    if (!m2l_work(T, P, kFp32Tile, s, w)) return false;
+    if (!m2l_work(T, P, simt ? kFp32Tile : kTcRows / CH, s, w)) return false;
     if (w.ntiles == 0) return true;
     // FP32 copy of the multipoles of levels >= 2
     const int lo = T.lstart[2];
@@ -593,10 +1010,51 @@ bool m2l_fp32(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 
             dst[i] = make_float2((float)src[i].x, (float)src[i].y);
         });
     }
-    if (p + 1 <= 12)
-        launch_fp32<12>(w, T, P, fp32_tables(p, 12, s), mp32.get(), loc, s);
-    else
-        launch_fp32<20>(w, T, P, fp32_tables(p, 20, s), mp32.get(), loc, s);
+    if (simt) {
+        if (p + 1 <= 12)
+            launch_fp32<12>(w, T, P, fp32_tables(p, 12, s), mp32.get(), loc, s);
+        else
+            launch_fp32<20>(w, T, P, fp32_tables(p, 20, s), mp32.get(), loc, s);
+        return true;
+    }
+    // tensor cores: K = N = 2 HALF with HALF = 12 (p < 12) or 20
+    const int HALF = p + 1 <= 12 ? 12 : 20;
+    const int KP = 2 * HALF;
+    const float2 *tab0 = nullptr;
+    const float *tab = tc_tables(p, KP, s, &tab0);
+    const size_t smem = (size_t)(2 * kTcRows * KP + 2 * KP * KP) * sizeof(float);
+    DevBuf<int> err(1, s);
+    err.zero(s);
+    auto launch = [&](auto kern, const M2LWork &ww, int c0) {
+        FMM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const int blocks = std::max(1, std::min(ww.ntiles, kNumSM * 4));
+        kern<<<blocks, kTcRows, smem, s>>>(ww.seg(), (const int *)ww.vals.get(), ww.slots.get(),
+                                           T.d_boxsize.get(), P.ndc, c0, p, tab, tab0,
+                                           mp32.get(), loc, ww.ntiles, err.get());
+        FMM_CHECK_LAUNCH();
+    };
+    int c0 = 0;
+    if (CH == 2) {
+        for (; P.ndc - c0 >= 2; c0 += 2) {
+            if (HALF == 12) launch(m2l_tc_kernel<2, 12>, w, c0);
+            else launch(m2l_tc_kernel<2, 20>, w, c0);
+        }
+    }
+    if (c0 < P.ndc) {
+        // remaining single channels, one channel per row
+        M2LWork w1;
+        const M2LWork *pw = &w;
+        if (CH != 1) {
+            if (!m2l_work(T, P, kTcRows, s, w1)) return false;
+            pw = &w1;
+        }
+        for (; c0 < P.ndc; c0++) {
+            if (HALF == 12) launch(m2l_tc_kernel<1, 12>, *pw, c0);
+            else launch(m2l_tc_kernel<1, 20>, *pw, c0);
+        }
+    }
+    if (read_scalar(err.get(), s) != 0)
+        throw FmmError(4, "tensor-core M2L: a wait for the MMA completion barrier timed out");
     return true;
 }
 

@@ -78,3 +78,33 @@ def test_mixed_variants_match_reference(mlib, family, variant):
     assert ier == 0 and ier2 == 0
     for k in want:
         assert W.rel_err(got[k], want[k]) <= 1e-6, k
+
+
+@pytest.mark.parametrize("fam,nd", [("c", 3), ("l", 2), ("c", 1)])
+@pytest.mark.parametrize("m2l", ["tc", "simt"])
+def test_mixed_multichannel_matches_fp64(mlib, fam, nd, m2l, monkeypatch):
+    """Guru drivers with several densities (odd and even channel counts) in
+    the mixed mode, both M2L paths, against the all-FP64 mode."""
+    import fmm2d_c_translation_b200 as fm
+    monkeypatch.setenv("FMM2D_B200_M2L", m2l)
+    rng = np.random.default_rng(13)
+    ns, nt = 40000, 9000
+    src = rng.random((2, ns))
+    trg = rng.random((2, nt))
+    shp = (nd, ns) if nd > 1 else (ns,)
+    q = rng.standard_normal(shp) + 1j * rng.standard_normal(shp)
+    d = rng.standard_normal(shp) + 1j * rng.standard_normal(shp)
+    kw = dict(eps=1e-6, sources=src, charges=q, dipstr=d, targets=trg, pg=2, pgt=2, nd=nd)
+    f = fm.cfmm2d if fam == "c" else fm.lfmm2d
+    if fam == "l":
+        kw["dipvec"] = rng.standard_normal((nd, 2, ns) if nd > 1 else (2, ns))
+    mixed = f(**kw)
+    mlib.fmm2d_b200_set_precision(1)
+    try:
+        ref = f(**dict(kw, eps=1e-12))
+    finally:
+        mlib.fmm2d_b200_set_precision(2)
+    assert W.rel_err(mixed.gradtarg, ref.gradtarg) < 1e-6
+    assert W.rel_err(mixed.grad, ref.grad) < 1e-6
+    if fam == "l":  # Cauchy potentials carry the branch term of log z
+        assert W.rel_err(mixed.pottarg, ref.pottarg) < 1e-6
