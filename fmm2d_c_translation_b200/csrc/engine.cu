@@ -123,14 +123,18 @@ int leaf_capacity(double eps, int ns, int nt) {
     return ns + nt;
 }
 
-// Leaf capacity of the mixed-precision Laplace / Cauchy evaluation.  That
+// Leaf capacity of the mixed-precision complex-Laplace evaluation.  That
 // mode is held to eps against the direct sum, not to the reference's tree,
 // so its leaf capacity is chosen for speed: FMM2D_B200_MIXED_NDIV, else the
-// tuned value for the order (fmm2d_b200_set_leaf_capacity), else the
-// reference's rule.
+// value set for the order (fmm2d_b200_set_leaf_capacity), else the default
+// measured on a B200 (10^7 + 10^7 uniform points, eps 1e-6: 64 points per
+// leaf against the reference's 15 cut the evaluation by a tenth, the GPU's
+// near field being cheap next to its per-box far field): 64 for orders
+// >= 14, 40 below.
 namespace {
 std::mutex g_ndiv_mu;
 int g_mixed_ndiv[128] = {0};
+bool g_mixed_default_off = false;
 }  // namespace
 
 int mixed_leaf_capacity(int p, int fallback) {
@@ -138,12 +142,16 @@ int mixed_leaf_capacity(int p, int fallback) {
     if (e && atoi(e) > 0) return atoi(e);
     std::lock_guard<std::mutex> g(g_ndiv_mu);
     if (p >= 0 && p < 128 && g_mixed_ndiv[p] > 0) return g_mixed_ndiv[p];
-    return fallback;
+    if (g_mixed_default_off) return fallback;
+    return p >= 14 ? 64 : 40;
 }
 
 void set_mixed_leaf_capacity(int p, int ndiv) {
     std::lock_guard<std::mutex> g(g_ndiv_mu);
     if (p >= 0 && p < 128) g_mixed_ndiv[p] = ndiv > 0 ? ndiv : 0;
+    // ndiv < 0 for every order: back to the reference's rule
+    if (ndiv < 0) g_mixed_default_off = true;
+    if (ndiv > 0) g_mixed_default_off = false;
 }
 
 namespace {
@@ -171,7 +179,10 @@ void run_laplace_family(const FmmCall &c, CallCtx &ctx) {
     const int prec = c.precision;
     const bool mixed = prec == kPrecMixed || (prec == kPrecAuto && c.eps >= 0.5e-6);
     int ndiv = c.ndiv >= 0 ? c.ndiv : leaf_capacity(c.eps, ns, nt);
-    if (c.ndiv < 0 && mixed) ndiv = mixed_leaf_capacity(laplace_nterms(c.eps), ndiv);
+    // (complex-Laplace only: the Cauchy potential's far field takes the
+    // complex q log z, whose branch terms depend on the tree, so the Cauchy
+    // form keeps the reference's tree to reproduce the reference's values)
+    if (c.ndiv < 0 && mixed && lap) ndiv = mixed_leaf_capacity(laplace_nterms(c.eps), ndiv);
     const int idivflag = c.ndiv >= 0 ? c.idivflag : 0;
     Tree T;
     build_tree(src_in.ptr, ns, trg_in.ptr, nt, ndiv, idivflag, kMaxLevels, s, T);

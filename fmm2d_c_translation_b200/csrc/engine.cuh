@@ -54,7 +54,7 @@ int laplace_nterms(double eps);
 // Leaf capacity (lndiv2d.f / hndiv2d.c).
 int leaf_capacity(double eps, int ns, int nt);
 
-// Leaf capacity of the mixed-precision Laplace / Cauchy mode for order p
+// Leaf capacity of the mixed-precision complex-Laplace mode for order p
 // (falls back to `fallback`), and its setter (ndiv <= 0 clears).
 int mixed_leaf_capacity(int p, int fallback);
 void set_mixed_leaf_capacity(int p, int ndiv);

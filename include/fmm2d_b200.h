@@ -661,11 +661,14 @@ int fmm2d_b200_release_memory(void);
  * and leaf capacity (src/laplace/lndiv2d.f:1) for a precision. */
 int fmm2d_b200_laplace_nterms(double eps);
 int fmm2d_b200_leaf_capacity(double eps, int ns, int nt);
-/* Leaf capacity of the mixed-precision Laplace / Cauchy mode (held to eps
- * against the direct sum, not to the reference's tree) for expansion order
- * nterms; ndiv <= 0 restores the reference's rule.  The environment
- * variable FMM2D_B200_MIXED_NDIV overrides both.  The second function
- * returns the capacity a mixed call at eps would use. */
+/* Leaf capacity of the mixed-precision complex-Laplace mode (held to eps
+ * against the direct sum, not to the reference's tree; the Cauchy form keeps
+ * the reference's tree, whose branch terms its potential carries) for order
+ * nterms.  Default: 64 for nterms >= 14, 40 below (measured on a B200).
+ * ndiv = 0 clears a setting for that order; ndiv < 0 selects the
+ * reference's rule (lndiv2d) for the orders without a setting.  The
+ * environment variable FMM2D_B200_MIXED_NDIV overrides all of these.  The
+ * second function returns the capacity a mixed call at eps would use. */
 int fmm2d_b200_set_leaf_capacity(int nterms, int ndiv);
 int fmm2d_b200_mixed_leaf_capacity(double eps, int ns, int nt);
 
