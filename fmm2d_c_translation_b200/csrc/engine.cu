@@ -286,6 +286,7 @@ void run_laplace_family(const FmmCall &c, CallCtx &ctx) {
     P.thresh = T.boxsize[0] * std::ldexp(1.0, -51);
     P.ifnear = c.ifnear;
     P.mixed = mixed;
+    P.real_charge = lap;
     cauchy_fmm(T, P, s);
     // ---- back to input order, in the caller's layout ----
     auto unsort = [&](int n, const int *perm, int pgh, const DevBuf<double2> &po,

@@ -638,7 +638,12 @@ __device__ __forceinline__ float rcp_pair(float x) { return rcp_fast(x); }
 __device__ __forceinline__ double half_ln_pair(double x) { return 0.5 * log(x); }
 __device__ __forceinline__ float half_ln_pair(float x) { return half_ln_fast(x); }
 
-template <int CH, int PGH, bool IFC, bool IFD, bool MIXED>
+// LAPR: the two channels of a complex-Laplace density carry real charges
+// and only the real part of each channel's potential is used
+// (lfmm2d.f:141-157, 168-225), so the charge terms drop their imaginary
+// halves and the potential keeps its real part only.  The results used are
+// the same to the bit.
+template <int CH, int PGH, bool IFC, bool IFD, bool MIXED, bool LAPR>
 __global__ void __launch_bounds__(kP2PWarps * 32) p2p_kernel(
     int lo, int hi, const int *__restrict__ nlist1,
     const int *__restrict__ list1, const int *__restrict__ nchild,
@@ -758,14 +763,30 @@ __global__ void __launch_bounds__(kP2PWarps * 32) p2p_kernel(
                         for (int q = 0; q < CH; q++) {
                             if (IFC) {
                                 const R2 qv = s_str[kk * kStr + q];
-                                po[q].x = fma(rl, qv.x, po[q].x);
-                                po[q].y = fma(rl, qv.y, po[q].y);
-                                if (PGH >= 2) zfma(gr[q], zi, qv);
-                                if (PGH >= 3) zfma(he[q], zscal(zi2, (R)-1), qv);
+                                if (LAPR) {
+                                    po[q].x = fma(rl, qv.x, po[q].x);
+                                    if (PGH >= 2) {
+                                        gr[q].x = fma(zi.x, qv.x, gr[q].x);
+                                        gr[q].y = fma(zi.y, qv.x, gr[q].y);
+                                    }
+                                    if (PGH >= 3) {
+                                        he[q].x = fma(-zi2.x, qv.x, he[q].x);
+                                        he[q].y = fma(-zi2.y, qv.x, he[q].y);
+                                    }
+                                } else {
+                                    po[q].x = fma(rl, qv.x, po[q].x);
+                                    po[q].y = fma(rl, qv.y, po[q].y);
+                                    if (PGH >= 2) zfma(gr[q], zi, qv);
+                                    if (PGH >= 3) zfma(he[q], zscal(zi2, (R)-1), qv);
+                                }
                             }
                             if (IFD) {
                                 const R2 dv = s_str[kk * kStr + (IFC ? CH : 0) + q];
-                                zfma(po[q], zi, dv);
+                                if (LAPR) {
+                                    po[q].x = fma(zi.x, dv.x, fma(-zi.y, dv.y, po[q].x));
+                                } else {
+                                    zfma(po[q], zi, dv);
+                                }
                                 if (PGH >= 2) zfma(gr[q], zscal(zi2, (R)-1), dv);
                                 if (PGH >= 3) zfma(he[q], zscal(zi3, (R)2), dv);
                             }
@@ -823,7 +844,7 @@ int grid_for(int nwarps) {
     return blocks < 1 ? 1 : blocks;
 }
 
-template <int CH, int PGH, bool MIXED>
+template <int CH, int PGH, bool MIXED, bool LAPR>
 void launch_p2p_t(const Tree &T, const CauchyProblem &P, int c0, double th2,
                   int lo, int hi, int leaves, cudaStream_t s) {
     typedef typename Real<MIXED>::T2 R2;
@@ -838,7 +859,7 @@ void launch_p2p_t(const Tree &T, const CauchyProblem &P, int c0, double th2,
 #define FMM_P2P_CASE(IFC, IFD)                                                  \
     do {                                                                        \
         constexpr size_t sm = p2p_smem_bytes<CH, IFC, IFD, MIXED>();            \
-        auto kern = p2p_kernel<CH, PGH, IFC, IFD, MIXED>;                       \
+        auto kern = p2p_kernel<CH, PGH, IFC, IFD, MIXED, LAPR>;                 \
         FMM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); \
         kern<<<g, kP2PWarps * 32, sm, s>>>(lo, hi, n1, l1, nc, leaves, sse,     \
                                           spos, chg, dip, P.sset, P.tset, spos, \
@@ -862,10 +883,15 @@ void launch_p2p(const Tree &T, const CauchyProblem &P, int c0, double th2,
                 int lo, int hi, int leaves, cudaStream_t s) {
     const int pgh = std::max(P.sset.n > 0 ? P.sset.pgh : 0, P.tset.n > 0 ? P.tset.pgh : 0);
 #define FMM_P2P_PGH(PG)                                                         \
-    if (P.mixed)                                                                \
-        launch_p2p_t<CH, PG, true>(T, P, c0, th2, lo, hi, leaves, s);           \
+    if (CH == 2 && P.real_charge) {                                             \
+        if (P.mixed)                                                            \
+            launch_p2p_t<CH, PG, true, true>(T, P, c0, th2, lo, hi, leaves, s); \
+        else                                                                    \
+            launch_p2p_t<CH, PG, false, true>(T, P, c0, th2, lo, hi, leaves, s); \
+    } else if (P.mixed)                                                         \
+        launch_p2p_t<CH, PG, true, false>(T, P, c0, th2, lo, hi, leaves, s);    \
     else                                                                        \
-        launch_p2p_t<CH, PG, false>(T, P, c0, th2, lo, hi, leaves, s);
+        launch_p2p_t<CH, PG, false, false>(T, P, c0, th2, lo, hi, leaves, s);
     switch (pgh) {
         case 1: FMM_P2P_PGH(1) break;
         case 2: FMM_P2P_PGH(2) break;

@@ -31,6 +31,8 @@ struct CauchyProblem {
     double thresh = 0;                // near-field exclusion radius
     int ifnear = 1;
     bool mixed = false;               // FP32 series / pair arithmetic
+    bool real_charge = false;         // complex-Laplace channels (real charges,
+                                      // real part of the potential used)
     const int *sleaf = nullptr;       // leaf of every sorted source (set by cauchy_fmm)
     const int *tleaf = nullptr;       // leaf of every sorted target
     const float2 *charge32 = nullptr; // FP32 strengths (mixed near field)
