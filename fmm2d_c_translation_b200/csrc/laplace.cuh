@@ -63,6 +63,13 @@ bool m2l_tensor_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp,
 bool m2l_fp32(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 *loc,
               cudaStream_t s);
 
+// M2L of the mixed mode over runs of same-row boxes with shifted tensor-core
+// windows (m2l_window.cu), for the target levels whose runs are dense
+// enough; returns the set of target levels it evaluated (bit l = level l),
+// 0 when it does not apply.  A bounded wait that runs out sets *err.
+uint64_t m2l_window_fp32(const Tree &T, const CauchyProblem &P, const float2 *mp32, double2 *loc,
+                         int *err, cudaStream_t s);
+
 // Binomial table C(l, m), l, m <= kLdc, built with the reference's Pascal
 // recurrence (init_carray, src/common/fmmcommon2d.f).
 constexpr int kLdc = 127;

@@ -22,6 +22,7 @@
 // the reference's trees) the caller falls back to the per-box kernel.
 #include "laplace.cuh"
 #include "sort.cuh"
+#include "tc_common.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -274,10 +275,11 @@ void ensure_slot_tables(cudaStream_t s) {
     }
 }
 
-// Builds the segments (tiles of `tile` boxes) and the slot table; false
-// when a list-2 entry falls outside the 27 slots or there are too many
-// segments.
-bool m2l_work(const Tree &T, const CauchyProblem &P, int tile, cudaStream_t s, M2LWork &w) {
+// Builds the segments (tiles of `tile` boxes) and the slot table, leaving
+// out the target levels set in skip_levels; false when a list-2 entry
+// falls outside the 27 slots or there are too many segments.
+bool m2l_work(const Tree &T, const CauchyProblem &P, int tile, cudaStream_t s, M2LWork &w,
+              uint64_t skip_levels = 0) {
     const int L = T.nlevels;
     ensure_slot_tables(s);
     const int lo = T.lstart[2], n = T.nboxes - lo;
@@ -301,7 +303,7 @@ bool m2l_work(const Tree &T, const CauchyProblem &P, int tile, cudaStream_t s, M
         if (tpgh > 0) np += tse[b].y - tse[b].x;
         if (spgh > 0) np += sse[b].y - sse[b].x;
         int key = nseg;
-        if (np > 0) {
+        if (np > 0 && !((skip_levels >> lev[b]) & 1ull)) {
             const int pb = par[b];
             int c = 0;
             for (int j = 0; j < 4; j++)
@@ -310,7 +312,11 @@ bool m2l_work(const Tree &T, const CauchyProblem &P, int tile, cudaStream_t s, M
         }
         kp[i] = (uint32_t)key;
         vp[i] = (uint32_t)b;
-        atomicAdd(&cp[key], 1);
+        // one atomic per group of lanes with the same segment
+        const unsigned am = __activemask();
+        const unsigned peers = __match_any_sync(am, key);
+        if (key < nseg && (int)(threadIdx.x & 31) == __ffs(peers) - 1)
+            atomicAdd(&cp[key], __popc(peers));
     });
     int bits = 1;
     while ((1 << bits) <= nseg) bits++;
@@ -567,77 +573,19 @@ void launch_fp32(const M2LWork &w, const Tree &T, const CauchyProblem &P, const 
 // ---------------------------------------------------------------------------
 constexpr int kTcRows = 128;
 constexpr int kTcMaxKP = 40;
-constexpr long kTcWaitLimit = 1L << 26;
-
-__device__ __forceinline__ uint32_t smem_u32(const void *ptr) {
-    return (uint32_t)__cvta_generic_to_shared(ptr);
-}
-
-// Shared-memory matrix descriptor: start, LBO, SBO (bytes, 16-byte units),
-// descriptor version 1 (bits 46-47), no swizzle.
-__device__ __forceinline__ uint64_t tc_sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-    uint64_t d = (uint64_t)((addr >> 4) & 0x3FFFu);
-    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
-    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
-    d |= (uint64_t)1 << 46;
-    return d;
-}
-
-__device__ __forceinline__ float tc_tf32(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return __uint_as_float(r);
-}
-
-__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc,
-                                       uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
-        :
-        : "r"(d), "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
-        : "memory");
-}
-
-__device__ __forceinline__ void tc_commit(uint32_t mbar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                 :
-                 : "r"(mbar)
-                 : "memory");
-}
+// longest wait for an MMA-completion barrier (the MMAs of one slot take
+// microseconds)
+constexpr uint64_t kTcWaitNs = 2000000000ull;
 
 // Bounded wait for the barrier phase with the given parity.
 __device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity) {
-    for (long it = 0; it < kTcWaitLimit; it++) {
-        uint32_t ok;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(ok)
-            : "r"(mbar), "r"(parity)
-            : "memory");
-        if (ok) return true;
-    }
-    return false;
-}
-
-__device__ __forceinline__ void tc_ld8(uint32_t taddr, float (&v)[8]) {
-    uint32_t r[8];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-          "=r"(r[7])
-        : "r"(taddr));
-#pragma unroll
-    for (int i = 0; i < 8; i++) v[i] = __uint_as_float(r[i]);
+    int never = 0;
+    return mbar_wait_bounded(mbar, parity, &never, kTcWaitNs);
 }
 
 // byte offset of element (row, k) in a K-major no-swizzle operand of
 // `rows` rows
-__host__ __device__ __forceinline__ int tc_off(int row, int k, int rows) {
-    return (((k >> 2) * (rows >> 3) + (row >> 3)) << 7) + ((row & 7) << 4) + ((k & 3) << 2);
-}
+__host__ __device__ __forceinline__ int tc_off(int row, int k, int rows) { return tc_fidx(row, k, rows) << 2; }
 
 template <int CH, int HALF>
 __global__ void __launch_bounds__(kTcRows, 1) m2l_tc_kernel(
@@ -992,12 +940,13 @@ bool m2l_fp32(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 
               cudaStream_t s) {
     const int L = T.nlevels, p = P.p;
     if (L < 2 || p + 1 > 20) return false;
+    // FMM2D_B200_M2L: "simt" = slot tables on the CUDA cores, "tile" =
+    // slot tables on the tensor cores only, default = windows on the
+    // tensor cores for the dense levels and slot tables for the rest
     const char *mode = getenv("FMM2D_B200_M2L");
     const bool simt = mode && !strcmp(mode, "simt");
+    const bool tile_only = mode && !strcmp(mode, "tile");
     const int CH = P.ndc >= 2 ? 2 : 1;
-    M2LWork w;
-    if (!m2l_work(T, P, simt ? kFp32Tile : kTcRows / CH, s, w)) return false;
-    if (w.ntiles == 0) return true;
     // FP32 copy of the multipoles of levels >= 2
     const int lo = T.lstart[2];
     const size_t stride = (size_t)(p + 1) * P.ndc;
@@ -1010,51 +959,55 @@ bool m2l_fp32(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 
             dst[i] = make_float2((float)src[i].x, (float)src[i].y);
         });
     }
-    if (simt) {
+    DevBuf<int> err(1, s);
+    err.zero(s);
+    const uint64_t done =
+        (simt || tile_only) ? 0 : m2l_window_fp32(T, P, mp32.get(), loc, err.get(), s);
+    M2LWork w;
+    if (!m2l_work(T, P, simt ? kFp32Tile : kTcRows / CH, s, w, done)) return false;
+    if (w.ntiles > 0 && simt) {
         if (p + 1 <= 12)
             launch_fp32<12>(w, T, P, fp32_tables(p, 12, s), mp32.get(), loc, s);
         else
             launch_fp32<20>(w, T, P, fp32_tables(p, 20, s), mp32.get(), loc, s);
-        return true;
-    }
-    // tensor cores: K = N = 2 HALF with HALF = 12 (p < 12) or 20
-    const int HALF = p + 1 <= 12 ? 12 : 20;
-    const int KP = 2 * HALF;
-    const float2 *tab0 = nullptr;
-    const float *tab = tc_tables(p, KP, s, &tab0);
-    const size_t smem = (size_t)(2 * kTcRows * KP + 2 * KP * KP) * sizeof(float);
-    DevBuf<int> err(1, s);
-    err.zero(s);
-    auto launch = [&](auto kern, const M2LWork &ww, int c0) {
-        FMM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        const int blocks = std::max(1, std::min(ww.ntiles, kNumSM * 4));
-        kern<<<blocks, kTcRows, smem, s>>>(ww.seg(), (const int *)ww.vals.get(), ww.slots.get(),
-                                           T.d_boxsize.get(), P.ndc, c0, p, tab, tab0,
-                                           mp32.get(), loc, ww.ntiles, err.get());
-        FMM_CHECK_LAUNCH();
-    };
-    int c0 = 0;
-    if (CH == 2) {
-        for (; P.ndc - c0 >= 2; c0 += 2) {
-            if (HALF == 12) launch(m2l_tc_kernel<2, 12>, w, c0);
-            else launch(m2l_tc_kernel<2, 20>, w, c0);
+    } else if (w.ntiles > 0) {
+        // tensor cores: K = N = 2 HALF with HALF = 12 (p < 12) or 20
+        const int HALF = p + 1 <= 12 ? 12 : 20;
+        const int KP = 2 * HALF;
+        const float2 *tab0 = nullptr;
+        const float *tab = tc_tables(p, KP, s, &tab0);
+        const size_t smem = (size_t)(2 * kTcRows * KP + 2 * KP * KP) * sizeof(float);
+        auto launch = [&](auto kern, const M2LWork &ww, int c0) {
+            FMM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            const int blocks = std::max(1, std::min(ww.ntiles, kNumSM * 4));
+            kern<<<blocks, kTcRows, smem, s>>>(ww.seg(), (const int *)ww.vals.get(), ww.slots.get(),
+                                               T.d_boxsize.get(), P.ndc, c0, p, tab, tab0,
+                                               mp32.get(), loc, ww.ntiles, err.get());
+            FMM_CHECK_LAUNCH();
+        };
+        int c0 = 0;
+        if (CH == 2) {
+            for (; P.ndc - c0 >= 2; c0 += 2) {
+                if (HALF == 12) launch(m2l_tc_kernel<2, 12>, w, c0);
+                else launch(m2l_tc_kernel<2, 20>, w, c0);
+            }
         }
-    }
-    if (c0 < P.ndc) {
-        // remaining single channels, one channel per row
-        M2LWork w1;
-        const M2LWork *pw = &w;
-        if (CH != 1) {
-            if (!m2l_work(T, P, kTcRows, s, w1)) return false;
-            pw = &w1;
-        }
-        for (; c0 < P.ndc; c0++) {
-            if (HALF == 12) launch(m2l_tc_kernel<1, 12>, *pw, c0);
-            else launch(m2l_tc_kernel<1, 20>, *pw, c0);
+        if (c0 < P.ndc) {
+            // remaining single channels, one channel per row
+            M2LWork w1;
+            const M2LWork *pw = &w;
+            if (CH != 1) {
+                if (!m2l_work(T, P, kTcRows, s, w1, done)) return false;
+                pw = &w1;
+            }
+            for (; c0 < P.ndc; c0++) {
+                if (HALF == 12) launch(m2l_tc_kernel<1, 12>, *pw, c0);
+                else launch(m2l_tc_kernel<1, 20>, *pw, c0);
+            }
         }
     }
     if (read_scalar(err.get(), s) != 0)
-        throw FmmError(4, "tensor-core M2L: a wait for the MMA completion barrier timed out");
+        throw FmmError(4, "tensor-core M2L: a wait for an MMA or operand barrier timed out");
     return true;
 }
 
