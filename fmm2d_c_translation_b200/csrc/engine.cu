@@ -127,9 +127,9 @@ int leaf_capacity(double eps, int ns, int nt) {
 // mode is held to eps against the direct sum, not to the reference's tree,
 // so its leaf capacity is chosen for speed: FMM2D_B200_MIXED_NDIV, else the
 // value set for the order (fmm2d_b200_set_leaf_capacity), else the default
-// measured on a B200 (10^7 + 10^7 uniform points, eps 1e-6: 64 points per
-// leaf against the reference's 15 cut the evaluation by a tenth, the GPU's
-// near field being cheap next to its per-box far field): 64 for orders
+// measured on a B200 (10^7 + 10^7 uniform points, eps 1e-6, windowed
+// tensor-core M2L: 24 points per leaf 26.6 ms, 16 27.1 ms, 64 28.1 ms, 32
+// and 40 slower still, their leaves straddling two levels): 24 for orders
 // >= 14, 40 below.
 namespace {
 std::mutex g_ndiv_mu;
@@ -143,7 +143,7 @@ int mixed_leaf_capacity(int p, int fallback) {
     std::lock_guard<std::mutex> g(g_ndiv_mu);
     if (p >= 0 && p < 128 && g_mixed_ndiv[p] > 0) return g_mixed_ndiv[p];
     if (g_mixed_default_off) return fallback;
-    return p >= 14 ? 64 : 40;
+    return p >= 14 ? 24 : 40;
 }
 
 void set_mixed_leaf_capacity(int p, int ndiv) {

@@ -1160,237 +1160,291 @@ const double2 *shift_tables(int p, bool m2m, cudaStream_t s) {
     return d;
 }
 
+
 // ---------------------------------------------------------------------------
-// Box-thread forms of P2M, P2L, M2M and L2L for orders p < P1 (P1 <= 20):
-// one thread per box keeps all p + 1 coefficients of CH channels in
-// registers, so each source's powers are built once by recurrence and each
-// child / parent coefficient is loaded once.  Same formulas as the
-// coefficient-thread kernels above; FP64 throughout.
+// M2M and L2L as Pascal-triangle passes, without shift matrices.  With the
+// child center at c_parent + d r_parent, d = (+-1 +- i) / 4, the entries of
+// the scaled shifts (the matrices of shift_tables above) give
+//   L2L: L'_i = 2^-i sum_{j>=i} C(j, i) d^(j-i) L_j
+//        = 2^-i d^-i e_i,  e_j = d^j L_j after the passes e_j += e_(j+1)
+//   M2M: M_i = d^i (sum_{j=1..i} C(i-1, j-1) (2d)^-j M'_j - M'_0 / i),
+//        the sum being f_i after the passes f_m += f_(m-1), f_j = (2d)^-j M'_j
+// so each (box, channel) costs p^2 / 2 complex additions and O(p) complex
+// products, all in registers.  L2L takes one thread per (child, channel);
+// M2M one per (parent, channel, child), the four children's parts summed
+// over adjacent lanes with shuffles.  FP64 throughout.
 // ---------------------------------------------------------------------------
-template <int P1, int CH>
-__global__ void __launch_bounds__(128) p2m_box_kernel(
+__device__ __forceinline__ double2 child_offset(int cs) {
+    return make_double2((cs & 1) ? 0.25 : -0.25, (cs & 2) ? 0.25 : -0.25);
+}
+
+template <int PMAX>
+__global__ void __launch_bounds__(128) l2l_pascal_kernel(
+    int lo, int hi, int p, EvalCounts ec, const int *__restrict__ parent,
+    const int *__restrict__ child, int ndc, int c0, int nch, double2 *__restrict__ loc) {
+    const int stride = (p + 1) * ndc;
+    const int64_t total = (int64_t)(hi - lo) * nch;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int b = lo + (int)(t / nch), q = c0 + (int)(t % nch);
+        const int pb = parent[b];
+        if (ec.npts(pb) <= 0) continue;
+        const double2 d = child_offset(child_pos(child, pb, b));
+        const double2 *Lp = loc + (size_t)pb * stride + q;
+        double2 e[PMAX];
+        double2 w = make_double2(1.0, 0.0);
+#pragma unroll
+        for (int j = 0; j < PMAX; j++) {
+            e[j] = j <= p ? cmul(w, Lp[(size_t)j * ndc]) : make_double2(0.0, 0.0);
+            w = cmul(w, d);
+        }
+#pragma unroll
+        for (int k = 0; k < PMAX - 1; k++)
+#pragma unroll
+            for (int j = PMAX - 2; j >= k; j--) e[j] = cadd(e[j], e[j + 1]);
+        // (d / 2)^-i
+        const double2 h = cinv(cscal(d, 2.0));
+        double2 v = make_double2(1.0, 0.0);
+        double2 *Lc = loc + (size_t)b * stride + q;
+#pragma unroll
+        for (int i = 0; i < PMAX; i++) {
+            if (i > p) break;
+            Lc[(size_t)i * ndc] = cadd(Lc[(size_t)i * ndc], cmul(v, e[i]));
+            v = cmul(v, h);
+        }
+    }
+}
+
+template <int PMAX>
+__global__ void __launch_bounds__(128) m2m_pascal_kernel(
+    int lo, int hi, int p, const int *__restrict__ nchild, const int *__restrict__ child,
+    const int2 *__restrict__ sse, int ndc, int c0, int nch, double2 *__restrict__ mp) {
+    const int stride = (p + 1) * ndc;
+    const int64_t total = (int64_t)(hi - lo) * nch * 4;
+    // warp-uniform trip count: the lanes of a parent meet in the shuffles
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < total;
+         base += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t t = base + threadIdx.x;
+        const bool valid = t < total;
+        const int64_t tt = valid ? t : 0;
+        const int b = lo + (int)(tt / (4 * nch));
+        const int q = c0 + (int)((tt / 4) % nch), cs = (int)(tt % 4);
+        const bool par = valid && nchild[b] > 0;
+        const double2 d = child_offset(cs);
+        double2 f[PMAX];
+#pragma unroll
+        for (int j = 0; j < PMAX; j++) f[j] = make_double2(0.0, 0.0);
+        double2 a0 = make_double2(0.0, 0.0);
+        const int cb = par ? child[4 * b + cs] : -1;
+        if (cb >= 0 && count(sse, cb) > 0) {
+            const double2 *M = mp + (size_t)cb * stride + q;
+            a0 = M[0];
+            // f_j = (2d)^-j M'_j
+            const double2 r2 = cinv(cscal(d, 2.0));
+            double2 w = r2;
+#pragma unroll
+            for (int j = 1; j < PMAX; j++) {
+                if (j <= p) f[j] = cmul(w, M[(size_t)j * ndc]);
+                w = cmul(w, r2);
+            }
+        }
+#pragma unroll
+        for (int k = 1; k < PMAX - 1; k++)
+#pragma unroll
+            for (int m = PMAX - 1; m > k; m--) f[m] = cadd(f[m], f[m - 1]);
+        // M_i = d^i (f_i - a0 / i), M_0 = a0; summed over the four children
+        double2 w = d;
+        f[0] = a0;
+#pragma unroll
+        for (int i = 1; i < PMAX; i++) {
+            f[i] = cmul(w, csub(f[i], cscal(a0, 1.0 / i)));
+            w = cmul(w, d);
+        }
+#pragma unroll
+        for (int i = 0; i < PMAX; i++) {
+            if (i > p) break;
+            double2 v = f[i];
+            v.x += __shfl_xor_sync(0xffffffffu, v.x, 1);
+            v.y += __shfl_xor_sync(0xffffffffu, v.y, 1);
+            v.x += __shfl_xor_sync(0xffffffffu, v.x, 2);
+            v.y += __shfl_xor_sync(0xffffffffu, v.y, 2);
+            if (par && cs == 0) mp[(size_t)b * stride + (size_t)i * ndc + q] = v;
+        }
+    }
+}
+
+inline int pascal_grid(int64_t nthreads) {
+    return (int)std::max<int64_t>(1, std::min<int64_t>((nthreads + 127) / 128, kNumSM * 16));
+}
+
+// ---------------------------------------------------------------------------
+// P2M (leaves of levels >= 2 with sources) and P2L (list 4) with one warp
+// per box.  Sources go in chunks of kPowSrc: the chunk's lanes build each
+// source's powers b^k (b = (x - c) / r for P2M, r / (x - c) for P2L) by
+// the same recurrence as the per-box form and stage them with the
+// strengths; then lane k sums coefficient k over the chunk.  P2M stores the
+// multipoles (their first writer), P2L adds to the locals.
+//   P2M: M_0 += q,  M_k += -q z^k / k + (d / r) z^(k-1)
+//   P2L: L_0 += q log|z0| - d / z0,  L_k += -q w^k / k - (d / z0) w^k
+// ---------------------------------------------------------------------------
+constexpr int kPowSrc = 16;
+constexpr int kPowWarps = 8;
+
+inline size_t pow_warp_smem(int p, int CH) {
+    // per warp: powers [kPowSrc][P], strengths [kPowSrc][2 CH], log|z0| [kPowSrc]
+    return (size_t)kPowWarps * ((size_t)kPowSrc * (p + 1 + 2 * CH) * sizeof(double2) +
+                                (size_t)kPowSrc * sizeof(double));
+}
+
+template <int CH, bool P2L>
+__device__ __forceinline__ void pow_warp_box(int b, int p, int lane, double2 *sPw, double2 *sSt,
+                                             double *sLz, const double2 c, const double r,
+                                             const int2 *rgs, int nrg,
+                                             const double2 *__restrict__ src,
+                                             const double2 *__restrict__ chg,
+                                             const double2 *__restrict__ dip, int ifc, int ifd,
+                                             int ndc, int c0, double2 (&acc)[2][CH]) {
+    const int P = p + 1;
+    for (int g = 0; g < nrg; g++) {
+        const int2 rg = rgs[g];
+        for (int j0 = rg.x; j0 < rg.y; j0 += kPowSrc) {
+            const int n = min(kPowSrc, rg.y - j0);
+            __syncwarp();
+            if (lane < n) {
+                const int j = j0 + lane;
+                const double2 x = src[j];
+                double2 base;
+                double2 dv[CH];
+                if (P2L) {
+                    const double2 z0 = make_double2(x.x - c.x, x.y - c.y);
+                    const double2 zi = cinv(z0);
+                    base = cscal(zi, r);  // r / z0
+                    sLz[lane] = 0.5 * log(z0.x * z0.x + z0.y * z0.y);
+#pragma unroll
+                    for (int q = 0; q < CH; q++)
+                        dv[q] = ifd ? cscal(cmul(dip[(size_t)j * ndc + c0 + q], zi), -1.0)
+                                    : make_double2(0.0, 0.0);
+                } else {
+                    base = make_double2((x.x - c.x) / r, (x.y - c.y) / r);
+                    const double rinv = 1.0 / r;
+#pragma unroll
+                    for (int q = 0; q < CH; q++)
+                        dv[q] = ifd ? cscal(dip[(size_t)j * ndc + c0 + q], rinv) : make_double2(0.0, 0.0);
+                }
+#pragma unroll
+                for (int q = 0; q < CH; q++) {
+                    sSt[lane * 2 * CH + q] = ifc ? chg[(size_t)j * ndc + c0 + q] : make_double2(0.0, 0.0);
+                    sSt[lane * 2 * CH + CH + q] = dv[q];
+                }
+                double2 w = make_double2(1.0, 0.0);
+                for (int k = 0; k < P; k++) {
+                    sPw[lane * P + k] = w;
+                    w = cmul(w, base);
+                }
+            }
+            __syncwarp();
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int k = lane + 32 * h;
+                if (k >= P) break;
+                const double ik = k > 0 ? -1.0 / k : 0.0;
+                for (int s = 0; s < n; s++) {
+                    const double2 pk = sPw[s * P + k];
+                    // P2M: the dipole term takes z^(k-1); P2L takes w^k
+                    const double2 pd = P2L ? pk : (k > 0 ? sPw[s * P + k - 1] : make_double2(0.0, 0.0));
+                    const double lz = P2L ? sLz[s] : 0.0;
+#pragma unroll
+                    for (int q = 0; q < CH; q++) {
+                        const double2 qv = sSt[s * 2 * CH + q], dv = sSt[s * 2 * CH + CH + q];
+                        if (k == 0)
+                            acc[h][q] = cadd(acc[h][q], P2L ? cscal(qv, lz) : qv);
+                        else
+                            cfma(acc[h][q], qv, cscal(pk, ik));
+                        cfma(acc[h][q], dv, pd);
+                    }
+                }
+            }
+        }
+    }
+}
+
+template <int CH>
+__global__ void __launch_bounds__(kPowWarps * 32) p2m_warp_kernel(
     int lo, int hi, int p, const int *__restrict__ nchild, const double2 *__restrict__ centers,
     const int *__restrict__ level, const double *__restrict__ bs, const int2 *__restrict__ sse,
     const double2 *__restrict__ src, const double2 *__restrict__ chg,
     const double2 *__restrict__ dip, int ifc, int ifd, int ndc, int c0,
     double2 *__restrict__ mp) {
-    const int stride = (p + 1) * ndc;
-    for (int b = lo + blockIdx.x * blockDim.x + threadIdx.x; b < hi;
-         b += gridDim.x * blockDim.x) {
+    extern __shared__ double2 pow_smem[];
+    const int P = p + 1, stride = P * ndc;
+    const int lane = lane_id(), wib = threadIdx.x >> 5;
+    double2 *sPw = pow_smem + (size_t)wib * kPowSrc * (P + 2 * CH);
+    double2 *sSt = sPw + kPowSrc * P;
+    double *sLz = reinterpret_cast<double *>(pow_smem + (size_t)kPowWarps * kPowSrc * (P + 2 * CH)) +
+                  wib * kPowSrc;
+    for (int b = lo + warp_global(); b < hi; b += warp_count()) {
         if (nchild[b] != 0) continue;
         const int2 rg = sse[b];
         if (rg.y <= rg.x) continue;
-        const double2 c = centers[b];
-        const double r = bs[level[b]], rinv = 1.0 / r;
-        double2 acc[CH][P1];
+        double2 acc[2][CH];
 #pragma unroll
-        for (int q = 0; q < CH; q++)
+        for (int h = 0; h < 2; h++)
 #pragma unroll
-            for (int k = 0; k < P1; k++) acc[q][k] = make_double2(0.0, 0.0);
-        for (int j = rg.x; j < rg.y; j++) {
-            const double2 x = src[j];
-            const double2 z = make_double2((x.x - c.x) / r, (x.y - c.y) / r);
-            double2 qv[CH], dv[CH];
+            for (int q = 0; q < CH; q++) acc[h][q] = make_double2(0.0, 0.0);
+        pow_warp_box<CH, false>(b, p, lane, sPw, sSt, sLz, centers[b], bs[level[b]], &rg, 1, src,
+                                chg, dip, ifc, ifd, ndc, c0, acc);
 #pragma unroll
-            for (int q = 0; q < CH; q++) {
-                qv[q] = ifc ? chg[(size_t)j * ndc + c0 + q] : make_double2(0.0, 0.0);
-                dv[q] = ifd ? cscal(dip[(size_t)j * ndc + c0 + q], rinv) : make_double2(0.0, 0.0);
-            }
+        for (int h = 0; h < 2; h++) {
+            const int k = lane + 32 * h;
+            if (k >= P) break;
 #pragma unroll
-            for (int q = 0; q < CH; q++) acc[q][0] = cadd(acc[q][0], qv[q]);
-            double2 zk1 = make_double2(1.0, 0.0);  // z^(k-1)
-#pragma unroll
-            for (int k = 1; k < P1; k++) {
-                if (k > p) break;
-                const double2 zk = cmul(zk1, z);
-                const double2 cz = cscal(zk, -1.0 / k);
-#pragma unroll
-                for (int q = 0; q < CH; q++) {
-                    cfma(acc[q][k], qv[q], cz);
-                    cfma(acc[q][k], dv[q], zk1);
-                }
-                zk1 = zk;
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < P1; k++) {
-            if (k > p) break;
-#pragma unroll
-            for (int q = 0; q < CH; q++) mp[(size_t)b * stride + (size_t)k * ndc + c0 + q] = acc[q][k];
+            for (int q = 0; q < CH; q++) mp[(size_t)b * stride + (size_t)k * ndc + c0 + q] = acc[h][q];
         }
     }
 }
 
-template <int P1, int CH>
-__global__ void __launch_bounds__(128) p2l_box_kernel(
+template <int CH>
+__global__ void __launch_bounds__(kPowWarps * 32) p2l_warp_kernel(
     int lo, int hi, int p, EvalCounts ec, const int *__restrict__ nlist4,
     const int *__restrict__ list4, const double2 *__restrict__ centers,
     const int *__restrict__ level, const double *__restrict__ bs,
     const double2 *__restrict__ src, const double2 *__restrict__ chg,
     const double2 *__restrict__ dip, int ifc, int ifd, int ndc, int c0,
     double2 *__restrict__ loc) {
-    const int stride = (p + 1) * ndc;
-    for (int b = lo + blockIdx.x * blockDim.x + threadIdx.x; b < hi;
-         b += gridDim.x * blockDim.x) {
+    extern __shared__ double2 pow_smem[];
+    const int P = p + 1, stride = P * ndc;
+    const int lane = lane_id(), wib = threadIdx.x >> 5;
+    double2 *sPw = pow_smem + (size_t)wib * kPowSrc * (P + 2 * CH);
+    double2 *sSt = sPw + kPowSrc * P;
+    double *sLz = reinterpret_cast<double *>(pow_smem + (size_t)kPowWarps * kPowSrc * (P + 2 * CH)) +
+                  wib * kPowSrc;
+    for (int b = lo + warp_global(); b < hi; b += warp_count()) {
         const int n4 = nlist4[b];
         if (n4 == 0 || ec.npts(b) <= 0) continue;
-        const double2 c = centers[b];
-        const double r = bs[level[b]];
-        double2 acc[CH][P1];
+        int2 rgs[kMaxList4];
+        for (int e = 0; e < n4; e++) rgs[e] = ec.sse[list4[kMaxList4 * b + e]];
+        double2 acc[2][CH];
 #pragma unroll
-        for (int q = 0; q < CH; q++)
+        for (int h = 0; h < 2; h++)
 #pragma unroll
-            for (int k = 0; k < P1; k++) acc[q][k] = make_double2(0.0, 0.0);
-        for (int e = 0; e < n4; e++) {
-            const int2 rg = ec.sse[list4[kMaxList4 * b + e]];
-            for (int j = rg.x; j < rg.y; j++) {
-                const double2 x = src[j];
-                const double2 z0 = make_double2(x.x - c.x, x.y - c.y);
-                const double2 zi = cinv(z0);
-                const double2 w = cscal(zi, r);  // r / z0
-                const double lz = 0.5 * log(z0.x * z0.x + z0.y * z0.y);
-                double2 qv[CH], dv[CH];
+            for (int q = 0; q < CH; q++) acc[h][q] = make_double2(0.0, 0.0);
+        pow_warp_box<CH, true>(b, p, lane, sPw, sSt, sLz, centers[b], bs[level[b]], rgs, n4, src,
+                               chg, dip, ifc, ifd, ndc, c0, acc);
 #pragma unroll
-                for (int q = 0; q < CH; q++) {
-                    qv[q] = ifc ? chg[(size_t)j * ndc + c0 + q] : make_double2(0.0, 0.0);
-                    // -d / z0
-                    dv[q] = ifd ? cscal(cmul(dip[(size_t)j * ndc + c0 + q], zi), -1.0)
-                                : make_double2(0.0, 0.0);
-                }
-                double2 wk = make_double2(1.0, 0.0);
-#pragma unroll
-                for (int k = 0; k < P1; k++) {
-                    if (k > p) break;
-#pragma unroll
-                    for (int q = 0; q < CH; q++) {
-                        if (k == 0)
-                            cfma(acc[q][0], qv[q], make_double2(lz, 0.0));
-                        else
-                            cfma(acc[q][k], qv[q], cscal(wk, -1.0 / k));
-                        cfma(acc[q][k], dv[q], wk);
-                    }
-                    wk = cmul(wk, w);
-                }
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < P1; k++) {
-            if (k > p) break;
+        for (int h = 0; h < 2; h++) {
+            const int k = lane + 32 * h;
+            if (k >= P) break;
 #pragma unroll
             for (int q = 0; q < CH; q++) {
                 double2 &o = loc[(size_t)b * stride + (size_t)k * ndc + c0 + q];
-                o = cadd(o, acc[q][k]);
+                o = cadd(o, acc[h][q]);
             }
         }
     }
 }
 
-// M2M: parent i = sum over children with sources of sum_{j <= i}
-// A[cpos][i][j] M_j (A staged in shared memory, read as broadcasts).
-template <int P1, int CH>
-__global__ void __launch_bounds__(128) m2m_box_kernel(
-    int lo, int hi, int p, const int *__restrict__ nchild, const int *__restrict__ child,
-    const int2 *__restrict__ sse, const double2 *__restrict__ A, int ndc, int c0,
-    double2 *__restrict__ mp) {
-    __shared__ double2 sA[4 * P1 * P1];
-    const int np1 = p + 1;
-    for (int e = threadIdx.x; e < 4 * P1 * P1; e += blockDim.x) {
-        const int cp = e / (P1 * P1), i = (e / P1) % P1, j = e % P1;
-        sA[e] = (i <= p && j <= p) ? A[((size_t)cp * np1 + i) * np1 + j] : make_double2(0.0, 0.0);
-    }
-    __syncthreads();
-    const int stride = np1 * ndc;
-    for (int b = lo + blockIdx.x * blockDim.x + threadIdx.x; b < hi;
-         b += gridDim.x * blockDim.x) {
-        if (nchild[b] == 0) continue;
-        double2 acc[CH][P1];
-#pragma unroll
-        for (int q = 0; q < CH; q++)
-#pragma unroll
-            for (int i = 0; i < P1; i++) acc[q][i] = make_double2(0.0, 0.0);
-        for (int cs = 0; cs < 4; cs++) {
-            const int cb = child[4 * b + cs];
-            if (count(sse, cb) <= 0) continue;
-            const double2 *M = mp + (size_t)cb * stride + c0;
-            const double2 *Ac = sA + cs * P1 * P1;
-#pragma unroll
-            for (int j = 0; j < P1; j++) {
-                if (j > p) break;
-                double2 m[CH];
-#pragma unroll
-                for (int q = 0; q < CH; q++) m[q] = M[(size_t)j * ndc + q];
-#pragma unroll
-                for (int i = j; i < P1; i++) {
-                    const double2 a = Ac[i * P1 + j];
-#pragma unroll
-                    for (int q = 0; q < CH; q++) cfma(acc[q][i], a, m[q]);
-                }
-            }
-        }
-#pragma unroll
-        for (int i = 0; i < P1; i++) {
-            if (i > p) break;
-#pragma unroll
-            for (int q = 0; q < CH; q++) mp[(size_t)b * stride + (size_t)i * ndc + c0 + q] = acc[q][i];
-        }
-    }
-}
-
-// L2L: child i += sum_{j >= i} A[cpos][i][j] Lp_j for the children of
-// parents that hold points.
-template <int P1, int CH>
-__global__ void __launch_bounds__(128) l2l_box_kernel(
-    int lo, int hi, int p, EvalCounts ec, const int *__restrict__ parent,
-    const int *__restrict__ child, const double2 *__restrict__ A, int ndc, int c0,
-    double2 *__restrict__ loc) {
-    __shared__ double2 sA[4 * P1 * P1];
-    const int np1 = p + 1;
-    for (int e = threadIdx.x; e < 4 * P1 * P1; e += blockDim.x) {
-        const int cp = e / (P1 * P1), i = (e / P1) % P1, j = e % P1;
-        sA[e] = (i <= p && j <= p) ? A[((size_t)cp * np1 + i) * np1 + j] : make_double2(0.0, 0.0);
-    }
-    __syncthreads();
-    const int stride = np1 * ndc;
-    for (int b = lo + blockIdx.x * blockDim.x + threadIdx.x; b < hi;
-         b += gridDim.x * blockDim.x) {
-        const int pb = parent[b];
-        if (ec.npts(pb) <= 0) continue;
-        const int cs = child_pos(child, pb, b);
-        const double2 *Lp = loc + (size_t)pb * stride + c0;
-        const double2 *Ac = sA + cs * P1 * P1;
-        double2 acc[CH][P1];
-#pragma unroll
-        for (int q = 0; q < CH; q++)
-#pragma unroll
-            for (int i = 0; i < P1; i++) acc[q][i] = make_double2(0.0, 0.0);
-#pragma unroll
-        for (int j = 0; j < P1; j++) {
-            if (j > p) break;
-            double2 l[CH];
-#pragma unroll
-            for (int q = 0; q < CH; q++) l[q] = Lp[(size_t)j * ndc + q];
-#pragma unroll
-            for (int i = 0; i <= j; i++) {
-                const double2 a = Ac[i * P1 + j];
-#pragma unroll
-                for (int q = 0; q < CH; q++) cfma(acc[q][i], a, l[q]);
-            }
-        }
-#pragma unroll
-        for (int i = 0; i < P1; i++) {
-            if (i > p) break;
-#pragma unroll
-            for (int q = 0; q < CH; q++) {
-                double2 &o = loc[(size_t)b * stride + (size_t)i * ndc + c0 + q];
-                o = cadd(o, acc[q][i]);
-            }
-        }
-    }
-}
-
-
-inline int box_blocks(int nbox) {
-    return std::max(1, std::min((nbox + 127) / 128, kNumSM * 16));
+inline int pow_grid(int nbox) {
+    return std::max(1, std::min((nbox + kPowWarps - 1) / kPowWarps, kNumSM * 8));
 }
 
 // Upward pass for channels [c0, c0 + CH): P2M at the leaves of levels >= 2,
@@ -1405,15 +1459,19 @@ void upward_chunk(const Tree &T, const CauchyProblem &P, int c0,
         const int64_t n = (int64_t)nbox * (p + 1);
         return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, kNumSM * 8));
     };
-    const bool boxk = p + 1 <= 20;
+    // warp-per-box kernels while their shared tables fit (p + 1 <= 40)
+    const bool warpk = p + 1 <= 40;
     if (L >= 2) {
         const int lo = T.lstart[2];
-        if (boxk)
-            p2m_box_kernel<20, CH><<<box_blocks(nb - lo), 128, 0, s>>>(
+        if (warpk) {
+            const size_t sm = pow_warp_smem(p, CH);
+            FMM_CUDA(cudaFuncSetAttribute(p2m_warp_kernel<CH>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            p2m_warp_kernel<CH><<<pow_grid(nb - lo), kPowWarps * 32, sm, s>>>(
                 lo, nb, p, T.nchild.get(), T.centers.get(), T.level.get(), bs,
                 T.srcse.get(), P.src, P.charge, P.dipstr, P.ifcharge, P.ifdipole,
                 P.ndc, c0, mp);
-        else
+        } else
             p2m_coef_kernel<CH><<<blocks(nb - lo), 256, 0, s>>>(
                 lo, nb, p, T.nchild.get(), T.centers.get(), T.level.get(), bs,
                 T.srcse.get(), P.src, P.charge, P.dipstr, P.ifcharge, P.ifdipole,
@@ -1424,9 +1482,13 @@ void upward_chunk(const Tree &T, const CauchyProblem &P, int c0,
     const double2 *A = shift_tables(p, true, s);
     for (int l = L - 1; l >= 1; l--) {
         const int lo = T.lstart[l], hi = T.lend[l];
-        if (boxk)
-            m2m_box_kernel<20, CH><<<box_blocks(hi - lo), 128, 0, s>>>(
-                lo, hi, p, T.nchild.get(), T.child.get(), T.srcse.get(), A, P.ndc, c0, mp);
+        const int64_t nt = (int64_t)(hi - lo) * CH * 4;
+        if (p + 1 <= 20)
+            m2m_pascal_kernel<20><<<pascal_grid(nt), 128, 0, s>>>(
+                lo, hi, p, T.nchild.get(), T.child.get(), T.srcse.get(), P.ndc, c0, CH, mp);
+        else if (p + 1 <= 40)
+            m2m_pascal_kernel<40><<<pascal_grid(nt), 128, 0, s>>>(
+                lo, hi, p, T.nchild.get(), T.child.get(), T.srcse.get(), P.ndc, c0, CH, mp);
         else
             m2m_coef_kernel<CH><<<blocks(hi - lo), 256, 0, s>>>(
                 lo, hi, p, T.nchild.get(), T.child.get(), T.srcse.get(), A, P.ndc,
@@ -1473,15 +1535,18 @@ void downward_chunk(const Tree &T, const CauchyProblem &P, int c0,
         return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, kNumSM * 8));
     };
     // step 2: P2L from list 4 (after M2L, which initialises the locals)
-    const bool boxk = p + 1 <= 20;
+    const bool warpk = p + 1 <= 40;
     if (L >= 2) {
         const int lo = T.lstart[2];
-        if (boxk)
-            p2l_box_kernel<20, CH><<<box_blocks(nb - lo), 128, 0, s>>>(
+        if (warpk) {
+            const size_t sm = pow_warp_smem(p, CH);
+            FMM_CUDA(cudaFuncSetAttribute(p2l_warp_kernel<CH>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            p2l_warp_kernel<CH><<<pow_grid(nb - lo), kPowWarps * 32, sm, s>>>(
                 lo, nb, p, ec, T.nlist4.get(), T.list4.get(), T.centers.get(),
                 T.level.get(), bs, P.src, P.charge, P.dipstr, P.ifcharge,
                 P.ifdipole, P.ndc, c0, loc);
-        else
+        } else
             p2l_coef_kernel<CH><<<blocks(nb - lo), 256, 0, s>>>(
                 lo, nb, p, ec, T.nlist4.get(), T.list4.get(), T.centers.get(),
                 T.level.get(), bs, P.src, P.charge, P.dipstr, P.ifcharge,
@@ -1493,9 +1558,13 @@ void downward_chunk(const Tree &T, const CauchyProblem &P, int c0,
     const double2 *A = shift_tables(p, false, s);
     for (int l = 1; l <= L - 1; l++) {
         const int lo = T.lstart[l + 1], hi = T.lend[l + 1];
-        if (boxk)
-            l2l_box_kernel<20, CH><<<box_blocks(hi - lo), 128, 0, s>>>(
-                lo, hi, p, ec, T.parent.get(), T.child.get(), A, P.ndc, c0, loc);
+        const int64_t nt = (int64_t)(hi - lo) * CH;
+        if (p + 1 <= 20)
+            l2l_pascal_kernel<20><<<pascal_grid(nt), 128, 0, s>>>(
+                lo, hi, p, ec, T.parent.get(), T.child.get(), P.ndc, c0, CH, loc);
+        else if (p + 1 <= 40)
+            l2l_pascal_kernel<40><<<pascal_grid(nt), 128, 0, s>>>(
+                lo, hi, p, ec, T.parent.get(), T.child.get(), P.ndc, c0, CH, loc);
         else
             l2l_coef_kernel<CH><<<blocks(hi - lo), 256, 0, s>>>(
                 lo, hi, p, ec, T.parent.get(), T.child.get(), A, P.ndc, c0, loc);

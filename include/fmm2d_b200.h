@@ -664,7 +664,7 @@ int fmm2d_b200_leaf_capacity(double eps, int ns, int nt);
 /* Leaf capacity of the mixed-precision complex-Laplace mode (held to eps
  * against the direct sum, not to the reference's tree; the Cauchy form keeps
  * the reference's tree, whose branch terms its potential carries) for order
- * nterms.  Default: 64 for nterms >= 14, 40 below (measured on a B200).
+ * nterms.  Default: 24 for nterms >= 14, 40 below (measured on a B200).
  * ndiv = 0 clears a setting for that order; ndiv < 0 selects the
  * reference's rule (lndiv2d) for the orders without a setting.  The
  * environment variable FMM2D_B200_MIXED_NDIV overrides all of these.  The
