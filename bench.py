@@ -492,7 +492,10 @@ def main():
     serving = None
     if args.serve_requests > 0:
         L.fmm2d_b200_reset_stream()
-        serving = measure_serving(fm, args)
+        try:
+            serving = measure_serving(fm, args)
+        except RuntimeError as e:
+            serving = {"error": str(e)}
 
     cpu = None
     if not args.no_cpu_baseline and ws == 1:
@@ -553,13 +556,14 @@ def measure_serving(fm, args):
         lat = [None] * len(stream)
         tickets = [None] * len(stream)
         done = threading.Semaphore(0)
+        failed = []
 
         def waiter():
             for i in range(len(stream)):
                 done.acquire()
                 ier, tms = srv.wait(tickets[i])
                 if ier != 0:
-                    raise RuntimeError("serving request failed: " + fm.last_error())
+                    failed.append((i, ier, fm.last_error()))
                 lat[i] = tms[2]
 
         th = threading.Thread(target=waiter)
@@ -578,6 +582,10 @@ def measure_serving(fm, args):
         wall = time.perf_counter() - t0
         st = srv.stats()
         srv.close()
+        if failed:
+            i, ier, msg = failed[0]
+            raise RuntimeError(f"{len(failed)} serving requests failed; request {i}: "
+                               f"ier={ier} {msg}")
         return wall, lat, sum(r["n"] for r in stream), st
 
     # warm the pool and the code paths

@@ -2,6 +2,7 @@
 #include "common.cuh"
 
 #include <atomic>
+#include <map>
 #include <mutex>
 
 namespace fmm2d {
@@ -167,6 +168,18 @@ std::string prof_report() {
     std::string out;
     for (auto &r : g_prof.result) out += r.first + "=" + std::to_string(r.second) + ";";
     return out;
+}
+
+void raise_smem_limit(const void *func, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void *>, size_t> set;
+    int dev = 0;
+    FMM_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> g(mu);
+    size_t &cur = set[{dev, func}];
+    if (cur >= bytes) return;
+    FMM_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    cur = bytes;
 }
 
 void set_last_error(const std::string &msg) {

@@ -43,6 +43,17 @@ void set_last_error(const std::string &msg);
         }                                                                     \
     } while (0)
 
+// Raises the dynamic shared-memory limit of `func` on the current device to
+// at least `bytes`.  The limit only ever grows: the request loop's worker
+// threads launch the same kernel with different sizes at the same time, and
+// lowering it between another thread's check and launch would fail that
+// launch with an invalid-argument error.
+void raise_smem_limit(const void *func, size_t bytes);
+template <class F>
+inline void raise_smem_limit(F *func, size_t bytes) {
+    raise_smem_limit((const void *)func, bytes);
+}
+
 // Every kernel launch of the library is followed by FMM_CHECK_LAUNCH, which
 // also counts it (fmm2d_b200_launch_count).
 void note_launch();

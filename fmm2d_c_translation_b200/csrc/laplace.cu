@@ -860,7 +860,7 @@ void launch_p2p_t(const Tree &T, const CauchyProblem &P, int c0, double th2,
     do {                                                                        \
         constexpr size_t sm = p2p_smem_bytes<CH, IFC, IFD, MIXED>();            \
         auto kern = p2p_kernel<CH, PGH, IFC, IFD, MIXED, LAPR>;                 \
-        FMM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); \
+        raise_smem_limit(kern, (int)sm); \
         kern<<<g, kP2PWarps * 32, sm, s>>>(lo, hi, n1, l1, nc, leaves, sse,     \
                                           spos, chg, dip, P.sset, P.tset, spos, \
                                           tpos, P.ndc, c0, th2);                \
@@ -1465,8 +1465,7 @@ void upward_chunk(const Tree &T, const CauchyProblem &P, int c0,
         const int lo = T.lstart[2];
         if (warpk) {
             const size_t sm = pow_warp_smem(p, CH);
-            FMM_CUDA(cudaFuncSetAttribute(p2m_warp_kernel<CH>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            raise_smem_limit(p2m_warp_kernel<CH>, (int)sm);
             p2m_warp_kernel<CH><<<pow_grid(nb - lo), kPowWarps * 32, sm, s>>>(
                 lo, nb, p, T.nchild.get(), T.centers.get(), T.level.get(), bs,
                 T.srcse.get(), P.src, P.charge, P.dipstr, P.ifcharge, P.ifdipole,
@@ -1507,8 +1506,7 @@ void m2l_chunk(const Tree &T, const CauchyProblem &P, int c0,
     const EvalCounts ec{T.srcse.get(), T.trgse.get(), P.sset.pgh, P.tset.pgh};
     const size_t sh_exp = (size_t)kWarpsPerBlock * (p + 1) * CH * sizeof(double2);
     const size_t sh_m2l = (size_t)(((p + 1) * (p + 1) + 1) & ~1) * sizeof(double) + sh_exp;
-    FMM_CUDA(cudaFuncSetAttribute(m2l_kernel<CH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)sh_m2l));
+    raise_smem_limit(m2l_kernel<CH>, (int)sh_m2l);
     for (int l = 2; l <= L; l++) {
         const int lo = T.lstart[l], hi = T.lend[l];
         m2l_kernel<CH><<<grid_for(hi - lo), kBlock, sh_m2l, s>>>(
@@ -1540,8 +1538,7 @@ void downward_chunk(const Tree &T, const CauchyProblem &P, int c0,
         const int lo = T.lstart[2];
         if (warpk) {
             const size_t sm = pow_warp_smem(p, CH);
-            FMM_CUDA(cudaFuncSetAttribute(p2l_warp_kernel<CH>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            raise_smem_limit(p2l_warp_kernel<CH>, (int)sm);
             p2l_warp_kernel<CH><<<pow_grid(nb - lo), kPowWarps * 32, sm, s>>>(
                 lo, nb, p, ec, T.nlist4.get(), T.list4.get(), T.centers.get(),
                 T.level.get(), bs, P.src, P.charge, P.dipstr, P.ifcharge,

@@ -978,7 +978,7 @@ bool m2l_fp32(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 
         const float *tab = tc_tables(p, KP, s, &tab0);
         const size_t smem = (size_t)(2 * kTcRows * KP + 2 * KP * KP) * sizeof(float);
         auto launch = [&](auto kern, const M2LWork &ww, int c0) {
-            FMM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            raise_smem_limit(kern, (int)smem);
             const int blocks = std::max(1, std::min(ww.ntiles, kNumSM * 4));
             kern<<<blocks, kTcRows, smem, s>>>(ww.seg(), (const int *)ww.vals.get(), ww.slots.get(),
                                                T.d_boxsize.get(), P.ndc, c0, p, tab, tab0,

@@ -769,7 +769,7 @@ void launch_win(const WinPlan &W, const WinTables &tb, const Tree &T, const Cauc
                 int c0, const float2 *mp32, double2 *loc, int *err, cudaStream_t s) {
     constexpr size_t sm = win_smem_bytes<CH, HALF>();
     auto kern = m2l_win_kernel<CH, HALF>;
-    FMM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    raise_smem_limit(kern, (int)sm);
     for (const auto &r : W.ranges) {
         WinArgs a;
         a.wbox = W.wbox.get();

@@ -75,3 +75,21 @@ def test_mixed_stream_matches_alone(fm):
     assert st["peak_bytes"] <= budget
     assert st["peak_running"] >= 2
     srv.close()
+
+
+@pytest.mark.gpu
+def test_concurrent_orders_all_succeed(fm):
+    # Requests of different expansion orders run the same kernels with
+    # different shared-memory sizes on concurrent worker threads; every one
+    # of them must launch (a kernel's shared-memory limit is only raised,
+    # never lowered under another thread's launch).
+    srv = fm.Server(slots=8, hbm_budget=100e9)
+    tickets = []
+    for i in range(96):
+        eps = (1e-3, 1e-6, 1e-9, 1e-12)[i % 4]
+        kern = "lch"[i % 3]
+        r, keep = _req(fm, kern, 2000 + 97 * i, 500 + i, eps=eps, zk=2.0 + i % 7, pgt=i % 2)
+        tickets.append(srv.submit(r, keep))
+    iers = [srv.wait(t)[0] for t in tickets]
+    srv.close()
+    assert iers == [0] * len(iers), fm.last_error()
