@@ -1,15 +1,17 @@
 // sort.cu -- stable LSD radix sort of (uint32 key, uint32 value) pairs.
 //
-// Used by the tree builder to turn "leaf of every point" into the reference's
-// stable point permutation (isrc / itarg): points are ordered by the
-// depth-first position of their leaf and, inside a leaf, by input index,
-// which is exactly what the reference's repeated stable partition
+// Used by the tree builder: once to order the points by their path keys
+// (the child digits of every level, most significant first), and once to
+// put the points of every leaf back in input order, which is the stable
+// permutation the reference's repeated partition
 // (c_translation/src/pts_tree2d.c:670-765) produces.
 //
-// One pass per 8-bit digit: a per-tile histogram, a scan of the
-// digit-major histogram table, and a scatter in which every tile ranks its
-// items stably (warp match for ties inside a warp, per-warp counts in shared
-// memory across warps, a running per-digit count across rounds).
+// One pass per 8-bit digit: a per-tile histogram, a scan of the digit-major
+// histogram table, and a scatter in which every tile first ranks its items
+// stably into shared memory (warp match for ties inside a warp, per-warp
+// counts across warps, a running per-digit count across rounds) and then
+// writes them out in digit order, so that consecutive threads write
+// consecutive addresses of the same digit run.
 #include "common.cuh"
 #include "sort.cuh"
 
@@ -22,9 +24,9 @@ constexpr int kRounds = 16;
 constexpr int kTile = kThreads * kRounds;  // 4096 items per block
 constexpr int kRadix = 256;
 
-__global__ void radix_hist_kernel(const uint32_t *__restrict__ keys, int64_t n,
-                                  int shift, int nblocks,
-                                  int *__restrict__ hist) {
+__global__ void __launch_bounds__(kThreads) radix_hist_kernel(
+    const uint32_t *__restrict__ keys, int64_t n, int shift, int nblocks,
+    int *__restrict__ hist) {
     __shared__ int h[kRadix];
     h[threadIdx.x] = 0;
     __syncthreads();
@@ -38,16 +40,34 @@ __global__ void radix_hist_kernel(const uint32_t *__restrict__ keys, int64_t n,
     hist[threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
 }
 
-__global__ void radix_scatter_kernel(const uint32_t *__restrict__ kin,
-                                     const uint32_t *__restrict__ vin,
-                                     uint32_t *__restrict__ kout,
-                                     uint32_t *__restrict__ vout, int64_t n,
-                                     int shift, int nblocks,
-                                     const int *__restrict__ offs) {
+__global__ void __launch_bounds__(kThreads) radix_scatter_kernel(
+    const uint32_t *__restrict__ kin, const uint32_t *__restrict__ vin,
+    uint32_t *__restrict__ kout, uint32_t *__restrict__ vout, int64_t n, int shift,
+    int nblocks, const int *__restrict__ hist, const int *__restrict__ offs) {
+    __shared__ uint32_t sk[kTile];
+    __shared__ uint32_t sv[kTile];
+    __shared__ int lstart[kRadix];  // tile-local start of each digit
+    __shared__ int gdelta[kRadix];  // global position - local position
     __shared__ int run[kRadix];
     __shared__ int wc[kWarps][kRadix];
+    __shared__ int wsum[kWarps];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    run[tid] = offs[tid * nblocks + blockIdx.x];
+    // exclusive scan of this tile's digit counts
+    const int h = hist[tid * nblocks + blockIdx.x];
+    int incl = h;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += y;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    int wpre = 0;
+    for (int w = 0; w < warp; w++) wpre += wsum[w];
+    const int excl = wpre + incl - h;
+    lstart[tid] = excl;
+    gdelta[tid] = offs[tid * nblocks + blockIdx.x] - excl;
+    run[tid] = 0;
     const unsigned lt_mask = (1u << lane) - 1u;
     const int64_t base = (int64_t)blockIdx.x * kTile;
     for (int r = 0; r < kRounds; r++) {
@@ -68,17 +88,24 @@ __global__ void radix_scatter_kernel(const uint32_t *__restrict__ kin,
         if (valid && rank == 0) wc[warp][d] = __popc(peers);
         __syncthreads();
         if (valid) {
-            int pos = run[d] + rank;
+            int pos = lstart[d] + run[d] + rank;
             for (int w = 0; w < warp; w++) pos += wc[w][d];
-            kout[pos] = key;
-            vout[pos] = val;
+            sk[pos] = key;
+            sv[pos] = val;
         }
         __syncthreads();
         int add = 0;
 #pragma unroll
         for (int w = 0; w < kWarps; w++) add += wc[w][tid];
         run[tid] += add;
-        __syncthreads();
+    }
+    __syncthreads();
+    const int cnt = n - base < kTile ? (int)(n - base) : kTile;
+    for (int i = tid; i < cnt; i += kThreads) {
+        const uint32_t key = sk[i];
+        const int64_t g = (int64_t)gdelta[(key >> shift) & 0xff] + i;
+        kout[g] = key;
+        vout[g] = sv[i];
     }
 }
 
@@ -86,21 +113,21 @@ __global__ void radix_scatter_kernel(const uint32_t *__restrict__ kin,
 
 void radix_sort_pairs(uint32_t *keys, uint32_t *vals, uint32_t *keys_tmp,
                       uint32_t *vals_tmp, int64_t n, int key_bits,
-                      cudaStream_t s) {
-    if (n <= 1 || key_bits <= 0) return;
+                      cudaStream_t s, int lo_bit) {
+    if (n <= 1 || key_bits <= lo_bit) return;
     const int nblocks = (int)((n + kTile - 1) / kTile);
     DevBuf<int> hist((size_t)kRadix * nblocks, s);
     DevBuf<int> offs((size_t)kRadix * nblocks, s);
     uint32_t *ka = keys, *va = vals, *kb = keys_tmp, *vb = vals_tmp;
     int passes = 0;
-    for (int shift = 0; shift < key_bits; shift += 8) {
+    for (int shift = lo_bit; shift < key_bits; shift += 8) {
         radix_hist_kernel<<<nblocks, kThreads, 0, s>>>(ka, n, shift, nblocks,
                                                        hist.get());
         FMM_CHECK_LAUNCH();
         exclusive_scan_i32(hist.get(), offs.get(), (int64_t)kRadix * nblocks,
                            nullptr, s);
         radix_scatter_kernel<<<nblocks, kThreads, 0, s>>>(
-            ka, va, kb, vb, n, shift, nblocks, offs.get());
+            ka, va, kb, vb, n, shift, nblocks, hist.get(), offs.get());
         FMM_CHECK_LAUNCH();
         std::swap(ka, kb);
         std::swap(va, vb);

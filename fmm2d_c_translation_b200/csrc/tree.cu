@@ -14,6 +14,7 @@
 #include "tree.cuh"
 
 #include <algorithm>
+#include <cstring>
 
 namespace fmm2d {
 namespace {
@@ -38,11 +39,89 @@ __device__ __forceinline__ bool within(double2 a, double2 b, double d) {
     return fabs(__dsub_rn(a.x, b.x)) <= d && fabs(__dsub_rn(a.y, b.y)) <= d;
 }
 
+// Path keys.  The box that holds a point at level m is fixed by the child
+// digits (0..3, the reference's child number minus 1) the point takes at
+// levels 1..m, each decided by `p - c < 0` against the FP64 center of its
+// box one level up.  A center depends only on the path (repeated
+// c +/- bs/2), so the digits of every level can be computed for every point
+// up front, without the tree.  Word w of a key holds the digits of levels
+// 16w+1 .. 16w+16, two bits each, the coarsest level in the top bits;
+// sorting by the words, first word most significant, orders the points by
+// path, which is the order of the reference's nested stable partitions.
+constexpr int kKeyWords = 4;  // up to 64 levels (nlmax of the reference is 51)
+
+struct KeyView {
+    const uint32_t *w[kKeyWords];  // sorted key words, one array per word
+};
+
+__device__ __forceinline__ int key_digit(const KeyView &kv, int64_t k, int m) {
+    const int w = (m - 1) >> 4, sh = 2 * (15 - ((m - 1) & 15));
+    return (int)((kv.w[w][k] >> sh) & 3u);
+}
+
+// Path keys of n points: nw words per point, word-major (word w of point i
+// at words[w * n + i]); digits of levels beyond `ds` are 0.  bsl[m] is the
+// box size of level m, obtained by repeated halving as the reference does.
+__global__ void __launch_bounds__(256) path_key_kernel(
+    const double2 *__restrict__ pts, int n, double2 c0, const double *__restrict__ bsl,
+    int ds, int nw, uint32_t *__restrict__ words) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double2 p = pts[i];
+        double2 c = c0;
+        for (int w = 0; w < nw; w++) {
+            uint32_t key = 0;
+#pragma unroll 4
+            for (int t = 0; t < 16; t++) {
+                const int m = 16 * w + t + 1;
+                int d = 0;
+                if (m <= ds) {
+                    d = child_digit(p, c);
+                    c = child_center(c, bsl[m], d);
+                }
+                key = (key << 2) | (uint32_t)d;
+            }
+            words[(size_t)w * n + i] = key;
+        }
+    }
+}
+
+// Input order inside every leaf of at most 32 points: one warp per leaf
+// sorts the leaf's input indices (bitonic network over the lanes).
+__global__ void __launch_bounds__(256) leaf_order_kernel(
+    int nb, const int *__restrict__ nch, const int2 *__restrict__ rng,
+    const uint32_t *__restrict__ idx, int *__restrict__ perm) {
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int b = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); b < nb; b += warps) {
+        if (nch[b] != 0) continue;
+        const int2 r = rng[b];
+        const int cnt = r.y - r.x;
+        if (cnt <= 0) continue;
+        uint32_t v = lane < cnt ? idx[r.x + lane] : 0xffffffffu;
+        if (cnt > 1) {
+#pragma unroll
+            for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    const uint32_t o = __shfl_xor_sync(0xffffffffu, v, j);
+                    const bool up = (lane & k) == 0, low = (lane & j) == 0;
+                    v = (low == up) ? min(v, o) : max(v, o);
+                }
+        }
+        if (lane < cnt) perm[r.x + lane] = (int)v;
+    }
+}
+
 struct Builder {
     Tree &T;
     cudaStream_t s;
     DevBuf<int> iflag;
-    DevBuf<int> cnt_s, cnt_t;  // point counts per box (initial build only)
+    DevBuf<int> cnt_s, cnt_t;  // point counts per box (levelwise build only)
+    // key build: every box's [start, end) range in the key-sorted sources
+    // and targets, and the sorted key words
+    bool ranges = false;
+    DevBuf<int2> rs, rt;
+    KeyView kvs{}, kvt{};
 
     Builder(Tree &t, cudaStream_t st) : T(t), s(st) {}
 
@@ -61,7 +140,45 @@ struct Builder {
         iflag.grow(nc, keep, s);
         if (cnt_s.size()) cnt_s.grow(nc, keep, s);
         if (cnt_t.size()) cnt_t.grow(nc, keep, s);
+        if (ranges) {
+            rs.grow(nc, keep, s);
+            rt.grow(nc, keep, s);
+        }
         T.cap = nc;
+    }
+
+    // Point ranges of the boxes [nb0, nb1), all just created as children (4
+    // per parent, in child order): within the parent's range the key-sorted
+    // points are ordered by their digit at the children's level, so child j
+    // starts at the first point whose digit is >= j (binary search).
+    void set_child_ranges(int nb0, int nb1) {
+        if (!ranges || nb1 <= nb0) return;
+        const int *par = T.parent.get(), *lev = T.level.get();
+        int2 *R[2] = {rs.get(), rt.get()};
+        const KeyView K[2] = {kvs, kvt};
+        for (int set = 0; set < 2; set++) {
+            int2 *r = R[set];
+            const KeyView kv = K[set];
+            for_each(nb1 - nb0, s, [=] __device__(int64_t i) {
+                const int kb = nb0 + (int)i, j = (int)(i & 3);
+                const int m = lev[kb];
+                const int2 pr = r[par[kb]];
+                auto first_ge = [&](int dj) {
+                    int lo = pr.x, hi = pr.y;
+                    while (lo < hi) {
+                        const int mid = lo + ((hi - lo) >> 1);
+                        if (key_digit(kv, mid, m) < dj)
+                            lo = mid + 1;
+                        else
+                            hi = mid;
+                    }
+                    return lo;
+                };
+                const int a = (j == 0 || pr.x == pr.y) ? pr.x : first_ge(j);
+                const int b = (j == 3 || pr.x == pr.y) ? pr.y : first_ge(j + 1);
+                r[kb] = make_int2(a, b);
+            });
+        }
     }
 
     // Appends 4 children to every box b in [lo, hi) with sel(b) true, in box
@@ -108,6 +225,7 @@ struct Builder {
             }
         });
         T.nboxes += 4 * nref;
+        set_child_ranges(nb0, T.nboxes);
         return nref;
     }
 
@@ -217,14 +335,25 @@ struct Builder {
         DevBuf<double2> cen2(T.cap, s);
         DevBuf<int> lev2(T.cap, s), par2(T.cap, s), nch2(T.cap, s),
             chi2((size_t)4 * T.cap, s), flg2(T.cap, s);
+        DevBuf<int2> rs2, rt2;
+        if (ranges) {
+            rs2.alloc(T.cap, s);
+            rt2.alloc(T.cap, s);
+        }
         const double2 *cen = T.centers.get();
         const int *par = T.parent.get(), *nch = T.nchild.get(),
                   *chi = T.child.get(), *flg = iflag.get();
+        const int2 *ra = rs.get(), *rb = rt.get();
         double2 *c2 = cen2.get();
         int *l2 = lev2.get(), *p2 = par2.get(), *n2 = nch2.get(),
             *h2 = chi2.get(), *f2 = flg2.get();
+        int2 *ra2 = rs2.get(), *rb2 = rt2.get();
         for_each(nb, s, [=] __device__(int64_t i) {
             const int b = (int)i, m = mp[b];
+            if (ra2) {
+                ra2[m] = ra[b];
+                rb2[m] = rb[b];
+            }
             c2[m] = cen[b];
             l2[m] = levp[b];
             n2[m] = nch[b];
@@ -241,10 +370,29 @@ struct Builder {
         T.nchild = std::move(nch2);
         T.child = std::move(chi2);
         iflag = std::move(flg2);
+        if (ranges) {
+            rs = std::move(rs2);
+            rt = std::move(rt2);
+        }
         for (int l = 2; l <= L; l++) {
             T.lstart[l] = nstart[l];
             T.lend[l] = nend[l];
         }
+    }
+
+    // Number of boxes whose flag lies in [f0, f1].
+    int count_flags(int f0, int f1) {
+        DevBuf<int> c(1, s);
+        c.zero(s);
+        int *cp = c.get();
+        const int *fl = iflag.get();
+        for_each(T.nboxes, s, [=] __device__(int64_t i) {
+            const int f = fl[i];
+            const bool hit = f >= f0 && f <= f1;
+            const unsigned m = __ballot_sync(__activemask(), hit);
+            if (hit && (threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(cp, __popc(m));
+        });
+        return read_scalar(cp, s);
     }
 
     // pts_tree_fix_lr (pts_tree2d.c:767-964).
@@ -295,6 +443,10 @@ struct Builder {
                 }
             });
         }
+        // Nothing flagged: the tree is level-restricted already, and every
+        // remaining step (subdivision, reorganisation, colleagues, the
+        // flag++ pass) would leave it as it is.
+        if (count_flags(1, 2) == 0) return;
         // Subdivide flag and flag+ boxes of the original levels.
         std::vector<int> ts(L + 1, 0), te(L + 1, 0);
         for (int l = 1; l <= L - 2; l++) {
@@ -313,6 +465,8 @@ struct Builder {
                 if (fl[i] != 3) fl[i] = 0;
             });
         }
+        // no flag++ box: no further subdivision
+        if (count_flags(3, 3) == 0) return;
         std::fill(ts.begin(), ts.end(), 0);
         std::fill(te.begin(), te.end(), 0);
         for (int l = 2; l <= L - 2; l++) {
@@ -451,7 +605,111 @@ struct Builder {
         FMM_CUDA(cudaMemcpyAsync(perm.get(), vp, (size_t)n * sizeof(int),
                                  cudaMemcpyDeviceToDevice, s));
     }
+
+    // Key build: the per-box ranges become srcse / itargse as they are (the
+    // leaves hold the same points, in the same order of leaves, as the
+    // reference's sorted arrays); inside every leaf the points go back to
+    // input order.  `idx` maps key-sorted positions to input indices.
+    void finish_points(const uint32_t *idx, const KeyView &kv, int n, const DevBuf<int2> &R,
+                       DevBuf<int2> &se, DevBuf<int> &perm) {
+        const int nb = T.nboxes;
+        se.alloc(nb, s);
+        FMM_CUDA(cudaMemcpyAsync(se.get(), R.get(), (size_t)nb * sizeof(int2),
+                                 cudaMemcpyDeviceToDevice, s));
+        perm.alloc(std::max(n, 1), s);
+        if (n == 0) return;
+        const int *nch = T.nchild.get(), *chi = T.child.get();
+        const int2 *rp = R.get();
+        DevBuf<int> big(1, s);
+        big.zero(s);
+        int *bp = big.get();
+        for_each(nb, s, [=] __device__(int64_t i) {
+            const int2 r = rp[i];
+            if (nch[i] == 0 && r.y - r.x > 32) atomicExch(bp, 1);
+        });
+        if (read_scalar(bp, s) == 0) {
+            const int blocks = std::max(1, std::min((nb + 7) / 8, kNumSM * 16));
+            leaf_order_kernel<<<blocks, 256, 0, s>>>(nb, nch, rp, idx, perm.get());
+            FMM_CHECK_LAUNCH();
+            return;
+        }
+        // some leaf holds more than 32 points: stable sort of the input
+        // order by the start of each point's leaf
+        DevBuf<uint32_t> keys(n, s), vals(n, s), kt(n, s), vt(n, s);
+        uint32_t *kp = keys.get(), *vp = vals.get();
+        for_each(n, s, [=] __device__(int64_t k) {
+            int b = 0, m = 0;
+            while (nch[b] > 0) {
+                m++;
+                b = chi[4 * b + key_digit(kv, k, m)];
+            }
+            kp[idx[k]] = (uint32_t)rp[b].x;
+            vp[k] = (uint32_t)k;
+        });
+        int bits = 1;
+        while ((1LL << bits) < (long long)n) bits++;
+        radix_sort_pairs(kp, vp, kt.get(), vt.get(), n, bits, s);
+        FMM_CUDA(cudaMemcpyAsync(perm.get(), vp, (size_t)n * sizeof(int),
+                                 cudaMemcpyDeviceToDevice, s));
+    }
 };
+
+// Key-sorted order of one point set: the input index of every sorted
+// position and the sorted key words.
+struct KeyedPoints {
+    DevBuf<uint32_t> idx;
+    std::vector<DevBuf<uint32_t>> words;
+    KeyView view() const {
+        KeyView v{};
+        for (size_t w = 0; w < words.size() && w < (size_t)kKeyWords; w++) v.w[w] = words[w].get();
+        return v;
+    }
+};
+
+// Computes the path keys of levels 1..ds and sorts the points by them
+// (stable, so equal keys keep input order).
+void key_sort(const double2 *pts, int n, double2 c0, const double *d_bsl, int ds,
+              KeyedPoints &kp, cudaStream_t s) {
+    const int nw = (ds + 15) / 16;
+    kp.words.clear();
+    kp.words.resize(nw);
+    if (n <= 0) return;
+    DevBuf<uint32_t> raw((size_t)nw * n, s);
+    {
+        const int blocks = (int)std::min<int64_t>(((int64_t)n + 255) / 256, kNumSM * 8);
+        path_key_kernel<<<blocks, 256, 0, s>>>(pts, n, c0, d_bsl, ds, nw, raw.get());
+        FMM_CHECK_LAUNCH();
+    }
+    kp.idx.alloc(n, s);
+    uint32_t *ip = kp.idx.get();
+    for_each(n, s, [=] __device__(int64_t i) { ip[i] = (uint32_t)i; });
+    DevBuf<uint32_t> key(n, s), kt(n, s), vt(n, s);
+    uint32_t *kp0 = key.get();
+    const uint32_t *rw = raw.get();
+    // least significant word first; only the bits of levels <= ds
+    for (int w = nw - 1; w >= 0; w--) {
+        const uint32_t *src = rw + (size_t)w * n;
+        if (w == nw - 1)
+            FMM_CUDA(cudaMemcpyAsync(kp0, src, (size_t)n * sizeof(uint32_t),
+                                     cudaMemcpyDeviceToDevice, s));
+        else
+            for_each(n, s, [=] __device__(int64_t k) { kp0[k] = src[ip[k]]; });
+        const int used = 2 * std::min(16, ds - 16 * w);
+        const int lo = (32 - used) & ~7;
+        radix_sort_pairs(kp0, ip, kt.get(), vt.get(), n, 32, s, lo);
+    }
+    for (int w = 0; w < nw; w++) {
+        kp.words[w].alloc(n, s);
+        uint32_t *o = kp.words[w].get();
+        if (w == 0) {
+            FMM_CUDA(cudaMemcpyAsync(o, kp0, (size_t)n * sizeof(uint32_t),
+                                     cudaMemcpyDeviceToDevice, s));
+        } else {
+            const uint32_t *src = rw + (size_t)w * n;
+            for_each(n, s, [=] __device__(int64_t k) { o[k] = src[ip[k]]; });
+        }
+    }
+}
 
 // Bounding box of sources and targets (pts_tree2d.c:493-513): exact min/max.
 __global__ void bbox_kernel(const double2 *__restrict__ a, int na,
@@ -541,31 +799,15 @@ __global__ void __launch_bounds__(256) assign_children_kernel(
 
 }  // namespace
 
-void build_tree(const double2 *d_src, int ns, const double2 *d_targ, int nt,
-                int ndiv, int idivflag, int nlmax, cudaStream_t s, Tree &T) {
-    T = Tree();
+namespace {
+
+// The reference's level-by-level construction (pts_tree2d.c:541-611): every
+// level moves each point of a refined box into its child.  Kept beside the
+// key build (FMM2D_B200_TREE=levelwise) as an independent construction of
+// the same tree.
+void build_levelwise(const double2 *d_src, int ns, const double2 *d_targ, int nt, int ndiv,
+                     int idivflag, int nlmax, double2 c0, cudaStream_t s, Tree &T) {
     Builder B(T, s);
-    // ---- root: bounding square of sources and targets ----
-    const int nblk = 2 * kNumSM;
-    prof_mark("tree_start", s);
-    DevBuf<double> part(4 * nblk, s);
-    bbox_kernel<<<nblk, 256, 0, s>>>(d_src, ns, d_targ, nt, part.get());
-    FMM_CHECK_LAUNCH();
-    std::vector<double> hp(4 * nblk);
-    FMM_CUDA(cudaMemcpyAsync(hp.data(), part.get(), hp.size() * sizeof(double),
-                             cudaMemcpyDeviceToHost, s));
-    FMM_CUDA(cudaStreamSynchronize(s));
-    double xmin = hp[0], xmax = hp[1], ymin = hp[2], ymax = hp[3];
-    for (int k = 1; k < nblk; k++) {
-        xmin = std::min(xmin, hp[4 * k]);
-        xmax = std::max(xmax, hp[4 * k + 1]);
-        ymin = std::min(ymin, hp[4 * k + 2]);
-        ymax = std::max(ymax, hp[4 * k + 3]);
-    }
-    double bs0 = xmax - xmin;
-    const double sizey = ymax - ymin;
-    if (sizey > bs0) bs0 = sizey;
-    T.boxsize.push_back(bs0);
     B.cnt_s.alloc(1, s);
     B.cnt_t.alloc(1, s);
     B.ensure(1024);
@@ -576,7 +818,7 @@ void build_tree(const double2 *d_src, int ns, const double2 *d_targ, int nt,
         double2 *cen = T.centers.get();
         int *lev = T.level.get(), *par = T.parent.get(), *nch = T.nchild.get(),
             *chi = T.child.get(), *cs = B.cnt_s.get(), *ct = B.cnt_t.get();
-        const double cx = (xmin + xmax) / 2, cy = (ymin + ymax) / 2;
+        const double cx = c0.x, cy = c0.y;
         for_each(1, s, [=] __device__(int64_t) {
             cen[0] = make_double2(cx, cy);
             lev[0] = 0;
@@ -650,6 +892,134 @@ void build_tree(const double2 *d_src, int ns, const double2 *d_targ, int nt,
     B.sort_points(d_src, ns, T.srcse, T.isrc);
     B.sort_points(d_targ, nt, T.trgse, T.itarg);
     prof_mark("tree_sort", s);
+}
+
+// Key build: sort the points once by their path keys of levels 1..ds, then
+// refine level by level with every box's point count read off its range in
+// the sorted order (three binary searches per refined box instead of a pass
+// over all points).  Returns false when the tree needs digits of levels
+// beyond ds; the caller then retries with more.
+bool build_by_keys(const double2 *d_src, int ns, const double2 *d_targ, int nt, int ndiv,
+                   int idivflag, int nlmax, double2 c0, int ds, cudaStream_t s, Tree &T) {
+    const double bs0 = T.boxsize[0];
+    T = Tree();
+    T.boxsize.push_back(bs0);
+    Builder B(T, s);
+    B.ranges = true;
+    std::vector<double> bsl(ds + 1);
+    bsl[0] = bs0;
+    for (int l = 1; l <= ds; l++) bsl[l] = bsl[l - 1] / 2;
+    DevBuf<double> d_bsl(ds + 1, s);
+    FMM_CUDA(cudaMemcpyAsync(d_bsl.get(), bsl.data(), bsl.size() * sizeof(double),
+                             cudaMemcpyHostToDevice, s));
+    KeyedPoints ks, kt;
+    key_sort(d_src, ns, c0, d_bsl.get(), ds, ks, s);
+    key_sort(d_targ, nt, c0, d_bsl.get(), ds, kt, s);
+    B.kvs = ks.view();
+    B.kvt = kt.view();
+    B.ensure(1024);
+    T.nboxes = 1;
+    T.lstart.push_back(0);
+    T.lend.push_back(1);
+    {
+        double2 *cen = T.centers.get();
+        int *lev = T.level.get(), *par = T.parent.get(), *nch = T.nchild.get(),
+            *chi = T.child.get();
+        int2 *r0 = B.rs.get(), *r1 = B.rt.get();
+        for_each(1, s, [=] __device__(int64_t) {
+            cen[0] = c0;
+            lev[0] = 0;
+            par[0] = -1;
+            nch[0] = 0;
+            for (int j = 0; j < 4; j++) chi[j] = -1;
+            r0[0] = make_int2(0, ns);
+            r1[0] = make_int2(0, nt);
+        });
+    }
+    DevBuf<int> nflag(1, s);
+    int ilev = 0;
+    for (ilev = 0; ilev <= nlmax - 1; ilev++) {
+        const int lo = T.lstart[ilev], hi = T.lend[ilev];
+        const int2 *ra = B.rs.get(), *rb = B.rt.get();
+        const int dflag = idivflag, nd = ndiv;
+        DevBuf<int> f(hi - lo, s);
+        int *fp = f.get();
+        const bool last = ilev + 1 > ds;
+        int *nf = nflag.get();
+        if (last) nflag.zero(s);
+        for_each(hi - lo, s, [=] __device__(int64_t i) {
+            const int b = lo + (int)i;
+            const int nss = ra[b].y - ra[b].x, ntt = rb[b].y - rb[b].x;
+            const int nn = dflag == 0 ? nss : (dflag == 1 ? ntt : (nss > ntt ? nss : ntt));
+            fp[i] = nn > nd ? 1 : 0;
+            if (last && nn > nd) atomicAdd(nf, 1);
+        });
+        if (last) {
+            if (read_scalar(nf, s) > 0) return false;
+            break;
+        }
+        T.boxsize.push_back(T.boxsize[ilev] / 2);
+        const int nb0 = T.nboxes;
+        const int nref = B.refine_range(
+            lo, hi, ilev + 1, T.boxsize[ilev + 1],
+            [=] __device__(int b) { return fp[b - lo] != 0; }, false);
+        if (nref == 0) {
+            T.boxsize.pop_back();
+            break;
+        }
+        T.lstart.push_back(nb0);
+        T.lend.push_back(T.nboxes);
+    }
+    T.nlevels = ilev;
+    prof_mark("tree_refine", s);
+    B.computecoll(0, T.nlevels);
+    if (T.nlevels >= 2) B.fix_lr();
+    prof_mark("tree_fixlr", s);
+    B.finish_points(ks.idx.get(), B.kvs, ns, B.rs, T.srcse, T.isrc);
+    B.finish_points(kt.idx.get(), B.kvt, nt, B.rt, T.trgse, T.itarg);
+    prof_mark("tree_sort", s);
+    return true;
+}
+
+}  // namespace
+
+void build_tree(const double2 *d_src, int ns, const double2 *d_targ, int nt,
+                int ndiv, int idivflag, int nlmax, cudaStream_t s, Tree &T) {
+    T = Tree();
+    // ---- root: bounding square of sources and targets ----
+    const int nblk = 2 * kNumSM;
+    prof_mark("tree_start", s);
+    DevBuf<double> part(4 * nblk, s);
+    bbox_kernel<<<nblk, 256, 0, s>>>(d_src, ns, d_targ, nt, part.get());
+    FMM_CHECK_LAUNCH();
+    std::vector<double> hp(4 * nblk);
+    FMM_CUDA(cudaMemcpyAsync(hp.data(), part.get(), hp.size() * sizeof(double),
+                             cudaMemcpyDeviceToHost, s));
+    FMM_CUDA(cudaStreamSynchronize(s));
+    double xmin = hp[0], xmax = hp[1], ymin = hp[2], ymax = hp[3];
+    for (int k = 1; k < nblk; k++) {
+        xmin = std::min(xmin, hp[4 * k]);
+        xmax = std::max(xmax, hp[4 * k + 1]);
+        ymin = std::min(ymin, hp[4 * k + 2]);
+        ymax = std::max(ymax, hp[4 * k + 3]);
+    }
+    double bs0 = xmax - xmin;
+    const double sizey = ymax - ymin;
+    if (sizey > bs0) bs0 = sizey;
+    T.boxsize.push_back(bs0);
+    const double2 c0 = make_double2((xmin + xmax) / 2, (ymin + ymax) / 2);
+    const char *mode = getenv("FMM2D_B200_TREE");
+    if (mode && !strcmp(mode, "levelwise")) {
+        build_levelwise(d_src, ns, d_targ, nt, ndiv, idivflag, nlmax, c0, s, T);
+    } else {
+        // first guess of the depth: a uniform distribution's, plus one level
+        const int64_t nref = idivflag == 0 ? ns : (idivflag == 1 ? nt : std::max(ns, nt));
+        int ds = 2;
+        for (int64_t q = std::max<int64_t>(ndiv, 1); q < nref && ds < nlmax; q *= 4) ds++;
+        ds = std::min(ds, nlmax);
+        while (!build_by_keys(d_src, ns, d_targ, nt, ndiv, idivflag, nlmax, c0, ds, s, T))
+            ds = std::min(nlmax, ds + 8);
+    }
     T.d_boxsize.alloc(T.nlevels + 2, s);
     std::vector<double> bsx(T.boxsize);
     bsx.push_back(T.boxsize.back() / 2);
@@ -658,6 +1028,7 @@ void build_tree(const double2 *d_src, int ns, const double2 *d_targ, int nt,
                              cudaMemcpyHostToDevice, s));
     FMM_CUDA(cudaStreamSynchronize(s));
 }
+
 
 void compute_lists(Tree &T, cudaStream_t s) {
     const int nb = T.nboxes;

@@ -22,11 +22,25 @@ CASES = {
     "single_box": lambda: (ps.uniform(10, 8), ps.uniform(5, 9), 15, 0),
     "targets_rule": lambda: (ps.uniform(3000, 10), ps.blobs(6000, 11), 12, 1),
     "max_rule": lambda: (ps.blobs(3000, 12), ps.uniform(6000, 13), 12, 2),
+    # deeper than the first guess of the key depth (20+ levels)
+    "tight_blobs": lambda: (ps.blobs(20000, 14, nblob=4, sigma=1e-6),
+                            ps.blobs(5000, 15, nblob=4, sigma=1e-5), 10, 0),
+    # enough points per set for the multi-block sort passes
+    "uniform_300000": lambda: (ps.uniform(300000, 16), ps.uniform(200000, 17), 24, 0),
 }
 
 
+@pytest.fixture(params=["keys", "levelwise"])
+def builder(request, monkeypatch):
+    if request.param == "levelwise":
+        monkeypatch.setenv("FMM2D_B200_TREE", "levelwise")
+    else:
+        monkeypatch.delenv("FMM2D_B200_TREE", raising=False)
+    return request.param
+
+
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_tree_bit_exact(name):
+def test_tree_bit_exact(name, builder):
     import fmm2d_c_translation_b200 as fm
     src, trg, ndiv, idiv = CASES[name]()
     got = fm.tree_build(src, trg, ndiv=ndiv, idivflag=idiv)
