@@ -638,11 +638,225 @@ __device__ __forceinline__ float rcp_pair(float x) { return rcp_fast(x); }
 __device__ __forceinline__ double half_ln_pair(double x) { return 0.5 * log(x); }
 __device__ __forceinline__ float half_ln_pair(float x) { return half_ln_fast(x); }
 
+// Steps 6 and 7 with one warp per leaf: the warp evaluates the leaf's
+// list-3 multipoles and local expansion at all of the leaf's points and
+// stores them (the near field adds to them afterwards).  The expansion
+// coefficients are staged once per box in shared memory, in the pass's
+// precision, instead of being loaded (and converted) by every point.  Same
+// arithmetic, in the same order, as eval_far_points_kernel.
+// Whether steps 6-7 run with one warp per leaf (coefficients staged once per
+// box) or one thread per point.  Measured on a B200 (10^7 + 10^7 uniform
+// points): per leaf is faster in FP64 at p = 37 (3.9 against 4.1 ms), per
+// point in the mixed mode at p = 18 (2.0 against 2.4 ms), where a leaf's
+// ~19 points leave a third of the warp idle.  FMM2D_B200_FAR=leaf / point
+// overrides.
+bool far_per_leaf(const CauchyProblem &P) {
+    const char *m = getenv("FMM2D_B200_FAR");
+    if (m && !strcmp(m, "leaf")) return true;
+    if (m && !strcmp(m, "point")) return false;
+    return !P.mixed;
+}
+
+constexpr int kFarWarps = 4;
+
+struct FarArgs {
+    int p = 0, nlevels = 0;
+    const int *level = nullptr;
+    const double2 *centers = nullptr;
+    const double *bs = nullptr;
+    const int *nlist3 = nullptr, *list3 = nullptr;
+    const double2 *mp = nullptr, *loc = nullptr;
+};
+
+template <int CH, int PGH, bool MIXED>
+__device__ __forceinline__ void far_field_box(int b, int ntb, int2 tr, int2 sr0, int ntot,
+                                              const FarArgs &fa, const int2 *__restrict__ sse,
+                                              const PointSet &sset, const PointSet &tset,
+                                              int ndc, int c0, typename Real<MIXED>::T2 *sm) {
+    typedef typename Real<MIXED>::T R;
+    typedef typename Real<MIXED>::T2 R2;
+    const int lane = lane_id();
+    const int p = fa.p, stride = (p + 1) * ndc, nc = (p + 1) * CH;
+    R2 *s_loc = sm, *s_mp = sm + nc;
+    for (int i = lane; i < nc; i += 32) {
+        const int m = i / CH, q = i - m * CH;
+        s_loc[i] = cv2<R2>(fa.loc[(size_t)b * stride + (size_t)m * ndc + c0 + q]);
+    }
+    const int lb = fa.level[b];
+    const int n3 = (lb >= 1 && lb <= fa.nlevels - 1) ? fa.nlist3[b] : 0;
+    const double2 cb = fa.centers[b];
+    const double rb = fa.bs[lb];
+    for (int t0 = 0; t0 < ntot; t0 += 32) {
+        const int t = t0 + lane;
+        const bool act = t < ntot, is_t = t < ntb;
+        const int k = is_t ? tr.x + t : sr0.x + t - ntb;
+        const double2 x = act ? (is_t ? tset.pos : sset.pos)[k] : cb;
+        R2 po[CH], gr[CH], he[CH];
+#pragma unroll
+        for (int q = 0; q < CH; q++) po[q] = gr[q] = he[q] = mk2<R2>(0.0, 0.0);
+        for (int e = 0; e < n3; e++) {
+            const int jb = fa.list3[kMaxList3 * b + e];
+            if (sse[jb].y <= sse[jb].x) continue;  // no multipole
+            __syncwarp();
+            for (int i = lane; i < nc; i += 32) {
+                const int m = i / CH, q = i - m * CH;
+                s_mp[i] = cv2<R2>(fa.mp[(size_t)jb * stride + (size_t)m * ndc + c0 + q]);
+            }
+            __syncwarp();
+            if (!act) continue;
+            const double2 cj = fa.centers[jb];
+            const double r = fa.bs[fa.level[jb]];
+            const double zx = x.x - cj.x, zy = x.y - cj.y;
+            const double zz = zx * zx + zy * zy;
+            const R2 zi = mk2<R2>(zx / zz, -zy / zz);         // 1/z
+            const R2 w = mk2<R2>(r * zx / zz, -r * zy / zz);  // r/z
+            const R lz = (R)0.5 * Real<MIXED>::log_((R)zz);
+            const R rinv = (R)(1.0 / r);
+#pragma unroll
+            for (int q = 0; q < CH; q++) {
+                R2 q0 = s_mp[p * CH + q], q1 = mk2<R2>(0.0, 0.0), q2 = mk2<R2>(0.0, 0.0);
+                for (int m = p - 1; m >= 1; m--) {
+                    if (PGH >= 3) q2 = zadd(zmul(q2, w), q1);
+                    if (PGH >= 2) q1 = zadd(zmul(q1, w), q0);
+                    q0 = zadd(zmul(q0, w), s_mp[m * CH + q]);
+                }
+                if (PGH >= 3) q2 = zadd(zmul(q2, w), q1);
+                if (PGH >= 2) q1 = zadd(zmul(q1, w), q0);
+                q0 = zmul(q0, w);
+                const R2 M0 = s_mp[q];
+                po[q] = zadd(po[q], zadd(zscal(M0, lz), q0));
+                if (PGH >= 2) {
+                    const R2 w2 = zmul(w, w);
+                    gr[q] = zadd(gr[q], zadd(zmul(M0, zi), zscal(zmul(q1, w2), -rinv)));
+                    if (PGH >= 3) {
+                        const R2 w3 = zmul(w2, w), w4 = zmul(w2, w2);
+                        R2 h = zscal(zmul(M0, zmul(zi, zi)), (R)-1);
+                        h = zadd(h, zscal(zmul(q2, w4), (R)2 * rinv * rinv));
+                        h = zadd(h, zscal(zmul(q1, w3), (R)2 * rinv * rinv));
+                        he[q] = zadd(he[q], h);
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        if (!act) continue;
+        {
+            const R2 z = mk2<R2>((x.x - cb.x) / rb, (x.y - cb.y) / rb);
+            const R rinv = (R)(1.0 / rb);
+#pragma unroll
+            for (int q = 0; q < CH; q++) {
+                R2 q0 = s_loc[p * CH + q], q1 = mk2<R2>(0.0, 0.0), q2 = mk2<R2>(0.0, 0.0);
+                for (int m = p - 1; m >= 0; m--) {
+                    if (PGH >= 3) q2 = zadd(zmul(q2, z), q1);
+                    if (PGH >= 2) q1 = zadd(zmul(q1, z), q0);
+                    q0 = zadd(zmul(q0, z), s_loc[m * CH + q]);
+                }
+                po[q] = zadd(po[q], q0);
+                if (PGH >= 2) gr[q] = zadd(gr[q], zscal(q1, rinv));
+                if (PGH >= 3) he[q] = zadd(he[q], zscal(q2, (R)2 * rinv * rinv));
+            }
+        }
+        const int pg = is_t ? tset.pgh : sset.pgh;
+        double2 *opot = is_t ? tset.pot : sset.pot;
+        double2 *ograd = is_t ? tset.grad : sset.grad;
+        double2 *ohess = is_t ? tset.hess : sset.hess;
+#pragma unroll
+        for (int q = 0; q < CH; q++) {
+            const size_t o = (size_t)k * ndc + c0 + q;
+            opot[o] = make_double2((double)po[q].x, (double)po[q].y);
+            if (PGH >= 2 && pg >= 2) ograd[o] = make_double2((double)gr[q].x, (double)gr[q].y);
+            if (PGH >= 3 && pg >= 3) ohess[o] = make_double2((double)he[q].x, (double)he[q].y);
+        }
+    }
+    __syncwarp();
+}
+
+// One warp per leaf with points of a set that wants outputs.
+template <int CH, int PGH, bool MIXED>
+__global__ void __launch_bounds__(kFarWarps * 32) far_leaf_kernel(
+    int nb, const int *__restrict__ nchild, FarArgs fa, const int2 *__restrict__ sse,
+    PointSet sset, PointSet tset, int ndc, int c0) {
+    typedef typename Real<MIXED>::T2 R2;
+    __shared__ R2 stage[kFarWarps][2 * (kLdc / 2 + 1) * CH];
+    R2 *sm = stage[threadIdx.x >> 5];
+    for (int b = warp_global(); b < nb; b += warp_count()) {
+        if (nchild[b] != 0) continue;
+        const int2 tr = tset.pgh > 0 ? tset.se[b] : make_int2(0, 0);
+        const int2 sr0 = sset.pgh > 0 ? sset.se[b] : make_int2(0, 0);
+        const int ntb = tr.y - tr.x, ntot = ntb + sr0.y - sr0.x;
+        if (ntot == 0) continue;
+        far_field_box<CH, PGH, MIXED>(b, ntb, tr, sr0, ntot, fa, sse, sset, tset, ndc, c0, sm);
+    }
+}
+
 // LAPR: the two channels of a complex-Laplace density carry real charges
 // and only the real part of each channel's potential is used
 // (lfmm2d.f:141-157, 168-225), so the charge terms drop their imaginary
 // halves and the potential keeps its real part only.  The results used are
 // the same to the bit.
+// One source's contribution to one target of the near field: pot += q
+// log|z| + d/z, grad += q/z - d/z^2, hess += -q/z^2 + 2d/z^3 (z = t - s),
+// with `st` the source's strengths (charges of the CH channels, then
+// dipoles).  Pairs inside the threshold contribute exactly zero.
+template <int CH, int PGH, bool IFC, bool IFD, bool MIXED, bool LAPR>
+__device__ __forceinline__ void p2p_pair(const typename PosT<MIXED>::T &x,
+                                         const typename PosT<MIXED>::T &sp,
+                                         const typename Real<MIXED>::T2 *st,
+                                         typename Real<MIXED>::T th2,
+                                         typename Real<MIXED>::T2 *po,
+                                         typename Real<MIXED>::T2 *gr,
+                                         typename Real<MIXED>::T2 *he) {
+    typedef typename Real<MIXED>::T R;
+    typedef typename Real<MIXED>::T2 R2;
+    R dx, dy;
+    pos_diff(x, sp, dx, dy);
+    const R rr = dx * dx + dy * dy;
+    // skipped pairs contribute exactly zero, without a branch
+    const bool skip = PGH == 1 ? (rr <= th2) : (rr < th2);
+    const R rrs = skip ? (R)1 : rr;
+    const R ri = skip ? (R)0 : rcp_pair(rrs);
+    R2 zi;
+    zi.x = dx * ri;
+    zi.y = -dy * ri;
+    R2 zi2 = mk2<R2>(0.0, 0.0), zi3 = mk2<R2>(0.0, 0.0);
+    if (PGH >= 2 || IFD) zi2 = zmul(zi, zi);
+    if (PGH >= 3 && IFD) zi3 = zmul(zi2, zi);
+    R rl = 0;
+    if (IFC) rl = skip ? (R)0 : half_ln_pair(rrs);
+#pragma unroll
+    for (int q = 0; q < CH; q++) {
+        if (IFC) {
+            const R2 qv = st[q];
+            if (LAPR) {
+                po[q].x = fma(rl, qv.x, po[q].x);
+                if (PGH >= 2) {
+                    gr[q].x = fma(zi.x, qv.x, gr[q].x);
+                    gr[q].y = fma(zi.y, qv.x, gr[q].y);
+                }
+                if (PGH >= 3) {
+                    he[q].x = fma(-zi2.x, qv.x, he[q].x);
+                    he[q].y = fma(-zi2.y, qv.x, he[q].y);
+                }
+            } else {
+                po[q].x = fma(rl, qv.x, po[q].x);
+                po[q].y = fma(rl, qv.y, po[q].y);
+                if (PGH >= 2) zfma(gr[q], zi, qv);
+                if (PGH >= 3) zfma(he[q], zscal(zi2, (R)-1), qv);
+            }
+        }
+        if (IFD) {
+            const R2 dv = st[(IFC ? CH : 0) + q];
+            if (LAPR) {
+                po[q].x = fma(zi.x, dv.x, fma(-zi.y, dv.y, po[q].x));
+            } else {
+                zfma(po[q], zi, dv);
+            }
+            if (PGH >= 2) zfma(gr[q], zscal(zi2, (R)-1), dv);
+            if (PGH >= 3) zfma(he[q], zscal(zi3, (R)2), dv);
+        }
+    }
+}
+
 template <int CH, int PGH, bool IFC, bool IFD, bool MIXED, bool LAPR>
 __global__ void __launch_bounds__(kP2PWarps * 32) p2p_kernel(
     int lo, int hi, const int *__restrict__ nlist1,
@@ -743,55 +957,9 @@ __global__ void __launch_bounds__(kP2PWarps * 32) p2p_kernel(
                 __syncwarp();
                 if (act) {
 #pragma unroll 4
-                    for (int kk = g; kk < nst; kk += G) {
-                        R dx, dy;
-                        pos_diff(x, s_pos[kk], dx, dy);
-                        const R rr = dx * dx + dy * dy;
-                        // skipped pairs contribute exactly zero, without a branch
-                        const bool skip = PGH == 1 ? (rr <= th2) : (rr < th2);
-                        const R rrs = skip ? (R)1 : rr;
-                        const R ri = skip ? (R)0 : rcp_pair(rrs);
-                        R2 zi;
-                        zi.x = dx * ri;
-                        zi.y = -dy * ri;
-                        R2 zi2 = mk2<R2>(0.0, 0.0), zi3 = mk2<R2>(0.0, 0.0);
-                        if (PGH >= 2 || IFD) zi2 = zmul(zi, zi);
-                        if (PGH >= 3 && IFD) zi3 = zmul(zi2, zi);
-                        R rl = 0;
-                        if (IFC) rl = skip ? (R)0 : half_ln_pair(rrs);
-#pragma unroll
-                        for (int q = 0; q < CH; q++) {
-                            if (IFC) {
-                                const R2 qv = s_str[kk * kStr + q];
-                                if (LAPR) {
-                                    po[q].x = fma(rl, qv.x, po[q].x);
-                                    if (PGH >= 2) {
-                                        gr[q].x = fma(zi.x, qv.x, gr[q].x);
-                                        gr[q].y = fma(zi.y, qv.x, gr[q].y);
-                                    }
-                                    if (PGH >= 3) {
-                                        he[q].x = fma(-zi2.x, qv.x, he[q].x);
-                                        he[q].y = fma(-zi2.y, qv.x, he[q].y);
-                                    }
-                                } else {
-                                    po[q].x = fma(rl, qv.x, po[q].x);
-                                    po[q].y = fma(rl, qv.y, po[q].y);
-                                    if (PGH >= 2) zfma(gr[q], zi, qv);
-                                    if (PGH >= 3) zfma(he[q], zscal(zi2, (R)-1), qv);
-                                }
-                            }
-                            if (IFD) {
-                                const R2 dv = s_str[kk * kStr + (IFC ? CH : 0) + q];
-                                if (LAPR) {
-                                    po[q].x = fma(zi.x, dv.x, fma(-zi.y, dv.y, po[q].x));
-                                } else {
-                                    zfma(po[q], zi, dv);
-                                }
-                                if (PGH >= 2) zfma(gr[q], zscal(zi2, (R)-1), dv);
-                                if (PGH >= 3) zfma(he[q], zscal(zi3, (R)2), dv);
-                            }
-                        }
-                    }
+                    for (int kk = g; kk < nst; kk += G)
+                        p2p_pair<CH, PGH, IFC, IFD, MIXED, LAPR>(x, s_pos[kk], s_str + kk * kStr,
+                                                                 th2, po, gr, he);
                 }
             }
             // sum the lane groups
@@ -832,6 +1000,168 @@ __global__ void __launch_bounds__(kP2PWarps * 32) p2p_kernel(
     }
 }
 
+// Near field with the (target, source block) work flattened over the lanes.
+// A warp takes up to 32 targets of a box at a time; the staged sources are
+// cut into B blocks and the T * B (target, block) items are dealt to the
+// lanes round by round, each item summing its block into registers and
+// leaving the partial sums in shared memory, from where the target's lane
+// adds the B partials in block order.  B is chosen per box to minimise the
+// lane sweeps, so that a box of 19 targets keeps 30 of 32 lanes busy instead
+// of 19.  Deterministic: every sum has a fixed order.
+template <bool MIXED> struct FlatItems { static constexpr int value = MIXED ? 96 : 64; };
+
+template <int CH, int PGH>
+constexpr int flat_outputs() { return CH * (1 + (PGH >= 2 ? 1 : 0) + (PGH >= 3 ? 1 : 0)); }
+
+template <int CH, int PGH, bool IFC, bool IFD, bool MIXED>
+constexpr size_t p2p_flat_warp_bytes() {
+    return (size_t)kP2PStage * (16 + ((IFC ? CH : 0) + (IFD ? CH : 0)) * sizeof(typename Real<MIXED>::T2)) +
+           32 * 16 + (size_t)FlatItems<MIXED>::value * flat_outputs<CH, PGH>() *
+                          sizeof(typename Real<MIXED>::T2);
+}
+
+template <int CH, int PGH, bool IFC, bool IFD, bool MIXED, bool LAPR>
+__global__ void __launch_bounds__(kP2PWarps * 32) p2p_flat_kernel(
+    int lo, int hi, const int *__restrict__ nlist1,
+    const int *__restrict__ list1, const int *__restrict__ nchild,
+    int leaves, const int2 *__restrict__ sse,
+    const typename PosT<MIXED>::T *__restrict__ src,
+    const typename Real<MIXED>::T2 *__restrict__ chg,
+    const typename Real<MIXED>::T2 *__restrict__ dip, PointSet sset,
+    PointSet tset, const typename PosT<MIXED>::T *__restrict__ spos,
+    const typename PosT<MIXED>::T *__restrict__ tpos, int ndc, int c0,
+    double th2d) {
+    typedef typename Real<MIXED>::T R;
+    typedef typename Real<MIXED>::T2 R2;
+    typedef typename PosT<MIXED>::T PT;
+    constexpr int kStr = (IFC ? CH : 0) + (IFD ? CH : 0);
+    constexpr int kNo = flat_outputs<CH, PGH>();
+    constexpr int kItems = FlatItems<MIXED>::value;
+    constexpr size_t kWarpBytes = p2p_flat_warp_bytes<CH, PGH, IFC, IFD, MIXED>();
+    extern __shared__ __align__(16) unsigned char p2p_smem[];
+    const int lane = lane_id(), wib = threadIdx.x >> 5;
+    PT *s_pos = reinterpret_cast<PT *>(p2p_smem + (size_t)wib * kWarpBytes);
+    R2 *s_str = reinterpret_cast<R2 *>(s_pos + kP2PStage);
+    PT *s_tgt = reinterpret_cast<PT *>(s_str + kP2PStage * kStr);
+    R2 *part = reinterpret_cast<R2 *>(s_tgt + 32);
+    const R th2 = MIXED ? (R)fmax(th2d, 1.1754943508222875e-38) : (R)th2d;
+    for (int b = lo + warp_global(); b < hi; b += warp_count()) {
+        const int n1 = nlist1[b];
+        if (n1 == 0) continue;
+        if ((nchild[b] == 0) != (leaves != 0)) continue;
+        const int2 tr = tset.pgh > 0 ? tset.se[b] : make_int2(0, 0);
+        const int2 sr0 = sset.pgh > 0 ? sset.se[b] : make_int2(0, 0);
+        const int ntb = tr.y - tr.x, nsb = sr0.y - sr0.x, ntot = ntb + nsb;
+        if (ntot == 0) continue;
+        int jstart = 0, jcount = 0;  // lane e < n1 holds list-1 entry e
+        if (lane < n1) {
+            const int2 r = sse[list1[kMaxList1 * b + lane]];
+            jstart = r.x;
+            jcount = r.y - r.x;
+        }
+        int jofs = jcount;
+#pragma unroll
+        for (int d = 1; d < 16; d <<= 1) {
+            const int o = __shfl_up_sync(0xffffffffu, jofs, d);
+            if (lane >= d) jofs += o;
+        }
+        const int nsrc = __shfl_sync(0xffffffffu, jofs, n1 - 1);
+        jofs -= jcount;
+        if (nsrc == 0) continue;
+        const int nchunk = (ntot + 31) / 32, T0 = (ntot + nchunk - 1) / nchunk;
+        const int ns_eff = min(nsrc, kP2PStage);
+        for (int t0 = 0; t0 < ntot; t0 += T0) {
+            const int T = min(T0, ntot - t0);
+            __syncwarp();
+            if (lane < T) {
+                const int it = t0 + lane;
+                s_tgt[lane] = it < ntb ? tpos[tr.x + it] : spos[sr0.x + it - ntb];
+            }
+            int B = 1, best = 1 << 30;
+            for (int bb = 1; bb * T <= kItems; bb++) {
+                const int cost = ((T * bb + 31) >> 5) * ((ns_eff + bb - 1) / bb);
+                if (cost < best) {
+                    best = cost;
+                    B = bb;
+                }
+            }
+            const int nit = T * B;
+            R2 po[CH], gr[CH], he[CH];
+#pragma unroll
+            for (int q = 0; q < CH; q++) po[q] = gr[q] = he[q] = mk2<R2>(0.0, 0.0);
+            for (int s0 = 0; s0 < nsrc; s0 += kP2PStage) {
+                const int nst = min(kP2PStage, nsrc - s0);
+                __syncwarp();
+                for (int i0 = 0; i0 < nst; i0 += 32) {  // warp-uniform trip count
+                    const int i = i0 + lane;
+                    const int gi = s0 + i;
+                    int e = 0;
+                    for (int u = 1; u < n1; u++)
+                        if (__shfl_sync(0xffffffffu, jofs, u) <= gi) e = u;
+                    const int k = __shfl_sync(0xffffffffu, jstart, e) + gi -
+                                  __shfl_sync(0xffffffffu, jofs, e);
+                    if (i >= nst) continue;
+                    s_pos[i] = src[k];
+#pragma unroll
+                    for (int q = 0; q < CH; q++) {
+                        if (IFC) s_str[i * kStr + q] = chg[(size_t)k * ndc + c0 + q];
+                        if (IFD) s_str[i * kStr + (IFC ? CH : 0) + q] = dip[(size_t)k * ndc + c0 + q];
+                    }
+                }
+                __syncwarp();
+                const int sb = (nst + B - 1) / B;
+                for (int i = lane; i < nit; i += 32) {
+                    const int t = i % T, blk = i / T;
+                    const PT x = s_tgt[t];
+                    R2 apo[CH], agr[CH], ahe[CH];
+#pragma unroll
+                    for (int q = 0; q < CH; q++) apo[q] = agr[q] = ahe[q] = mk2<R2>(0.0, 0.0);
+                    const int j0 = blk * sb, j1 = min(nst, j0 + sb);
+#pragma unroll 4
+                    for (int kk = j0; kk < j1; kk++)
+                        p2p_pair<CH, PGH, IFC, IFD, MIXED, LAPR>(x, s_pos[kk], s_str + kk * kStr,
+                                                                 th2, apo, agr, ahe);
+                    R2 *pp = part + (size_t)i * kNo;
+#pragma unroll
+                    for (int q = 0; q < CH; q++) {
+                        pp[q] = apo[q];
+                        if (PGH >= 2) pp[CH + q] = agr[q];
+                        if (PGH >= 3) pp[2 * CH + q] = ahe[q];
+                    }
+                }
+                __syncwarp();
+                if (lane < T) {
+                    for (int blk = 0; blk < B; blk++) {
+                        const R2 *pp = part + (size_t)(lane + blk * T) * kNo;
+#pragma unroll
+                        for (int q = 0; q < CH; q++) {
+                            po[q] = zadd(po[q], pp[q]);
+                            if (PGH >= 2) gr[q] = zadd(gr[q], pp[CH + q]);
+                            if (PGH >= 3) he[q] = zadd(he[q], pp[2 * CH + q]);
+                        }
+                    }
+                }
+            }
+            if (lane < T) {
+                const int it = t0 + lane;
+                const bool is_t = it < ntb;
+                const int t = is_t ? tr.x + it : sr0.x + it - ntb;
+                const int pg = is_t ? tset.pgh : sset.pgh;
+                double2 *opot = is_t ? tset.pot : sset.pot;
+                double2 *ograd = is_t ? tset.grad : sset.grad;
+                double2 *ohess = is_t ? tset.hess : sset.hess;
+#pragma unroll
+                for (int q = 0; q < CH; q++) {
+                    const size_t o = (size_t)t * ndc + c0 + q;
+                    add_out(opot[o], po[q]);
+                    if (PGH >= 2 && pg >= 2) add_out(ograd[o], gr[q]);
+                    if (PGH >= 3 && pg >= 3) add_out(ohess[o], he[q]);
+                }
+            }
+        }
+    }
+}
+
 template <int CH, bool IFC, bool IFD, bool MIXED>
 constexpr size_t p2p_smem_bytes() {
     return (size_t)kP2PWarps * kP2PStage *
@@ -856,14 +1186,31 @@ void launch_p2p_t(const Tree &T, const CauchyProblem &P, int c0, double th2,
     const R2 *dip = MIXED ? (const R2 *)P.dipstr32 : (const R2 *)P.dipstr;
     const PT *spos = MIXED ? (const PT *)P.src_hl : (const PT *)P.src;
     const PT *tpos = MIXED ? (const PT *)P.trg_hl : (const PT *)P.tset.pos;
+    // Flattened items in the mixed mode, equal lane groups in FP64: measured
+    // on a B200 (10^7 + 10^7 uniform points, lfmm2d_st_cd_g) 5.56 against
+    // 5.75 ms mixed, 19.1 against 17.1 ms FP64, where the flattened form's
+    // larger register and shared-memory footprint costs occupancy.
+    // FMM2D_B200_P2P=flat / group overrides.
+    const char *mode = getenv("FMM2D_B200_P2P");
+    const bool flat = mode ? !strcmp(mode, "flat") : MIXED;
 #define FMM_P2P_CASE(IFC, IFD)                                                  \
     do {                                                                        \
-        constexpr size_t sm = p2p_smem_bytes<CH, IFC, IFD, MIXED>();            \
-        auto kern = p2p_kernel<CH, PGH, IFC, IFD, MIXED, LAPR>;                 \
-        raise_smem_limit(kern, (int)sm); \
-        kern<<<g, kP2PWarps * 32, sm, s>>>(lo, hi, n1, l1, nc, leaves, sse,     \
-                                          spos, chg, dip, P.sset, P.tset, spos, \
-                                          tpos, P.ndc, c0, th2);                \
+        if (flat) {                                                             \
+            constexpr size_t sm =                                               \
+                kP2PWarps * p2p_flat_warp_bytes<CH, PGH, IFC, IFD, MIXED>();    \
+            auto kern = p2p_flat_kernel<CH, PGH, IFC, IFD, MIXED, LAPR>;        \
+            raise_smem_limit(kern, sm);                                         \
+            kern<<<g, kP2PWarps * 32, sm, s>>>(lo, hi, n1, l1, nc, leaves, sse, \
+                                              spos, chg, dip, P.sset, P.tset,   \
+                                              spos, tpos, P.ndc, c0, th2);      \
+        } else {                                                                \
+            constexpr size_t sm = p2p_smem_bytes<CH, IFC, IFD, MIXED>();        \
+            auto kern = p2p_kernel<CH, PGH, IFC, IFD, MIXED, LAPR>;             \
+            raise_smem_limit(kern, sm);                                         \
+            kern<<<g, kP2PWarps * 32, sm, s>>>(lo, hi, n1, l1, nc, leaves, sse, \
+                                              spos, chg, dip, P.sset, P.tset,   \
+                                              spos, tpos, P.ndc, c0, th2);      \
+        }                                                                       \
     } while (0)
     if (P.ifcharge && P.ifdipole)
         FMM_P2P_CASE(true, true);
@@ -1568,11 +1915,39 @@ void downward_chunk(const Tree &T, const CauchyProblem &P, int c0,
         FMM_CHECK_LAUNCH();
     }
     prof_mark("l2l", s);
-    // steps 6-7: list-3 multipoles and local expansions at the points
-    for (const PointSet *set : {&P.tset, &P.sset}) {
-        if (set->pgh <= 0 || set->n <= 0) continue;
-        launch_eval_far<CH>(T, P, *set, set == &P.tset ? P.tleaf : P.sleaf, c0,
-                            mp, loc, s);
+    // steps 6-7: list-3 multipoles and local expansions at the points, in
+    // the near-field pass over the leaves when there is one
+    FarArgs fa;
+    fa.p = p;
+    fa.nlevels = L;
+    fa.level = T.level.get();
+    fa.centers = T.centers.get();
+    fa.bs = bs;
+    fa.nlist3 = T.nlist3.get();
+    fa.list3 = T.list3.get();
+    fa.mp = mp;
+    fa.loc = loc;
+    if (far_per_leaf(P)) {
+        const int pgh = std::max(P.sset.n > 0 ? P.sset.pgh : 0, P.tset.n > 0 ? P.tset.pgh : 0);
+        const int g = std::max(1, std::min((nb + kFarWarps - 1) / kFarWarps, kNumSM * 16));
+#define FMM_FAR_CASE(PG)                                                                 \
+    if (P.mixed)                                                                         \
+        far_leaf_kernel<CH, PG, true><<<g, kFarWarps * 32, 0, s>>>(                      \
+            nb, T.nchild.get(), fa, T.srcse.get(), P.sset, P.tset, P.ndc, c0);           \
+    else                                                                                 \
+        far_leaf_kernel<CH, PG, false><<<g, kFarWarps * 32, 0, s>>>(                     \
+            nb, T.nchild.get(), fa, T.srcse.get(), P.sset, P.tset, P.ndc, c0);
+        if (pgh == 1) { FMM_FAR_CASE(1) }
+        if (pgh == 2) { FMM_FAR_CASE(2) }
+        if (pgh == 3) { FMM_FAR_CASE(3) }
+#undef FMM_FAR_CASE
+        if (pgh > 0) FMM_CHECK_LAUNCH();
+    } else {
+        for (const PointSet *set : {&P.tset, &P.sset}) {
+            if (set->pgh <= 0 || set->n <= 0) continue;
+            launch_eval_far<CH>(T, P, *set, set == &P.tset ? P.tleaf : P.sleaf, c0,
+                                mp, loc, s);
+        }
     }
     prof_mark("m2p_l2p", s);
     // step 8: near field over list 1 (leaves, then any non-leaf box that
@@ -1665,7 +2040,7 @@ void cauchy_fmm(const Tree &T, const CauchyProblem &P0, cudaStream_t s) {
     CauchyProblem P = P0;
     // leaf of every sorted point, for the per-point far-field evaluation
     DevBuf<int> sleaf(std::max(P.sset.n, 1), s), tleaf(std::max(P.tset.n, 1), s);
-    {
+    if (!far_per_leaf(P)) {
         const int blocks = std::max(1, std::min((T.nboxes + 255) / 256, kNumSM * 8));
         if (P.sset.pgh > 0 && P.sset.n > 0) {
             leaf_of_kernel<<<blocks, 256, 0, s>>>(T.nboxes, T.nchild.get(), T.srcse.get(), sleaf.get());

@@ -85,30 +85,60 @@ __global__ void __launch_bounds__(256) path_key_kernel(
     }
 }
 
-// Input order inside every leaf of at most 32 points: one warp per leaf
-// sorts the leaf's input indices (bitonic network over the lanes).
+// Input order inside every leaf of at most kLeafSort points: one warp per
+// leaf sorts the leaf's input indices with a bitonic network, over the
+// lanes' registers for up to 32 points, in shared memory for more.
+constexpr int kLeafSort = 256;
+
 __global__ void __launch_bounds__(256) leaf_order_kernel(
     int nb, const int *__restrict__ nch, const int2 *__restrict__ rng,
     const uint32_t *__restrict__ idx, int *__restrict__ perm) {
+    __shared__ uint32_t sh_all[8][kLeafSort];
     const int lane = threadIdx.x & 31;
+    uint32_t *sh = sh_all[threadIdx.x >> 5];
     const int warps = gridDim.x * (blockDim.x >> 5);
     for (int b = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); b < nb; b += warps) {
         if (nch[b] != 0) continue;
         const int2 r = rng[b];
         const int cnt = r.y - r.x;
         if (cnt <= 0) continue;
-        uint32_t v = lane < cnt ? idx[r.x + lane] : 0xffffffffu;
-        if (cnt > 1) {
+        if (cnt <= 32) {
+            uint32_t v = lane < cnt ? idx[r.x + lane] : 0xffffffffu;
+            if (cnt > 1) {
 #pragma unroll
-            for (int k = 2; k <= 32; k <<= 1)
+                for (int k = 2; k <= 32; k <<= 1)
 #pragma unroll
-                for (int j = k >> 1; j > 0; j >>= 1) {
-                    const uint32_t o = __shfl_xor_sync(0xffffffffu, v, j);
-                    const bool up = (lane & k) == 0, low = (lane & j) == 0;
-                    v = (low == up) ? min(v, o) : max(v, o);
-                }
+                    for (int j = k >> 1; j > 0; j >>= 1) {
+                        const uint32_t o = __shfl_xor_sync(0xffffffffu, v, j);
+                        const bool up = (lane & k) == 0, low = (lane & j) == 0;
+                        v = (low == up) ? min(v, o) : max(v, o);
+                    }
+            }
+            if (lane < cnt) perm[r.x + lane] = (int)v;
+            continue;
         }
-        if (lane < cnt) perm[r.x + lane] = (int)v;
+        // 33 .. kLeafSort points (the caller guarantees the bound)
+        int n2 = 64;
+        while (n2 < cnt) n2 <<= 1;
+        for (int i = lane; i < n2; i += 32) sh[i] = i < cnt ? idx[r.x + i] : 0xffffffffu;
+        __syncwarp();
+        for (int k = 2; k <= n2; k <<= 1)
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int i = lane; i < n2; i += 32) {
+                    const int ij = i ^ j;
+                    if (ij > i) {
+                        const uint32_t a = sh[i], c = sh[ij];
+                        const bool up = (i & k) == 0;
+                        if ((a > c) == up) {
+                            sh[i] = c;
+                            sh[ij] = a;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        for (int i = lane; i < cnt; i += 32) perm[r.x + i] = (int)sh[i];
+        __syncwarp();
     }
 }
 
@@ -625,7 +655,7 @@ struct Builder {
         int *bp = big.get();
         for_each(nb, s, [=] __device__(int64_t i) {
             const int2 r = rp[i];
-            if (nch[i] == 0 && r.y - r.x > 32) atomicExch(bp, 1);
+            if (nch[i] == 0 && r.y - r.x > kLeafSort) atomicExch(bp, 1);
         });
         if (read_scalar(bp, s) == 0) {
             const int blocks = std::max(1, std::min((nb + 7) / 8, kNumSM * 16));
@@ -633,8 +663,8 @@ struct Builder {
             FMM_CHECK_LAUNCH();
             return;
         }
-        // some leaf holds more than 32 points: stable sort of the input
-        // order by the start of each point's leaf
+        // some leaf holds more than kLeafSort points: stable sort of the
+        // input order by the start of each point's leaf
         DevBuf<uint32_t> keys(n, s), vals(n, s), kt(n, s), vt(n, s);
         uint32_t *kp = keys.get(), *vp = vals.get();
         for_each(n, s, [=] __device__(int64_t k) {

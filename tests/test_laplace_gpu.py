@@ -118,3 +118,16 @@ def test_against_direct_sum(glib):
             0, m, W._p(s), 2, W._p(pot), W._p(grad), None, 1e-300)
         assert W.rel_err(got["pot"][:m], pot) < 10 * eps
         assert W.rel_err(got["grad"][:m], grad) < 100 * eps
+
+
+@pytest.mark.parametrize("p2p", ["flat", "group"])
+@pytest.mark.parametrize("far", ["leaf", "point"])
+@pytest.mark.parametrize("variant", ["st_cd_h", "st_c_g", "t_d_p"])
+def test_pass_forms_agree(glib, monkeypatch, p2p, far, variant):
+    """Every form of the evaluation passes (near field with flattened or
+    grouped lanes; far field per leaf or per point) gives the reference's
+    values, on a tree with list-3 and list-4 boxes."""
+    monkeypatch.setenv("FMM2D_B200_P2P", p2p)
+    monkeypatch.setenv("FMM2D_B200_FAR", far)
+    src, trg, q, d, v = inputs(20000, 8000, 51, "starfish")
+    compare(glib, "l", variant, 1e-9, src, trg, q, d, v, TOL_FP64)

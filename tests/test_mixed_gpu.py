@@ -108,3 +108,19 @@ def test_mixed_multichannel_matches_fp64(mlib, fam, nd, m2l, monkeypatch):
     assert W.rel_err(mixed.grad, ref.grad) < 1e-6
     if fam == "l":  # Cauchy potentials carry the branch term of log z
         assert W.rel_err(mixed.pottarg, ref.pottarg) < 1e-6
+
+
+@pytest.mark.parametrize("p2p", ["flat", "group"])
+@pytest.mark.parametrize("far", ["leaf", "point"])
+def test_mixed_pass_forms(mlib, monkeypatch, p2p, far):
+    """Both near-field forms and both far-field forms of the mixed mode stay
+    within eps of the reference FMM (starfish tree: list 3 and list 4)."""
+    monkeypatch.setenv("FMM2D_B200_P2P", p2p)
+    monkeypatch.setenv("FMM2D_B200_FAR", far)
+    src, trg, q, d, v = inputs(30000, 10000, 17, "starfish")
+    got, ier = W.call(mlib, "l", "st_cd_h", 1e-6, src, q, d, v, trg)
+    want, ier2 = W.call(refimpl.ref(), "l", "st_cd_h", 1e-6, src, q, d, v, trg)
+    assert ier == 0 and ier2 == 0
+    for k in want:
+        tol = 1e-5 if k.startswith("hess") else 1e-6
+        assert W.rel_err(got[k], want[k]) <= tol, k

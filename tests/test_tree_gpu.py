@@ -27,6 +27,10 @@ CASES = {
                             ps.blobs(5000, 15, nblob=4, sigma=1e-5), 10, 0),
     # enough points per set for the multi-block sort passes
     "uniform_300000": lambda: (ps.uniform(300000, 16), ps.uniform(200000, 17), 24, 0),
+    # target leaves of 33..256 points (shared-memory leaf sort) and of more
+    # than 256 points (the global sort)
+    "targets_per_leaf_40": lambda: (ps.uniform(20000, 18), ps.uniform(100000, 19), 15, 0),
+    "targets_per_leaf_1000": lambda: (ps.uniform(1000, 20), ps.uniform(150000, 21), 15, 0),
 }
 
 
