@@ -252,9 +252,97 @@ def cfmm2d(*, eps, sources, charges=None, dipstr=None, targets=None, pg=0, pgt=0
                 dipvec=None, targets=targets, pg=pg, pgt=pgt, nd=nd)
 
 
+class Plan:
+    """Resident geometry for repeated lfmm2d / cfmm2d evaluations on the same
+    points (plan.cu): the tree, its lists and the sorted points stay on the
+    device; each eval() only brings new strengths.  Outputs as lfmm2d /
+    cfmm2d return them."""
+
+    def __init__(self, kernel="l", *, eps, sources, targets=None, charges=True, dipoles=False,
+                 pg=1, pgt=0, nd=1):
+        L = lib()
+        L.fmm2d_b200_plan_create.argtypes = [_I, _I, ctypes.c_double, _I, _P, _I, _I, _I, _I,
+                                             _P, _I, ctypes.POINTER(_P)]
+        L.fmm2d_b200_plan_eval.argtypes = [_P] * 10
+        L.fmm2d_b200_plan_destroy.argtypes = [_P]
+        self.kernel, self.nd, self.pg = kernel, nd, pg
+        sources = np.asarray(sources, dtype=np.float64)
+        self.ns = sources.shape[1]
+        src = _as_f(sources, np.float64)
+        if targets is not None:
+            trg = _as_f(targets, np.float64)
+            self.nt = trg.shape[1]
+        else:
+            trg, self.nt, pgt = None, 0, 0
+        self.pgt = pgt
+        self.ifcharge, self.ifdipole = int(bool(charges)), int(bool(dipoles))
+        h = _P()
+        ier = L.fmm2d_b200_plan_create({"l": 0, "c": 1}[kernel], nd, eps, self.ns, _ptr(src),
+                                       self.ifcharge, self.ifdipole, pg, self.nt, _ptr(trg),
+                                       pgt, ctypes.byref(h))
+        _check(ier, "fmm2d_b200_plan_create")
+        self._h = h
+
+    def eval(self, charges=None, dipstr=None, dipvec=None):
+        nd, ns, nt = self.nd, self.ns, self.nt
+        q = _as_f(charges, np.complex128) if self.ifcharge else None
+        d = _as_f(dipstr, np.complex128) if self.ifdipole else None
+        v = _as_f(dipvec, np.float64) if (self.ifdipole and self.kernel == "l") else None
+        gc, hc = (1, 1) if self.kernel == "c" else (2, 3)
+
+        def alloc(n, comps, need):
+            if not need or n == 0:
+                return None
+            shape = (nd, n) if comps == 1 else (nd, comps, n)
+            return np.zeros(shape, np.complex128, order="F")
+
+        pg, pgt = self.pg, self.pgt
+        outs = [alloc(ns, 1, pg >= 1), alloc(ns, gc, pg >= 2), alloc(ns, hc, pg >= 3),
+                alloc(nt, 1, pgt >= 1), alloc(nt, gc, pgt >= 2), alloc(nt, hc, pgt >= 3)]
+        ier = lib().fmm2d_b200_plan_eval(self._h, _ptr(q), _ptr(d), _ptr(v),
+                                         *[_ptr(o) for o in outs])
+        _check(ier, "fmm2d_b200_plan_eval")
+        out = Output()
+        shaped = (lambda a: a if a is None or nd > 1 else a[0])
+        out.pot, out.grad, out.hess, out.pottarg, out.gradtarg, out.hesstarg = map(shaped, outs)
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fmm2d_b200_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 # ---------------------------------------------------------------------------
 # Request loop (serve.cu): continuous admission of independent evaluations.
 # ---------------------------------------------------------------------------
+def autotune(kernel="l", *, eps, ns, nt=0, sources=None, targets=None, charges=True,
+             dipoles=False, pg=1, pgt=0):
+    """Autotunes the mixed-precision path for the order of `eps` on a
+    workload of this shape (the given points, or seeded uniform ones) and
+    keeps the choice for later calls.  Returns (leaf capacity, M2L form,
+    ms per evaluation)."""
+    L = lib()
+    L.fmm2d_b200_autotune.argtypes = [_I, ctypes.c_double, _I, _P, _I, _P, _I, _I, _I, _I,
+                                      _P, _P, _P]
+    src = None if sources is None else _as_f(sources, np.float64)
+    trg = None if targets is None else _as_f(targets, np.float64)
+    nd_, fm_, ms_ = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_double(0)
+    ier = L.fmm2d_b200_autotune({"l": 0, "c": 1}[kernel], eps, ns,
+                                None if src is None else _ptr(src), nt,
+                                None if trg is None else _ptr(trg), int(bool(charges)),
+                                int(bool(dipoles)), pg, pgt, ctypes.byref(nd_),
+                                ctypes.byref(fm_), ctypes.byref(ms_))
+    _check(ier, "fmm2d_b200_autotune")
+    return nd_.value, fm_.value, ms_.value
+
+
 class Request(ctypes.Structure):
     """fmm2d_b200_request: the guru drivers' arguments of one evaluation."""
     _fields_ = [("kernel", _I), ("nd", _I), ("eps", ctypes.c_double),

@@ -154,54 +154,70 @@ void set_mixed_leaf_capacity(int p, int ndiv) {
     if (ndiv > 0) g_mixed_default_off = false;
 }
 
-namespace {
-
-void run_laplace_family(const FmmCall &c, CallCtx &ctx) {
-    cudaStream_t s = ctx.stream();
+// Geometry of a Laplace / Cauchy evaluation: the tree, its lists and the
+// points in tree order.  It depends on the points, eps and the precision
+// only, so a plan keeps it on the device for many evaluations.
+void laplace_geometry(const FmmCall &c, bool on_dev, cudaStream_t s, LapGeometry &G) {
     const bool lap = c.kernel == kLaplace;
-    const int nd = c.nd, ndc = lap ? 2 * nd : nd;
-    const int ns = c.ns, nt = c.nt;
-    const bool on_dev = is_device_ptr(c.sources);
-    prof_begin(s);
-    // ---- inputs ----
-    InBuf<double2> src_in, trg_in, chg_in, dip_in;
+    G.lap = lap;
+    G.nd = c.nd;
+    G.ndc = lap ? 2 * c.nd : c.nd;
+    G.ns = c.ns;
+    G.nt = c.nt;
+    G.eps = c.eps;
+    G.p = laplace_nterms(c.eps);
+    // mixed precision for eps >= 1e-6 unless all-FP64 is requested
+    const int prec = c.precision;
+    G.mixed = prec == kPrecMixed || (prec == kPrecAuto && c.eps >= 0.5e-6);
+    InBuf<double2> src_in, trg_in;
+    src_in.set(c.sources, c.ns, on_dev, s);
+    trg_in.set(c.nt > 0 ? c.targ : nullptr, c.nt, on_dev, s);
+    prof_mark("h2d", s);
+    int ndiv = c.ndiv >= 0 ? c.ndiv : leaf_capacity(c.eps, c.ns, c.nt);
+    // (complex-Laplace only: the Cauchy potential's far field takes the
+    // complex q log z, whose branch terms depend on the tree, so the Cauchy
+    // form keeps the reference's tree to reproduce the reference's values)
+    if (c.ndiv < 0 && G.mixed && lap) ndiv = mixed_leaf_capacity(G.p, ndiv);
+    const int idivflag = c.ndiv >= 0 ? c.idivflag : 0;
+    build_tree(src_in.ptr, c.ns, trg_in.ptr, c.nt, ndiv, idivflag, kMaxLevels, s, G.T);
+    compute_lists(G.T, s);
+    prof_mark("lists", s);
+    const Tree &T = G.T;
+    G.src_s.alloc(c.ns, s);
+    G.trg_s.alloc(std::max(c.nt, 1), s);
+    const int *perm = T.isrc.get();
+    const double2 *sp = src_in.ptr;
+    double2 *so = G.src_s.get();
+    for_each(c.ns, s, [=] __device__(int64_t k) { so[k] = sp[perm[k]]; });
+    if (c.nt > 0) {
+        const int *pt = T.itarg.get();
+        const double2 *tp = trg_in.ptr;
+        double2 *to = G.trg_s.get();
+        for_each(c.nt, s, [=] __device__(int64_t k) { to[k] = tp[pt[k]]; });
+    }
+    // thresh = boxsize(0) * 2^-51 (c_translation/src/cfmm2d.c:994)
+    G.thresh = T.boxsize[0] * std::ldexp(1.0, -51);
+    // (the caller's host copies are released on this stream)
+}
+
+// One evaluation over a geometry: strengths into tree order, the FMM
+// passes, outputs back to input order in the caller's layout.  Only the
+// strength and output pointers and the flags of `c` are read.
+void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaStream_t s) {
+    const bool lap = G.lap;
+    const int nd = G.nd, ndc = G.ndc, ns = G.ns, nt = G.nt;
+    const Tree &T = G.T;
+    InBuf<double2> chg_in, dip_in;
     InBuf<double> dv_in;
-    src_in.set(c.sources, ns, on_dev, s);
-    trg_in.set(nt > 0 ? c.targ : nullptr, nt, on_dev, s);
     if (c.ifcharge) chg_in.set(c.charge, (size_t)nd * ns, on_dev, s);
     if (c.ifdipole) {
         dip_in.set(c.dipstr, (size_t)nd * ns, on_dev, s);
         if (lap) dv_in.set(c.dipvec, (size_t)2 * nd * ns, on_dev, s);
     }
-    prof_mark("h2d", s);
-    // ---- tree ----
-    // mixed precision for eps >= 1e-6 unless all-FP64 is requested
-    const int prec = c.precision;
-    const bool mixed = prec == kPrecMixed || (prec == kPrecAuto && c.eps >= 0.5e-6);
-    int ndiv = c.ndiv >= 0 ? c.ndiv : leaf_capacity(c.eps, ns, nt);
-    // (complex-Laplace only: the Cauchy potential's far field takes the
-    // complex q log z, whose branch terms depend on the tree, so the Cauchy
-    // form keeps the reference's tree to reproduce the reference's values)
-    if (c.ndiv < 0 && mixed && lap) ndiv = mixed_leaf_capacity(laplace_nterms(c.eps), ndiv);
-    const int idivflag = c.ndiv >= 0 ? c.idivflag : 0;
-    Tree T;
-    build_tree(src_in.ptr, ns, trg_in.ptr, nt, ndiv, idivflag, kMaxLevels, s, T);
-    compute_lists(T, s);
-    prof_mark("lists", s);
-    // ---- gather into tree order ----
-    DevBuf<double2> src_s(ns, s), trg_s(std::max(nt, 1), s);
+    // ---- strengths into tree order ----
     DevBuf<double2> chg_s, dip_s;
     {
         const int *perm = T.isrc.get();
-        const double2 *sp = src_in.ptr;
-        double2 *so = src_s.get();
-        for_each(ns, s, [=] __device__(int64_t k) { so[k] = sp[perm[k]]; });
-        if (nt > 0) {
-            const int *pt = T.itarg.get();
-            const double2 *tp = trg_in.ptr;
-            double2 *to = trg_s.get();
-            for_each(nt, s, [=] __device__(int64_t k) { to[k] = tp[pt[k]]; });
-        }
         if (c.ifcharge) {
             chg_s.alloc((size_t)ns * ndc, s);
             const double2 *q = chg_in.ptr;
@@ -243,7 +259,6 @@ void run_laplace_family(const FmmCall &c, CallCtx &ctx) {
         }
     }
     prof_mark("gather", s);
-    src_in.own.release();
     chg_in.own.release();
     dip_in.own.release();
     dv_in.own.release();
@@ -262,30 +277,29 @@ void run_laplace_family(const FmmCall &c, CallCtx &ctx) {
     mk(thess, nt, tpgh >= 3);
     CauchyProblem P;
     P.ndc = ndc;
-    P.p = laplace_nterms(c.eps);
+    P.p = G.p;
     P.ifcharge = c.ifcharge;
     P.ifdipole = c.ifdipole;
-    P.src = src_s.get();
+    P.src = G.src_s.get();
     P.charge = chg_s.get();
     P.dipstr = dip_s.get();
-    P.sset.pos = src_s.get();
+    P.sset.pos = G.src_s.get();
     P.sset.se = T.srcse.get();
     P.sset.n = ns;
     P.sset.pgh = spgh;
     P.sset.pot = spot.get();
     P.sset.grad = sgrad.get();
     P.sset.hess = shess.get();
-    P.tset.pos = trg_s.get();
+    P.tset.pos = G.trg_s.get();
     P.tset.se = T.trgse.get();
     P.tset.n = nt;
     P.tset.pgh = tpgh;
     P.tset.pot = tpot.get();
     P.tset.grad = tgrad.get();
     P.tset.hess = thess.get();
-    // thresh = boxsize(0) * 2^-51 (c_translation/src/cfmm2d.c:994)
-    P.thresh = T.boxsize[0] * std::ldexp(1.0, -51);
+    P.thresh = G.thresh;
     P.ifnear = c.ifnear;
-    P.mixed = mixed;
+    P.mixed = G.mixed;
     P.real_charge = lap;
     cauchy_fmm(T, P, s);
     // ---- back to input order, in the caller's layout ----
@@ -338,9 +352,20 @@ void run_laplace_family(const FmmCall &c, CallCtx &ctx) {
     unsort(nt, T.itarg.get(), tpgh, tpot, tgrad, thess, c.pottarg, c.gradtarg,
            c.hesstarg);
     prof_mark("scatter_d2h", s);
-    prof_end(s);
     if (c.timeinfo)
         for (int k = 0; k < 8; k++) c.timeinfo[k] = 0.0;
+}
+
+namespace {
+
+void run_laplace_family(const FmmCall &c, CallCtx &ctx) {
+    cudaStream_t s = ctx.stream();
+    const bool on_dev = is_device_ptr(c.sources);
+    prof_begin(s);
+    LapGeometry G;
+    laplace_geometry(c, on_dev, s, G);
+    laplace_evaluate(c, G, on_dev, s);
+    prof_end(s);
 }
 
 

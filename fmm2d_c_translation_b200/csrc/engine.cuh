@@ -2,6 +2,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "tree.cuh"
 
 namespace fmm2d {
 
@@ -37,6 +38,20 @@ struct FmmCall {
     double *timeinfo = nullptr;  // 8 entries, optional
     int precision = kPrecAuto;
 };
+
+// Geometry of a Laplace / Cauchy evaluation (tree, lists, points in tree
+// order); laplace_geometry builds it from the positions of `c` (host or
+// device arrays, on_dev saying which), laplace_evaluate runs one evaluation
+// over it with the strengths and outputs of `c`.
+struct LapGeometry {
+    bool lap = true, mixed = false;
+    int nd = 1, ndc = 2, ns = 0, nt = 0, p = 0;
+    double eps = 0, thresh = 0;
+    Tree T;
+    DevBuf<double2> src_s, trg_s;
+};
+void laplace_geometry(const FmmCall &c, bool on_dev, cudaStream_t s, LapGeometry &G);
+void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaStream_t s);
 
 // Runs the evaluation on the calling thread's current device; returns the
 // reference's ier (0 ok, 4 failure) after recording any error message.

@@ -63,6 +63,11 @@ bool m2l_tensor_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp,
 bool m2l_fp32(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 *loc,
               cudaStream_t s);
 
+// Forms of the mixed-mode M2L, selectable per expansion order.
+enum M2LForm { kM2LWindow = 0, kM2LTile = 1, kM2LSimt = 2 };
+int m2l_form(int p);
+void set_m2l_form(int p, int form);
+
 // M2L of the mixed mode over runs of same-row boxes with shifted tensor-core
 // windows (m2l_window.cu), for the target levels whose runs are dense
 // enough; returns the set of target levels it evaluated (bit l = level l),

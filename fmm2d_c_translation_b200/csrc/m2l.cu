@@ -25,6 +25,7 @@
 #include "tc_common.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <mutex>
 #include <stdlib.h>
@@ -936,16 +937,32 @@ bool m2l_tensor_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp,
     return false;
 }
 
+namespace {
+std::atomic<int> g_m2l_form[128];
+}
+
+// Form of the mixed-mode M2L for order p: FMM2D_B200_M2L ("simt", "tile"),
+// else the setting for the order (fmm2d_b200_set_m2l_form, the autotuner),
+// else windows on the tensor cores for the dense levels with slot tables
+// for the rest.
+int m2l_form(int p) {
+    const char *mode = getenv("FMM2D_B200_M2L");
+    if (mode && !strcmp(mode, "simt")) return kM2LSimt;
+    if (mode && !strcmp(mode, "tile")) return kM2LTile;
+    return (p >= 0 && p < 128) ? g_m2l_form[p].load() : kM2LWindow;
+}
+
+void set_m2l_form(int p, int form) {
+    if (p >= 0 && p < 128) g_m2l_form[p].store(form);
+}
+
 bool m2l_fp32(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 *loc,
               cudaStream_t s) {
     const int L = T.nlevels, p = P.p;
     if (L < 2 || p + 1 > 20) return false;
-    // FMM2D_B200_M2L: "simt" = slot tables on the CUDA cores, "tile" =
-    // slot tables on the tensor cores only, default = windows on the
-    // tensor cores for the dense levels and slot tables for the rest
-    const char *mode = getenv("FMM2D_B200_M2L");
-    const bool simt = mode && !strcmp(mode, "simt");
-    const bool tile_only = mode && !strcmp(mode, "tile");
+    const int form = m2l_form(p);
+    const bool simt = form == kM2LSimt;
+    const bool tile_only = form == kM2LTile;
     const int CH = P.ndc >= 2 ? 2 : 1;
     // FP32 copy of the multipoles of levels >= 2
     const int lo = T.lstart[2];

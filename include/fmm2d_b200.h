@@ -671,6 +671,48 @@ int fmm2d_b200_leaf_capacity(double eps, int ns, int nt);
  * second function returns the capacity a mixed call at eps would use. */
 int fmm2d_b200_set_leaf_capacity(int nterms, int ndiv);
 int fmm2d_b200_mixed_leaf_capacity(double eps, int ns, int nt);
+/* Form of the mixed-mode M2L for order nterms: 0 tensor-core windows on the
+ * dense levels and tensor-core slot tables on the rest (default), 1 slot
+ * tables on the tensor cores only, 2 slot tables on the CUDA cores (FP32).
+ * FMM2D_B200_M2L=tile|simt overrides. */
+int fmm2d_b200_set_m2l_form(int nterms, int form);
+int fmm2d_b200_m2l_form(int nterms);
+/* Autotuner of the mixed-precision path for the order of eps: times full
+ * evaluations (kernel 0 = lfmm2d, 1 = cfmm2d; nd = 1; the given flags) of
+ * ns sources and nt targets -- the caller's points (host or device arrays,
+ * 2 x n), or seeded uniform points in [0,1]^2 where a pointer is null --
+ * over leaf capacities {12 .. 64} and the M2L forms above, and keeps the
+ * fastest pair for that order (fmm2d_b200_set_leaf_capacity /
+ * fmm2d_b200_set_m2l_form; the leaf capacity applies to lfmm2d, whose
+ * mixed mode is free of the reference's tree).  Returns 0 and the choice
+ * with its time per evaluation in ms, or 4. */
+int fmm2d_b200_autotune(int kernel, double eps, int ns, const double *sources,
+                        int nt, const double *targ, int ifcharge,
+                        int ifdipole, int ifpgh, int ifpghtarg,
+                        int *best_ndiv, int *best_form, double *best_ms);
+
+/* Resident geometry (no counterpart in the reference): a plan keeps the
+ * tree, its lists and the points in tree order of one lfmm2d (kernel 0) or
+ * cfmm2d (kernel 1) problem on the device -- the geometry the drivers
+ * rebuild on every call -- so that evaluating new strengths on the same
+ * points (an iterative solver's operator applications) skips the tree.
+ * Arguments as the guru drivers (src/laplace/lfmm2d.f:29,
+ * src/laplace/cfmm2d.f:23) without the strengths and outputs; eps and the
+ * precision policy in force at creation are fixed.  plan_eval takes the
+ * strengths (charge and dipstr as (nd, ns) complex, dipvec (nd, 2, ns))
+ * and overwrites the outputs in the guru drivers' layouts; host or device
+ * arrays.  A plan is used on the device it was made on; evaluations may
+ * run from several threads at once.  Each returns 0 or 4. */
+int fmm2d_b200_plan_create(int kernel, int nd, double eps, int ns,
+                           const double *sources, int ifcharge, int ifdipole,
+                           int ifpgh, int nt, const double *targ,
+                           int ifpghtarg, void **plan);
+int fmm2d_b200_plan_eval(void *plan, const double _Complex *charge,
+                         const double _Complex *dipstr, const double *dipvec,
+                         double _Complex *pot, double _Complex *grad,
+                         double _Complex *hess, double _Complex *pottarg,
+                         double _Complex *gradtarg, double _Complex *hesstarg);
+int fmm2d_b200_plan_destroy(void *plan);
 
 /* Direct sums on the GPU, incrementing the outputs (the reference's
  * l2d_direct* / c2d_direct* kernels, src/laplace/lapkernels2d.f,
