@@ -266,6 +266,8 @@ def main():
     ap.add_argument("--cpu-threads", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other configurations (c1, c3, c4)")
     ap.add_argument("--serve-requests", type=int, default=2000)
     ap.add_argument("--serve-slots", type=int, default=6)
     ap.add_argument("--serve-budget-gb", type=float, default=120.0)
@@ -489,6 +491,11 @@ def main():
         roof["phase_ms"] = {k: round(v_, 4) for k, v_ in times.items()}
         roof["counts"] = counts
 
+    configs = None
+    if not args.no_configs and ws == 1:
+        configs = measure_configs(fm, L, args)
+        L.fmm2d_b200_set_precision(prec_code[args.precision])
+
     serving = None
     if args.serve_requests > 0:
         L.fmm2d_b200_reset_stream()
@@ -512,7 +519,7 @@ def main():
                    "l2": "inputs 0.8 GB > L2; no flush"},
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": nlaunch, "clocks": clk, "fp64_plain": fp64,
-        "accuracy": acc, "serving": serving,
+        "accuracy": acc, "serving": serving, "configs": configs,
     }
     print(json.dumps(line))
     return 0
@@ -611,6 +618,163 @@ def measure_serving(fm, args):
                                "p50_ms": float(np.percentile(lat1, 50))},
         "points": "N log-uniform [1e3, 1e6], uniform or Gaussian blobs, host arrays",
     }
+
+
+def measure_configs(fm, L, args):
+    """The other configurations the reference's FMM is quoted on, each timed
+    device-resident through the C ABI (CUDA events, 3 warm-up + 3 timed
+    calls) with its accuracy against the GPU FP64 direct sum on sampled
+    points:
+      c1 lfmm2d_s_c_g, 1e5 uniform sources, eps 1e-6 (with the reference's
+         C translation on one host core for the same call);
+      c3 lfmm2d_st_d_p on the starfish r = 1 + 0.3 cos 5t: 4e6 sources with
+         outward normals as dipole vectors and real N(0,1) dipole strengths,
+         4e6 targets at normal distance 10^U[-3,-1], eps 1e-9 (FP64);
+      c4 hfmm2d_s_cd_p, 2e6 uniform sources, zk = 200, eps 1e-6 (FP64)."""
+    import torch
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.current_stream()
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    ptr = lambda x: ctypes.c_void_p(x.data_ptr())
+    ier = ctypes.c_int(0)
+    rel = lambda a, b: float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
+    sys.path.insert(0, os.path.join(REPO, "tests"))
+    import pointsets as ps
+
+    def timed(f, reps=3, warm=3):
+        for _ in range(warm):
+            f()
+        torch.cuda.synchronize()
+        L.fmm2d_b200_set_profiling(1)
+        buf = ctypes.create_string_buffer(4096)
+        ms = []
+        for _ in range(reps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            f()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        L.fmm2d_b200_last_profile(buf, len(buf))
+        L.fmm2d_b200_set_profiling(0)
+        prof = parse_profile(buf.value.decode())
+        return min(ms), prof
+
+    def check():
+        if ier.value != 0:
+            raise RuntimeError(fm.last_error())
+
+    out = {}
+    L.fmm2d_b200_set_precision(0)
+    # ---- c1 ----
+    rng = np.random.default_rng(101)
+    ns = 100_000
+    src = rng.random((ns, 2))
+    q = rng.standard_normal(ns) + 1j * rng.standard_normal(ns)
+    d_src, d_q = T(src), T(q.view(np.float64))
+    d_pot = torch.zeros(2 * ns, dtype=torch.float64, device=dev)
+    d_grad = torch.zeros(4 * ns, dtype=torch.float64, device=dev)
+    eps = ctypes.c_double(1e-6)
+    cns = ctypes.c_int(ns)
+
+    def c1():
+        L.lfmm2d_s_c_g_(ctypes.byref(eps), ctypes.byref(cns), ptr(d_src), ptr(d_q), ptr(d_pot),
+                        ptr(d_grad), ctypes.byref(ier))
+        check()
+
+    ms, prof = timed(c1)
+    m = 1000
+    sub = T(src[:m])
+    pot = torch.zeros(2 * m, dtype=torch.float64, device=dev)
+    grad = torch.zeros(4 * m, dtype=torch.float64, device=dev)
+    # (thresh^2 must stay above zero to skip each sampled source's own pair)
+    L.fmm2d_b200_l2d_direct(1, ns, ptr(d_src), 1, ptr(d_q), 0, None, None, m, ptr(sub), 2,
+                            ptr(pot), ptr(grad), None, ctypes.c_double(1e-150))
+    torch.cuda.synchronize()
+    c1r = {"workload": "lfmm2d_s_c_g uniform 1e5 eps 1e-6 (auto: mixed)", "ms": ms,
+           "points_s": ns / (ms * 1e-3),
+           "pot_rel_l2": rel(d_pot.view(-1, 2)[:m], pot.view(-1, 2)),
+           "grad_rel_l2": rel(d_grad.view(-1, 4)[:m], grad.view(-1, 4)),
+           "accuracy_sample": f"{m} sources vs GPU FP64 direct sum"}
+    import refimpl
+    if refimpl.have_ref():
+        R = refimpl.ref()
+        hp, hg = np.zeros(ns, complex), np.zeros((ns, 2), complex)
+        t0 = time.perf_counter()
+        R.lfmm2d_s_c_g_(ctypes.byref(eps), ctypes.byref(cns), src.ctypes.data_as(P),
+                        q.ctypes.data_as(P), hp.ctypes.data_as(P), hg.ctypes.data_as(P),
+                        ctypes.byref(ier))
+        tr = time.perf_counter() - t0
+        c1r["reference_1core_ms"] = tr * 1e3
+        c1r["vs_reference_1core"] = tr * 1e3 / ms
+        c1r["pot_rel_l2_vs_reference"] = float(np.linalg.norm(
+            d_pot.view(-1, 2).cpu().numpy().view(complex).ravel() - hp) / np.linalg.norm(hp))
+    out["c1"] = c1r
+    # ---- c3 ----
+    n3 = 4_000_000
+    x, nrm = ps.starfish(n3, 0)
+    y = ps.near_curve_targets(n3, 1)
+    ds = np.random.default_rng(3).standard_normal(n3) + 0j
+    d_src, d_trg = T(x.T), T(y.T)
+    d_ds, d_nv = T(ds.view(np.float64)), T(nrm.T)
+    d_pot = torch.zeros(2 * n3, dtype=torch.float64, device=dev)
+    d_pt = torch.zeros(2 * n3, dtype=torch.float64, device=dev)
+    eps3 = ctypes.c_double(1e-9)
+    c3n = ctypes.c_int(n3)
+
+    def c3():
+        L.lfmm2d_st_d_p_(ctypes.byref(eps3), ctypes.byref(c3n), ptr(d_src), ptr(d_ds),
+                         ptr(d_nv), ptr(d_pot), ctypes.byref(c3n), ptr(d_trg), ptr(d_pt),
+                         ctypes.byref(ier))
+        check()
+
+    ms, prof = timed(c3)
+    m = 10000
+    idx = np.random.default_rng(5).choice(n3, m, replace=False)
+    sub = T(y.T[idx])
+    pot = torch.zeros(2 * m, dtype=torch.float64, device=dev)
+    L.fmm2d_b200_l2d_direct(1, n3, ptr(d_src), 0, None, 1, ptr(d_ds), ptr(d_nv), m, ptr(sub), 1,
+                            ptr(pot), None, None, ctypes.c_double(1e-300))
+    torch.cuda.synchronize()
+    out["c3"] = {"workload": "lfmm2d_st_d_p starfish 4e6 + 4e6 near-curve targets eps 1e-9 (FP64)",
+                 "ms": ms, "points_s": 2 * n3 / (ms * 1e-3),
+                 "nlevels": prof.get("#nlevels"), "nboxes": prof.get("#nboxes"),
+                 "pottarg_rel_l2": rel(d_pt.view(-1, 2)[T(idx)], pot.view(-1, 2)),
+                 "accuracy_sample": f"{m} targets vs GPU FP64 direct sum"}
+    del d_src, d_trg, d_ds, d_nv, d_pot, d_pt
+    # ---- c4 ----
+    n4 = 2_000_000
+    rng = np.random.default_rng(404)
+    src = rng.random((n4, 2))
+    q = rng.standard_normal(n4) + 1j * rng.standard_normal(n4)
+    dd = rng.standard_normal(n4) + 1j * rng.standard_normal(n4)
+    th = rng.uniform(0, 2 * np.pi, n4)
+    v = np.stack([np.cos(th), np.sin(th)], axis=1)
+    d_src, d_q, d_d, d_v = T(src), T(q.view(np.float64)), T(dd.view(np.float64)), T(v)
+    d_pot = torch.zeros(2 * n4, dtype=torch.float64, device=dev)
+    zk = np.array([200.0, 0.0])
+    eps4 = ctypes.c_double(1e-6)
+    c4n = ctypes.c_int(n4)
+
+    def c4():
+        L.hfmm2d_s_cd_p_(ctypes.byref(eps4), zk.ctypes.data_as(P), ctypes.byref(c4n), ptr(d_src),
+                         ptr(d_q), ptr(d_d), ptr(d_v), ptr(d_pot), ctypes.byref(ier))
+        check()
+
+    ms, prof = timed(c4)
+    m = 1000
+    sub = T(src[:m])
+    pot = torch.zeros(2 * m, dtype=torch.float64, device=dev)
+    L.fmm2d_b200_h2d_direct(1, zk.ctypes.data_as(P), n4, ptr(d_src), 1, ptr(d_q), 1, ptr(d_d),
+                            ptr(d_v), m, ptr(sub), 1, ptr(pot), None, None,
+                            ctypes.c_double(1e-150))
+    torch.cuda.synchronize()
+    out["c4"] = {"workload": "hfmm2d_s_cd_p uniform 2e6 zk 200 eps 1e-6 (FP64)", "ms": ms,
+                 "points_s": n4 / (ms * 1e-3), "nlevels": prof.get("#nlevels"),
+                 "pot_rel_l2": rel(d_pot.view(-1, 2)[:m], pot.view(-1, 2)),
+                 "accuracy_sample": f"{m} sources vs GPU FP64 direct sum"}
+    return out
 
 
 def measure_fp32_peak(L):

@@ -185,16 +185,21 @@ void laplace_geometry(const FmmCall &c, bool on_dev, cudaStream_t s, LapGeometry
     const Tree &T = G.T;
     G.src_s.alloc(c.ns, s);
     G.trg_s.alloc(std::max(c.nt, 1), s);
-    const int *perm = T.isrc.get();
-    const double2 *sp = src_in.ptr;
-    double2 *so = G.src_s.get();
-    for_each(c.ns, s, [=] __device__(int64_t k) { so[k] = sp[perm[k]]; });
-    if (c.nt > 0) {
-        const int *pt = T.itarg.get();
-        const double2 *tp = trg_in.ptr;
-        double2 *to = G.trg_s.get();
-        for_each(c.nt, s, [=] __device__(int64_t k) { to[k] = tp[pt[k]]; });
+    if (G.mixed) {
+        G.src_hl.alloc(c.ns, s);
+        G.trg_hl.alloc(std::max(c.nt, 1), s);
     }
+    // points in tree order (and their hi/lo FP32 split for the mixed near
+    // field)
+    auto gather = [&](int n, const int *perm, const double2 *in, double2 *o, float4 *hl) {
+        for_each(n, s, [=] __device__(int64_t k) {
+            const double2 v = in[perm[k]];
+            o[k] = v;
+            if (hl) hl[k] = split_pos(v);
+        });
+    };
+    gather(c.ns, T.isrc.get(), src_in.ptr, G.src_s.get(), G.src_hl.get());
+    if (c.nt > 0) gather(c.nt, T.itarg.get(), trg_in.ptr, G.trg_s.get(), G.trg_hl.get());
     // thresh = boxsize(0) * 2^-51 (c_translation/src/cfmm2d.c:994)
     G.thresh = T.boxsize[0] * std::ldexp(1.0, -51);
     // (the caller's host copies are released on this stream)
@@ -214,33 +219,44 @@ void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaS
         dip_in.set(c.dipstr, (size_t)nd * ns, on_dev, s);
         if (lap) dv_in.set(c.dipvec, (size_t)2 * nd * ns, on_dev, s);
     }
-    // ---- strengths into tree order ----
+    // ---- strengths into tree order (and their FP32 copies for the mixed
+    // near field) ----
     DevBuf<double2> chg_s, dip_s;
+    DevBuf<float2> chg32, dip32;
+    const bool mixed = G.mixed;
     {
         const int *perm = T.isrc.get();
+        auto put = [=] __device__(double2 *o, float2 *o32, size_t a, double2 v) {
+            o[a] = v;
+            if (o32) o32[a] = make_float2((float)v.x, (float)v.y);
+        };
         if (c.ifcharge) {
             chg_s.alloc((size_t)ns * ndc, s);
+            if (mixed) chg32.alloc((size_t)ns * ndc, s);
             const double2 *q = chg_in.ptr;
             double2 *qo = chg_s.get();
+            float2 *q32 = chg32.get();
             for_each(ns, s, [=] __device__(int64_t k) {
                 const int i = perm[k];
                 for (int j = 0; j < nd; j++) {
                     const double2 v = q[(size_t)i * nd + j];
                     if (lap) {
                         // charge1(1:2, j, i) = (Re q, Im q)  (lfmm2d.f:141-147)
-                        qo[(size_t)k * ndc + 2 * j] = make_double2(v.x, 0.0);
-                        qo[(size_t)k * ndc + 2 * j + 1] = make_double2(v.y, 0.0);
+                        put(qo, q32, (size_t)k * ndc + 2 * j, make_double2(v.x, 0.0));
+                        put(qo, q32, (size_t)k * ndc + 2 * j + 1, make_double2(v.y, 0.0));
                     } else {
-                        qo[(size_t)k * ndc + j] = v;
+                        put(qo, q32, (size_t)k * ndc + j, v);
                     }
                 }
             });
         }
         if (c.ifdipole) {
             dip_s.alloc((size_t)ns * ndc, s);
+            if (mixed) dip32.alloc((size_t)ns * ndc, s);
             const double2 *d = dip_in.ptr;
             const double *dv = dv_in.ptr;
             double2 *dout = dip_s.get();
+            float2 *d32 = dip32.get();
             for_each(ns, s, [=] __device__(int64_t k) {
                 const int i = perm[k];
                 for (int j = 0; j < nd; j++) {
@@ -249,10 +265,11 @@ void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaS
                         // dipstr1 = (Re d, Im d) * (-(v1 + i v2))  (lfmm2d.f:149-157)
                         const double v1 = dv[((size_t)i * 2 + 0) * nd + j];
                         const double v2 = dv[((size_t)i * 2 + 1) * nd + j];
-                        dout[(size_t)k * ndc + 2 * j] = make_double2(-v.x * v1, -v.x * v2);
-                        dout[(size_t)k * ndc + 2 * j + 1] = make_double2(-v.y * v1, -v.y * v2);
+                        put(dout, d32, (size_t)k * ndc + 2 * j, make_double2(-v.x * v1, -v.x * v2));
+                        put(dout, d32, (size_t)k * ndc + 2 * j + 1,
+                            make_double2(-v.y * v1, -v.y * v2));
                     } else {
-                        dout[(size_t)k * ndc + j] = v;
+                        put(dout, d32, (size_t)k * ndc + j, v);
                     }
                 }
             });
@@ -301,6 +318,12 @@ void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaS
     P.ifnear = c.ifnear;
     P.mixed = G.mixed;
     P.real_charge = lap;
+    if (mixed) {
+        P.charge32 = chg32.get();
+        P.dipstr32 = dip32.get();
+        P.src_hl = G.src_hl.get();
+        P.trg_hl = G.trg_hl.get();
+    }
     cauchy_fmm(T, P, s);
     // ---- back to input order, in the caller's layout ----
     auto unsort = [&](int n, const int *perm, int pgh, const DevBuf<double2> &po,

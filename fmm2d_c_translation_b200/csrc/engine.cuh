@@ -49,6 +49,7 @@ struct LapGeometry {
     double eps = 0, thresh = 0;
     Tree T;
     DevBuf<double2> src_s, trg_s;
+    DevBuf<float4> src_hl, trg_hl;  // mixed mode: FP32 hi/lo positions
 };
 void laplace_geometry(const FmmCall &c, bool on_dev, cudaStream_t s, LapGeometry &G);
 void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaStream_t s);

@@ -609,10 +609,6 @@ constexpr int kP2PWarps = 4;
 template <bool MIXED> struct PosT { typedef double2 T; };
 template <> struct PosT<true> { typedef float4 T; };
 
-__device__ __forceinline__ float4 split_pos(double2 p) {
-    const float xh = (float)p.x, yh = (float)p.y;
-    return make_float4(xh, (float)(p.x - (double)xh), yh, (float)(p.y - (double)yh));
-}
 
 __device__ __forceinline__ void pos_diff(double2 a, double2 b, double &dx, double &dy) {
     dx = a.x - b.x;
@@ -2055,7 +2051,7 @@ void cauchy_fmm(const Tree &T, const CauchyProblem &P0, cudaStream_t s) {
     }
     // FP32 copies of the strengths for the mixed-precision near field
     DevBuf<float2> chg32, dip32;
-    if (P.mixed) {
+    if (P.mixed && !P.charge32 && !P.dipstr32) {
         const size_t nv = (size_t)P.sset.n * P.ndc;
         auto conv = [&](const double2 *in, DevBuf<float2> &out) {
             if (!in || !nv) return;
@@ -2072,7 +2068,7 @@ void cauchy_fmm(const Tree &T, const CauchyProblem &P0, cudaStream_t s) {
     }
     // hi/lo FP32 positions for the mixed near field
     DevBuf<float4> shl, thl;
-    if (P.mixed) {
+    if (P.mixed && !P.src_hl) {
         auto split = [&](const double2 *in, int n, DevBuf<float4> &out) {
             out.alloc(std::max(n, 1), s);
             float4 *o = out.get();

@@ -43,7 +43,14 @@ struct CauchyProblem {
 };
 
 // Runs steps 1-8 of cfmm2dmain (src/laplace/cfmm2d.f:442-1340) on the
-// device.  The outputs in sset / tset are overwritten.
+// device.  The outputs in sset / tset are overwritten.  In the mixed mode
+// the FP32 strengths and hi/lo positions are made here unless the caller
+// supplies them (charge32 / dipstr32, src_hl / trg_hl).
+// FP32 (x_hi, x_lo, y_hi, y_lo) split of an FP64 position.
+__device__ __forceinline__ float4 split_pos(double2 p) {
+    const float xh = (float)p.x, yh = (float)p.y;
+    return make_float4(xh, (float)(p.x - (double)xh), yh, (float)(p.y - (double)yh));
+}
 void cauchy_fmm(const Tree &T, const CauchyProblem &P, cudaStream_t s);
 
 // Direct sums over all sources for every point of `set` (the reference's

@@ -70,19 +70,23 @@ __global__ void __launch_bounds__(kThreads) radix_scatter_kernel(
     run[tid] = 0;
     const unsigned lt_mask = (1u << lane) - 1u;
     const int64_t base = (int64_t)blockIdx.x * kTile;
+    // the tile's items, loaded up front (coalesced, all in flight at once)
+    uint32_t kr[kRounds], vr[kRounds];
+#pragma unroll
+    for (int r = 0; r < kRounds; r++) {
+        const int64_t idx = base + (int64_t)r * kThreads + tid;
+        kr[r] = idx < n ? kin[idx] : 0u;
+        vr[r] = idx < n ? vin[idx] : 0u;
+    }
+#pragma unroll
     for (int r = 0; r < kRounds; r++) {
 #pragma unroll
         for (int w = 0; w < kWarps; w++) wc[w][tid] = 0;
         __syncthreads();
         const int64_t idx = base + (int64_t)r * kThreads + tid;
         const bool valid = idx < n;
-        uint32_t key = 0, val = 0;
-        int d = -1;
-        if (valid) {
-            key = kin[idx];
-            val = vin[idx];
-            d = (int)((key >> shift) & 0xff);
-        }
+        const uint32_t key = kr[r], val = vr[r];
+        const int d = valid ? (int)((key >> shift) & 0xff) : -1;
         const unsigned peers = __match_any_sync(0xffffffffu, d);
         const int rank = __popc(peers & lt_mask);
         if (valid && rank == 0) wc[warp][d] = __popc(peers);
