@@ -693,6 +693,7 @@ def measure_configs(fm, L, args):
                             ptr(pot), ptr(grad), None, ctypes.c_double(1e-150))
     torch.cuda.synchronize()
     c1r = {"workload": "lfmm2d_s_c_g uniform 1e5 eps 1e-6 (auto: mixed)", "ms": ms,
+           "phase_ms": {k: round(v, 3) for k, v in prof.items() if not k.startswith("#")},
            "points_s": ns / (ms * 1e-3),
            "pot_rel_l2": rel(d_pot.view(-1, 2)[:m], pot.view(-1, 2)),
            "grad_rel_l2": rel(d_grad.view(-1, 4)[:m], grad.view(-1, 4)),
@@ -710,6 +711,13 @@ def measure_configs(fm, L, args):
         c1r["vs_reference_1core"] = tr * 1e3 / ms
         c1r["pot_rel_l2_vs_reference"] = float(np.linalg.norm(
             d_pot.view(-1, 2).cpu().numpy().view(complex).ravel() - hp) / np.linalg.norm(hp))
+        gg = d_grad.view(-1, 4).cpu().numpy().view(complex).reshape(ns, 2)
+        c1r["grad_rel_l2_vs_reference"] = float(np.linalg.norm(gg - hg) / np.linalg.norm(hg))
+        # the reference FMM's own errors at the same eps, same sampled sources
+        dp = pot.view(-1, 2).cpu().numpy().view(complex).ravel()
+        dg = grad.view(-1, 4).cpu().numpy().view(complex).reshape(m, 2)
+        c1r["reference_pot_rel_l2"] = float(np.linalg.norm(hp[:m] - dp) / np.linalg.norm(dp))
+        c1r["reference_grad_rel_l2"] = float(np.linalg.norm(hg[:m] - dg) / np.linalg.norm(dg))
     out["c1"] = c1r
     # ---- c3 ----
     n3 = 4_000_000
@@ -740,6 +748,7 @@ def measure_configs(fm, L, args):
     out["c3"] = {"workload": "lfmm2d_st_d_p starfish 4e6 + 4e6 near-curve targets eps 1e-9 (FP64)",
                  "ms": ms, "points_s": 2 * n3 / (ms * 1e-3),
                  "nlevels": prof.get("#nlevels"), "nboxes": prof.get("#nboxes"),
+                 "phase_ms": {k: round(v, 3) for k, v in prof.items() if not k.startswith("#")},
                  "pottarg_rel_l2": rel(d_pt.view(-1, 2)[T(idx)], pot.view(-1, 2)),
                  "accuracy_sample": f"{m} targets vs GPU FP64 direct sum"}
     del d_src, d_trg, d_ds, d_nv, d_pot, d_pt
@@ -771,7 +780,8 @@ def measure_configs(fm, L, args):
                             ctypes.c_double(1e-150))
     torch.cuda.synchronize()
     out["c4"] = {"workload": "hfmm2d_s_cd_p uniform 2e6 zk 200 eps 1e-6 (FP64)", "ms": ms,
-                 "points_s": n4 / (ms * 1e-3), "nlevels": prof.get("#nlevels"),
+                 "points_s": n4 / (ms * 1e-3),
+                 "phase_ms": {k: round(v, 3) for k, v in prof.items() if not k.startswith("#")},
                  "pot_rel_l2": rel(d_pot.view(-1, 2)[:m], pot.view(-1, 2)),
                  "accuracy_sample": f"{m} sources vs GPU FP64 direct sum"}
     return out

@@ -452,6 +452,9 @@ template <class T2> __device__ __forceinline__ T2 mk2(double a, double b);
 template <> __device__ __forceinline__ double2 mk2<double2>(double a, double b) { return make_double2(a, b); }
 template <> __device__ __forceinline__ float2 mk2<float2>(double a, double b) { return make_float2((float)a, (float)b); }
 template <class T2> __device__ __forceinline__ T2 cv2(double2 v) { return mk2<T2>(v.x, v.y); }
+template <class T2> __device__ __forceinline__ T2 cvf(float2 v);
+template <> __device__ __forceinline__ float2 cvf<float2>(float2 v) { return v; }
+template <> __device__ __forceinline__ double2 cvf<double2>(float2 v) { return make_double2(v.x, v.y); }
 
 template <class T2> __device__ __forceinline__ T2 zmul(T2 a, T2 b) {
     T2 r;
@@ -504,10 +507,15 @@ __global__ void __launch_bounds__(256) eval_far_points_kernel(
     const int *__restrict__ nlist3, const int *__restrict__ list3,
     const int2 *__restrict__ sse, PointSet set, int ndc, int c0, int p,
     int nlevels, const double2 *__restrict__ mp,
-    const double2 *__restrict__ loc) {
+    const double2 *__restrict__ loc, const float2 *__restrict__ mp32,
+    const float2 *__restrict__ loc32) {
     typedef typename Real<MIXED>::T R;
     typedef typename Real<MIXED>::T2 R2;
     const int stride = (p + 1) * ndc;
+    // coefficient m of an expansion at base offset `o`: from the FP32 copy
+    // when there is one (mixed mode), else converted from FP64
+    auto mcoef = [&](size_t o) -> R2 { return MIXED && mp32 ? cvf<R2>(mp32[o]) : cv2<R2>(mp[o]); };
+    auto lcoef = [&](size_t o) -> R2 { return MIXED && loc32 ? cvf<R2>(loc32[o]) : cv2<R2>(loc[o]); };
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const int b = leaf[k];
         const int lb = level[b];
@@ -529,17 +537,17 @@ __global__ void __launch_bounds__(256) eval_far_points_kernel(
             const R rinv = (R)(1.0 / r);
 #pragma unroll
             for (int q = 0; q < CH; q++) {
-                const double2 *M = mp + (size_t)jb * stride + c0 + q;
-                R2 q0 = cv2<R2>(M[(size_t)p * ndc]), q1 = mk2<R2>(0.0, 0.0), q2 = mk2<R2>(0.0, 0.0);
+                const size_t mo = (size_t)jb * stride + c0 + q;
+                R2 q0 = mcoef(mo + (size_t)p * ndc), q1 = mk2<R2>(0.0, 0.0), q2 = mk2<R2>(0.0, 0.0);
                 for (int m = p - 1; m >= 1; m--) {
                     if (PGH >= 3) q2 = zadd(zmul(q2, w), q1);
                     if (PGH >= 2) q1 = zadd(zmul(q1, w), q0);
-                    q0 = zadd(zmul(q0, w), cv2<R2>(M[(size_t)m * ndc]));
+                    q0 = zadd(zmul(q0, w), mcoef(mo + (size_t)m * ndc));
                 }
                 if (PGH >= 3) q2 = zadd(zmul(q2, w), q1);
                 if (PGH >= 2) q1 = zadd(zmul(q1, w), q0);
                 q0 = zmul(q0, w);
-                const R2 M0 = cv2<R2>(M[0]);
+                const R2 M0 = mcoef(mo);
                 po[q] = zadd(po[q], zadd(zscal(M0, lz), q0));
                 if (PGH >= 2) {
                     const R2 w2 = zmul(w, w);
@@ -561,12 +569,12 @@ __global__ void __launch_bounds__(256) eval_far_points_kernel(
             const R rinv = (R)(1.0 / rb);
 #pragma unroll
             for (int q = 0; q < CH; q++) {
-                const double2 *Lc = loc + (size_t)b * stride + c0 + q;
-                R2 q0 = cv2<R2>(Lc[(size_t)p * ndc]), q1 = mk2<R2>(0.0, 0.0), q2 = mk2<R2>(0.0, 0.0);
+                const size_t lo_ = (size_t)b * stride + c0 + q;
+                R2 q0 = lcoef(lo_ + (size_t)p * ndc), q1 = mk2<R2>(0.0, 0.0), q2 = mk2<R2>(0.0, 0.0);
                 for (int m = p - 1; m >= 0; m--) {
                     if (PGH >= 3) q2 = zadd(zmul(q2, z), q1);
                     if (PGH >= 2) q1 = zadd(zmul(q1, z), q0);
-                    q0 = zadd(zmul(q0, z), cv2<R2>(Lc[(size_t)m * ndc]));
+                    q0 = zadd(zmul(q0, z), lcoef(lo_ + (size_t)m * ndc));
                 }
                 po[q] = zadd(po[q], q0);
                 if (PGH >= 2) gr[q] = zadd(gr[q], zscal(q1, rinv));
@@ -1247,13 +1255,14 @@ void launch_p2p(const Tree &T, const CauchyProblem &P, int c0, double th2,
 template <int CH>
 void launch_eval_far(const Tree &T, const CauchyProblem &P, const PointSet &set,
                      const int *leaf, int c0, const double2 *mp,
-                     const double2 *loc, cudaStream_t s) {
+                     const double2 *loc, const float2 *mp32, const float2 *loc32,
+                     cudaStream_t s) {
     const int blocks = std::max(1, std::min((set.n + 255) / 256, kNumSM * 8));
 #define FMM_EVAL_CASE(PG, MX)                                                   \
     eval_far_points_kernel<CH, PG, MX><<<blocks, 256, 0, s>>>(                  \
         set.n, leaf, T.level.get(), T.centers.get(), T.d_boxsize.get(),         \
         T.nlist3.get(), T.list3.get(), T.srcse.get(), set, P.ndc, c0, P.p,      \
-        T.nlevels, mp, loc)
+        T.nlevels, mp, loc, mp32, loc32)
     if (P.mixed) {
         if (set.pgh == 1) FMM_EVAL_CASE(1, true);
         if (set.pgh == 2) FMM_EVAL_CASE(2, true);
@@ -1524,7 +1533,8 @@ __device__ __forceinline__ double2 child_offset(int cs) {
 template <int PMAX>
 __global__ void __launch_bounds__(128) l2l_pascal_kernel(
     int lo, int hi, int p, EvalCounts ec, const int *__restrict__ parent,
-    const int *__restrict__ child, int ndc, int c0, int nch, double2 *__restrict__ loc) {
+    const int *__restrict__ child, int ndc, int c0, int nch, double2 *__restrict__ loc,
+    float2 *__restrict__ loc32) {
     const int stride = (p + 1) * ndc;
     const int64_t total = (int64_t)(hi - lo) * nch;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
@@ -1552,7 +1562,11 @@ __global__ void __launch_bounds__(128) l2l_pascal_kernel(
 #pragma unroll
         for (int i = 0; i < PMAX; i++) {
             if (i > p) break;
-            Lc[(size_t)i * ndc] = cadd(Lc[(size_t)i * ndc], cmul(v, e[i]));
+            const double2 r = cadd(Lc[(size_t)i * ndc], cmul(v, e[i]));
+            Lc[(size_t)i * ndc] = r;
+            // (the box's local expansion is final here: FP32 copy for the
+            // mixed-mode evaluation at the points)
+            if (loc32) loc32[(size_t)b * stride + (size_t)i * ndc + q] = make_float2((float)r.x, (float)r.y);
             v = cmul(v, h);
         }
     }
@@ -1864,7 +1878,7 @@ void m2l_chunk(const Tree &T, const CauchyProblem &P, int c0,
 template <int CH>
 void downward_chunk(const Tree &T, const CauchyProblem &P, int c0,
                     const double *binom, const double2 *mp, double2 *loc,
-                    cudaStream_t s) {
+                    const float2 *mp32, float2 *loc32, cudaStream_t s) {
     const int L = T.nlevels, p = P.p, nb = T.nboxes;
     const double *bs = T.d_boxsize.get();
     const EvalCounts ec{T.srcse.get(), T.trgse.get(), P.sset.pgh, P.tset.pgh};
@@ -1901,10 +1915,10 @@ void downward_chunk(const Tree &T, const CauchyProblem &P, int c0,
         const int64_t nt = (int64_t)(hi - lo) * CH;
         if (p + 1 <= 20)
             l2l_pascal_kernel<20><<<pascal_grid(nt), 128, 0, s>>>(
-                lo, hi, p, ec, T.parent.get(), T.child.get(), P.ndc, c0, CH, loc);
+                lo, hi, p, ec, T.parent.get(), T.child.get(), P.ndc, c0, CH, loc, loc32);
         else if (p + 1 <= 40)
             l2l_pascal_kernel<40><<<pascal_grid(nt), 128, 0, s>>>(
-                lo, hi, p, ec, T.parent.get(), T.child.get(), P.ndc, c0, CH, loc);
+                lo, hi, p, ec, T.parent.get(), T.child.get(), P.ndc, c0, CH, loc, loc32);
         else
             l2l_coef_kernel<CH><<<blocks(hi - lo), 256, 0, s>>>(
                 lo, hi, p, ec, T.parent.get(), T.child.get(), A, P.ndc, c0, loc);
@@ -1942,7 +1956,7 @@ void downward_chunk(const Tree &T, const CauchyProblem &P, int c0,
         for (const PointSet *set : {&P.tset, &P.sset}) {
             if (set->pgh <= 0 || set->n <= 0) continue;
             launch_eval_far<CH>(T, P, *set, set == &P.tset ? P.tleaf : P.sleaf, c0,
-                                mp, loc, s);
+                                mp, loc, mp32, loc32, s);
         }
     }
     prof_mark("m2p_l2p", s);
@@ -2105,13 +2119,27 @@ void cauchy_fmm(const Tree &T, const CauchyProblem &P0, cudaStream_t s) {
     const char *mode = getenv("FMM2D_B200_M2L");
     const bool simple = mode && !strcmp(mode, "simple");
     const bool fp32 = P.mixed && !(mode && !strcmp(mode, "fp64"));
-    if (simple || !((fp32 && m2l_fp32(T, P, mp.get(), loc.get(), s)) ||
+    // Mixed mode with the per-point far field: FP32 copies of the
+    // multipoles (made for the M2L) and of the final locals (written by
+    // L2L) feed the evaluation at the points, which then loads half the
+    // bytes and converts nothing.
+    const bool copies = fp32 && !simple && !far_per_leaf(P) && T.nlevels >= 2 && P.p + 1 <= 20;
+    DevBuf<float2> mp32, loc32;
+    if (copies) {
+        mp32.alloc(nexp, s);
+        loc32.alloc(nexp, s);
+        FMM_CUDA(cudaMemsetAsync(loc32.get(), 0,
+                                 (size_t)nlow * (P.p + 1) * P.ndc * sizeof(float2), s));
+    }
+    if (simple || !((fp32 && m2l_fp32(T, P, mp.get(), loc.get(), s, mp32.get())) ||
                     m2l_tensor_fp64(T, P, mp.get(), loc.get(), s)))
         per_chunk([&](int c0) { m2l_chunk<2>(T, P, c0, binom, mp.get(), loc.get(), s); },
                   [&](int c0) { m2l_chunk<1>(T, P, c0, binom, mp.get(), loc.get(), s); });
     prof_mark("m2l", s);
-    per_chunk([&](int c0) { downward_chunk<2>(T, P, c0, binom, mp.get(), loc.get(), s); },
-              [&](int c0) { downward_chunk<1>(T, P, c0, binom, mp.get(), loc.get(), s); });
+    per_chunk([&](int c0) { downward_chunk<2>(T, P, c0, binom, mp.get(), loc.get(), mp32.get(),
+                                              loc32.get(), s); },
+              [&](int c0) { downward_chunk<1>(T, P, c0, binom, mp.get(), loc.get(), mp32.get(),
+                                              loc32.get(), s); });
 }
 
 void cauchy_direct(const CauchyProblem &P, int ns, PointSet set,

@@ -67,8 +67,10 @@ bool m2l_tensor_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp,
 // FP32 M2L of the mixed-precision mode (m2l.cu): one complex matrix per
 // (child position, slot) applied to FP32 copies of the multipoles; false
 // when the order or the tree does not fit (the caller then uses FP64).
+// mp32_out (optional, nboxes * (p + 1) * ndc): receives the FP32 copy of
+// the multipoles of levels >= 2 that the M2L reads.
 bool m2l_fp32(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 *loc,
-              cudaStream_t s);
+              cudaStream_t s, float2 *mp32_out = nullptr);
 
 // Forms of the mixed-mode M2L, selectable per expansion order.
 enum M2LForm { kM2LWindow = 0, kM2LTile = 1, kM2LSimt = 2 };

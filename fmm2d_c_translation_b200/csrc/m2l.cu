@@ -957,7 +957,7 @@ void set_m2l_form(int p, int form) {
 }
 
 bool m2l_fp32(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 *loc,
-              cudaStream_t s) {
+              cudaStream_t s, float2 *mp32_out) {
     const int L = T.nlevels, p = P.p;
     if (L < 2 || p + 1 > 20) return false;
     const int form = m2l_form(p);
@@ -968,10 +968,12 @@ bool m2l_fp32(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 
     const int lo = T.lstart[2];
     const size_t stride = (size_t)(p + 1) * P.ndc;
     const size_t nv = (size_t)(T.nboxes - lo) * stride;
-    DevBuf<float2> mp32((size_t)T.nboxes * stride, s);
+    DevBuf<float2> mp32_own;
+    if (!mp32_out) mp32_own.alloc((size_t)T.nboxes * stride, s);
+    float2 *mp32p = mp32_out ? mp32_out : mp32_own.get();
     {
         const double2 *src = mp + (size_t)lo * stride;
-        float2 *dst = mp32.get() + (size_t)lo * stride;
+        float2 *dst = mp32p + (size_t)lo * stride;
         for_each((int64_t)nv, s, [=] __device__(int64_t i) {
             dst[i] = make_float2((float)src[i].x, (float)src[i].y);
         });
@@ -979,14 +981,14 @@ bool m2l_fp32(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 
     DevBuf<int> err(1, s);
     err.zero(s);
     const uint64_t done =
-        (simt || tile_only) ? 0 : m2l_window_fp32(T, P, mp32.get(), loc, err.get(), s);
+        (simt || tile_only) ? 0 : m2l_window_fp32(T, P, mp32p, loc, err.get(), s);
     M2LWork w;
     if (!m2l_work(T, P, simt ? kFp32Tile : kTcRows / CH, s, w, done)) return false;
     if (w.ntiles > 0 && simt) {
         if (p + 1 <= 12)
-            launch_fp32<12>(w, T, P, fp32_tables(p, 12, s), mp32.get(), loc, s);
+            launch_fp32<12>(w, T, P, fp32_tables(p, 12, s), mp32p, loc, s);
         else
-            launch_fp32<20>(w, T, P, fp32_tables(p, 20, s), mp32.get(), loc, s);
+            launch_fp32<20>(w, T, P, fp32_tables(p, 20, s), mp32p, loc, s);
     } else if (w.ntiles > 0) {
         // tensor cores: K = N = 2 HALF with HALF = 12 (p < 12) or 20
         const int HALF = p + 1 <= 12 ? 12 : 20;
@@ -999,7 +1001,7 @@ bool m2l_fp32(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 
             const int blocks = std::max(1, std::min(ww.ntiles, kNumSM * 4));
             kern<<<blocks, kTcRows, smem, s>>>(ww.seg(), (const int *)ww.vals.get(), ww.slots.get(),
                                                T.d_boxsize.get(), P.ndc, c0, p, tab, tab0,
-                                               mp32.get(), loc, ww.ntiles, err.get());
+                                               mp32p, loc, ww.ntiles, err.get());
             FMM_CHECK_LAUNCH();
         };
         int c0 = 0;
