@@ -394,14 +394,17 @@ bool m2l_work(const Tree &T, const CauchyProblem &P, int tile, cudaStream_t s, M
 // the P1 x CH accumulators in registers (FP32 arithmetic, FP32
 // accumulation over the 27 slots, stored as FP64).
 // ---------------------------------------------------------------------------
+// NR < P1: only the rows i < NR (the leading local coefficients) are
+// computed and stored; the tensor-core forms use this to recompute the rows
+// that carry most of the gradient in FP32 (see the end of m2l_fp32).
 constexpr int kFp32Tile = 128;
 
-template <int P1, int CH>
+template <int P1, int CH, int NR = P1>
 __global__ void __launch_bounds__(kFp32Tile) m2l_fp32_kernel(
     SegTable seg, const int *__restrict__ boxes, const int *__restrict__ slots,
     const double *__restrict__ bs, int ndc, int c0, int p, const float2 *__restrict__ Tall,
     const float2 *__restrict__ mp32, double2 *__restrict__ loc, int ntiles) {
-    __shared__ float2 sT[P1 * P1];
+    __shared__ float2 sT[NR * P1];
     __shared__ int s_tb[257];
     for (int e = threadIdx.x; e <= seg.nseg && e < 257; e += blockDim.x) s_tb[e] = seg.tile_base[e];
     __syncthreads();
@@ -417,18 +420,18 @@ __global__ void __launch_bounds__(kFp32Tile) m2l_fp32_kernel(
         const bool valid = q < seg.start[sg] + seg.count[sg];
         const int cp = seg.cpos[sg];
         const float lr = (float)log(bs[seg.level[sg]]);
-        float2 acc[CH][P1];
+        float2 acc[CH][NR];
         float2 s0[CH];
 #pragma unroll
         for (int c = 0; c < CH; c++) {
             s0[c] = make_float2(0.f, 0.f);
 #pragma unroll
-            for (int i = 0; i < P1; i++) acc[c][i] = make_float2(0.f, 0.f);
+            for (int i = 0; i < NR; i++) acc[c][i] = make_float2(0.f, 0.f);
         }
         for (int k = 0; k < kSlots; k++) {
             __syncthreads();  // the previous slot's matrix is no longer read
             const float2 *Tk = Tall + ((size_t)cp * kSlots + k) * P1 * P1;
-            for (int e = threadIdx.x; e < P1 * P1; e += blockDim.x) sT[e] = Tk[e];
+            for (int e = threadIdx.x; e < NR * P1; e += blockDim.x) sT[e] = Tk[e];
             __syncthreads();
             const int sb = valid ? slots[(size_t)q * kSlots + k] : -1;
             if (sb < 0) continue;
@@ -447,7 +450,7 @@ __global__ void __launch_bounds__(kFp32Tile) m2l_fp32_kernel(
                     }
                 }
 #pragma unroll
-                for (int i = 0; i < P1; i++) {
+                for (int i = 0; i < NR; i++) {
                     const float2 t = sT[i * P1 + j];
 #pragma unroll
                     for (int c = 0; c < CH; c++) {
@@ -465,7 +468,7 @@ __global__ void __launch_bounds__(kFp32Tile) m2l_fp32_kernel(
                 acc[c][0].y += lr * s0[c].y;
             }
 #pragma unroll
-            for (int i = 0; i < P1; i++) {
+            for (int i = 0; i < NR; i++) {
                 if (i > p) break;
 #pragma unroll
                 for (int c = 0; c < CH; c++)
@@ -528,7 +531,7 @@ const float2 *fp32_tables(int p, int P1, cudaStream_t s) {
     return d;
 }
 
-template <int P1>
+template <int P1, int NR = P1>
 void launch_fp32(const M2LWork &w, const Tree &T, const CauchyProblem &P, const float2 *Tab,
                  const float2 *mp32, double2 *loc, cudaStream_t s) {
     const int blocks = std::max(1, std::min(w.ntiles, kNumSM * 16));
@@ -536,12 +539,12 @@ void launch_fp32(const M2LWork &w, const Tree &T, const CauchyProblem &P, const 
     const int *boxes = (const int *)w.vals.get();
     for (int c0 = 0; c0 < P.ndc;) {
         if (P.ndc - c0 >= 2) {
-            m2l_fp32_kernel<P1, 2><<<blocks, kFp32Tile, 0, s>>>(
+            m2l_fp32_kernel<P1, 2, NR><<<blocks, kFp32Tile, 0, s>>>(
                 sg, boxes, w.slots.get(), T.d_boxsize.get(), P.ndc, c0, P.p, Tab, mp32, loc,
                 w.ntiles);
             c0 += 2;
         } else {
-            m2l_fp32_kernel<P1, 1><<<blocks, kFp32Tile, 0, s>>>(
+            m2l_fp32_kernel<P1, 1, NR><<<blocks, kFp32Tile, 0, s>>>(
                 sg, boxes, w.slots.get(), T.d_boxsize.get(), P.ndc, c0, P.p, Tab, mp32, loc,
                 w.ntiles);
             c0 += 1;
@@ -939,6 +942,10 @@ bool m2l_tensor_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp,
 
 namespace {
 std::atomic<int> g_m2l_form[128];
+// orders from which the tensor-core forms recompute the leading local
+// coefficients in FP32, and how many (see the end of m2l_fp32)
+constexpr int kExactFrom = 17;
+constexpr int kExactRows = 4;
 }
 
 // Form of the mixed-mode M2L for order p: FMM2D_B200_M2L ("simt", "tile"),
@@ -1027,6 +1034,21 @@ bool m2l_fp32(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 
     }
     if (read_scalar(err.get(), s) != 0)
         throw FmmError(4, "tensor-core M2L: a wait for an MMA or operand barrier timed out");
+    // A TF32 x 3 product is accurate to about 2^-22, four times an FP32
+    // product.  Measured on 10^5 uniform charges at eps 1e-6 (order 18),
+    // the gradient at the sources then has a relative error of 1.6e-6 with
+    // the tensor-core forms against 2.0e-7 with the FP32 CUDA-core form.
+    // From order kExactFrom on, the leading kExactRows local coefficients
+    // -- L_0 .. L_3, which carry most of the gradient at a leaf's points --
+    // are therefore recomputed in FP32 on the CUDA cores over all levels
+    // (FMM2D_B200_M2L_EXACT_ROWS=0 turns this off).
+    const char *xr = getenv("FMM2D_B200_M2L_EXACT_ROWS");
+    if (!simt && p >= kExactFrom && !(xr && !strcmp(xr, "0"))) {
+        M2LWork wr;
+        if (!m2l_work(T, P, kFp32Tile, s, wr, 0)) return false;
+        if (wr.ntiles > 0)
+            launch_fp32<20, kExactRows>(wr, T, P, fp32_tables(p, 20, s), mp32p, loc, s);
+    }
     return true;
 }
 

@@ -124,3 +124,30 @@ def test_mixed_pass_forms(mlib, monkeypatch, p2p, far):
     for k in want:
         tol = 1e-5 if k.startswith("hess") else 1e-6
         assert W.rel_err(got[k], want[k]) <= tol, k
+
+
+@pytest.mark.parametrize("m2l", ["window", "tile", "simt"])
+def test_mixed_charge_gradient_at_sources(mlib, monkeypatch, m2l):
+    """Charges only, gradient at the sources (the far field carries a large
+    share of it): every M2L form stays within eps of the direct sum at
+    eps 1e-6.  The tensor-core forms pass because they recompute the
+    leading local coefficients in FP32 from order 17 on."""
+    if m2l != "window":
+        monkeypatch.setenv("FMM2D_B200_M2L", m2l)
+    rng = np.random.default_rng(101)
+    ns = 100000
+    src = rng.random((2, ns))
+    q = rng.standard_normal(ns) + 1j * rng.standard_normal(ns)
+    got, ier = W.call(mlib, "l", "s_c_g", 1e-6, src, q, None, None)
+    assert ier == 0
+    m = 300
+    d = np.zeros(ns, complex)
+    v = np.zeros((2, ns))
+    pot = np.zeros(m, complex)
+    grad = np.zeros((m, 2), complex)
+    s = np.ascontiguousarray(src.T)
+    refimpl.orc().oracle_l2d_direct(
+        ns, W._p(s), 1, W._p(q), 0, W._p(d), W._p(np.ascontiguousarray(v.T)), 0, m,
+        W._p(s), 2, W._p(pot), W._p(grad), None, 1e-150)
+    assert W.rel_err(got["pot"][:m], pot) <= 1e-6
+    assert W.rel_err(got["grad"][:m], grad) <= 1e-6
