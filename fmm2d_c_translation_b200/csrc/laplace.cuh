@@ -8,6 +8,9 @@
 #include "common.cuh"
 #include "tree.cuh"
 
+#include <stdlib.h>
+#include <string.h>
+
 namespace fmm2d {
 
 // Sorted-order point data and outputs of one evaluation.
@@ -71,6 +74,17 @@ bool m2l_tensor_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp,
 // the multipoles of levels >= 2 that the M2L reads.
 bool m2l_fp32(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 *loc,
               cudaStream_t s, float2 *mp32_out = nullptr);
+
+// Orders from which the tensor-core forms of the mixed M2L recompute the
+// leading kM2LExactRows local coefficients in FP32 on the CUDA cores (a
+// TF32 x 3 product holds 22 of FP32's 24 bits); FMM2D_B200_M2L_EXACT_ROWS=0
+// turns it off.
+constexpr int kM2LExactFrom = 17;
+constexpr int kM2LExactRows = 4;
+inline bool m2l_exact_rows(int p) {
+    const char *e = getenv("FMM2D_B200_M2L_EXACT_ROWS");
+    return p >= kM2LExactFrom && !(e && !strcmp(e, "0"));
+}
 
 // Forms of the mixed-mode M2L, selectable per expansion order.
 enum M2LForm { kM2LWindow = 0, kM2LTile = 1, kM2LSimt = 2 };

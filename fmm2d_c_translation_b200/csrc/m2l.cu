@@ -942,10 +942,6 @@ bool m2l_tensor_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp,
 
 namespace {
 std::atomic<int> g_m2l_form[128];
-// orders from which the tensor-core forms recompute the leading local
-// coefficients in FP32, and how many (see the end of m2l_fp32)
-constexpr int kExactFrom = 17;
-constexpr int kExactRows = 4;
 }
 
 // Form of the mixed-mode M2L for order p: FMM2D_B200_M2L ("simt", "tile"),
@@ -1038,16 +1034,16 @@ bool m2l_fp32(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 
     // product.  Measured on 10^5 uniform charges at eps 1e-6 (order 18),
     // the gradient at the sources then has a relative error of 1.6e-6 with
     // the tensor-core forms against 2.0e-7 with the FP32 CUDA-core form.
-    // From order kExactFrom on, the leading kExactRows local coefficients
-    // -- L_0 .. L_3, which carry most of the gradient at a leaf's points --
-    // are therefore recomputed in FP32 on the CUDA cores over all levels
-    // (FMM2D_B200_M2L_EXACT_ROWS=0 turns this off).
-    const char *xr = getenv("FMM2D_B200_M2L_EXACT_ROWS");
-    if (!simt && p >= kExactFrom && !(xr && !strcmp(xr, "0"))) {
+    // From order kM2LExactFrom on, the leading kM2LExactRows local
+    // coefficients -- L_0 .. L_3, which carry most of the gradient at a
+    // leaf's points -- are therefore recomputed in FP32 on the CUDA cores:
+    // on the window levels from the windows (m2l_window.cu), on the other
+    // levels here with the slot tables.
+    if (!simt && m2l_exact_rows(p)) {
         M2LWork wr;
-        if (!m2l_work(T, P, kFp32Tile, s, wr, 0)) return false;
+        if (!m2l_work(T, P, kFp32Tile, s, wr, done)) return false;
         if (wr.ntiles > 0)
-            launch_fp32<20, kExactRows>(wr, T, P, fp32_tables(p, 20, s), mp32p, loc, s);
+            launch_fp32<20, kM2LExactRows>(wr, T, P, fp32_tables(p, 20, s), mp32p, loc, s);
     }
     return true;
 }

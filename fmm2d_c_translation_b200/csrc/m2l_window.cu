@@ -764,6 +764,143 @@ bool win_plan(const Tree &T, const CauchyProblem &P, int CH, cudaStream_t s, Win
     return true;
 }
 
+// ---------------------------------------------------------------------------
+// Rows 0 .. kM2LExactRows-1 of the run's locals in FP32 on the CUDA cores.
+// The tensor-core kernel's TF32 x 3 products hold 22 of FP32's 24 bits;
+// from order kM2LExactFrom on, these leading coefficients -- which carry
+// most of the gradient at a leaf's points -- are recomputed here from FP32
+// windows of the multipoles and FP32 rows of the scaled shift
+// (T_ij = t^-i B_ij (-1/t)^j, T_00 = log|t|, B as in l2dmploc) and stored
+// over the tensor-core values.  One block per run, one thread per row
+// (parent column t, channel) of the run, as in the tensor-core kernel; each
+// window is read from shared memory by the 3 shifts and 4 child positions
+// that use it.
+// ---------------------------------------------------------------------------
+template <int CH, int HALF>
+__global__ void __launch_bounds__(128) m2l_win_rows_kernel(WinArgs A,
+                                                           const float2 *__restrict__ Trows) {
+    constexpr int TB = 128 / CH, WP = TB + 2, NR = kM2LExactRows;
+    constexpr int CS = HALF * CH + 1;  // padded column stride of the window
+    __shared__ float2 sTr[kWinOffsets * NR * HALF];
+    __shared__ float2 sWin[WP * CS];
+    const int tid = threadIdx.x, tcol = tid / CH, chn = tid - tcol * CH;
+    for (int e = tid; e < kWinOffsets * NR * HALF; e += blockDim.x) sTr[e] = Trows[e];
+    const int P = A.p + 1, stride = P * A.ndc;
+    for (int run = blockIdx.x; run < A.nrun; run += gridDim.x) {
+        const int R = A.run0 + run;
+        float2 acc[4][NR], s0[4];
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            s0[c] = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int i = 0; i < NR; i++) acc[c][i] = make_float2(0.f, 0.f);
+        }
+        for (int s = 0; s < 12; s++) {
+            __syncthreads();  // the previous stage's window is no longer read
+            const int *wrow = A.wbox + ((size_t)R * 12 + s) * WP;
+            for (int e = tid; e < WP * HALF * CH; e += blockDim.x) {
+                const int col = e / (HALF * CH), r = e - col * HALF * CH;
+                const int j = r / CH, c = r - j * CH;
+                const int box = wrow[col];
+                sWin[col * CS + j * CH + c] =
+                    (box >= 0 && j < P) ? A.mp32[(size_t)box * stride + (size_t)j * A.ndc + A.c0 + c]
+                                        : make_float2(0.f, 0.f);
+            }
+            __syncthreads();
+#pragma unroll 1
+            for (int jj = -1; jj <= 1; jj++) {
+                const float2 *w = sWin + (tcol + jj + 1) * CS + chn;
+                float2 m[HALF];
+#pragma unroll
+                for (int j = 0; j < HALF; j++) m[j] = w[j * CH];
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    int dx, dy;
+                    if (!win_slot(s, jj, c, dx, dy)) continue;
+                    const float2 *tr = sTr + win_offset_index(dx, dy) * NR * HALF;
+                    s0[c].x += m[0].x;
+                    s0[c].y += m[0].y;
+#pragma unroll
+                    for (int i = 0; i < NR; i++) {
+                        float ax = acc[c][i].x, ay = acc[c][i].y;
+#pragma unroll
+                        for (int j = 0; j < HALF; j++) {
+                            const float2 t = tr[i * HALF + j];  // zero beyond the order
+                            ax = fmaf(t.x, m[j].x, fmaf(-t.y, m[j].y, ax));
+                            ay = fmaf(t.x, m[j].y, fmaf(t.y, m[j].x, ay));
+                        }
+                        acc[c][i] = make_float2(ax, ay);
+                    }
+                }
+            }
+        }
+        const double lr = log(A.bs[A.rlev[R]]);
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int box = A.tbox[((size_t)R * 4 + c) * TB + tcol];
+            if (box < 0) continue;
+            double2 *o = A.loc + (size_t)box * stride + A.c0 + chn;
+            o[0] = make_double2((double)acc[c][0].x + lr * (double)s0[c].x,
+                                (double)acc[c][0].y + lr * (double)s0[c].y);
+#pragma unroll
+            for (int i = 1; i < NR; i++)
+                if (i < P)
+                    o[(size_t)i * A.ndc] = make_double2((double)acc[c][i].x, (double)acc[c][i].y);
+        }
+    }
+}
+
+// FP32 rows i < kM2LExactRows of the scaled shift for the 40 window offsets,
+// [offset][i][HALF], zero from the order on; cached per device.
+const float2 *win_row_tables(int p, int HALF, cudaStream_t s) {
+    static std::mutex mu;
+    static std::vector<std::pair<long, const float2 *>> cache;
+    int dev;
+    FMM_CUDA(cudaGetDevice(&dev));
+    const long key = ((long)dev << 20) | ((long)p << 8) | HALF;
+    std::lock_guard<std::mutex> g(mu);
+    for (auto &e : cache)
+        if (e.first == key) return e.second;
+    constexpr int NR = kM2LExactRows;
+    std::vector<double> C((size_t)(NR + HALF + 1) * (NR + HALF + 1), 0.0);
+    const int nc = NR + HALF + 1;
+    for (int l = 0; l < nc; l++) {
+        C[(size_t)l * nc] = 1.0;
+        for (int m = 1; m <= l; m++)
+            C[(size_t)l * nc + m] = C[(size_t)(l - 1) * nc + m - 1] + (m < l ? C[(size_t)(l - 1) * nc + m] : 0.0);
+    }
+    std::vector<float2> h((size_t)kWinOffsets * NR * HALF, make_float2(0.f, 0.f));
+    for (int dy = -3; dy <= 3; dy++)
+        for (int dx = -3; dx <= 3; dx++) {
+            if (dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1) continue;
+            float2 *T = h.data() + (size_t)win_offset_index(dx, dy) * NR * HALF;
+            const double tn = 1.0 / (double)(dx * dx + dy * dy);
+            const double2 w2 = make_double2(dx * tn, -dy * tn), w1 = make_double2(-w2.x, -w2.y);
+            double2 w2i = make_double2(1.0, 0.0);
+            for (int i = 0; i < NR; i++) {
+                double2 w1j = make_double2(1.0, 0.0);
+                for (int j = 0; j <= p && j < HALF; j++) {
+                    double b;
+                    if (i == 0)
+                        b = j == 0 ? 0.0 : 1.0;
+                    else
+                        b = j == 0 ? -1.0 / i : C[(size_t)(i + j - 1) * nc + (j - 1)];
+                    double2 v = cscal(cmul(w2i, w1j), b);
+                    if (i == 0 && j == 0) v = make_double2(0.5 * std::log((double)(dx * dx + dy * dy)), 0.0);
+                    T[i * HALF + j] = make_float2((float)v.x, (float)v.y);
+                    w1j = cmul(w1j, w1);
+                }
+                w2i = cmul(w2i, w2);
+            }
+        }
+    float2 *d = nullptr;
+    FMM_CUDA(cudaMalloc(&d, h.size() * sizeof(float2)));
+    FMM_CUDA(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(float2), cudaMemcpyHostToDevice, s));
+    FMM_CUDA(cudaStreamSynchronize(s));
+    cache.push_back({key, d});
+    return d;
+}
+
 template <int CH, int HALF>
 void launch_win(const WinPlan &W, const WinTables &tb, const Tree &T, const CauchyProblem &P,
                 int c0, const float2 *mp32, double2 *loc, int *err, cudaStream_t s) {
@@ -791,6 +928,11 @@ void launch_win(const WinPlan &W, const WinTables &tb, const Tree &T, const Cauc
         const int grid = std::max(1, std::min(r.second, kNumSM));
         kern<<<grid, kWinThreads, sm, s>>>(a);
         FMM_CHECK_LAUNCH();
+        if (m2l_exact_rows(P.p)) {
+            const int g2 = std::max(1, std::min(r.second, kNumSM * 8));
+            m2l_win_rows_kernel<CH, HALF><<<g2, 128, 0, s>>>(a, win_row_tables(P.p, HALF, s));
+            FMM_CHECK_LAUNCH();
+        }
     }
 }
 
