@@ -765,11 +765,12 @@ bool win_plan(const Tree &T, const CauchyProblem &P, int CH, cudaStream_t s, Win
 }
 
 // ---------------------------------------------------------------------------
-// Rows 0 .. kM2LExactRows-1 of the run's locals in FP32 on the CUDA cores.
+// Rows 1 .. kM2LExactRows-1 of the run's locals in FP32 on the CUDA cores.
 // The tensor-core kernel's TF32 x 3 products hold 22 of FP32's 24 bits;
 // from order kM2LExactFrom on, these leading coefficients -- which carry
 // most of the gradient at a leaf's points -- are recomputed here from FP32
-// windows of the multipoles and FP32 rows of the scaled shift
+// windows of the multipoles and FP32 rows of the scaled shift (row 0 is
+// already summed on the CUDA cores by the tensor-core kernel)
 // (T_ij = t^-i B_ij (-1/t)^j, T_00 = log|t|, B as in l2dmploc) and stored
 // over the tensor-core values.  One block per run, one thread per row
 // (parent column t, channel) of the run, as in the tensor-core kernel; each
@@ -788,13 +789,11 @@ __global__ void __launch_bounds__(128) m2l_win_rows_kernel(WinArgs A,
     const int P = A.p + 1, stride = P * A.ndc;
     for (int run = blockIdx.x; run < A.nrun; run += gridDim.x) {
         const int R = A.run0 + run;
-        float2 acc[4][NR], s0[4];
+        float2 acc[4][NR];
 #pragma unroll
-        for (int c = 0; c < 4; c++) {
-            s0[c] = make_float2(0.f, 0.f);
+        for (int c = 0; c < 4; c++)
 #pragma unroll
-            for (int i = 0; i < NR; i++) acc[c][i] = make_float2(0.f, 0.f);
-        }
+            for (int i = 1; i < NR; i++) acc[c][i] = make_float2(0.f, 0.f);
         for (int s = 0; s < 12; s++) {
             __syncthreads();  // the previous stage's window is no longer read
             const int *wrow = A.wbox + ((size_t)R * 12 + s) * WP;
@@ -818,10 +817,8 @@ __global__ void __launch_bounds__(128) m2l_win_rows_kernel(WinArgs A,
                     int dx, dy;
                     if (!win_slot(s, jj, c, dx, dy)) continue;
                     const float2 *tr = sTr + win_offset_index(dx, dy) * NR * HALF;
-                    s0[c].x += m[0].x;
-                    s0[c].y += m[0].y;
 #pragma unroll
-                    for (int i = 0; i < NR; i++) {
+                    for (int i = 1; i < NR; i++) {
                         float ax = acc[c][i].x, ay = acc[c][i].y;
 #pragma unroll
                         for (int j = 0; j < HALF; j++) {
@@ -834,14 +831,11 @@ __global__ void __launch_bounds__(128) m2l_win_rows_kernel(WinArgs A,
                 }
             }
         }
-        const double lr = log(A.bs[A.rlev[R]]);
 #pragma unroll
         for (int c = 0; c < 4; c++) {
             const int box = A.tbox[((size_t)R * 4 + c) * TB + tcol];
             if (box < 0) continue;
             double2 *o = A.loc + (size_t)box * stride + A.c0 + chn;
-            o[0] = make_double2((double)acc[c][0].x + lr * (double)s0[c].x,
-                                (double)acc[c][0].y + lr * (double)s0[c].y);
 #pragma unroll
             for (int i = 1; i < NR; i++)
                 if (i < P)
