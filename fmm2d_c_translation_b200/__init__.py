@@ -307,6 +307,13 @@ class Plan:
         out.pot, out.grad, out.hess, out.pottarg, out.gradtarg, out.hesstarg = map(shaped, outs)
         return out
 
+    @property
+    def uses_graph(self):
+        """True once evaluations replay the captured CUDA graph."""
+        L = lib()
+        L.fmm2d_b200_plan_uses_graph.argtypes = [_P]
+        return bool(L.fmm2d_b200_plan_uses_graph(self._h))
+
     def close(self):
         if getattr(self, "_h", None):
             lib().fmm2d_b200_plan_destroy(self._h)

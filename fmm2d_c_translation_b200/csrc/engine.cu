@@ -208,7 +208,8 @@ void laplace_geometry(const FmmCall &c, bool on_dev, cudaStream_t s, LapGeometry
 // One evaluation over a geometry: strengths into tree order, the FMM
 // passes, outputs back to input order in the caller's layout.  Only the
 // strength and output pointers and the flags of `c` are read.
-void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaStream_t s) {
+void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaStream_t s,
+                      M2LCache *m2l, bool sync) {
     const bool lap = G.lap;
     const int nd = G.nd, ndc = G.ndc, ns = G.ns, nt = G.nt;
     const Tree &T = G.T;
@@ -318,6 +319,7 @@ void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaS
     P.ifnear = c.ifnear;
     P.mixed = G.mixed;
     P.real_charge = lap;
+    P.m2l_cache = m2l;
     if (mixed) {
         P.charge32 = chg32.get();
         P.dipstr32 = dip32.get();
@@ -369,7 +371,7 @@ void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaS
         op.flush(s);
         og.flush(s);
         oh.flush(s);
-        FMM_CUDA(cudaStreamSynchronize(s));
+        if (sync) FMM_CUDA(cudaStreamSynchronize(s));
     };
     unsort(ns, T.isrc.get(), spgh, spot, sgrad, shess, c.pot, c.grad, c.hess);
     unsort(nt, T.itarg.get(), tpgh, tpot, tgrad, thess, c.pottarg, c.gradtarg,

@@ -52,7 +52,12 @@ struct LapGeometry {
     DevBuf<float4> src_hl, trg_hl;  // mixed mode: FP32 hi/lo positions
 };
 void laplace_geometry(const FmmCall &c, bool on_dev, cudaStream_t s, LapGeometry &G);
-void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaStream_t s);
+// m2l: planning kept across evaluations (plans), null for a one-shot call;
+// sync = false leaves the final stream synchronisation to the caller (the
+// form a CUDA graph can capture).
+struct M2LCache;
+void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaStream_t s,
+                      M2LCache *m2l = nullptr, bool sync = true);
 
 // Runs the evaluation on the calling thread's current device; returns the
 // reference's ier (0 ok, 4 failure) after recording any error message.

@@ -2046,7 +2046,8 @@ const double *device_binomials(cudaStream_t s) {
 }
 
 void cauchy_fmm(const Tree &T, const CauchyProblem &P0, cudaStream_t s) {
-    if (profiling_enabled()) count_work(T, P0, s);
+    // (the work counts synchronise the stream: not inside a graph capture)
+    if (profiling_enabled() && !(P0.m2l_cache && P0.m2l_cache->deferred)) count_work(T, P0, s);
     CauchyProblem P = P0;
     // leaf of every sorted point, for the per-point far-field evaluation
     DevBuf<int> sleaf(std::max(P.sset.n, 1), s), tleaf(std::max(P.tset.n, 1), s);

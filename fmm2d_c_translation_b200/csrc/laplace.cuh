@@ -11,6 +11,9 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <map>
+#include <memory>
+
 namespace fmm2d {
 
 // Sorted-order point data and outputs of one evaluation.
@@ -21,6 +24,39 @@ struct PointSet {
     int pgh = 0;                   // 0 none, 1 pot, 2 +grad, 3 +hess
     double2 *pot = nullptr, *grad = nullptr, *hess = nullptr;  // [i*ndc + c]
 };
+
+// Planning state of the M2L passes that depends on the tree alone (work
+// lists of the slot-table kernels, the window runs).  A plan keeps one per
+// geometry so that repeated evaluations skip the planning and its host
+// synchronisations; with `deferred`, the M2L's bounded-wait error flag is
+// left in *err for the caller to read after the evaluation instead of being
+// read at the end of the M2L (the form a CUDA graph can hold).
+struct M2LCache {
+    std::map<uint64_t, std::shared_ptr<void>> items;
+    std::map<uint64_t, bool> ok;
+    int *err = nullptr;  // device flag of the deferred mode
+    bool deferred = false;
+};
+
+// The cached object of `key`, or a new one built by build(W &) -> bool
+// (kept in the cache when there is one); `ok` receives build's result.
+template <class W, class Build>
+std::shared_ptr<W> m2l_cached(M2LCache *c, uint64_t key, bool &ok, Build build) {
+    if (c) {
+        auto it = c->items.find(key);
+        if (it != c->items.end()) {
+            ok = c->ok[key];
+            return std::static_pointer_cast<W>(it->second);
+        }
+    }
+    auto w = std::make_shared<W>();
+    ok = build(*w);
+    if (c) {
+        c->items[key] = w;
+        c->ok[key] = ok;
+    }
+    return w;
+}
 
 struct CauchyProblem {
     int ndc = 1;        // Cauchy channels
@@ -43,6 +79,7 @@ struct CauchyProblem {
     const float4 *src_hl = nullptr;   // hi/lo FP32 positions (mixed near field)
     const float4 *trg_hl = nullptr;
     double *timeinfo = nullptr;       // 8 phase times (s), optional
+    M2LCache *m2l_cache = nullptr;    // planning kept across evaluations (plans)
 };
 
 // Runs steps 1-8 of cfmm2dmain (src/laplace/cfmm2d.f:442-1340) on the

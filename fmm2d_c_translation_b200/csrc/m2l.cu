@@ -260,6 +260,11 @@ struct M2LWork {
     }
 };
 
+// Cache key of a planning object: its kind, tile size and skipped levels.
+inline uint64_t m2l_key(int kind, int tile, uint64_t skip) {
+    return ((uint64_t)kind << 56) | ((uint64_t)tile << 40) | (skip & ((1ull << 40) - 1));
+}
+
 void ensure_slot_tables(cudaStream_t s) {
     static std::mutex tables_mu;
     static bool tables_ready[64] = {false};
@@ -913,8 +918,11 @@ bool m2l_tensor_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp,
                      double2 *loc, cudaStream_t s) {
     const int L = T.nlevels, p = P.p;
     if (L < 2 || p > 63) return false;
-    M2LWork w;
-    if (!m2l_work(T, P, 8, s, w)) return false;
+    bool ok = false;
+    const auto wp = m2l_cached<M2LWork>(P.m2l_cache, m2l_key(1, 8, 0), ok,
+                                        [&](M2LWork &x) { return m2l_work(T, P, 8, s, x); });
+    if (!ok) return false;
+    const M2LWork &w = *wp;
     if (w.ntiles == 0) return true;
     const SegTable sg = w.seg();
     const int *boxes = (const int *)w.vals.get();
@@ -981,12 +989,22 @@ bool m2l_fp32(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 
             dst[i] = make_float2((float)src[i].x, (float)src[i].y);
         });
     }
-    DevBuf<int> err(1, s);
-    err.zero(s);
+    // the bounded waits' error flag: read at the end, or by the caller in
+    // the deferred mode
+    M2LCache *cache = P.m2l_cache;
+    const bool deferred = cache && cache->deferred;
+    DevBuf<int> err_own;
+    if (!deferred) err_own.alloc(1, s);
+    int *errp = deferred ? cache->err : err_own.get();
+    FMM_CUDA(cudaMemsetAsync(errp, 0, sizeof(int), s));
     const uint64_t done =
-        (simt || tile_only) ? 0 : m2l_window_fp32(T, P, mp32p, loc, err.get(), s);
-    M2LWork w;
-    if (!m2l_work(T, P, simt ? kFp32Tile : kTcRows / CH, s, w, done)) return false;
+        (simt || tile_only) ? 0 : m2l_window_fp32(T, P, mp32p, loc, errp, s);
+    const int wtile = simt ? kFp32Tile : kTcRows / CH;
+    bool ok = false;
+    const auto wp = m2l_cached<M2LWork>(cache, m2l_key(3, wtile, done), ok,
+                                        [&](M2LWork &x) { return m2l_work(T, P, wtile, s, x, done); });
+    if (!ok) return false;
+    const M2LWork &w = *wp;
     if (w.ntiles > 0 && simt) {
         if (p + 1 <= 12)
             launch_fp32<12>(w, T, P, fp32_tables(p, 12, s), mp32p, loc, s);
@@ -1004,7 +1022,7 @@ bool m2l_fp32(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 
             const int blocks = std::max(1, std::min(ww.ntiles, kNumSM * 4));
             kern<<<blocks, kTcRows, smem, s>>>(ww.seg(), (const int *)ww.vals.get(), ww.slots.get(),
                                                T.d_boxsize.get(), P.ndc, c0, p, tab, tab0,
-                                               mp32p, loc, ww.ntiles, err.get());
+                                               mp32p, loc, ww.ntiles, errp);
             FMM_CHECK_LAUNCH();
         };
         int c0 = 0;
@@ -1016,11 +1034,15 @@ bool m2l_fp32(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 
         }
         if (c0 < P.ndc) {
             // remaining single channels, one channel per row
-            M2LWork w1;
+            std::shared_ptr<M2LWork> w1;
             const M2LWork *pw = &w;
             if (CH != 1) {
-                if (!m2l_work(T, P, kTcRows, s, w1, done)) return false;
-                pw = &w1;
+                bool ok1 = false;
+                w1 = m2l_cached<M2LWork>(cache, m2l_key(4, kTcRows, done), ok1, [&](M2LWork &x) {
+                    return m2l_work(T, P, kTcRows, s, x, done);
+                });
+                if (!ok1) return false;
+                pw = w1.get();
             }
             for (; c0 < P.ndc; c0++) {
                 if (HALF == 12) launch(m2l_tc_kernel<1, 12>, *pw, c0);
@@ -1028,7 +1050,7 @@ bool m2l_fp32(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 
             }
         }
     }
-    if (read_scalar(err.get(), s) != 0)
+    if (!deferred && read_scalar(errp, s) != 0)
         throw FmmError(4, "tensor-core M2L: a wait for an MMA or operand barrier timed out");
     // A TF32 x 3 product is accurate to about 2^-22, four times an FP32
     // product.  Measured on 10^5 uniform charges at eps 1e-6 (order 18),
@@ -1040,10 +1062,14 @@ bool m2l_fp32(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 
     // on the window levels from the windows (m2l_window.cu), on the other
     // levels here with the slot tables.
     if (!simt && m2l_exact_rows(p)) {
-        M2LWork wr;
-        if (!m2l_work(T, P, kFp32Tile, s, wr, done)) return false;
-        if (wr.ntiles > 0)
-            launch_fp32<20, kM2LExactRows>(wr, T, P, fp32_tables(p, 20, s), mp32p, loc, s);
+        bool okr = false;
+        const auto wr = m2l_cached<M2LWork>(cache, m2l_key(5, kFp32Tile, done), okr,
+                                            [&](M2LWork &x) {
+                                                return m2l_work(T, P, kFp32Tile, s, x, done);
+                                            });
+        if (!okr) return false;
+        if (wr->ntiles > 0)
+            launch_fp32<20, kM2LExactRows>(*wr, T, P, fp32_tables(p, 20, s), mp32p, loc, s);
     }
     return true;
 }

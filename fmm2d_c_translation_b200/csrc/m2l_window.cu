@@ -948,8 +948,11 @@ uint64_t m2l_window_fp32(const Tree &T, const CauchyProblem &P, const float2 *mp
     const int HALF = P.p + 1 <= 12 ? 12 : (P.p + 1 <= 16 ? 16 : (P.p + 1 <= 20 ? 20 : 0));
     if (HALF == 0) return 0;
     const int CH = P.ndc % 2 == 0 ? 2 : 1;
-    WinPlan W;
-    if (!win_plan(T, P, CH, s, W) || W.ranges.empty()) return 0;
+    bool ok = false;
+    const auto Wp = m2l_cached<WinPlan>(P.m2l_cache, ((uint64_t)2 << 56) | (uint64_t)CH, ok,
+                                        [&](WinPlan &x) { return win_plan(T, P, CH, s, x); });
+    const WinPlan &W = *Wp;
+    if (!ok || W.ranges.empty()) return 0;
     const WinTables tb = win_tables(P.p, HALF, s);
     int nrun = 0;
     for (const auto &r : W.ranges) nrun += r.second;

@@ -701,8 +701,12 @@ int fmm2d_b200_autotune(int kernel, double eps, int ns, const double *sources,
  * precision policy in force at creation are fixed.  plan_eval takes the
  * strengths (charge and dipstr as (nd, ns) complex, dipvec (nd, 2, ns))
  * and overwrites the outputs in the guru drivers' layouts; host or device
- * arrays.  A plan is used on the device it was made on; evaluations may
- * run from several threads at once.  Each returns 0 or 4. */
+ * arrays.  The first evaluation runs eagerly; the later ones replay a CUDA
+ * graph of the whole evaluation captured over plan-owned staging buffers
+ * (FMM2D_B200_PLAN_GRAPH=0 keeps them eager).  A plan is used on the
+ * device it was made on; evaluations of one plan are serialised.  Each
+ * returns 0 or 4; plan_uses_graph returns 1 once evaluations replay the
+ * graph. */
 int fmm2d_b200_plan_create(int kernel, int nd, double eps, int ns,
                            const double *sources, int ifcharge, int ifdipole,
                            int ifpgh, int nt, const double *targ,
@@ -713,6 +717,7 @@ int fmm2d_b200_plan_eval(void *plan, const double _Complex *charge,
                          double _Complex *hess, double _Complex *pottarg,
                          double _Complex *gradtarg, double _Complex *hesstarg);
 int fmm2d_b200_plan_destroy(void *plan);
+int fmm2d_b200_plan_uses_graph(void *plan);
 
 /* Direct sums on the GPU, incrementing the outputs (the reference's
  * l2d_direct* / c2d_direct* kernels, src/laplace/lapkernels2d.f,

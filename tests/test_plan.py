@@ -28,10 +28,18 @@ def test_plan_rejects_bad_arguments():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("graph", ["on", "off"])
 @pytest.mark.parametrize("precision", [1, 2])
 @pytest.mark.parametrize("kernel", ["l", "c"])
-def test_plan_matches_one_shot(kernel, precision):
+def test_plan_matches_one_shot(kernel, precision, graph, monkeypatch):
+    """Evaluation 1 runs eagerly, 2 and 3 replay the captured CUDA graph
+    (or stay eager with FMM2D_B200_PLAN_GRAPH=0); all equal the one-shot
+    drivers' results on the same points."""
     import fmm2d_c_translation_b200 as fm
+    if graph == "off":
+        monkeypatch.setenv("FMM2D_B200_PLAN_GRAPH", "0")
+    else:
+        monkeypatch.delenv("FMM2D_B200_PLAN_GRAPH", raising=False)
     L = fm.lib()
     L.fmm2d_b200_set_precision(precision)
     try:
@@ -52,6 +60,7 @@ def test_plan_matches_one_shot(kernel, precision):
             want = f(eps=eps, sources=src, targets=trg, pg=2, pgt=3, **kw)
             for k in ("pot", "grad", "pottarg", "gradtarg", "hesstarg"):
                 assert W.rel_err(getattr(got, k), getattr(want, k)) <= 1e-14, (it, k)
+            assert plan.uses_graph == (graph == "on" and it >= 1), it
         plan.close()
     finally:
         L.fmm2d_b200_set_precision(0)
