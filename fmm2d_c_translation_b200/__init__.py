@@ -252,6 +252,69 @@ def cfmm2d(*, eps, sources, charges=None, dipstr=None, targets=None, pg=0, pgt=0
                 dipvec=None, targets=targets, pg=pg, pgt=pgt, nd=nd)
 
 
+def fmm2d_batch(kernel="l", *, eps, problems, pg=1, pgt=0):
+    """Many independent lfmm2d / cfmm2d problems (nd = 1) with the same eps
+    and flags, evaluated as one forest (fmm2d_b200_fmm2d_batch).  Each
+    problem is a dict with "sources" (2, n), optional "charges" / "dipstr"
+    (n,) complex, "dipvec" (2, n) and "targets" (2, m); every problem must
+    have the same kinds of strengths.  Returns a list of Output."""
+    L = lib()
+    n = len(problems)
+    L.fmm2d_b200_fmm2d_batch.argtypes = [_I, _I, ctypes.c_double, _P, _P, _P, _P, _P, _I, _P, _P,
+                                         _P, _P, _P, _I, _P, _P, _P]
+    keep = []
+
+    def arr(a, dtype):
+        x = np.asfortranarray(np.asarray(a, dtype=dtype))
+        keep.append(x)
+        return x
+
+    def plist(xs):
+        if xs is None:
+            return None
+        v = (ctypes.c_void_p * n)(*[None if x is None else x.ctypes.data for x in xs])
+        keep.append(v)
+        return ctypes.cast(v, _P)
+
+    src = [arr(p["sources"], np.float64) for p in problems]
+    ns = np.array([x.shape[1] for x in src], np.int32)
+    has_c = "charges" in problems[0] and problems[0]["charges"] is not None
+    has_d = "dipstr" in problems[0] and problems[0]["dipstr"] is not None
+    q = [arr(p["charges"], np.complex128) for p in problems] if has_c else None
+    d = [arr(p["dipstr"], np.complex128) for p in problems] if has_d else None
+    v = [arr(p["dipvec"], np.float64) for p in problems] if (has_d and kernel == "l") else None
+    trg = [arr(p["targets"], np.float64) if p.get("targets") is not None else None
+           for p in problems]
+    nt = np.array([0 if t is None else t.shape[1] for t in trg], np.int32)
+    if nt.sum() == 0:
+        pgt = 0
+    gc, hc = (1, 1) if kernel == "c" else (2, 3)
+    outs = [Output() for _ in problems]
+
+    def alloc(count, comps, need):
+        if not need:
+            return None
+        return [np.zeros((comps, k) if comps > 1 else (k,), np.complex128, order="F")
+                for k in count]
+
+    pot, grad, hess = alloc(ns, 1, pg >= 1), alloc(ns, gc, pg >= 2), alloc(ns, hc, pg >= 3)
+    pt, gt, ht = alloc(nt, 1, pgt >= 1), alloc(nt, gc, pgt >= 2), alloc(nt, hc, pgt >= 3)
+    ier = L.fmm2d_b200_fmm2d_batch({"l": 0, "c": 1}[kernel], n, eps, _ptr(ns), plist(src),
+                                   plist(q), plist(d), plist(v), pg, plist(pot), plist(grad),
+                                   plist(hess), _ptr(nt), plist(trg), pgt, plist(pt),
+                                   plist(gt), plist(ht))
+    _check(ier, "fmm2d_b200_fmm2d_batch")
+    for k, o in enumerate(outs):
+        o.pot = pot[k] if pot else None
+        o.grad = grad[k] if grad else None
+        o.hess = hess[k] if hess else None
+        if nt[k] > 0:
+            o.pottarg = pt[k] if pt else None
+            o.gradtarg = gt[k] if gt else None
+            o.hesstarg = ht[k] if ht else None
+    return outs
+
+
 class Plan:
     """Resident geometry for repeated lfmm2d / cfmm2d evaluations on the same
     points (plan.cu): the tree, its lists and the sorted points stay on the

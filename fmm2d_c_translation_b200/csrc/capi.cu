@@ -309,6 +309,46 @@ FMM_EXPORT void hfmm2d_ndiv_(const fint *nd, const double *eps,
 // Library knobs with no counterpart in the reference.
 // ---------------------------------------------------------------------------
 // Precision policy: 0 auto (mixed for eps >= 1e-6), 1 all-FP64, 2 mixed.
+// A batch of independent lfmm2d (kernel 0) / cfmm2d (kernel 1) problems,
+// nd = 1, same eps and output flags, evaluated as one forest.
+FMM_EXPORT int fmm2d_b200_fmm2d_batch(int kernel, int nprob, double eps, const int *ns,
+                                      const double *const *sources, const double *const *charge,
+                                      const double *const *dipstr, const double *const *dipvec,
+                                      int ifpgh, double *const *pot, double *const *grad,
+                                      double *const *hess, const int *nt,
+                                      const double *const *targ, int ifpghtarg,
+                                      double *const *pottarg, double *const *gradtarg,
+                                      double *const *hesstarg) {
+    BatchCall b;
+    b.kernel = (Kernel)kernel;
+    b.eps = eps;
+    b.nprob = nprob;
+    b.ns = ns;
+    b.nt = nt;
+    b.sources = sources;
+    b.targ = targ;
+    b.charge = charge;
+    b.dipstr = dipstr;
+    b.dipvec = dipvec;
+    b.ifpgh = ifpgh;
+    b.ifpghtarg = ifpghtarg;
+    b.pot = pot;
+    b.grad = grad;
+    b.hess = hess;
+    b.pottarg = pottarg;
+    b.gradtarg = gradtarg;
+    b.hesstarg = hesstarg;
+    b.precision = current_precision();
+    if (!ns || !sources || (ifpgh >= 1 && !pot) || (ifpgh >= 2 && !grad) ||
+        (ifpgh >= 3 && !hess) || (ifpghtarg >= 1 && nt && !pottarg) ||
+        (ifpghtarg >= 2 && nt && !gradtarg) || (ifpghtarg >= 3 && nt && !hesstarg) ||
+        (nt && !targ)) {
+        set_last_error("batch: an array list the flags ask for is missing");
+        return 4;
+    }
+    return run_laplace_batch(b);
+}
+
 FMM_EXPORT int fmm2d_b200_set_precision(int mode) {
     if (mode < 0 || mode > 2) return 4;
     set_precision(mode);

@@ -586,6 +586,203 @@ int run_helm_direct(int nd, const double *zk, int ns, const double *sources, int
 }
 
 
+namespace {
+
+// Bounding box of each problem's sources and targets: one block per
+// problem, exact min / max (as the single-problem bounding box).
+__global__ void __launch_bounds__(256) seg_bbox_kernel(const double2 *__restrict__ src,
+                                                       const int *__restrict__ so,
+                                                       const double2 *__restrict__ trg,
+                                                       const int *__restrict__ to,
+                                                       double *__restrict__ out) {
+    const int k = blockIdx.x;
+    double xmn = INFINITY, xmx = -INFINITY, ymn = INFINITY, ymx = -INFINITY;
+    for (int set = 0; set < 2; set++) {
+        const double2 *p = set ? trg : src;
+        const int a = set ? to[k] : so[k], b = set ? to[k + 1] : so[k + 1];
+        for (int i = a + threadIdx.x; i < b; i += blockDim.x) {
+            const double2 v = p[i];
+            xmn = fmin(xmn, v.x);
+            xmx = fmax(xmx, v.x);
+            ymn = fmin(ymn, v.y);
+            ymx = fmax(ymx, v.y);
+        }
+    }
+    __shared__ double sh[4][256];
+    sh[0][threadIdx.x] = xmn;
+    sh[1][threadIdx.x] = xmx;
+    sh[2][threadIdx.x] = ymn;
+    sh[3][threadIdx.x] = ymx;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) {
+            sh[0][threadIdx.x] = fmin(sh[0][threadIdx.x], sh[0][threadIdx.x + h]);
+            sh[1][threadIdx.x] = fmax(sh[1][threadIdx.x], sh[1][threadIdx.x + h]);
+            sh[2][threadIdx.x] = fmin(sh[2][threadIdx.x], sh[2][threadIdx.x + h]);
+            sh[3][threadIdx.x] = fmax(sh[3][threadIdx.x], sh[3][threadIdx.x + h]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < 4) out[4 * k + threadIdx.x] = sh[threadIdx.x][0];
+}
+
+// p -= center of its problem, one block per problem.
+__global__ void __launch_bounds__(256) seg_shift_kernel(double2 *__restrict__ p,
+                                                        const int *__restrict__ off,
+                                                        const double2 *__restrict__ cen) {
+    const int k = blockIdx.x;
+    const double2 c = cen[k];
+    for (int i = off[k] + threadIdx.x; i < off[k + 1]; i += blockDim.x) {
+        const double2 v = p[i];
+        p[i] = make_double2(v.x - c.x, v.y - c.y);
+    }
+}
+
+}  // namespace
+
+int run_laplace_batch(const BatchCall &b) {
+    return guarded([&] {
+        const int np = b.nprob;
+        if (np < 1) throw FmmError(4, "batch: no problems");
+        if (b.kernel != kLaplace && b.kernel != kCauchy)
+            throw FmmError(4, "batch: kernel must be 0 (lfmm2d) or 1 (cfmm2d)");
+        const bool ifc = b.charge != nullptr, ifd = b.dipstr != nullptr;
+        const bool lap = b.kernel == kLaplace;
+        if (!ifc && !ifd) throw FmmError(4, "batch: no charges and no dipoles");
+        if (ifd && lap && !b.dipvec) throw FmmError(4, "batch: dipole vectors missing");
+        std::vector<int> so(np + 1, 0), to(np + 1, 0);
+        for (int k = 0; k < np; k++) {
+            const int nk = b.ns[k], mk = b.nt ? b.nt[k] : 0;
+            if (nk < 1 || mk < 0) throw FmmError(4, "batch: ns must be >= 1 and nt >= 0");
+            if ((int64_t)so[k] + nk > INT32_MAX || (int64_t)to[k] + mk > INT32_MAX)
+                throw FmmError(4, "batch: more than 2^31 points in all");
+            so[k + 1] = so[k] + nk;
+            to[k + 1] = to[k] + mk;
+        }
+        const int NS = so[np], NT = to[np];
+        CallCtx ctx;
+        cudaStream_t s = ctx.stream();
+        prof_begin(s);
+        // ---- concatenated inputs ----
+        DevBuf<double2> src(NS, s), trg(std::max(NT, 1), s);
+        DevBuf<double2> chg(ifc ? NS : 0, s), dip(ifd ? NS : 0, s);
+        DevBuf<double> dv((ifd && lap) ? 2 * (size_t)NS : 0, s);
+        auto in = [&](void *dst, const double *user, size_t bytes) {
+            if (bytes) FMM_CUDA(cudaMemcpyAsync(dst, user, bytes, cudaMemcpyDefault, s));
+        };
+        for (int k = 0; k < np; k++) {
+            const size_t nk = b.ns[k], mk = to[k + 1] - to[k];
+            in(src.get() + so[k], b.sources[k], nk * sizeof(double2));
+            if (mk) in(trg.get() + to[k], b.targ[k], mk * sizeof(double2));
+            if (ifc) in(chg.get() + so[k], b.charge[k], nk * sizeof(double2));
+            if (ifd) in(dip.get() + so[k], b.dipstr[k], nk * sizeof(double2));
+            if (ifd && lap) in(dv.get() + 2 * (size_t)so[k], b.dipvec[k], 2 * nk * sizeof(double));
+        }
+        prof_mark("h2d", s);
+        // ---- every problem centred at the origin, one common root size ----
+        DevBuf<int> dso(np + 1, s), dto(np + 1, s);
+        FMM_CUDA(cudaMemcpyAsync(dso.get(), so.data(), (np + 1) * sizeof(int), cudaMemcpyHostToDevice, s));
+        FMM_CUDA(cudaMemcpyAsync(dto.get(), to.data(), (np + 1) * sizeof(int), cudaMemcpyHostToDevice, s));
+        DevBuf<double> bb(4 * (size_t)np, s);
+        seg_bbox_kernel<<<np, 256, 0, s>>>(src.get(), dso.get(), trg.get(), dto.get(), bb.get());
+        FMM_CHECK_LAUNCH();
+        std::vector<double> hb(4 * (size_t)np);
+        FMM_CUDA(cudaMemcpyAsync(hb.data(), bb.get(), hb.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+        FMM_CUDA(cudaStreamSynchronize(s));
+        std::vector<double2> cen(np);
+        double R = 0.0;
+        for (int k = 0; k < np; k++) {
+            const double *q = &hb[4 * (size_t)k];
+            cen[k] = make_double2((q[0] + q[1]) / 2, (q[2] + q[3]) / 2);
+            R = std::max(R, std::max(q[1] - q[0], q[3] - q[2]));
+        }
+        if (!(R > 0.0)) R = 1.0;  // every problem a single point
+        DevBuf<double2> dcen(np, s);
+        FMM_CUDA(cudaMemcpyAsync(dcen.get(), cen.data(), np * sizeof(double2), cudaMemcpyHostToDevice, s));
+        seg_shift_kernel<<<np, 256, 0, s>>>(src.get(), dso.get(), dcen.get());
+        FMM_CHECK_LAUNCH();
+        if (NT > 0) {
+            seg_shift_kernel<<<np, 256, 0, s>>>(trg.get(), dto.get(), dcen.get());
+            FMM_CHECK_LAUNCH();
+        }
+        // ---- the forest and the geometry ----
+        LapGeometry G;
+        G.lap = lap;
+        G.nd = 1;
+        G.ndc = lap ? 2 : 1;
+        G.ns = NS;
+        G.nt = NT;
+        G.eps = b.eps;
+        G.p = laplace_nterms(b.eps);
+        G.mixed = b.precision == kPrecMixed || (b.precision == kPrecAuto && b.eps >= 0.5e-6);
+        int ndiv = leaf_capacity(b.eps, NS, NT);
+        if (G.mixed && lap) ndiv = mixed_leaf_capacity(G.p, ndiv);
+        build_forest(src.get(), so, NT > 0 ? trg.get() : nullptr, to, ndiv, 0, kMaxLevels, R, s, G.T);
+        compute_lists(G.T, s);
+        prof_mark("lists", s);
+        G.src_s.alloc(NS, s);
+        G.trg_s.alloc(std::max(NT, 1), s);
+        if (G.mixed) {
+            G.src_hl.alloc(NS, s);
+            G.trg_hl.alloc(std::max(NT, 1), s);
+        }
+        auto gather = [&](int n, const int *perm, const double2 *inp, double2 *o, float4 *hl) {
+            for_each(n, s, [=] __device__(int64_t k) {
+                const double2 v = inp[perm[k]];
+                o[k] = v;
+                if (hl) hl[k] = split_pos(v);
+            });
+        };
+        gather(NS, G.T.isrc.get(), src.get(), G.src_s.get(), G.src_hl.get());
+        if (NT > 0) gather(NT, G.T.itarg.get(), trg.get(), G.trg_s.get(), G.trg_hl.get());
+        G.thresh = R * std::ldexp(1.0, -51);
+        // ---- one evaluation of the whole forest into concatenated outputs ----
+        const size_t gc = lap ? 2 : 1, hc = lap ? 3 : 1;
+        const int sp = b.ifpgh, tp = NT > 0 ? b.ifpghtarg : 0;
+        DevBuf<double2> opot(sp >= 1 ? NS : 0, s), ograd(sp >= 2 ? gc * NS : 0, s),
+            ohess(sp >= 3 ? hc * NS : 0, s), tpot(tp >= 1 ? NT : 0, s),
+            tgrad(tp >= 2 ? gc * NT : 0, s), thess(tp >= 3 ? hc * NT : 0, s);
+        FmmCall c;
+        c.kernel = b.kernel;
+        c.nd = 1;
+        c.eps = b.eps;
+        c.ns = NS;
+        c.nt = NT;
+        c.ifcharge = ifc;
+        c.ifdipole = ifd;
+        c.charge = reinterpret_cast<const double *>(chg.get());
+        c.dipstr = reinterpret_cast<const double *>(dip.get());
+        c.dipvec = dv.get();
+        c.ifpgh = sp;
+        c.ifpghtarg = tp;
+        c.pot = reinterpret_cast<double *>(opot.get());
+        c.grad = reinterpret_cast<double *>(ograd.get());
+        c.hess = reinterpret_cast<double *>(ohess.get());
+        c.pottarg = reinterpret_cast<double *>(tpot.get());
+        c.gradtarg = reinterpret_cast<double *>(tgrad.get());
+        c.hesstarg = reinterpret_cast<double *>(thess.get());
+        laplace_evaluate(c, G, true, s);
+        // ---- back to each problem's arrays ----
+        auto outk = [&](double *user, const DevBuf<double2> &d, size_t comps, size_t off, size_t n) {
+            if (user && n)
+                FMM_CUDA(cudaMemcpyAsync(user, d.get() + comps * off, comps * n * sizeof(double2),
+                                         cudaMemcpyDefault, s));
+        };
+        for (int k = 0; k < np; k++) {
+            const size_t nk = b.ns[k], mk = to[k + 1] - to[k];
+            if (sp >= 1) outk(b.pot[k], opot, 1, so[k], nk);
+            if (sp >= 2) outk(b.grad[k], ograd, gc, so[k], nk);
+            if (sp >= 3) outk(b.hess[k], ohess, hc, so[k], nk);
+            if (tp >= 1) outk(b.pottarg[k], tpot, 1, to[k], mk);
+            if (tp >= 2) outk(b.gradtarg[k], tgrad, gc, to[k], mk);
+            if (tp >= 3) outk(b.hesstarg[k], thess, hc, to[k], mk);
+        }
+        FMM_CUDA(cudaStreamSynchronize(s));
+        prof_mark("scatter_d2h", s);
+        prof_end(s);
+    });
+}
+
 int run_fmm(const FmmCall &c) {
     return guarded([&] {
         if (c.ns < 1) throw FmmError(4, "ns must be at least 1");

@@ -59,6 +59,24 @@ struct M2LCache;
 void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaStream_t s,
                       M2LCache *m2l = nullptr, bool sync = true);
 
+// A batch of independent lfmm2d / cfmm2d problems (nd = 1) with the same
+// eps and flags, evaluated as one forest: one launch per level and pass for
+// the whole batch.  Arrays per problem, host or device (all of one kind
+// per array list); a null charge / dipstr list means no charges / dipoles.
+struct BatchCall {
+    Kernel kernel = kLaplace;
+    double eps = 1e-6;
+    int nprob = 0;
+    const int *ns = nullptr, *nt = nullptr;
+    const double *const *sources = nullptr, *const *targ = nullptr;
+    const double *const *charge = nullptr, *const *dipstr = nullptr, *const *dipvec = nullptr;
+    int ifpgh = 0, ifpghtarg = 0;
+    double *const *pot = nullptr, *const *grad = nullptr, *const *hess = nullptr;
+    double *const *pottarg = nullptr, *const *gradtarg = nullptr, *const *hesstarg = nullptr;
+    int precision = kPrecAuto;
+};
+int run_laplace_batch(const BatchCall &b);
+
 // Runs the evaluation on the calling thread's current device; returns the
 // reference's ier (0 ok, 4 failure) after recording any error message.
 int run_fmm(const FmmCall &c);

@@ -947,6 +947,9 @@ uint64_t m2l_window_fp32(const Tree &T, const CauchyProblem &P, const float2 *mp
                          int *err, cudaStream_t s) {
     const int HALF = P.p + 1 <= 12 ? 12 : (P.p + 1 <= 16 ? 16 : (P.p + 1 <= 20 ? 20 : 0));
     if (HALF == 0) return 0;
+    // (the runs are found from box positions, which the trees of a forest
+    // share: forests use the slot tables)
+    if (T.nroots > 1) return 0;
     const int CH = P.ndc % 2 == 0 ? 2 : 1;
     bool ok = false;
     const auto Wp = m2l_cached<WinPlan>(P.m2l_cache, ((uint64_t)2 << 56) | (uint64_t)CH, ok,

@@ -290,10 +290,12 @@ struct Builder {
         const int *par = T.parent.get(), *chi = T.child.get();
         const double2 *cen = T.centers.get();
         if (l0 == 0) {
-            for_each(1, s, [=] __device__(int64_t) {
-                nnb[0] = 1;
-                nb[0] = 0;
-                for (int k = 1; k < 9; k++) nb[k] = -1;
+            // roots (one per problem of a forest): their own only colleague
+            for_each(T.lend[0] - T.lstart[0], s, [=] __device__(int64_t i) {
+                const int b = (int)i;
+                nnb[b] = 1;
+                nb[9 * b] = b;
+                for (int k = 1; k < 9; k++) nb[9 * b + k] = -1;
             });
             l0 = 1;
         }
@@ -640,8 +642,9 @@ struct Builder {
     // leaves hold the same points, in the same order of leaves, as the
     // reference's sorted arrays); inside every leaf the points go back to
     // input order.  `idx` maps key-sorted positions to input indices.
+    // prob (forests): the problem, i.e. the root, of every input point.
     void finish_points(const uint32_t *idx, const KeyView &kv, int n, const DevBuf<int2> &R,
-                       DevBuf<int2> &se, DevBuf<int> &perm) {
+                       DevBuf<int2> &se, DevBuf<int> &perm, const uint32_t *prob = nullptr) {
         const int nb = T.nboxes;
         se.alloc(nb, s);
         FMM_CUDA(cudaMemcpyAsync(se.get(), R.get(), (size_t)nb * sizeof(int2),
@@ -668,7 +671,7 @@ struct Builder {
         DevBuf<uint32_t> keys(n, s), vals(n, s), kt(n, s), vt(n, s);
         uint32_t *kp = keys.get(), *vp = vals.get();
         for_each(n, s, [=] __device__(int64_t k) {
-            int b = 0, m = 0;
+            int b = prob ? (int)prob[idx[k]] : 0, m = 0;
             while (nch[b] > 0) {
                 m++;
                 b = chi[4 * b + key_digit(kv, k, m)];
@@ -698,8 +701,10 @@ struct KeyedPoints {
 
 // Computes the path keys of levels 1..ds and sorts the points by them
 // (stable, so equal keys keep input order).
+// prob (optional): the problem of every input point of a forest, pbits its
+// bit count; the points are then sorted by (problem, path).
 void key_sort(const double2 *pts, int n, double2 c0, const double *d_bsl, int ds,
-              KeyedPoints &kp, cudaStream_t s) {
+              KeyedPoints &kp, cudaStream_t s, const uint32_t *prob = nullptr, int pbits = 0) {
     const int nw = (ds + 15) / 16;
     kp.words.clear();
     kp.words.resize(nw);
@@ -728,10 +733,14 @@ void key_sort(const double2 *pts, int n, double2 c0, const double *d_bsl, int ds
         const int lo = (32 - used) & ~7;
         radix_sort_pairs(kp0, ip, kt.get(), vt.get(), n, 32, s, lo);
     }
+    if (prob && pbits > 0) {
+        for_each(n, s, [=] __device__(int64_t k) { kp0[k] = prob[ip[k]]; });
+        radix_sort_pairs(kp0, ip, kt.get(), vt.get(), n, pbits, s);
+    }
     for (int w = 0; w < nw; w++) {
         kp.words[w].alloc(n, s);
         uint32_t *o = kp.words[w].get();
-        if (w == 0) {
+        if (w == 0 && !(prob && pbits > 0)) {
             FMM_CUDA(cudaMemcpyAsync(o, kp0, (size_t)n * sizeof(uint32_t),
                                      cudaMemcpyDeviceToDevice, s));
         } else {
@@ -929,8 +938,19 @@ void build_levelwise(const double2 *d_src, int ns, const double2 *d_targ, int nt
 // the sorted order (three binary searches per refined box instead of a pass
 // over all points).  Returns false when the tree needs digits of levels
 // beyond ds; the caller then retries with more.
+// Forest (F non-null): F->nroots roots share the root square; root r holds
+// the points [soff[r], soff[r+1]) and [toff[r], toff[r+1]) of the
+// concatenated arrays, whose problem ids (sprob, tprob) order the sort.
+struct ForestRoots {
+    int nroots = 1;
+    const int *d_soff = nullptr, *d_toff = nullptr;
+    const uint32_t *sprob = nullptr, *tprob = nullptr;
+    int pbits = 0;
+};
+
 bool build_by_keys(const double2 *d_src, int ns, const double2 *d_targ, int nt, int ndiv,
-                   int idivflag, int nlmax, double2 c0, int ds, cudaStream_t s, Tree &T) {
+                   int idivflag, int nlmax, double2 c0, int ds, cudaStream_t s, Tree &T,
+                   const ForestRoots *F = nullptr) {
     const double bs0 = T.boxsize[0];
     T = Tree();
     T.boxsize.push_back(bs0);
@@ -943,27 +963,30 @@ bool build_by_keys(const double2 *d_src, int ns, const double2 *d_targ, int nt, 
     FMM_CUDA(cudaMemcpyAsync(d_bsl.get(), bsl.data(), bsl.size() * sizeof(double),
                              cudaMemcpyHostToDevice, s));
     KeyedPoints ks, kt;
-    key_sort(d_src, ns, c0, d_bsl.get(), ds, ks, s);
-    key_sort(d_targ, nt, c0, d_bsl.get(), ds, kt, s);
+    const int nroots = F ? F->nroots : 1;
+    key_sort(d_src, ns, c0, d_bsl.get(), ds, ks, s, F ? F->sprob : nullptr, F ? F->pbits : 0);
+    key_sort(d_targ, nt, c0, d_bsl.get(), ds, kt, s, F ? F->tprob : nullptr, F ? F->pbits : 0);
     B.kvs = ks.view();
     B.kvt = kt.view();
-    B.ensure(1024);
-    T.nboxes = 1;
+    B.ensure(std::max(1024, 4 * nroots));
+    T.nboxes = nroots;
     T.lstart.push_back(0);
-    T.lend.push_back(1);
+    T.lend.push_back(nroots);
     {
         double2 *cen = T.centers.get();
         int *lev = T.level.get(), *par = T.parent.get(), *nch = T.nchild.get(),
             *chi = T.child.get();
         int2 *r0 = B.rs.get(), *r1 = B.rt.get();
-        for_each(1, s, [=] __device__(int64_t) {
-            cen[0] = c0;
-            lev[0] = 0;
-            par[0] = -1;
-            nch[0] = 0;
-            for (int j = 0; j < 4; j++) chi[j] = -1;
-            r0[0] = make_int2(0, ns);
-            r1[0] = make_int2(0, nt);
+        const int *so = F ? F->d_soff : nullptr, *to = F ? F->d_toff : nullptr;
+        for_each(nroots, s, [=] __device__(int64_t i) {
+            const int b = (int)i;
+            cen[b] = c0;
+            lev[b] = 0;
+            par[b] = -1;
+            nch[b] = 0;
+            for (int j = 0; j < 4; j++) chi[4 * b + j] = -1;
+            r0[b] = so ? make_int2(so[b], so[b + 1]) : make_int2(0, ns);
+            r1[b] = to ? make_int2(to[b], to[b + 1]) : make_int2(0, nt);
         });
     }
     DevBuf<int> nflag(1, s);
@@ -1005,8 +1028,8 @@ bool build_by_keys(const double2 *d_src, int ns, const double2 *d_targ, int nt, 
     B.computecoll(0, T.nlevels);
     if (T.nlevels >= 2) B.fix_lr();
     prof_mark("tree_fixlr", s);
-    B.finish_points(ks.idx.get(), B.kvs, ns, B.rs, T.srcse, T.isrc);
-    B.finish_points(kt.idx.get(), B.kvt, nt, B.rt, T.trgse, T.itarg);
+    B.finish_points(ks.idx.get(), B.kvs, ns, B.rs, T.srcse, T.isrc, F ? F->sprob : nullptr);
+    B.finish_points(kt.idx.get(), B.kvt, nt, B.rt, T.trgse, T.itarg, F ? F->tprob : nullptr);
     prof_mark("tree_sort", s);
     return true;
 }
@@ -1059,6 +1082,61 @@ void build_tree(const double2 *d_src, int ns, const double2 *d_targ, int nt,
     FMM_CUDA(cudaStreamSynchronize(s));
 }
 
+void build_forest(const double2 *d_src, const std::vector<int> &soff, const double2 *d_targ,
+                  const std::vector<int> &toff, int ndiv, int idivflag, int nlmax, double bs0,
+                  cudaStream_t s, Tree &T) {
+    T = Tree();
+    const int nprob = (int)soff.size() - 1;
+    const int ns = soff.back(), nt = toff.back();
+    T.boxsize.push_back(bs0);
+    DevBuf<int> dso(nprob + 1, s), dto(nprob + 1, s);
+    FMM_CUDA(cudaMemcpyAsync(dso.get(), soff.data(), (nprob + 1) * sizeof(int),
+                             cudaMemcpyHostToDevice, s));
+    FMM_CUDA(cudaMemcpyAsync(dto.get(), toff.data(), (nprob + 1) * sizeof(int),
+                             cudaMemcpyHostToDevice, s));
+    // problem of every point (binary search in the offsets)
+    DevBuf<uint32_t> sp(std::max(ns, 1), s), tp(std::max(nt, 1), s);
+    auto prob_of = [&](int n, const int *off, uint32_t *out) {
+        for_each(n, s, [=] __device__(int64_t i) {
+            int lo = 0, hi = nprob;
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (off[mid] <= i) lo = mid; else hi = mid;
+            }
+            out[i] = (uint32_t)lo;
+        });
+    };
+    prob_of(ns, dso.get(), sp.get());
+    prob_of(nt, dto.get(), tp.get());
+    ForestRoots F;
+    F.nroots = nprob;
+    F.d_soff = dso.get();
+    F.d_toff = dto.get();
+    F.sprob = sp.get();
+    F.tprob = tp.get();
+    F.pbits = 1;
+    while ((1 << F.pbits) < nprob) F.pbits++;
+    int64_t nref = 0;
+    for (int k = 0; k < nprob; k++) {
+        const int64_t a = soff[k + 1] - soff[k], b = toff[k + 1] - toff[k];
+        nref = std::max<int64_t>(nref, idivflag == 0 ? a : (idivflag == 1 ? b : std::max(a, b)));
+    }
+    int ds = 2;
+    for (int64_t q = std::max<int64_t>(ndiv, 1); q < nref && ds < nlmax; q *= 4) ds++;
+    ds = std::min(ds, nlmax);
+    const double2 c0 = make_double2(0.0, 0.0);
+    while (!build_by_keys(d_src, ns, d_targ, nt, ndiv, idivflag, nlmax, c0, ds, s, T, &F)) {
+        T.boxsize.assign(1, bs0);
+        ds = std::min(nlmax, ds + 8);
+    }
+    T.nroots = nprob;
+    T.d_boxsize.alloc(T.nlevels + 2, s);
+    std::vector<double> bsx(T.boxsize);
+    bsx.push_back(T.boxsize.back() / 2);
+    FMM_CUDA(cudaMemcpyAsync(T.d_boxsize.get(), bsx.data(), bsx.size() * sizeof(double),
+                             cudaMemcpyHostToDevice, s));
+    FMM_CUDA(cudaStreamSynchronize(s));
+}
 
 void compute_lists(Tree &T, cudaStream_t s) {
     const int nb = T.nboxes;
@@ -1097,7 +1175,7 @@ void compute_lists(Tree &T, cudaStream_t s) {
         const int l = lev[b];
         int c1 = 0, c2 = 0, c3 = 0, c4 = 0;
         if (l == 0) {
-            if (nch[0] == 0) l1[c1++] = 0;
+            if (nch[b] == 0) l1[kMaxList1 * b + c1++] = b;
             n1[b] = c1;
             n2[b] = 0;
             n3[b] = 0;

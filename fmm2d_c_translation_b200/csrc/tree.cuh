@@ -35,6 +35,7 @@ struct Tree {
     // interaction lists
     DevBuf<int> nlist1, list1, nlist2, list2, nlist3, list3, nlist4, list4;
     DevBuf<double> d_boxsize;  // boxsize per level on the device
+    int nroots = 1;            // > 1: a forest of independent problems
 };
 
 // Builds the tree over ns sources and nt targets (device arrays of (x, y)
@@ -42,6 +43,16 @@ struct Tree {
 // larger.  Follows pts_tree_mem / pts_tree_build / pts_tree_sort.
 void build_tree(const double2 *d_src, int ns, const double2 *d_targ, int nt,
                 int ndiv, int idivflag, int nlmax, cudaStream_t s, Tree &T);
+
+// A forest of independent trees for a batch of problems: the concatenated
+// points of problem k are [soff[k], soff[k+1]) and [toff[k], toff[k+1]),
+// already translated so that every problem's bounding square is centred at
+// the origin; bs0 is the common root size.  The roots are boxes 0 .. k-1,
+// each level holds the boxes of all problems, and no list crosses problems
+// (each root is its own only colleague).
+void build_forest(const double2 *d_src, const std::vector<int> &soff, const double2 *d_targ,
+                  const std::vector<int> &toff, int ndiv, int idivflag, int nlmax, double bs0,
+                  cudaStream_t s, Tree &T);
 
 // computelists (c_translation/src/tree_routs2d.c:369-510).
 void compute_lists(Tree &T, cudaStream_t s);

@@ -719,6 +719,32 @@ int fmm2d_b200_plan_eval(void *plan, const double _Complex *charge,
 int fmm2d_b200_plan_destroy(void *plan);
 int fmm2d_b200_plan_uses_graph(void *plan);
 
+/* Batch of independent problems (no counterpart in the reference): nprob
+ * lfmm2d (kernel 0) or cfmm2d (kernel 1) evaluations with nd = 1 and the
+ * same eps and output flags, run as one forest of trees -- one launch per
+ * level and pass for the whole batch.  Problem k has ns[k] sources
+ * sources[k] (2 x ns[k]) with charge[k] / dipstr[k] (ns[k] complex;
+ * pass charge = NULL or dipstr = NULL for none) and dipvec[k] (2 x ns[k],
+ * lfmm2d dipoles), nt[k] targets targ[k] (nt may be NULL: no targets), and
+ * its outputs in pot[k], grad[k], hess[k], pottarg[k], ... in the guru
+ * drivers' layouts (overwritten).  Host or device arrays.  Each problem is
+ * translated so that its bounding square is centred at the origin and all
+ * trees share the largest root size, so the trees differ from the
+ * one-problem calls' and the results agree with them to the accuracy eps
+ * asks for, not to the bit.  Returns 0 or 4. */
+int fmm2d_b200_fmm2d_batch(int kernel, int nprob, double eps, const int *ns,
+                           const double *const *sources,
+                           const double _Complex *const *charge,
+                           const double _Complex *const *dipstr,
+                           const double *const *dipvec, int ifpgh,
+                           double _Complex *const *pot,
+                           double _Complex *const *grad,
+                           double _Complex *const *hess, const int *nt,
+                           const double *const *targ, int ifpghtarg,
+                           double _Complex *const *pottarg,
+                           double _Complex *const *gradtarg,
+                           double _Complex *const *hesstarg);
+
 /* Direct sums on the GPU, incrementing the outputs (the reference's
  * l2d_direct* / c2d_direct* kernels, src/laplace/lapkernels2d.f,
  * src/laplace/cauchykernels2d.f): every target against every source. */
