@@ -604,7 +604,12 @@ def measure_serving(fm, args):
     wall, lat, pts, st = run(reqs, args.serve_slots, 0, rate=rate)
     lat = np.array(lat)
     base = reqs[: min(len(reqs), 200)]
-    wall1, lat1, pts1, _ = run(base, 1, 1)
+    # the baseline runs one request at a time: no batching either
+    os.environ["FMM2D_B200_SERVE_BATCH"] = "0"
+    try:
+        wall1, lat1, pts1, _ = run(base, 1, 1)
+    finally:
+        os.environ.pop("FMM2D_B200_SERVE_BATCH", None)
     return {
         "requests": len(reqs), "slots": args.serve_slots,
         "hbm_budget_gb": args.serve_budget_gb,
@@ -613,6 +618,7 @@ def measure_serving(fm, args):
         "mean_ms": float(lat.mean()), "throughput_req_s": len(reqs) / wall,
         "throughput_points_s": pts / wall, "burst_points_s": pts_b / wall_b,
         "peak_running": st["peak_running"], "peak_budget_gb": st["peak_bytes"] / 1e9,
+        "batched_requests": st.get("batched", 0),
         "one_at_a_time_fp64": {"requests": len(base), "points_s": pts1 / wall1,
                                "req_s": len(base) / wall1,
                                "p50_ms": float(np.percentile(lat1, 50))},

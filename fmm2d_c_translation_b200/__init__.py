@@ -464,8 +464,11 @@ class Server:
     def stats(self):
         out = np.zeros(6)
         self._L.fmm2d_b200_server_stats(self._h, _ptr(out))
+        self._L.fmm2d_b200_server_batched.restype = ctypes.c_longlong
+        self._L.fmm2d_b200_server_batched.argtypes = [_P]
         return dict(bytes_in_use=out[0], peak_bytes=out[1], queued=int(out[2]),
-                    running=int(out[3]), rejected=int(out[4]), peak_running=int(out[5]))
+                    running=int(out[3]), rejected=int(out[4]), peak_running=int(out[5]),
+                    batched=int(self._L.fmm2d_b200_server_batched(self._h)))
 
     def request_bytes(self, req):
         return self._L.fmm2d_b200_request_bytes(ctypes.byref(req))

@@ -11,6 +11,15 @@
 // comes from the device's stream-ordered pool, so a finished request's
 // blocks are reused by the next ones without returning to the driver.
 //
+// Continuous batching: a worker that takes a small lfmm2d request also
+// takes the queued requests of the same kind (eps, precision, strengths,
+// output flags) that fit the budget, up to kBatchMax requests and
+// kBatchPoints points, and evaluates them together as one forest
+// (run_laplace_batch): one launch per level and pass for all of them.  Their
+// trees differ from the ones they would get alone, so their results agree
+// with the alone ones to the requested eps.  FMM2D_B200_SERVE_BATCH=0, read
+// when the server is made, turns batching off.
+//
 // The reference has no counterpart (its entry points are single calls).
 #include <algorithm>
 #include <chrono>
@@ -20,6 +29,8 @@
 #include <thread>
 #include <unordered_map>
 #include <vector>
+#include <stdlib.h>
+#include <string.h>
 
 #include "engine.cuh"
 #include "helmholtz.cuh"
@@ -60,6 +71,21 @@ double footprint_bytes(const FmmCall &c) {
     return 1.25 * (pts + strengths + outs + tree + 16.0 * coeffs) + (1 << 20);
 }
 
+constexpr int kBatchMax = 64;
+constexpr int kBatchPoints = 200000;   // points of one batch
+constexpr int kBatchRequest = 50000;   // largest request that is batched
+
+bool batchable(const FmmCall &c) {
+    return c.kernel == kLaplace && c.nd == 1 && c.ndiv < 0 && c.ifnear == 1 && !c.timeinfo &&
+           (int64_t)c.ns + c.nt <= kBatchRequest;
+}
+
+bool same_kind(const FmmCall &a, const FmmCall &b) {
+    return a.eps == b.eps && a.precision == b.precision && a.ifcharge == b.ifcharge &&
+           a.ifdipole == b.ifdipole && a.ifpgh == b.ifpgh && (a.nt > 0) == (b.nt > 0) &&
+           (a.nt == 0 || a.ifpghtarg == b.ifpghtarg);
+}
+
 struct Request {
     FmmCall call;
     double bytes = 0;
@@ -72,6 +98,8 @@ class Server {
   public:
     Server(int slots, double budget, int device)
         : budget_(budget), device_(device) {
+        const char *e = getenv("FMM2D_B200_SERVE_BATCH");
+        batch_ = !(e && !strcmp(e, "0"));
         for (int i = 0; i < slots; i++) workers_.emplace_back([this] { loop(); });
     }
     ~Server() {
@@ -136,6 +164,12 @@ class Server {
         out[5] = peak_running_;
     }
 
+    // requests that ran in batches of two or more
+    long long batched() {
+        std::lock_guard<std::mutex> g(mu_);
+        return batched_;
+    }
+
   private:
     static constexpr size_t kWindow = 64;
 
@@ -153,32 +187,103 @@ class Server {
         return false;
     }
 
+    // Queued requests of r's kind that fit the budget (mu_ held).
+    void gather_batch(Request *r, std::vector<Request *> &batch) {
+        int64_t pts = (int64_t)r->call.ns + r->call.nt;
+        size_t i = 0;
+        while (i < std::min(queue_.size(), kWindow) && (int)batch.size() < kBatchMax) {
+            Request *q = reqs_[queue_[i]];
+            const int64_t n = (int64_t)q->call.ns + q->call.nt;
+            if (batchable(q->call) && same_kind(r->call, q->call) && pts + n <= kBatchPoints &&
+                in_use_ + q->bytes <= budget_) {
+                batch.push_back(q);
+                in_use_ += q->bytes;
+                pts += n;
+                queue_.erase(queue_.begin() + (long)i);
+            } else {
+                i++;
+            }
+        }
+    }
+
+    int run_batch(const std::vector<Request *> &batch) {
+        const size_t n = batch.size();
+        std::vector<int> ns(n), nt(n);
+        std::vector<const double *> src(n), trg(n), q(n), d(n), v(n);
+        std::vector<double *> o[6];
+        for (auto &x : o) x.resize(n);
+        for (size_t k = 0; k < n; k++) {
+            const FmmCall &c = batch[k]->call;
+            ns[k] = c.ns;
+            nt[k] = c.nt;
+            src[k] = c.sources;
+            trg[k] = c.targ;
+            q[k] = c.charge;
+            d[k] = c.dipstr;
+            v[k] = c.dipvec;
+            o[0][k] = c.pot;
+            o[1][k] = c.grad;
+            o[2][k] = c.hess;
+            o[3][k] = c.pottarg;
+            o[4][k] = c.gradtarg;
+            o[5][k] = c.hesstarg;
+        }
+        const FmmCall &c0 = batch[0]->call;
+        BatchCall b;
+        b.kernel = c0.kernel;
+        b.eps = c0.eps;
+        b.nprob = (int)n;
+        b.ns = ns.data();
+        b.nt = nt.data();
+        b.sources = src.data();
+        b.targ = trg.data();
+        b.charge = c0.ifcharge ? q.data() : nullptr;
+        b.dipstr = c0.ifdipole ? d.data() : nullptr;
+        b.dipvec = c0.ifdipole ? v.data() : nullptr;
+        b.ifpgh = c0.ifpgh;
+        b.ifpghtarg = c0.ifpghtarg;
+        b.pot = o[0].data();
+        b.grad = o[1].data();
+        b.hess = o[2].data();
+        b.pottarg = o[3].data();
+        b.gradtarg = o[4].data();
+        b.hesstarg = o[5].data();
+        b.precision = c0.precision;
+        return run_laplace_batch(b);
+    }
+
     void loop() {
         cudaSetDevice(device_);
         for (;;) {
             long long id = -1;
-            Request *r = nullptr;
+            std::vector<Request *> batch;
             {
                 std::unique_lock<std::mutex> lk(mu_);
                 // queued work is drained before a stopping server exits
                 cv_work_.wait(lk, [&] { return pick(id) || (stop_ && queue_.empty()); });
                 if (id < 0) return;
-                r = reqs_[id];
+                Request *r = reqs_[id];
+                batch.push_back(r);
                 in_use_ += r->bytes;
+                if (batch_ && batchable(r->call)) gather_batch(r, batch);
                 peak_in_use_ = std::max(peak_in_use_, in_use_);
-                running_++;
+                running_ += (int)batch.size();
                 peak_running_ = std::max(peak_running_, running_);
+                if (batch.size() > 1) batched_ += (long long)batch.size();
             }
-            r->t_start = now_ms();
-            const int ier = run_fmm(r->call);
+            const double t0 = now_ms();
+            for (Request *r : batch) r->t_start = t0;
+            const int ier = batch.size() == 1 ? run_fmm(batch[0]->call) : run_batch(batch);
             const double t_end = now_ms();
             {
                 std::lock_guard<std::mutex> g(mu_);
-                r->ier = ier;
-                r->t_end = t_end;
-                r->done = true;
-                in_use_ -= r->bytes;
-                running_--;
+                for (Request *r : batch) {
+                    r->ier = ier;
+                    r->t_end = t_end;
+                    r->done = true;
+                    in_use_ -= r->bytes;
+                }
+                running_ -= (int)batch.size();
             }
             cv_done_.notify_all();
             cv_work_.notify_all();
@@ -195,7 +300,8 @@ class Server {
     long long next_id_ = 0;
     double in_use_ = 0, peak_in_use_ = 0;
     int running_ = 0, peak_running_ = 0, rejected_ = 0;
-    bool stop_ = false;
+    long long batched_ = 0;
+    bool stop_ = false, batch_ = true;
 };
 
 }  // namespace
@@ -290,3 +396,8 @@ FMM_EXPORT double fmm2d_b200_request_bytes(const fmm2d_b200_request *q) {
 }
 
 FMM_EXPORT void fmm2d_b200_server_destroy(void *srv) { delete static_cast<Server *>(srv); }
+
+// Requests of the server that ran in batches of two or more so far.
+FMM_EXPORT long long fmm2d_b200_server_batched(void *srv) {
+    return srv ? static_cast<Server *>(srv)->batched() : 0;
+}

@@ -845,6 +845,14 @@ void fmm2d_b200_server_stats(void *server, double *out6);
 double fmm2d_b200_request_bytes(const fmm2d_b200_request *req);
 /* Finishes the queued requests, then stops the workers. */
 void fmm2d_b200_server_destroy(void *server);
+/* Requests that ran in batches of two or more so far: a worker that takes
+ * a small lfmm2d request (nd = 1, at most 50,000 points) also takes the
+ * queued requests of the same eps, precision, strengths and output flags
+ * that fit the budget (up to 64 requests, 200,000 points) and evaluates
+ * them as one forest (fmm2d_b200_fmm2d_batch); their results agree with
+ * the alone ones to the requested eps.  FMM2D_B200_SERVE_BATCH=0, read when
+ * the server is made, turns this off. */
+long long fmm2d_b200_server_batched(void *server);
 
 /* Quadtree inspection in the reference's layout (pts_tree_mem/build/sort,
  * src/common/pts_tree2d.f:34,406,1222; computelists,

@@ -43,7 +43,9 @@ def test_footprint_grows_with_size(fm):
 
 
 @pytest.mark.gpu
-def test_mixed_stream_matches_alone(fm):
+def test_mixed_stream_matches_alone(fm, monkeypatch):
+    # (without batching: every request runs on its own tree, as alone)
+    monkeypatch.setenv("FMM2D_B200_SERVE_BATCH", "0")
     specs = [("l", 20000, 1e-6, 0), ("h", 8000, 1e-6, 1), ("c", 15000, 1e-9, 0),
              ("l", 3000, 1e-3, 1), ("h", 30000, 1e-9, 0), ("l", 60000, 1e-9, 1),
              ("c", 1000, 1e-3, 1), ("h", 2000, 1e-6, 1)] * 3
@@ -93,3 +95,31 @@ def test_concurrent_orders_all_succeed(fm):
     iers = [srv.wait(t)[0] for t in tickets]
     srv.close()
     assert iers == [0] * len(iers), fm.last_error()
+
+
+@pytest.mark.gpu
+def test_batched_stream_matches_alone(fm, monkeypatch):
+    """Small lfmm2d requests queued together run in batches (one forest per
+    batch); each result agrees with the request run alone to its eps."""
+    monkeypatch.delenv("FMM2D_B200_SERVE_BATCH", raising=False)
+    specs = [(500 + 331 * i, 1e-6 if i % 2 else 1e-9, i % 3 == 0) for i in range(40)]
+    alone = []
+    for i, (n, eps, pgt) in enumerate(specs):
+        r, keep = _req(fm, "l", n, 700 + i, eps=eps, pgt=int(pgt))
+        srv1 = fm.Server(slots=1, hbm_budget=100e9)
+        t = srv1.submit(r, keep)
+        assert srv1.wait(t)[0] == 0
+        srv1.close()
+        alone.append((keep, eps))
+    srv = fm.Server(slots=2, hbm_budget=100e9)
+    tickets = []
+    for i, (n, eps, pgt) in enumerate(specs):
+        r, keep = _req(fm, "l", n, 700 + i, eps=eps, pgt=int(pgt))
+        tickets.append((srv.submit(r, keep), keep))
+    for (t, keep), (ref, eps) in zip(tickets, alone):
+        assert srv.wait(t)[0] == 0
+        for key in ref:
+            if key.startswith(("pot", "grad")):
+                assert W.rel_err(keep[key], ref[key]) <= max(2 * eps, 1e-12), key
+    assert srv.stats()["batched"] >= 2
+    srv.close()
