@@ -138,6 +138,24 @@ def parse_profile(s):
     return out
 
 
+def max_over_ranks(value, ws, device=None):
+    """The largest of a per-rank value over all ranks (the step time of the
+    rank that finished last); the value itself on one rank."""
+    if ws <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(points_per_rank, ws, step_ms):
+    """points/s of the whole job: every rank's points over the slowest
+    rank's step time (replicas: each rank evaluates a full problem)."""
+    return ws * points_per_rank / (step_ms * 1e-3)
+
+
 def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -266,6 +284,8 @@ def main():
     ap.add_argument("--cpu-threads", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the library's default leaf capacity and M2L form")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the other configurations (c1, c3, c4)")
     ap.add_argument("--serve-requests", type=int, default=2000)
@@ -323,6 +343,25 @@ def main():
 
     dev_args = (d_src, d_trg, d_q, d_d, d_v, d_pot, d_grad, d_pt, d_gt)
 
+    # the library's autotuner picks the leaf capacity and M2L form of the
+    # mixed path for this workload's order on its own points (untimed)
+    tuned = None
+    mixed_run = args.precision == "mixed" or (args.precision == "auto" and args.eps >= 0.5e-6)
+    if mixed_run and not args.no_autotune:
+        nd_, fm_, ms_ = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_double(0)
+        t0 = time.perf_counter()
+        L.fmm2d_b200_autotune.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, P,
+                                          ctypes.c_int, P, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_int, P, P, P]
+        ier_t = L.fmm2d_b200_autotune(0, args.eps, ns, ptr(d_src), nt, ptr(d_trg), 1, 1, 2, 2,
+                                      ctypes.byref(nd_), ctypes.byref(fm_), ctypes.byref(ms_))
+        torch.cuda.synchronize()
+        if ier_t == 0:
+            tuned = {"leaf_capacity": nd_.value,
+                     "m2l_form": ["window", "tile", "simt"][fm_.value],
+                     "best_ms": ms_.value, "tuning_s": time.perf_counter() - t0,
+                     "grid": "leaf capacity {12..64} x M2L form {window, tile, simt}"}
+
     def timed(a, steps, profile=False):
         L.fmm2d_b200_set_profiling(1 if profile else 0)
         evs = []
@@ -363,11 +402,7 @@ def main():
         barrier()
         clk = clocks.stop()
         eps.value = args.eps
-        t = sum(ms) / len(ms)
-        if ws > 1:
-            tt = torch.tensor([t], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t = float(tt.item())
+        t = max_over_ranks(sum(ms) / len(ms), ws, dev)
         return t, prof, clk, int(n1 - n0)
 
     def accuracy(precision, eps_value=None):
@@ -396,7 +431,7 @@ def main():
                 "gradtarg_rel_l2": rel(got_g, grad.view(-1, 4)), "targets": m}
 
     t_step, prof, clk, nlaunch = measure(args.precision)
-    value = ws * (ns + nt) / (t_step * 1e-3)
+    value = whole_job_rate(ns + nt, ws, t_step)
     fp64 = None
     if args.precision != "fp64" and not args.no_fp64_compare:
         # the plain form of the workload: all-FP64 at eps = plain_eps
@@ -429,11 +464,7 @@ def main():
         barrier()
         ms_e2e, _ = timed(h_args, args.steps)
         barrier()
-        te = sum(ms_e2e) / len(ms_e2e)
-        if ws > 1:
-            tt = torch.tensor([te], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            te = float(tt.item())
+        te = max_over_ranks(sum(ms_e2e) / len(ms_e2e), ws, dev)
         h2d = sum(x.numel() * 8 for x in h_args[:5])
         d2h = sum(x.numel() * 8 for x in h_args[5:])
         e2e = {"value": ws * (ns + nt) / (te * 1e-3), "unit": "points/s",
@@ -519,7 +550,7 @@ def main():
                    "l2": "inputs 0.8 GB > L2; no flush"},
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": nlaunch, "clocks": clk, "fp64_plain": fp64,
-        "accuracy": acc, "serving": serving, "configs": configs,
+        "accuracy": acc, "serving": serving, "configs": configs, "autotune": tuned,
     }
     print(json.dumps(line))
     return 0

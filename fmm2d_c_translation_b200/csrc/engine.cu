@@ -231,15 +231,24 @@ void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaS
             o[a] = v;
             if (o32) o32[a] = make_float2((float)v.x, (float)v.y);
         };
-        if (c.ifcharge) {
+        // one pass over the points for charges and dipoles together
+        const bool ifc = c.ifcharge, ifd = c.ifdipole;
+        if (ifc) {
             chg_s.alloc((size_t)ns * ndc, s);
             if (mixed) chg32.alloc((size_t)ns * ndc, s);
-            const double2 *q = chg_in.ptr;
-            double2 *qo = chg_s.get();
-            float2 *q32 = chg32.get();
-            for_each(ns, s, [=] __device__(int64_t k) {
-                const int i = perm[k];
-                for (int j = 0; j < nd; j++) {
+        }
+        if (ifd) {
+            dip_s.alloc((size_t)ns * ndc, s);
+            if (mixed) dip32.alloc((size_t)ns * ndc, s);
+        }
+        const double2 *q = chg_in.ptr, *d = dip_in.ptr;
+        const double *dv = dv_in.ptr;
+        double2 *qo = chg_s.get(), *dout = dip_s.get();
+        float2 *q32 = chg32.get(), *d32 = dip32.get();
+        for_each(ns, s, [=] __device__(int64_t k) {
+            const int i = perm[k];
+            for (int j = 0; j < nd; j++) {
+                if (ifc) {
                     const double2 v = q[(size_t)i * nd + j];
                     if (lap) {
                         // charge1(1:2, j, i) = (Re q, Im q)  (lfmm2d.f:141-147)
@@ -249,18 +258,7 @@ void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaS
                         put(qo, q32, (size_t)k * ndc + j, v);
                     }
                 }
-            });
-        }
-        if (c.ifdipole) {
-            dip_s.alloc((size_t)ns * ndc, s);
-            if (mixed) dip32.alloc((size_t)ns * ndc, s);
-            const double2 *d = dip_in.ptr;
-            const double *dv = dv_in.ptr;
-            double2 *dout = dip_s.get();
-            float2 *d32 = dip32.get();
-            for_each(ns, s, [=] __device__(int64_t k) {
-                const int i = perm[k];
-                for (int j = 0; j < nd; j++) {
+                if (ifd) {
                     const double2 v = d[(size_t)i * nd + j];
                     if (lap) {
                         // dipstr1 = (Re d, Im d) * (-(v1 + i v2))  (lfmm2d.f:149-157)
@@ -273,8 +271,8 @@ void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaS
                         put(dout, d32, (size_t)k * ndc + j, v);
                     }
                 }
-            });
-        }
+            }
+        });
     }
     prof_mark("gather", s);
     chg_in.own.release();
@@ -371,11 +369,13 @@ void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaS
         op.flush(s);
         og.flush(s);
         oh.flush(s);
-        if (sync) FMM_CUDA(cudaStreamSynchronize(s));
     };
     unsort(ns, T.isrc.get(), spgh, spot, sgrad, shess, c.pot, c.grad, c.hess);
     unsort(nt, T.itarg.get(), tpgh, tpot, tgrad, thess, c.pottarg, c.gradtarg,
            c.hesstarg);
+    // (the outputs, copied to host arrays where the caller's are, are
+    // complete when the call returns)
+    if (sync) FMM_CUDA(cudaStreamSynchronize(s));
     prof_mark("scatter_d2h", s);
     if (c.timeinfo)
         for (int k = 0; k < 8; k++) c.timeinfo[k] = 0.0;
