@@ -288,6 +288,8 @@ def main():
                     help="keep the library's default leaf capacity and M2L form")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the other configurations (c1, c3, c4)")
+    ap.add_argument("--configs", default="c1,c3,c4",
+                    help="which of the other configurations to run (comma list)")
     ap.add_argument("--serve-requests", type=int, default=2000)
     ap.add_argument("--serve-slots", type=int, default=6)
     ap.add_argument("--serve-budget-gb", type=float, default=120.0)
@@ -704,123 +706,127 @@ def measure_configs(fm, L, args):
 
     out = {}
     L.fmm2d_b200_set_precision(0)
-    # ---- c1 ----
-    rng = np.random.default_rng(101)
-    ns = 100_000
-    src = rng.random((ns, 2))
-    q = rng.standard_normal(ns) + 1j * rng.standard_normal(ns)
-    d_src, d_q = T(src), T(q.view(np.float64))
-    d_pot = torch.zeros(2 * ns, dtype=torch.float64, device=dev)
-    d_grad = torch.zeros(4 * ns, dtype=torch.float64, device=dev)
-    eps = ctypes.c_double(1e-6)
-    cns = ctypes.c_int(ns)
+    want = set(c for c in args.configs.split(",") if c)
+    if "c1" in want:
+        # ---- c1 ----
+        rng = np.random.default_rng(101)
+        ns = 100_000
+        src = rng.random((ns, 2))
+        q = rng.standard_normal(ns) + 1j * rng.standard_normal(ns)
+        d_src, d_q = T(src), T(q.view(np.float64))
+        d_pot = torch.zeros(2 * ns, dtype=torch.float64, device=dev)
+        d_grad = torch.zeros(4 * ns, dtype=torch.float64, device=dev)
+        eps = ctypes.c_double(1e-6)
+        cns = ctypes.c_int(ns)
 
-    def c1():
-        L.lfmm2d_s_c_g_(ctypes.byref(eps), ctypes.byref(cns), ptr(d_src), ptr(d_q), ptr(d_pot),
-                        ptr(d_grad), ctypes.byref(ier))
-        check()
+        def c1():
+            L.lfmm2d_s_c_g_(ctypes.byref(eps), ctypes.byref(cns), ptr(d_src), ptr(d_q), ptr(d_pot),
+                            ptr(d_grad), ctypes.byref(ier))
+            check()
 
-    ms, prof = timed(c1)
-    m = 1000
-    sub = T(src[:m])
-    pot = torch.zeros(2 * m, dtype=torch.float64, device=dev)
-    grad = torch.zeros(4 * m, dtype=torch.float64, device=dev)
-    # (thresh^2 must stay above zero to skip each sampled source's own pair)
-    L.fmm2d_b200_l2d_direct(1, ns, ptr(d_src), 1, ptr(d_q), 0, None, None, m, ptr(sub), 2,
-                            ptr(pot), ptr(grad), None, ctypes.c_double(1e-150))
-    torch.cuda.synchronize()
-    c1r = {"workload": "lfmm2d_s_c_g uniform 1e5 eps 1e-6 (auto: mixed)", "ms": ms,
-           "phase_ms": {k: round(v, 3) for k, v in prof.items() if not k.startswith("#")},
-           "points_s": ns / (ms * 1e-3),
-           "pot_rel_l2": rel(d_pot.view(-1, 2)[:m], pot.view(-1, 2)),
-           "grad_rel_l2": rel(d_grad.view(-1, 4)[:m], grad.view(-1, 4)),
-           "accuracy_sample": f"{m} sources vs GPU FP64 direct sum"}
-    import refimpl
-    if refimpl.have_ref():
-        R = refimpl.ref()
-        hp, hg = np.zeros(ns, complex), np.zeros((ns, 2), complex)
-        t0 = time.perf_counter()
-        R.lfmm2d_s_c_g_(ctypes.byref(eps), ctypes.byref(cns), src.ctypes.data_as(P),
-                        q.ctypes.data_as(P), hp.ctypes.data_as(P), hg.ctypes.data_as(P),
-                        ctypes.byref(ier))
-        tr = time.perf_counter() - t0
-        c1r["reference_1core_ms"] = tr * 1e3
-        c1r["vs_reference_1core"] = tr * 1e3 / ms
-        c1r["pot_rel_l2_vs_reference"] = float(np.linalg.norm(
-            d_pot.view(-1, 2).cpu().numpy().view(complex).ravel() - hp) / np.linalg.norm(hp))
-        gg = d_grad.view(-1, 4).cpu().numpy().view(complex).reshape(ns, 2)
-        c1r["grad_rel_l2_vs_reference"] = float(np.linalg.norm(gg - hg) / np.linalg.norm(hg))
-        # the reference FMM's own errors at the same eps, same sampled sources
-        dp = pot.view(-1, 2).cpu().numpy().view(complex).ravel()
-        dg = grad.view(-1, 4).cpu().numpy().view(complex).reshape(m, 2)
-        c1r["reference_pot_rel_l2"] = float(np.linalg.norm(hp[:m] - dp) / np.linalg.norm(dp))
-        c1r["reference_grad_rel_l2"] = float(np.linalg.norm(hg[:m] - dg) / np.linalg.norm(dg))
-    out["c1"] = c1r
-    # ---- c3 ----
-    n3 = 4_000_000
-    x, nrm = ps.starfish(n3, 0)
-    y = ps.near_curve_targets(n3, 1)
-    ds = np.random.default_rng(3).standard_normal(n3) + 0j
-    d_src, d_trg = T(x.T), T(y.T)
-    d_ds, d_nv = T(ds.view(np.float64)), T(nrm.T)
-    d_pot = torch.zeros(2 * n3, dtype=torch.float64, device=dev)
-    d_pt = torch.zeros(2 * n3, dtype=torch.float64, device=dev)
-    eps3 = ctypes.c_double(1e-9)
-    c3n = ctypes.c_int(n3)
+        ms, prof = timed(c1)
+        m = 1000
+        sub = T(src[:m])
+        pot = torch.zeros(2 * m, dtype=torch.float64, device=dev)
+        grad = torch.zeros(4 * m, dtype=torch.float64, device=dev)
+        # (thresh^2 must stay above zero to skip each sampled source's own pair)
+        L.fmm2d_b200_l2d_direct(1, ns, ptr(d_src), 1, ptr(d_q), 0, None, None, m, ptr(sub), 2,
+                                ptr(pot), ptr(grad), None, ctypes.c_double(1e-150))
+        torch.cuda.synchronize()
+        c1r = {"workload": "lfmm2d_s_c_g uniform 1e5 eps 1e-6 (auto: mixed)", "ms": ms,
+               "phase_ms": {k: round(v, 3) for k, v in prof.items() if not k.startswith("#")},
+               "points_s": ns / (ms * 1e-3),
+               "pot_rel_l2": rel(d_pot.view(-1, 2)[:m], pot.view(-1, 2)),
+               "grad_rel_l2": rel(d_grad.view(-1, 4)[:m], grad.view(-1, 4)),
+               "accuracy_sample": f"{m} sources vs GPU FP64 direct sum"}
+        import refimpl
+        if refimpl.have_ref():
+            R = refimpl.ref()
+            hp, hg = np.zeros(ns, complex), np.zeros((ns, 2), complex)
+            t0 = time.perf_counter()
+            R.lfmm2d_s_c_g_(ctypes.byref(eps), ctypes.byref(cns), src.ctypes.data_as(P),
+                            q.ctypes.data_as(P), hp.ctypes.data_as(P), hg.ctypes.data_as(P),
+                            ctypes.byref(ier))
+            tr = time.perf_counter() - t0
+            c1r["reference_1core_ms"] = tr * 1e3
+            c1r["vs_reference_1core"] = tr * 1e3 / ms
+            c1r["pot_rel_l2_vs_reference"] = float(np.linalg.norm(
+                d_pot.view(-1, 2).cpu().numpy().view(complex).ravel() - hp) / np.linalg.norm(hp))
+            gg = d_grad.view(-1, 4).cpu().numpy().view(complex).reshape(ns, 2)
+            c1r["grad_rel_l2_vs_reference"] = float(np.linalg.norm(gg - hg) / np.linalg.norm(hg))
+            # the reference FMM's own errors at the same eps, same sampled sources
+            dp = pot.view(-1, 2).cpu().numpy().view(complex).ravel()
+            dg = grad.view(-1, 4).cpu().numpy().view(complex).reshape(m, 2)
+            c1r["reference_pot_rel_l2"] = float(np.linalg.norm(hp[:m] - dp) / np.linalg.norm(dp))
+            c1r["reference_grad_rel_l2"] = float(np.linalg.norm(hg[:m] - dg) / np.linalg.norm(dg))
+        out["c1"] = c1r
+    if "c3" in want:
+        # ---- c3 ----
+        n3 = 4_000_000
+        x, nrm = ps.starfish(n3, 0)
+        y = ps.near_curve_targets(n3, 1)
+        ds = np.random.default_rng(3).standard_normal(n3) + 0j
+        d_src, d_trg = T(x.T), T(y.T)
+        d_ds, d_nv = T(ds.view(np.float64)), T(nrm.T)
+        d_pot = torch.zeros(2 * n3, dtype=torch.float64, device=dev)
+        d_pt = torch.zeros(2 * n3, dtype=torch.float64, device=dev)
+        eps3 = ctypes.c_double(1e-9)
+        c3n = ctypes.c_int(n3)
 
-    def c3():
-        L.lfmm2d_st_d_p_(ctypes.byref(eps3), ctypes.byref(c3n), ptr(d_src), ptr(d_ds),
-                         ptr(d_nv), ptr(d_pot), ctypes.byref(c3n), ptr(d_trg), ptr(d_pt),
-                         ctypes.byref(ier))
-        check()
+        def c3():
+            L.lfmm2d_st_d_p_(ctypes.byref(eps3), ctypes.byref(c3n), ptr(d_src), ptr(d_ds),
+                             ptr(d_nv), ptr(d_pot), ctypes.byref(c3n), ptr(d_trg), ptr(d_pt),
+                             ctypes.byref(ier))
+            check()
 
-    ms, prof = timed(c3)
-    m = 10000
-    idx = np.random.default_rng(5).choice(n3, m, replace=False)
-    sub = T(y.T[idx])
-    pot = torch.zeros(2 * m, dtype=torch.float64, device=dev)
-    L.fmm2d_b200_l2d_direct(1, n3, ptr(d_src), 0, None, 1, ptr(d_ds), ptr(d_nv), m, ptr(sub), 1,
-                            ptr(pot), None, None, ctypes.c_double(1e-300))
-    torch.cuda.synchronize()
-    out["c3"] = {"workload": "lfmm2d_st_d_p starfish 4e6 + 4e6 near-curve targets eps 1e-9 (FP64)",
-                 "ms": ms, "points_s": 2 * n3 / (ms * 1e-3),
-                 "nlevels": prof.get("#nlevels"), "nboxes": prof.get("#nboxes"),
-                 "phase_ms": {k: round(v, 3) for k, v in prof.items() if not k.startswith("#")},
-                 "pottarg_rel_l2": rel(d_pt.view(-1, 2)[T(idx)], pot.view(-1, 2)),
-                 "accuracy_sample": f"{m} targets vs GPU FP64 direct sum"}
-    del d_src, d_trg, d_ds, d_nv, d_pot, d_pt
-    # ---- c4 ----
-    n4 = 2_000_000
-    rng = np.random.default_rng(404)
-    src = rng.random((n4, 2))
-    q = rng.standard_normal(n4) + 1j * rng.standard_normal(n4)
-    dd = rng.standard_normal(n4) + 1j * rng.standard_normal(n4)
-    th = rng.uniform(0, 2 * np.pi, n4)
-    v = np.stack([np.cos(th), np.sin(th)], axis=1)
-    d_src, d_q, d_d, d_v = T(src), T(q.view(np.float64)), T(dd.view(np.float64)), T(v)
-    d_pot = torch.zeros(2 * n4, dtype=torch.float64, device=dev)
-    zk = np.array([200.0, 0.0])
-    eps4 = ctypes.c_double(1e-6)
-    c4n = ctypes.c_int(n4)
+        ms, prof = timed(c3)
+        m = 10000
+        idx = np.random.default_rng(5).choice(n3, m, replace=False)
+        sub = T(y.T[idx])
+        pot = torch.zeros(2 * m, dtype=torch.float64, device=dev)
+        L.fmm2d_b200_l2d_direct(1, n3, ptr(d_src), 0, None, 1, ptr(d_ds), ptr(d_nv), m, ptr(sub), 1,
+                                ptr(pot), None, None, ctypes.c_double(1e-300))
+        torch.cuda.synchronize()
+        out["c3"] = {"workload": "lfmm2d_st_d_p starfish 4e6 + 4e6 near-curve targets eps 1e-9 (FP64)",
+                     "ms": ms, "points_s": 2 * n3 / (ms * 1e-3),
+                     "nlevels": prof.get("#nlevels"), "nboxes": prof.get("#nboxes"),
+                     "phase_ms": {k: round(v, 3) for k, v in prof.items() if not k.startswith("#")},
+                     "pottarg_rel_l2": rel(d_pt.view(-1, 2)[T(idx)], pot.view(-1, 2)),
+                     "accuracy_sample": f"{m} targets vs GPU FP64 direct sum"}
+        del d_src, d_trg, d_ds, d_nv, d_pot, d_pt
+    if "c4" in want:
+        # ---- c4 ----
+        n4 = 2_000_000
+        rng = np.random.default_rng(404)
+        src = rng.random((n4, 2))
+        q = rng.standard_normal(n4) + 1j * rng.standard_normal(n4)
+        dd = rng.standard_normal(n4) + 1j * rng.standard_normal(n4)
+        th = rng.uniform(0, 2 * np.pi, n4)
+        v = np.stack([np.cos(th), np.sin(th)], axis=1)
+        d_src, d_q, d_d, d_v = T(src), T(q.view(np.float64)), T(dd.view(np.float64)), T(v)
+        d_pot = torch.zeros(2 * n4, dtype=torch.float64, device=dev)
+        zk = np.array([200.0, 0.0])
+        eps4 = ctypes.c_double(1e-6)
+        c4n = ctypes.c_int(n4)
 
-    def c4():
-        L.hfmm2d_s_cd_p_(ctypes.byref(eps4), zk.ctypes.data_as(P), ctypes.byref(c4n), ptr(d_src),
-                         ptr(d_q), ptr(d_d), ptr(d_v), ptr(d_pot), ctypes.byref(ier))
-        check()
+        def c4():
+            L.hfmm2d_s_cd_p_(ctypes.byref(eps4), zk.ctypes.data_as(P), ctypes.byref(c4n), ptr(d_src),
+                             ptr(d_q), ptr(d_d), ptr(d_v), ptr(d_pot), ctypes.byref(ier))
+            check()
 
-    ms, prof = timed(c4)
-    m = 1000
-    sub = T(src[:m])
-    pot = torch.zeros(2 * m, dtype=torch.float64, device=dev)
-    L.fmm2d_b200_h2d_direct(1, zk.ctypes.data_as(P), n4, ptr(d_src), 1, ptr(d_q), 1, ptr(d_d),
-                            ptr(d_v), m, ptr(sub), 1, ptr(pot), None, None,
-                            ctypes.c_double(1e-150))
-    torch.cuda.synchronize()
-    out["c4"] = {"workload": "hfmm2d_s_cd_p uniform 2e6 zk 200 eps 1e-6 (FP64)", "ms": ms,
-                 "points_s": n4 / (ms * 1e-3),
-                 "phase_ms": {k: round(v, 3) for k, v in prof.items() if not k.startswith("#")},
-                 "pot_rel_l2": rel(d_pot.view(-1, 2)[:m], pot.view(-1, 2)),
-                 "accuracy_sample": f"{m} sources vs GPU FP64 direct sum"}
+        ms, prof = timed(c4)
+        m = 1000
+        sub = T(src[:m])
+        pot = torch.zeros(2 * m, dtype=torch.float64, device=dev)
+        L.fmm2d_b200_h2d_direct(1, zk.ctypes.data_as(P), n4, ptr(d_src), 1, ptr(d_q), 1, ptr(d_d),
+                                ptr(d_v), m, ptr(sub), 1, ptr(pot), None, None,
+                                ctypes.c_double(1e-150))
+        torch.cuda.synchronize()
+        out["c4"] = {"workload": "hfmm2d_s_cd_p uniform 2e6 zk 200 eps 1e-6 (FP64)", "ms": ms,
+                     "points_s": n4 / (ms * 1e-3),
+                     "phase_ms": {k: round(v, 3) for k, v in prof.items() if not k.startswith("#")},
+                     "pot_rel_l2": rel(d_pot.view(-1, 2)[:m], pot.view(-1, 2)),
+                     "accuracy_sample": f"{m} sources vs GPU FP64 direct sum"}
     return out
 
 

@@ -36,6 +36,7 @@
 #include <vector>
 
 #include "hankel.cuh"
+#include "laplace.cuh"
 
 namespace fmm2d {
 
@@ -602,6 +603,141 @@ __global__ void __launch_bounds__(256) helm_m2l_kernel(
     }
 }
 
+// M2L over list 2 at level l for tiles of kHTile target boxes with the
+// same child position (plan_slots): every slot is one offset for the whole
+// tile, so a thread per output coefficient (i, channel) reads each table
+// entry once for the tile's boxes and the source coefficients are
+// broadcasts.  A block of at most 128 threads takes as many tiles at once
+// as it has groups of 2p + 1 (times nd) threads, at most kHGroups, packed
+// without padding (a warp may span two tiles: fewer idle lanes measured
+// faster than whole warps per tile); with more coefficients than threads
+// one tile loops over them.  Missing sources read the zero block `zero`
+// ((2p + 1) nd zeros), so every slot does the same work.
+//
+// The weight rs^e, e = |i| + |j| - |i - j|, of helm_m2l_kernel
+// (toeplitz_sum, kind 2) is 1 when i and j differ in sign or one is 0, and
+// rs^(2 min(|i|, |j|)) otherwise; it factors as rs^|i| rs^|j| rs^-|i - j|.
+// SC (scaled form): T holds T_q rs^-|q| and mp the multipoles times rs^|j|
+// (helm_scale_mp_kernel), so the j loop is a plain complex multiply-add and
+// rs^|i| (pw[|i|]) scales the sum; the host takes it where those powers
+// stay far inside the FP64 range.  Otherwise the weight is applied per
+// term, from the case split above.
+constexpr int kHTile = 4;  // boxes per tile (8 measured slower: registers)
+constexpr int kHGroups = 8;
+struct HTiles {
+    int tb[5];     // tiles of the level's four segments: [tb[c], tb[c + 1])
+    int start[4];  // first target of each segment
+    int count[4];  // targets of each segment
+};
+
+template <bool SC>
+__global__ void __launch_bounds__(128, 6) helm_m2l_tile_kernel(
+    HTiles lt, const int *__restrict__ boxes, const int *__restrict__ slots,
+    const int2 *__restrict__ dxy, int nd, const HLevel *__restrict__ lv, int l,
+    const double2 *__restrict__ T, const double *__restrict__ pw,
+    const double2 *__restrict__ zero, const double2 *__restrict__ mp,
+    double2 *__restrict__ loc) {
+    constexpr int R = kHTile;
+    __shared__ int s_src[kHGroups][R][27];
+    __shared__ int s_trg[kHGroups][R];
+    __shared__ int s_cp[kHGroups];
+    const HLevel L = lv[l];
+    const int p = L.p, w = 2 * p + 1, tw = 4 * p + 1, wn = w * nd;
+    const int G = wn <= (int)blockDim.x ? min(kHGroups, (int)blockDim.x / wn) : 1;
+    const int ntiles = lt.tb[4] - lt.tb[0];
+    for (int base = blockIdx.x * G; base < ntiles; base += gridDim.x * G) {
+        __syncthreads();  // the previous pass's reads of the shared tables are done
+        for (int e = threadIdx.x; e < G * R * 27; e += blockDim.x) {
+            const int g = e / (R * 27), r = (e / 27) % R, k = e % 27;
+            const int tile = base + g;
+            int v = -1, tb = -1, cp = 0;
+            if (tile < ntiles) {
+                const int t = lt.tb[0] + tile;
+                while (cp < 3 && t >= lt.tb[cp + 1]) cp++;
+                const int q = lt.start[cp] + (t - lt.tb[cp]) * R + r;
+                if (q < lt.start[cp] + lt.count[cp]) {
+                    v = slots[(size_t)q * 27 + k];
+                    tb = boxes[q];
+                }
+            }
+            s_src[g][r][k] = v;
+            if (k == 0) s_trg[g][r] = tb;
+            if (k == 0 && r == 0) s_cp[g] = cp;
+        }
+        __syncthreads();
+        for (int u = threadIdx.x; u < G * wn; u += blockDim.x) {
+            const int g = u / wn, o = u - g * wn;
+            if (s_trg[g][0] < 0) continue;  // past the last tile
+            const int i = o / nd - p, c = o - (o / nd) * nd;
+            const int ai = abs(i), cp = s_cp[g];
+            const double ci = pw[2 * ai], w0 = pw[0];
+            double2 acc[R];
+#pragma unroll
+            for (int r = 0; r < R; r++) acc[r] = make_double2(0.0, 0.0);
+            for (int k = 0; k < 27; k++) {
+                const double2 *in[R];
+                bool any = false;
+#pragma unroll
+                for (int r = 0; r < R; r++) {
+                    const int sb = s_src[g][r][k];
+                    // coefficient j = -p of this channel
+                    in[r] = (sb >= 0 ? coef0(mp, L, sb, nd) : zero + (size_t)p * nd) + c -
+                            (size_t)p * nd;
+                    any |= sb >= 0;
+                }
+                if (!any) continue;
+                const int2 d = dxy[cp * 27 + k];
+                // T[i - j] from j = -p down
+                const double2 *tp = T + (size_t)((3 - d.y) * 7 + (3 - d.x)) * tw + 2 * p + i + p;
+                for (int j = -p; j <= p; j++, tp--) {
+                    double2 tt = *tp;
+                    if (!SC) {
+                        const int aj = abs(j);
+                        const bool same = (i > 0 && j > 0) || (i < 0 && j < 0);
+                        const double wt = same ? (aj <= ai ? pw[2 * aj] : ci) : w0;
+                        tt = make_double2(tt.x * wt, tt.y * wt);
+                    }
+#pragma unroll
+                    for (int r = 0; r < R; r++) {
+                        const double2 m = *in[r];
+                        in[r] += nd;
+                        acc[r].x = fma(m.x, tt.x, acc[r].x);
+                        acc[r].x = fma(-m.y, tt.y, acc[r].x);
+                        acc[r].y = fma(m.x, tt.y, acc[r].y);
+                        acc[r].y = fma(m.y, tt.x, acc[r].y);
+                    }
+                }
+            }
+            const double sc = SC ? pw[ai] : 1.0;
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                if (s_trg[g][r] < 0) continue;
+                double2 *op = coef0(loc, L, s_trg[g][r], nd) + (long long)i * nd + c;
+                *op = cadd(*op, SC ? cscal(acc[r], sc) : acc[r]);
+            }
+        }
+    }
+}
+
+// Scaled multipoles of the level-l boxes for the scaled M2L form:
+// out = mp * rs^|j| for coefficient j (pw[|j|]).
+__global__ void __launch_bounds__(256) helm_scale_mp_kernel(
+    long long off, long long n, int p, int nd, const double *__restrict__ pw,
+    const double2 *__restrict__ mp, double2 *__restrict__ out) {
+    const int wn = (2 * p + 1) * nd;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(t % wn) / nd - p;
+        out[off + t] = cscal(mp[off + t], pw[abs(j)]);
+    }
+}
+
+// The tile form of the Helmholtz M2L unless FMM2D_B200_HELM_M2L=box.
+bool helm_m2l_tiled() {
+    const char *e = getenv("FMM2D_B200_HELM_M2L");
+    return !(e && !strcmp(e, "box"));
+}
+
 // ---------------------------------------------------------------------------
 // M2P + L2P for one point set: thread per point.
 // ---------------------------------------------------------------------------
@@ -1074,6 +1210,8 @@ void helmholtz_fmm(const Tree &T, const HelmProblem &P, cudaStream_t s) {
     // M2L [49][4p+1] + pw
     struct LevTab {
         size_t m2m = 0, m2m_s = 0, m2m_pw = 0, l2l = 0, l2l_s = 0, l2l_pw = 0, m2l = 0, m2l_pw = 0;
+        size_t m2l_sc = 0;   // M2L table of the scaled form, T_q rs^-|q|
+        bool sc_ok = false;  // the scaled form applies on this level
     };
     std::vector<LevTab> lt(nl + 1);
     std::vector<double2> ct;  // complex tables
@@ -1141,6 +1279,28 @@ void helmholtz_fmm(const Tree &T, const HelmProblem &P, cudaStream_t s) {
                                 ct.data() + lt[l].m2l + (size_t)((iy + 3) * 7 + (ix + 3)) * (2 * N + 1));
                 }
             lt[l].m2l_pw = powtab(L.rs, 2 * p);
+            // the scaled form where rs^(2p) and the scaled entries stay
+            // inside 1e-250 .. 1e250
+            if (L.rs > 0.0 && 2.0 * p * std::fabs(std::log10(L.rs)) < 250.0) {
+                const size_t n = (size_t)49 * (2 * N + 1), o = ct.size();
+                ct.resize(o + n);
+                bool fine = true;
+                std::vector<double> f(N + 1);  // rs^-q
+                f[0] = 1.0;
+                for (int q = 1; q <= N; q++) f[q] = f[q - 1] / L.rs;
+                for (size_t e = 0; e < n; e++) {
+                    const int q = (int)(e % (2 * N + 1)) - N;
+                    const double2 v = cscal(ct[lt[l].m2l + e], f[std::abs(q)]);
+                    if (!(std::fabs(v.x) <= 1e250 && std::fabs(v.y) <= 1e250)) fine = false;
+                    ct[o + e] = v;
+                }
+                if (fine) {
+                    lt[l].m2l_sc = o;
+                    lt[l].sc_ok = true;
+                } else {
+                    ct.resize(o);
+                }
+            }
         }
     }
     DevBuf<double2> d_ct(std::max<size_t>(ct.size(), 1), s);
@@ -1178,8 +1338,48 @@ void helmholtz_fmm(const Tree &T, const HelmProblem &P, cudaStream_t s) {
     prof_mark("h_m2m", s);
     // ---- M2L ----
     const int sp = P.sset.pgh > 0 ? 1 : 0, tp = P.tset.pgh > 0 ? 1 : 0;
+    SlotPlan spl;
+    const bool tiled = helm_m2l_tiled() && plan_slots(T, sp, tp, kHTile, s, spl);
+    int pmax = 0;
+    for (int l = 2; l <= nl; l++) pmax = std::max(pmax, hl[l].p);
+    DevBuf<double2> zero(tiled ? (size_t)(2 * pmax + 1) * nd : 0, s), mps;
+    if (tiled) zero.zero(s);
     for (int l = 2; l <= nl; l++) {
         if (!hl[l].flag) continue;
+        if (tiled) {
+            if (spl.ntiles == 0) continue;
+            HTiles ht;
+            const int g0 = 4 * (l - 2);
+            for (int c = 0; c <= 4; c++) ht.tb[c] = spl.tile_base[g0 + c];
+            for (int c = 0; c < 4; c++) {
+                ht.start[c] = spl.start[g0 + c];
+                ht.count[c] = spl.count[g0 + c];
+            }
+            const int ntl = ht.tb[4] - ht.tb[0];
+            if (ntl == 0) continue;
+            // 128 threads at most: groups of wn threads, one tile each
+            const int wn = (2 * hl[l].p + 1) * nd;
+            const int G = wn <= 128 ? std::min(kHGroups, 128 / wn) : 1;
+            const int threads = std::min(128, (G * wn + 31) / 32 * 32);
+            const int grid = std::min((ntl + G - 1) / G, kNumSM * 64);
+            const double *pw = d_rt.get() + lt[l].m2l_pw;
+            if (lt[l].sc_ok) {
+                if (!mps.get()) mps.alloc(std::max<long long>(off, 1), s);
+                const long long n = (long long)(T.lend[l] - T.lstart[l]) * wn;
+                helm_scale_mp_kernel<<<grid_for(n, 256), 256, 0, s>>>(hl[l].off, n, hl[l].p, nd,
+                                                                      pw, mp.get(), mps.get());
+                FMM_CHECK_LAUNCH();
+                helm_m2l_tile_kernel<true><<<grid, threads, 0, s>>>(
+                    ht, spl.boxes, spl.slots, spl.dxy, nd, d_lv.get(), l,
+                    d_ct.get() + lt[l].m2l_sc, pw, zero.get(), mps.get(), loc.get());
+            } else {
+                helm_m2l_tile_kernel<false><<<grid, threads, 0, s>>>(
+                    ht, spl.boxes, spl.slots, spl.dxy, nd, d_lv.get(), l, d_ct.get() + lt[l].m2l,
+                    pw, zero.get(), mp.get(), loc.get());
+            }
+            FMM_CHECK_LAUNCH();
+            continue;
+        }
         const int lo = T.lstart[l], hi = T.lend[l];
         const int64_t work = (int64_t)(hi - lo) * (2 * hl[l].p + 1) * nd;
         helm_m2l_kernel<<<grid_for(work, 256), 256, 0, s>>>(

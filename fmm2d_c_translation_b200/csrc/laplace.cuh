@@ -135,6 +135,24 @@ void set_m2l_form(int p, int form);
 uint64_t m2l_window_fp32(const Tree &T, const CauchyProblem &P, const float2 *mp32, double2 *loc,
                          int *err, cudaStream_t s);
 
+// Target boxes of levels >= 2 (those with points of an evaluated set)
+// grouped into segments by (level, child position) and cut into tiles of
+// `tile` boxes, with the source box of each of the 27 list-2 slots of every
+// target (m2l.cu).  Within a segment a slot is one translation offset, so a
+// tile shares each slot's translation operator.  Segment (l - 2) * 4 + c
+// holds the level-l boxes that are child c of their parent.  Source boxes
+// without sources are left out of the slots; false when a list-2 entry
+// falls outside them.
+struct SlotPlan {
+    std::shared_ptr<void> hold;  // owns the device arrays below
+    const int *boxes = nullptr;  // [ntarg] target boxes, segment after segment
+    const int *slots = nullptr;  // [ntarg][27] source box per slot, -1 when none
+    const int2 *dxy = nullptr;   // [4][27] slot offset (source - target, box units)
+    std::vector<int> tile_base, start, count;  // per segment (host)
+    int nseg = 0, ntarg = 0, ntiles = 0;
+};
+bool plan_slots(const Tree &T, int spgh, int tpgh, int tile, cudaStream_t s, SlotPlan &sp);
+
 // Binomial table C(l, m), l, m <= kLdc, built with the reference's Pascal
 // recurrence (init_carray, src/common/fmmcommon2d.f).
 constexpr int kLdc = 127;

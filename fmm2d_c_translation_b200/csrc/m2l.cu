@@ -252,6 +252,7 @@ void launch_dmma(const SegTable &sg, const int *boxes, const int *slots,
 struct M2LWork {
     DevBuf<uint32_t> keys, vals, kt, vt;
     DevBuf<int> segd, slots;
+    std::vector<int> hseg;  // host copy of segd
     int nseg = 0, ntarg = 0, ntiles = 0;
     SegTable seg() const {
         const int *h = segd.get();
@@ -345,6 +346,7 @@ bool m2l_work(const Tree &T, const CauchyProblem &P, int tile, cudaStream_t s, M
     tb[nseg] = run;
     w.ntiles = run;
     w.ntarg = start;
+    w.hseg = h;
     if (w.ntiles == 0) return true;
     if (nseg + 1 > 257) return false;
     w.segd.alloc(h.size(), s);
@@ -946,6 +948,45 @@ bool m2l_tensor_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp,
     FMM_M2L_CASE(8, 16)
 #undef FMM_M2L_CASE
     return false;
+}
+
+namespace {
+struct SlotHold {
+    M2LWork w;
+    DevBuf<int2> dxy;
+};
+}  // namespace
+
+bool plan_slots(const Tree &T, int spgh, int tpgh, int tile, cudaStream_t s, SlotPlan &sp) {
+    sp = SlotPlan();
+    if (T.nlevels < 2) return true;
+    CauchyProblem P;
+    P.sset.pgh = spgh;
+    P.tset.pgh = tpgh;
+    auto h = std::make_shared<SlotHold>();
+    if (!m2l_work(T, P, tile, s, h->w)) return false;
+    const M2LWork &w = h->w;
+    sp.nseg = w.nseg;
+    sp.ntarg = w.ntarg;
+    sp.ntiles = w.ntiles;
+    if (w.ntiles == 0) return true;
+    const int n = w.nseg;
+    sp.tile_base.assign(w.hseg.begin(), w.hseg.begin() + n + 1);
+    sp.start.assign(w.hseg.begin() + n + 1, w.hseg.begin() + 2 * n + 1);
+    sp.count.assign(w.hseg.begin() + 2 * n + 1, w.hseg.begin() + 3 * n + 1);
+    const SlotTables st = make_slot_tables();
+    std::vector<int2> d(4 * kSlots);
+    for (int c = 0; c < 4; c++)
+        for (int k = 0; k < kSlots; k++) d[c * kSlots + k] = make_int2(st.dx[c][k], st.dy[c][k]);
+    h->dxy.alloc(d.size(), s);
+    FMM_CUDA(cudaMemcpyAsync(h->dxy.get(), d.data(), d.size() * sizeof(int2),
+                             cudaMemcpyHostToDevice, s));
+    FMM_CUDA(cudaStreamSynchronize(s));  // (d is a pageable host vector)
+    sp.boxes = (const int *)w.vals.get();
+    sp.slots = w.slots.get();
+    sp.dxy = h->dxy.get();
+    sp.hold = h;
+    return true;
 }
 
 namespace {

@@ -9,7 +9,8 @@
   levels to the diagonal (FFT) translations and this library keeps the
   coefficient-space Graf translations (the same truncated operators);
 * the guru driver with nd = 2, the ndiv driver, the bind(c) entry, and the
-  GPU direct sum against the reference's h2d_direct kernels.
+  GPU direct sum against the reference's h2d_direct kernels;
+* the tiled M2L (both of its forms) against the per-box M2L kernel.
 """
 import ctypes
 
@@ -127,6 +128,24 @@ def test_hfmm2d_eps_and_zk(glib, eps, zk):
     pot, grad, _ = h_direct(glib, zk, src, q, d, v, trg[:, :50], 2, 1, 1)
     assert W.rel_err(out["pottarg"][:50], pot) < 10 * eps
     assert W.rel_err(out["gradtarg"][:50], grad) < 100 * eps
+
+
+@pytest.mark.parametrize("zk,eps", [(200.0 + 0j, 1e-6), (30.0 + 0j, 1e-9), (2.0 + 3.0j, 1e-6),
+                                    (1e-3 + 0j, 1e-12)],
+                         ids=["zk200", "zk30", "zk2+3i", "zk1e-3-weighted"])
+def test_m2l_tile_form_matches_box_form(glib, monkeypatch, zk, eps):
+    """The M2L over tiles of boxes that share their child position (the
+    default; scaled Toeplitz sums, or per-term weights where the scaling
+    would leave the FP64 range, as for zk = 1e-3 at eps 1e-12) against the
+    per-box kernel that follows h2dmploc term by term."""
+    src, trg, q, d, v = inputs(ns=20000, nt=3000, seed=5)
+    out, ier = W.call(glib, "h", "st_cd_g", eps, src, q, d, v, trg, zk=zk)
+    assert ier == 0
+    monkeypatch.setenv("FMM2D_B200_HELM_M2L", "box")
+    ob, ierb = W.call(glib, "h", "st_cd_g", eps, src, q, d, v, trg, zk=zk)
+    assert ierb == 0
+    for k in out:
+        assert W.rel_err(out[k], ob[k]) < 1e-11, (k, W.rel_err(out[k], ob[k]))
 
 
 def _guru(lib, fn_name, nd, zk, src, q, d, v, trg, ndiv=None):
