@@ -605,10 +605,12 @@ __global__ void __launch_bounds__(256) helm_m2l_kernel(
 
 // M2L over list 2 at level l for tiles of kHTile target boxes with the
 // same child position (plan_slots): every slot is one offset for the whole
-// tile, so a thread per output coefficient (i, channel) reads each table
-// entry once for the tile's boxes and the source coefficients are
-// broadcasts.  A block of at most 128 threads takes as many tiles at once
-// as it has groups of 2p + 1 (times nd) threads, at most kHGroups, packed
+// tile, so a thread per two consecutive output coefficients (i0, i0 + 1,
+// channel) reads each table entry once for the tile's boxes and both
+// outputs (T[i0 + 1 - j] is the previous step's T[i0 - j]), and the source
+// coefficients are broadcasts.  A block of at most 128 threads takes as
+// many tiles at once as it has groups of p + 1 (times nd) threads, at most
+// kHGroups, packed
 // without padding (a warp may span two tiles: fewer idle lanes measured
 // faster than whole warps per tile); with more coefficients than threads
 // one tile loops over them.  Missing sources read the zero block `zero`
@@ -631,7 +633,7 @@ struct HTiles {
 };
 
 template <bool SC>
-__global__ void __launch_bounds__(128, 6) helm_m2l_tile_kernel(
+__global__ void __launch_bounds__(128, 5) helm_m2l_tile_kernel(
     HTiles lt, const int *__restrict__ boxes, const int *__restrict__ slots,
     const int2 *__restrict__ dxy, int nd, const HLevel *__restrict__ lv, int l,
     const double2 *__restrict__ T, const double *__restrict__ pw,
@@ -642,7 +644,7 @@ __global__ void __launch_bounds__(128, 6) helm_m2l_tile_kernel(
     __shared__ int s_trg[kHGroups][R];
     __shared__ int s_cp[kHGroups];
     const HLevel L = lv[l];
-    const int p = L.p, w = 2 * p + 1, tw = 4 * p + 1, wn = w * nd;
+    const int p = L.p, tw = 4 * p + 1, wn = (p + 1) * nd;  // a thread per two outputs
     const int G = wn <= (int)blockDim.x ? min(kHGroups, (int)blockDim.x / wn) : 1;
     const int ntiles = lt.tb[4] - lt.tb[0];
     for (int base = blockIdx.x * G; base < ntiles; base += gridDim.x * G) {
@@ -668,12 +670,14 @@ __global__ void __launch_bounds__(128, 6) helm_m2l_tile_kernel(
         for (int u = threadIdx.x; u < G * wn; u += blockDim.x) {
             const int g = u / wn, o = u - g * wn;
             if (s_trg[g][0] < 0) continue;  // past the last tile
-            const int i = o / nd - p, c = o - (o / nd) * nd;
-            const int ai = abs(i), cp = s_cp[g];
-            const double ci = pw[2 * ai], w0 = pw[0];
-            double2 acc[R];
+            // outputs i0 and i0 + 1 (the second absent for i0 = p)
+            const int i0 = 2 * (o / nd) - p, c = o - (o / nd) * nd;
+            const bool two = i0 < p;
+            const int i1 = i0 + 1, ai0 = abs(i0), ai1 = abs(i1), cp = s_cp[g];
+            const double c0 = pw[2 * ai0], c1 = pw[2 * min(ai1, p)], w0 = pw[0];
+            double2 acc0[R], acc1[R];
 #pragma unroll
-            for (int r = 0; r < R; r++) acc[r] = make_double2(0.0, 0.0);
+            for (int r = 0; r < R; r++) acc0[r] = acc1[r] = make_double2(0.0, 0.0);
             for (int k = 0; k < 27; k++) {
                 const double2 *in[R];
                 bool any = false;
@@ -687,33 +691,45 @@ __global__ void __launch_bounds__(128, 6) helm_m2l_tile_kernel(
                 }
                 if (!any) continue;
                 const int2 d = dxy[cp * 27 + k];
-                // T[i - j] from j = -p down
-                const double2 *tp = T + (size_t)((3 - d.y) * 7 + (3 - d.x)) * tw + 2 * p + i + p;
+                // T[i0 - j] from j = -p down; T[i1 - j] is the previous step's T[i0 - j]
+                const double2 *tp = T + (size_t)((3 - d.y) * 7 + (3 - d.x)) * tw + 2 * p + i0 + p;
+                double2 tb = two ? tp[1] : make_double2(0.0, 0.0);
                 for (int j = -p; j <= p; j++, tp--) {
-                    double2 tt = *tp;
+                    const double2 ta = *tp;
+                    double2 t0 = ta, t1 = tb;
+                    tb = ta;
                     if (!SC) {
                         const int aj = abs(j);
-                        const bool same = (i > 0 && j > 0) || (i < 0 && j < 0);
-                        const double wt = same ? (aj <= ai ? pw[2 * aj] : ci) : w0;
-                        tt = make_double2(tt.x * wt, tt.y * wt);
+                        const bool s0 = (i0 > 0 && j > 0) || (i0 < 0 && j < 0);
+                        const bool s1 = (i1 > 0 && j > 0) || (i1 < 0 && j < 0);
+                        const double pj = pw[2 * min(aj, p)];
+                        const double w0j = s0 ? (aj <= ai0 ? pj : c0) : w0;
+                        const double w1j = s1 ? (aj <= ai1 ? pj : c1) : w0;
+                        t0 = make_double2(t0.x * w0j, t0.y * w0j);
+                        t1 = make_double2(t1.x * w1j, t1.y * w1j);
                     }
 #pragma unroll
                     for (int r = 0; r < R; r++) {
                         const double2 m = *in[r];
                         in[r] += nd;
-                        acc[r].x = fma(m.x, tt.x, acc[r].x);
-                        acc[r].x = fma(-m.y, tt.y, acc[r].x);
-                        acc[r].y = fma(m.x, tt.y, acc[r].y);
-                        acc[r].y = fma(m.y, tt.x, acc[r].y);
+                        acc0[r].x = fma(m.x, t0.x, acc0[r].x);
+                        acc0[r].x = fma(-m.y, t0.y, acc0[r].x);
+                        acc0[r].y = fma(m.x, t0.y, acc0[r].y);
+                        acc0[r].y = fma(m.y, t0.x, acc0[r].y);
+                        acc1[r].x = fma(m.x, t1.x, acc1[r].x);
+                        acc1[r].x = fma(-m.y, t1.y, acc1[r].x);
+                        acc1[r].y = fma(m.x, t1.y, acc1[r].y);
+                        acc1[r].y = fma(m.y, t1.x, acc1[r].y);
                     }
                 }
             }
-            const double sc = SC ? pw[ai] : 1.0;
+            const double sc0 = SC ? pw[ai0] : 1.0, sc1 = SC ? pw[min(ai1, p)] : 1.0;
 #pragma unroll
             for (int r = 0; r < R; r++) {
                 if (s_trg[g][r] < 0) continue;
-                double2 *op = coef0(loc, L, s_trg[g][r], nd) + (long long)i * nd + c;
-                *op = cadd(*op, SC ? cscal(acc[r], sc) : acc[r]);
+                double2 *op = coef0(loc, L, s_trg[g][r], nd) + (long long)i0 * nd + c;
+                *op = cadd(*op, SC ? cscal(acc0[r], sc0) : acc0[r]);
+                if (two) op[nd] = cadd(op[nd], SC ? cscal(acc1[r], sc1) : acc1[r]);
             }
         }
     }
@@ -1357,15 +1373,16 @@ void helmholtz_fmm(const Tree &T, const HelmProblem &P, cudaStream_t s) {
             }
             const int ntl = ht.tb[4] - ht.tb[0];
             if (ntl == 0) continue;
-            // 128 threads at most: groups of wn threads, one tile each
-            const int wn = (2 * hl[l].p + 1) * nd;
+            // 128 threads at most: groups of wn threads (two outputs
+            // each), one tile per group
+            const int wn = (hl[l].p + 1) * nd;
             const int G = wn <= 128 ? std::min(kHGroups, 128 / wn) : 1;
             const int threads = std::min(128, (G * wn + 31) / 32 * 32);
             const int grid = std::min((ntl + G - 1) / G, kNumSM * 64);
             const double *pw = d_rt.get() + lt[l].m2l_pw;
             if (lt[l].sc_ok) {
                 if (!mps.get()) mps.alloc(std::max<long long>(off, 1), s);
-                const long long n = (long long)(T.lend[l] - T.lstart[l]) * wn;
+                const long long n = (long long)(T.lend[l] - T.lstart[l]) * (2 * hl[l].p + 1) * nd;
                 helm_scale_mp_kernel<<<grid_for(n, 256), 256, 0, s>>>(hl[l].off, n, hl[l].p, nd,
                                                                       pw, mp.get(), mps.get());
                 FMM_CHECK_LAUNCH();
