@@ -632,21 +632,26 @@ struct HTiles {
     int count[4];  // targets of each segment
 };
 
-template <bool SC>
+template <bool SC, bool SPLIT>
 __global__ void __launch_bounds__(128, 5) helm_m2l_tile_kernel(
     HTiles lt, const int *__restrict__ boxes, const int *__restrict__ slots,
     const int2 *__restrict__ dxy, int nd, const HLevel *__restrict__ lv, int l,
     const double2 *__restrict__ T, const double *__restrict__ pw,
     const double2 *__restrict__ zero, const double2 *__restrict__ mp,
-    double2 *__restrict__ loc) {
+    double2 *__restrict__ loc, double2 *__restrict__ part) {
     constexpr int R = kHTile;
     __shared__ int s_src[kHGroups][R][27];
     __shared__ int s_trg[kHGroups][R];
+    __shared__ int s_q[kHGroups][R];
     __shared__ int s_cp[kHGroups];
     const HLevel L = lv[l];
     const int p = L.p, tw = 4 * p + 1, wn = (p + 1) * nd;  // a thread per two outputs
     const int G = wn <= (int)blockDim.x ? min(kHGroups, (int)blockDim.x / wn) : 1;
     const int ntiles = lt.tb[4] - lt.tb[0];
+    // slots [k0, k1) of slice blockIdx.y; with several slices each writes
+    // its own partial sums (part: [slice][level target][(2p + 1) nd])
+    const int k0 = SPLIT ? blockIdx.y * 27 / gridDim.y : 0;
+    const int k1 = SPLIT ? (blockIdx.y + 1) * 27 / gridDim.y : 27;
     for (int base = blockIdx.x * G; base < ntiles; base += gridDim.x * G) {
         __syncthreads();  // the previous pass's reads of the shared tables are done
         for (int e = threadIdx.x; e < G * R * 27; e += blockDim.x) {
@@ -660,6 +665,7 @@ __global__ void __launch_bounds__(128, 5) helm_m2l_tile_kernel(
                 if (q < lt.start[cp] + lt.count[cp]) {
                     v = slots[(size_t)q * 27 + k];
                     tb = boxes[q];
+                    if (k == 0) s_q[g][r] = q - lt.start[0];
                 }
             }
             s_src[g][r][k] = v;
@@ -678,7 +684,7 @@ __global__ void __launch_bounds__(128, 5) helm_m2l_tile_kernel(
             double2 acc0[R], acc1[R];
 #pragma unroll
             for (int r = 0; r < R; r++) acc0[r] = acc1[r] = make_double2(0.0, 0.0);
-            for (int k = 0; k < 27; k++) {
+            for (int k = k0; k < k1; k++) {
                 const double2 *in[R];
                 bool any = false;
 #pragma unroll
@@ -727,11 +733,38 @@ __global__ void __launch_bounds__(128, 5) helm_m2l_tile_kernel(
 #pragma unroll
             for (int r = 0; r < R; r++) {
                 if (s_trg[g][r] < 0) continue;
-                double2 *op = coef0(loc, L, s_trg[g][r], nd) + (long long)i0 * nd + c;
-                *op = cadd(*op, SC ? cscal(acc0[r], sc0) : acc0[r]);
-                if (two) op[nd] = cadd(op[nd], SC ? cscal(acc1[r], sc1) : acc1[r]);
+                const double2 v0 = SC ? cscal(acc0[r], sc0) : acc0[r];
+                const double2 v1 = SC ? cscal(acc1[r], sc1) : acc1[r];
+                if (SPLIT) {  // this slice's partial sums, added in order by helm_m2l_sum_kernel
+                    const int nq = lt.start[3] + lt.count[3] - lt.start[0];
+                    double2 *op = part + ((size_t)blockIdx.y * nq + s_q[g][r]) * (2 * p + 1) * nd +
+                                  (size_t)(i0 + p) * nd + c;
+                    op[0] = v0;
+                    if (two) op[nd] = v1;
+                } else {
+                    double2 *op = coef0(loc, L, s_trg[g][r], nd) + (long long)i0 * nd + c;
+                    *op = cadd(*op, v0);
+                    if (two) op[nd] = cadd(op[nd], v1);
+                }
             }
         }
+    }
+}
+
+// Sum of the slices' partial M2L sums of helm_m2l_tile_kernel, in slice
+// order, into the local expansions of the level's targets.
+__global__ void __launch_bounds__(256) helm_m2l_sum_kernel(
+    int nq, int wf, int nslice, const double2 *__restrict__ part, const int *__restrict__ boxes,
+    int q_lo, const HLevel *__restrict__ lv, int l, int nd, double2 *__restrict__ loc) {
+    const HLevel L = lv[l];
+    const long long n = (long long)nq * wf;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int q = (int)(t / wf), o = (int)(t - (long long)q * wf);
+        double2 acc = make_double2(0.0, 0.0);
+        for (int y = 0; y < nslice; y++) acc = cadd(acc, part[(size_t)y * n + t]);
+        double2 *op = coef0(loc, L, boxes[q_lo + q], nd) - (long long)L.p * nd + o;
+        *op = cadd(*op, acc);
     }
 }
 
@@ -1378,7 +1411,14 @@ void helmholtz_fmm(const Tree &T, const HelmProblem &P, cudaStream_t s) {
             const int wn = (hl[l].p + 1) * nd;
             const int G = wn <= 128 ? std::min(kHGroups, 128 / wn) : 1;
             const int threads = std::min(128, (G * wn + 31) / 32 * 32);
-            const int grid = std::min((ntl + G - 1) / G, kNumSM * 64);
+            const int nblk = (ntl + G - 1) / G;
+            // levels with fewer blocks than half the SMs (few boxes, high
+            // orders) split the 27 slots over slices of blocks
+            const int nslice = nblk < kNumSM / 2 ? std::min(27, std::max(2, 2 * kNumSM / nblk)) : 1;
+            const dim3 grid(std::min(nblk, kNumSM * 64), nslice);
+            const int q_lo = ht.start[0], nq = ht.start[3] + ht.count[3] - q_lo;
+            const int wf = (2 * hl[l].p + 1) * nd;
+            DevBuf<double2> part(nslice > 1 ? (size_t)nslice * nq * wf : 0, s);
             const double *pw = d_rt.get() + lt[l].m2l_pw;
             if (lt[l].sc_ok) {
                 if (!mps.get()) mps.alloc(std::max<long long>(off, 1), s);
@@ -1386,15 +1426,23 @@ void helmholtz_fmm(const Tree &T, const HelmProblem &P, cudaStream_t s) {
                 helm_scale_mp_kernel<<<grid_for(n, 256), 256, 0, s>>>(hl[l].off, n, hl[l].p, nd,
                                                                       pw, mp.get(), mps.get());
                 FMM_CHECK_LAUNCH();
-                helm_m2l_tile_kernel<true><<<grid, threads, 0, s>>>(
-                    ht, spl.boxes, spl.slots, spl.dxy, nd, d_lv.get(), l,
-                    d_ct.get() + lt[l].m2l_sc, pw, zero.get(), mps.get(), loc.get());
+#define HM2L(SC_, SPLIT_, TAB_, MP_)                                                       \
+    helm_m2l_tile_kernel<SC_, SPLIT_><<<grid, threads, 0, s>>>(                            \
+        ht, spl.boxes, spl.slots, spl.dxy, nd, d_lv.get(), l, TAB_, pw, zero.get(), MP_, \
+        loc.get(), part.get())
+                if (nslice > 1) HM2L(true, true, d_ct.get() + lt[l].m2l_sc, mps.get());
+                else HM2L(true, false, d_ct.get() + lt[l].m2l_sc, mps.get());
             } else {
-                helm_m2l_tile_kernel<false><<<grid, threads, 0, s>>>(
-                    ht, spl.boxes, spl.slots, spl.dxy, nd, d_lv.get(), l, d_ct.get() + lt[l].m2l,
-                    pw, zero.get(), mp.get(), loc.get());
+                if (nslice > 1) HM2L(false, true, d_ct.get() + lt[l].m2l, mp.get());
+                else HM2L(false, false, d_ct.get() + lt[l].m2l, mp.get());
+#undef HM2L
             }
             FMM_CHECK_LAUNCH();
+            if (nslice > 1) {
+                helm_m2l_sum_kernel<<<grid_for((int64_t)nq * wf, 256), 256, 0, s>>>(
+                    nq, wf, nslice, part.get(), spl.boxes, q_lo, d_lv.get(), l, nd, loc.get());
+                FMM_CHECK_LAUNCH();
+            }
             continue;
         }
         const int lo = T.lstart[l], hi = T.lend[l];
