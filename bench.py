@@ -80,7 +80,11 @@ def read_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
+    """nvidia-smi clock / throttle sampling during the timed region.
+
+    The sampler is started and its first sample awaited before the timed
+    region begins; the samples kept are those from mark() on, plus the first
+    one after stop() is called (short timed regions fall between samples)."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -88,26 +92,51 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.out = None
+        self.lines = []
+        self.lock = threading.Lock()
+        self.first = threading.Event()
+        self.mark_at = 0
+
+    def _read(self):
+        for line in self.proc.stdout:
+            with self.lock:
+                self.lines.append(line)
+            self.first.set()
 
     def start(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+            return
+        threading.Thread(target=self._read, daemon=True).start()
+        self.first.wait(10.0)
+
+    def mark(self):
+        with self.lock:
+            self.mark_at = len(self.lines)
 
     def stop(self):
         if self.proc is None:
             return None
+        with self.lock:
+            n_end = len(self.lines)
+        t0 = time.time()
+        while time.time() - t0 < 2.0:
+            with self.lock:
+                if len(self.lines) > n_end:
+                    break
+            time.sleep(0.01)
         self.proc.terminate()
         try:
-            out, _ = self.proc.communicate(timeout=5)
+            self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
-            out, _ = self.proc.communicate()
+        with self.lock:
+            out = "".join(self.lines[self.mark_at:n_end + 1])
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
                  "sw_power_cap"]
@@ -397,6 +426,7 @@ def main():
         clocks.start()
         torch.cuda.synchronize()
         barrier()
+        clocks.mark()
         n0 = L.fmm2d_b200_launch_count()
         ms, prof = timed(dev_args, args.steps, profile=True)
         n1 = L.fmm2d_b200_launch_count()
