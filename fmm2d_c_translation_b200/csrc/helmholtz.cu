@@ -274,9 +274,38 @@ __device__ __forceinline__ void emit_warp(double2 *E, int n, int nd, int c, doub
     }
 }
 
+// emit_warp over a group of W lanes (W = 32 or 16, mask the group's lanes).
+template <int W>
+__device__ __forceinline__ double group_sum(double v, unsigned mask) {
+#pragma unroll
+    for (int o = W / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+    return v;
+}
+template <int W>
+__device__ __forceinline__ void emit_group(double2 *E, int n, int nd, int c, double2 cp,
+                                           double2 cm, int lane, unsigned mask) {
+    const double a = group_sum<W>(cp.x, mask), b = group_sum<W>(cp.y, mask);
+    double e = 0.0, f = 0.0;
+    if (n != 0) {
+        e = group_sum<W>(cm.x, mask);
+        f = group_sum<W>(cm.y, mask);
+    }
+    if (lane == 0) {
+        double2 &o = E[(long long)n * nd + c];
+        o = make_double2(o.x + a, o.y + b);
+        if (n != 0) {
+            double2 &u = E[-(long long)n * nd + c];
+            u = make_double2(u.x + e, u.y + f);
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
-// P2M (h2dformmpc/d/cd, helmrouts2d.c:294-393): warp per leaf at level >= 2.
+// P2M (h2dformmpc/d/cd, helmrouts2d.c:294-393): a group of W lanes (a warp,
+// or a half warp for leaves of few sources) per leaf at level >= 2; every
+// shuffle stays within the group.
 // ---------------------------------------------------------------------------
+template <int W>
 __global__ void __launch_bounds__(256) helm_p2m_kernel(
     int nb, const int *__restrict__ nchild, const int *__restrict__ level,
     const int2 *__restrict__ sse, const double2 *__restrict__ centers,
@@ -284,9 +313,10 @@ __global__ void __launch_bounds__(256) helm_p2m_kernel(
     const double2 *__restrict__ charge, const double2 *__restrict__ dipstr,
     const double2 *__restrict__ dipvec, int ifc, int ifd, int nd, double2 zk,
     double2 *__restrict__ mp) {
-    const int lane = threadIdx.x & 31;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nb; b += nw) {
+    const int lane = threadIdx.x & (W - 1);
+    const unsigned gmask = W == 32 ? 0xffffffffu : (0xffffu << (threadIdx.x & 16));
+    const int nw = (gridDim.x * blockDim.x) / W;
+    for (int b = (blockIdx.x * blockDim.x + threadIdx.x) / W; b < nb; b += nw) {
         if (nchild[b] != 0) continue;
         const int l = level[b];
         if (l < 2) continue;
@@ -298,7 +328,7 @@ __global__ void __launch_bounds__(256) helm_p2m_kernel(
         const double rs = L.rs, rs2 = rs * rs;
         double2 *M = const_cast<double2 *>(coef0(mp, L, b, nd));
         const double2 ctr = centers[b];
-        for (int k0 = r.x; k0 < r.y; k0 += 32) {
+        for (int k0 = r.x; k0 < r.y; k0 += W) {
             const int k = k0 + lane;
             const bool valid = k < r.y;
             SrcGeo g{make_double2(1.0, 0.0), make_double2(1.0, 0.0)};
@@ -349,7 +379,7 @@ __global__ void __launch_bounds__(256) helm_p2m_kernel(
             // pass B: the same recurrence, emitting normalised J_i downward
             int nmax = ntop;
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
+            for (int o = W / 2; o > 0; o >>= 1) nmax = max(nmax, __shfl_xor_sync(gmask, nmax, o));
             double2 gp1 = make_double2(0.0, 0.0), gc = make_double2(0.0, 0.0);
             int ev = 0;
             double2 ja = make_double2(0.0, 0.0), jb = ja, jc = ja;  // J_i, J_{i+1}, J_{i+2}
@@ -394,7 +424,7 @@ __global__ void __launch_bounds__(256) helm_p2m_kernel(
                                     ifc ? charge[(long long)k * nd + c] : cp, ifd,
                                     ifd ? dipstr[(long long)k * nd + c] : cp,
                                     ifd ? dipvec[(long long)k * nd + c] : cp, cp, cm);
-                        emit_warp(M, n, nd, c, cp, cm, lane);
+                        emit_group<W>(M, n, nd, c, cp, cm, lane, gmask);
                     }
                     pw = cmul(pw, g.ep);
                 }
@@ -406,7 +436,7 @@ __global__ void __launch_bounds__(256) helm_p2m_kernel(
                             ifc ? charge[(long long)k * nd + c] : cp, ifd,
                             ifd ? dipstr[(long long)k * nd + c] : cp,
                             ifd ? dipvec[(long long)k * nd + c] : cp, cp, cm);
-                emit_warp(M, 0, nd, c, cp, cm, lane);
+                emit_group<W>(M, 0, nd, c, cp, cm, lane, gmask);
             }
         }
     }
@@ -1364,9 +1394,16 @@ void helmholtz_fmm(const Tree &T, const HelmProblem &P, cudaStream_t s) {
     const int nb = T.nboxes;
     const int ifc = P.ifcharge, ifd = P.ifdipole;
     // ---- P2M, P2L ----
-    helm_p2m_kernel<<<grid_for((int64_t)nb * 32, 256), 256, 0, s>>>(
-        nb, T.nchild.get(), T.level.get(), T.srcse.get(), T.centers.get(), d_lv.get(), P.src,
-        P.charge, P.dipstr, P.dipvec, ifc, ifd, nd, zk, mp.get());
+    // half warps per leaf when the leaves hold about 12 sources or fewer
+    // (leaves are about three quarters of the boxes)
+    if ((double)P.sset.n <= 9.0 * nb)
+        helm_p2m_kernel<16><<<grid_for((int64_t)nb * 16, 256), 256, 0, s>>>(
+            nb, T.nchild.get(), T.level.get(), T.srcse.get(), T.centers.get(), d_lv.get(), P.src,
+            P.charge, P.dipstr, P.dipvec, ifc, ifd, nd, zk, mp.get());
+    else
+        helm_p2m_kernel<32><<<grid_for((int64_t)nb * 32, 256), 256, 0, s>>>(
+            nb, T.nchild.get(), T.level.get(), T.srcse.get(), T.centers.get(), d_lv.get(), P.src,
+            P.charge, P.dipstr, P.dipvec, ifc, ifd, nd, zk, mp.get());
     FMM_CHECK_LAUNCH();
     helm_p2l_kernel<<<grid_for((int64_t)nb * 32, 256), 256, 0, s>>>(
         nb, T.level.get(), T.nlist4.get(), T.list4.get(), T.srcse.get(), T.centers.get(),
