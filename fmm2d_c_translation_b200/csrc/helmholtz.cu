@@ -1449,9 +1449,9 @@ void helmholtz_fmm(const Tree &T, const HelmProblem &P, cudaStream_t s) {
             const int G = wn <= 128 ? std::min(kHGroups, 128 / wn) : 1;
             const int threads = std::min(128, (G * wn + 31) / 32 * 32);
             const int nblk = (ntl + G - 1) / G;
-            // levels with fewer blocks than half the SMs (few boxes, high
+            // levels with fewer blocks than SMs (few boxes, high
             // orders) split the 27 slots over slices of blocks
-            const int nslice = nblk < kNumSM / 2 ? std::min(27, std::max(2, 2 * kNumSM / nblk)) : 1;
+            const int nslice = nblk < kNumSM ? std::min(27, std::max(2, 2 * kNumSM / nblk)) : 1;
             const dim3 grid(std::min(nblk, kNumSM * 64), nslice);
             const int q_lo = ht.start[0], nq = ht.start[3] + ht.count[3] - q_lo;
             const int wf = (2 * hl[l].p + 1) * nd;
