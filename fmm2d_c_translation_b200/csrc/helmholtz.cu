@@ -1254,6 +1254,45 @@ void shift_table(double2 zk, double dx, double dy, int N, double rs1, bool hanke
 
 }  // namespace
 
+namespace {
+
+// Host translation tables of one evaluation.  Layout per level: M2M
+// [4][2N+1] + S + pw, L2L likewise, M2L [49][4p+1] + pw (+ the scaled M2L
+// table where it applies).
+struct LevTab {
+    size_t m2m = 0, m2m_s = 0, m2m_pw = 0, l2l = 0, l2l_s = 0, l2l_pw = 0, m2l = 0, m2l_pw = 0;
+    size_t m2l_sc = 0;   // M2L table of the scaled form, T_q rs^-|q|
+    bool sc_ok = false;  // the scaled form applies on this level
+};
+struct HTables {
+    std::vector<LevTab> lt;
+    std::vector<double2> ct;  // complex tables
+    std::vector<double> rt;   // real tables
+};
+using HTabKey = std::tuple<double, double, double, double, int>;  // zk, eps, root box, depth
+
+// The last kHTabCache table sets, shared by the threads of the process.
+constexpr size_t kHTabCache = 16;
+std::mutex g_htab_mu;
+std::vector<std::pair<HTabKey, std::shared_ptr<HTables>>> g_htab;
+
+std::shared_ptr<HTables> htables_find(const HTabKey &k) {
+    std::lock_guard<std::mutex> lock(g_htab_mu);
+    for (auto &e : g_htab)
+        if (e.first == k) return e.second;
+    return nullptr;
+}
+
+void htables_store(const HTabKey &k, const std::shared_ptr<HTables> &t) {
+    std::lock_guard<std::mutex> lock(g_htab_mu);
+    for (auto &e : g_htab)
+        if (e.first == k) return;
+    if (g_htab.size() >= kHTabCache) g_htab.erase(g_htab.begin());
+    g_htab.emplace_back(k, t);
+}
+
+}  // namespace
+
 void helmholtz_fmm(const Tree &T, const HelmProblem &P, cudaStream_t s) {
     const int nl = T.nlevels, nd = P.nd;
     const double2 zk = P.zk;
@@ -1284,104 +1323,108 @@ void helmholtz_fmm(const Tree &T, const HelmProblem &P, cudaStream_t s) {
     DevBuf<double2> mp(std::max<long long>(off, 1), s), loc(std::max<long long>(off, 1), s);
     mp.zero(s);
     loc.zero(s);
-    // ---- translation tables ----
-    // host layout: for each level, M2M [4][2N+1] + S + pw, L2L likewise,
-    // M2L [49][4p+1] + pw
-    struct LevTab {
-        size_t m2m = 0, m2m_s = 0, m2m_pw = 0, l2l = 0, l2l_s = 0, l2l_pw = 0, m2l = 0, m2l_pw = 0;
-        size_t m2l_sc = 0;   // M2L table of the scaled form, T_q rs^-|q|
-        bool sc_ok = false;  // the scaled form applies on this level
-    };
-    std::vector<LevTab> lt(nl + 1);
-    std::vector<double2> ct;  // complex tables
-    std::vector<double> rt;   // real tables
-    auto powtab = [&](double r, int n) {
-        const size_t o = rt.size();
-        double v = 1.0;
-        for (int e = 0; e <= n; e++) {
-            rt.push_back(v);
-            v *= r;
-        }
-        return o;
-    };
-    for (int l = 2; l <= nl; l++) {
-        const HLevel &L = hl[l];
-        if (l + 1 <= nl) {
-            const HLevel &C = hl[l + 1];
-            const double hb = T.boxsize[l + 1] / 2.0;
-            // M2M: child (scale r1) -> parent (scale r2), d = parent - child
+    // ---- translation tables (kept for calls with the same zk, eps, root
+    // box and depth, which fix every level's order, scale and offsets) ----
+    const HTabKey tkey{zk.x, zk.y, P.eps, T.boxsize[0], nl};
+    std::shared_ptr<HTables> tabs = htables_find(tkey);
+    if (!tabs) {
+        tabs = std::make_shared<HTables>();
+        std::vector<LevTab> &lt = tabs->lt;
+        std::vector<double2> &ct = tabs->ct;
+        std::vector<double> &rt = tabs->rt;
+        lt.resize(nl + 1);
+        auto powtab = [&](double r, int n) {
+            const size_t o = rt.size();
+            double v = 1.0;
+            for (int e = 0; e <= n; e++) {
+                rt.push_back(v);
+                v *= r;
+            }
+            return o;
+        };
+        for (int l = 2; l <= nl; l++) {
+            const HLevel &L = hl[l];
+            if (l + 1 <= nl) {
+                const HLevel &C = hl[l + 1];
+                const double hb = T.boxsize[l + 1] / 2.0;
+                // M2M: child (scale r1) -> parent (scale r2), d = parent - child
+                {
+                    const int n1 = C.p, n2 = L.p, N = n1 + n2;
+                    lt[l].m2m = ct.size();
+                    ct.resize(ct.size() + (size_t)4 * (2 * N + 1));
+                    for (int cs = 0; cs < 4; cs++) {
+                        const double sx = (cs & 1) ? 1.0 : -1.0, sy = (cs & 2) ? 1.0 : -1.0;
+                        shift_table(zk, -sx * hb, -sy * hb, N, C.rs, false,
+                                    ct.data() + lt[l].m2m + (size_t)cs * (2 * N + 1));
+                    }
+                    lt[l].m2m_s = rt.size();
+                    double f = 1.0;
+                    for (int i = 0; i <= n2; i++) {
+                        rt.push_back(f);
+                        f = f * C.rs / L.rs;
+                    }
+                    lt[l].m2m_pw = powtab(C.rs, 2 * n1);
+                }
+                // L2L: parent (scale r1) -> child (scale r2), d = child - parent
+                {
+                    const int n1 = L.p, n2 = C.p, N = n1 + n2;
+                    lt[l].l2l = ct.size();
+                    ct.resize(ct.size() + (size_t)4 * (2 * N + 1));
+                    for (int cs = 0; cs < 4; cs++) {
+                        const double sx = (cs & 1) ? 1.0 : -1.0, sy = (cs & 2) ? 1.0 : -1.0;
+                        shift_table(zk, sx * hb, sy * hb, N, L.rs, false,
+                                    ct.data() + lt[l].l2l + (size_t)cs * (2 * N + 1));
+                    }
+                    lt[l].l2l_s = rt.size();
+                    double f = 1.0;
+                    for (int i = 0; i <= n2; i++) {
+                        rt.push_back(f);
+                        f = f * C.rs / L.rs;
+                    }
+                    lt[l].l2l_pw = powtab(L.rs, 2 * n2);
+                }
+            }
+            // M2L: d = target - source = (ix, iy) * boxsize
             {
-                const int n1 = C.p, n2 = L.p, N = n1 + n2;
-                lt[l].m2m = ct.size();
-                ct.resize(ct.size() + (size_t)4 * (2 * N + 1));
-                for (int cs = 0; cs < 4; cs++) {
-                    const double sx = (cs & 1) ? 1.0 : -1.0, sy = (cs & 2) ? 1.0 : -1.0;
-                    shift_table(zk, -sx * hb, -sy * hb, N, C.rs, false,
-                                ct.data() + lt[l].m2m + (size_t)cs * (2 * N + 1));
-                }
-                lt[l].m2m_s = rt.size();
-                double f = 1.0;
-                for (int i = 0; i <= n2; i++) {
-                    rt.push_back(f);
-                    f = f * C.rs / L.rs;
-                }
-                lt[l].m2m_pw = powtab(C.rs, 2 * n1);
-            }
-            // L2L: parent (scale r1) -> child (scale r2), d = child - parent
-            {
-                const int n1 = L.p, n2 = C.p, N = n1 + n2;
-                lt[l].l2l = ct.size();
-                ct.resize(ct.size() + (size_t)4 * (2 * N + 1));
-                for (int cs = 0; cs < 4; cs++) {
-                    const double sx = (cs & 1) ? 1.0 : -1.0, sy = (cs & 2) ? 1.0 : -1.0;
-                    shift_table(zk, sx * hb, sy * hb, N, L.rs, false,
-                                ct.data() + lt[l].l2l + (size_t)cs * (2 * N + 1));
-                }
-                lt[l].l2l_s = rt.size();
-                double f = 1.0;
-                for (int i = 0; i <= n2; i++) {
-                    rt.push_back(f);
-                    f = f * C.rs / L.rs;
-                }
-                lt[l].l2l_pw = powtab(L.rs, 2 * n2);
-            }
-        }
-        // M2L: d = target - source = (ix, iy) * boxsize
-        {
-            const int p = L.p, N = 2 * p;
-            lt[l].m2l = ct.size();
-            ct.resize(ct.size() + (size_t)49 * (2 * N + 1), make_double2(0.0, 0.0));
-            for (int iy = -3; iy <= 3; iy++)
-                for (int ix = -3; ix <= 3; ix++) {
-                    if (std::abs(ix) <= 1 && std::abs(iy) <= 1) continue;
-                    shift_table(zk, ix * T.boxsize[l], iy * T.boxsize[l], N, L.rs, true,
-                                ct.data() + lt[l].m2l + (size_t)((iy + 3) * 7 + (ix + 3)) * (2 * N + 1));
-                }
-            lt[l].m2l_pw = powtab(L.rs, 2 * p);
-            // the scaled form where rs^(2p) and the scaled entries stay
-            // inside 1e-250 .. 1e250
-            if (L.rs > 0.0 && 2.0 * p * std::fabs(std::log10(L.rs)) < 250.0) {
-                const size_t n = (size_t)49 * (2 * N + 1), o = ct.size();
-                ct.resize(o + n);
-                bool fine = true;
-                std::vector<double> f(N + 1);  // rs^-q
-                f[0] = 1.0;
-                for (int q = 1; q <= N; q++) f[q] = f[q - 1] / L.rs;
-                for (size_t e = 0; e < n; e++) {
-                    const int q = (int)(e % (2 * N + 1)) - N;
-                    const double2 v = cscal(ct[lt[l].m2l + e], f[std::abs(q)]);
-                    if (!(std::fabs(v.x) <= 1e250 && std::fabs(v.y) <= 1e250)) fine = false;
-                    ct[o + e] = v;
-                }
-                if (fine) {
-                    lt[l].m2l_sc = o;
-                    lt[l].sc_ok = true;
-                } else {
-                    ct.resize(o);
+                const int p = L.p, N = 2 * p;
+                lt[l].m2l = ct.size();
+                ct.resize(ct.size() + (size_t)49 * (2 * N + 1), make_double2(0.0, 0.0));
+                for (int iy = -3; iy <= 3; iy++)
+                    for (int ix = -3; ix <= 3; ix++) {
+                        if (std::abs(ix) <= 1 && std::abs(iy) <= 1) continue;
+                        shift_table(zk, ix * T.boxsize[l], iy * T.boxsize[l], N, L.rs, true,
+                                    ct.data() + lt[l].m2l + (size_t)((iy + 3) * 7 + (ix + 3)) * (2 * N + 1));
+                    }
+                lt[l].m2l_pw = powtab(L.rs, 2 * p);
+                // the scaled form where rs^(2p) and the scaled entries stay
+                // inside 1e-250 .. 1e250
+                if (L.rs > 0.0 && 2.0 * p * std::fabs(std::log10(L.rs)) < 250.0) {
+                    const size_t n = (size_t)49 * (2 * N + 1), o = ct.size();
+                    ct.resize(o + n);
+                    bool fine = true;
+                    std::vector<double> f(N + 1);  // rs^-q
+                    f[0] = 1.0;
+                    for (int q = 1; q <= N; q++) f[q] = f[q - 1] / L.rs;
+                    for (size_t e = 0; e < n; e++) {
+                        const int q = (int)(e % (2 * N + 1)) - N;
+                        const double2 v = cscal(ct[lt[l].m2l + e], f[std::abs(q)]);
+                        if (!(std::fabs(v.x) <= 1e250 && std::fabs(v.y) <= 1e250)) fine = false;
+                        ct[o + e] = v;
+                    }
+                    if (fine) {
+                        lt[l].m2l_sc = o;
+                        lt[l].sc_ok = true;
+                    } else {
+                        ct.resize(o);
+                    }
                 }
             }
         }
+        htables_store(tkey, tabs);
     }
+    const std::vector<LevTab> &lt = tabs->lt;
+    const std::vector<double2> &ct = tabs->ct;
+    const std::vector<double> &rt = tabs->rt;
     DevBuf<double2> d_ct(std::max<size_t>(ct.size(), 1), s);
     DevBuf<double> d_rt(std::max<size_t>(rt.size(), 1), s);
     if (!ct.empty())
