@@ -96,6 +96,7 @@ class ClockSampler:
         self.lock = threading.Lock()
         self.first = threading.Event()
         self.mark_at = 0
+        self.reader = None
 
     def _read(self):
         for line in self.proc.stdout:
@@ -112,7 +113,8 @@ class ClockSampler:
         except OSError:
             self.proc = None
             return
-        threading.Thread(target=self._read, daemon=True).start()
+        self.reader = threading.Thread(target=self._read, daemon=True)
+        self.reader.start()
         self.first.wait(10.0)
 
     def mark(self):
@@ -135,6 +137,8 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
+            self.proc.wait()
+        self.reader.join(5.0)  # ends at the pipe's end of file
         with self.lock:
             out = "".join(self.lines[self.mark_at:n_end + 1])
         sm, smax, reasons = [], [], set()
