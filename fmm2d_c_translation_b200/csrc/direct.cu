@@ -186,6 +186,24 @@ void launch_partial(const DirectArgs &a, int chunk, int nchunk, double2 *part,
 
 int direct_outputs(int form, int pgh) { return nouts(form, pgh); }
 
+void check_direct_arrays(int form, const void *sources, int ifcharge,
+                         const void *charge, int ifdipole, const void *dipstr,
+                         const void *dipvec, const void *targ, int ifpgh,
+                         const void *pot, const void *grad, const void *hess) {
+    const char *missing = nullptr;
+    if (!sources) missing = "sources";
+    else if (!targ) missing = "targ";
+    else if (!pot) missing = "pot";
+    else if (ifcharge && !charge) missing = "charge";
+    else if (ifdipole && !dipstr) missing = "dipstr";
+    else if (ifdipole && form == kFormLaplace && !dipvec) missing = "dipvec";
+    else if (ifpgh >= 2 && !grad) missing = "grad";
+    else if (ifpgh >= 3 && !hess) missing = "hess";
+    if (missing)
+        throw FmmError(4, std::string("direct sum: ") + missing +
+                              " is NULL but the flags require it");
+}
+
 int direct_chunks(int ns, int nt, int nd) {
     const int tblocks = (nt + kDThreads - 1) / kDThreads;
     int want = (4 * kNumSM + tblocks * nd - 1) / std::max(1, tblocks * nd);
@@ -257,9 +275,24 @@ int run_direct(int form, int nd, int ns, const double *sources, int ifcharge,
             (!ifcharge && !ifdipole))
             throw FmmError(4, "invalid direct-sum arguments");
         if (nt == 0 || ns == 0) return;
+        check_direct_arrays(form, sources, ifcharge, charge, ifdipole, dipstr,
+                            dipvec, targ, ifpgh, pot, grad, hess);
         CallCtx ctx;
         cudaStream_t s = ctx.stream();
         const bool od = dev_ptr(sources);
+        {
+            // Every array the flags use must live where `sources` lives: a
+            // device kernel given a host pointer, or a host copy given a
+            // device pointer, would fault.
+            const void *used[] = {targ, pot, ifcharge ? charge : nullptr,
+                                  ifdipole ? dipstr : nullptr,
+                                  (ifdipole && form == kFormLaplace) ? dipvec : nullptr,
+                                  ifpgh >= 2 ? grad : nullptr,
+                                  ifpgh >= 3 ? hess : nullptr};
+            for (const void *p : used)
+                if (p && dev_ptr(p) != od)
+                    throw FmmError(4, "direct sum: arrays mix host and device memory");
+        }
         const int gc = form == kFormLaplace ? 2 : 1, hc = form == kFormLaplace ? 3 : 1;
         Staged S, T, Q, D, V, Po, G, H;
         S.in(sources, ns, od, s);

@@ -30,6 +30,13 @@ struct DirectArgs {
 int direct_outputs(int form, int pgh);
 int direct_chunks(int ns, int nt, int nd);
 int direct_strict(int form, int ifcharge, int ifdipole, int pgh);
+// Throws FmmError(4) when an array that the flags require is NULL: sources,
+// targ and pot always; charge when ifcharge; dipstr (and, for the Laplace
+// form, dipvec) when ifdipole; grad when ifpgh >= 2; hess when ifpgh == 3.
+void check_direct_arrays(int form, const void *sources, int ifcharge,
+                         const void *charge, int ifdipole, const void *dipstr,
+                         const void *dipvec, const void *targ, int ifpgh,
+                         const void *pot, const void *grad, const void *hess);
 // Adds the direct sum into a.pot/grad/hess; `part` holds
 // nchunk * nd * nt * direct_outputs(form, pgh) double2 of scratch.
 void direct_sum(const DirectArgs &a, double2 *part, int nchunk, cudaStream_t s);

@@ -21,8 +21,14 @@
 //  * The first call on a device looks up the array's device address (with
 //    that device current) and keeps it; make that first call before any
 //    stream capture begins.
-//  * All arrays must be device memory of the current device; host arrays
-//    are rejected (copying them would need device memory).
+//  * All arrays must be device memory of the current device; host arrays,
+//    arrays of another device and NULL arrays that the flags require are
+//    rejected with ier = 4 before any GPU work (copying host arrays would
+//    need device memory).
+//  * The scratch address is looked up once per device and kept for the life
+//    of the process: do not call this entry point on a device after
+//    cudaDeviceReset (or any other teardown of its primary context) in the
+//    same process, since the kept address then no longer names the array.
 //  * Every call on a device shares the one array.  A call first writes every
 //    scratch value it later reads, so what a previous call left behind is
 //    never read; but calls whose work overlaps on the GPU (for example from
@@ -63,13 +69,15 @@ double2 *noalloc_scratch(int dev) {
     return g_noalloc_addr[dev];
 }
 
-bool on_device(const void *p) {
+// True when p is device (or managed) memory that device `dev` owns.
+bool on_device(const void *p, int dev) {
     cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    if (a.type == cudaMemoryTypeManaged) return true;
+    return a.type == cudaMemoryTypeDevice && a.device == dev;
 }
 
 }  // namespace
@@ -89,6 +97,8 @@ FMM_EXPORT int fmm2d_b200_l2d_direct_noalloc(
             (!ifcharge && !ifdipole))
             throw FmmError(4, "invalid direct-sum arguments");
         if (nt == 0 || ns == 0) return;
+        check_direct_arrays(kFormLaplace, sources, ifcharge, charge, ifdipole,
+                            dipstr, dipvec, targ, ifpgh, pot, grad, hess);
         const int nout = direct_outputs(kFormLaplace, ifpgh);
         const size_t per_chunk = (size_t)nd * nt * nout;
         if (per_chunk > kNoAllocScratchValues)
@@ -101,12 +111,13 @@ FMM_EXPORT int fmm2d_b200_l2d_direct_noalloc(
                                 ifdipole ? dipvec : nullptr,
                                 ifpgh >= 2 ? grad : nullptr,
                                 ifpgh >= 3 ? hess : nullptr};
-        for (const void *p : arrays)
-            if (p && !on_device(p))
-                throw FmmError(4, "the no-allocation entry point takes device arrays only");
         int dev = 0;
         FMM_CUDA(cudaGetDevice(&dev));
         if (dev < 0 || dev >= 64) throw FmmError(4, "device index out of range");
+        for (const void *p : arrays)
+            if (p && !on_device(p, dev))
+                throw FmmError(4, "the no-allocation entry point takes device arrays "
+                                  "of the current device only");
         double2 *scratch = noalloc_scratch(dev);
         int nchunk = direct_chunks(ns, nt, nd);
         const int cap = (int)(kNoAllocScratchValues / per_chunk);

@@ -75,8 +75,13 @@ constexpr int kBatchMax = 64;
 constexpr int kBatchPoints = 200000;   // points of one batch
 constexpr int kBatchRequest = 50000;   // largest request that is batched
 
+// A request may join a batch only if it would also pass the batch driver's
+// own argument checks (at least one source, a charge or a dipole, valid
+// output flags), so one malformed request cannot fail its neighbours.
 bool batchable(const FmmCall &c) {
     return c.kernel == kLaplace && c.nd == 1 && c.ndiv < 0 && c.ifnear == 1 && !c.timeinfo &&
+           c.ns >= 1 && c.nt >= 0 && (c.ifcharge || c.ifdipole) && c.ifpgh >= 0 &&
+           c.ifpgh <= 3 && c.ifpghtarg >= 0 && c.ifpghtarg <= 3 &&
            (int64_t)c.ns + c.nt <= kBatchRequest;
 }
 
@@ -273,12 +278,20 @@ class Server {
             }
             const double t0 = now_ms();
             for (Request *r : batch) r->t_start = t0;
-            const int ier = batch.size() == 1 ? run_fmm(batch[0]->call) : run_batch(batch);
+            std::vector<int> iers(batch.size(), 0);
+            if (batch.size() == 1) {
+                iers[0] = run_fmm(batch[0]->call);
+            } else if (run_batch(batch) != 0) {
+                // a failed batch is rerun one request at a time, so each
+                // request gets the status it would have had alone
+                for (size_t i = 0; i < batch.size(); i++) iers[i] = run_fmm(batch[i]->call);
+            }
             const double t_end = now_ms();
             {
                 std::lock_guard<std::mutex> g(mu_);
-                for (Request *r : batch) {
-                    r->ier = ier;
+                for (size_t i = 0; i < batch.size(); i++) {
+                    Request *r = batch[i];
+                    r->ier = iers[i];
                     r->t_end = t_end;
                     r->done = true;
                     in_use_ -= r->bytes;

@@ -791,10 +791,13 @@ void fmm2d_b200_helm_jvec(int n, double z_re, double z_im, double rscale,
  * that cannot have device memory allocated for them (GPU memory owned by
  * another allocator or a fixed budget; callers that cannot accept an
  * allocation call's possible device synchronization).  Same arguments plus
- * a stream; device arrays only; scratch is a fixed 4 MiB device array
- * (nd * nt * outputs <= 262144, outputs = 1, 3 or 6), held by every GPU
- * that loads the library.  The first call on a device sets the array up
- * and should come before any stream capture; calls that overlap on the GPU
+ * a stream; device arrays of the current device only (host arrays, another
+ * device's arrays and NULL arrays the flags require give ier = 4); scratch
+ * is a fixed 4 MiB device array (nd * nt * outputs <= 262144, outputs = 1,
+ * 3 or 6), held by every GPU that loads the library.  The first call on a
+ * device sets the array up and should come before any stream capture; the
+ * address it looks up is kept for the process, so the entry point must not
+ * be used on a device after cudaDeviceReset.  Calls that overlap on the GPU
  * race on the shared array.  Returns after `stream` has finished the call. */
 int fmm2d_b200_l2d_direct_noalloc(int nd, int ns, const double *sources,
                                   int ifcharge, const double _Complex *charge,

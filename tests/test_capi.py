@@ -70,3 +70,37 @@ def test_leaf_capacity_matches_reference_hndiv2d():
                    I(0), I(1), I(0), ctypes.byref(nd), ctypes.byref(idf))
         assert L.fmm2d_b200_leaf_capacity(ctypes.c_double(eps), 100, 50) == nd.value
         assert idf.value == 0
+
+
+def _direct_argtypes(L):
+    base = ([ctypes.c_int] * 2 + [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                  ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                  ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
+            + [ctypes.c_void_p] * 3 + [ctypes.c_double])
+    L.fmm2d_b200_l2d_direct.argtypes = base
+    L.fmm2d_b200_l2d_direct_noalloc.argtypes = base + [ctypes.c_void_p]
+
+
+@pytest.mark.parametrize("missing", ["charge", "dipstr", "dipvec", "grad", "hess",
+                                     "sources", "targ", "pot"])
+@pytest.mark.parametrize("entry", ["l2d_direct", "l2d_direct_noalloc"])
+def test_direct_refuses_null_required_arrays(entry, missing):
+    """A NULL array that the flags require is refused with ier = 4 on the
+    host, before any device work (no GPU is touched)."""
+    import fmm2d_c_translation_b200 as fm
+    L = fm.lib()
+    _direct_argtypes(L)
+    ns, nt = 10, 5
+    a = {k: np.zeros(n) for k, n in [("sources", 2 * ns), ("charge", 2 * ns),
+                                      ("dipstr", 2 * ns), ("dipvec", 2 * ns),
+                                      ("targ", 2 * nt), ("pot", 2 * nt),
+                                      ("grad", 4 * nt), ("hess", 6 * nt)]}
+    P = {k: (None if k == missing else v.ctypes.data_as(ctypes.c_void_p))
+         for k, v in a.items()}
+    args = [1, ns, P["sources"], 1, P["charge"], 1, P["dipstr"], P["dipvec"], nt,
+            P["targ"], 3, P["pot"], P["grad"], P["hess"], 1e-14]
+    if entry.endswith("noalloc"):
+        args.append(None)
+    ier = getattr(L, "fmm2d_b200_" + entry)(*args)
+    assert ier == 4
+    assert missing in fm.last_error() and "NULL" in fm.last_error()
