@@ -124,11 +124,12 @@ unsigned long long launch_count() { return g_launches.load(); }
 void set_profiling(int on) { g_profiling.store(on); }
 bool profiling_enabled() { return g_profiling.load() != 0; }
 
-void prof_begin(cudaStream_t s) {
+void prof_begin(cudaStream_t s, bool force) {
     g_prof.marks.clear();
     g_prof.counts.clear();
-    g_prof.active = profiling_enabled();
+    g_prof.active = force || profiling_enabled();
     if (!g_prof.active) return;
+    g_prof.result.clear();
     g_prof.marks.push_back({"", 0});
     FMM_CUDA(cudaEventRecord(g_prof.ev(0), s));
 }
@@ -161,6 +162,20 @@ void prof_end(cudaStream_t s) {
 
 void prof_set_count(const char *name, double value) {
     if (g_prof.active) g_prof.counts.push_back({name, value});
+}
+
+void prof_timeinfo(double *timeinfo) {
+    static const struct {
+        const char *phase;
+        int slot;
+    } map[] = {{"p2m", 0},       {"p2l", 1},       {"m2m", 2},         {"m2l", 3},
+               {"l2l", 4},       {"m2p_l2p", 6},   {"p2p", 7},         {"h_p2m_p2l", 0},
+               {"h_m2m", 2},     {"h_m2l", 3},     {"h_l2l", 4},       {"h_eval_src", 6},
+               {"h_eval_trg", 6}, {"h_p2p_src", 7}, {"h_p2p_trg", 7}};
+    for (int k = 0; k < 8; k++) timeinfo[k] = 0.0;
+    for (auto &r : g_prof.result)
+        for (auto &m : map)
+            if (r.first == m.phase) timeinfo[m.slot] += r.second * 1e-3;
 }
 
 // "name=value;" pairs of the last profiled call on this thread.

@@ -70,10 +70,20 @@ void note_launch();
 // fmm2d_b200_last_profile().
 // ---------------------------------------------------------------------------
 bool profiling_enabled();
-void prof_begin(cudaStream_t s);
+// force: record this call's phases even when profiling is off (used to fill
+// a caller's timeinfo array).
+void prof_begin(cudaStream_t s, bool force = false);
 void prof_mark(const char *phase, cudaStream_t s);
 void prof_end(cudaStream_t s);
 void prof_set_count(const char *name, double value);
+// The reference's timeinfo(8) (src/laplace/cfmm2d.f:827-1330,
+// src/helmholtz/hfmm2d.f) in seconds, from the phases of the last profiled
+// call on this thread: 1 P2M, 2 P2L (list 4), 3 M2M, 4 M2L, 5 L2L,
+// 6 M2P (list 3), 7 L2P, 8 P2P.  Phases that one kernel does together are
+// reported in the first of their entries: the Laplace M2P and L2P share
+// entry 7 (entry 6 is 0), the Helmholtz P2M and P2L share entry 1 (entry 2
+// is 0) and its M2P and L2P share entry 7.
+void prof_timeinfo(double *timeinfo);
 
 // ---------------------------------------------------------------------------
 // Device buffers: stream-ordered allocations from the device's default pool.

@@ -377,8 +377,6 @@ void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaS
     // complete when the call returns)
     if (sync) FMM_CUDA(cudaStreamSynchronize(s));
     prof_mark("scatter_d2h", s);
-    if (c.timeinfo)
-        for (int k = 0; k < 8; k++) c.timeinfo[k] = 0.0;
 }
 
 namespace {
@@ -386,11 +384,12 @@ namespace {
 void run_laplace_family(const FmmCall &c, CallCtx &ctx) {
     cudaStream_t s = ctx.stream();
     const bool on_dev = is_device_ptr(c.sources);
-    prof_begin(s);
+    prof_begin(s, c.timeinfo != nullptr);
     LapGeometry G;
     laplace_geometry(c, on_dev, s, G);
     laplace_evaluate(c, G, on_dev, s);
     prof_end(s);
+    if (c.timeinfo) prof_timeinfo(c.timeinfo);
 }
 
 
@@ -441,7 +440,7 @@ void run_helmholtz(const FmmCall &c, CallCtx &ctx) {
     const int nd = c.nd, ns = c.ns, nt = c.nt;
     if (c.zk[0] == 0.0 && c.zk[1] == 0.0) throw FmmError(4, "zk must be nonzero");
     const bool on_dev = is_device_ptr(c.sources);
-    prof_begin(s);
+    prof_begin(s, c.timeinfo != nullptr);
     InBuf<double2> src_in, trg_in, chg_in, dip_in;
     InBuf<double> dv_in;
     src_in.set(c.sources, ns, on_dev, s);
@@ -517,8 +516,7 @@ void run_helmholtz(const FmmCall &c, CallCtx &ctx) {
     unsort(nt, T.itarg.get(), tpgh, tpot, tgrad, thess, c.pottarg, c.gradtarg, c.hesstarg);
     prof_mark("scatter_d2h", s);
     prof_end(s);
-    if (c.timeinfo)
-        for (int k = 0; k < 8; k++) c.timeinfo[k] = 0.0;
+    if (c.timeinfo) prof_timeinfo(c.timeinfo);
 }
 
 }  // namespace

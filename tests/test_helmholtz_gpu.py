@@ -244,3 +244,29 @@ def test_h2d_direct_vs_reference(glib, zk, ifc, ifd, pgh):
         assert W.rel_err(grad, rg) < 1e-13
     if pgh >= 3:
         assert W.rel_err(hess, rh) < 1e-13
+
+
+def test_hfmm2d_zk200_against_reference(glib):
+    """The zk = 200, eps = 1e-6 case (hfmm2d_s_cd_p, uniform points, complex
+    charges and dipoles N(0,1), unit dipole vectors) at 2e5 sources against
+    the reference's C translation on the same inputs.  The tree is the
+    reference's (bit-exact), so the expansion orders -- up to p = 94 on
+    level 1 here -- are the same and both sides differ only by round-off."""
+    if not refimpl.have_ref():
+        pytest.skip("reference build absent")
+    rng = np.random.default_rng(200)
+    ns = 200000
+    src = rng.random((2, ns))
+    q = rng.standard_normal(ns) + 1j * rng.standard_normal(ns)
+    d = rng.standard_normal(ns) + 1j * rng.standard_normal(ns)
+    th = rng.uniform(0, 2 * np.pi, ns)
+    v = np.stack([np.cos(th), np.sin(th)])
+    zk = 200.0 + 0j
+    out, ier = W.call(glib, "h", "s_cd_p", 1e-6, src, q, d, v, None, zk=zk)
+    assert ier == 0
+    ro, rier = W.call(refimpl.ref(), "h", "s_cd_p", 1e-6, src, q, d, v, None, zk=zk)
+    assert rier == 0
+    assert W.rel_err(out["pot"], ro["pot"]) < 1e-10, W.rel_err(out["pot"], ro["pot"])
+    # and both against the direct sum at 200 sources, to the requested eps
+    pot, _, _ = h_direct(glib, zk, src, q, d, v, src[:, :200], 1, 1, 1)
+    assert W.rel_err(out["pot"][:200], pot) < 1e-6
