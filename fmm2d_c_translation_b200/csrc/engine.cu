@@ -489,6 +489,7 @@ void run_helmholtz(const FmmCall &c, CallCtx &ctx) {
     P.sset = HPointSet{in.src.get(), T.srcse.get(), ns, spgh, spot.get(), sgrad.get(), shess.get()};
     P.tset = HPointSet{in.trg.get(), T.trgse.get(), nt, tpgh, tpot.get(), tgrad.get(), thess.get()};
     P.ifnear = c.ifnear;
+    P.mixed = c.precision == kPrecMixed || (c.precision == kPrecAuto && c.eps >= 0.5e-6);
     helmholtz_fmm(T, P, s);
     // back to input order: per point, nd * comps consecutive values
     auto unsort = [&](int n, const int *perm, int pgh, const DevBuf<double2> &po,

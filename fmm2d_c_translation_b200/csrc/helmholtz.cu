@@ -817,6 +817,13 @@ bool helm_m2l_tiled() {
     return !(e && !strcmp(e, "box"));
 }
 
+// The tensor-core form in the mixed mode unless FMM2D_B200_HELM_M2L is
+// "box" or "tile" (both FP64).
+bool helm_m2l_tc_enabled() {
+    const char *e = getenv("FMM2D_B200_HELM_M2L");
+    return !(e && (!strcmp(e, "box") || !strcmp(e, "tile")));
+}
+
 // ---------------------------------------------------------------------------
 // M2P + L2P for one point set: thread per point.
 // ---------------------------------------------------------------------------
@@ -1263,6 +1270,7 @@ struct LevTab {
     size_t m2m = 0, m2m_s = 0, m2m_pw = 0, l2l = 0, l2l_s = 0, l2l_pw = 0, m2l = 0, m2l_pw = 0;
     size_t m2l_sc = 0;   // M2L table of the scaled form, T_q rs^-|q|
     bool sc_ok = false;  // the scaled form applies on this level
+    double m2l_max = 0;  // largest |T_q| of the M2L table (tensor-core form's scale)
 };
 struct HTables {
     std::vector<LevTab> lt;
@@ -1396,6 +1404,15 @@ void helmholtz_fmm(const Tree &T, const HelmProblem &P, cudaStream_t s) {
                                     ct.data() + lt[l].m2l + (size_t)((iy + 3) * 7 + (ix + 3)) * (2 * N + 1));
                     }
                 lt[l].m2l_pw = powtab(L.rs, 2 * p);
+                {
+                    double mx = 0.0;
+                    const size_t n = (size_t)49 * (2 * N + 1);
+                    for (size_t e = 0; e < n; e++) {
+                        const double2 v = ct[lt[l].m2l + e];
+                        mx = std::max(mx, std::max(std::fabs(v.x), std::fabs(v.y)));
+                    }
+                    lt[l].m2l_max = mx;
+                }
                 // the scaled form where rs^(2p) and the scaled entries stay
                 // inside 1e-250 .. 1e250
                 if (L.rs > 0.0 && 2.0 * p * std::fabs(std::log10(L.rs)) < 250.0) {
@@ -1473,8 +1490,32 @@ void helmholtz_fmm(const Tree &T, const HelmProblem &P, cudaStream_t s) {
     for (int l = 2; l <= nl; l++) pmax = std::max(pmax, hl[l].p);
     DevBuf<double2> zero(tiled ? (size_t)(2 * pmax + 1) * nd : 0, s), mps;
     if (tiled) zero.zero(s);
+    // mixed mode: levels of order <= 23 on the tensor cores (tiles of
+    // 128 / nd target boxes)
+    SlotPlan spl_tc;
+    const bool tc = P.mixed && nd <= 128 && helm_m2l_tc_enabled() &&
+                    plan_slots(T, sp, tp, 128 / nd, s, spl_tc);
+    DevBuf<int> tc_err(tc ? 1 : 0, s);
+    if (tc) FMM_CUDA(cudaMemsetAsync(tc_err.get(), 0, sizeof(int), s));
+    bool tc_used = false;
     for (int l = 2; l <= nl; l++) {
         if (!hl[l].flag) continue;
+        if (tc && hl[l].p <= helm_m2l_tc_max_order()) {
+            HtLevel hv;
+            hv.level = l;
+            hv.p = hl[l].p;
+            hv.nd = nd;
+            hv.lstart = hl[l].lstart;
+            hv.nbox = T.lend[l] - T.lstart[l];
+            hv.off = hl[l].off;
+            hv.maxabs = lt[l].m2l_max;
+            hv.table = d_ct.get() + lt[l].m2l;
+            hv.pw = d_rt.get() + lt[l].m2l_pw;
+            if (helm_m2l_tc_level(hv, spl_tc, mp.get(), loc.get(), tc_err.get(), s)) {
+                tc_used = true;
+                continue;
+            }
+        }
         if (tiled) {
             if (spl.ntiles == 0) continue;
             HTiles ht;
@@ -1534,6 +1575,8 @@ void helmholtz_fmm(const Tree &T, const HelmProblem &P, cudaStream_t s) {
         FMM_CHECK_LAUNCH();
     }
     prof_mark("h_m2l", s);
+    if (tc_used && read_scalar(tc_err.get(), s) != 0)
+        throw FmmError(4, "tensor-core Helmholtz M2L: a wait for an MMA or operand barrier timed out");
     // ---- L2L, downward (parents at levels 2 .. nl-1) ----
     for (int l = 2; l <= nl - 1; l++) {
         if (!hl[l].flag) continue;

@@ -36,6 +36,9 @@ struct HelmProblem {
     const double2 *dipvec = nullptr;  // [k*nd + c] = (v1, v2)
     HPointSet sset, tset;
     int ifnear = 1;
+    // M2L of the levels of order <= 23 on the tensor cores in TF32 x 3
+    // (helm_m2l_tc.cu); everything else stays FP64
+    bool mixed = false;
 };
 
 // Runs the steps of hfmm2dmain (c_translation/src/hfmm2d.c:619-1528) on the
@@ -47,6 +50,25 @@ void helmholtz_fmm(const Tree &T, const HelmProblem &P, cudaStream_t s);
 // outputs; pairs with |zk r| below thresh are skipped.
 void helmholtz_direct(const HelmProblem &P, int ns, HPointSet set, double thresh,
                       cudaStream_t s);
+
+// One level of the tensor-core M2L of the mixed mode (helm_m2l_tc.cu).
+struct HtLevel {
+    int level = 0, p = 0, nd = 1, lstart = 0;
+    long long nbox = 0;         // boxes of the level
+    long long off = 0;          // offset of the level's block in the expansions
+    double maxabs = 0.0;        // largest |T(q)| of the level's M2L tables
+    const double2 *table = nullptr;  // device: [49][4p + 1] M2L table
+    const double *pw = nullptr;      // device: rs^e, e = 0 .. 2p
+};
+struct SlotPlan;
+// Highest expansion order the tensor-core M2L takes.
+int helm_m2l_tc_max_order();
+// Adds the list-2 interactions of level lv.level to the local expansions
+// with the tensor-core M2L; false (nothing launched) when the level does not
+// qualify.  spl: slot plan with tiles of 128 / nd target boxes; *err is set
+// when a bounded wait of the kernel runs out.
+bool helm_m2l_tc_level(const HtLevel &lv, const SlotPlan &spl, const double2 *mp, double2 *loc,
+                       int *err, cudaStream_t s);
 
 // Host restatements of the reference's scalar routines.
 // h2dterms (c_translation/src/h2dterms.c:19-69): expansion order for a box

@@ -33,10 +33,6 @@ __device__ __forceinline__ double2 shfl_up2(double2 v, int d) {
     return make_double2(__shfl_up_sync(0xffffffffu, v.x, d),
                         __shfl_up_sync(0xffffffffu, v.y, d));
 }
-__device__ __forceinline__ double2 shfl2(double2 v, int l) {
-    return make_double2(__shfl_sync(0xffffffffu, v.x, l),
-                        __shfl_sync(0xffffffffu, v.y, l));
-}
 
 // Lane k receives z^k (lane 0: 1), by a warp prefix product.
 __device__ __forceinline__ double2 warp_powers(double2 z) {
@@ -82,204 +78,6 @@ struct EvalCounts {
         return n;
     }
 };
-
-// ---------------------------------------------------------------------------
-// Step 1, P2M (l2dformmpc/d/cd, laprouts2d.c:41-190):
-//   M_0 += q,  M_n += -q (z/r)^n / n,  M_n += d z^(n-1) / r^n,  z = x - c.
-// ---------------------------------------------------------------------------
-template <int CH>
-__global__ void __launch_bounds__(kBlock) p2m_kernel(
-    int lo, int hi, const int *__restrict__ nchild,
-    const double2 *__restrict__ centers, const int *__restrict__ level,
-    const double *__restrict__ bs, const int2 *__restrict__ sse,
-    const double2 *__restrict__ src, const double2 *__restrict__ chg,
-    const double2 *__restrict__ dip, int ifc, int ifd, int ndc, int c0, int p,
-    double2 *__restrict__ mp) {
-    const int lane = lane_id();
-    const int stride = (p + 1) * ndc;
-    for (int b = lo + warp_global(); b < hi; b += warp_count()) {
-        if (nchild[b] != 0) continue;
-        const int2 r_ = sse[b];
-        if (r_.y <= r_.x) continue;
-        const double2 c = centers[b];
-        const double r = bs[level[b]], rinv = 1.0 / r;
-        for (int kb = 0; kb <= p; kb += 32) {
-            const int k = kb + lane;
-            double2 acc[CH];
-#pragma unroll
-            for (int q = 0; q < CH; q++) acc[q] = make_double2(0.0, 0.0);
-            for (int j = r_.x; j < r_.y; j++) {
-                const double2 x = src[j];
-                const double2 z = make_double2((x.x - c.x) / r, (x.y - c.y) / r);
-                const double2 pw = warp_powers(z);
-                const double2 zk = chunk_power(pw, z, kb);  // z^k
-                double2 zk1 = shfl_up2(zk, 1);               // z^(k-1)
-                if (lane == 0) zk1 = kb == 0 ? make_double2(0.0, 0.0) : zpow_int(z, kb - 1);
-                if (k <= p) {
-#pragma unroll
-                    for (int q = 0; q < CH; q++) {
-                        if (ifc) {
-                            const double2 qq = chg[(size_t)j * ndc + c0 + q];
-                            if (k == 0)
-                                acc[q] = cadd(acc[q], qq);
-                            else
-                                cfma(acc[q], qq, cscal(zk, -1.0 / k));
-                        }
-                        if (ifd && k >= 1) {
-                            const double2 dd = dip[(size_t)j * ndc + c0 + q];
-                            cfma(acc[q], dd, cscal(zk1, rinv));
-                        }
-                    }
-                }
-            }
-            if (k <= p) {
-#pragma unroll
-                for (int q = 0; q < CH; q++)
-                    mp[(size_t)b * stride + (size_t)k * ndc + c0 + q] = acc[q];
-            }
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Step 2, P2L from list 4 (l2dformtac/d/cd, laprouts2d.c:358-505):
-//   L_0 += q log|z|,  L_n += -q (r/z)^n / n,  L_n += -d (r/z)^n / z.
-// ---------------------------------------------------------------------------
-template <int CH>
-__global__ void __launch_bounds__(kBlock) p2l_kernel(
-    int lo, int hi, EvalCounts ec, const int *__restrict__ nlist4,
-    const int *__restrict__ list4, const double2 *__restrict__ centers,
-    const int *__restrict__ level, const double *__restrict__ bs,
-    const double2 *__restrict__ src, const double2 *__restrict__ chg,
-    const double2 *__restrict__ dip, int ifc, int ifd, int ndc, int c0, int p,
-    double2 *__restrict__ loc) {
-    const int lane = lane_id();
-    const int stride = (p + 1) * ndc;
-    for (int b = lo + warp_global(); b < hi; b += warp_count()) {
-        const int n4 = nlist4[b];
-        if (n4 == 0 || ec.npts(b) <= 0) continue;
-        const double2 c = centers[b];
-        const double r = bs[level[b]];
-        for (int kb = 0; kb <= p; kb += 32) {
-            const int k = kb + lane;
-            double2 acc[CH];
-#pragma unroll
-            for (int q = 0; q < CH; q++) acc[q] = make_double2(0.0, 0.0);
-            for (int e = 0; e < n4; e++) {
-                const int jb = list4[kMaxList4 * b + e];
-                const int2 r_ = ec.sse[jb];
-                for (int j = r_.x; j < r_.y; j++) {
-                    const double2 x = src[j];
-                    const double2 z0 = make_double2(x.x - c.x, x.y - c.y);
-                    const double2 zi = cinv(z0);
-                    const double2 w = cscal(zi, r);                     // r/z
-                    const double2 wk = chunk_power(warp_powers(w), w, kb);  // (r/z)^k
-                    const double lz = 0.5 * log(z0.x * z0.x + z0.y * z0.y);
-                    if (k <= p) {
-#pragma unroll
-                        for (int q = 0; q < CH; q++) {
-                            if (ifc) {
-                                const double2 qq = chg[(size_t)j * ndc + c0 + q];
-                                if (k == 0)
-                                    cfma(acc[q], qq, make_double2(lz, 0.0));
-                                else
-                                    cfma(acc[q], qq, cscal(wk, -1.0 / k));
-                            }
-                            if (ifd) {
-                                const double2 dd = dip[(size_t)j * ndc + c0 + q];
-                                cfma(acc[q], dd, cscal(cmul(wk, zi), -1.0));
-                            }
-                        }
-                    }
-                }
-            }
-            if (k <= p) {
-#pragma unroll
-                for (int q = 0; q < CH; q++) {
-                    double2 &o = loc[(size_t)b * stride + (size_t)k * ndc + c0 + q];
-                    o = cadd(o, acc[q]);
-                }
-            }
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Step 3, M2M (l2dmpmp, laprouts2d.c:666-775), child c1 -> parent c2:
-//   h~_j = h_j (r1/z0)^j,  z0 = c1 - c2
-//   H_0 += h_0,  H_i += [-h~_0/i + sum_{j=1..i} C(i-1,j-1) h~_j] (z0/r2)^i
-// ---------------------------------------------------------------------------
-template <int CH>
-__global__ void __launch_bounds__(kBlock) m2m_kernel(
-    int lo, int hi, const int *__restrict__ nchild,
-    const int *__restrict__ child, const double2 *__restrict__ centers,
-    double r1, double r2, const int2 *__restrict__ sse, int ndc, int c0,
-    int p, const double *__restrict__ binom, double2 *__restrict__ mp) {
-    extern __shared__ double2 sh_m2m[];
-    const int lane = lane_id();
-    const int wib = threadIdx.x >> 5;
-    double2 *ht = sh_m2m + (size_t)wib * (p + 1) * CH;
-    // binomials C(l, m), 0 <= m <= l < p, row stride p (after the warp buffers)
-    double *bsh = reinterpret_cast<double *>(sh_m2m + (size_t)kWarpsPerBlock * (p + 1) * CH);
-    for (int e = threadIdx.x; e < p * p; e += blockDim.x)
-        bsh[e] = binom[(size_t)(e / p) * (kLdc + 1) + (e % p)];
-    __syncthreads();
-    const int stride = (p + 1) * ndc;
-    for (int b = lo + warp_global(); b < hi; b += warp_count()) {
-        if (nchild[b] == 0) continue;
-        const double2 c2 = centers[b];
-        for (int kb = 0; kb <= p; kb += 32) {
-            const int i = kb + lane;
-            double2 acc[CH];
-#pragma unroll
-            for (int q = 0; q < CH; q++) acc[q] = make_double2(0.0, 0.0);
-            for (int ch = 0; ch < 4; ch++) {
-                const int cb = child[4 * b + ch];
-                if (count(sse, cb) <= 0) continue;
-                const double2 c1 = centers[cb];
-                const double2 z0 = make_double2(c1.x - c2.x, c1.y - c2.y);
-                const double2 w1 = cinv(make_double2(z0.x / r1, z0.y / r1));
-                const double2 w2 = make_double2(z0.x / r2, z0.y / r2);
-                const double2 pw1 = warp_powers(w1);
-                for (int jb = 0; jb <= p; jb += 32) {
-                    const int j = jb + lane;
-                    const double2 wj = chunk_power(pw1, w1, jb);
-                    if (j <= p)
-#pragma unroll
-                        for (int q = 0; q < CH; q++)
-                            ht[j * CH + q] = cmul(mp[(size_t)cb * stride + (size_t)j * ndc + c0 + q], wj);
-                }
-                __syncwarp();
-                const double2 wi = chunk_power(warp_powers(w2), w2, kb);
-                if (i <= p) {
-#pragma unroll
-                    for (int q = 0; q < CH; q++) {
-                        double2 t;
-                        if (i == 0) {
-                            t = ht[q];
-                        } else {
-                            t = cscal(ht[q], -1.0 / i);
-                            const double *brow = bsh + (size_t)(i - 1) * p;
-                            for (int j = 1; j <= i; j++) {
-                                const double cb_ = brow[j - 1];
-                                t.x = fma(cb_, ht[j * CH + q].x, t.x);
-                                t.y = fma(cb_, ht[j * CH + q].y, t.y);
-                            }
-                            t = cmul(t, wi);
-                        }
-                        acc[q] = cadd(acc[q], t);
-                    }
-                }
-                __syncwarp();
-            }
-            if (i <= p) {
-#pragma unroll
-                for (int q = 0; q < CH; q++)
-                    mp[(size_t)b * stride + (size_t)i * ndc + c0 + q] = acc[q];
-            }
-        }
-    }
-}
 
 // ---------------------------------------------------------------------------
 // Step 4, M2L over list 2 (l2dmploc, laprouts2d.c:886-994), source c1 ->
@@ -366,66 +164,6 @@ __global__ void __launch_bounds__(kBlock) m2l_kernel(
                     loc[(size_t)b * stride + (size_t)i * ndc + c0 + q] = acc[q];
             }
         }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Step 5, L2L (l2dlocloc, laprouts2d.c:777-884), parent c1 -> child c2:
-//   J~_j = J_j (z0/r1)^j,  z0 = c2 - c1
-//   L_i += [sum_{j>=i} C(j, i) J~_j] (r2/z0)^i
-// ---------------------------------------------------------------------------
-template <int CH>
-__global__ void __launch_bounds__(kBlock) l2l_kernel(
-    int lo, int hi, EvalCounts ec, const int *__restrict__ parent,
-    const double2 *__restrict__ centers, double r1, double r2, int ndc,
-    int c0, int p, const double *__restrict__ binom,
-    double2 *__restrict__ loc) {
-    extern __shared__ double2 sh_l2l[];
-    const int lane = lane_id();
-    const int wib = threadIdx.x >> 5;
-    double2 *jt = sh_l2l + (size_t)wib * (p + 1) * CH;
-    // binomials C(j, i), 0 <= i, j <= p, as bsh[j * (p + 1) + i]
-    double *bsh = reinterpret_cast<double *>(sh_l2l + (size_t)kWarpsPerBlock * (p + 1) * CH);
-    for (int e = threadIdx.x; e < (p + 1) * (p + 1); e += blockDim.x)
-        bsh[e] = binom[(size_t)(e / (p + 1)) * (kLdc + 1) + (e % (p + 1))];
-    __syncthreads();
-    const int stride = (p + 1) * ndc;
-    for (int b = lo + warp_global(); b < hi; b += warp_count()) {
-        const int pb = parent[b];
-        if (ec.npts(pb) <= 0) continue;
-        const double2 c1 = centers[pb], c2 = centers[b];
-        const double2 z0 = make_double2(c2.x - c1.x, c2.y - c1.y);
-        const double2 w1 = make_double2(z0.x / r1, z0.y / r1);
-        const double2 w2 = cinv(make_double2(z0.x / r2, z0.y / r2));
-        const double2 pw1 = warp_powers(w1);
-        for (int jb = 0; jb <= p; jb += 32) {
-            const int j = jb + lane;
-            const double2 wj = chunk_power(pw1, w1, jb);
-            if (j <= p)
-#pragma unroll
-                for (int q = 0; q < CH; q++)
-                    jt[j * CH + q] = cmul(loc[(size_t)pb * stride + (size_t)j * ndc + c0 + q], wj);
-        }
-        __syncwarp();
-        const double2 pw2 = warp_powers(w2);
-        for (int kb = 0; kb <= p; kb += 32) {
-            const int i = kb + lane;
-            const double2 wi = chunk_power(pw2, w2, kb);
-            if (i <= p) {
-#pragma unroll
-                for (int q = 0; q < CH; q++) {
-                    double2 t = make_double2(0.0, 0.0);
-                    for (int j = i; j <= p; j++) {
-                        const double cb_ = bsh[(size_t)j * (p + 1) + i];
-                        t.x = fma(cb_, jt[j * CH + q].x, t.x);
-                        t.y = fma(cb_, jt[j * CH + q].y, t.y);
-                    }
-                    double2 &o = loc[(size_t)b * stride + (size_t)i * ndc + c0 + q];
-                    o = cadd(o, cmul(t, wi));
-                }
-            }
-        }
-        __syncwarp();
     }
 }
 
@@ -2141,12 +1879,6 @@ void cauchy_fmm(const Tree &T, const CauchyProblem &P0, cudaStream_t s) {
                                               loc32.get(), s); },
               [&](int c0) { downward_chunk<1>(T, P, c0, binom, mp.get(), loc.get(), mp32.get(),
                                               loc32.get(), s); });
-}
-
-void cauchy_direct(const CauchyProblem &P, int ns, PointSet set,
-                   cudaStream_t s) {
-    (void)P; (void)ns; (void)set; (void)s;
-    throw FmmError(4, "cauchy_direct: not implemented");
 }
 
 }  // namespace fmm2d

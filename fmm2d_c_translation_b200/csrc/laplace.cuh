@@ -93,11 +93,6 @@ __device__ __forceinline__ float4 split_pos(double2 p) {
 }
 void cauchy_fmm(const Tree &T, const CauchyProblem &P, cudaStream_t s);
 
-// Direct sums over all sources for every point of `set` (the reference's
-// c2d_direct* kernels, src/laplace/cauchykernels2d.f).
-void cauchy_direct(const CauchyProblem &P, int ns, PointSet set,
-                   cudaStream_t s);
-
 // M2L over list 2 on the FP64 tensor cores for all channels and levels
 // (m2l.cu); false when the tree does not fit its tiling (the caller then
 // uses the per-box kernel).

@@ -878,6 +878,9 @@ int fmm2d_b200_last_profile(char *buf, int len);
 unsigned long long fmm2d_b200_launch_count(void);
 double fmm2d_b200_fp64_peak_tflops(void);
 double fmm2d_b200_fp32_peak_tflops(void);
+/* Dense tcgen05.mma kind::tf32 rate (128 x 256 x 8 MMAs, FP32
+ * accumulation, one CTA per SM), TFLOP/s; 0 on failure. */
+double fmm2d_b200_tf32_peak_tflops(void);
 
 #ifdef __cplusplus
 }

@@ -42,8 +42,14 @@ def inputs(ns=1000, nt=1001, seed=7):
 
 @pytest.fixture(scope="module")
 def glib():
+    """The library in its all-FP64 mode: these are parity tests against the
+    reference's FP64 FMM (the mixed mode is tested in
+    test_helmholtz_mixed_gpu.py)."""
     import fmm2d_c_translation_b200 as fm
-    return fm.lib()
+    L = fm.lib()
+    L.fmm2d_b200_set_precision(1)
+    yield L
+    L.fmm2d_b200_set_precision(0)
 
 
 def h_direct(lib, zk, src, q, d, v, trg, pgh, ifc, ifd, nd=1):
@@ -251,7 +257,8 @@ def test_hfmm2d_zk200_against_reference(glib):
     charges and dipoles N(0,1), unit dipole vectors) at 2e5 sources against
     the reference's C translation on the same inputs.  The tree is the
     reference's (bit-exact), so the expansion orders -- up to p = 94 on
-    level 1 here -- are the same and both sides differ only by round-off."""
+    level 1 here -- are the same and both sides differ only by round-off
+    (all-FP64 mode)."""
     if not refimpl.have_ref():
         pytest.skip("reference build absent")
     rng = np.random.default_rng(200)
