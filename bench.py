@@ -242,6 +242,23 @@ def run_reference(args):
     times = [step() for _ in range(args.steps)]
     tm = sum(times) / len(times)
     value = threads * (ns + nt) / tm
+    full = None
+    if args.reference_full:
+        # one call of the full workload (sequential: the C translation has no
+        # threads), timed once; minutes of host time, hence off by default
+        src, trg, q, d, v = make_inputs(args.ns, args.nt, 7)
+        outs = [np.zeros(args.ns, complex), np.zeros((args.ns, 2), complex),
+                np.zeros(args.nt, complex), np.zeros((args.nt, 2), complex)]
+        ierf = ctypes.c_int(0)
+        t0 = time.perf_counter()
+        R.lfmm2d_st_cd_g_(ctypes.byref(eps), ctypes.byref(ctypes.c_int(args.ns)),
+                          src.ctypes.data_as(P), q.ctypes.data_as(P), d.ctypes.data_as(P),
+                          v.ctypes.data_as(P), outs[0].ctypes.data_as(P), outs[1].ctypes.data_as(P),
+                          ctypes.byref(ctypes.c_int(args.nt)), trg.ctypes.data_as(P),
+                          outs[2].ctypes.data_as(P), outs[3].ctypes.data_as(P), ctypes.byref(ierf))
+        tf = time.perf_counter() - t0
+        full = {"seconds": tf, "points_s": (args.ns + args.nt) / tf, "cores": 1, "ier": ierf.value,
+                "call": f"lfmm2d_st_cd_g_ {args.ns}+{args.nt} points eps={args.eps:g}, one call"}
     sample = (f"{threads} concurrent lfmm2d_st_cd_g calls of {ns}+{nt} points "
               f"(same distributions, eps={args.eps:g}) per step")
     line = {
@@ -252,7 +269,8 @@ def run_reference(args):
         "config": {"workload": "lfmm2d_st_cd_g uniform 1e7+1e7 eps 1e-6 (bounded CPU sample)",
                    "precision": "fp64", "sample": sample},
         "cpu_baseline": {"value": value, "unit": "points/s", "cores": threads,
-                         "kind": "reference", "sample": sample},
+                         "kind": "reference", "sample": sample, "full_size_once": full,
+                         "openmp_fortran": openmp_fortran_probe()},
         "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -296,7 +314,18 @@ def cpu_baseline_sample(args):
     sample = (f"{threads} concurrent reference lfmm2d_st_cd_g calls of "
               f"{ns}+{nt} points, eps={args.eps:g}, {dt:.1f} s wall")
     return {"value": threads * (ns + nt) / dt, "unit": "points/s",
-            "cores": threads, "kind": "reference", "sample": sample}
+            "cores": threads, "kind": "reference", "sample": sample,
+            "openmp_fortran": openmp_fortran_probe()}
+
+
+def openmp_fortran_probe():
+    """The reference's preferred CPU baseline is its OpenMP Fortran library,
+    which needs gfortran on the host: report whether this host has one."""
+    import shutil
+    fc = shutil.which("gfortran")
+    return ("gfortran found at " + fc + " (the Fortran library is not built by this bench)"
+            if fc else "gfortran absent on this host: the reference's OpenMP Fortran path "
+                       "cannot be built; the C translation (sequential per call) is timed")
 
 
 def main():
@@ -315,6 +344,9 @@ def main():
     ap.add_argument("--eps", type=float, default=1e-6)
     ap.add_argument("--cpu-sample", type=int, default=100_000)
     ap.add_argument("--cpu-threads", type=int, default=0)
+    ap.add_argument("--reference-full", action="store_true",
+                    help="with --impl reference: also time one call of the full workload "
+                         "(minutes on one core)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",
@@ -557,6 +589,21 @@ def main():
         roof["peak_file"] = peak_kind
         roof["phase_ms"] = {k: round(v_, 4) for k, v_ in times.items()}
         roof["counts"] = counts
+    # second entry: the M2L phase against the tensor pipe (mixed mode: the
+    # tcgen05 kind::tf32 rate / 3, since a TF32x3 product issues three MMAs)
+    roof_m2l = None
+    if mixed and times.get("m2l"):
+        tf32 = measure_tf32_peak(L)
+        f_m2l = 8.0 * counts.get("m2l_pairs", 0) * (pterm + 1) ** 2 * ndc
+        ach = f_m2l / (times["m2l"] * 1e-3) / 1e12
+        roof_m2l = {"kernel": "m2l (phase: windowed tcgen05 TF32x3 + slot tables + FP32 rows)",
+                    "bound": "tensor", "achieved": ach,
+                    "peak": tf32 / 3.0 if tf32 else None, "unit": "TFLOP/s",
+                    "frac": ach / (tf32 / 3.0) if tf32 else None,
+                    "tf32_peak_tflops": tf32,
+                    "peak_source": "tcgen05 kind::tf32 microbenchmark on this GPU "
+                                   "(fmm2d_b200_tf32_peak_tflops), divided by 3",
+                    "flops_per_launch": f_m2l}
 
     configs = None
     if not args.no_configs and ws == 1:
@@ -584,7 +631,7 @@ def main():
                    "precision": args.precision, "ns": ns, "nt": nt,
                    "eps": args.eps, "parallelism": f"replicas{ws}",
                    "l2": "inputs 0.8 GB > L2; no flush"},
-        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+        "roofline": roof, "roofline_m2l": roof_m2l, "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": nlaunch, "clocks": clk, "fp64_plain": fp64,
         "accuracy": acc, "serving": serving, "configs": configs, "autotune": tuned,
     }
@@ -703,7 +750,8 @@ def measure_configs(fm, L, args):
       c3 lfmm2d_st_d_p on the starfish r = 1 + 0.3 cos 5t: 4e6 sources with
          outward normals as dipole vectors and real N(0,1) dipole strengths,
          4e6 targets at normal distance 10^U[-3,-1], eps 1e-9 (FP64);
-      c4 hfmm2d_s_cd_p, 2e6 uniform sources, zk = 200, eps 1e-6 (FP64)."""
+      c4 hfmm2d_s_cd_p, 2e6 uniform sources, zk = 200, eps 1e-6 (mixed: M2L as
+         TF32x3 contractions on the tensor cores; also timed all-FP64)."""
     import torch
     dev = torch.device("cuda", torch.cuda.current_device())
     stream = torch.cuda.current_stream()
@@ -848,6 +896,9 @@ def measure_configs(fm, L, args):
                              ptr(d_q), ptr(d_d), ptr(d_v), ptr(d_pot), ctypes.byref(ier))
             check()
 
+        L.fmm2d_b200_set_precision(1)
+        ms64, prof64 = timed(c4)
+        L.fmm2d_b200_set_precision(0)
         ms, prof = timed(c4)
         m = 1000
         sub = T(src[:m])
@@ -856,17 +907,41 @@ def measure_configs(fm, L, args):
                                 ptr(d_v), m, ptr(sub), 1, ptr(pot), None, None,
                                 ctypes.c_double(1e-150))
         torch.cuda.synchronize()
-        out["c4"] = {"workload": "hfmm2d_s_cd_p uniform 2e6 zk 200 eps 1e-6 (FP64)", "ms": ms,
-                     "points_s": n4 / (ms * 1e-3),
+        h_ms = prof.get("h_m2l", 0.0)
+        tf32 = measure_tf32_peak(L)
+        m2l_ach = prof.get("#h_m2l_flops", 0.0) / (h_ms * 1e-3) / 1e12 if h_ms else None
+        out["c4"] = {"workload": "hfmm2d_s_cd_p uniform 2e6 zk 200 eps 1e-6 "
+                                 "(auto: mixed, TF32x3 tensor-core M2L on levels of order <= 23)",
+                     "ms": ms, "points_s": n4 / (ms * 1e-3),
                      "phase_ms": {k: round(v, 3) for k, v in prof.items() if not k.startswith("#")},
+                     "counts": {k[1:]: v for k, v in prof.items() if k.startswith("#")},
                      "pot_rel_l2": rel(d_pot.view(-1, 2)[:m], pot.view(-1, 2)),
-                     "accuracy_sample": f"{m} sources vs GPU FP64 direct sum"}
+                     "accuracy_sample": f"{m} sources vs GPU FP64 direct sum",
+                     "m2l_roofline": {
+                         "bound": "tensor", "unit": "TFLOP/s",
+                         "achieved": m2l_ach,
+                         "peak": tf32 / 3.0 if tf32 else None,
+                         "frac": (m2l_ach / (tf32 / 3.0)) if (m2l_ach and tf32) else None,
+                         "peak_source": "tcgen05 kind::tf32 microbenchmark "
+                                        "(fmm2d_b200_tf32_peak_tflops) / 3: a TF32x3 product "
+                                        "issues three MMAs",
+                         "tf32_peak_tflops": tf32,
+                         "flops": "F_M2L = 8 sum_l list2_pairs_l (2 p_l + 1)^2 nd over the whole "
+                                  "M2L phase (tensor-core and FP64 levels)"},
+                     "fp64": {"ms": ms64, "points_s": n4 / (ms64 * 1e-3),
+                              "phase_ms": {k: round(v, 3) for k, v in prof64.items()
+                                           if not k.startswith("#")}}}
     return out
 
 
 def measure_fp32_peak(L):
     L.fmm2d_b200_fp32_peak_tflops.restype = ctypes.c_double
     return L.fmm2d_b200_fp32_peak_tflops()
+
+
+def measure_tf32_peak(L):
+    L.fmm2d_b200_tf32_peak_tflops.restype = ctypes.c_double
+    return L.fmm2d_b200_tf32_peak_tflops()
 
 
 def measure_fp64_peak(L):

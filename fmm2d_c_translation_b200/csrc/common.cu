@@ -119,6 +119,29 @@ struct ProfState {
 thread_local ProfState g_prof;
 }  // namespace
 
+namespace {
+std::atomic<long long> g_alloc_countdown{0};
+std::atomic<int> g_tc_stall{0};
+std::atomic<unsigned long long> g_tc_wait_ns{2000000000ull};
+}  // namespace
+
+void inject_alloc_failure(long long nth) { g_alloc_countdown.store(nth > 0 ? nth : 0); }
+
+bool injected_alloc_failure() {
+    long long c = g_alloc_countdown.load();
+    while (c > 0) {
+        if (g_alloc_countdown.compare_exchange_weak(c, c - 1)) return c == 1;
+    }
+    return false;
+}
+
+void inject_tc_stall(int on, unsigned long long wait_ns) {
+    g_tc_stall.store(on ? 1 : 0);
+    g_tc_wait_ns.store(on ? wait_ns : 2000000000ull);
+}
+int tc_stall_injected() { return g_tc_stall.load(); }
+unsigned long long tc_wait_limit_ns() { return g_tc_wait_ns.load(); }
+
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 unsigned long long launch_count() { return g_launches.load(); }
 void set_profiling(int on) { g_profiling.store(on); }

@@ -86,6 +86,21 @@ void prof_set_count(const char *name, double value);
 void prof_timeinfo(double *timeinfo);
 
 // ---------------------------------------------------------------------------
+// Host-side fault injection for the failure tests (no GPU fault involved):
+//  * the n-th device allocation from now (n >= 1) fails as if the pool were
+//    out of memory; 0 turns it off;
+//  * the tensor-core kernels' MMA issuers skip their MMAs and commits, and
+//    every bounded wait of those kernels gives up after `wait_ns` instead of
+//    2 s, so their consumers' waits run out and the kernels report the
+//    error status that the host turns into ier = 4.
+// ---------------------------------------------------------------------------
+void inject_alloc_failure(long long nth);
+bool injected_alloc_failure();
+void inject_tc_stall(int on, unsigned long long wait_ns);
+int tc_stall_injected();
+unsigned long long tc_wait_limit_ns();
+
+// ---------------------------------------------------------------------------
 // Device buffers: stream-ordered allocations from the device's default pool.
 // The pool keeps freed blocks (release threshold raised at set-up), so a
 // repeated call of the same size allocates nothing from the driver.
@@ -119,7 +134,8 @@ class DevBuf {
         n_ = n;
         if (n) {
             void *q = nullptr;
-            cudaError_t e = cudaMallocAsync(&q, n * sizeof(T), s);
+            cudaError_t e = injected_alloc_failure() ? cudaErrorMemoryAllocation
+                                                     : cudaMallocAsync(&q, n * sizeof(T), s);
             if (e != cudaSuccess) {
                 cudaGetLastError();
                 n_ = 0;

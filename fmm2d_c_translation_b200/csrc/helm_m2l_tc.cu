@@ -72,6 +72,8 @@ struct HtArgs {
     double2 *locl;      // the level's local expansions, [level box][2p + 1][nd]
     double oscale;      // 1 / (scale of Bop)
     int *err;
+    int stall;                 // fault injection: the issuer issues nothing
+    unsigned long long wait_ns;  // limit of every bounded wait
 };
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, uint32_t bytes) {
@@ -161,7 +163,7 @@ __global__ void __launch_bounds__(kHtThreads, 1) helm_m2l_tc_kernel(HtArgs A) {
                     const long long u = step / kHtStages;
                     if (u >= 1 &&
                         !mbar_wait_bounded(HBAR(kHtStages + s), (uint32_t)((u - 1) & 1), abort_flag,
-                                           kHtWaitNs)) {
+                                           A.wait_ns)) {
                         ok = false;
                         break;
                     }
@@ -203,7 +205,7 @@ __global__ void __launch_bounds__(kHtThreads, 1) helm_m2l_tc_kernel(HtArgs A) {
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, tl++) {
             const int a = tl & 1;
             const bool got = mbar_wait_backoff(HBAR(2 * kHtStages + a), (uint32_t)((tl >> 1) & 1),
-                                               abort_flag, kHtWaitNs);
+                                               abort_flag, A.wait_ns);
             if (!__all_sync(0xffffffffu, got)) {
                 ok = false;
                 break;
@@ -244,11 +246,13 @@ __global__ void __launch_bounds__(kHtThreads, 1) helm_m2l_tc_kernel(HtArgs A) {
         long long step = 0;
         int tl = 0;
         bool ok = true, issued = false;
-        for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x, tl++) {
+        // (fault injection: nothing is issued or committed, so the other
+        // roles' bounded waits run out)
+        for (int tile = blockIdx.x; ok && !A.stall && tile < ntiles; tile += gridDim.x, tl++) {
             const int a = tl & 1;
             const bool freed = tl < 2 || mbar_wait_bounded(HBAR(2 * kHtStages + 2 + a),
                                                            (uint32_t)(((tl >> 1) - 1) & 1), abort_flag,
-                                                           kHtWaitNs);
+                                                           A.wait_ns);
             if (!__all_sync(0xffffffffu, freed)) {
                 ok = false;
                 break;
@@ -261,7 +265,7 @@ __global__ void __launch_bounds__(kHtThreads, 1) helm_m2l_tc_kernel(HtArgs A) {
                     const int s = (int)(step % kHtStages);
                     const long long u = step / kHtStages;
                     if (!__all_sync(0xffffffffu, mbar_wait_bounded(HBAR(s), (uint32_t)(u & 1),
-                                                                   abort_flag, kHtWaitNs))) {
+                                                                   abort_flag, A.wait_ns))) {
                         ok = false;
                         break;
                     }
@@ -451,6 +455,8 @@ bool helm_m2l_tc_level(const HtLevel &lv, const SlotPlan &spl, const double2 *mp
     a.locl = loc + lv.off;
     a.oscale = 1.0 / scale;
     a.err = err;
+    a.stall = tc_stall_injected();
+    a.wait_ns = tc_wait_limit_ns();
     switch (KP) {
         case 32: launch_ht<32, 32>(a, ntiles, s); break;
         case 48: launch_ht<48, 48>(a, ntiles, s); break;

@@ -1214,6 +1214,19 @@ __global__ void __launch_bounds__(128) helm_direct_kernel(
     }
 }
 
+// List-2 pairs per level for the roofline (target boxes holding points of
+// a set with outputs, as the M2L plan takes them).
+__global__ void helm_count_m2l_kernel(int nb, const int *__restrict__ lev,
+                                      const int *__restrict__ n2, const int2 *__restrict__ sse,
+                                      const int2 *__restrict__ tse, int sp, int tp,
+                                      unsigned long long *__restrict__ per_level) {
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+        const int np = (sp ? sse[b].y - sse[b].x : 0) + (tp ? tse[b].y - tse[b].x : 0);
+        if (lev[b] >= 2 && np > 0 && n2[b] > 0)
+            atomicAdd(&per_level[lev[b]], (unsigned long long)n2[b]);
+    }
+}
+
 __global__ void helm_leaf_of_kernel(int nb, const int *__restrict__ nchild,
                                     const int2 *__restrict__ se, int *__restrict__ leaf) {
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
@@ -1498,6 +1511,7 @@ void helmholtz_fmm(const Tree &T, const HelmProblem &P, cudaStream_t s) {
     DevBuf<int> tc_err(tc ? 1 : 0, s);
     if (tc) FMM_CUDA(cudaMemsetAsync(tc_err.get(), 0, sizeof(int), s));
     bool tc_used = false;
+    std::vector<char> tc_lev(nl + 1, 0);
     for (int l = 2; l <= nl; l++) {
         if (!hl[l].flag) continue;
         if (tc && hl[l].p <= helm_m2l_tc_max_order()) {
@@ -1513,6 +1527,7 @@ void helmholtz_fmm(const Tree &T, const HelmProblem &P, cudaStream_t s) {
             hv.pw = d_rt.get() + lt[l].m2l_pw;
             if (helm_m2l_tc_level(hv, spl_tc, mp.get(), loc.get(), tc_err.get(), s)) {
                 tc_used = true;
+                tc_lev[l] = 1;
                 continue;
             }
         }
@@ -1575,6 +1590,34 @@ void helmholtz_fmm(const Tree &T, const HelmProblem &P, cudaStream_t s) {
         FMM_CHECK_LAUNCH();
     }
     prof_mark("h_m2l", s);
+    if (profiling_enabled()) {
+        // F_M2L = 8 sum_l pairs_l (2 p_l + 1)^2 nd, and the part on the tensor cores
+        DevBuf<unsigned long long> cnt(nl + 1, s);
+        cnt.zero(s);
+        helm_count_m2l_kernel<<<kNumSM * 2, 256, 0, s>>>(nb, T.level.get(), T.nlist2.get(),
+                                                         T.srcse.get(), T.trgse.get(), sp, tp,
+                                                         cnt.get());
+        FMM_CHECK_LAUNCH();
+        std::vector<unsigned long long> h(nl + 1);
+        FMM_CUDA(cudaMemcpyAsync(h.data(), cnt.get(), h.size() * sizeof(unsigned long long),
+                                 cudaMemcpyDeviceToHost, s));
+        FMM_CUDA(cudaStreamSynchronize(s));
+        double f = 0.0, ftc = 0.0, pairs = 0.0;
+        for (int l = 2; l <= nl; l++) {
+            if (!hl[l].flag) continue;
+            const double w = 2.0 * hl[l].p + 1.0, fl = 8.0 * (double)h[l] * w * w * nd;
+            f += fl;
+            pairs += (double)h[l];
+            if (tc_lev[l]) ftc += fl;
+        }
+        prof_set_count("h_m2l_pairs", pairs);
+        prof_set_count("h_m2l_flops", f);
+        prof_set_count("h_m2l_tc_flops", ftc);
+        prof_set_count("nlevels", (double)nl);
+        prof_set_count("nboxes", (double)nb);
+        // the mark above closed the M2L phase; this sync belongs to no phase
+        prof_mark("h_count", s);
+    }
     if (tc_used && read_scalar(tc_err.get(), s) != 0)
         throw FmmError(4, "tensor-core Helmholtz M2L: a wait for an MMA or operand barrier timed out");
     // ---- L2L, downward (parents at levels 2 .. nl-1) ----

@@ -103,6 +103,8 @@ struct WinArgs {
     const float2 *mp32;
     double2 *loc;
     int *err;
+    int stall;                   // fault injection: the issuer issues nothing
+    unsigned long long wait_ns;  // limit of every bounded wait of the roles
 };
 
 __device__ __forceinline__ void split_tf32(float v, float &hi, float &lo) {
@@ -279,8 +281,8 @@ __global__ void __launch_bounds__(kWinThreads, 1) m2l_win_kernel(WinArgs A) {
                 float *Whi = sW + (2 * b) * WSZ, *Wlo = Whi + WSZ;
                 if (g >= 2) {
                     const uint32_t par = (uint32_t)(((g >> 1) - 1) & 1);
-                    if (!mbar_wait_bounded(WBAR(2 + b), par, abort_flag, kWinWaitNs) ||
-                        !mbar_wait_bounded(WBAR(4 + b), par, abort_flag, kWinWaitNs)) {
+                    if (!mbar_wait_bounded(WBAR(2 + b), par, abort_flag, A.wait_ns) ||
+                        !mbar_wait_bounded(WBAR(4 + b), par, abort_flag, A.wait_ns)) {
                         ok = false;
                         break;
                     }
@@ -291,7 +293,7 @@ __global__ void __launch_bounds__(kWinThreads, 1) m2l_win_kernel(WinArgs A) {
                 for (int j = 0; j < 3; j++, u++) {
                     const int ob = u & 1;
                     if (u >= 2 && !mbar_wait_bounded(WBAR(8 + ob), (uint32_t)(((u >> 1) - 1) & 1),
-                                                     abort_flag, kWinWaitNs)) {
+                                                     abort_flag, A.wait_ns)) {
                         ok = false;
                         break;
                     }
@@ -326,7 +328,7 @@ __global__ void __launch_bounds__(kWinThreads, 1) m2l_win_kernel(WinArgs A) {
             for (int c = 0; c < 4; c++) l0[c] = s0[c] = make_float2(0.f, 0.f);
             for (int s = 0; ok && s < 12; s++, g++) {
                 const int b = g & 1;
-                if (!mbar_wait_bounded(WBAR(0 + b), (uint32_t)((g >> 1) & 1), abort_flag, kWinWaitNs)) {
+                if (!mbar_wait_bounded(WBAR(0 + b), (uint32_t)((g >> 1) & 1), abort_flag, A.wait_ns)) {
                     ok = false;
                     break;
                 }
@@ -383,7 +385,7 @@ __global__ void __launch_bounds__(kWinThreads, 1) m2l_win_kernel(WinArgs A) {
             const int b = kr & 1;
             // (tcgen05.ld is warp-collective: the warp decides as one)
             const bool got =
-                mbar_wait_backoff(WBAR(10 + b), (uint32_t)((kr >> 1) & 1), abort_flag, kWinWaitNs);
+                mbar_wait_backoff(WBAR(10 + b), (uint32_t)((kr >> 1) & 1), abort_flag, A.wait_ns);
             if (!__all_sync(0xffffffffu, got)) {
                 ok = false;
                 break;
@@ -422,10 +424,12 @@ __global__ void __launch_bounds__(kWinThreads, 1) m2l_win_kernel(WinArgs A) {
         // ------------------------------------------------------------ issuer
         int g = 0, u = 0, kr = 0;
         bool ok = true, issued = false;
-        for (int run = blockIdx.x; ok && run < A.nrun; run += gridDim.x, kr++) {
+        // (fault injection: nothing is issued or committed, so the other
+        // roles' bounded waits run out)
+        for (int run = blockIdx.x; ok && !A.stall && run < A.nrun; run += gridDim.x, kr++) {
             const int b = kr & 1;
             const bool freed = kr < 2 || mbar_wait_bounded(WBAR(12 + b), (uint32_t)(((kr >> 1) - 1) & 1),
-                                                           abort_flag, kWinWaitNs);
+                                                           abort_flag, A.wait_ns);
             if (!__all_sync(0xffffffffu, freed)) {
                 ok = false;
                 break;
@@ -436,7 +440,7 @@ __global__ void __launch_bounds__(kWinThreads, 1) m2l_win_kernel(WinArgs A) {
             for (int s = 0; ok && s < 12; s++, g++) {
                 const int wb = g & 1;
                 if (!__all_sync(0xffffffffu, mbar_wait_bounded(WBAR(0 + wb), (uint32_t)((g >> 1) & 1),
-                                                               abort_flag, kWinWaitNs))) {
+                                                               abort_flag, A.wait_ns))) {
                     ok = false;
                     break;
                 }
@@ -444,7 +448,7 @@ __global__ void __launch_bounds__(kWinThreads, 1) m2l_win_kernel(WinArgs A) {
                 for (int j = 0; j < 3; j++, u++) {
                     const int ob = u & 1;
                     if (!__all_sync(0xffffffffu, mbar_wait_bounded(WBAR(6 + ob), (uint32_t)((u >> 1) & 1),
-                                                                   abort_flag, kWinWaitNs))) {
+                                                                   abort_flag, A.wait_ns))) {
                         ok = false;
                         break;
                     }
@@ -919,6 +923,8 @@ void launch_win(const WinPlan &W, const WinTables &tb, const Tree &T, const Cauc
         a.mp32 = mp32;
         a.loc = loc;
         a.err = err;
+        a.stall = tc_stall_injected();
+        a.wait_ns = tc_wait_limit_ns();
         const int grid = std::max(1, std::min(r.second, kNumSM));
         kern<<<grid, kWinThreads, sm, s>>>(a);
         FMM_CHECK_LAUNCH();

@@ -107,6 +107,37 @@ FMM_EXPORT int fmm2d_b200_last_profile(char *buf, int len) {
     return (int)m.size();
 }
 
+// Failure injection for the failure tests (host side only; no GPU fault):
+// the nth device allocation from now fails as out of memory (0: off).
+FMM_EXPORT int fmm2d_b200_inject_alloc_failure(long long nth) {
+    inject_alloc_failure(nth);
+    return 0;
+}
+
+// Failure injection: the tensor-core M2L kernels issue no MMAs and their
+// bounded waits give up after wait_ms (on = 0 restores the normal 2 s limit),
+// so the evaluation returns ier = 4.
+FMM_EXPORT int fmm2d_b200_inject_tc_stall(int on, double wait_ms) {
+    const double ns = wait_ms > 0 ? wait_ms * 1e6 : 1e6;
+    inject_tc_stall(on, (unsigned long long)ns);
+    return 0;
+}
+
+// Bytes of the current device's memory pool held by live allocations of
+// this process (cudaMemPoolAttrUsedMemCurrent): the same before and after a
+// call, failed or not, when the call released everything it allocated.
+FMM_EXPORT int fmm2d_b200_device_bytes_in_use(unsigned long long *bytes) {
+    return guarded([&] {
+        int dev;
+        FMM_CUDA(cudaGetDevice(&dev));
+        cudaMemPool_t pool;
+        FMM_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+        uint64_t v = 0;
+        FMM_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &v));
+        *bytes = (unsigned long long)v;
+    });
+}
+
 // Returns cached device workspace of the current device to the driver.
 FMM_EXPORT int fmm2d_b200_release_memory(void) {
     return guarded([&] {

@@ -872,6 +872,19 @@ int fmm2d_b200_tree_lists(void *handle, int *nlist1, int *list1,
                           int *nlist4, int *list4);
 void fmm2d_b200_tree_free(void *handle);
 
+/* Failure injection for tests (no counterpart in the reference; host side
+ * only, no GPU fault).  inject_alloc_failure: the nth device allocation from
+ * now fails as out of memory, so the call returns ier = 4 (the reference's
+ * allocation-failure code, src/helmholtz/hfmm2d.f:374-381); 0 turns it off.
+ * inject_tc_stall: the tensor-core M2L kernels issue no MMAs and their
+ * bounded waits give up after wait_ms, so a mixed-mode call returns ier = 4;
+ * on = 0 restores the normal limit.  device_bytes_in_use: bytes of the
+ * device's memory pool held by live allocations (to check that a failed
+ * call released its workspace). */
+int fmm2d_b200_inject_alloc_failure(long long nth);
+int fmm2d_b200_inject_tc_stall(int on, double wait_ms);
+int fmm2d_b200_device_bytes_in_use(unsigned long long *bytes);
+
 /* Measurement helpers. */
 int fmm2d_b200_set_profiling(int on);
 int fmm2d_b200_last_profile(char *buf, int len);
