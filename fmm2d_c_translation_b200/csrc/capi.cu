@@ -6,9 +6,11 @@
 //   lfmm2d_{s,t,st}_{c,d,cd}_{p,g,h}_   src/laplace/lfmm2dwrap.f:31-1704
 //   cfmm2d_{s,t,st}_{c,d,cd}_{p,g,h}_   src/laplace/cfmm2dwrap.f:31-1659
 //   hfmm2d_{s,t,st}_{c,d,cd}_{p,g,h}_   src/helmholtz/hfmm2dwrap.f:41-1871
-//   lfmm2d_ / cfmm2d_ / hfmm2d_         guru drivers (lfmm2d.f:29, cfmm2d.f:23,
-//                                       hfmm2d.f:19)
-//   lfmm2d_ndiv_ / cfmm2d_ndiv_ / hfmm2d_ndiv_   MATLAB-path drivers
+//   rfmm2d_{s,t,st}_{c,d,cd}_{p,g,h}_   src/laplace/rfmm2dwrap.f:36-1709
+//   {l,c,h,r}fmm2d_*_vec_               the *wrap_vec.f files (leading nd)
+//   lfmm2d_ / cfmm2d_ / hfmm2d_ / rfmm2d_   guru drivers (lfmm2d.f:29,
+//                                       cfmm2d.f:23, hfmm2d.f:19, rfmm2d.f:27)
+//   {l,c,h,r}fmm2d_ndiv_                MATLAB-path drivers
 //   hfmm2d_s_c_p                        src/helmholtz_c.f03:5-15
 //
 // Each wrapper fixes ifcharge / ifdipole / ifpgh / ifpghtarg with nd = 1,
@@ -43,12 +45,13 @@ FmmCall base_call(Kernel k, const double *eps, const double *zk, const fint *ns,
     return c;
 }
 
-void wrap(Kernel k, const double *eps, const double *zk, const fint *ns,
+void wrap(Kernel k, int nd, const double *eps, const double *zk, const fint *ns,
           const double *src, const double *chg, const double *dip,
           const double *dv, int ifc, int ifd, int pgh, double *pot,
           double *grad, double *hess, int nt, const double *targ, int pght,
           double *pt, double *gt, double *ht, fint *ier) {
     FmmCall c = base_call(k, eps, zk, ns, src);
+    c.nd = nd;
     c.ifcharge = ifc;
     c.charge = chg;
     c.ifdipole = ifd;
@@ -69,21 +72,23 @@ void wrap(Kernel k, const double *eps, const double *zk, const fint *ns,
 
 }  // namespace
 
-typedef double cplx_t;  // complex*16 arrays are passed as interleaved doubles
+// Complex*16 arrays are passed as interleaved doubles, real*8 arrays as
+// doubles: every array argument is a double pointer in the C ABI.
+typedef double arr_t;
 
 // source-strength argument lists: c = charge, d = dipole, cd = both
-#define SRC_c(V) const cplx_t *charge
-#define SRC_d(V) const cplx_t *dipstr V(const double *dipvec)
-#define SRC_cd(V) const cplx_t *charge, const cplx_t *dipstr V(const double *dipvec)
+#define SRC_c(V) const arr_t *charge
+#define SRC_d(V) const arr_t *dipstr V(const double *dipvec)
+#define SRC_cd(V) const arr_t *charge, const arr_t *dipstr V(const double *dipvec)
 #define PASS_c charge, nullptr, nullptr, 1, 0
 #define PASS_d nullptr, dipstr, DV(dipvec), 0, 1
 #define PASS_cd charge, dipstr, DV(dipvec), 1, 1
-#define OUT_S_p cplx_t *pot
-#define OUT_S_g cplx_t *pot, cplx_t *grad
-#define OUT_S_h cplx_t *pot, cplx_t *grad, cplx_t *hess
-#define OUT_T_p cplx_t *pottarg
-#define OUT_T_g cplx_t *pottarg, cplx_t *gradtarg
-#define OUT_T_h cplx_t *pottarg, cplx_t *gradtarg, cplx_t *hesstarg
+#define OUT_S_p arr_t *pot
+#define OUT_S_g arr_t *pot, arr_t *grad
+#define OUT_S_h arr_t *pot, arr_t *grad, arr_t *hess
+#define OUT_T_p arr_t *pottarg
+#define OUT_T_g arr_t *pottarg, arr_t *gradtarg
+#define OUT_T_h arr_t *pottarg, arr_t *gradtarg, arr_t *hesstarg
 #define PS_p 1, pot, nullptr, nullptr
 #define PS_g 2, pot, grad, nullptr
 #define PS_h 3, pot, grad, hess
@@ -92,88 +97,68 @@ typedef double cplx_t;  // complex*16 arrays are passed as interleaved doubles
 #define PT_h 3, pottarg, gradtarg, hesstarg
 #define WITH_DV(x) , x
 #define NO_DV(x)
+#define ND_ARG() const fint *nd,
+#define ZK_ARG() const arr_t *zk,
+#define NONE()
+
+// The three wrappers (sources only, targets only, both) of one strength
+// kind K and output level P of a family: NAME prefix, SUF "_" or "_vec_",
+// kernel KERN, NDP/NDA the nd argument (the _vec forms) or nd = 1, ZKP/ZKA
+// the wavenumber argument (Helmholtz), DVM whether dipoles carry dipvec.
+#define WRAP3(NAME, SUF, KERN, NDP, NDA, ZKP, ZKA, DVM, K, P)                        \
+    FMM_EXPORT void NAME##_s_##K##_##P##SUF(NDP() const double *eps, ZKP() const fint *ns, \
+                                            const double *sources, SRC_##K(DVM),       \
+                                            OUT_S_##P, fint *ier) {                    \
+        wrap(KERN, NDA, eps, ZKA, ns, sources, PASS_##K, PS_##P, 0, nullptr, 0,      \
+             nullptr, nullptr, nullptr, ier);                                        \
+    }                                                                                \
+    FMM_EXPORT void NAME##_t_##K##_##P##SUF(                                         \
+        NDP() const double *eps, ZKP() const fint *ns, const double *sources,        \
+        SRC_##K(DVM), const fint *nt, const double *targ, OUT_T_##P, fint *ier) {    \
+        wrap(KERN, NDA, eps, ZKA, ns, sources, PASS_##K, 0, nullptr, nullptr,        \
+             nullptr, *nt, targ, PT_##P, ier);                                       \
+    }                                                                                \
+    FMM_EXPORT void NAME##_st_##K##_##P##SUF(                                        \
+        NDP() const double *eps, ZKP() const fint *ns, const double *sources,        \
+        SRC_##K(DVM), OUT_S_##P, const fint *nt, const double *targ, OUT_T_##P,      \
+        fint *ier) {                                                                 \
+        wrap(KERN, NDA, eps, ZKA, ns, sources, PASS_##K, PS_##P, *nt, targ, PT_##P,  \
+             ier);                                                                   \
+    }
+
+// All 27 (strength kind x output level) of a family.
+#define WRAP27(NAME, SUF, KERN, NDP, NDA, ZKP, ZKA, DVM)                \
+    WRAP3(NAME, SUF, KERN, NDP, NDA, ZKP, ZKA, DVM, c, p)               \
+    WRAP3(NAME, SUF, KERN, NDP, NDA, ZKP, ZKA, DVM, c, g)               \
+    WRAP3(NAME, SUF, KERN, NDP, NDA, ZKP, ZKA, DVM, c, h)               \
+    WRAP3(NAME, SUF, KERN, NDP, NDA, ZKP, ZKA, DVM, d, p)               \
+    WRAP3(NAME, SUF, KERN, NDP, NDA, ZKP, ZKA, DVM, d, g)               \
+    WRAP3(NAME, SUF, KERN, NDP, NDA, ZKP, ZKA, DVM, d, h)               \
+    WRAP3(NAME, SUF, KERN, NDP, NDA, ZKP, ZKA, DVM, cd, p)              \
+    WRAP3(NAME, SUF, KERN, NDP, NDA, ZKP, ZKA, DVM, cd, g)              \
+    WRAP3(NAME, SUF, KERN, NDP, NDA, ZKP, ZKA, DVM, cd, h)
 
 #define DV(x) x
-#define LWRAP(K, P)                                                           \
-    FMM_EXPORT void lfmm2d_s_##K##_##P##_(const double *eps, const fint *ns,  \
-                                          const double *sources,              \
-                                          SRC_##K(WITH_DV), OUT_S_##P,        \
-                                          fint *ier) {                        \
-        wrap(kLaplace, eps, nullptr, ns, sources, PASS_##K, PS_##P, 0,        \
-             nullptr, 0, nullptr, nullptr, nullptr, ier);                     \
-    }                                                                         \
-    FMM_EXPORT void lfmm2d_t_##K##_##P##_(                                    \
-        const double *eps, const fint *ns, const double *sources,             \
-        SRC_##K(WITH_DV), const fint *nt, const double *targ, OUT_T_##P,      \
-        fint *ier) {                                                          \
-        wrap(kLaplace, eps, nullptr, ns, sources, PASS_##K, 0, nullptr,       \
-             nullptr, nullptr, *nt, targ, PT_##P, ier);                       \
-    }                                                                         \
-    FMM_EXPORT void lfmm2d_st_##K##_##P##_(                                   \
-        const double *eps, const fint *ns, const double *sources,             \
-        SRC_##K(WITH_DV), OUT_S_##P, const fint *nt, const double *targ,      \
-        OUT_T_##P, fint *ier) {                                               \
-        wrap(kLaplace, eps, nullptr, ns, sources, PASS_##K, PS_##P, *nt,      \
-             targ, PT_##P, ier);                                              \
-    }
-
-#define HWRAP(K, P)                                                           \
-    FMM_EXPORT void hfmm2d_s_##K##_##P##_(                                    \
-        const double *eps, const cplx_t *zk, const fint *ns,                  \
-        const double *sources, SRC_##K(WITH_DV), OUT_S_##P, fint *ier) {      \
-        wrap(kHelmholtz, eps, zk, ns, sources, PASS_##K, PS_##P, 0, nullptr,  \
-             0, nullptr, nullptr, nullptr, ier);                              \
-    }                                                                         \
-    FMM_EXPORT void hfmm2d_t_##K##_##P##_(                                    \
-        const double *eps, const cplx_t *zk, const fint *ns,                  \
-        const double *sources, SRC_##K(WITH_DV), const fint *nt,              \
-        const double *targ, OUT_T_##P, fint *ier) {                           \
-        wrap(kHelmholtz, eps, zk, ns, sources, PASS_##K, 0, nullptr, nullptr, \
-             nullptr, *nt, targ, PT_##P, ier);                                \
-    }                                                                         \
-    FMM_EXPORT void hfmm2d_st_##K##_##P##_(                                   \
-        const double *eps, const cplx_t *zk, const fint *ns,                  \
-        const double *sources, SRC_##K(WITH_DV), OUT_S_##P, const fint *nt,   \
-        const double *targ, OUT_T_##P, fint *ier) {                           \
-        wrap(kHelmholtz, eps, zk, ns, sources, PASS_##K, PS_##P, *nt, targ,   \
-             PT_##P, ier);                                                    \
-    }
-
-LWRAP(c, p) LWRAP(c, g) LWRAP(c, h)
-LWRAP(d, p) LWRAP(d, g) LWRAP(d, h)
-LWRAP(cd, p) LWRAP(cd, g) LWRAP(cd, h)
-HWRAP(c, p) HWRAP(c, g) HWRAP(c, h)
-HWRAP(d, p) HWRAP(d, g) HWRAP(d, h)
-HWRAP(cd, p) HWRAP(cd, g) HWRAP(cd, h)
+// lfmm2d_*_ (src/laplace/lfmm2dwrap.f:31-1704), lfmm2d_*_vec_
+// (src/laplace/lfmm2dwrap_vec.f:31-1685)
+WRAP27(lfmm2d, _, kLaplace, NONE, 1, NONE, nullptr, WITH_DV)
+WRAP27(lfmm2d, _vec_, kLaplace, ND_ARG, *nd, NONE, nullptr, WITH_DV)
+// rfmm2d_*_ (src/laplace/rfmm2dwrap.f:36-1709), rfmm2d_*_vec_
+// (src/laplace/rfmm2dwrap_vec.f:36-1690): real charges, dipole strengths
+// and outputs
+WRAP27(rfmm2d, _, kReal, NONE, 1, NONE, nullptr, WITH_DV)
+WRAP27(rfmm2d, _vec_, kReal, ND_ARG, *nd, NONE, nullptr, WITH_DV)
+// hfmm2d_*_ (src/helmholtz/hfmm2dwrap.f:41-1871), hfmm2d_*_vec_
+// (src/helmholtz/hfmm2dwrap_vec.f:6-1790)
+WRAP27(hfmm2d, _, kHelmholtz, NONE, 1, ZK_ARG, zk, WITH_DV)
+WRAP27(hfmm2d, _vec_, kHelmholtz, ND_ARG, *nd, ZK_ARG, zk, WITH_DV)
 #undef DV
 
 #define DV(x) nullptr
-#define CWRAP(K, P)                                                           \
-    FMM_EXPORT void cfmm2d_s_##K##_##P##_(const double *eps, const fint *ns,  \
-                                          const double *sources,              \
-                                          SRC_##K(NO_DV), OUT_S_##P,          \
-                                          fint *ier) {                        \
-        wrap(kCauchy, eps, nullptr, ns, sources, PASS_##K, PS_##P, 0,         \
-             nullptr, 0, nullptr, nullptr, nullptr, ier);                     \
-    }                                                                         \
-    FMM_EXPORT void cfmm2d_t_##K##_##P##_(                                    \
-        const double *eps, const fint *ns, const double *sources,             \
-        SRC_##K(NO_DV), const fint *nt, const double *targ, OUT_T_##P,        \
-        fint *ier) {                                                          \
-        wrap(kCauchy, eps, nullptr, ns, sources, PASS_##K, 0, nullptr,        \
-             nullptr, nullptr, *nt, targ, PT_##P, ier);                       \
-    }                                                                         \
-    FMM_EXPORT void cfmm2d_st_##K##_##P##_(                                   \
-        const double *eps, const fint *ns, const double *sources,             \
-        SRC_##K(NO_DV), OUT_S_##P, const fint *nt, const double *targ,        \
-        OUT_T_##P, fint *ier) {                                               \
-        wrap(kCauchy, eps, nullptr, ns, sources, PASS_##K, PS_##P, *nt, targ, \
-             PT_##P, ier);                                                    \
-    }
-
-CWRAP(c, p) CWRAP(c, g) CWRAP(c, h)
-CWRAP(d, p) CWRAP(d, g) CWRAP(d, h)
-CWRAP(cd, p) CWRAP(cd, g) CWRAP(cd, h)
+// cfmm2d_*_ (src/laplace/cfmm2dwrap.f:31-1659), cfmm2d_*_vec_
+// (src/laplace/cfmm2dwrap_vec.f:37-1646): no dipole vectors
+WRAP27(cfmm2d, _, kCauchy, NONE, 1, NONE, nullptr, NO_DV)
+WRAP27(cfmm2d, _vec_, kCauchy, ND_ARG, *nd, NONE, nullptr, NO_DV)
 #undef DV
 
 // ---------------------------------------------------------------------------
@@ -219,12 +204,12 @@ void guru(Kernel k, const fint *nd, const double *eps, const double *zk,
 
 FMM_EXPORT void lfmm2d_(const fint *nd, const double *eps, const fint *ns,
                         const double *sources, const fint *ifcharge,
-                        const cplx_t *charge, const fint *ifdipole,
-                        const cplx_t *dipstr, const double *dipvec, fint *iper,
-                        const fint *ifpgh, cplx_t *pot, cplx_t *grad,
-                        cplx_t *hess, const fint *nt, const double *targ,
-                        const fint *ifpghtarg, cplx_t *pottarg,
-                        cplx_t *gradtarg, cplx_t *hesstarg, fint *ier) {
+                        const arr_t *charge, const fint *ifdipole,
+                        const arr_t *dipstr, const double *dipvec, fint *iper,
+                        const fint *ifpgh, arr_t *pot, arr_t *grad,
+                        arr_t *hess, const fint *nt, const double *targ,
+                        const fint *ifpghtarg, arr_t *pottarg,
+                        arr_t *gradtarg, arr_t *hesstarg, fint *ier) {
     guru(kLaplace, nd, eps, nullptr, ns, sources, ifcharge, charge, ifdipole,
          dipstr, dipvec, iper, ifpgh, pot, grad, hess, nt, targ, ifpghtarg,
          pottarg, gradtarg, hesstarg, nullptr, nullptr, nullptr, nullptr, ier);
@@ -232,25 +217,25 @@ FMM_EXPORT void lfmm2d_(const fint *nd, const double *eps, const fint *ns,
 
 FMM_EXPORT void cfmm2d_(const fint *nd, const double *eps, const fint *ns,
                         const double *sources, const fint *ifcharge,
-                        const cplx_t *charge, const fint *ifdipole,
-                        const cplx_t *dipstr, fint *iper, const fint *ifpgh,
-                        cplx_t *pot, cplx_t *grad, cplx_t *hess, const fint *nt,
+                        const arr_t *charge, const fint *ifdipole,
+                        const arr_t *dipstr, fint *iper, const fint *ifpgh,
+                        arr_t *pot, arr_t *grad, arr_t *hess, const fint *nt,
                         const double *targ, const fint *ifpghtarg,
-                        cplx_t *pottarg, cplx_t *gradtarg, cplx_t *hesstarg,
+                        arr_t *pottarg, arr_t *gradtarg, arr_t *hesstarg,
                         fint *ier) {
     guru(kCauchy, nd, eps, nullptr, ns, sources, ifcharge, charge, ifdipole,
          dipstr, nullptr, iper, ifpgh, pot, grad, hess, nt, targ, ifpghtarg,
          pottarg, gradtarg, hesstarg, nullptr, nullptr, nullptr, nullptr, ier);
 }
 
-FMM_EXPORT void hfmm2d_(const fint *nd, const double *eps, const cplx_t *zk,
+FMM_EXPORT void hfmm2d_(const fint *nd, const double *eps, const arr_t *zk,
                         const fint *ns, const double *sources,
-                        const fint *ifcharge, const cplx_t *charge,
-                        const fint *ifdipole, const cplx_t *dipstr,
+                        const fint *ifcharge, const arr_t *charge,
+                        const fint *ifdipole, const arr_t *dipstr,
                         const double *dipvec, fint *iper, const fint *ifpgh,
-                        cplx_t *pot, cplx_t *grad, cplx_t *hess, const fint *nt,
+                        arr_t *pot, arr_t *grad, arr_t *hess, const fint *nt,
                         const double *targ, const fint *ifpghtarg,
-                        cplx_t *pottarg, cplx_t *gradtarg, cplx_t *hesstarg,
+                        arr_t *pottarg, arr_t *gradtarg, arr_t *hesstarg,
                         fint *ier) {
     guru(kHelmholtz, nd, eps, zk, ns, sources, ifcharge, charge, ifdipole,
          dipstr, dipvec, iper, ifpgh, pot, grad, hess, nt, targ, ifpghtarg,
@@ -259,13 +244,13 @@ FMM_EXPORT void hfmm2d_(const fint *nd, const double *eps, const cplx_t *zk,
 
 FMM_EXPORT void lfmm2d_ndiv_(const fint *nd, const double *eps, const fint *ns,
                              const double *sources, const fint *ifcharge,
-                             const cplx_t *charge, const fint *ifdipole,
-                             const cplx_t *dipstr, const double *dipvec,
-                             fint *iper, const fint *ifpgh, cplx_t *pot,
-                             cplx_t *grad, cplx_t *hess, const fint *nt,
+                             const arr_t *charge, const fint *ifdipole,
+                             const arr_t *dipstr, const double *dipvec,
+                             fint *iper, const fint *ifpgh, arr_t *pot,
+                             arr_t *grad, arr_t *hess, const fint *nt,
                              const double *targ, const fint *ifpghtarg,
-                             cplx_t *pottarg, cplx_t *gradtarg,
-                             cplx_t *hesstarg, const fint *ndiv,
+                             arr_t *pottarg, arr_t *gradtarg,
+                             arr_t *hesstarg, const fint *ndiv,
                              const fint *idivflag, const fint *ifnear,
                              double *timeinfo, fint *ier) {
     guru(kLaplace, nd, eps, nullptr, ns, sources, ifcharge, charge, ifdipole,
@@ -275,12 +260,12 @@ FMM_EXPORT void lfmm2d_ndiv_(const fint *nd, const double *eps, const fint *ns,
 
 FMM_EXPORT void cfmm2d_ndiv_(const fint *nd, const double *eps, const fint *ns,
                              const double *sources, const fint *ifcharge,
-                             const cplx_t *charge, const fint *ifdipole,
-                             const cplx_t *dipstr, fint *iper,
-                             const fint *ifpgh, cplx_t *pot, cplx_t *grad,
-                             cplx_t *hess, const fint *nt, const double *targ,
-                             const fint *ifpghtarg, cplx_t *pottarg,
-                             cplx_t *gradtarg, cplx_t *hesstarg,
+                             const arr_t *charge, const fint *ifdipole,
+                             const arr_t *dipstr, fint *iper,
+                             const fint *ifpgh, arr_t *pot, arr_t *grad,
+                             arr_t *hess, const fint *nt, const double *targ,
+                             const fint *ifpghtarg, arr_t *pottarg,
+                             arr_t *gradtarg, arr_t *hesstarg,
                              const fint *ndiv, const fint *idivflag,
                              const fint *ifnear, double *timeinfo, fint *ier) {
     guru(kCauchy, nd, eps, nullptr, ns, sources, ifcharge, charge, ifdipole,
@@ -289,20 +274,50 @@ FMM_EXPORT void cfmm2d_ndiv_(const fint *nd, const double *eps, const fint *ns,
 }
 
 FMM_EXPORT void hfmm2d_ndiv_(const fint *nd, const double *eps,
-                             const cplx_t *zk, const fint *ns,
+                             const arr_t *zk, const fint *ns,
                              const double *sources, const fint *ifcharge,
-                             const cplx_t *charge, const fint *ifdipole,
-                             const cplx_t *dipstr, const double *dipvec,
-                             fint *iper, const fint *ifpgh, cplx_t *pot,
-                             cplx_t *grad, cplx_t *hess, const fint *nt,
+                             const arr_t *charge, const fint *ifdipole,
+                             const arr_t *dipstr, const double *dipvec,
+                             fint *iper, const fint *ifpgh, arr_t *pot,
+                             arr_t *grad, arr_t *hess, const fint *nt,
                              const double *targ, const fint *ifpghtarg,
-                             cplx_t *pottarg, cplx_t *gradtarg,
-                             cplx_t *hesstarg, const fint *ndiv,
+                             arr_t *pottarg, arr_t *gradtarg,
+                             arr_t *hesstarg, const fint *ndiv,
                              const fint *idivflag, const fint *ifnear,
                              double *timeinfo, fint *ier) {
     guru(kHelmholtz, nd, eps, zk, ns, sources, ifcharge, charge, ifdipole,
          dipstr, dipvec, iper, ifpgh, pot, grad, hess, nt, targ, ifpghtarg,
          pottarg, gradtarg, hesstarg, ndiv, idivflag, ifnear, timeinfo, ier);
+}
+
+// Real-valued Laplace FMM (src/laplace/rfmm2d.f:27; the ndiv form
+// src/laplace/rfmm2d_ndiv.f:27, c_translation/src/rfmm2d_ndiv.c:51): real
+// charge(nd,ns), dipstr(nd,ns), dipvec(nd,2,ns), pot(nd,*), grad(nd,2,*),
+// hess(nd,3,*).
+FMM_EXPORT void rfmm2d_(const fint *nd, const double *eps, const fint *ns,
+                        const double *sources, const fint *ifcharge,
+                        const double *charge, const fint *ifdipole,
+                        const double *dipstr, const double *dipvec, fint *iper,
+                        const fint *ifpgh, double *pot, double *grad, double *hess,
+                        const fint *nt, const double *targ, const fint *ifpghtarg,
+                        double *pottarg, double *gradtarg, double *hesstarg, fint *ier) {
+    guru(kReal, nd, eps, nullptr, ns, sources, ifcharge, charge, ifdipole, dipstr, dipvec,
+         iper, ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg, gradtarg, hesstarg,
+         nullptr, nullptr, nullptr, nullptr, ier);
+}
+
+FMM_EXPORT void rfmm2d_ndiv_(const fint *nd, const double *eps, const fint *ns,
+                             const double *sources, const fint *ifcharge,
+                             const double *charge, const fint *ifdipole,
+                             const double *dipstr, const double *dipvec, fint *iper,
+                             const fint *ifpgh, double *pot, double *grad, double *hess,
+                             const fint *nt, const double *targ, const fint *ifpghtarg,
+                             double *pottarg, double *gradtarg, double *hesstarg,
+                             const fint *ndiv, const fint *idivflag, const fint *ifnear,
+                             double *timeinfo, fint *ier) {
+    guru(kReal, nd, eps, nullptr, ns, sources, ifcharge, charge, ifdipole, dipstr, dipvec,
+         iper, ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg, gradtarg, hesstarg, ndiv,
+         idivflag, ifnear, timeinfo, ier);
 }
 
 // ---------------------------------------------------------------------------
@@ -372,7 +387,7 @@ struct cplx_by_value {
 };
 
 FMM_EXPORT void hfmm2d_s_c_p(double eps, cplx_by_value zk, int64_t ns, const double *sources,
-                             const cplx_t *charge, cplx_t *pot, int64_t *ier) {
+                             const arr_t *charge, arr_t *pot, int64_t *ier) {
     if (ns < 1 || ns > INT32_MAX) {
         set_last_error("ns out of range for the 32-bit drivers");
         *ier = 4;
@@ -381,7 +396,7 @@ FMM_EXPORT void hfmm2d_s_c_p(double eps, cplx_by_value zk, int64_t ns, const dou
     const double zkv[2] = {zk.re, zk.im};
     const fint ns32 = (fint)ns;
     fint ier32 = 0;
-    wrap(kHelmholtz, &eps, zkv, &ns32, sources, charge, nullptr, nullptr, 1, 0, 1, pot, nullptr,
+    wrap(kHelmholtz, 1, &eps, zkv, &ns32, sources, charge, nullptr, nullptr, 1, 0, 1, pot, nullptr,
          nullptr, 0, nullptr, 0, nullptr, nullptr, nullptr, &ier32);
     *ier = ier32;
 }

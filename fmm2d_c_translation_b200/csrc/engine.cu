@@ -54,10 +54,12 @@ struct InBuf {
     }
 };
 
-// Outputs in the caller's layout on the device.
-struct OutBuf {
-    DevBuf<double2> own;
-    double2 *ptr = nullptr;
+// Outputs in the caller's layout on the device (T = double2 for complex
+// outputs, double for the real-valued Laplace FMM).
+template <class T = double2>
+struct OutBufT {
+    DevBuf<T> own;
+    T *ptr = nullptr;
     void *user = nullptr;
     size_t n = 0;
     bool on_dev = false;
@@ -70,7 +72,7 @@ struct OutBuf {
             return;
         }
         if (dev) {
-            ptr = static_cast<double2 *>(u);
+            ptr = static_cast<T *>(u);
         } else {
             own.alloc(count, s);
             ptr = own.get();
@@ -78,10 +80,11 @@ struct OutBuf {
     }
     void flush(cudaStream_t s) {
         if (ptr && !on_dev)
-            FMM_CUDA(cudaMemcpyAsync(user, ptr, n * sizeof(double2),
+            FMM_CUDA(cudaMemcpyAsync(user, ptr, n * sizeof(T),
                                      cudaMemcpyDeviceToHost, s));
     }
 };
+using OutBuf = OutBufT<double2>;
 
 }  // namespace
 
@@ -158,10 +161,13 @@ void set_mixed_leaf_capacity(int p, int ndiv) {
 // points in tree order.  It depends on the points, eps and the precision
 // only, so a plan keeps it on the device for many evaluations.
 void laplace_geometry(const FmmCall &c, bool on_dev, cudaStream_t s, LapGeometry &G) {
-    const bool lap = c.kernel == kLaplace;
+    // (the real-valued form takes the complex-Laplace paths with one
+    // real-charge channel per density)
+    const bool lap = c.kernel == kLaplace || c.kernel == kReal;
     G.lap = lap;
+    G.real = c.kernel == kReal;
     G.nd = c.nd;
-    G.ndc = lap ? 2 * c.nd : c.nd;
+    G.ndc = c.kernel == kLaplace ? 2 * c.nd : c.nd;
     G.ns = c.ns;
     G.nt = c.nt;
     G.eps = c.eps;
@@ -210,14 +216,16 @@ void laplace_geometry(const FmmCall &c, bool on_dev, cudaStream_t s, LapGeometry
 // strength and output pointers and the flags of `c` are read.
 void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaStream_t s,
                       M2LCache *m2l, bool sync) {
-    const bool lap = G.lap;
+    const bool lap = G.lap, real = G.real;
     const int nd = G.nd, ndc = G.ndc, ns = G.ns, nt = G.nt;
     const Tree &T = G.T;
-    InBuf<double2> chg_in, dip_in;
+    // strengths: complex (interleaved doubles) or, for rfmm2d, real
+    InBuf<double> chg_in, dip_in;
     InBuf<double> dv_in;
-    if (c.ifcharge) chg_in.set(c.charge, (size_t)nd * ns, on_dev, s);
+    const size_t sw = real ? 1 : 2;
+    if (c.ifcharge) chg_in.set(c.charge, sw * nd * ns, on_dev, s);
     if (c.ifdipole) {
-        dip_in.set(c.dipstr, (size_t)nd * ns, on_dev, s);
+        dip_in.set(c.dipstr, sw * nd * ns, on_dev, s);
         if (lap) dv_in.set(c.dipvec, (size_t)2 * nd * ns, on_dev, s);
     }
     // ---- strengths into tree order (and their FP32 copies for the mixed
@@ -241,13 +249,27 @@ void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaS
             dip_s.alloc((size_t)ns * ndc, s);
             if (mixed) dip32.alloc((size_t)ns * ndc, s);
         }
-        const double2 *q = chg_in.ptr, *d = dip_in.ptr;
+        const double2 *q = reinterpret_cast<const double2 *>(chg_in.ptr),
+                      *d = reinterpret_cast<const double2 *>(dip_in.ptr);
+        const double *qr = chg_in.ptr, *dr = dip_in.ptr;
         const double *dv = dv_in.ptr;
         double2 *qo = chg_s.get(), *dout = dip_s.get();
         float2 *q32 = chg32.get(), *d32 = dip32.get();
         for_each(ns, s, [=] __device__(int64_t k) {
             const int i = perm[k];
             for (int j = 0; j < nd; j++) {
+                if (real) {
+                    // charge1 = charge, dipstr1 = dipstr * (-(v1 + i v2))
+                    // (rfmm2d.f:133-149)
+                    if (ifc) put(qo, q32, (size_t)k * ndc + j, make_double2(qr[(size_t)i * nd + j], 0.0));
+                    if (ifd) {
+                        const double dd = dr[(size_t)i * nd + j];
+                        const double v1 = dv[((size_t)i * 2 + 0) * nd + j];
+                        const double v2 = dv[((size_t)i * 2 + 1) * nd + j];
+                        put(dout, d32, (size_t)k * ndc + j, make_double2(-dd * v1, -dd * v2));
+                    }
+                    continue;
+                }
                 if (ifc) {
                     const double2 v = q[(size_t)i * nd + j];
                     if (lap) {
@@ -331,6 +353,36 @@ void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaS
                       double *upot, double *ugrad, double *uhess) {
         if (pgh <= 0 || n <= 0) return;
         const int gcomp = lap ? 2 : 1, hcomp = lap ? 3 : 1;
+        if (real) {
+            // rfmm2d.f:159-214: pot = Re pot1, grad = (Re g1, -Im g1),
+            // hess = (Re h1, -Im h1, -Re h1), all real
+            OutBufT<double> op, og, oh;
+            op.set(upot, (size_t)nd * n, on_dev, s);
+            if (pgh >= 2) og.set(ugrad, (size_t)nd * 2 * n, on_dev, s);
+            if (pgh >= 3) oh.set(uhess, (size_t)nd * 3 * n, on_dev, s);
+            const double2 *P0 = po.get(), *G0 = gr.get(), *H0 = he.get();
+            double *up = op.ptr, *ug = og.ptr, *uh = oh.ptr;
+            for_each(n, s, [=] __device__(int64_t k) {
+                const int i = perm[k];
+                for (int j = 0; j < nd; j++) {
+                    const size_t a = (size_t)k * ndc + j;
+                    up[(size_t)i * nd + j] = P0[a].x;
+                    if (pgh >= 2) {
+                        ug[((size_t)i * 2 + 0) * nd + j] = G0[a].x;
+                        ug[((size_t)i * 2 + 1) * nd + j] = -G0[a].y;
+                    }
+                    if (pgh >= 3) {
+                        uh[((size_t)i * 3 + 0) * nd + j] = H0[a].x;
+                        uh[((size_t)i * 3 + 1) * nd + j] = -H0[a].y;
+                        uh[((size_t)i * 3 + 2) * nd + j] = -H0[a].x;
+                    }
+                }
+            });
+            op.flush(s);
+            og.flush(s);
+            oh.flush(s);
+            return;
+        }
         OutBuf op, og, oh;
         op.set(upot, (size_t)nd * n, on_dev, s);
         if (pgh >= 2) og.set(ugrad, (size_t)nd * gcomp * n, on_dev, s);
@@ -793,6 +845,7 @@ int run_fmm(const FmmCall &c) {
         switch (c.kernel) {
             case kLaplace:
             case kCauchy:
+            case kReal:
                 run_laplace_family(c, ctx);
                 break;
             case kHelmholtz:

@@ -33,7 +33,8 @@ extern "C" {
 #endif
 
 /* ===================================================================== */
-/* Flag wrappers: {l,c,h}fmm2d_{s,t,st}_{c,d,cd}_{p,g,h}_                 */
+/* Flag wrappers: {l,c,h}fmm2d_{s,t,st}_{c,d,cd}_{p,g,h}_ (rfmm2d and    */
+/* the _vec forms follow below)                                          */
 /*   s / t / st : evaluate at sources, at targets, at both               */
 /*   c / d / cd : charges, dipoles, both                                 */
 /*   p / g / h  : potential, + gradient, + Hessian                       */
@@ -553,6 +554,885 @@ void hfmm2d_st_cd_h_(const double *eps, const double _Complex *zk,
                      int32_t *ier);
 
 /* ===================================================================== */
+/* rfmm2d_{s,t,st}_{c,d,cd}_{p,g,h}_: the real-valued Laplace FMM        */
+/* (src/laplace/rfmm2d.f:27): real charge(n), dipstr(n), dipvec(2,n),    */
+/* real pot(n), grad(2,n), hess(3,n).                                    */
+/* ===================================================================== */
+/* src/laplace/rfmm2dwrap.f:36 */
+void rfmm2d_s_c_p_(const double *eps, const int32_t *ns,
+                   const double *sources, const double *charge, double *pot,
+                   int32_t *ier);
+/* src/laplace/rfmm2dwrap.f:98 */
+void rfmm2d_s_c_g_(const double *eps, const int32_t *ns,
+                   const double *sources, const double *charge, double *pot,
+                   double *grad, int32_t *ier);
+/* src/laplace/rfmm2dwrap.f:161 */
+void rfmm2d_s_c_h_(const double *eps, const int32_t *ns,
+                   const double *sources, const double *charge, double *pot,
+                   double *grad, double *hess, int32_t *ier);
+/* src/laplace/rfmm2dwrap.f:222 */
+void rfmm2d_s_d_p_(const double *eps, const int32_t *ns,
+                   const double *sources, const double *dipstr,
+                   const double *dipvec, double *pot, int32_t *ier);
+/* src/laplace/rfmm2dwrap.f:285 */
+void rfmm2d_s_d_g_(const double *eps, const int32_t *ns,
+                   const double *sources, const double *dipstr,
+                   const double *dipvec, double *pot, double *grad,
+                   int32_t *ier);
+/* src/laplace/rfmm2dwrap.f:349 */
+void rfmm2d_s_d_h_(const double *eps, const int32_t *ns,
+                   const double *sources, const double *dipstr,
+                   const double *dipvec, double *pot, double *grad,
+                   double *hess, int32_t *ier);
+/* src/laplace/rfmm2dwrap.f:411 */
+void rfmm2d_s_cd_p_(const double *eps, const int32_t *ns,
+                    const double *sources, const double *charge,
+                    const double *dipstr, const double *dipvec, double *pot,
+                    int32_t *ier);
+/* src/laplace/rfmm2dwrap.f:473 */
+void rfmm2d_s_cd_g_(const double *eps, const int32_t *ns,
+                    const double *sources, const double *charge,
+                    const double *dipstr, const double *dipvec, double *pot,
+                    double *grad, int32_t *ier);
+/* src/laplace/rfmm2dwrap.f:536 */
+void rfmm2d_s_cd_h_(const double *eps, const int32_t *ns,
+                    const double *sources, const double *charge,
+                    const double *dipstr, const double *dipvec, double *pot,
+                    double *grad, double *hess, int32_t *ier);
+/* src/laplace/rfmm2dwrap.f:599 */
+void rfmm2d_t_c_p_(const double *eps, const int32_t *ns,
+                   const double *sources, const double *charge,
+                   const int32_t *nt, const double *targ, double *pottarg,
+                   int32_t *ier);
+/* src/laplace/rfmm2dwrap.f:659 */
+void rfmm2d_t_c_g_(const double *eps, const int32_t *ns,
+                   const double *sources, const double *charge,
+                   const int32_t *nt, const double *targ, double *pottarg,
+                   double *gradtarg, int32_t *ier);
+/* src/laplace/rfmm2dwrap.f:720 */
+void rfmm2d_t_c_h_(const double *eps, const int32_t *ns,
+                   const double *sources, const double *charge,
+                   const int32_t *nt, const double *targ, double *pottarg,
+                   double *gradtarg, double *hesstarg, int32_t *ier);
+/* src/laplace/rfmm2dwrap.f:780 */
+void rfmm2d_t_d_p_(const double *eps, const int32_t *ns,
+                   const double *sources, const double *dipstr,
+                   const double *dipvec, const int32_t *nt,
+                   const double *targ, double *pottarg, int32_t *ier);
+/* src/laplace/rfmm2dwrap.f:841 */
+void rfmm2d_t_d_g_(const double *eps, const int32_t *ns,
+                   const double *sources, const double *dipstr,
+                   const double *dipvec, const int32_t *nt,
+                   const double *targ, double *pottarg, double *gradtarg,
+                   int32_t *ier);
+/* src/laplace/rfmm2dwrap.f:903 */
+void rfmm2d_t_d_h_(const double *eps, const int32_t *ns,
+                   const double *sources, const double *dipstr,
+                   const double *dipvec, const int32_t *nt,
+                   const double *targ, double *pottarg, double *gradtarg,
+                   double *hesstarg, int32_t *ier);
+/* src/laplace/rfmm2dwrap.f:964 */
+void rfmm2d_t_cd_p_(const double *eps, const int32_t *ns,
+                    const double *sources, const double *charge,
+                    const double *dipstr, const double *dipvec,
+                    const int32_t *nt, const double *targ, double *pottarg,
+                    int32_t *ier);
+/* src/laplace/rfmm2dwrap.f:1024 */
+void rfmm2d_t_cd_g_(const double *eps, const int32_t *ns,
+                    const double *sources, const double *charge,
+                    const double *dipstr, const double *dipvec,
+                    const int32_t *nt, const double *targ, double *pottarg,
+                    double *gradtarg, int32_t *ier);
+/* src/laplace/rfmm2dwrap.f:1085 */
+void rfmm2d_t_cd_h_(const double *eps, const int32_t *ns,
+                    const double *sources, const double *charge,
+                    const double *dipstr, const double *dipvec,
+                    const int32_t *nt, const double *targ, double *pottarg,
+                    double *gradtarg, double *hesstarg, int32_t *ier);
+/* src/laplace/rfmm2dwrap.f:1148 */
+void rfmm2d_st_c_p_(const double *eps, const int32_t *ns,
+                    const double *sources, const double *charge, double *pot,
+                    const int32_t *nt, const double *targ, double *pottarg,
+                    int32_t *ier);
+/* src/laplace/rfmm2dwrap.f:1209 */
+void rfmm2d_st_c_g_(const double *eps, const int32_t *ns,
+                    const double *sources, const double *charge, double *pot,
+                    double *grad, const int32_t *nt, const double *targ,
+                    double *pottarg, double *gradtarg, int32_t *ier);
+/* src/laplace/rfmm2dwrap.f:1272 */
+void rfmm2d_st_c_h_(const double *eps, const int32_t *ns,
+                    const double *sources, const double *charge, double *pot,
+                    double *grad, double *hess, const int32_t *nt,
+                    const double *targ, double *pottarg, double *gradtarg,
+                    double *hesstarg, int32_t *ier);
+/* src/laplace/rfmm2dwrap.f:1335 */
+void rfmm2d_st_d_p_(const double *eps, const int32_t *ns,
+                    const double *sources, const double *dipstr,
+                    const double *dipvec, double *pot, const int32_t *nt,
+                    const double *targ, double *pottarg, int32_t *ier);
+/* src/laplace/rfmm2dwrap.f:1397 */
+void rfmm2d_st_d_g_(const double *eps, const int32_t *ns,
+                    const double *sources, const double *dipstr,
+                    const double *dipvec, double *pot, double *grad,
+                    const int32_t *nt, const double *targ, double *pottarg,
+                    double *gradtarg, int32_t *ier);
+/* src/laplace/rfmm2dwrap.f:1461 */
+void rfmm2d_st_d_h_(const double *eps, const int32_t *ns,
+                    const double *sources, const double *dipstr,
+                    const double *dipvec, double *pot, double *grad,
+                    double *hess, const int32_t *nt, const double *targ,
+                    double *pottarg, double *gradtarg, double *hesstarg,
+                    int32_t *ier);
+/* src/laplace/rfmm2dwrap.f:1525 */
+void rfmm2d_st_cd_p_(const double *eps, const int32_t *ns,
+                     const double *sources, const double *charge,
+                     const double *dipstr, const double *dipvec, double *pot,
+                     const int32_t *nt, const double *targ, double *pottarg,
+                     int32_t *ier);
+/* src/laplace/rfmm2dwrap.f:1586 */
+void rfmm2d_st_cd_g_(const double *eps, const int32_t *ns,
+                     const double *sources, const double *charge,
+                     const double *dipstr, const double *dipvec, double *pot,
+                     double *grad, const int32_t *nt, const double *targ,
+                     double *pottarg, double *gradtarg, int32_t *ier);
+/* src/laplace/rfmm2dwrap.f:1649 */
+void rfmm2d_st_cd_h_(const double *eps, const int32_t *ns,
+                     const double *sources, const double *charge,
+                     const double *dipstr, const double *dipvec, double *pot,
+                     double *grad, double *hess, const int32_t *nt,
+                     const double *targ, double *pottarg, double *gradtarg,
+                     double *hesstarg, int32_t *ier);
+
+
+/* ===================================================================== */
+/* Vectorised wrappers {l,c,h,r}fmm2d_*_vec_: the same 27 flag sets per  */
+/* family with a leading nd (number of densities); strengths (nd, n),    */
+/* dipvec (nd, 2, n), pot (nd, n), grad (nd, 2, n) or (nd, n) for        */
+/* cfmm2d, hess (nd, 3, n) or (nd, n) for cfmm2d.                        */
+/* ===================================================================== */
+/* src/laplace/lfmm2dwrap_vec.f:31 */
+void lfmm2d_s_c_p_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double _Complex *charge, double _Complex *pot,
+                       int32_t *ier);
+/* src/laplace/lfmm2dwrap_vec.f:91 */
+void lfmm2d_s_c_g_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double _Complex *charge, double _Complex *pot,
+                       double _Complex *grad, int32_t *ier);
+/* src/laplace/lfmm2dwrap_vec.f:154 */
+void lfmm2d_s_c_h_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double _Complex *charge, double _Complex *pot,
+                       double _Complex *grad, double _Complex *hess,
+                       int32_t *ier);
+/* src/laplace/lfmm2dwrap_vec.f:215 */
+void lfmm2d_s_d_p_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double _Complex *dipstr, const double *dipvec,
+                       double _Complex *pot, int32_t *ier);
+/* src/laplace/lfmm2dwrap_vec.f:276 */
+void lfmm2d_s_d_g_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double _Complex *dipstr, const double *dipvec,
+                       double _Complex *pot, double _Complex *grad,
+                       int32_t *ier);
+/* src/laplace/lfmm2dwrap_vec.f:340 */
+void lfmm2d_s_d_h_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double _Complex *dipstr, const double *dipvec,
+                       double _Complex *pot, double _Complex *grad,
+                       double _Complex *hess, int32_t *ier);
+/* src/laplace/lfmm2dwrap_vec.f:401 */
+void lfmm2d_s_cd_p_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double _Complex *charge,
+                        const double _Complex *dipstr, const double *dipvec,
+                        double _Complex *pot, int32_t *ier);
+/* src/laplace/lfmm2dwrap_vec.f:461 */
+void lfmm2d_s_cd_g_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double _Complex *charge,
+                        const double _Complex *dipstr, const double *dipvec,
+                        double _Complex *pot, double _Complex *grad,
+                        int32_t *ier);
+/* src/laplace/lfmm2dwrap_vec.f:523 */
+void lfmm2d_s_cd_h_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double _Complex *charge,
+                        const double _Complex *dipstr, const double *dipvec,
+                        double _Complex *pot, double _Complex *grad,
+                        double _Complex *hess, int32_t *ier);
+/* src/laplace/lfmm2dwrap_vec.f:585 */
+void lfmm2d_t_c_p_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double _Complex *charge, const int32_t *nt,
+                       const double *targ, double _Complex *pottarg,
+                       int32_t *ier);
+/* src/laplace/lfmm2dwrap_vec.f:643 */
+void lfmm2d_t_c_g_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double _Complex *charge, const int32_t *nt,
+                       const double *targ, double _Complex *pottarg,
+                       double _Complex *gradtarg, int32_t *ier);
+/* src/laplace/lfmm2dwrap_vec.f:704 */
+void lfmm2d_t_c_h_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double _Complex *charge, const int32_t *nt,
+                       const double *targ, double _Complex *pottarg,
+                       double _Complex *gradtarg, double _Complex *hesstarg,
+                       int32_t *ier);
+/* src/laplace/lfmm2dwrap_vec.f:763 */
+void lfmm2d_t_d_p_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double _Complex *dipstr, const double *dipvec,
+                       const int32_t *nt, const double *targ,
+                       double _Complex *pottarg, int32_t *ier);
+/* src/laplace/lfmm2dwrap_vec.f:822 */
+void lfmm2d_t_d_g_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double _Complex *dipstr, const double *dipvec,
+                       const int32_t *nt, const double *targ,
+                       double _Complex *pottarg, double _Complex *gradtarg,
+                       int32_t *ier);
+/* src/laplace/lfmm2dwrap_vec.f:884 */
+void lfmm2d_t_d_h_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double _Complex *dipstr, const double *dipvec,
+                       const int32_t *nt, const double *targ,
+                       double _Complex *pottarg, double _Complex *gradtarg,
+                       double _Complex *hesstarg, int32_t *ier);
+/* src/laplace/lfmm2dwrap_vec.f:944 */
+void lfmm2d_t_cd_p_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double _Complex *charge,
+                        const double _Complex *dipstr, const double *dipvec,
+                        const int32_t *nt, const double *targ,
+                        double _Complex *pottarg, int32_t *ier);
+/* src/laplace/lfmm2dwrap_vec.f:1002 */
+void lfmm2d_t_cd_g_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double _Complex *charge,
+                        const double _Complex *dipstr, const double *dipvec,
+                        const int32_t *nt, const double *targ,
+                        double _Complex *pottarg, double _Complex *gradtarg,
+                        int32_t *ier);
+/* src/laplace/lfmm2dwrap_vec.f:1062 */
+void lfmm2d_t_cd_h_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double _Complex *charge,
+                        const double _Complex *dipstr, const double *dipvec,
+                        const int32_t *nt, const double *targ,
+                        double _Complex *pottarg, double _Complex *gradtarg,
+                        double _Complex *hesstarg, int32_t *ier);
+/* src/laplace/lfmm2dwrap_vec.f:1126 */
+void lfmm2d_st_c_p_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double _Complex *charge, double _Complex *pot,
+                        const int32_t *nt, const double *targ,
+                        double _Complex *pottarg, int32_t *ier);
+/* src/laplace/lfmm2dwrap_vec.f:1185 */
+void lfmm2d_st_c_g_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double _Complex *charge, double _Complex *pot,
+                        double _Complex *grad, const int32_t *nt,
+                        const double *targ, double _Complex *pottarg,
+                        double _Complex *gradtarg, int32_t *ier);
+/* src/laplace/lfmm2dwrap_vec.f:1248 */
+void lfmm2d_st_c_h_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double _Complex *charge, double _Complex *pot,
+                        double _Complex *grad, double _Complex *hess,
+                        const int32_t *nt, const double *targ,
+                        double _Complex *pottarg, double _Complex *gradtarg,
+                        double _Complex *hesstarg, int32_t *ier);
+/* src/laplace/lfmm2dwrap_vec.f:1311 */
+void lfmm2d_st_d_p_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double _Complex *dipstr, const double *dipvec,
+                        double _Complex *pot, const int32_t *nt,
+                        const double *targ, double _Complex *pottarg,
+                        int32_t *ier);
+/* src/laplace/lfmm2dwrap_vec.f:1371 */
+void lfmm2d_st_d_g_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double _Complex *dipstr, const double *dipvec,
+                        double _Complex *pot, double _Complex *grad,
+                        const int32_t *nt, const double *targ,
+                        double _Complex *pottarg, double _Complex *gradtarg,
+                        int32_t *ier);
+/* src/laplace/lfmm2dwrap_vec.f:1436 */
+void lfmm2d_st_d_h_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double _Complex *dipstr, const double *dipvec,
+                        double _Complex *pot, double _Complex *grad,
+                        double _Complex *hess, const int32_t *nt,
+                        const double *targ, double _Complex *pottarg,
+                        double _Complex *gradtarg, double _Complex *hesstarg,
+                        int32_t *ier);
+/* src/laplace/lfmm2dwrap_vec.f:1500 */
+void lfmm2d_st_cd_p_vec_(const int32_t *nd, const double *eps,
+                         const int32_t *ns, const double *sources,
+                         const double _Complex *charge,
+                         const double _Complex *dipstr, const double *dipvec,
+                         double _Complex *pot, const int32_t *nt,
+                         const double *targ, double _Complex *pottarg,
+                         int32_t *ier);
+/* src/laplace/lfmm2dwrap_vec.f:1560 */
+void lfmm2d_st_cd_g_vec_(const int32_t *nd, const double *eps,
+                         const int32_t *ns, const double *sources,
+                         const double _Complex *charge,
+                         const double _Complex *dipstr, const double *dipvec,
+                         double _Complex *pot, double _Complex *grad,
+                         const int32_t *nt, const double *targ,
+                         double _Complex *pottarg, double _Complex *gradtarg,
+                         int32_t *ier);
+/* src/laplace/lfmm2dwrap_vec.f:1623 */
+void lfmm2d_st_cd_h_vec_(const int32_t *nd, const double *eps,
+                         const int32_t *ns, const double *sources,
+                         const double _Complex *charge,
+                         const double _Complex *dipstr, const double *dipvec,
+                         double _Complex *pot, double _Complex *grad,
+                         double _Complex *hess, const int32_t *nt,
+                         const double *targ, double _Complex *pottarg,
+                         double _Complex *gradtarg, double _Complex *hesstarg,
+                         int32_t *ier);
+/* src/laplace/cfmm2dwrap_vec.f:37 */
+void cfmm2d_s_c_p_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double _Complex *charge, double _Complex *pot,
+                       int32_t *ier);
+/* src/laplace/cfmm2dwrap_vec.f:96 */
+void cfmm2d_s_c_g_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double _Complex *charge, double _Complex *pot,
+                       double _Complex *grad, int32_t *ier);
+/* src/laplace/cfmm2dwrap_vec.f:158 */
+void cfmm2d_s_c_h_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double _Complex *charge, double _Complex *pot,
+                       double _Complex *grad, double _Complex *hess,
+                       int32_t *ier);
+/* src/laplace/cfmm2dwrap_vec.f:218 */
+void cfmm2d_s_d_p_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double _Complex *dipstr, double _Complex *pot,
+                       int32_t *ier);
+/* src/laplace/cfmm2dwrap_vec.f:277 */
+void cfmm2d_s_d_g_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double _Complex *dipstr, double _Complex *pot,
+                       double _Complex *grad, int32_t *ier);
+/* src/laplace/cfmm2dwrap_vec.f:339 */
+void cfmm2d_s_d_h_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double _Complex *dipstr, double _Complex *pot,
+                       double _Complex *grad, double _Complex *hess,
+                       int32_t *ier);
+/* src/laplace/cfmm2dwrap_vec.f:398 */
+void cfmm2d_s_cd_p_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double _Complex *charge,
+                        const double _Complex *dipstr, double _Complex *pot,
+                        int32_t *ier);
+/* src/laplace/cfmm2dwrap_vec.f:456 */
+void cfmm2d_s_cd_g_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double _Complex *charge,
+                        const double _Complex *dipstr, double _Complex *pot,
+                        double _Complex *grad, int32_t *ier);
+/* src/laplace/cfmm2dwrap_vec.f:516 */
+void cfmm2d_s_cd_h_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double _Complex *charge,
+                        const double _Complex *dipstr, double _Complex *pot,
+                        double _Complex *grad, double _Complex *hess,
+                        int32_t *ier);
+/* src/laplace/cfmm2dwrap_vec.f:576 */
+void cfmm2d_t_c_p_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double _Complex *charge, const int32_t *nt,
+                       const double *targ, double _Complex *pottarg,
+                       int32_t *ier);
+/* src/laplace/cfmm2dwrap_vec.f:633 */
+void cfmm2d_t_c_g_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double _Complex *charge, const int32_t *nt,
+                       const double *targ, double _Complex *pottarg,
+                       double _Complex *gradtarg, int32_t *ier);
+/* src/laplace/cfmm2dwrap_vec.f:693 */
+void cfmm2d_t_c_h_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double _Complex *charge, const int32_t *nt,
+                       const double *targ, double _Complex *pottarg,
+                       double _Complex *gradtarg, double _Complex *hesstarg,
+                       int32_t *ier);
+/* src/laplace/cfmm2dwrap_vec.f:751 */
+void cfmm2d_t_d_p_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double _Complex *dipstr, const int32_t *nt,
+                       const double *targ, double _Complex *pottarg,
+                       int32_t *ier);
+/* src/laplace/cfmm2dwrap_vec.f:808 */
+void cfmm2d_t_d_g_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double _Complex *dipstr, const int32_t *nt,
+                       const double *targ, double _Complex *pottarg,
+                       double _Complex *gradtarg, int32_t *ier);
+/* src/laplace/cfmm2dwrap_vec.f:868 */
+void cfmm2d_t_d_h_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double _Complex *dipstr, const int32_t *nt,
+                       const double *targ, double _Complex *pottarg,
+                       double _Complex *gradtarg, double _Complex *hesstarg,
+                       int32_t *ier);
+/* src/laplace/cfmm2dwrap_vec.f:926 */
+void cfmm2d_t_cd_p_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double _Complex *charge,
+                        const double _Complex *dipstr, const int32_t *nt,
+                        const double *targ, double _Complex *pottarg,
+                        int32_t *ier);
+/* src/laplace/cfmm2dwrap_vec.f:982 */
+void cfmm2d_t_cd_g_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double _Complex *charge,
+                        const double _Complex *dipstr, const int32_t *nt,
+                        const double *targ, double _Complex *pottarg,
+                        double _Complex *gradtarg, int32_t *ier);
+/* src/laplace/cfmm2dwrap_vec.f:1040 */
+void cfmm2d_t_cd_h_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double _Complex *charge,
+                        const double _Complex *dipstr, const int32_t *nt,
+                        const double *targ, double _Complex *pottarg,
+                        double _Complex *gradtarg, double _Complex *hesstarg,
+                        int32_t *ier);
+/* src/laplace/cfmm2dwrap_vec.f:1102 */
+void cfmm2d_st_c_p_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double _Complex *charge, double _Complex *pot,
+                        const int32_t *nt, const double *targ,
+                        double _Complex *pottarg, int32_t *ier);
+/* src/laplace/cfmm2dwrap_vec.f:1160 */
+void cfmm2d_st_c_g_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double _Complex *charge, double _Complex *pot,
+                        double _Complex *grad, const int32_t *nt,
+                        const double *targ, double _Complex *pottarg,
+                        double _Complex *gradtarg, int32_t *ier);
+/* src/laplace/cfmm2dwrap_vec.f:1222 */
+void cfmm2d_st_c_h_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double _Complex *charge, double _Complex *pot,
+                        double _Complex *grad, double _Complex *hess,
+                        const int32_t *nt, const double *targ,
+                        double _Complex *pottarg, double _Complex *gradtarg,
+                        double _Complex *hesstarg, int32_t *ier);
+/* src/laplace/cfmm2dwrap_vec.f:1284 */
+void cfmm2d_st_d_p_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double _Complex *dipstr, double _Complex *pot,
+                        const int32_t *nt, const double *targ,
+                        double _Complex *pottarg, int32_t *ier);
+/* src/laplace/cfmm2dwrap_vec.f:1342 */
+void cfmm2d_st_d_g_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double _Complex *dipstr, double _Complex *pot,
+                        double _Complex *grad, const int32_t *nt,
+                        const double *targ, double _Complex *pottarg,
+                        double _Complex *gradtarg, int32_t *ier);
+/* src/laplace/cfmm2dwrap_vec.f:1405 */
+void cfmm2d_st_d_h_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double _Complex *dipstr, double _Complex *pot,
+                        double _Complex *grad, double _Complex *hess,
+                        const int32_t *nt, const double *targ,
+                        double _Complex *pottarg, double _Complex *gradtarg,
+                        double _Complex *hesstarg, int32_t *ier);
+/* src/laplace/cfmm2dwrap_vec.f:1467 */
+void cfmm2d_st_cd_p_vec_(const int32_t *nd, const double *eps,
+                         const int32_t *ns, const double *sources,
+                         const double _Complex *charge,
+                         const double _Complex *dipstr, double _Complex *pot,
+                         const int32_t *nt, const double *targ,
+                         double _Complex *pottarg, int32_t *ier);
+/* src/laplace/cfmm2dwrap_vec.f:1525 */
+void cfmm2d_st_cd_g_vec_(const int32_t *nd, const double *eps,
+                         const int32_t *ns, const double *sources,
+                         const double _Complex *charge,
+                         const double _Complex *dipstr, double _Complex *pot,
+                         double _Complex *grad, const int32_t *nt,
+                         const double *targ, double _Complex *pottarg,
+                         double _Complex *gradtarg, int32_t *ier);
+/* src/laplace/cfmm2dwrap_vec.f:1586 */
+void cfmm2d_st_cd_h_vec_(const int32_t *nd, const double *eps,
+                         const int32_t *ns, const double *sources,
+                         const double _Complex *charge,
+                         const double _Complex *dipstr, double _Complex *pot,
+                         double _Complex *grad, double _Complex *hess,
+                         const int32_t *nt, const double *targ,
+                         double _Complex *pottarg, double _Complex *gradtarg,
+                         double _Complex *hesstarg, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap_vec.f:6 */
+void hfmm2d_s_c_p_vec_(const int32_t *nd, const double *eps,
+                       const double _Complex *zk, const int32_t *ns,
+                       const double *sources, const double _Complex *charge,
+                       double _Complex *pot, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap_vec.f:70 */
+void hfmm2d_s_c_g_vec_(const int32_t *nd, const double *eps,
+                       const double _Complex *zk, const int32_t *ns,
+                       const double *sources, const double _Complex *charge,
+                       double _Complex *pot, double _Complex *grad,
+                       int32_t *ier);
+/* src/helmholtz/hfmm2dwrap_vec.f:138 */
+void hfmm2d_s_c_h_vec_(const int32_t *nd, const double *eps,
+                       const double _Complex *zk, const int32_t *ns,
+                       const double *sources, const double _Complex *charge,
+                       double _Complex *pot, double _Complex *grad,
+                       double _Complex *hess, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap_vec.f:205 */
+void hfmm2d_s_d_p_vec_(const int32_t *nd, const double *eps,
+                       const double _Complex *zk, const int32_t *ns,
+                       const double *sources, const double _Complex *dipstr,
+                       const double *dipvec, double _Complex *pot,
+                       int32_t *ier);
+/* src/helmholtz/hfmm2dwrap_vec.f:270 */
+void hfmm2d_s_d_g_vec_(const int32_t *nd, const double *eps,
+                       const double _Complex *zk, const int32_t *ns,
+                       const double *sources, const double _Complex *dipstr,
+                       const double *dipvec, double _Complex *pot,
+                       double _Complex *grad, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap_vec.f:339 */
+void hfmm2d_s_d_h_vec_(const int32_t *nd, const double *eps,
+                       const double _Complex *zk, const int32_t *ns,
+                       const double *sources, const double _Complex *dipstr,
+                       const double *dipvec, double _Complex *pot,
+                       double _Complex *grad, double _Complex *hess,
+                       int32_t *ier);
+/* src/helmholtz/hfmm2dwrap_vec.f:407 */
+void hfmm2d_s_cd_p_vec_(const int32_t *nd, const double *eps,
+                        const double _Complex *zk, const int32_t *ns,
+                        const double *sources, const double _Complex *charge,
+                        const double _Complex *dipstr, const double *dipvec,
+                        double _Complex *pot, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap_vec.f:472 */
+void hfmm2d_s_cd_g_vec_(const int32_t *nd, const double *eps,
+                        const double _Complex *zk, const int32_t *ns,
+                        const double *sources, const double _Complex *charge,
+                        const double _Complex *dipstr, const double *dipvec,
+                        double _Complex *pot, double _Complex *grad,
+                        int32_t *ier);
+/* src/helmholtz/hfmm2dwrap_vec.f:540 */
+void hfmm2d_s_cd_h_vec_(const int32_t *nd, const double *eps,
+                        const double _Complex *zk, const int32_t *ns,
+                        const double *sources, const double _Complex *charge,
+                        const double _Complex *dipstr, const double *dipvec,
+                        double _Complex *pot, double _Complex *grad,
+                        double _Complex *hess, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap_vec.f:609 */
+void hfmm2d_t_c_p_vec_(const int32_t *nd, const double *eps,
+                       const double _Complex *zk, const int32_t *ns,
+                       const double *sources, const double _Complex *charge,
+                       const int32_t *nt, const double *targ,
+                       double _Complex *pottarg, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap_vec.f:671 */
+void hfmm2d_t_c_g_vec_(const int32_t *nd, const double *eps,
+                       const double _Complex *zk, const int32_t *ns,
+                       const double *sources, const double _Complex *charge,
+                       const int32_t *nt, const double *targ,
+                       double _Complex *pottarg, double _Complex *gradtarg,
+                       int32_t *ier);
+/* src/helmholtz/hfmm2dwrap_vec.f:737 */
+void hfmm2d_t_c_h_vec_(const int32_t *nd, const double *eps,
+                       const double _Complex *zk, const int32_t *ns,
+                       const double *sources, const double _Complex *charge,
+                       const int32_t *nt, const double *targ,
+                       double _Complex *pottarg, double _Complex *gradtarg,
+                       double _Complex *hesstarg, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap_vec.f:803 */
+void hfmm2d_t_d_p_vec_(const int32_t *nd, const double *eps,
+                       const double _Complex *zk, const int32_t *ns,
+                       const double *sources, const double _Complex *dipstr,
+                       const double *dipvec, const int32_t *nt,
+                       const double *targ, double _Complex *pottarg,
+                       int32_t *ier);
+/* src/helmholtz/hfmm2dwrap_vec.f:866 */
+void hfmm2d_t_d_g_vec_(const int32_t *nd, const double *eps,
+                       const double _Complex *zk, const int32_t *ns,
+                       const double *sources, const double _Complex *dipstr,
+                       const double *dipvec, const int32_t *nt,
+                       const double *targ, double _Complex *pottarg,
+                       double _Complex *gradtarg, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap_vec.f:933 */
+void hfmm2d_t_d_h_vec_(const int32_t *nd, const double *eps,
+                       const double _Complex *zk, const int32_t *ns,
+                       const double *sources, const double _Complex *dipstr,
+                       const double *dipvec, const int32_t *nt,
+                       const double *targ, double _Complex *pottarg,
+                       double _Complex *gradtarg, double _Complex *hesstarg,
+                       int32_t *ier);
+/* src/helmholtz/hfmm2dwrap_vec.f:1000 */
+void hfmm2d_t_cd_p_vec_(const int32_t *nd, const double *eps,
+                        const double _Complex *zk, const int32_t *ns,
+                        const double *sources, const double _Complex *charge,
+                        const double _Complex *dipstr, const double *dipvec,
+                        const int32_t *nt, const double *targ,
+                        double _Complex *pottarg, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap_vec.f:1063 */
+void hfmm2d_t_cd_g_vec_(const int32_t *nd, const double *eps,
+                        const double _Complex *zk, const int32_t *ns,
+                        const double *sources, const double _Complex *charge,
+                        const double _Complex *dipstr, const double *dipvec,
+                        const int32_t *nt, const double *targ,
+                        double _Complex *pottarg, double _Complex *gradtarg,
+                        int32_t *ier);
+/* src/helmholtz/hfmm2dwrap_vec.f:1129 */
+void hfmm2d_t_cd_h_vec_(const int32_t *nd, const double *eps,
+                        const double _Complex *zk, const int32_t *ns,
+                        const double *sources, const double _Complex *charge,
+                        const double _Complex *dipstr, const double *dipvec,
+                        const int32_t *nt, const double *targ,
+                        double _Complex *pottarg, double _Complex *gradtarg,
+                        double _Complex *hesstarg, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap_vec.f:1196 */
+void hfmm2d_st_c_p_vec_(const int32_t *nd, const double *eps,
+                        const double _Complex *zk, const int32_t *ns,
+                        const double *sources, const double _Complex *charge,
+                        double _Complex *pot, const int32_t *nt,
+                        const double *targ, double _Complex *pottarg,
+                        int32_t *ier);
+/* src/helmholtz/hfmm2dwrap_vec.f:1259 */
+void hfmm2d_st_c_g_vec_(const int32_t *nd, const double *eps,
+                        const double _Complex *zk, const int32_t *ns,
+                        const double *sources, const double _Complex *charge,
+                        double _Complex *pot, double _Complex *grad,
+                        const int32_t *nt, const double *targ,
+                        double _Complex *pottarg, double _Complex *gradtarg,
+                        int32_t *ier);
+/* src/helmholtz/hfmm2dwrap_vec.f:1326 */
+void hfmm2d_st_c_h_vec_(const int32_t *nd, const double *eps,
+                        const double _Complex *zk, const int32_t *ns,
+                        const double *sources, const double _Complex *charge,
+                        double _Complex *pot, double _Complex *grad,
+                        double _Complex *hess, const int32_t *nt,
+                        const double *targ, double _Complex *pottarg,
+                        double _Complex *gradtarg, double _Complex *hesstarg,
+                        int32_t *ier);
+/* src/helmholtz/hfmm2dwrap_vec.f:1393 */
+void hfmm2d_st_d_p_vec_(const int32_t *nd, const double *eps,
+                        const double _Complex *zk, const int32_t *ns,
+                        const double *sources, const double _Complex *dipstr,
+                        const double *dipvec, double _Complex *pot,
+                        const int32_t *nt, const double *targ,
+                        double _Complex *pottarg, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap_vec.f:1457 */
+void hfmm2d_st_d_g_vec_(const int32_t *nd, const double *eps,
+                        const double _Complex *zk, const int32_t *ns,
+                        const double *sources, const double _Complex *dipstr,
+                        const double *dipvec, double _Complex *pot,
+                        double _Complex *grad, const int32_t *nt,
+                        const double *targ, double _Complex *pottarg,
+                        double _Complex *gradtarg, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap_vec.f:1525 */
+void hfmm2d_st_d_h_vec_(const int32_t *nd, const double *eps,
+                        const double _Complex *zk, const int32_t *ns,
+                        const double *sources, const double _Complex *dipstr,
+                        const double *dipvec, double _Complex *pot,
+                        double _Complex *grad, double _Complex *hess,
+                        const int32_t *nt, const double *targ,
+                        double _Complex *pottarg, double _Complex *gradtarg,
+                        double _Complex *hesstarg, int32_t *ier);
+/* src/helmholtz/hfmm2dwrap_vec.f:1593 */
+void hfmm2d_st_cd_p_vec_(const int32_t *nd, const double *eps,
+                         const double _Complex *zk, const int32_t *ns,
+                         const double *sources, const double _Complex *charge,
+                         const double _Complex *dipstr, const double *dipvec,
+                         double _Complex *pot, const int32_t *nt,
+                         const double *targ, double _Complex *pottarg,
+                         int32_t *ier);
+/* src/helmholtz/hfmm2dwrap_vec.f:1657 */
+void hfmm2d_st_cd_g_vec_(const int32_t *nd, const double *eps,
+                         const double _Complex *zk, const int32_t *ns,
+                         const double *sources, const double _Complex *charge,
+                         const double _Complex *dipstr, const double *dipvec,
+                         double _Complex *pot, double _Complex *grad,
+                         const int32_t *nt, const double *targ,
+                         double _Complex *pottarg, double _Complex *gradtarg,
+                         int32_t *ier);
+/* src/helmholtz/hfmm2dwrap_vec.f:1724 */
+void hfmm2d_st_cd_h_vec_(const int32_t *nd, const double *eps,
+                         const double _Complex *zk, const int32_t *ns,
+                         const double *sources, const double _Complex *charge,
+                         const double _Complex *dipstr, const double *dipvec,
+                         double _Complex *pot, double _Complex *grad,
+                         double _Complex *hess, const int32_t *nt,
+                         const double *targ, double _Complex *pottarg,
+                         double _Complex *gradtarg, double _Complex *hesstarg,
+                         int32_t *ier);
+/* src/laplace/rfmm2dwrap_vec.f:36 */
+void rfmm2d_s_c_p_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double *charge, double *pot, int32_t *ier);
+/* src/laplace/rfmm2dwrap_vec.f:96 */
+void rfmm2d_s_c_g_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double *charge, double *pot, double *grad,
+                       int32_t *ier);
+/* src/laplace/rfmm2dwrap_vec.f:159 */
+void rfmm2d_s_c_h_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double *charge, double *pot, double *grad,
+                       double *hess, int32_t *ier);
+/* src/laplace/rfmm2dwrap_vec.f:220 */
+void rfmm2d_s_d_p_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double *dipstr, const double *dipvec,
+                       double *pot, int32_t *ier);
+/* src/laplace/rfmm2dwrap_vec.f:281 */
+void rfmm2d_s_d_g_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double *dipstr, const double *dipvec,
+                       double *pot, double *grad, int32_t *ier);
+/* src/laplace/rfmm2dwrap_vec.f:345 */
+void rfmm2d_s_d_h_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double *dipstr, const double *dipvec,
+                       double *pot, double *grad, double *hess, int32_t *ier);
+/* src/laplace/rfmm2dwrap_vec.f:406 */
+void rfmm2d_s_cd_p_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double *charge, const double *dipstr,
+                        const double *dipvec, double *pot, int32_t *ier);
+/* src/laplace/rfmm2dwrap_vec.f:466 */
+void rfmm2d_s_cd_g_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double *charge, const double *dipstr,
+                        const double *dipvec, double *pot, double *grad,
+                        int32_t *ier);
+/* src/laplace/rfmm2dwrap_vec.f:528 */
+void rfmm2d_s_cd_h_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double *charge, const double *dipstr,
+                        const double *dipvec, double *pot, double *grad,
+                        double *hess, int32_t *ier);
+/* src/laplace/rfmm2dwrap_vec.f:590 */
+void rfmm2d_t_c_p_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double *charge, const int32_t *nt,
+                       const double *targ, double *pottarg, int32_t *ier);
+/* src/laplace/rfmm2dwrap_vec.f:648 */
+void rfmm2d_t_c_g_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double *charge, const int32_t *nt,
+                       const double *targ, double *pottarg, double *gradtarg,
+                       int32_t *ier);
+/* src/laplace/rfmm2dwrap_vec.f:709 */
+void rfmm2d_t_c_h_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double *charge, const int32_t *nt,
+                       const double *targ, double *pottarg, double *gradtarg,
+                       double *hesstarg, int32_t *ier);
+/* src/laplace/rfmm2dwrap_vec.f:768 */
+void rfmm2d_t_d_p_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double *dipstr, const double *dipvec,
+                       const int32_t *nt, const double *targ, double *pottarg,
+                       int32_t *ier);
+/* src/laplace/rfmm2dwrap_vec.f:827 */
+void rfmm2d_t_d_g_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double *dipstr, const double *dipvec,
+                       const int32_t *nt, const double *targ, double *pottarg,
+                       double *gradtarg, int32_t *ier);
+/* src/laplace/rfmm2dwrap_vec.f:889 */
+void rfmm2d_t_d_h_vec_(const int32_t *nd, const double *eps,
+                       const int32_t *ns, const double *sources,
+                       const double *dipstr, const double *dipvec,
+                       const int32_t *nt, const double *targ, double *pottarg,
+                       double *gradtarg, double *hesstarg, int32_t *ier);
+/* src/laplace/rfmm2dwrap_vec.f:949 */
+void rfmm2d_t_cd_p_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double *charge, const double *dipstr,
+                        const double *dipvec, const int32_t *nt,
+                        const double *targ, double *pottarg, int32_t *ier);
+/* src/laplace/rfmm2dwrap_vec.f:1007 */
+void rfmm2d_t_cd_g_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double *charge, const double *dipstr,
+                        const double *dipvec, const int32_t *nt,
+                        const double *targ, double *pottarg, double *gradtarg,
+                        int32_t *ier);
+/* src/laplace/rfmm2dwrap_vec.f:1067 */
+void rfmm2d_t_cd_h_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double *charge, const double *dipstr,
+                        const double *dipvec, const int32_t *nt,
+                        const double *targ, double *pottarg, double *gradtarg,
+                        double *hesstarg, int32_t *ier);
+/* src/laplace/rfmm2dwrap_vec.f:1131 */
+void rfmm2d_st_c_p_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double *charge, double *pot, const int32_t *nt,
+                        const double *targ, double *pottarg, int32_t *ier);
+/* src/laplace/rfmm2dwrap_vec.f:1190 */
+void rfmm2d_st_c_g_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double *charge, double *pot, double *grad,
+                        const int32_t *nt, const double *targ,
+                        double *pottarg, double *gradtarg, int32_t *ier);
+/* src/laplace/rfmm2dwrap_vec.f:1253 */
+void rfmm2d_st_c_h_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double *charge, double *pot, double *grad,
+                        double *hess, const int32_t *nt, const double *targ,
+                        double *pottarg, double *gradtarg, double *hesstarg,
+                        int32_t *ier);
+/* src/laplace/rfmm2dwrap_vec.f:1316 */
+void rfmm2d_st_d_p_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double *dipstr, const double *dipvec,
+                        double *pot, const int32_t *nt, const double *targ,
+                        double *pottarg, int32_t *ier);
+/* src/laplace/rfmm2dwrap_vec.f:1376 */
+void rfmm2d_st_d_g_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double *dipstr, const double *dipvec,
+                        double *pot, double *grad, const int32_t *nt,
+                        const double *targ, double *pottarg, double *gradtarg,
+                        int32_t *ier);
+/* src/laplace/rfmm2dwrap_vec.f:1441 */
+void rfmm2d_st_d_h_vec_(const int32_t *nd, const double *eps,
+                        const int32_t *ns, const double *sources,
+                        const double *dipstr, const double *dipvec,
+                        double *pot, double *grad, double *hess,
+                        const int32_t *nt, const double *targ,
+                        double *pottarg, double *gradtarg, double *hesstarg,
+                        int32_t *ier);
+/* src/laplace/rfmm2dwrap_vec.f:1505 */
+void rfmm2d_st_cd_p_vec_(const int32_t *nd, const double *eps,
+                         const int32_t *ns, const double *sources,
+                         const double *charge, const double *dipstr,
+                         const double *dipvec, double *pot, const int32_t *nt,
+                         const double *targ, double *pottarg, int32_t *ier);
+/* src/laplace/rfmm2dwrap_vec.f:1565 */
+void rfmm2d_st_cd_g_vec_(const int32_t *nd, const double *eps,
+                         const int32_t *ns, const double *sources,
+                         const double *charge, const double *dipstr,
+                         const double *dipvec, double *pot, double *grad,
+                         const int32_t *nt, const double *targ,
+                         double *pottarg, double *gradtarg, int32_t *ier);
+/* src/laplace/rfmm2dwrap_vec.f:1628 */
+void rfmm2d_st_cd_h_vec_(const int32_t *nd, const double *eps,
+                         const int32_t *ns, const double *sources,
+                         const double *charge, const double *dipstr,
+                         const double *dipvec, double *pot, double *grad,
+                         double *hess, const int32_t *nt, const double *targ,
+                         double *pottarg, double *gradtarg, double *hesstarg,
+                         int32_t *ier);
+
+/* ===================================================================== */
 /* Guru drivers (full flag sets, nd densities).  iper is ignored and set */
 /* to 0, as in the reference (src/laplace/cfmm2d.f:150).                 */
 /* ===================================================================== */
@@ -586,6 +1466,17 @@ void hfmm2d_(const int32_t *nd, const double *eps, const double _Complex *zk,
              double _Complex *hess, const int32_t *nt, const double *targ,
              const int32_t *ifpghtarg, double _Complex *pottarg,
              double _Complex *gradtarg, double _Complex *hesstarg,
+             int32_t *ier);
+
+/* src/laplace/rfmm2d.f:27 (real charge(nd,ns), dipstr(nd,ns),
+ * dipvec(nd,2,ns); real pot(nd,*), grad(nd,2,*), hess(nd,3,*)) */
+void rfmm2d_(const int32_t *nd, const double *eps, const int32_t *ns,
+             const double *sources, const int32_t *ifcharge,
+             const double *charge, const int32_t *ifdipole,
+             const double *dipstr, const double *dipvec, int32_t *iper,
+             const int32_t *ifpgh, double *pot, double *grad, double *hess,
+             const int32_t *nt, const double *targ, const int32_t *ifpghtarg,
+             double *pottarg, double *gradtarg, double *hesstarg,
              int32_t *ier);
 
 /* Drivers with caller-chosen leaf capacity ndiv, subdivision rule idivflag
@@ -628,6 +1519,18 @@ void hfmm2d_ndiv_(const int32_t *nd, const double *eps,
                   double _Complex *gradtarg, double _Complex *hesstarg,
                   const int32_t *ndiv, const int32_t *idivflag,
                   const int32_t *ifnear, double *timeinfo, int32_t *ier);
+
+/* src/laplace/rfmm2d_ndiv.f:27, c_translation/src/rfmm2d_ndiv.c:51 */
+void rfmm2d_ndiv_(const int32_t *nd, const double *eps, const int32_t *ns,
+                  const double *sources, const int32_t *ifcharge,
+                  const double *charge, const int32_t *ifdipole,
+                  const double *dipstr, const double *dipvec, int32_t *iper,
+                  const int32_t *ifpgh, double *pot, double *grad,
+                  double *hess, const int32_t *nt, const double *targ,
+                  const int32_t *ifpghtarg, double *pottarg,
+                  double *gradtarg, double *hesstarg, const int32_t *ndiv,
+                  const int32_t *idivflag, const int32_t *ifnear,
+                  double *timeinfo, int32_t *ier);
 
 /* bind(c) entry, src/helmholtz_c.f03:5-15: eps, zk and ns by value, ns
  * and ier 64-bit (c_int64_t).  C++ callers pass zk as a struct of two

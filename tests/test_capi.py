@@ -22,13 +22,14 @@ def declared_names():
 
 def test_header_declares_the_reference_surface():
     names = declared_names()
-    for fam in "lch":
+    for fam in "lchr":
         for st in ("s", "t", "st"):
             for cd in ("c", "d", "cd"):
                 for p in "pgh":
                     assert f"{fam}fmm2d_{st}_{cd}_{p}_" in names
-    for g in ("lfmm2d_", "cfmm2d_", "hfmm2d_", "lfmm2d_ndiv_", "cfmm2d_ndiv_",
-              "hfmm2d_ndiv_"):
+                    assert f"{fam}fmm2d_{st}_{cd}_{p}_vec_" in names
+    for g in ("lfmm2d_", "cfmm2d_", "hfmm2d_", "rfmm2d_", "lfmm2d_ndiv_", "cfmm2d_ndiv_",
+              "hfmm2d_ndiv_", "rfmm2d_ndiv_"):
         assert g in names
 
 
