@@ -11,6 +11,7 @@
 #include "tree.cuh"
 
 #include <atomic>
+#include <memory>
 #include <mutex>
 #include <cmath>
 #include <stdlib.h>
@@ -215,7 +216,7 @@ void laplace_geometry(const FmmCall &c, bool on_dev, cudaStream_t s, LapGeometry
 // passes, outputs back to input order in the caller's layout.  Only the
 // strength and output pointers and the flags of `c` are read.
 void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaStream_t s,
-                      M2LCache *m2l, bool sync) {
+                      M2LCache *m2l, bool sync, const EvalIO &io) {
     const bool lap = G.lap, real = G.real;
     const int nd = G.nd, ndc = G.ndc, ns = G.ns, nt = G.nt;
     const Tree &T = G.T;
@@ -223,10 +224,11 @@ void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaS
     InBuf<double> chg_in, dip_in;
     InBuf<double> dv_in;
     const size_t sw = real ? 1 : 2;
-    if (c.ifcharge) chg_in.set(c.charge, sw * nd * ns, on_dev, s);
+    const bool in_dev = on_dev || io.strengths_dev;
+    if (c.ifcharge) chg_in.set(c.charge, sw * nd * ns, in_dev, s);
     if (c.ifdipole) {
-        dip_in.set(c.dipstr, sw * nd * ns, on_dev, s);
-        if (lap) dv_in.set(c.dipvec, (size_t)2 * nd * ns, on_dev, s);
+        dip_in.set(c.dipstr, sw * nd * ns, in_dev, s);
+        if (lap) dv_in.set(c.dipvec, (size_t)2 * nd * ns, in_dev, s);
     }
     // ---- strengths into tree order (and their FP32 copies for the mixed
     // near field) ----
@@ -348,6 +350,35 @@ void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaS
     }
     cauchy_fmm(T, P, s);
     // ---- back to input order, in the caller's layout ----
+    // (with a copy stream, each output's device-to-host copy starts once its
+    // scatter is done; the staging buffers live until the copies are)
+    std::vector<std::unique_ptr<OutBufT<double2>>> keep2;
+    std::vector<std::unique_ptr<OutBufT<double>>> keep1;
+    std::vector<cudaEvent_t> evs;
+    const bool overlap = io.copy && !on_dev;
+    // (declared after the buffers, so it runs first: on any exit, copies
+    // still in flight finish before the buffers are freed)
+    struct CopyGuard {
+        cudaStream_t c;
+        std::vector<cudaEvent_t> &e;
+        ~CopyGuard() {
+            if (c) cudaStreamSynchronize(c);
+            for (cudaEvent_t x : e) cudaEventDestroy(x);
+        }
+    } copy_guard{overlap ? io.copy : nullptr, evs};
+    auto flush = [&](auto &ob) {
+        if (!ob.ptr || on_dev) return;
+        if (!overlap) {
+            ob.flush(s);
+            return;
+        }
+        cudaEvent_t e;
+        FMM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        evs.push_back(e);
+        FMM_CUDA(cudaEventRecord(e, s));
+        FMM_CUDA(cudaStreamWaitEvent(io.copy, e, 0));
+        ob.flush(io.copy);
+    };
     auto unsort = [&](int n, const int *perm, int pgh, const DevBuf<double2> &po,
                       const DevBuf<double2> &gr, const DevBuf<double2> &he,
                       double *upot, double *ugrad, double *uhess) {
@@ -356,7 +387,11 @@ void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaS
         if (real) {
             // rfmm2d.f:159-214: pot = Re pot1, grad = (Re g1, -Im g1),
             // hess = (Re h1, -Im h1, -Re h1), all real
-            OutBufT<double> op, og, oh;
+            keep1.emplace_back(new OutBufT<double>());
+            keep1.emplace_back(new OutBufT<double>());
+            keep1.emplace_back(new OutBufT<double>());
+            OutBufT<double> &op = *keep1[keep1.size() - 3], &og = *keep1[keep1.size() - 2],
+                            &oh = *keep1.back();
             op.set(upot, (size_t)nd * n, on_dev, s);
             if (pgh >= 2) og.set(ugrad, (size_t)nd * 2 * n, on_dev, s);
             if (pgh >= 3) oh.set(uhess, (size_t)nd * 3 * n, on_dev, s);
@@ -378,12 +413,15 @@ void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaS
                     }
                 }
             });
-            op.flush(s);
-            og.flush(s);
-            oh.flush(s);
+            flush(op);
+            flush(og);
+            flush(oh);
             return;
         }
-        OutBuf op, og, oh;
+        keep2.emplace_back(new OutBuf());
+        keep2.emplace_back(new OutBuf());
+        keep2.emplace_back(new OutBuf());
+        OutBuf &op = *keep2[keep2.size() - 3], &og = *keep2[keep2.size() - 2], &oh = *keep2.back();
         op.set(upot, (size_t)nd * n, on_dev, s);
         if (pgh >= 2) og.set(ugrad, (size_t)nd * gcomp * n, on_dev, s);
         if (pgh >= 3) oh.set(uhess, (size_t)nd * hcomp * n, on_dev, s);
@@ -418,13 +456,21 @@ void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaS
                 }
             }
         });
-        op.flush(s);
-        og.flush(s);
-        oh.flush(s);
+        flush(op);
+        flush(og);
+        flush(oh);
     };
     unsort(ns, T.isrc.get(), spgh, spot, sgrad, shess, c.pot, c.grad, c.hess);
     unsort(nt, T.itarg.get(), tpgh, tpot, tgrad, thess, c.pottarg, c.gradtarg,
            c.hesstarg);
+    if (overlap) {
+        // the call ends (and the staging buffers are freed on s) after the copies
+        cudaEvent_t e;
+        FMM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        evs.push_back(e);
+        FMM_CUDA(cudaEventRecord(e, io.copy));
+        FMM_CUDA(cudaStreamWaitEvent(s, e, 0));
+    }
     // (the outputs, copied to host arrays where the caller's are, are
     // complete when the call returns)
     if (sync) FMM_CUDA(cudaStreamSynchronize(s));
@@ -437,9 +483,59 @@ void run_laplace_family(const FmmCall &c, CallCtx &ctx) {
     cudaStream_t s = ctx.stream();
     const bool on_dev = is_device_ptr(c.sources);
     prof_begin(s, c.timeinfo != nullptr);
-    LapGeometry G;
-    laplace_geometry(c, on_dev, s, G);
-    laplace_evaluate(c, G, on_dev, s);
+    if (on_dev) {
+        LapGeometry G;
+        laplace_geometry(c, on_dev, s, G);
+        laplace_evaluate(c, G, on_dev, s);
+    } else {
+        // Host arrays: the strengths go to the device on the copy stream
+        // while the positions are copied and the tree is built on s; the
+        // outputs come back on the copy stream array by array.
+        cudaStream_t cs = ctx.copy_stream();
+        const size_t sw = c.kernel == kReal ? 1 : 2;
+        const size_t nsd = (size_t)c.nd * c.ns;
+        DevBuf<double> dq, dd, dv;
+        if (c.ifcharge) dq.alloc(sw * nsd, s);
+        if (c.ifdipole) {
+            dd.alloc(sw * nsd, s);
+            if (c.kernel != kCauchy) dv.alloc(2 * nsd, s);
+        }
+        cudaEvent_t e0, e1;
+        FMM_CUDA(cudaEventCreateWithFlags(&e0, cudaEventDisableTiming));
+        FMM_CUDA(cudaEventCreateWithFlags(&e1, cudaEventDisableTiming));
+        // (declared after the buffers, so it runs first: on any exit the
+        // copies finish before the buffers are freed)
+        struct EvGuard {
+            cudaEvent_t a, b;
+            cudaStream_t cs;
+            ~EvGuard() {
+                cudaStreamSynchronize(cs);
+                cudaEventDestroy(a);
+                cudaEventDestroy(b);
+            }
+        } guard{e0, e1, cs};
+        FMM_CUDA(cudaEventRecord(e0, s));  // the allocations above are ordered on s
+        FMM_CUDA(cudaStreamWaitEvent(cs, e0, 0));
+        auto up = [&](DevBuf<double> &b, const double *h, size_t n) {
+            if (b.get() && h)
+                FMM_CUDA(cudaMemcpyAsync(b.get(), h, n * sizeof(double), cudaMemcpyHostToDevice, cs));
+        };
+        up(dq, c.charge, sw * nsd);
+        up(dd, c.dipstr, sw * nsd);
+        up(dv, c.dipvec, 2 * nsd);
+        FMM_CUDA(cudaEventRecord(e1, cs));
+        LapGeometry G;
+        laplace_geometry(c, false, s, G);
+        FMM_CUDA(cudaStreamWaitEvent(s, e1, 0));
+        FmmCall c2 = c;
+        c2.charge = c.ifcharge ? dq.get() : nullptr;
+        c2.dipstr = c.ifdipole ? dd.get() : nullptr;
+        c2.dipvec = (c.ifdipole && c.kernel != kCauchy) ? dv.get() : nullptr;
+        EvalIO io;
+        io.strengths_dev = true;
+        io.copy = cs;
+        laplace_evaluate(c2, G, false, s, nullptr, true, io);
+    }
     prof_end(s);
     if (c.timeinfo) prof_timeinfo(c.timeinfo);
 }

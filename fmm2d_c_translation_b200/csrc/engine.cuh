@@ -58,9 +58,20 @@ void laplace_geometry(const FmmCall &c, bool on_dev, cudaStream_t s, LapGeometry
 // m2l: planning kept across evaluations (plans), null for a one-shot call;
 // sync = false leaves the final stream synchronisation to the caller (the
 // form a CUDA graph can capture).
+//
+// Host-array calls overlap their copies with the compute through `io`:
+// strengths_dev says the strength pointers of `c` already hold device
+// copies (staged on a copy stream while the tree was built; the caller made
+// `s` wait for them), and with a copy stream each output array's
+// device-to-host copy runs there as soon as its scatter kernel has
+// finished, overlapping the remaining scatters.
 struct M2LCache;
+struct EvalIO {
+    bool strengths_dev = false;
+    cudaStream_t copy = nullptr;
+};
 void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaStream_t s,
-                      M2LCache *m2l = nullptr, bool sync = true);
+                      M2LCache *m2l = nullptr, bool sync = true, const EvalIO &io = EvalIO());
 
 // A batch of independent lfmm2d / cfmm2d problems (nd = 1) with the same
 // eps and flags, evaluated as one forest: one launch per level and pass for

@@ -46,6 +46,13 @@ CallCtx::CallCtx() : dev_(0), s_(nullptr) {
     s_ = streams[dev_];
 }
 
+cudaStream_t CallCtx::copy_stream() const {
+    static thread_local cudaStream_t streams[64];
+    if (!streams[dev_])
+        FMM_CUDA(cudaStreamCreateWithFlags(&streams[dev_], cudaStreamNonBlocking));
+    return streams[dev_];
+}
+
 void set_user_stream(cudaStream_t s, bool on) {
     g_user_stream = s;
     g_user_stream_set = on;

@@ -28,6 +28,9 @@ class CallCtx {
     CallCtx &operator=(const CallCtx &) = delete;
     cudaStream_t stream() const { return s_; }
     int device() const { return dev_; }
+    // A second non-blocking stream of the calling thread and device, for
+    // host<->device copies that overlap the work on stream().
+    cudaStream_t copy_stream() const;
 
   private:
     int dev_;
