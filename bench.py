@@ -36,8 +36,8 @@ at 70 % of the throughput measured on a saturating burst of the same
 stream; latency = submission to completion (host arrays, copies
 included); p50 / p99 over all requests.  Beside it, the same requests one
 at a time in all-FP64 mode (one slot).  ``--serve-requests`` sets the
-stream length (the configuration names 20,000; the default run uses 2,000
-to stay within minutes).
+stream length (20,000 by default, as the configuration names); the
+one-at-a-time baseline runs the first --serve-baseline requests of it.
 """
 import argparse
 import ctypes
@@ -355,7 +355,9 @@ def main():
                     help="skip the other configurations (c1, c3, c4)")
     ap.add_argument("--configs", default="c1,c3,c4",
                     help="which of the other configurations to run (comma list)")
-    ap.add_argument("--serve-requests", type=int, default=2000)
+    ap.add_argument("--serve-requests", type=int, default=20000)
+    ap.add_argument("--serve-baseline", type=int, default=2000,
+                    help="requests of the one-at-a-time FP64 baseline (a prefix of the stream)")
     ap.add_argument("--serve-slots", type=int, default=6)
     ap.add_argument("--serve-budget-gb", type=float, default=120.0)
     args = ap.parse_args()
@@ -712,12 +714,12 @@ def measure_serving(fm, args):
     # warm the pool and the code paths
     run(reqs[:20], args.serve_slots, 0)
     burst = reqs[: min(len(reqs), 300)]
-    wall_b, _, pts_b, _ = run(burst, args.serve_slots, 0)
+    wall_b, _, pts_b, st_b = run(burst, args.serve_slots, 0)
     cap = len(burst) / wall_b
     rate = 0.7 * cap
     wall, lat, pts, st = run(reqs, args.serve_slots, 0, rate=rate)
     lat = np.array(lat)
-    base = reqs[: min(len(reqs), 200)]
+    base = reqs[: min(len(reqs), args.serve_baseline)]
     # the baseline runs one request at a time: no batching either
     os.environ["FMM2D_B200_SERVE_BATCH"] = "0"
     try:
@@ -733,7 +735,14 @@ def measure_serving(fm, args):
         "throughput_points_s": pts / wall, "burst_points_s": pts_b / wall_b,
         "peak_running": st["peak_running"], "peak_budget_gb": st["peak_bytes"] / 1e9,
         "batched_requests": st.get("batched", 0),
+        "burst_batched_requests": st_b.get("batched", 0),
+        "batching_note": "small lfmm2d requests of one kind are batched when they meet in the "
+                         "queue: rarely at 70% load (short queues), often in the saturating burst; "
+                         "Helmholtz requests carry their own zk (tables) and are not batched",
         "one_at_a_time_fp64": {"requests": len(base), "points_s": pts1 / wall1,
+                               "sample": "the first requests of the same stream (one at a time "
+                                         "they take about 8 ms each; all 20,000 would hold the GPU "
+                                         "for minutes)",
                                "req_s": len(base) / wall1,
                                "p50_ms": float(np.percentile(lat1, 50))},
         "points": "N log-uniform [1e3, 1e6], uniform or Gaussian blobs, host arrays",
