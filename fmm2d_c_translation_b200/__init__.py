@@ -17,7 +17,7 @@ import os
 
 import numpy as np
 
-__all__ = ["Output", "lfmm2d", "cfmm2d", "hfmm2d", "lib", "lib_path",
+__all__ = ["Output", "lfmm2d", "cfmm2d", "hfmm2d", "rfmm2d", "lib", "lib_path",
            "last_error", "tree_build", "FmmError", "Server", "Request",
            "make_request"]
 
@@ -138,9 +138,9 @@ def tree_build(sources, targets=None, ndiv=15, idivflag=0, lists=True):
 
 
 # ---------------------------------------------------------------------------
-# fmm2dpy-compatible front end (python/fmm2dpy/fmm2d.py:20 hfmm2d, :459
-# lfmm2d, :715 cfmm2d): same keyword arguments, array shapes and Output
-# fields.  Every call goes through the guru drivers of the C ABI.
+# fmm2dpy-compatible front end (python/fmm2dpy/fmm2d.py:20 hfmm2d, :201
+# rfmm2d, :459 lfmm2d, :715 cfmm2d): same keyword arguments, array shapes
+# and Output fields.  Every call goes through the guru drivers of the C ABI.
 # ---------------------------------------------------------------------------
 def _as_f(a, dtype):
     return np.asfortranarray(np.asarray(a, dtype=dtype))
@@ -148,6 +148,8 @@ def _as_f(a, dtype):
 
 def _run(kernel, *, eps, zk, sources, charges, dipstr, dipvec, targets, pg, pgt, nd):
     out = Output()
+    # strengths and outputs: complex, or real for the real-valued Laplace FMM
+    cdt = np.float64 if kernel == "r" else np.complex128
     sources = np.asarray(sources, dtype=np.float64)
     assert sources.shape[0] == 2, "The first dimension of sources must be 2"
     ns = sources.shape[1] if sources.ndim == 2 else 1
@@ -158,12 +160,12 @@ def _run(kernel, *, eps, zk, sources, charges, dipstr, dipvec, targets, pg, pgt,
     ifcharge = int(charges is not None)
     ifdipole = int(dipstr is not None or dipvec is not None)
     if ifcharge:
-        q = _as_f(charges, np.complex128)
+        q = _as_f(charges, cdt)
         assert q.size == nd * ns, "Charges must be of shape [nd,ns] (or [ns] for nd = 1)"
     else:
-        q = np.zeros(nd * ns, np.complex128)
+        q = np.zeros(nd * ns, cdt)
     if ifdipole:
-        d = _as_f(dipstr, np.complex128)
+        d = _as_f(dipstr, cdt)
         assert d.size == nd * ns, "Dipole strengths must be of shape [nd,ns] (or [ns])"
         if kernel != "c":
             v = _as_f(dipvec, np.float64)
@@ -171,7 +173,7 @@ def _run(kernel, *, eps, zk, sources, charges, dipstr, dipvec, targets, pg, pgt,
         else:
             v = np.zeros(1)
     else:
-        d = np.zeros(nd * ns, np.complex128)
+        d = np.zeros(nd * ns, cdt)
         v = np.zeros(nd * 2 * ns)
     if targets is not None:
         targets = np.asarray(targets, dtype=np.float64)
@@ -184,7 +186,7 @@ def _run(kernel, *, eps, zk, sources, charges, dipstr, dipvec, targets, pg, pgt,
 
     def alloc(n, comps):
         shape = (nd, n) if comps == 1 else (nd, comps, n)
-        return np.zeros(shape, np.complex128, order="F")
+        return np.zeros(shape, cdt, order="F")
 
     pot, grad, hess = alloc(ns, 1), alloc(ns, gc), alloc(ns, hc)
     pt, gt, ht = alloc(max(nt, 1), 1), alloc(max(nt, 1), gc), alloc(max(nt, 1), hc)
@@ -240,6 +242,16 @@ def lfmm2d(*, eps, sources, charges=None, dipstr=None, dipvec=None, targets=None
     u(x) = sum_j [c_j log|x - x_j| - d_j (v_j . (x - x_j)) / |x - x_j|^2]
     (fmm2dpy.lfmm2d); arguments and outputs as for hfmm2d."""
     return _run("l", eps=eps, zk=None, sources=sources, charges=charges, dipstr=dipstr,
+                dipvec=dipvec, targets=targets, pg=pg, pgt=pgt, nd=nd)
+
+
+def rfmm2d(*, eps, sources, charges=None, dipstr=None, dipvec=None, targets=None, pg=0,
+           pgt=0, nd=1):
+    """Real-valued Laplace FMM (fmm2dpy.rfmm2d, python/fmm2dpy/fmm2d.py:201),
+    u(x) = sum_j [c_j log|x - x_j| - d_j (v_j . (x - x_j)) / |x - x_j|^2] with
+    real charges c_j, dipole strengths d_j and dipole vectors v_j; real pot
+    (n) or (nd, n), grad (2, n) or (nd, 2, n), hess (3, n) or (nd, 3, n)."""
+    return _run("r", eps=eps, zk=None, sources=sources, charges=charges, dipstr=dipstr,
                 dipvec=dipvec, targets=targets, pg=pg, pgt=pgt, nd=nd)
 
 

@@ -73,3 +73,20 @@ def test_front_end_nd(fm, fam):
         oj = f(**kj)
         assert W.rel_err(out.pot[j], oj.pot) < 1e-12
         assert W.rel_err(out.gradtarg[j], oj.gradtarg) < 1e-12
+
+
+def test_rfmm2d_front_end(fm):
+    """fmm2dpy-style rfmm2d: real outputs equal the rfmm2d wrappers'."""
+    rng = np.random.default_rng(31)
+    ns, nt = 3000, 700
+    src, trg = rng.random((2, ns)), rng.random((2, nt))
+    q, d = rng.standard_normal(ns), rng.standard_normal(ns)
+    v = rng.standard_normal((2, ns))
+    out = fm.rfmm2d(eps=1e-9, sources=src, charges=q, dipstr=d, dipvec=v, targets=trg, pg=2,
+                    pgt=3)
+    assert out.ier == 0 and out.pot.dtype == np.float64
+    ref, ier = W.call_nd(fm.lib(), "r", "st_cd_h", 1e-9, src, 1, False, q, d, v, trg)
+    assert ier == 0
+    np.testing.assert_array_equal(out.pot, ref["pot"][:, 0])
+    np.testing.assert_array_equal(out.grad.T, ref["grad"][:, :, 0])
+    np.testing.assert_array_equal(out.hesstarg.T, ref["hesstarg"][:, :, 0])
