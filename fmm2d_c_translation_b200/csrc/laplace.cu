@@ -345,8 +345,16 @@ __global__ void __launch_bounds__(256) eval_far_points_kernel(
 // lanes forming G = 32 / T groups that split the staged sources and are
 // summed at the end.  Point differences are formed in FP64 in both
 // precisions.
-constexpr int kP2PStage = 128;
-constexpr int kP2PWarps = 4;
+// (compile-time sizes; -DFMM2D_P2P_STAGE / -DFMM2D_P2P_WARPS override them
+// for measurements of other shapes)
+#ifndef FMM2D_P2P_STAGE
+#define FMM2D_P2P_STAGE 128
+#endif
+#ifndef FMM2D_P2P_WARPS
+#define FMM2D_P2P_WARPS 4
+#endif
+constexpr int kP2PStage = FMM2D_P2P_STAGE;
+constexpr int kP2PWarps = FMM2D_P2P_WARPS;
 
 // Point positions as the near field reads them: FP64 (x, y), or for the
 // mixed pass a float4 (x_hi, x_lo, y_hi, y_lo) with x = x_hi + x_lo, whose
