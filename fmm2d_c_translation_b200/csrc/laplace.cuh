@@ -113,6 +113,9 @@ bool m2l_fp32(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 
 // turns it off.
 constexpr int kM2LExactFrom = 17;
 constexpr int kM2LExactRows = 4;
+// with Hessians requested the rows 0 .. 5: the Hessian at a leaf's points
+// takes its leading terms from L_2 .. L_5
+constexpr int kM2LExactRowsHess = 6;
 inline bool m2l_exact_rows(int p) {
     const char *e = getenv("FMM2D_B200_M2L_EXACT_ROWS");
     return p >= kM2LExactFrom && !(e && !strcmp(e, "0"));

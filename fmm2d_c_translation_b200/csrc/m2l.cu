@@ -1109,8 +1109,13 @@ bool m2l_fp32(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 
                                                 return m2l_work(T, P, kFp32Tile, s, x, done);
                                             });
         if (!okr) return false;
-        if (wr->ntiles > 0)
-            launch_fp32<20, kM2LExactRows>(*wr, T, P, fp32_tables(p, 20, s), mp32p, loc, s);
+        if (wr->ntiles > 0) {
+            const bool hess = std::max(P.sset.n > 0 ? P.sset.pgh : 0, P.tset.n > 0 ? P.tset.pgh : 0) >= 3;
+            if (hess)
+                launch_fp32<20, kM2LExactRowsHess>(*wr, T, P, fp32_tables(p, 20, s), mp32p, loc, s);
+            else
+                launch_fp32<20, kM2LExactRows>(*wr, T, P, fp32_tables(p, 20, s), mp32p, loc, s);
+        }
     }
     return true;
 }

@@ -769,7 +769,8 @@ bool win_plan(const Tree &T, const CauchyProblem &P, int CH, cudaStream_t s, Win
 }
 
 // ---------------------------------------------------------------------------
-// Rows 1 .. kM2LExactRows-1 of the run's locals in FP32 on the CUDA cores.
+// Rows 1 .. NR-1 of the run's locals in FP32 on the CUDA cores (NR = 4, or
+// 6 when Hessians are requested).
 // The tensor-core kernel's TF32 x 3 products hold 22 of FP32's 24 bits;
 // from order kM2LExactFrom on, these leading coefficients -- which carry
 // most of the gradient at a leaf's points -- are recomputed here from FP32
@@ -781,10 +782,10 @@ bool win_plan(const Tree &T, const CauchyProblem &P, int CH, cudaStream_t s, Win
 // window is read from shared memory by the 3 shifts and 4 child positions
 // that use it.
 // ---------------------------------------------------------------------------
-template <int CH, int HALF>
+template <int CH, int HALF, int NR>
 __global__ void __launch_bounds__(128) m2l_win_rows_kernel(WinArgs A,
                                                            const float2 *__restrict__ Trows) {
-    constexpr int TB = 128 / CH, WP = TB + 2, NR = kM2LExactRows;
+    constexpr int TB = 128 / CH, WP = TB + 2;
     constexpr int CS = HALF * CH + 1;  // padded column stride of the window
     __shared__ float2 sTr[kWinOffsets * NR * HALF];
     __shared__ float2 sWin[WP * CS];
@@ -848,18 +849,17 @@ __global__ void __launch_bounds__(128) m2l_win_rows_kernel(WinArgs A,
     }
 }
 
-// FP32 rows i < kM2LExactRows of the scaled shift for the 40 window offsets,
+// FP32 rows i < NR of the scaled shift for the 40 window offsets,
 // [offset][i][HALF], zero from the order on; cached per device.
-const float2 *win_row_tables(int p, int HALF, cudaStream_t s) {
+const float2 *win_row_tables(int p, int HALF, int NR, cudaStream_t s) {
     static std::mutex mu;
     static std::vector<std::pair<long, const float2 *>> cache;
     int dev;
     FMM_CUDA(cudaGetDevice(&dev));
-    const long key = ((long)dev << 20) | ((long)p << 8) | HALF;
+    const long key = ((long)dev << 24) | ((long)NR << 16) | ((long)p << 8) | HALF;
     std::lock_guard<std::mutex> g(mu);
     for (auto &e : cache)
         if (e.first == key) return e.second;
-    constexpr int NR = kM2LExactRows;
     std::vector<double> C((size_t)(NR + HALF + 1) * (NR + HALF + 1), 0.0);
     const int nc = NR + HALF + 1;
     for (int l = 0; l < nc; l++) {
@@ -930,7 +930,14 @@ void launch_win(const WinPlan &W, const WinTables &tb, const Tree &T, const Cauc
         FMM_CHECK_LAUNCH();
         if (m2l_exact_rows(P.p)) {
             const int g2 = std::max(1, std::min(r.second, kNumSM * 8));
-            m2l_win_rows_kernel<CH, HALF><<<g2, 128, 0, s>>>(a, win_row_tables(P.p, HALF, s));
+            const bool hess =
+                std::max(P.sset.n > 0 ? P.sset.pgh : 0, P.tset.n > 0 ? P.tset.pgh : 0) >= 3;
+            if (hess)
+                m2l_win_rows_kernel<CH, HALF, kM2LExactRowsHess><<<g2, 128, 0, s>>>(
+                    a, win_row_tables(P.p, HALF, kM2LExactRowsHess, s));
+            else
+                m2l_win_rows_kernel<CH, HALF, kM2LExactRows><<<g2, 128, 0, s>>>(
+                    a, win_row_tables(P.p, HALF, kM2LExactRows, s));
             FMM_CHECK_LAUNCH();
         }
     }
