@@ -593,11 +593,51 @@ void run_helmholtz(const FmmCall &c, CallCtx &ctx) {
     InBuf<double> dv_in;
     src_in.set(c.sources, ns, on_dev, s);
     trg_in.set(nt > 0 ? c.targ : nullptr, nt, on_dev, s);
-    if (c.ifcharge) chg_in.set(c.charge, (size_t)nd * ns, on_dev, s);
-    if (c.ifdipole) {
-        dip_in.set(c.dipstr, (size_t)nd * ns, on_dev, s);
-        dv_in.set(c.dipvec, (size_t)2 * nd * ns, on_dev, s);
+    // Host arrays: the strengths go to the device on the copy stream while
+    // the tree is built on s, and the outputs come back on it array by array.
+    cudaStream_t cs = on_dev ? nullptr : ctx.copy_stream();
+    std::vector<cudaEvent_t> evs;
+    auto event_on = [&](cudaStream_t st) {
+        cudaEvent_t e;
+        FMM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        evs.push_back(e);
+        FMM_CUDA(cudaEventRecord(e, st));
+        return e;
+    };
+    if (on_dev) {
+        if (c.ifcharge) chg_in.set(c.charge, (size_t)nd * ns, true, s);
+        if (c.ifdipole) {
+            dip_in.set(c.dipstr, (size_t)nd * ns, true, s);
+            dv_in.set(c.dipvec, (size_t)2 * nd * ns, true, s);
+        }
+    } else {
+        if (c.ifcharge) chg_in.own.alloc((size_t)nd * ns, s);
+        if (c.ifdipole) {
+            dip_in.own.alloc((size_t)nd * ns, s);
+            dv_in.own.alloc((size_t)2 * nd * ns, s);
+        }
+        FMM_CUDA(cudaStreamWaitEvent(cs, event_on(s), 0));  // the allocations are ordered on s
+        auto up = [&](auto &b, const double *h, size_t bytes) {
+            if (!b.own.get() || !h) return;
+            FMM_CUDA(cudaMemcpyAsync(b.own.get(), h, bytes, cudaMemcpyHostToDevice, cs));
+            b.ptr = b.own.get();
+        };
+        up(chg_in, c.charge, (size_t)nd * ns * sizeof(double2));
+        up(dip_in, c.dipstr, (size_t)nd * ns * sizeof(double2));
+        up(dv_in, c.dipvec, (size_t)2 * nd * ns * sizeof(double));
     }
+    const cudaEvent_t strengths_in = on_dev ? nullptr : event_on(cs);
+    std::vector<std::unique_ptr<OutBuf>> keep;  // output staging, alive until the copies end
+    // (declared after every buffer that a copy uses, so that on any exit the
+    // copies still in flight finish before those buffers are freed)
+    struct CopyGuard {
+        cudaStream_t c;
+        std::vector<cudaEvent_t> &e;
+        ~CopyGuard() {
+            if (c) cudaStreamSynchronize(c);
+            for (cudaEvent_t x : e) cudaEventDestroy(x);
+        }
+    } copy_guard{cs, evs};
     prof_mark("h2d", s);
     // hndiv2d (c_translation/src/hndiv2d.c) has the lndiv2d table
     const int ndiv = c.ndiv >= 0 ? c.ndiv : leaf_capacity(c.eps, ns, nt);
@@ -607,6 +647,7 @@ void run_helmholtz(const FmmCall &c, CallCtx &ctx) {
     compute_lists(T, s);
     prof_mark("lists", s);
     HelmInputs in;
+    if (strengths_in) FMM_CUDA(cudaStreamWaitEvent(s, strengths_in, 0));
     gather_helm(c, T, src_in.ptr, trg_in.ptr, chg_in.ptr, dip_in.ptr, dv_in.ptr, in, s);
     prof_mark("gather", s);
     src_in.own.release();
@@ -645,7 +686,8 @@ void run_helmholtz(const FmmCall &c, CallCtx &ctx) {
                       double *ugrad, double *uhess) {
         if (pgh <= 0 || n <= 0) return;
         auto one = [&](const DevBuf<double2> &b, double *user, int comps) {
-            OutBuf ob;
+            keep.emplace_back(new OutBuf());
+            OutBuf &ob = *keep.back();
             ob.set(user, (size_t)n * nd * comps, on_dev, s);
             const int w = nd * comps;
             const double2 *src = b.get();
@@ -654,8 +696,10 @@ void run_helmholtz(const FmmCall &c, CallCtx &ctx) {
                 const int64_t k = t / w, j = t % w;
                 dst[(int64_t)perm[k] * w + j] = src[t];
             });
-            ob.flush(s);
-            FMM_CUDA(cudaStreamSynchronize(s));
+            if (cs) {
+                FMM_CUDA(cudaStreamWaitEvent(cs, event_on(s), 0));
+                ob.flush(cs);
+            }
         };
         one(po, upot, 1);
         if (pgh >= 2) one(gr, ugrad, 2);
@@ -663,6 +707,8 @@ void run_helmholtz(const FmmCall &c, CallCtx &ctx) {
     };
     unsort(ns, T.isrc.get(), spgh, spot, sgrad, shess, c.pot, c.grad, c.hess);
     unsort(nt, T.itarg.get(), tpgh, tpot, tgrad, thess, c.pottarg, c.gradtarg, c.hesstarg);
+    if (cs) FMM_CUDA(cudaStreamWaitEvent(s, event_on(cs), 0));
+    FMM_CUDA(cudaStreamSynchronize(s));
     prof_mark("scatter_d2h", s);
     prof_end(s);
     if (c.timeinfo) prof_timeinfo(c.timeinfo);
