@@ -355,6 +355,9 @@ def main():
                     help="skip the other configurations (c1, c3, c4)")
     ap.add_argument("--configs", default="c1,c3,c4",
                     help="which of the other configurations to run (comma list)")
+    ap.add_argument("--c4-points", type=int, default=2_000_000,
+                    help="sources of the Helmholtz configuration (2e6 as named; smaller for "
+                         "profiler captures)")
     ap.add_argument("--serve-requests", type=int, default=20000)
     ap.add_argument("--serve-baseline", type=int, default=2000,
                     help="requests of the one-at-a-time FP64 baseline (a prefix of the stream)")
@@ -887,7 +890,7 @@ def measure_configs(fm, L, args):
         del d_src, d_trg, d_ds, d_nv, d_pot, d_pt
     if "c4" in want:
         # ---- c4 ----
-        n4 = 2_000_000
+        n4 = args.c4_points
         rng = np.random.default_rng(404)
         src = rng.random((n4, 2))
         q = rng.standard_normal(n4) + 1j * rng.standard_normal(n4)
@@ -919,7 +922,7 @@ def measure_configs(fm, L, args):
         h_ms = prof.get("h_m2l", 0.0)
         tf32 = measure_tf32_peak(L)
         m2l_ach = prof.get("#h_m2l_flops", 0.0) / (h_ms * 1e-3) / 1e12 if h_ms else None
-        out["c4"] = {"workload": "hfmm2d_s_cd_p uniform 2e6 zk 200 eps 1e-6 "
+        out["c4"] = {"workload": f"hfmm2d_s_cd_p uniform {n4:.0e} zk 200 eps 1e-6 "
                                  "(auto: mixed, TF32x3 tensor-core M2L on levels of order <= 23)",
                      "ms": ms, "points_s": n4 / (ms * 1e-3),
                      "phase_ms": {k: round(v, 3) for k, v in prof.items() if not k.startswith("#")},
