@@ -1512,8 +1512,14 @@ void helmholtz_fmm(const Tree &T, const HelmProblem &P, cudaStream_t s) {
     if (tc) FMM_CUDA(cudaMemsetAsync(tc_err.get(), 0, sizeof(int), s));
     bool tc_used = false;
     std::vector<char> tc_lev(nl + 1, 0);
+    const bool hf_on = !(getenv("FMM2D_B200_HELM_HF") && !strcmp(getenv("FMM2D_B200_HELM_HF"), "0"));
     for (int l = 2; l <= nl; l++) {
         if (!hl[l].flag) continue;
+        if (hf_on && helm_hf_level(hk::cabs_(zk) * T.boxsize[l] / (2.0 * pi), hl[l].rs)) {
+            helm_m2l_hf(T, l, hl[l].p, nd, hl[l].off, d_ct.get() + lt[l].m2l, mp.get(), loc.get(),
+                        sp, tp, s);
+            continue;
+        }
         if (tc && hl[l].p <= helm_m2l_tc_max_order()) {
             HtLevel hv;
             hv.level = l;

@@ -70,6 +70,15 @@ int helm_m2l_tc_max_order();
 bool helm_m2l_tc_level(const HtLevel &lv, const SlotPlan &spl, const double2 *mp, double2 *loc,
                        int *err, cudaStream_t s);
 
+// High-frequency levels (helm_hf.cu): boxes of more than 16 wavelengths
+// (boxlam = |zk| boxsize / 2 pi > 16, the reference's switch) with scale 1,
+// where the M2L runs in the diagonal (signature) form.
+bool helm_hf_level(double boxlam, double rs);
+// The M2L of level l in the diagonal form: d_table is the level's M2L
+// table [49][4p + 1] (device), off the level's offset in mp / loc.
+void helm_m2l_hf(const Tree &T, int l, int p, int nd, long long off, const double2 *d_table,
+                 const double2 *mp, double2 *loc, int sp, int tp, cudaStream_t s);
+
 // Host restatements of the reference's scalar routines.
 // h2dterms (c_translation/src/h2dterms.c:19-69): expansion order for a box
 // of size bsize; -1 when no order up to 50000 reaches eps.

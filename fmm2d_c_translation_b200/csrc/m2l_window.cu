@@ -787,8 +787,10 @@ __global__ void __launch_bounds__(128) m2l_win_rows_kernel(WinArgs A,
                                                            const float2 *__restrict__ Trows) {
     constexpr int TB = 128 / CH, WP = TB + 2;
     constexpr int CS = HALF * CH + 1;  // padded column stride of the window
-    __shared__ float2 sTr[kWinOffsets * NR * HALF];
-    __shared__ float2 sWin[WP * CS];
+    // (dynamic: with six rows the tables and the window exceed 48 KB)
+    extern __shared__ float2 rows_smem[];
+    float2 *sTr = rows_smem;                         // [kWinOffsets * NR * HALF]
+    float2 *sWin = rows_smem + kWinOffsets * NR * HALF;  // [WP * CS]
     const int tid = threadIdx.x, tcol = tid / CH, chn = tid - tcol * CH;
     for (int e = tid; e < kWinOffsets * NR * HALF; e += blockDim.x) sTr[e] = Trows[e];
     const int P = A.p + 1, stride = P * A.ndc;
@@ -932,12 +934,16 @@ void launch_win(const WinPlan &W, const WinTables &tb, const Tree &T, const Cauc
             const int g2 = std::max(1, std::min(r.second, kNumSM * 8));
             const bool hess =
                 std::max(P.sset.n > 0 ? P.sset.pgh : 0, P.tset.n > 0 ? P.tset.pgh : 0) >= 3;
+            auto rows = [&](auto kern, int nr) {
+                const size_t sm = (size_t)(kWinOffsets * nr * HALF + (128 / CH + 2) * (HALF * CH + 1)) *
+                                  sizeof(float2);
+                raise_smem_limit((const void *)kern, sm);
+                kern<<<g2, 128, sm, s>>>(a, win_row_tables(P.p, HALF, nr, s));
+            };
             if (hess)
-                m2l_win_rows_kernel<CH, HALF, kM2LExactRowsHess><<<g2, 128, 0, s>>>(
-                    a, win_row_tables(P.p, HALF, kM2LExactRowsHess, s));
+                rows(m2l_win_rows_kernel<CH, HALF, kM2LExactRowsHess>, kM2LExactRowsHess);
             else
-                m2l_win_rows_kernel<CH, HALF, kM2LExactRows><<<g2, 128, 0, s>>>(
-                    a, win_row_tables(P.p, HALF, kM2LExactRows, s));
+                rows(m2l_win_rows_kernel<CH, HALF, kM2LExactRows>, kM2LExactRows);
             FMM_CHECK_LAUNCH();
         }
     }

@@ -277,3 +277,23 @@ def test_hfmm2d_zk200_against_reference(glib):
     # and both against the direct sum at 200 sources, to the requested eps
     pot, _, _ = h_direct(glib, zk, src, q, d, v, src[:, :200], 1, 1, 1)
     assert W.rel_err(out["pot"][:200], pot) < 1e-6
+
+
+@pytest.mark.parametrize("zk", [1500.0 + 0j, 900.0 + 0j])
+def test_high_frequency_diagonal_m2l(glib, monkeypatch, zk):
+    """Levels of more than 16 wavelengths per box take the M2L in the
+    diagonal (signature) form (helm_hf.cu); it applies the same truncated
+    operator as the coefficient-space shift, so the two agree to round-off,
+    and both stay within eps of the direct sum."""
+    src, trg, q, d, v = inputs(ns=30000, nt=4000, seed=15)
+    eps = 1e-6
+    out, ier = W.call(glib, "h", "st_cd_g", eps, src, q, d, v, trg, zk=zk)
+    assert ier == 0
+    monkeypatch.setenv("FMM2D_B200_HELM_HF", "0")
+    oc, ier = W.call(glib, "h", "st_cd_g", eps, src, q, d, v, trg, zk=zk)
+    assert ier == 0
+    for k in out:
+        assert W.rel_err(out[k], oc[k]) < 1e-11, (k, W.rel_err(out[k], oc[k]))
+    pot, grad, _ = h_direct(glib, zk, src, q, d, v, trg[:, :100], 2, 1, 1)
+    assert W.rel_err(out["pottarg"][:100], pot) < eps
+    assert W.rel_err(out["gradtarg"][:100], grad) < eps
