@@ -33,9 +33,13 @@
 // contiguous block of the per-level images, also cp.async) into one of
 // kHtStages shared-memory stages.  Warps 0-3 (one thread per A row) fill
 // the stages, keeping kHtLag groups of copies in flight; warp 8 issues
-// 3 x 2 MMAs per step and commits the stage back; warps 4-7 read the
-// finished accumulator (double-buffered in tensor memory) and add it to the
-// local expansions.  Every wait is bounded in time; a wait that runs out
+// 3 x 2 MMAs per step and commits the stage back.  Each slot accumulates
+// in a fresh tensor-memory tile (two alternate), and warps 4-7 add every
+// slot's tile to FP64 sums in shared memory: the FP32 accumulation then
+// spans one slot's K chunks (a few tens of MMAs) instead of all 27 slots,
+// whose hundreds of FP32 roundings measured 4e-6 relative in the
+// potential.  At the end of a tile the FP64 sums are added to the local
+// expansions.  Every wait is bounded in time; a wait that runs out
 // stops all roles of the block, sets *err, and the block still frees its
 // tensor memory after its MMAs have completed.
 #include "helmholtz.cuh"
@@ -50,7 +54,7 @@ namespace fmm2d {
 namespace {
 
 constexpr int kHtRows = 128;
-constexpr int kHtStages = 6;
+constexpr int kHtStages = 4;
 constexpr int kHtLag = 2;
 constexpr int kHtEpi0 = 4;             // warps 4-7 read the accumulators
 constexpr int kHtThreads = 9 * 32;     // warp 8 issues the MMAs
@@ -98,6 +102,9 @@ __global__ void __launch_bounds__(kHtThreads, 1) helm_m2l_tc_kernel(HtArgs A) {
     constexpr uint32_t IDESC = tc_idesc_tf32(kHtRows, NP);
     static_assert(KP % 16 == 0 && NP % 16 == 0 && NP <= 128, "operand shape");
     extern __shared__ __align__(1024) unsigned char ht_smem[];
+    // FP64 sums of the slots' partial products, column-major [NP][128] (the
+    // epilogue thread of row r owns column entries c * 128 + r)
+    double *sSum = reinterpret_cast<double *>(ht_smem + (size_t)kHtStages * STAGE);
     // barriers: [0, S) stage full, [S, 2S) stage free, 2S + a accumulator a
     // full, 2S + 2 + a accumulator a free, 2S + 4 final
     __shared__ __align__(8) uint64_t s_bar[2 * kHtStages + 5];
@@ -197,32 +204,43 @@ __global__ void __launch_bounds__(kHtThreads, 1) helm_m2l_tc_kernel(HtArgs A) {
         }
     } else if (warp < kHtEpi0 + 4) {
         // -------------------------------------------------------- epilogue
+        // Each slot's products accumulate in a fresh tensor-memory tile
+        // (two alternate between slots); this thread adds its row of every
+        // slot's tile in FP64, so the FP32 accumulation spans only the
+        // slot's own K chunks.
         const int e = warp - kHtEpi0;  // tensor-memory lanes 32 e .. 32 e + 31
         const int r = (e << 5) + lane;
         const int bx = r / A.nd, ch = r - bx * A.nd;
-        int tl = 0;
+        long long g = 0;  // slots finished by this block
         bool ok = true;
-        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, tl++) {
-            const int a = tl & 1;
-            const bool got = mbar_wait_backoff(HBAR(2 * kHtStages + a), (uint32_t)((tl >> 1) & 1),
-                                               abort_flag, A.wait_ns);
-            if (!__all_sync(0xffffffffu, got)) {
-                ok = false;
-                break;
-            }
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t taddr = tmem + ((uint32_t)(e << 5) << 16) + (uint32_t)(a * 128);
-            float d[NP];
+        for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x) {
+#pragma unroll 4
+            for (int c = 0; c < NP; c++) sSum[c * kHtRows + r] = 0.0;
+            for (int k = 0; k < kHtSlots; k++, g++) {
+                const int a = (int)(g & 1);
+                const bool got = mbar_wait_backoff(HBAR(2 * kHtStages + a), (uint32_t)((g >> 1) & 1),
+                                                   abort_flag, A.wait_ns);
+                if (!__all_sync(0xffffffffu, got)) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t taddr = tmem + ((uint32_t)(e << 5) << 16) + (uint32_t)(a * 128);
+                float d[NP];
 #pragma unroll
-            for (int c8 = 0; c8 < NP / 8; c8++) {
-                float v[8];
-                tc_ld8(taddr + (uint32_t)(8 * c8), v);
+                for (int c8 = 0; c8 < NP / 8; c8++) {
+                    float v[8];
+                    tc_ld8(taddr + (uint32_t)(8 * c8), v);
 #pragma unroll
-                for (int i = 0; i < 8; i++) d[8 * c8 + i] = v[i];
+                    for (int i = 0; i < 8; i++) d[8 * c8 + i] = v[i];
+                }
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                mbar_arrive(HBAR(2 * kHtStages + 2 + a));
+#pragma unroll
+                for (int c = 0; c < NP; c++) sSum[c * kHtRows + r] += (double)d[c];
             }
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            mbar_arrive(HBAR(2 * kHtStages + 2 + a));
+            if (!ok) break;
             int cp, q0;
             tile_seg(tile, cp, q0);
             const int q = q0 + bx;
@@ -231,36 +249,37 @@ __global__ void __launch_bounds__(kHtThreads, 1) helm_m2l_tc_kernel(HtArgs A) {
                 double *o = reinterpret_cast<double *>(A.locl + (size_t)(b - A.lstart) * A.W * A.nd + ch);
                 const size_t st = 2 * (size_t)A.nd;
                 // column c: Re L_(c - p) for c < W, Im L_(c - W - p) for W <= c < 2W
-#pragma unroll
-                for (int c = 0; c < NP; c++) {
+                for (int c = 0; c < 2 * A.W; c++) {
+                    const double v = A.oscale * sSum[c * kHtRows + r];
                     if (c < A.W)
-                        o[(size_t)c * st] += A.oscale * (double)d[c];
-                    else if (c < 2 * A.W)
-                        o[(size_t)(c - A.W) * st + 1] += A.oscale * (double)d[c];
+                        o[(size_t)c * st] += v;
+                    else
+                        o[(size_t)(c - A.W) * st + 1] += v;
                 }
             }
         }
         if (!ok) *abort_flag = 1;
     } else {
         // ---------------------------------------------------------- issuer
-        long long step = 0;
-        int tl = 0;
+        long long step = 0, g = 0;
         bool ok = true, issued = false;
         // (fault injection: nothing is issued or committed, so the other
         // roles' bounded waits run out)
-        for (int tile = blockIdx.x; ok && !A.stall && tile < ntiles; tile += gridDim.x, tl++) {
-            const int a = tl & 1;
-            const bool freed = tl < 2 || mbar_wait_bounded(HBAR(2 * kHtStages + 2 + a),
-                                                           (uint32_t)(((tl >> 1) - 1) & 1), abort_flag,
-                                                           A.wait_ns);
-            if (!__all_sync(0xffffffffu, freed)) {
-                ok = false;
-                break;
-            }
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t dt = tmem + (uint32_t)(a * 128);
-            uint32_t acc = 0u;
-            for (int k = 0; ok && k < kHtSlots; k++) {
+        for (int tile = blockIdx.x; ok && !A.stall && tile < ntiles; tile += gridDim.x) {
+            for (int k = 0; ok && k < kHtSlots; k++, g++) {
+                // the slot's accumulator tile, once the epilogue has read it
+                // two slots ago
+                const int a = (int)(g & 1);
+                const bool freed = g < 2 || mbar_wait_bounded(HBAR(2 * kHtStages + 2 + a),
+                                                              (uint32_t)(((g >> 1) - 1) & 1),
+                                                              abort_flag, A.wait_ns);
+                if (!__all_sync(0xffffffffu, freed)) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t dt = tmem + (uint32_t)(a * 128);
+                uint32_t acc = 0u;
                 for (int kc = 0; kc < KC; kc++, step++) {
                     const int s = (int)(step % kHtStages);
                     const long long u = step / kHtStages;
@@ -290,10 +309,10 @@ __global__ void __launch_bounds__(kHtThreads, 1) helm_m2l_tc_kernel(HtArgs A) {
                     __syncwarp();
                     issued = true;
                 }
+                if (!ok) break;
+                if (lane == 0) tc_commit(HBAR(2 * kHtStages + a));
+                __syncwarp();
             }
-            if (!ok) break;
-            if (lane == 0) tc_commit(HBAR(2 * kHtStages + a));
-            __syncwarp();
         }
         if (!ok) *abort_flag = 1;
         // the MMAs still in flight finish before the tensor memory is freed
@@ -317,7 +336,8 @@ __global__ void __launch_bounds__(kHtThreads, 1) helm_m2l_tc_kernel(HtArgs A) {
 
 template <int KP, int NP>
 constexpr size_t ht_smem_bytes() {
-    return (size_t)kHtStages * (2 * kHtRows * 16 * 4 + 2 * NP * 16 * 4);
+    return (size_t)kHtStages * (2 * kHtRows * 16 * 4 + 2 * NP * 16 * 4) +
+           (size_t)NP * kHtRows * sizeof(double);
 }
 
 // x rounded to TF32 (nearest, ties away from zero), as cvt.rna does.

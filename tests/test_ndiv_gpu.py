@@ -104,7 +104,7 @@ def test_ndiv_matches_default_driver_at_the_rule(glib):
     ndiv = glib.fmm2d_b200_leaf_capacity(ctypes.c_double(EPS), 2000, 900)
     ier, got, _ = _call(glib, "l", nd, src, q, d, v, trg, ndiv, 0, 1)
     assert ier == 0, fm.last_error()
-    want, ier2 = W.call(glib, "l", "st_cd_h", EPS, src, q[:, 0], d[:, 0], v[:, :, 0], trg)
+    want, ier2 = W.call(glib, "l", "st_cd_h", EPS, src, q[:, 0], d[:, 0], v[:, :, 0].T, trg)
     assert ier2 == 0
     assert W.rel_err(got[0][:, 0], want["pot"]) <= 1e-14
     assert W.rel_err(got[3][:, 0], want["pottarg"]) <= 1e-14
