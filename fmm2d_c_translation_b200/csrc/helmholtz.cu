@@ -1188,6 +1188,146 @@ __global__ void __launch_bounds__(128) helm_p2p_kernel(
     }
 }
 
+// P2P over list 1 for one point set with one warp per leaf (nd = 1): the
+// leaf's list-1 sources are staged in shared memory in chunks, and the
+// (target, source block) items of up to 32 targets are dealt to the lanes,
+// each item summing its block into registers; the target's lane then adds
+// the blocks' partial sums in block order.  Every lane runs the same
+// number of pairs, where one thread per target ran as many pairs as its
+// own leaf's list 1 held (lanes of one warp spanning leaves of different
+// sizes idled).  Deterministic: every sum has a fixed order.
+constexpr int kHfStage = 64;
+constexpr int kHfWarps = 4;
+constexpr int kHfItems = 64;
+
+template <int PGH>
+constexpr int hf_outs() { return PGH >= 3 ? 6 : (PGH >= 2 ? 3 : 1); }
+
+template <int PGH>
+constexpr size_t helm_p2p_flat_warp_bytes() {
+    return (size_t)kHfStage * 4 * sizeof(double2) + 32 * sizeof(double2) +
+           (size_t)kHfItems * hf_outs<PGH>() * sizeof(double2);
+}
+
+template <int PGH, bool REALK>
+__global__ void __launch_bounds__(kHfWarps * 32) helm_p2p_flat_kernel(
+    int nb, const int *__restrict__ nchild, const int2 *__restrict__ tse,
+    const double2 *__restrict__ pos, const int *__restrict__ nlist1,
+    const int *__restrict__ list1, const int2 *__restrict__ sse, const double2 *__restrict__ src,
+    const double2 *__restrict__ charge, const double2 *__restrict__ dipstr,
+    const double2 *__restrict__ dipvec, int ifc, int ifd, double2 zk, double thresh,
+    double2 *__restrict__ pot, double2 *__restrict__ grad, double2 *__restrict__ hess) {
+    constexpr int NO = hf_outs<PGH>();
+    extern __shared__ __align__(16) unsigned char hf_smem[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    double2 *s_pos = reinterpret_cast<double2 *>(hf_smem + (size_t)wib * helm_p2p_flat_warp_bytes<PGH>());
+    double2 *s_q = s_pos + kHfStage, *s_d = s_q + kHfStage, *s_v = s_d + kHfStage;
+    double2 *s_tgt = s_v + kHfStage;
+    double2 *part = s_tgt + 32;
+    const bool le = ifc && !ifd && PGH == 1;
+    const double2 zero = make_double2(0.0, 0.0);
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nb; b += nwarps) {
+        if (nchild[b] != 0) continue;
+        const int2 tr = tse[b];
+        const int ntot = tr.y - tr.x;
+        const int n1 = nlist1[b];
+        if (ntot <= 0 || n1 == 0) continue;
+        int jstart = 0, jcount = 0;  // lane e < n1 holds list-1 entry e
+        if (lane < n1) {
+            const int2 r = sse[list1[b * 13 + lane]];
+            jstart = r.x;
+            jcount = r.y - r.x;
+        }
+        int jofs = jcount;
+#pragma unroll
+        for (int dd = 1; dd < 16; dd <<= 1) {
+            const int o = __shfl_up_sync(0xffffffffu, jofs, dd);
+            if (lane >= dd) jofs += o;
+        }
+        const int nsrc = __shfl_sync(0xffffffffu, jofs, n1 - 1);
+        jofs -= jcount;
+        if (nsrc == 0) continue;
+        const int nchunk = (ntot + 31) / 32, T0 = (ntot + nchunk - 1) / nchunk;
+        const int ns_eff = min(nsrc, kHfStage);
+        for (int t0 = 0; t0 < ntot; t0 += T0) {
+            const int T = min(T0, ntot - t0);
+            __syncwarp();
+            if (lane < T) s_tgt[lane] = pos[tr.x + t0 + lane];
+            int B = 1, best = 1 << 30;
+            for (int bb = 1; bb * T <= kHfItems; bb++) {
+                const int cost = ((T * bb + 31) >> 5) * ((ns_eff + bb - 1) / bb);
+                if (cost < best) {
+                    best = cost;
+                    B = bb;
+                }
+            }
+            const int nit = T * B;
+            Acc tot;
+            tot.zero();
+            for (int s0 = 0; s0 < nsrc; s0 += kHfStage) {
+                const int nst = min(kHfStage, nsrc - s0);
+                __syncwarp();
+                for (int i0 = 0; i0 < nst; i0 += 32) {  // warp-uniform trip count
+                    const int i = i0 + lane, gi = s0 + i;
+                    int e = 0;
+                    for (int u = 1; u < n1; u++)
+                        if (__shfl_sync(0xffffffffu, jofs, u) <= gi) e = u;
+                    const int k = __shfl_sync(0xffffffffu, jstart, e) + gi -
+                                  __shfl_sync(0xffffffffu, jofs, e);
+                    if (i >= nst) continue;
+                    s_pos[i] = src[k];
+                    s_q[i] = ifc ? charge[k] : zero;
+                    s_d[i] = ifd ? dipstr[k] : zero;
+                    s_v[i] = ifd ? dipvec[k] : zero;
+                }
+                __syncwarp();
+                const int sb = (nst + B - 1) / B;
+                for (int it = lane; it < nit; it += 32) {
+                    const int t = it % T, blk = it / T;
+                    const double2 x = s_tgt[t];
+                    Acc a;
+                    a.zero();
+                    const int j1 = min(nst, blk * sb + sb);
+                    for (int kk = blk * sb; kk < j1; kk++) {
+                        const double2 y = s_pos[kk];
+                        pair_add<PGH, REALK>(a, x.x - y.x, x.y - y.y, zk, thresh, le, ifc, s_q[kk],
+                                             ifd, s_d[kk], s_v[kk]);
+                    }
+                    double2 *pp = part + (size_t)it * NO;
+                    pp[0] = a.p;
+                    if (PGH >= 2) {
+                        pp[1] = a.gx;
+                        pp[2] = a.gy;
+                    }
+                    if (PGH >= 3) {
+                        pp[3] = a.hxx;
+                        pp[4] = a.hxy;
+                        pp[5] = a.hyy;
+                    }
+                }
+                __syncwarp();
+                if (lane < T) {
+                    for (int blk = 0; blk < B; blk++) {
+                        const double2 *pp = part + (size_t)(lane + blk * T) * NO;
+                        tot.p = cadd(tot.p, pp[0]);
+                        if (PGH >= 2) {
+                            tot.gx = cadd(tot.gx, pp[1]);
+                            tot.gy = cadd(tot.gy, pp[2]);
+                        }
+                        if (PGH >= 3) {
+                            tot.hxx = cadd(tot.hxx, pp[3]);
+                            tot.hxy = cadd(tot.hxy, pp[4]);
+                            tot.hyy = cadd(tot.hyy, pp[5]);
+                        }
+                    }
+                }
+            }
+            if (lane < T) store_add<PGH>(tot, (long long)(tr.x + t0 + lane), 1, 0, pot, grad, hess);
+        }
+    }
+}
+
 // All-pairs direct sum for one point set (adds).
 template <int PGH, bool REALK>
 __global__ void __launch_bounds__(128) helm_direct_kernel(
@@ -1664,7 +1804,31 @@ void helmholtz_fmm(const Tree &T, const HelmProblem &P, cudaStream_t s) {
                                               T.list1.get(), T.srcse.get(), P.src, P.charge, \
                                               P.dipstr, P.dipvec, ifc, ifd, nd, zk, thresh,  \
                                               X.pot, X.grad, X.hess)
-        if (realk) {
+#define HP2PF(PG, RK)                                                                        \
+    do {                                                                                     \
+        constexpr size_t sm = kHfWarps * helm_p2p_flat_warp_bytes<PG>();                     \
+        auto kern = helm_p2p_flat_kernel<PG, RK>;                                            \
+        raise_smem_limit((const void *)kern, sm);                                            \
+        const int gw = std::max(1, std::min((nb + kHfWarps - 1) / kHfWarps, kNumSM * 16));   \
+        kern<<<gw, kHfWarps * 32, sm, s>>>(nb, T.nchild.get(), X.se, X.pos, T.nlist1.get(),   \
+                                          T.list1.get(), T.srcse.get(), P.src, P.charge,      \
+                                          P.dipstr, P.dipvec, ifc, ifd, zk, thresh, X.pot,    \
+                                          X.grad, X.hess);                                    \
+    } while (0)
+        // one warp per leaf (nd = 1; FMM2D_B200_HELM_P2P=point keeps a thread per point)
+        const char *pm = getenv("FMM2D_B200_HELM_P2P");
+        const bool flat = nd == 1 && !(pm && !strcmp(pm, "point"));
+        if (flat) {
+            if (realk) {
+                if (X.pgh == 1) HP2PF(1, true);
+                else if (X.pgh == 2) HP2PF(2, true);
+                else HP2PF(3, true);
+            } else {
+                if (X.pgh == 1) HP2PF(1, false);
+                else if (X.pgh == 2) HP2PF(2, false);
+                else HP2PF(3, false);
+            }
+        } else if (realk) {
             if (X.pgh == 1) HP2P(1, true);
             else if (X.pgh == 2) HP2P(2, true);
             else HP2P(3, true);
@@ -1674,6 +1838,7 @@ void helmholtz_fmm(const Tree &T, const HelmProblem &P, cudaStream_t s) {
             else HP2P(3, false);
         }
 #undef HP2P
+#undef HP2PF
         FMM_CHECK_LAUNCH();
         prof_mark(set == 0 ? "h_p2p_src" : "h_p2p_trg", s);
     }

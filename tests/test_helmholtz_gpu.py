@@ -297,3 +297,18 @@ def test_high_frequency_diagonal_m2l(glib, monkeypatch, zk):
     pot, grad, _ = h_direct(glib, zk, src, q, d, v, trg[:, :100], 2, 1, 1)
     assert W.rel_err(out["pottarg"][:100], pot) < eps
     assert W.rel_err(out["gradtarg"][:100], grad) < eps
+
+
+@pytest.mark.parametrize("zk", [200.0 + 0j, 2.0 + 3.0j])
+@pytest.mark.parametrize("variant", ["st_cd_h", "s_c_p", "t_d_g"])
+def test_p2p_forms_agree(glib, monkeypatch, zk, variant):
+    """The near field with one warp per leaf (default for nd = 1) against one
+    thread per point: the same pairs summed in another order."""
+    src, trg, q, d, v = inputs(ns=20000, nt=5000, seed=23)
+    out, ier = W.call(glib, "h", variant, 1e-9, src, q, d, v, trg, zk=zk)
+    assert ier == 0
+    monkeypatch.setenv("FMM2D_B200_HELM_P2P", "point")
+    op, ier = W.call(glib, "h", variant, 1e-9, src, q, d, v, trg, zk=zk)
+    assert ier == 0
+    for k in out:
+        assert W.rel_err(out[k], op[k]) < 1e-13, (k, W.rel_err(out[k], op[k]))
