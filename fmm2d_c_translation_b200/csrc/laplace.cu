@@ -347,11 +347,15 @@ __global__ void __launch_bounds__(256) eval_far_points_kernel(
 // precisions.
 // (compile-time sizes; -DFMM2D_P2P_STAGE / -DFMM2D_P2P_WARPS override them
 // for measurements of other shapes)
+// (64 staged sources and 8 warps per block: measured on a B200, 10^7 +
+// 10^7 uniform points, mixed mode, the near field took 4.64 ms against
+// 5.53 ms with 128 sources and 4 warps -- less shared memory per warp,
+// more warps resident)
 #ifndef FMM2D_P2P_STAGE
-#define FMM2D_P2P_STAGE 128
+#define FMM2D_P2P_STAGE 64
 #endif
 #ifndef FMM2D_P2P_WARPS
-#define FMM2D_P2P_WARPS 4
+#define FMM2D_P2P_WARPS 8
 #endif
 constexpr int kP2PStage = FMM2D_P2P_STAGE;
 constexpr int kP2PWarps = FMM2D_P2P_WARPS;
