@@ -39,7 +39,9 @@
 // spans one slot's K chunks (a few tens of MMAs) instead of all 27 slots,
 // whose hundreds of FP32 roundings measured 4e-6 relative in the
 // potential.  At the end of a tile the FP64 sums are added to the local
-// expansions.  Every wait is bounded in time; a wait that runs out
+// expansions.  Levels with fewer tiles than SMs split the 27 slots over
+// slices of blocks (grid rows), each writing FP64 partial sums that a
+// second kernel adds in slice order.  Every wait is bounded in time; a wait that runs out
 // stops all roles of the block, sets *err, and the block still frees its
 // tensor memory after its MMAs have completed.
 #include "helmholtz.cuh"
@@ -78,6 +80,11 @@ struct HtArgs {
     int *err;
     int stall;                 // fault injection: the issuer issues nothing
     unsigned long long wait_ns;  // limit of every bounded wait
+    // slot slices (levels with fewer tiles than SMs): block row y takes the
+    // slots [27 y / gridDim.y, 27 (y + 1) / gridDim.y) and, with more than
+    // one slice, writes its FP64 partial sums to part[y][plan row - q_lo][W][nd]
+    double2 *part;
+    int q_lo, nq;
 };
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, uint32_t bytes) {
@@ -139,6 +146,8 @@ __global__ void __launch_bounds__(kHtThreads, 1) helm_m2l_tc_kernel(HtArgs A) {
     const uint32_t tmem = s_tmem;
     const uint32_t sbase = smem_u32(ht_smem);
     const int ntiles = A.tb[4] - A.tb[0];
+    const int k0 = (int)blockIdx.y * kHtSlots / (int)gridDim.y;
+    const int k1 = ((int)blockIdx.y + 1) * kHtSlots / (int)gridDim.y;
     // segment (child position) and first plan row of a tile
     auto tile_seg = [&](int tile, int &cp, int &q0) {
         const int t = A.tb[0] + tile;
@@ -160,7 +169,7 @@ __global__ void __launch_bounds__(kHtThreads, 1) helm_m2l_tc_kernel(HtArgs A) {
             const int q = q0 + bx;
             const bool valid = bx < A.tpt && q < A.start[cp] + A.count[cp];
             const int *qs = A.slots + (size_t)(valid ? q : 0) * kHtSlots;
-            for (int k = 0; ok && k < kHtSlots; k++) {
+            for (int k = k0; ok && k < k1; k++) {
                 const int sb = valid ? __ldg(qs + k) : -1;
                 const float *src = A.arow + (sb >= 0 ? ((size_t)(sb - A.lstart) * A.nd + ch) * 2 * KP : 0);
                 const uint32_t abytes = sb >= 0 ? 16u : 0u;  // 0: zero fill
@@ -216,7 +225,7 @@ __global__ void __launch_bounds__(kHtThreads, 1) helm_m2l_tc_kernel(HtArgs A) {
         for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x) {
 #pragma unroll 4
             for (int c = 0; c < NP; c++) sSum[c * kHtRows + r] = 0.0;
-            for (int k = 0; k < kHtSlots; k++, g++) {
+            for (int k = k0; k < k1; k++, g++) {
                 const int a = (int)(g & 1);
                 const bool got = mbar_wait_backoff(HBAR(2 * kHtStages + a), (uint32_t)((g >> 1) & 1),
                                                    abort_flag, A.wait_ns);
@@ -245,16 +254,22 @@ __global__ void __launch_bounds__(kHtThreads, 1) helm_m2l_tc_kernel(HtArgs A) {
             tile_seg(tile, cp, q0);
             const int q = q0 + bx;
             if (bx < A.tpt && q < A.start[cp] + A.count[cp]) {
-                const int b = A.boxes[q];
-                double *o = reinterpret_cast<double *>(A.locl + (size_t)(b - A.lstart) * A.W * A.nd + ch);
+                double *o;
+                bool add = true;
+                if (gridDim.y > 1) {  // this slice's partial sums
+                    o = reinterpret_cast<double *>(
+                        A.part + ((size_t)blockIdx.y * A.nq + (q - A.q_lo)) * A.W * A.nd + ch);
+                    add = false;
+                } else {
+                    const int b = A.boxes[q];
+                    o = reinterpret_cast<double *>(A.locl + (size_t)(b - A.lstart) * A.W * A.nd + ch);
+                }
                 const size_t st = 2 * (size_t)A.nd;
                 // column c: Re L_(c - p) for c < W, Im L_(c - W - p) for W <= c < 2W
                 for (int c = 0; c < 2 * A.W; c++) {
                     const double v = A.oscale * sSum[c * kHtRows + r];
-                    if (c < A.W)
-                        o[(size_t)c * st] += v;
-                    else
-                        o[(size_t)(c - A.W) * st + 1] += v;
+                    double &dst = c < A.W ? o[(size_t)c * st] : o[(size_t)(c - A.W) * st + 1];
+                    dst = add ? dst + v : v;
                 }
             }
         }
@@ -266,7 +281,7 @@ __global__ void __launch_bounds__(kHtThreads, 1) helm_m2l_tc_kernel(HtArgs A) {
         // (fault injection: nothing is issued or committed, so the other
         // roles' bounded waits run out)
         for (int tile = blockIdx.x; ok && !A.stall && tile < ntiles; tile += gridDim.x) {
-            for (int k = 0; ok && k < kHtSlots; k++, g++) {
+            for (int k = k0; ok && k < k1; k++, g++) {
                 // the slot's accumulator tile, once the epilogue has read it
                 // two slots ago
                 const int a = (int)(g & 1);
@@ -411,12 +426,28 @@ __global__ void __launch_bounds__(256) helm_tc_bimg_kernel(int p, int KP, int NP
 }
 
 template <int KP, int NP>
-void launch_ht(const HtArgs &a, int ntiles, cudaStream_t s) {
+void launch_ht(const HtArgs &a, int ntiles, int nslice, cudaStream_t s) {
     const size_t smem = ht_smem_bytes<KP, NP>();
     raise_smem_limit((const void *)helm_m2l_tc_kernel<KP, NP>, smem);
-    const int blocks = std::max(1, std::min(ntiles, kNumSM));
-    helm_m2l_tc_kernel<KP, NP><<<blocks, kHtThreads, smem, s>>>(a);
+    const dim3 grid(std::max(1, std::min(ntiles, kNumSM)), nslice);
+    helm_m2l_tc_kernel<KP, NP><<<grid, kHtThreads, smem, s>>>(a);
     FMM_CHECK_LAUNCH();
+}
+
+// The slices' partial sums, added in slice order to the local expansions
+// of the level's plan rows.
+__global__ void __launch_bounds__(256) helm_tc_slices_kernel(
+    int nq, int wf, int nslice, const double2 *__restrict__ part, const int *__restrict__ boxes,
+    int q_lo, int lstart, double2 *__restrict__ locl) {
+    const long long n = (long long)nq * wf;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int q = (int)(t / wf), o = (int)(t - (long long)q * wf);
+        double2 acc = make_double2(0.0, 0.0);
+        for (int y = 0; y < nslice; y++) acc = cadd(acc, part[(size_t)y * n + t]);
+        double2 *dst = locl + (size_t)(boxes[q_lo + q] - lstart) * wf + o;
+        *dst = cadd(*dst, acc);
+    }
 }
 
 }  // namespace
@@ -477,13 +508,27 @@ bool helm_m2l_tc_level(const HtLevel &lv, const SlotPlan &spl, const double2 *mp
     a.err = err;
     a.stall = tc_stall_injected();
     a.wait_ns = tc_wait_limit_ns();
+    // levels with fewer tiles than SMs (the coarse ones) split the 27 slots
+    // over slices of blocks, whose FP64 partial sums are added in slice order
+    const int nslice = ntiles < kNumSM ? std::min(kHtSlots, std::max(1, kNumSM / ntiles)) : 1;
+    a.q_lo = a.start[0];
+    a.nq = a.start[3] + a.count[3] - a.q_lo;
+    DevBuf<double2> part(nslice > 1 ? (size_t)nslice * a.nq * W * nd : 0, s);
+    a.part = part.get();
     switch (KP) {
-        case 32: launch_ht<32, 32>(a, ntiles, s); break;
-        case 48: launch_ht<48, 48>(a, ntiles, s); break;
-        case 64: launch_ht<64, 64>(a, ntiles, s); break;
-        case 80: launch_ht<80, 80>(a, ntiles, s); break;
-        case 96: launch_ht<96, 96>(a, ntiles, s); break;
+        case 32: launch_ht<32, 32>(a, ntiles, nslice, s); break;
+        case 48: launch_ht<48, 48>(a, ntiles, nslice, s); break;
+        case 64: launch_ht<64, 64>(a, ntiles, nslice, s); break;
+        case 80: launch_ht<80, 80>(a, ntiles, nslice, s); break;
+        case 96: launch_ht<96, 96>(a, ntiles, nslice, s); break;
         default: return false;
+    }
+    if (nslice > 1) {
+        const long long n = (long long)a.nq * W * nd;
+        const int blocks = (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, kNumSM * 8));
+        helm_tc_slices_kernel<<<blocks, 256, 0, s>>>(a.nq, W * nd, nslice, part.get(), spl.boxes,
+                                                     a.q_lo, lv.lstart, loc + lv.off);
+        FMM_CHECK_LAUNCH();
     }
     return true;
 }
