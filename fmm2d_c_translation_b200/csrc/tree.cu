@@ -59,6 +59,39 @@ __device__ __forceinline__ int key_digit(const KeyView &kv, int64_t k, int m) {
     return (int)((kv.w[w][k] >> sh) & 3u);
 }
 
+// Common leading digits (levels) of the sorted keys at positions a and b.
+__device__ __forceinline__ int key_lcp(const KeyView &kv, int nw, int64_t a, int64_t b) {
+    for (int w = 0; w < nw; w++) {
+        const uint32_t x = kv.w[w][a] ^ kv.w[w][b];
+        if (x) return 16 * w + (__clz(x) >> 1);
+    }
+    return 16 * nw;
+}
+
+// Number of boxes of every level 1..ds that hold more than ndiv of the
+// n key-sorted points: a box of level l is a run of equal l-digit prefixes,
+// and the run starting at k (a start when the prefix differs from k-1's,
+// i.e. l > lcp(k-1, k)) holds more than ndiv points when the point ndiv
+// further on still shares the prefix (l <= lcp(k, k + ndiv)).  Each point
+// adds one to the levels in (lcp(k-1, k), lcp(k, k + ndiv)].
+__global__ void __launch_bounds__(256) refine_count_kernel(KeyView kv, int64_t n, int ndiv,
+                                                           int ds, int nw,
+                                                           unsigned long long *__restrict__ cnt) {
+    __shared__ unsigned int sc[65];
+    for (int l = threadIdx.x; l <= 64; l += blockDim.x) sc[l] = 0;
+    __syncthreads();
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        if (k + ndiv >= n) continue;
+        const int a = k == 0 ? 0 : key_lcp(kv, nw, k - 1, k);
+        const int b = min(key_lcp(kv, nw, k, k + ndiv), ds);
+        for (int l = a + 1; l <= b; l++) atomicAdd(&sc[l], 1u);
+    }
+    __syncthreads();
+    for (int l = threadIdx.x; l <= 64; l += blockDim.x)
+        if (sc[l]) atomicAdd(&cnt[l], (unsigned long long)sc[l]);
+}
+
 // Path keys of n points: nw words per point, word-major (word w of point i
 // at words[w * n + i]); digits of levels beyond `ds` are 0.  bsl[m] is the
 // box size of level m, obtained by repeated halving as the reference does.
@@ -216,18 +249,22 @@ struct Builder {
     // tree_refine_boxes and, with set_flags, tree_refine_boxes_flag, whose
     // children get flag 3 under a flag-1 parent and 0 otherwise.  `sel` is
     // evaluated before any array grows.
+    // known >= 0: the caller knows the number of refined boxes (no host
+    // synchronisation); the device's own count goes to *check, and no child
+    // is written beyond the capacity in case the two differ.
     template <class Sel>
     int refine_range(int lo, int hi, int newlevel, double bs, Sel sel,
-                     bool set_flags) {
+                     bool set_flags, int known = -1, int *check = nullptr) {
         const int n = hi - lo;
         if (n <= 0) return 0;
         DevBuf<int> f(n, s), off(n, s), tot(1, s);
         int *fp = f.get();
         for_each(n, s, [=] __device__(int64_t i) { fp[i] = sel(lo + (int)i) ? 1 : 0; });
-        exclusive_scan_i32(fp, off.get(), n, tot.get(), s);
-        const int nref = read_scalar(tot.get(), s);
+        exclusive_scan_i32(fp, off.get(), n, check ? check : tot.get(), s);
+        const int nref = known >= 0 ? known : read_scalar(tot.get(), s);
         if (nref == 0) return 0;
         ensure(T.nboxes + 4 * nref);
+        const int cap = T.cap;
         const int nb0 = T.nboxes;
         double2 *cen = T.centers.get();
         int *lev = T.level.get(), *par = T.parent.get(), *nch = T.nchild.get();
@@ -238,6 +275,7 @@ struct Builder {
             if (!fp[i]) return;
             const int b = lo + (int)i;
             const int base = nb0 + 4 * op[i];
+            if (base + 4 > cap) return;  // (a known count that was wrong: caught by *check)
             const double2 c = cen[b];
             const int cf = (set_flags && flg[b] == 1) ? 3 : 0;
             nch[b] = 4;
@@ -948,9 +986,20 @@ struct ForestRoots {
     int pbits = 0;
 };
 
+// Refinement without a host synchronisation per level: for one tree split
+// on the source counts (idivflag 0) the number of boxes refined on every
+// level follows from the sorted keys alone (refine_count_kernel), so the
+// levels are built with known counts, each level's own device count is
+// checked against them at the end, and a mismatch rebuilds the tree the
+// synchronous way.  FMM2D_B200_TREE_SYNC=1 always takes the synchronous way.
+bool presized_refinement(const ForestRoots *F, int idivflag) {
+    const char *e = getenv("FMM2D_B200_TREE_SYNC");
+    return !F && idivflag == 0 && !(e && !strcmp(e, "1"));
+}
+
 bool build_by_keys(const double2 *d_src, int ns, const double2 *d_targ, int nt, int ndiv,
                    int idivflag, int nlmax, double2 c0, int ds, cudaStream_t s, Tree &T,
-                   const ForestRoots *F = nullptr) {
+                   const ForestRoots *F = nullptr, bool sync_levels = false) {
     const double bs0 = T.boxsize[0];
     T = Tree();
     T.boxsize.push_back(bs0);
@@ -989,15 +1038,45 @@ bool build_by_keys(const double2 *d_src, int ns, const double2 *d_targ, int nt, 
             r1[b] = to ? make_int2(to[b], to[b + 1]) : make_int2(0, nt);
         });
     }
+    // known refinement counts per level (presized form): level 0 from the
+    // source count, levels 1..ds from the keys, one synchronisation
+    const bool known = !sync_levels && presized_refinement(F, idivflag);
+    std::vector<unsigned long long> kc(65, 0);
+    DevBuf<int> chk(known ? nlmax + 1 : 0, s);
+    if (known) {
+        kc[0] = ns > ndiv ? 1 : 0;
+        if (ns > 0 && ds >= 1) {
+            DevBuf<unsigned long long> dc(65, s);
+            dc.zero(s);
+            const int nw = (ds + 15) / 16;
+            const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)ns + 255) / 256, kNumSM * 8));
+            refine_count_kernel<<<blocks, 256, 0, s>>>(B.kvs, ns, ndiv, ds, nw, dc.get());
+            FMM_CHECK_LAUNCH();
+            FMM_CUDA(cudaMemcpyAsync(kc.data() + 1, dc.get() + 1, 64 * sizeof(unsigned long long),
+                                     cudaMemcpyDeviceToHost, s));
+            FMM_CUDA(cudaStreamSynchronize(s));
+        }
+        // a box of the deepest digit level still to be split: more digits
+        if (ds < 64 && ds <= nlmax - 1 && kc[ds] > 0) return false;
+        long long tot = nroots;
+        for (int l = 0; l < std::min(ds, nlmax); l++) {
+            if (kc[l] == 0) break;
+            tot += 4 * (long long)kc[l];
+        }
+        if (tot > (long long)INT32_MAX / 20) throw FmmError(4, "tree too large");
+        B.ensure((int)tot);
+        chk.zero(s);
+    }
     DevBuf<int> nflag(1, s);
     int ilev = 0;
     for (ilev = 0; ilev <= nlmax - 1; ilev++) {
         const int lo = T.lstart[ilev], hi = T.lend[ilev];
         const int2 *ra = B.rs.get(), *rb = B.rt.get();
         const int dflag = idivflag, nd = ndiv;
+        const bool last = ilev + 1 > ds;
+        if (known && last) break;  // (no box of level ds is split: checked above)
         DevBuf<int> f(hi - lo, s);
         int *fp = f.get();
-        const bool last = ilev + 1 > ds;
         int *nf = nflag.get();
         if (last) nflag.zero(s);
         for_each(hi - lo, s, [=] __device__(int64_t i) {
@@ -1013,9 +1092,14 @@ bool build_by_keys(const double2 *d_src, int ns, const double2 *d_targ, int nt, 
         }
         T.boxsize.push_back(T.boxsize[ilev] / 2);
         const int nb0 = T.nboxes;
+        if (known && kc[ilev] == 0) {
+            T.boxsize.pop_back();
+            break;
+        }
         const int nref = B.refine_range(
             lo, hi, ilev + 1, T.boxsize[ilev + 1],
-            [=] __device__(int b) { return fp[b - lo] != 0; }, false);
+            [=] __device__(int b) { return fp[b - lo] != 0; }, false,
+            known ? (int)kc[ilev] : -1, known ? chk.get() + ilev : nullptr);
         if (nref == 0) {
             T.boxsize.pop_back();
             break;
@@ -1024,6 +1108,18 @@ bool build_by_keys(const double2 *d_src, int ns, const double2 *d_targ, int nt, 
         T.lend.push_back(T.nboxes);
     }
     T.nlevels = ilev;
+    if (known && ilev > 0) {
+        // every level's own count must equal the one the keys gave
+        std::vector<int> h(ilev);
+        FMM_CUDA(cudaMemcpyAsync(h.data(), chk.get(), ilev * sizeof(int), cudaMemcpyDeviceToHost, s));
+        FMM_CUDA(cudaStreamSynchronize(s));
+        for (int l = 0; l < ilev; l++)
+            if ((unsigned long long)h[l] != kc[l]) {
+                T.boxsize.resize(1);
+                return build_by_keys(d_src, ns, d_targ, nt, ndiv, idivflag, nlmax, c0, ds, s, T, F,
+                                     true);
+            }
+    }
     prof_mark("tree_refine", s);
     B.computecoll(0, T.nlevels);
     if (T.nlevels >= 2) B.fix_lr();

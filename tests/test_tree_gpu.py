@@ -34,12 +34,19 @@ CASES = {
 }
 
 
-@pytest.fixture(params=["keys", "levelwise"])
+@pytest.fixture(params=["keys", "keys_sync", "levelwise"])
 def builder(request, monkeypatch):
+    """keys: path keys with the refinement counts of every level taken from
+    the sorted keys (one host synchronisation); keys_sync: path keys with a
+    synchronisation per level; levelwise: the reference's level-by-level
+    point partition."""
+    monkeypatch.delenv("FMM2D_B200_TREE_SYNC", raising=False)
     if request.param == "levelwise":
         monkeypatch.setenv("FMM2D_B200_TREE", "levelwise")
     else:
         monkeypatch.delenv("FMM2D_B200_TREE", raising=False)
+        if request.param == "keys_sync":
+            monkeypatch.setenv("FMM2D_B200_TREE_SYNC", "1")
     return request.param
 
 
