@@ -611,6 +611,15 @@ __device__ __forceinline__ void p2p_pair(const typename PosT<MIXED>::T &x,
     }
 }
 
+// Strength slots per warp of p2p_kernel: the staged strengths, or the
+// 32 lanes' group sums (3 CH values each) when those are more.
+template <int CH, bool IFC, bool IFD>
+constexpr int p2p_str_slots() {
+    return kP2PStage * ((IFC ? CH : 0) + (IFD ? CH : 0)) > 32 * 3 * CH
+               ? kP2PStage * ((IFC ? CH : 0) + (IFD ? CH : 0))
+               : 32 * 3 * CH;
+}
+
 template <int CH, int PGH, bool IFC, bool IFD, bool MIXED, bool LAPR>
 __global__ void __launch_bounds__(kP2PWarps * 32) p2p_kernel(
     int lo, int hi, const int *__restrict__ nlist1,
@@ -627,7 +636,10 @@ __global__ void __launch_bounds__(kP2PWarps * 32) p2p_kernel(
     typedef typename PosT<MIXED>::T PT;
     constexpr int kStr = (IFC ? CH : 0) + (IFD ? CH : 0);
     constexpr int kRed = 3 * CH;
-    constexpr int kWarpBytes = kP2PStage * (16 + kStr * (int)sizeof(R2));
+    // the strengths' slots double as the 32 lanes' group sums (kRed values
+    // each), so they hold the larger of the two
+    constexpr int kStrSlots = p2p_str_slots<CH, IFC, IFD>();
+    constexpr int kWarpBytes = kP2PStage * 16 + kStrSlots * (int)sizeof(R2);
     extern __shared__ __align__(16) unsigned char p2p_smem[];
     const int lane = lane_id(), wib = threadIdx.x >> 5;
     PT *s_pos = reinterpret_cast<PT *>(p2p_smem + (size_t)wib * kWarpBytes);
@@ -918,8 +930,8 @@ __global__ void __launch_bounds__(kP2PWarps * 32) p2p_flat_kernel(
 
 template <int CH, bool IFC, bool IFD, bool MIXED>
 constexpr size_t p2p_smem_bytes() {
-    return (size_t)kP2PWarps * kP2PStage *
-           (16 + ((IFC ? CH : 0) + (IFD ? CH : 0)) * sizeof(typename Real<MIXED>::T2));
+    return (size_t)kP2PWarps * ((size_t)kP2PStage * 16 +
+                                (size_t)p2p_str_slots<CH, IFC, IFD>() * sizeof(typename Real<MIXED>::T2));
 }
 
 int grid_for(int nwarps) {

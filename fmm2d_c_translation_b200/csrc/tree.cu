@@ -265,6 +265,23 @@ struct Builder {
         if (nref == 0) return 0;
         ensure(T.nboxes + 4 * nref);
         const int cap = T.cap;
+        if (known >= 0) {
+            // a known count that was too large must leave no box unset: the
+            // ones no parent fills hang under the root (the check at the end
+            // of the build then rebuilds the tree)
+            const int nb0k = T.nboxes;
+            int *lev = T.level.get(), *par = T.parent.get(), *nch = T.nchild.get(),
+                *chi = T.child.get();
+            double2 *cenk = T.centers.get();
+            for_each(4 * (int64_t)nref, s, [=] __device__(int64_t i) {
+                const int kb = nb0k + (int)i;
+                cenk[kb] = cenk[0];
+                par[kb] = 0;
+                lev[kb] = newlevel;
+                nch[kb] = 0;
+                for (int l = 0; l < 4; l++) chi[4 * kb + l] = -1;
+            });
+        }
         const int nb0 = T.nboxes;
         double2 *cen = T.centers.get();
         int *lev = T.level.get(), *par = T.parent.get(), *nch = T.nchild.get();
