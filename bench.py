@@ -71,6 +71,18 @@ def make_inputs(ns, nt, seed):
     return src, trg, q, d, v
 
 
+# DRAM bytes (read + write) per launch of the dominant kernel at 2e6 + 2e6
+# uniform points, from `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum`
+# on the bench command with --ns 2000000 --nt 2000000 (the summary with the
+# full command is kept in profiles/)
+TRAFFIC_2E6 = {
+    ("mixed", "m2l"): (245e6, "profiles/kernels_mixed_2e6_dram.md: m2l_win_kernel<2,20> "
+                              "102 MB read + 143 MB write at 2e6+2e6, scaled by points"),
+    ("mixed", "p2p"): (663e6, "profiles/kernels_mixed_2e6_dram.md: p2p_flat_kernel "
+                              "450 MB read + 213 MB write at 2e6+2e6, scaled by points"),
+}
+
+
 def read_peaks():
     p = os.path.join(REPO, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -561,27 +573,58 @@ def main():
     peaks, peak_kind = read_peaks()
     ndc = counts.get("ndc", 2)
     pterm = counts.get("nterms", 18)
-    roof = None
     mixed = args.precision == "mixed" or (args.precision == "auto" and args.eps >= 0.5e-6)
     pipe = "fp32" if mixed else "fp64"
     pk_pipe = measure_fp32_peak(L) if mixed else measure_fp64_peak(L)
-    pk_src = (f"{pipe.upper()} FMA microbenchmark on this GPU (fmm2d_b200_{pipe}_peak_tflops); "
-              "the kernel runs on the CUDA-core " + pipe.upper() + " pipe")
-    if dom == "m2l":
+    entries = {}
+    if times.get("m2l"):
         # F_M2L = 8 * list-2 pairs * (p+1)^2 * nd_c
-        flops = 8.0 * counts.get("m2l_pairs", 0) * (pterm + 1) ** 2 * ndc
-        ach = flops / (times[dom] * 1e-3) / 1e12
-        roof = {"kernel": "m2l", "bound": pipe, "achieved": ach, "peak": pk_pipe,
-                "unit": "TFLOP/s", "frac": ach / pk_pipe if pk_pipe else None, "traffic": None,
-                "peak_source": pk_src}
-    elif dom == "p2p":
+        f_m2l = 8.0 * counts.get("m2l_pairs", 0) * (pterm + 1) ** 2 * ndc
+        ach = f_m2l / (times["m2l"] * 1e-3) / 1e12
+        if mixed:
+            # the tcgen05 kind::tf32 rate / 3: a TF32x3 product issues three MMAs
+            tf32 = measure_tf32_peak(L)
+            pk = tf32 / 3.0 if tf32 else None
+            entries["m2l"] = {
+                "kernel": "m2l phase (m2l_win_kernel tcgen05 TF32x3 on dense levels, "
+                          "m2l_tc_kernel slot tables on sparse levels, FP32 leading rows)",
+                "bound": "tensor", "achieved": ach, "peak": pk, "unit": "TFLOP/s",
+                "frac": ach / pk if pk else None, "tf32_peak_tflops": tf32,
+                "peak_source": "tcgen05 kind::tf32 microbenchmark on this GPU "
+                               "(fmm2d_b200_tf32_peak_tflops), divided by 3",
+                "flops_per_launch": f_m2l}
+        else:
+            entries["m2l"] = {
+                "kernel": "m2l phase (m2l_dmma_kernel, FP64 DMMA)", "bound": "fp64",
+                "achieved": ach, "peak": pk_pipe, "unit": "TFLOP/s",
+                "frac": ach / pk_pipe if pk_pipe else None,
+                "peak_source": "FP64 FMA microbenchmark on this GPU "
+                               "(fmm2d_b200_fp64_peak_tflops)",
+                "flops_per_launch": f_m2l}
+    if times.get("p2p"):
         # F_P2P = pairs * (10 + nd_c * sum_out w), charge and dipole, pot + grad
         pairs = counts.get("p2p_pairs_src", 0) + counts.get("p2p_pairs_targ", 0)
-        flops = pairs * (10 + ndc * 20)
-        ach = flops / (times[dom] * 1e-3) / 1e12
-        roof = {"kernel": "p2p", "bound": pipe, "achieved": ach, "peak": pk_pipe,
-                "unit": "TFLOP/s", "frac": ach / pk_pipe if pk_pipe else None, "traffic": None,
-                "peak_source": pk_src}
+        f_p2p = pairs * (10 + ndc * 20)
+        ach = f_p2p / (times["p2p"] * 1e-3) / 1e12
+        entries["p2p"] = {
+            "kernel": "p2p phase (p2p_flat_kernel)" if mixed else "p2p phase (p2p_kernel)",
+            "bound": pipe, "achieved": ach, "peak": pk_pipe, "unit": "TFLOP/s",
+            "frac": ach / pk_pipe if pk_pipe else None,
+            "peak_source": f"{pipe.upper()} FMA microbenchmark on this GPU "
+                           f"(fmm2d_b200_{pipe}_peak_tflops); the kernel runs on the CUDA-core "
+                           f"{pipe.upper()} pipe",
+            "flops_per_launch": f_p2p}
+    # DRAM bytes per launch of the dominant kernel from the ncu capture of the
+    # same kernel at 2e6 + 2e6 points, scaled by the points (the traffic
+    # grows with the boxes and points in proportion)
+    tr = TRAFFIC_2E6.get(("mixed" if mixed else "fp64", dom))
+    if tr is not None:
+        entries[dom]["traffic"] = tr[0] * (ns + nt) / 4e6
+        entries[dom]["traffic_source"] = tr[1]
+    elif dom in entries:
+        entries[dom]["traffic"] = None
+    if dom in entries:
+        roof = entries[dom]
     elif dom is not None:
         # memory-bound phases: compulsory bytes of the whole evaluation
         byts = (ns * (16 + 16 * ndc * 2 + 16) + nt * 16 +
@@ -590,25 +633,14 @@ def main():
         pk = peaks.get("hbm_gbs")
         roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": pk,
                 "unit": "GB/s", "frac": ach / pk if pk else None, "traffic": None}
+    else:
+        roof = None
     if roof is not None:
         roof["peak_file"] = peak_kind
+        roof["hbm_peak_gbs"] = peaks.get("hbm_gbs")
         roof["phase_ms"] = {k: round(v_, 4) for k, v_ in times.items()}
         roof["counts"] = counts
-    # second entry: the M2L phase against the tensor pipe (mixed mode: the
-    # tcgen05 kind::tf32 rate / 3, since a TF32x3 product issues three MMAs)
-    roof_m2l = None
-    if mixed and times.get("m2l"):
-        tf32 = measure_tf32_peak(L)
-        f_m2l = 8.0 * counts.get("m2l_pairs", 0) * (pterm + 1) ** 2 * ndc
-        ach = f_m2l / (times["m2l"] * 1e-3) / 1e12
-        roof_m2l = {"kernel": "m2l (phase: windowed tcgen05 TF32x3 + slot tables + FP32 rows)",
-                    "bound": "tensor", "achieved": ach,
-                    "peak": tf32 / 3.0 if tf32 else None, "unit": "TFLOP/s",
-                    "frac": ach / (tf32 / 3.0) if tf32 else None,
-                    "tf32_peak_tflops": tf32,
-                    "peak_source": "tcgen05 kind::tf32 microbenchmark on this GPU "
-                                   "(fmm2d_b200_tf32_peak_tflops), divided by 3",
-                    "flops_per_launch": f_m2l}
+    roof_other = {k: v_ for k, v_ in entries.items() if k != dom}
 
     configs = None
     if not args.no_configs and ws == 1:
@@ -636,7 +668,7 @@ def main():
                    "precision": args.precision, "ns": ns, "nt": nt,
                    "eps": args.eps, "parallelism": f"replicas{ws}",
                    "l2": "inputs 0.8 GB > L2; no flush"},
-        "roofline": roof, "roofline_m2l": roof_m2l, "cpu_baseline": cpu, "e2e": e2e,
+        "roofline": roof, "roofline_other_phases": roof_other, "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": nlaunch, "clocks": clk, "fp64_plain": fp64,
         "accuracy": acc, "serving": serving, "configs": configs, "autotune": tuned,
     }
@@ -761,7 +793,8 @@ def measure_configs(fm, L, args):
          C translation on one host core for the same call);
       c3 lfmm2d_st_d_p on the starfish r = 1 + 0.3 cos 5t: 4e6 sources with
          outward normals as dipole vectors and real N(0,1) dipole strengths,
-         4e6 targets at normal distance 10^U[-3,-1], eps 1e-9 (FP64);
+         4e6 targets at normal distance 10^U[-3,-1], eps 1e-9 (split-precision
+         M2L, and all-FP64);
       c4 hfmm2d_s_cd_p, 2e6 uniform sources, zk = 200, eps 1e-6 (mixed: M2L as
          TF32x3 contractions on the tensor cores; also timed all-FP64)."""
     import torch
@@ -873,7 +906,6 @@ def measure_configs(fm, L, args):
                              ctypes.byref(ier))
             check()
 
-        ms, prof = timed(c3)
         m = 10000
         idx = np.random.default_rng(5).choice(n3, m, replace=False)
         sub = T(y.T[idx])
@@ -881,12 +913,27 @@ def measure_configs(fm, L, args):
         L.fmm2d_b200_l2d_direct(1, n3, ptr(d_src), 0, None, 1, ptr(d_ds), ptr(d_nv), m, ptr(sub), 1,
                                 ptr(pot), None, None, ctypes.c_double(1e-300))
         torch.cuda.synchronize()
-        out["c3"] = {"workload": "lfmm2d_st_d_p starfish 4e6 + 4e6 near-curve targets eps 1e-9 (FP64)",
+        # split-precision M2L (FP64 triangle + TF32x3 tail on the tensor
+        # cores), then the same call all-FP64
+        L.fmm2d_b200_set_precision(3)
+        ms, prof = timed(c3)
+        err_split = rel(d_pt.view(-1, 2)[T(idx)], pot.view(-1, 2))
+        L.fmm2d_b200_set_precision(1)
+        ms64, prof64 = timed(c3)
+        err64 = rel(d_pt.view(-1, 2)[T(idx)], pot.view(-1, 2))
+        L.fmm2d_b200_set_precision(0)
+        out["c3"] = {"workload": "lfmm2d_st_d_p starfish 4e6 + 4e6 near-curve targets eps 1e-9 "
+                                 "(split: FP64 passes, M2L terms of total order >= "
+                                 f"{int(prof.get('#m2l_split_nt', 0))} as TF32x3 on the tensor cores)",
                      "ms": ms, "points_s": 2 * n3 / (ms * 1e-3),
                      "nlevels": prof.get("#nlevels"), "nboxes": prof.get("#nboxes"),
                      "phase_ms": {k: round(v, 3) for k, v in prof.items() if not k.startswith("#")},
-                     "pottarg_rel_l2": rel(d_pt.view(-1, 2)[T(idx)], pot.view(-1, 2)),
-                     "accuracy_sample": f"{m} targets vs GPU FP64 direct sum"}
+                     "pottarg_rel_l2": err_split,
+                     "accuracy_sample": f"{m} targets vs GPU FP64 direct sum",
+                     "fp64": {"ms": ms64, "points_s": 2 * n3 / (ms64 * 1e-3),
+                              "pottarg_rel_l2": err64,
+                              "phase_ms": {k: round(v, 3) for k, v in prof64.items()
+                                           if not k.startswith("#")}}}
         del d_src, d_trg, d_ds, d_nv, d_pot, d_pt
     if "c4" in want:
         # ---- c4 ----

@@ -365,7 +365,7 @@ FMM_EXPORT int fmm2d_b200_fmm2d_batch(int kernel, int nprob, double eps, const i
 }
 
 FMM_EXPORT int fmm2d_b200_set_precision(int mode) {
-    if (mode < 0 || mode > 2) return 4;
+    if (mode < 0 || mode > 3) return 4;
     set_precision(mode);
     return 0;
 }

@@ -96,6 +96,7 @@ int current_precision() {
         p = kPrecAuto;
         if (e && !strcmp(e, "fp64")) p = kPrecFP64;
         if (e && !strcmp(e, "mixed")) p = kPrecMixed;
+        if (e && !strcmp(e, "split")) p = kPrecSplit;
         g_precision.store(p);
     }
     return p;
@@ -176,6 +177,7 @@ void laplace_geometry(const FmmCall &c, bool on_dev, cudaStream_t s, LapGeometry
     // mixed precision for eps >= 1e-6 unless all-FP64 is requested
     const int prec = c.precision;
     G.mixed = prec == kPrecMixed || (prec == kPrecAuto && c.eps >= 0.5e-6);
+    G.split = !G.mixed && prec == kPrecSplit;
     InBuf<double2> src_in, trg_in;
     src_in.set(c.sources, c.ns, on_dev, s);
     trg_in.set(c.nt > 0 ? c.targ : nullptr, c.nt, on_dev, s);
@@ -340,6 +342,7 @@ void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaS
     P.thresh = G.thresh;
     P.ifnear = c.ifnear;
     P.mixed = G.mixed;
+    P.split = G.split;
     P.real_charge = lap;
     P.m2l_cache = m2l;
     if (mixed) {
@@ -908,6 +911,7 @@ int run_laplace_batch(const BatchCall &b) {
         G.eps = b.eps;
         G.p = laplace_nterms(b.eps);
         G.mixed = b.precision == kPrecMixed || (b.precision == kPrecAuto && b.eps >= 0.5e-6);
+        G.split = !G.mixed && b.precision == kPrecSplit;
         int ndiv = leaf_capacity(b.eps, NS, NT);
         if (G.mixed && lap) ndiv = mixed_leaf_capacity(G.p, ndiv);
         build_forest(src.get(), so, NT > 0 ? trg.get() : nullptr, to, ndiv, 0, kMaxLevels, R, s, G.T);

@@ -9,7 +9,7 @@ namespace fmm2d {
 // kReal: the real-valued Laplace FMM (rfmm2d, src/laplace/rfmm2d.f:27-214):
 // real charges, real dipole strengths with dipole vectors, real outputs.
 enum Kernel { kLaplace = 0, kCauchy = 1, kHelmholtz = 2, kReal = 3 };
-enum Precision { kPrecAuto = 0, kPrecFP64 = 1, kPrecMixed = 2 };
+enum Precision { kPrecAuto = 0, kPrecFP64 = 1, kPrecMixed = 2, kPrecSplit = 3 };
 
 // Arguments of the reference's guru drivers (lfmm2d / cfmm2d / hfmm2d and
 // their _ndiv forms).  Complex arrays are interleaved (re, im) doubles in
@@ -47,6 +47,7 @@ struct FmmCall {
 // over it with the strengths and outputs of `c`.
 struct LapGeometry {
     bool lap = true, mixed = false;
+    bool split = false;  // split-precision M2L, every other pass FP64
     bool real = false;  // rfmm2d: one real-charge channel per density
     int nd = 1, ndc = 2, ns = 0, nt = 0, p = 0;
     double eps = 0, thresh = 0;

@@ -100,7 +100,7 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 
 template <int KP, int NP>
-__global__ void __launch_bounds__(kHtThreads, 1) helm_m2l_tc_kernel(HtArgs A) {
+__global__ void __launch_bounds__(kHtThreads, 1) slot_gemm_tc_kernel(HtArgs A) {
     constexpr int KC = KP / 16;                      // K chunks per slot
     constexpr uint32_t A_BYTES = kHtRows * 16 * 4;   // one of hi / lo
     constexpr uint32_t B_BYTES = NP * 16 * 4;
@@ -363,7 +363,7 @@ __device__ __forceinline__ void ht_split(float v, float &hi, float &lo) {
 
 // Operand-ready A rows of the level's boxes: [box][ch][hi KP | lo KP] of
 // [Re M_-p..p | Im M_-p..p | 0].
-__global__ void __launch_bounds__(256) helm_tc_rows_kernel(long long nrow, int nd, int W, int KP,
+__global__ void __launch_bounds__(256) slot_rows_kernel(long long nrow, int nd, int W, int KP,
                                                           const double2 *__restrict__ mpl,
                                                           float *__restrict__ arow) {
     const long long n = nrow * KP;
@@ -417,20 +417,18 @@ __global__ void __launch_bounds__(256) helm_tc_bimg_kernel(int p, int KP, int NP
         }
         float hi, lo;
         ht_split((float)(v * scale), hi, lo);
-        const int kc = k >> 4, cc = (k >> 2) & 3, el = k & 3;
-        float *blk = bimg + ((size_t)cs * KC + kc) * (2 * NP * 16);
-        const int f = ((cc * (NP / 8) + (nn >> 3)) << 5) + ((nn & 7) << 2) + el;
-        blk[f] = hi;
-        blk[NP * 16 + f] = lo;
+        float *blk = bimg + (size_t)cs * KC * (2 * NP * 16) + slot_bimg_at(nn, k, NP);
+        blk[0] = hi;
+        blk[NP * 16] = lo;
     }
 }
 
 template <int KP, int NP>
 void launch_ht(const HtArgs &a, int ntiles, int nslice, cudaStream_t s) {
     const size_t smem = ht_smem_bytes<KP, NP>();
-    raise_smem_limit((const void *)helm_m2l_tc_kernel<KP, NP>, smem);
+    raise_smem_limit((const void *)slot_gemm_tc_kernel<KP, NP>, smem);
     const dim3 grid(std::max(1, std::min(ntiles, kNumSM)), nslice);
-    helm_m2l_tc_kernel<KP, NP><<<grid, kHtThreads, smem, s>>>(a);
+    slot_gemm_tc_kernel<KP, NP><<<grid, kHtThreads, smem, s>>>(a);
     FMM_CHECK_LAUNCH();
 }
 
@@ -454,18 +452,25 @@ __global__ void __launch_bounds__(256) helm_tc_slices_kernel(
 
 int helm_m2l_tc_max_order() { return kHtMaxOrder; }
 
-bool helm_m2l_tc_level(const HtLevel &lv, const SlotPlan &spl, const double2 *mp, double2 *loc,
-                       int *err, cudaStream_t s) {
-    const int p = lv.p, W = 2 * p + 1, nd = lv.nd;
-    if (p > kHtMaxOrder || p < 1 || nd < 1 || nd > kHtRows) return false;
-    if (!(lv.maxabs > 0.0) || !std::isfinite(lv.maxabs)) return false;
-    // a power of two that brings the largest entry of Bop to about 1; the
-    // level keeps the FP64 form if that scale or the entries leave the
-    // FP32 range
-    const int ex = (int)std::floor(std::log2(lv.maxabs));
-    if (ex > 120 || ex < -120) return false;
-    const double scale = std::ldexp(1.0, -ex);
-    const int g0 = 4 * (lv.level - 2);
+int slot_gemm_kp(int W) {
+    int KP = 32;
+    while (KP < 2 * W) KP += 16;
+    return KP <= 96 ? KP : 0;
+}
+
+void slot_gemm_rows(long long nrow, int nd, int W, int KP, const double2 *x, float *arow,
+                    cudaStream_t s) {
+    const long long n = nrow * KP;
+    if (n <= 0) return;
+    const int blocks = (int)std::min<long long>((n + 255) / 256, (long long)kNumSM * 16);
+    slot_rows_kernel<<<std::max(blocks, 1), 256, 0, s>>>(nrow, nd, W, KP, x, arow);
+    FMM_CHECK_LAUNCH();
+}
+
+bool slot_gemm_tc_level(const SlotGemmLevel &g, const SlotPlan &spl, int *err, cudaStream_t s) {
+    const int W = g.W, nd = g.nd, KP = g.KP;
+    if (W < 1 || nd < 1 || nd > kHtRows || KP != slot_gemm_kp(W) || KP == 0) return false;
+    const int g0 = 4 * (g.level - 2);
     if (g0 < 0 || g0 + 4 > spl.nseg) return false;
     HtArgs a;
     for (int c = 0; c <= 4; c++) a.tb[c] = spl.tile_base[g0 + c];
@@ -475,36 +480,16 @@ bool helm_m2l_tc_level(const HtLevel &lv, const SlotPlan &spl, const double2 *mp
     }
     const int ntiles = a.tb[4] - a.tb[0];
     if (ntiles == 0) return true;
-    int KP = 32;
-    while (KP < 2 * W) KP += 16;
-    const int NP = KP;
-    const long long nbox = lv.nbox;
-    DevBuf<float> arow((size_t)nbox * nd * 2 * KP, s);
-    DevBuf<float> bimg((size_t)4 * kHtSlots * 2 * NP * KP, s);
-    const double2 *mpl = mp + lv.off;
-    {
-        const long long n = nbox * nd * KP;
-        const int blocks = (int)std::min<long long>((n + 255) / 256, (long long)kNumSM * 16);
-        helm_tc_rows_kernel<<<std::max(blocks, 1), 256, 0, s>>>(nbox * nd, nd, W, KP, mpl, arow.get());
-        FMM_CHECK_LAUNCH();
-    }
-    {
-        const long long n = (long long)4 * kHtSlots * NP * KP;
-        const int blocks = (int)std::min<long long>((n + 255) / 256, (long long)kNumSM * 16);
-        helm_tc_bimg_kernel<<<blocks, 256, 0, s>>>(p, KP, NP, scale, spl.dxy, lv.table, lv.pw,
-                                                   bimg.get());
-        FMM_CHECK_LAUNCH();
-    }
     a.boxes = spl.boxes;
     a.slots = spl.slots;
-    a.lstart = lv.lstart;
+    a.lstart = g.lstart;
     a.nd = nd;
     a.tpt = kHtRows / nd;
     a.W = W;
-    a.arow = arow.get();
-    a.bimg = bimg.get();
-    a.locl = loc + lv.off;
-    a.oscale = 1.0 / scale;
+    a.arow = g.arow;
+    a.bimg = g.bimg;
+    a.locl = g.out;
+    a.oscale = g.oscale;
     a.err = err;
     a.stall = tc_stall_injected();
     a.wait_ns = tc_wait_limit_ns();
@@ -527,10 +512,51 @@ bool helm_m2l_tc_level(const HtLevel &lv, const SlotPlan &spl, const double2 *mp
         const long long n = (long long)a.nq * W * nd;
         const int blocks = (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, kNumSM * 8));
         helm_tc_slices_kernel<<<blocks, 256, 0, s>>>(a.nq, W * nd, nslice, part.get(), spl.boxes,
-                                                     a.q_lo, lv.lstart, loc + lv.off);
+                                                     a.q_lo, g.lstart, g.out);
         FMM_CHECK_LAUNCH();
     }
     return true;
+}
+
+bool helm_m2l_tc_level(const HtLevel &lv, const SlotPlan &spl, const double2 *mp, double2 *loc,
+                       int *err, cudaStream_t s) {
+    const int p = lv.p, W = 2 * p + 1, nd = lv.nd;
+    if (p > kHtMaxOrder || p < 1 || nd < 1 || nd > kHtRows) return false;
+    if (!(lv.maxabs > 0.0) || !std::isfinite(lv.maxabs)) return false;
+    // a power of two that brings the largest entry of Bop to about 1; the
+    // level keeps the FP64 form if that scale or the entries leave the
+    // FP32 range
+    const int ex = (int)std::floor(std::log2(lv.maxabs));
+    if (ex > 120 || ex < -120) return false;
+    const double scale = std::ldexp(1.0, -ex);
+    const int g0 = 4 * (lv.level - 2);
+    if (g0 < 0 || g0 + 4 > spl.nseg) return false;
+    if (spl.tile_base[g0 + 4] == spl.tile_base[g0]) return true;
+    const int KP = slot_gemm_kp(W);
+    if (KP == 0) return false;
+    const int NP = KP;
+    const long long nbox = lv.nbox;
+    DevBuf<float> arow((size_t)nbox * nd * 2 * KP, s);
+    DevBuf<float> bimg((size_t)4 * kHtSlots * 2 * NP * KP, s);
+    slot_gemm_rows(nbox * nd, nd, W, KP, mp + lv.off, arow.get(), s);
+    {
+        const long long n = (long long)4 * kHtSlots * NP * KP;
+        const int blocks = (int)std::min<long long>((n + 255) / 256, (long long)kNumSM * 16);
+        helm_tc_bimg_kernel<<<blocks, 256, 0, s>>>(p, KP, NP, scale, spl.dxy, lv.table, lv.pw,
+                                                   bimg.get());
+        FMM_CHECK_LAUNCH();
+    }
+    SlotGemmLevel g;
+    g.level = lv.level;
+    g.lstart = lv.lstart;
+    g.nd = nd;
+    g.W = W;
+    g.KP = KP;
+    g.arow = arow.get();
+    g.bimg = bimg.get();
+    g.out = loc + lv.off;
+    g.oscale = 1.0 / scale;
+    return slot_gemm_tc_level(g, spl, err, s);
 }
 
 }  // namespace fmm2d

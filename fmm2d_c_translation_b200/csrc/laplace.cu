@@ -1895,6 +1895,7 @@ void cauchy_fmm(const Tree &T, const CauchyProblem &P0, cudaStream_t s) {
                                  (size_t)nlow * (P.p + 1) * P.ndc * sizeof(float2), s));
     }
     if (simple || !((fp32 && m2l_fp32(T, P, mp.get(), loc.get(), s, mp32.get())) ||
+                    (P.split && !P.mixed && m2l_split_fp64(T, P, mp.get(), loc.get(), s)) ||
                     m2l_tensor_fp64(T, P, mp.get(), loc.get(), s)))
         per_chunk([&](int c0) { m2l_chunk<2>(T, P, c0, binom, mp.get(), loc.get(), s); },
                   [&](int c0) { m2l_chunk<1>(T, P, c0, binom, mp.get(), loc.get(), s); });

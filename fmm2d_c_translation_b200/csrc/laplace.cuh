@@ -70,6 +70,7 @@ struct CauchyProblem {
     double thresh = 0;                // near-field exclusion radius
     int ifnear = 1;
     bool mixed = false;               // FP32 series / pair arithmetic
+    bool split = false;               // split-precision M2L (FP64 triangle + TF32 x 3 tail)
     bool real_charge = false;         // complex-Laplace channels (real charges,
                                       // real part of the potential used)
     const int *sleaf = nullptr;       // leaf of every sorted source (set by cauchy_fmm)
@@ -98,6 +99,13 @@ void cauchy_fmm(const Tree &T, const CauchyProblem &P, cudaStream_t s);
 // uses the per-box kernel).
 bool m2l_tensor_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp,
                      double2 *loc, cudaStream_t s);
+// Split-precision M2L (m2l.cu): the terms of total order i + j below
+// split_triangle_order(p) in FP64 on the DMMA kernel, the rest as TF32 x 3
+// slot GEMMs on the tcgen05 tensor cores; false (nothing launched) when
+// the order or the tree does not fit.
+bool m2l_split_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 *loc,
+                    cudaStream_t s);
+int split_triangle_order(int p);
 
 // FP32 M2L of the mixed-precision mode (m2l.cu): one complex matrix per
 // (child position, slot) applied to FP32 copies of the multipoles; false
@@ -150,6 +158,44 @@ struct SlotPlan {
     int nseg = 0, ntarg = 0, ntiles = 0;
 };
 bool plan_slots(const Tree &T, int spgh, int tpgh, int tile, cudaStream_t s, SlotPlan &sp);
+
+// Slot GEMMs of one level on the tensor cores (helm_m2l_tc.cu): for every
+// plan row q of the level's four segments (child positions cp) and every
+// slot k with a source box sb = slots[q][k],
+//     out[boxes[q]] += oscale * Bop[cp][k] A[sb]      (in real form)
+// where A[sb] = [Re X_0..W-1 | Im X_0..W-1 | 0] are the source's W complex
+// coefficients per channel split into TF32 hi / lo (slot_gemm_rows), and
+// Bop[cp][k] the KP x KP real form [[Re B, -Im B], [Im B, Re B]] of the
+// slot's complex operator B (entry (n, k) of the hi image at
+// slot_bimg_at(n, k, KP), the lo image KP * 16 floats further).  TF32 x 3
+// products accumulate in tensor memory one slot at a time, and the slots
+// are summed in FP64.
+struct SlotGemmLevel {
+    int level = 0;                // level of the target boxes (>= 2)
+    int lstart = 0;               // box of row 0 of arow and out
+    int nd = 1, W = 0, KP = 0;    // channels, coefficients, padded K = N
+    const float *arow = nullptr;  // [box - lstart][nd][hi KP | lo KP]
+    const float *bimg = nullptr;  // [cp][27][KP / 16][hi KP x 16 | lo KP x 16]
+    double2 *out = nullptr;       // [box - lstart][W][nd]
+    double oscale = 1.0;
+};
+// K (= N) of W complex coefficients: 2 W rounded up to 16 (at least 32),
+// 0 when above the largest supported (96).
+int slot_gemm_kp(int W);
+// Operand-ready rows of nrow = boxes x nd rows of x ([box][W][nd]).
+void slot_gemm_rows(long long nrow, int nd, int W, int KP, const double2 *x, float *arow,
+                    cudaStream_t s);
+// false (nothing launched) when the level has no tiles or the shape is
+// unsupported; *err is set when a bounded wait runs out.
+bool slot_gemm_tc_level(const SlotGemmLevel &g, const SlotPlan &spl, int *err, cudaStream_t s);
+// Index of Bop entry (output column n, input k) in the hi images of one
+// (child position, slot): K chunk k / 16, then the no-swizzle K-major
+// layout of the chunk's N x 16 block.
+__host__ __device__ inline size_t slot_bimg_at(int n, int k, int KP) {
+    const int kc = k >> 4, cc = (k >> 2) & 3, el = k & 3;
+    return (size_t)kc * (2 * KP * 16) +
+           (size_t)((((cc * (KP / 8) + (n >> 3)) << 5) + ((n & 7) << 2) + el));
+}
 
 // Binomial table C(l, m), l, m <= kLdc, built with the reference's Pascal
 // recurrence (init_carray, src/common/fmmcommon2d.f).

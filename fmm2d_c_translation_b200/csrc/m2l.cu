@@ -86,7 +86,10 @@ struct SegTable {
     int nseg;
 };
 
-template <int MT, int KS, int CH>
+// NT > 0: only the terms with i + j < NT (the leading triangle of the
+// shift; the split-precision M2L adds the rest on the tensor cores), every
+// row of the locals still stored.
+template <int MT, int KS, int CH, int NT = 0>
 __global__ void __launch_bounds__(128, 4) m2l_dmma_kernel(
     SegTable seg, const int *__restrict__ boxes, const int *__restrict__ slots,
     const double *__restrict__ bs, int ndc, int c0, int p,
@@ -95,11 +98,13 @@ __global__ void __launch_bounds__(128, 4) m2l_dmma_kernel(
     // A-operand fragments of B: [mt][ks][lane]
     __shared__ double s_a[MT * KS * 32];
     __shared__ int s_tb[257];
+    // (mt, ks) tiles with a term of the triangle
+    auto live = [](int mt, int ks) { return NT == 0 || mt * 8 + ks * 4 < NT; };
     for (int e = threadIdx.x; e < MT * KS * 32; e += blockDim.x) {
         const int l = e & 31, ks = (e >> 5) % KS, mt = (e >> 5) / KS;
         const int i = mt * 8 + (l >> 2), j = ks * 4 + (l & 3);
         double v = 0.0;
-        if (i <= p && j <= p) {
+        if (i <= p && j <= p && (NT == 0 || i + j < NT)) {
             if (i == 0)
                 v = j == 0 ? 0.0 : 1.0;
             else
@@ -163,7 +168,7 @@ __global__ void __launch_bounds__(128, 4) m2l_dmma_kernel(
                 for (int ks = 0; ks < KS; ks++) {
                     const int j = ks * 4 + tig;
                     double2 h = make_double2(0.0, 0.0);
-                    if (sg_box >= 0 && j <= p)
+                    if (live(0, ks) && sg_box >= 0 && j <= p)
                         h = cmul(mp[(size_t)sg_box * stride + (size_t)j * ndc + c0 + c], wj);
                     bre[ks] = h.x;
                     bim[ks] = h.y;
@@ -175,6 +180,7 @@ __global__ void __launch_bounds__(128, 4) m2l_dmma_kernel(
                     tre[mt][0] = tre[mt][1] = tim[mt][0] = tim[mt][1] = 0.0;
 #pragma unroll
                     for (int ks = 0; ks < KS; ks++) {
+                        if (!live(mt, ks)) continue;
                         const double a = s_a[(mt * KS + ks) * 32 + lane];
                         dmma(tre[mt][0], tre[mt][1], a, bre[ks]);
                         dmma(tim[mt][0], tim[mt][1], a, bim[ks]);
@@ -183,6 +189,7 @@ __global__ void __launch_bounds__(128, 4) m2l_dmma_kernel(
                 double2 wi = w2p;
 #pragma unroll
                 for (int mt = 0; mt < MT; mt++) {
+                    if (!live(mt, 0)) break;  // (rows of no triangle term stay zero)
 #pragma unroll
                     for (int e = 0; e < 2; e++) {
                         const double2 tt = make_double2(tre[mt][e], tim[mt][e]);
@@ -224,7 +231,7 @@ __global__ void __launch_bounds__(128, 4) m2l_dmma_kernel(
     }
 }
 
-template <int MT, int KS>
+template <int MT, int KS, int NT = 0>
 void launch_dmma(const SegTable &sg, const int *boxes, const int *slots,
                  const double *bs, int ndc, int p, const double *binom,
                  const double2 *mp, double2 *loc, int ntiles, cudaStream_t s) {
@@ -233,11 +240,11 @@ void launch_dmma(const SegTable &sg, const int *boxes, const int *slots,
     const bool ch2 = e && e[0] == '1';
     for (int c0 = 0; c0 < ndc;) {
         if (ch2 && ndc - c0 >= 2 && MT <= 5) {
-            m2l_dmma_kernel<MT, KS, 2><<<blocks, 128, 0, s>>>(
+            m2l_dmma_kernel<MT, KS, 2, NT><<<blocks, 128, 0, s>>>(
                 sg, boxes, slots, bs, ndc, c0, p, binom, mp, loc, ntiles);
             c0 += 2;
         } else {
-            m2l_dmma_kernel<MT, KS, 1><<<blocks, 128, 0, s>>>(
+            m2l_dmma_kernel<MT, KS, 1, NT><<<blocks, 128, 0, s>>>(
                 sg, boxes, slots, bs, ndc, c0, p, binom, mp, loc, ntiles);
             c0 += 1;
         }
@@ -948,6 +955,191 @@ bool m2l_tensor_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp,
     FMM_M2L_CASE(8, 16)
 #undef FMM_M2L_CASE
     return false;
+}
+
+// ---------------------------------------------------------------------------
+// Split-precision M2L (eps below the mixed mode's range, all other passes
+// FP64).  The scaled shift's terms T_ij M_j fall off with the total order
+// i + j (about 0.47^(i+j) relative in the reference's worst case, the
+// ratio behind l2dterms).  The leading triangle i + j < NT, which carries
+// the potential down to that ratio to the NT, runs in FP64 on the DMMA
+// kernel (the first writer of every local); the tail i + j >= NT runs as
+// TF32 x 3 slot GEMMs on the tcgen05 tensor cores (slot_gemm_tc_level,
+// about 2^-22 relative per product, every slot summed in FP64) and is added
+// on top.  With NT = p + 1 - kSplitTailOrders the tail's share of the
+// potential is about 0.47^-kSplitTailOrders below eps in the worst case.
+// ---------------------------------------------------------------------------
+constexpr int kSplitTailOrders = 14;
+
+// The tail images (i + j >= nt) of the 4 x 27 slot operators in real form,
+// T_ij = w2^i B_ij w1^j (w2 = 1/t, w1 = -1/t, t the slot offset), TF32
+// split; cached per device, order and nt.
+const float *split_tail_tables(int p, int KP, int nt, cudaStream_t s) {
+    static std::mutex mu;
+    static std::vector<std::pair<long, const float *>> cache;
+    int dev;
+    FMM_CUDA(cudaGetDevice(&dev));
+    const long key = ((long)dev << 24) | ((long)nt << 16) | ((long)p << 8) | KP;
+    std::lock_guard<std::mutex> g(mu);
+    for (auto &e : cache)
+        if (e.first == key) return e.second;
+    const int W = p + 1, nc = 2 * W + 2;
+    std::vector<double> C((size_t)nc * nc, 0.0);
+    for (int l = 0; l < nc; l++) {
+        C[(size_t)l * nc] = 1.0;
+        for (int m = 1; m <= l; m++)
+            C[(size_t)l * nc + m] =
+                C[(size_t)(l - 1) * nc + m - 1] + (m < l ? C[(size_t)(l - 1) * nc + m] : 0.0);
+    }
+    const SlotTables st = make_slot_tables();
+    const size_t per = (size_t)(KP / 16) * 2 * KP * 16;  // floats per (position, slot)
+    std::vector<float> h((size_t)4 * kSlots * per, 0.f);
+    std::vector<double2> T((size_t)W * W);
+    for (int cp = 0; cp < 4; cp++)
+        for (int k = 0; k < kSlots; k++) {
+            const double tx = st.dx[cp][k], ty = st.dy[cp][k];
+            const double tn = 1.0 / (tx * tx + ty * ty);
+            const double2 w2 = make_double2(tx * tn, -ty * tn), w1 = make_double2(-w2.x, -w2.y);
+            double2 w2i = make_double2(1.0, 0.0);
+            for (int i = 0; i < W; i++) {
+                double2 w1j = make_double2(1.0, 0.0);
+                for (int j = 0; j < W; j++) {
+                    double b;
+                    if (i == 0)
+                        b = j == 0 ? 0.0 : 1.0;
+                    else
+                        b = j == 0 ? -1.0 / i : C[(size_t)(i + j - 1) * nc + (j - 1)];
+                    T[(size_t)i * W + j] =
+                        i + j >= nt ? cscal(cmul(w2i, w1j), b) : make_double2(0.0, 0.0);
+                    w1j = cmul(w1j, w1);
+                }
+                w2i = cmul(w2i, w2);
+            }
+            float *img = h.data() + (size_t)(cp * kSlots + k) * per;
+            for (int n = 0; n < 2 * W; n++)
+                for (int kk = 0; kk < 2 * W; kk++) {
+                    const double2 t = T[(size_t)(n < W ? n : n - W) * W + (kk < W ? kk : kk - W)];
+                    const bool re_out = n < W, re_in = kk < W;
+                    const double v = re_out ? (re_in ? t.x : -t.y) : (re_in ? t.y : t.x);
+                    const float f = (float)v, fh = tf32_round_host(f);
+                    const size_t at = slot_bimg_at(n, kk, KP);
+                    img[at] = fh;
+                    img[at + (size_t)KP * 16] = tf32_round_host(f - fh);
+                }
+        }
+    float *d = nullptr;
+    FMM_CUDA(cudaMalloc(&d, h.size() * sizeof(float)));
+    FMM_CUDA(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+    FMM_CUDA(cudaStreamSynchronize(s));
+    cache.push_back({key, d});
+    return d;
+}
+
+// The FP64 triangle on the DMMA kernel for the supported (MT, KS, NT).
+template <int NT>
+bool launch_split_triangle(const SegTable &sg, const int *boxes, const int *slots, const double *bs,
+                           int ndc, int p, const double *binom, const double2 *mp, double2 *loc,
+                           int ntiles, cudaStream_t s) {
+    const int ks = (p + 1 + 3) / 4, mt = (p + 1 + 7) / 8;
+#define FMM_SPLIT_CASE(MT_, KS_)                                                           \
+    if (mt <= MT_ && ks <= KS_) {                                                          \
+        launch_dmma<MT_, KS_, NT>(sg, boxes, slots, bs, ndc, p, binom, mp, loc, ntiles, s); \
+        return true;                                                                       \
+    }
+    FMM_SPLIT_CASE(3, 6)
+    FMM_SPLIT_CASE(4, 8)
+    FMM_SPLIT_CASE(5, 10)
+    FMM_SPLIT_CASE(6, 12)
+#undef FMM_SPLIT_CASE
+    return false;
+}
+
+namespace {
+struct SplitHold {
+    SlotPlan spl;
+};
+}  // namespace
+
+int split_triangle_order(int p) {
+    const char *e = getenv("FMM2D_B200_SPLIT_NT");
+    int nt = e ? atoi(e) : p + 1 - kSplitTailOrders;
+    // the supported triangles: 8, 12, 16, 20, 24
+    if (nt < 8) nt = 8;
+    nt = (nt + 3) / 4 * 4;
+    return nt > 24 ? 24 : nt;
+}
+
+bool m2l_split_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 *loc,
+                    cudaStream_t s) {
+    const int L = T.nlevels, p = P.p, W = p + 1;
+    if (L < 2 || W < 12 || W > 48 || P.ndc > 128) return false;
+    const int KP = slot_gemm_kp(W);
+    const int nt = split_triangle_order(p);
+    if (KP == 0 || nt >= 2 * W - 1) return false;
+    // planning first (nothing is launched when it fails)
+    bool ok = false;
+    const auto wp = m2l_cached<M2LWork>(P.m2l_cache, m2l_key(1, 8, 0), ok,
+                                        [&](M2LWork &x) { return m2l_work(T, P, 8, s, x); });
+    if (!ok) return false;
+    bool ok2 = false;
+    const int tpt = 128 / P.ndc;
+    const auto hp = m2l_cached<SplitHold>(P.m2l_cache, m2l_key(6, tpt, 0), ok2, [&](SplitHold &x) {
+        return plan_slots(T, P.sset.pgh, P.tset.pgh, tpt, s, x.spl);
+    });
+    if (!ok2) return false;
+    const M2LWork &w = *wp;
+    if (w.ntiles == 0) return true;
+    const float *bimg = split_tail_tables(p, KP, nt, s);
+    // 1. the FP64 triangle, storing every local of levels >= 2 with points
+    const double *binom = device_binomials(s);
+    const SegTable sg = w.seg();
+    const int *boxes = (const int *)w.vals.get();
+    const double *bs = T.d_boxsize.get();
+    bool launched = false;
+    switch (nt) {
+        case 8: launched = launch_split_triangle<8>(sg, boxes, w.slots.get(), bs, P.ndc, p, binom, mp, loc, w.ntiles, s); break;
+        case 12: launched = launch_split_triangle<12>(sg, boxes, w.slots.get(), bs, P.ndc, p, binom, mp, loc, w.ntiles, s); break;
+        case 16: launched = launch_split_triangle<16>(sg, boxes, w.slots.get(), bs, P.ndc, p, binom, mp, loc, w.ntiles, s); break;
+        case 20: launched = launch_split_triangle<20>(sg, boxes, w.slots.get(), bs, P.ndc, p, binom, mp, loc, w.ntiles, s); break;
+        case 24: launched = launch_split_triangle<24>(sg, boxes, w.slots.get(), bs, P.ndc, p, binom, mp, loc, w.ntiles, s); break;
+        default: break;
+    }
+    if (!launched) return false;
+    prof_set_count("m2l_split_nt", (double)nt);
+    // 2. the tail on the tensor cores, level by level, added to the locals
+    M2LCache *cache = P.m2l_cache;
+    const bool deferred = cache && cache->deferred;
+    DevBuf<int> err_own;
+    if (!deferred) {
+        err_own.alloc(1, s);
+        FMM_CUDA(cudaMemsetAsync(err_own.get(), 0, sizeof(int), s));
+    }
+    int *errp = deferred ? cache->err : err_own.get();
+    const size_t stride = (size_t)W * P.ndc;
+    long long maxbox = 0;
+    for (int l = 2; l <= L; l++) maxbox = std::max<long long>(maxbox, T.lend[l] - T.lstart[l]);
+    DevBuf<float> arow((size_t)maxbox * P.ndc * 2 * KP, s);
+    for (int l = 2; l <= L; l++) {
+        const int g0 = 4 * (l - 2);
+        if (g0 + 4 > hp->spl.nseg || hp->spl.tile_base[g0 + 4] == hp->spl.tile_base[g0]) continue;
+        const int lo = T.lstart[l], nb = T.lend[l] - lo;
+        slot_gemm_rows((long long)nb * P.ndc, P.ndc, W, KP, mp + (size_t)lo * stride, arow.get(), s);
+        SlotGemmLevel g;
+        g.level = l;
+        g.lstart = lo;
+        g.nd = P.ndc;
+        g.W = W;
+        g.KP = KP;
+        g.arow = arow.get();
+        g.bimg = bimg;
+        g.out = loc + (size_t)lo * stride;
+        g.oscale = 1.0;
+        if (!slot_gemm_tc_level(g, hp->spl, errp, s))
+            throw FmmError(4, "split-precision M2L: unsupported tensor-core level shape");
+    }
+    if (!deferred && read_scalar(errp, s) != 0)
+        throw FmmError(4, "tensor-core M2L: a wait for an MMA or operand barrier timed out");
+    return true;
 }
 
 namespace {

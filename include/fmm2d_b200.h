@@ -1552,8 +1552,11 @@ void hfmm2d_s_c_p(double eps, double _Complex zk, int64_t ns,
 const char *fmm2d_b200_version(void);
 /* Message of the last failed call (any thread); returns its length. */
 int fmm2d_b200_last_error(char *buf, int len);
-/* Precision policy of later calls: 0 auto (mixed when eps >= 1e-6),
- * 1 all-FP64, 2 mixed.  Also FMM2D_B200_PRECISION=auto|fp64|mixed. */
+/* Precision policy of later calls: 0 auto (mixed when eps >= 0.5e-6, else
+ * all-FP64), 1 all-FP64, 2 mixed, 3 split (Laplace / Cauchy: every pass
+ * FP64 except the M2L's terms of high total order, which run as TF32 x 3 on
+ * the tensor cores; Helmholtz: all-FP64).
+ * Also FMM2D_B200_PRECISION=auto|fp64|mixed|split. */
 int fmm2d_b200_set_precision(int mode);
 /* Run the calling thread's later calls on a caller-owned cudaStream_t. */
 int fmm2d_b200_set_stream(void *stream);
