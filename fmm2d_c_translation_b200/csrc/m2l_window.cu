@@ -37,13 +37,18 @@
 // hi / lo.  Row 0 (L_0, whose terms cancel across slots and reach the
 // potential undamped) is summed on the CUDA cores in FP32 from the same
 // windows, and the level's log(r) M_0 term is added in FP64, as in the
-// slot-table kernels.
+// slot-table kernels; from order kM2LExactFrom on so are rows 1-3 (1-5
+// with Hessians), which carry most of the gradient at a leaf's points and
+// need FP32's 24 bits rather than the 22 of a TF32 x 3 product.  The
+// window's lo plane holds the exact FP32 residual v - hi, so hi + lo gives
+// back the FP32 window value for those sums.
 //
 // Warp roles (416 threads, one block per SM): warps 0-7 convert the
 // windows (FP32 multipoles -> b_j-scaled TF32 hi/lo in the operand
 // layout) and copy the shift matrices; warp 12 issues the MMAs; warps
-// 8-11, one thread per accumulator row, sum row 0 from each window and at
-// the end of a run read the accumulators back and store the locals.
+// 8-11, one thread per accumulator row, sum the leading rows from each
+// window and at the end of a run read the accumulators back and store the
+// locals.
 // Windows, matrices and accumulators are double-buffered and handed over
 // with mbarriers; every wait is bounded in time and a wait that runs out
 // stops all roles of the block and sets *err.
@@ -99,7 +104,8 @@ struct WinArgs {
     const float4 *H;   // [40][2 HALF] h_k(t), TF32 split: (re hi, re lo, im hi, im lo); h_0 = 0
     const float *Bj;   // [HALF] b_j
     const double *Ai;  // [HALF] a_i = 1 / i!
-    const float2 *R0;  // [40][HALF] row 0 over the window values: -log|t|, h_j(t)
+    const float2 *Hf;  // [40][2 HALF] h_k(t) in FP32, with -log|t| at k = 0 (the rows
+                       // summed on the CUDA cores over the window values)
     const float2 *mp32;
     double2 *loc;
     int *err;
@@ -112,18 +118,28 @@ __device__ __forceinline__ void split_tf32(float v, float &hi, float &lo) {
     lo = tc_tf32(v - hi);
 }
 
+// Window values: hi = tf32(v) and lo = v - hi, the exact FP32 residual, so
+// that hi + lo gives back v for the rows summed on the CUDA cores (the MMA
+// reads lo at TF32 precision).
+__device__ __forceinline__ void split_exact(float v, float &hi, float &lo) {
+    hi = tc_tf32(v);
+    lo = v - hi;
+}
+
 __device__ __forceinline__ void put4(float *hi, float *lo, int f, float a, float b, float c,
                                      float d) {
     float4 h, l;
-    split_tf32(a, h.x, l.x);
-    split_tf32(b, h.y, l.y);
-    split_tf32(c, h.z, l.z);
-    split_tf32(d, h.w, l.w);
+    split_exact(a, h.x, l.x);
+    split_exact(b, h.y, l.y);
+    split_exact(c, h.z, l.z);
+    split_exact(d, h.w, l.w);
     *reinterpret_cast<float4 *>(hi + f) = h;
     *reinterpret_cast<float4 *>(lo + f) = l;
 }
 
-template <int CH, int HALF>
+// NR: the leading rows L_0 .. L_(NR-1) summed in FP32 on the CUDA cores by
+// the epilogue warps (1: row 0 only).
+template <int CH, int HALF, int NR>
 __global__ void __launch_bounds__(kWinThreads, 1) m2l_win_kernel(WinArgs A) {
     constexpr int KP = 2 * HALF, NQ = HALF / 4, NOP = 4 * KP;
     constexpr int TB = 128 / CH, WP = TB + 2;
@@ -137,8 +153,8 @@ __global__ void __launch_bounds__(kWinThreads, 1) m2l_win_kernel(WinArgs A) {
     float *sW = reinterpret_cast<float *>(win_smem);                 // [buf][hi, lo]
     float *sO = sW + 4 * WSZ;                                         // [buf][hi, lo]
     float4 *sH = reinterpret_cast<float4 *>(sO + 4 * OSZ);            // [40][KH]
-    float2 *sR0 = reinterpret_cast<float2 *>(sH + kWinOffsets * KH);  // [40][HALF]
-    double *sAi = reinterpret_cast<double *>(sR0 + kWinOffsets * HALF);  // [HALF]
+    float2 *sHf = reinterpret_cast<float2 *>(sH + kWinOffsets * KH);  // [40][KH]
+    double *sAi = reinterpret_cast<double *>(sHf + kWinOffsets * KH);  // [HALF]
     float *sBj = reinterpret_cast<float *>(sAi + HALF);               // [HALF]
     // barriers: 0-1 window full, 2-3 window free of MMAs, 4-5 window free
     // of row-0 reads, 6-7 matrices full, 8-9 matrices free, 10-11
@@ -165,7 +181,7 @@ __global__ void __launch_bounds__(kWinThreads, 1) m2l_win_kernel(WinArgs A) {
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     for (int e = tid; e < kWinOffsets * KH; e += blockDim.x) sH[e] = A.H[e];
-    for (int e = tid; e < kWinOffsets * HALF; e += blockDim.x) sR0[e] = A.R0[e];
+    for (int e = tid; e < kWinOffsets * KH; e += blockDim.x) sHf[e] = A.Hf[e];
     for (int e = tid; e < HALF; e += blockDim.x) {
         sAi[e] = A.Ai[e];
         sBj[e] = A.Bj[e];
@@ -313,7 +329,7 @@ __global__ void __launch_bounds__(kWinThreads, 1) m2l_win_kernel(WinArgs A) {
         }
         if (!ok) *abort_flag = 1;
     } else if (warp < kWinEpi0 + 4) {
-        // --------------------------------------------- row 0 and epilogue
+        // ------------------------------------- leading rows and epilogue
         // thread = accumulator row (t, ch) for all four child positions
         const int e = warp - kWinEpi0;  // tensor-memory lanes 32 e .. 32 e + 31
         const int rho = (e << 5) + lane, tcol = rho / CH, chn = rho - tcol * CH;
@@ -321,11 +337,16 @@ __global__ void __launch_bounds__(kWinThreads, 1) m2l_win_kernel(WinArgs A) {
         bool ok = true;
         for (int run = blockIdx.x; ok && run < A.nrun; run += gridDim.x, kr++) {
             const int R = A.run0 + run;
-            // L_0 = sum_slots sum_j T_0j M_j in FP32 from the windows
-            // (window value W_j = b_j M_j, coefficient R0_j = T_0j / b_j)
-            float2 l0[4], s0[4];
+            // L_i = a_i sum_slots sum_j h_(i+j)(t) W_j (i = 1 .. NR-1) and
+            // L_0 = sum_slots (sum_(j>=1) h_j(t) W_j - log|t| W_0) in FP32
+            // from the windows (window value W_j = b_j M_j, W_0 = -M_0)
+            float2 lr_[4][NR], s0[4];
 #pragma unroll
-            for (int c = 0; c < 4; c++) l0[c] = s0[c] = make_float2(0.f, 0.f);
+            for (int c = 0; c < 4; c++) {
+                s0[c] = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int i = 0; i < NR; i++) lr_[c][i] = make_float2(0.f, 0.f);
+            }
             for (int s = 0; ok && s < 12; s++, g++) {
                 const int b = g & 1;
                 if (!mbar_wait_bounded(WBAR(0 + b), (uint32_t)((g >> 1) & 1), abort_flag, A.wait_ns)) {
@@ -365,15 +386,19 @@ __global__ void __launch_bounds__(kWinThreads, 1) m2l_win_kernel(WinArgs A) {
 #pragma unroll
                     for (int c = 0; c < 4; c++) {
                         if (!v[c]) continue;
-                        const float2 *r0 = sR0 + win_offset_index(dxs[c], dys[c]) * HALF;
-                        float ax = l0[c].x, ay = l0[c].y;
+                        // (window values beyond the order are zero)
+                        const float2 *hf = sHf + win_offset_index(dxs[c], dys[c]) * KH;
 #pragma unroll
-                        for (int jp = 0; jp < HALF; jp++) {
-                            const float2 t = r0[jp];  // zero beyond the order
-                            ax = fmaf(t.x, mr[jp], fmaf(-t.y, mi[jp], ax));
-                            ay = fmaf(t.x, mi[jp], fmaf(t.y, mr[jp], ay));
+                        for (int i = 0; i < NR; i++) {
+                            float ax = lr_[c][i].x, ay = lr_[c][i].y;
+#pragma unroll
+                            for (int jp = 0; jp < HALF; jp++) {
+                                const float2 t = hf[i + jp];
+                                ax = fmaf(t.x, mr[jp], fmaf(-t.y, mi[jp], ax));
+                                ay = fmaf(t.x, mi[jp], fmaf(t.y, mr[jp], ay));
+                            }
+                            lr_[c][i] = make_float2(ax, ay);
                         }
-                        l0[c] = make_float2(ax, ay);
                         s0[c].x -= mr[0];  // M_0 = -W_0
                         s0[c].y -= mi[0];
                     }
@@ -407,13 +432,15 @@ __global__ void __launch_bounds__(kWinThreads, 1) m2l_win_kernel(WinArgs A) {
                 const int box = A.tbox[((size_t)R * 4 + c) * TB + tcol];
                 if (box >= 0) {
                     double2 *o = A.loc + (size_t)box * stride + A.c0 + chn;
-                    o[0] = make_double2((double)l0[c].x + lr * (double)s0[c].x,
-                                        (double)l0[c].y + lr * (double)s0[c].y);
+                    o[0] = make_double2((double)lr_[c][0].x + lr * (double)s0[c].x,
+                                        (double)lr_[c][0].y + lr * (double)s0[c].y);
 #pragma unroll
                     for (int i = 1; i < HALF; i++)
-                        if (i < P)
-                            o[(size_t)i * A.ndc] =
-                                make_double2(sAi[i] * (double)d[i], sAi[i] * (double)d[HALF + i]);
+                        if (i < P) {
+                            const double re = i < NR ? (double)lr_[c][i < NR ? i : 0].x : (double)d[i];
+                            const double im = i < NR ? (double)lr_[c][i < NR ? i : 0].y : (double)d[HALF + i];
+                            o[(size_t)i * A.ndc] = make_double2(sAi[i] * re, sAi[i] * im);
+                        }
                 }
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -503,16 +530,16 @@ template <int CH, int HALF>
 constexpr size_t win_smem_bytes() {
     return (size_t)(4 * kWinRows * 2 * HALF + 4 * 8 * HALF * 2 * HALF) * sizeof(float) +
            (size_t)kWinOffsets * 2 * HALF * sizeof(float4) +
-           (size_t)kWinOffsets * HALF * sizeof(float2) + (size_t)HALF * sizeof(double) +
+           (size_t)kWinOffsets * 2 * HALF * sizeof(float2) + (size_t)HALF * sizeof(double) +
            (size_t)HALF * sizeof(float);
 }
 
 // Tables of one (order, HALF): h_k(t) for the 40 offsets split into TF32
-// hi / lo, row 0 over the window values (-log|t| at j = 0, h_j(t) beyond,
-// zero from the order on), b_j and a_i; cached per device.
+// hi / lo, the same in FP32 with -log|t| at k = 0 (the leading rows over
+// the window values), b_j and a_i; cached per device.
 struct WinTables {
     const float4 *H = nullptr;
-    const float2 *R0 = nullptr;
+    const float2 *Hf = nullptr;
     const float *Bj = nullptr;
     const double *Ai = nullptr;
 };
@@ -543,21 +570,21 @@ WinTables win_tables(int p, int HALF, cudaStream_t s) {
         if (e.first == key) return e.second;
     const int KH = 2 * HALF;
     std::vector<float4> H((size_t)kWinOffsets * KH, make_float4(0.f, 0.f, 0.f, 0.f));
-    std::vector<float2> R0((size_t)kWinOffsets * HALF, make_float2(0.f, 0.f));
+    std::vector<float2> Hf((size_t)kWinOffsets * KH, make_float2(0.f, 0.f));
     for (int dy = -3; dy <= 3; dy++)
         for (int dx = -3; dx <= 3; dx++) {
             if (dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1) continue;
             const int o = win_offset_index(dx, dy);
             float4 *row = H.data() + (size_t)o * KH;
-            float2 *r0 = R0.data() + (size_t)o * HALF;
-            r0[0] = make_float2((float)(-0.5 * std::log((double)(dx * dx + dy * dy))), 0.f);
+            float2 *hf = Hf.data() + (size_t)o * KH;
+            hf[0] = make_float2((float)(-0.5 * std::log((double)(dx * dx + dy * dy))), 0.f);
             // h_1 = 1/t, h_{k+1} = h_k k / t
             const double2 ti = cinv(make_double2(dx, dy));
             double2 h = ti;
             for (int k = 1; k < KH; k++) {
                 const float2 re = tf32_split_host(h.x), im = tf32_split_host(h.y);
                 row[k] = make_float4(re.x, re.y, im.x, im.y);
-                if (k < HALF && k <= p) r0[k] = make_float2((float)h.x, (float)h.y);
+                hf[k] = make_float2((float)h.x, (float)h.y);
                 h = cscal(cmul(h, ti), (double)k);
             }
         }
@@ -583,16 +610,16 @@ WinTables win_tables(int p, int HALF, cudaStream_t s) {
     float *dB = nullptr;
     double *dA = nullptr;
     FMM_CUDA(cudaMalloc(&dH, H.size() * sizeof(float4)));
-    FMM_CUDA(cudaMalloc(&dR, R0.size() * sizeof(float2)));
+    FMM_CUDA(cudaMalloc(&dR, Hf.size() * sizeof(float2)));
     FMM_CUDA(cudaMalloc(&dB, Bj.size() * sizeof(float)));
     FMM_CUDA(cudaMalloc(&dA, Ai.size() * sizeof(double)));
     FMM_CUDA(cudaMemcpyAsync(dH, H.data(), H.size() * sizeof(float4), cudaMemcpyHostToDevice, s));
-    FMM_CUDA(cudaMemcpyAsync(dR, R0.data(), R0.size() * sizeof(float2), cudaMemcpyHostToDevice, s));
+    FMM_CUDA(cudaMemcpyAsync(dR, Hf.data(), Hf.size() * sizeof(float2), cudaMemcpyHostToDevice, s));
     FMM_CUDA(cudaMemcpyAsync(dB, Bj.data(), Bj.size() * sizeof(float), cudaMemcpyHostToDevice, s));
     FMM_CUDA(cudaMemcpyAsync(dA, Ai.data(), Ai.size() * sizeof(double), cudaMemcpyHostToDevice, s));
     FMM_CUDA(cudaStreamSynchronize(s));
     t.H = dH;
-    t.R0 = dR;
+    t.Hf = dR;
     t.Bj = dB;
     t.Ai = dA;
     cache.push_back({key, t});
@@ -768,144 +795,20 @@ bool win_plan(const Tree &T, const CauchyProblem &P, int CH, cudaStream_t s, Win
     return true;
 }
 
-// ---------------------------------------------------------------------------
-// Rows 1 .. NR-1 of the run's locals in FP32 on the CUDA cores (NR = 4, or
-// 6 when Hessians are requested).
-// The tensor-core kernel's TF32 x 3 products hold 22 of FP32's 24 bits;
-// from order kM2LExactFrom on, these leading coefficients -- which carry
-// most of the gradient at a leaf's points -- are recomputed here from FP32
-// windows of the multipoles and FP32 rows of the scaled shift (row 0 is
-// already summed on the CUDA cores by the tensor-core kernel)
-// (T_ij = t^-i B_ij (-1/t)^j, T_00 = log|t|, B as in l2dmploc) and stored
-// over the tensor-core values.  One block per run, one thread per row
-// (parent column t, channel) of the run, as in the tensor-core kernel; each
-// window is read from shared memory by the 3 shifts and 4 child positions
-// that use it.
-// ---------------------------------------------------------------------------
-template <int CH, int HALF, int NR>
-__global__ void __launch_bounds__(128) m2l_win_rows_kernel(WinArgs A,
-                                                           const float2 *__restrict__ Trows) {
-    constexpr int TB = 128 / CH, WP = TB + 2;
-    constexpr int CS = HALF * CH + 1;  // padded column stride of the window
-    // (dynamic: with six rows the tables and the window exceed 48 KB)
-    extern __shared__ float2 rows_smem[];
-    float2 *sTr = rows_smem;                         // [kWinOffsets * NR * HALF]
-    float2 *sWin = rows_smem + kWinOffsets * NR * HALF;  // [WP * CS]
-    const int tid = threadIdx.x, tcol = tid / CH, chn = tid - tcol * CH;
-    for (int e = tid; e < kWinOffsets * NR * HALF; e += blockDim.x) sTr[e] = Trows[e];
-    const int P = A.p + 1, stride = P * A.ndc;
-    for (int run = blockIdx.x; run < A.nrun; run += gridDim.x) {
-        const int R = A.run0 + run;
-        float2 acc[4][NR];
-#pragma unroll
-        for (int c = 0; c < 4; c++)
-#pragma unroll
-            for (int i = 1; i < NR; i++) acc[c][i] = make_float2(0.f, 0.f);
-        for (int s = 0; s < 12; s++) {
-            __syncthreads();  // the previous stage's window is no longer read
-            const int *wrow = A.wbox + ((size_t)R * 12 + s) * WP;
-            for (int e = tid; e < WP * HALF * CH; e += blockDim.x) {
-                const int col = e / (HALF * CH), r = e - col * HALF * CH;
-                const int j = r / CH, c = r - j * CH;
-                const int box = wrow[col];
-                sWin[col * CS + j * CH + c] =
-                    (box >= 0 && j < P) ? A.mp32[(size_t)box * stride + (size_t)j * A.ndc + A.c0 + c]
-                                        : make_float2(0.f, 0.f);
-            }
-            __syncthreads();
-#pragma unroll 1
-            for (int jj = -1; jj <= 1; jj++) {
-                const float2 *w = sWin + (tcol + jj + 1) * CS + chn;
-                float2 m[HALF];
-#pragma unroll
-                for (int j = 0; j < HALF; j++) m[j] = w[j * CH];
-#pragma unroll
-                for (int c = 0; c < 4; c++) {
-                    int dx, dy;
-                    if (!win_slot(s, jj, c, dx, dy)) continue;
-                    const float2 *tr = sTr + win_offset_index(dx, dy) * NR * HALF;
-#pragma unroll
-                    for (int i = 1; i < NR; i++) {
-                        float ax = acc[c][i].x, ay = acc[c][i].y;
-#pragma unroll
-                        for (int j = 0; j < HALF; j++) {
-                            const float2 t = tr[i * HALF + j];  // zero beyond the order
-                            ax = fmaf(t.x, m[j].x, fmaf(-t.y, m[j].y, ax));
-                            ay = fmaf(t.x, m[j].y, fmaf(t.y, m[j].x, ay));
-                        }
-                        acc[c][i] = make_float2(ax, ay);
-                    }
-                }
-            }
-        }
-#pragma unroll
-        for (int c = 0; c < 4; c++) {
-            const int box = A.tbox[((size_t)R * 4 + c) * TB + tcol];
-            if (box < 0) continue;
-            double2 *o = A.loc + (size_t)box * stride + A.c0 + chn;
-#pragma unroll
-            for (int i = 1; i < NR; i++)
-                if (i < P)
-                    o[(size_t)i * A.ndc] = make_double2((double)acc[c][i].x, (double)acc[c][i].y);
-        }
-    }
-}
-
-// FP32 rows i < NR of the scaled shift for the 40 window offsets,
-// [offset][i][HALF], zero from the order on; cached per device.
-const float2 *win_row_tables(int p, int HALF, int NR, cudaStream_t s) {
-    static std::mutex mu;
-    static std::vector<std::pair<long, const float2 *>> cache;
-    int dev;
-    FMM_CUDA(cudaGetDevice(&dev));
-    const long key = ((long)dev << 24) | ((long)NR << 16) | ((long)p << 8) | HALF;
-    std::lock_guard<std::mutex> g(mu);
-    for (auto &e : cache)
-        if (e.first == key) return e.second;
-    std::vector<double> C((size_t)(NR + HALF + 1) * (NR + HALF + 1), 0.0);
-    const int nc = NR + HALF + 1;
-    for (int l = 0; l < nc; l++) {
-        C[(size_t)l * nc] = 1.0;
-        for (int m = 1; m <= l; m++)
-            C[(size_t)l * nc + m] = C[(size_t)(l - 1) * nc + m - 1] + (m < l ? C[(size_t)(l - 1) * nc + m] : 0.0);
-    }
-    std::vector<float2> h((size_t)kWinOffsets * NR * HALF, make_float2(0.f, 0.f));
-    for (int dy = -3; dy <= 3; dy++)
-        for (int dx = -3; dx <= 3; dx++) {
-            if (dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1) continue;
-            float2 *T = h.data() + (size_t)win_offset_index(dx, dy) * NR * HALF;
-            const double tn = 1.0 / (double)(dx * dx + dy * dy);
-            const double2 w2 = make_double2(dx * tn, -dy * tn), w1 = make_double2(-w2.x, -w2.y);
-            double2 w2i = make_double2(1.0, 0.0);
-            for (int i = 0; i < NR; i++) {
-                double2 w1j = make_double2(1.0, 0.0);
-                for (int j = 0; j <= p && j < HALF; j++) {
-                    double b;
-                    if (i == 0)
-                        b = j == 0 ? 0.0 : 1.0;
-                    else
-                        b = j == 0 ? -1.0 / i : C[(size_t)(i + j - 1) * nc + (j - 1)];
-                    double2 v = cscal(cmul(w2i, w1j), b);
-                    if (i == 0 && j == 0) v = make_double2(0.5 * std::log((double)(dx * dx + dy * dy)), 0.0);
-                    T[i * HALF + j] = make_float2((float)v.x, (float)v.y);
-                    w1j = cmul(w1j, w1);
-                }
-                w2i = cmul(w2i, w2);
-            }
-        }
-    float2 *d = nullptr;
-    FMM_CUDA(cudaMalloc(&d, h.size() * sizeof(float2)));
-    FMM_CUDA(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(float2), cudaMemcpyHostToDevice, s));
-    FMM_CUDA(cudaStreamSynchronize(s));
-    cache.push_back({key, d});
-    return d;
-}
-
 template <int CH, int HALF>
 void launch_win(const WinPlan &W, const WinTables &tb, const Tree &T, const CauchyProblem &P,
                 int c0, const float2 *mp32, double2 *loc, int *err, cudaStream_t s) {
     constexpr size_t sm = win_smem_bytes<CH, HALF>();
-    auto kern = m2l_win_kernel<CH, HALF>;
+    // The tensor-core kernel's TF32 x 3 products hold 22 of FP32's 24 bits;
+    // from order kM2LExactFrom on, the leading coefficients -- which carry
+    // most of the gradient (and, with six, the Hessian) at a leaf's points
+    // -- are summed in FP32 on the CUDA cores from the same windows instead
+    // (row 0 always is: its terms cancel across the slots).
+    const bool hess = std::max(P.sset.n > 0 ? P.sset.pgh : 0, P.tset.n > 0 ? P.tset.pgh : 0) >= 3;
+    const int nr = !m2l_exact_rows(P.p) ? 1 : (hess ? kM2LExactRowsHess : kM2LExactRows);
+    auto kern = nr == 1 ? m2l_win_kernel<CH, HALF, 1>
+                        : (nr == kM2LExactRows ? m2l_win_kernel<CH, HALF, kM2LExactRows>
+                                               : m2l_win_kernel<CH, HALF, kM2LExactRowsHess>);
     raise_smem_limit(kern, (int)sm);
     for (const auto &r : W.ranges) {
         WinArgs a;
@@ -921,7 +824,7 @@ void launch_win(const WinPlan &W, const WinTables &tb, const Tree &T, const Cauc
         a.H = tb.H;
         a.Bj = tb.Bj;
         a.Ai = tb.Ai;
-        a.R0 = tb.R0;
+        a.Hf = tb.Hf;
         a.mp32 = mp32;
         a.loc = loc;
         a.err = err;
@@ -930,22 +833,6 @@ void launch_win(const WinPlan &W, const WinTables &tb, const Tree &T, const Cauc
         const int grid = std::max(1, std::min(r.second, kNumSM));
         kern<<<grid, kWinThreads, sm, s>>>(a);
         FMM_CHECK_LAUNCH();
-        if (m2l_exact_rows(P.p)) {
-            const int g2 = std::max(1, std::min(r.second, kNumSM * 8));
-            const bool hess =
-                std::max(P.sset.n > 0 ? P.sset.pgh : 0, P.tset.n > 0 ? P.tset.pgh : 0) >= 3;
-            auto rows = [&](auto kern, int nr) {
-                const size_t sm = (size_t)(kWinOffsets * nr * HALF + (128 / CH + 2) * (HALF * CH + 1)) *
-                                  sizeof(float2);
-                raise_smem_limit((const void *)kern, sm);
-                kern<<<g2, 128, sm, s>>>(a, win_row_tables(P.p, HALF, nr, s));
-            };
-            if (hess)
-                rows(m2l_win_rows_kernel<CH, HALF, kM2LExactRowsHess>, kM2LExactRowsHess);
-            else
-                rows(m2l_win_rows_kernel<CH, HALF, kM2LExactRows>, kM2LExactRows);
-            FMM_CHECK_LAUNCH();
-        }
     }
 }
 
