@@ -1,6 +1,8 @@
 // common.cu -- device-wide exclusive scan and the library's last-error slot.
 #include "common.cuh"
 
+#include <string.h>
+
 #include <atomic>
 #include <map>
 #include <mutex>
@@ -181,6 +183,31 @@ void prof_end(cudaStream_t s) {
     }
     for (auto &c : g_prof.counts) g_prof.result.push_back({"#" + c.first, c.second});
     g_prof.active = false;
+}
+
+void read_small(void *host, const void *dptr, size_t bytes, cudaStream_t s) {
+    static thread_local void *buf = nullptr;
+    static thread_local size_t cap = 0;
+    if (bytes > cap) {
+        if (buf) cudaFreeHost(buf);
+        buf = nullptr;
+        cap = 0;
+        const size_t want = bytes > 4096 ? bytes : 4096;
+        if (cudaHostAlloc(&buf, want, cudaHostAllocPortable) == cudaSuccess)
+            cap = want;
+        else {
+            cudaGetLastError();
+            buf = nullptr;
+        }
+    }
+    if (!buf) {
+        FMM_CUDA(cudaMemcpyAsync(host, dptr, bytes, cudaMemcpyDeviceToHost, s));
+        FMM_CUDA(cudaStreamSynchronize(s));
+        return;
+    }
+    FMM_CUDA(cudaMemcpyAsync(buf, dptr, bytes, cudaMemcpyDeviceToHost, s));
+    FMM_CUDA(cudaStreamSynchronize(s));
+    memcpy(host, buf, bytes);
 }
 
 void prof_set_count(const char *name, double value) {

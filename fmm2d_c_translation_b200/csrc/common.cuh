@@ -201,11 +201,16 @@ void exclusive_scan_i32(const int *in, int *out, int64_t n, int *d_total,
                         cudaStream_t s);
 
 // Device -> host copy of a few scalars with a stream sync.
+// Copies a few bytes (counts, flags) from device to host memory and waits
+// for the stream.  The copy goes through a pinned buffer of the calling
+// thread, so it is not staged behind large copies that other streams have
+// in flight (as a copy into pageable memory can be).
+void read_small(void *host, const void *dptr, size_t bytes, cudaStream_t s);
+
 template <class T>
 inline T read_scalar(const T *dptr, cudaStream_t s) {
     T v;
-    FMM_CUDA(cudaMemcpyAsync(&v, dptr, sizeof(T), cudaMemcpyDeviceToHost, s));
-    FMM_CUDA(cudaStreamSynchronize(s));
+    read_small(&v, dptr, sizeof(T), s);
     return v;
 }
 

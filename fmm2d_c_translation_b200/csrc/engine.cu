@@ -351,7 +351,6 @@ void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaS
         P.src_hl = G.src_hl.get();
         P.trg_hl = G.trg_hl.get();
     }
-    cauchy_fmm(T, P, s);
     // ---- back to input order, in the caller's layout ----
     // (with a copy stream, each output's device-to-host copy starts once its
     // scatter is done; the staging buffers live until the copies are)
@@ -463,9 +462,9 @@ void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaS
         flush(og);
         flush(oh);
     };
+    cauchy_fmm(T, P, s);
+    unsort(nt, T.itarg.get(), tpgh, tpot, tgrad, thess, c.pottarg, c.gradtarg, c.hesstarg);
     unsort(ns, T.isrc.get(), spgh, spot, sgrad, shess, c.pot, c.grad, c.hess);
-    unsort(nt, T.itarg.get(), tpgh, tpot, tgrad, thess, c.pottarg, c.gradtarg,
-           c.hesstarg);
     if (overlap) {
         // the call ends (and the staging buffers are freed on s) after the copies
         cudaEvent_t e;
@@ -491,12 +490,19 @@ void run_laplace_family(const FmmCall &c, CallCtx &ctx) {
         laplace_geometry(c, on_dev, s, G);
         laplace_evaluate(c, G, on_dev, s);
     } else {
-        // Host arrays: the strengths go to the device on the copy stream
-        // while the positions are copied and the tree is built on s; the
-        // outputs come back on the copy stream array by array.
+        // Host arrays: the positions go to the device first, at the link's
+        // full rate; the strengths follow on the copy stream while the tree
+        // is built on s; the targets' outputs come back on the copy stream
+        // while the sources' are computed, then the sources'.
         cudaStream_t cs = ctx.copy_stream();
         const size_t sw = c.kernel == kReal ? 1 : 2;
         const size_t nsd = (size_t)c.nd * c.ns;
+        DevBuf<double2> dsrc(c.ns, s), dtrg(c.nt > 0 ? c.nt : 0, s);
+        FMM_CUDA(cudaMemcpyAsync(dsrc.get(), c.sources, (size_t)c.ns * sizeof(double2),
+                                 cudaMemcpyHostToDevice, s));
+        if (c.nt > 0 && c.targ)
+            FMM_CUDA(cudaMemcpyAsync(dtrg.get(), c.targ, (size_t)c.nt * sizeof(double2),
+                                     cudaMemcpyHostToDevice, s));
         DevBuf<double> dq, dd, dv;
         if (c.ifcharge) dq.alloc(sw * nsd, s);
         if (c.ifdipole) {
@@ -517,7 +523,8 @@ void run_laplace_family(const FmmCall &c, CallCtx &ctx) {
                 cudaEventDestroy(b);
             }
         } guard{e0, e1, cs};
-        FMM_CUDA(cudaEventRecord(e0, s));  // the allocations above are ordered on s
+        // (after the positions' copies and the allocations, which are ordered on s)
+        FMM_CUDA(cudaEventRecord(e0, s));
         FMM_CUDA(cudaStreamWaitEvent(cs, e0, 0));
         auto up = [&](DevBuf<double> &b, const double *h, size_t n) {
             if (b.get() && h)
@@ -528,7 +535,12 @@ void run_laplace_family(const FmmCall &c, CallCtx &ctx) {
         up(dv, c.dipvec, 2 * nsd);
         FMM_CUDA(cudaEventRecord(e1, cs));
         LapGeometry G;
-        laplace_geometry(c, false, s, G);
+        FmmCall cg = c;
+        cg.sources = reinterpret_cast<const double *>(dsrc.get());
+        cg.targ = c.nt > 0 ? reinterpret_cast<const double *>(dtrg.get()) : nullptr;
+        laplace_geometry(cg, true, s, G);
+        dsrc.release();
+        dtrg.release();
         FMM_CUDA(cudaStreamWaitEvent(s, e1, 0));
         FmmCall c2 = c;
         c2.charge = c.ifcharge ? dq.get() : nullptr;

@@ -38,7 +38,9 @@
 // slot's tile to FP64 sums in shared memory: the FP32 accumulation then
 // spans one slot's K chunks (a few tens of MMAs) instead of all 27 slots,
 // whose hundreds of FP32 roundings measured 4e-6 relative in the
-// potential.  At the end of a tile the FP64 sums are added to the local
+// potential.  (A caller whose products are small beside the result -- the
+// tail of the split-precision Laplace M2L -- accumulates a tile's slots in
+// one tile and has it summed once, `group`.)  At the end of a tile the FP64 sums are added to the local
 // expansions.  Levels with fewer tiles than SMs split the 27 slots over
 // slices of blocks (grid rows), each writing FP64 partial sums that a
 // second kernel adds in slice order.  Every wait is bounded in time; a wait that runs out
@@ -85,6 +87,11 @@ struct HtArgs {
     // one slice, writes its FP64 partial sums to part[y][plan row - q_lo][W][nd]
     double2 *part;
     int q_lo, nq;
+    // consecutive slots that share one tensor-memory accumulator before the
+    // epilogue adds it to the FP64 sums: 1 (every slot summed in FP64), or
+    // 27 (one FP32 accumulation over the tile's slots, for products whose
+    // FP32 accumulation error is far below the result's tolerance)
+    int group;
 };
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, uint32_t bytes) {
@@ -225,7 +232,8 @@ __global__ void __launch_bounds__(kHtThreads, 1) slot_gemm_tc_kernel(HtArgs A) {
         for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x) {
 #pragma unroll 4
             for (int c = 0; c < NP; c++) sSum[c * kHtRows + r] = 0.0;
-            for (int k = k0; k < k1; k++, g++) {
+            for (int k = k0; k < k1; k++) {
+                if ((k - k0) % A.group != A.group - 1 && k != k1 - 1) continue;  // (not a group's end)
                 const int a = (int)(g & 1);
                 const bool got = mbar_wait_backoff(HBAR(2 * kHtStages + a), (uint32_t)((g >> 1) & 1),
                                                    abort_flag, A.wait_ns);
@@ -248,6 +256,7 @@ __global__ void __launch_bounds__(kHtThreads, 1) slot_gemm_tc_kernel(HtArgs A) {
                 mbar_arrive(HBAR(2 * kHtStages + 2 + a));
 #pragma unroll
                 for (int c = 0; c < NP; c++) sSum[c * kHtRows + r] += (double)d[c];
+                g++;
             }
             if (!ok) break;
             int cp, q0;
@@ -281,20 +290,26 @@ __global__ void __launch_bounds__(kHtThreads, 1) slot_gemm_tc_kernel(HtArgs A) {
         // (fault injection: nothing is issued or committed, so the other
         // roles' bounded waits run out)
         for (int tile = blockIdx.x; ok && !A.stall && tile < ntiles; tile += gridDim.x) {
-            for (int k = k0; ok && k < k1; k++, g++) {
-                // the slot's accumulator tile, once the epilogue has read it
-                // two slots ago
-                const int a = (int)(g & 1);
-                const bool freed = g < 2 || mbar_wait_bounded(HBAR(2 * kHtStages + 2 + a),
-                                                              (uint32_t)(((g >> 1) - 1) & 1),
-                                                              abort_flag, A.wait_ns);
-                if (!__all_sync(0xffffffffu, freed)) {
-                    ok = false;
-                    break;
+            uint32_t acc = 0u, dt = tmem;
+            int a = 0;
+            for (int k = k0; ok && k < k1; k++) {
+                const bool gstart = (k - k0) % A.group == 0;
+                const bool gend = (k - k0) % A.group == A.group - 1 || k == k1 - 1;
+                if (gstart) {
+                    // the group's accumulator tile, once the epilogue has
+                    // read it two groups ago
+                    a = (int)(g & 1);
+                    const bool freed = g < 2 || mbar_wait_bounded(HBAR(2 * kHtStages + 2 + a),
+                                                                  (uint32_t)(((g >> 1) - 1) & 1),
+                                                                  abort_flag, A.wait_ns);
+                    if (!__all_sync(0xffffffffu, freed)) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    dt = tmem + (uint32_t)(a * 128);
+                    acc = 0u;
                 }
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t dt = tmem + (uint32_t)(a * 128);
-                uint32_t acc = 0u;
                 for (int kc = 0; kc < KC; kc++, step++) {
                     const int s = (int)(step % kHtStages);
                     const long long u = step / kHtStages;
@@ -325,8 +340,11 @@ __global__ void __launch_bounds__(kHtThreads, 1) slot_gemm_tc_kernel(HtArgs A) {
                     issued = true;
                 }
                 if (!ok) break;
-                if (lane == 0) tc_commit(HBAR(2 * kHtStages + a));
-                __syncwarp();
+                if (gend) {
+                    if (lane == 0) tc_commit(HBAR(2 * kHtStages + a));
+                    __syncwarp();
+                    g++;
+                }
             }
         }
         if (!ok) *abort_flag = 1;
@@ -493,6 +511,7 @@ bool slot_gemm_tc_level(const SlotGemmLevel &g, const SlotPlan &spl, int *err, c
     a.err = err;
     a.stall = tc_stall_injected();
     a.wait_ns = tc_wait_limit_ns();
+    a.group = g.group >= 1 ? g.group : 1;
     // levels with fewer tiles than SMs (the coarse ones) split the 27 slots
     // over slices of blocks, whose FP64 partial sums are added in slice order
     const int nslice = ntiles < kNumSM ? std::min(kHtSlots, std::max(1, kNumSM / ntiles)) : 1;

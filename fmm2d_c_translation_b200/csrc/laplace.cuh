@@ -178,6 +178,9 @@ struct SlotGemmLevel {
     const float *bimg = nullptr;  // [cp][27][KP / 16][hi KP x 16 | lo KP x 16]
     double2 *out = nullptr;       // [box - lstart][W][nd]
     double oscale = 1.0;
+    // slots accumulated in FP32 before each FP64 sum: 1, or 27 for one
+    // FP32 accumulation over all slots of a tile
+    int group = 1;
 };
 // K (= N) of W complex coefficients: 2 W rounded up to 16 (at least 32),
 // 0 when above the largest supported (96).

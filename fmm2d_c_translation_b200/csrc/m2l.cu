@@ -336,8 +336,7 @@ bool m2l_work(const Tree &T, const CauchyProblem &P, int tile, cudaStream_t s, M
     while ((1 << bits) <= nseg) bits++;
     radix_sort_pairs(kp, vp, w.kt.get(), w.vt.get(), n, bits, s);
     std::vector<int> hc(nseg + 1);
-    FMM_CUDA(cudaMemcpyAsync(hc.data(), cp, (nseg + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
-    FMM_CUDA(cudaStreamSynchronize(s));
+    read_small(hc.data(), cp, (nseg + 1) * sizeof(int), s);
     std::vector<int> h(5 * nseg + 1);
     int *tb = h.data(), *st = tb + nseg + 1, *ct = st + nseg, *lv = ct + nseg, *cpv = lv + nseg;
     int run = 0, start = 0;
@@ -960,16 +959,21 @@ bool m2l_tensor_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp,
 // ---------------------------------------------------------------------------
 // Split-precision M2L (eps below the mixed mode's range, all other passes
 // FP64).  The scaled shift's terms T_ij M_j fall off with the total order
-// i + j (about 0.47^(i+j) relative in the reference's worst case, the
-// ratio behind l2dterms).  The leading triangle i + j < NT, which carries
-// the potential down to that ratio to the NT, runs in FP64 on the DMMA
-// kernel (the first writer of every local); the tail i + j >= NT runs as
-// TF32 x 3 slot GEMMs on the tcgen05 tensor cores (slot_gemm_tc_level,
-// about 2^-22 relative per product, every slot summed in FP64) and is added
-// on top.  With NT = p + 1 - kSplitTailOrders the tail's share of the
-// potential is about 0.47^-kSplitTailOrders below eps in the worst case.
+// n = i + j: for the nearest list-2 offsets (|t| = 2) and points at the
+// box corners their share of the potential is about 0.707^n, and measured
+// errors fall about 8x per 4 orders.  The leading triangle i + j < NT runs
+// in FP64 on the DMMA kernel (the first writer of every local); the tail
+// i + j >= NT runs as TF32 x 3 slot GEMMs on the tcgen05 tensor cores
+// (slot_gemm_tc_level, about 2^-22 relative per product, one FP32
+// accumulation over a tile's slots: the tail is small beside the result)
+// and is added on top.  The tail's error falls about 0.59x per order of NT
+// and eps about 0.47x per order of p, so NT grows faster than p:
+// NT = 4 (p - 13) / 3 (rounded up to a multiple of 4) holds gradients and
+// Hessians on clustered points within eps at 1e-9 (p = 28, NT = 20) and
+// 1e-10 (p = 31, NT = 24).  At 1e-12 (p = 37) even NT = 32 left the
+// Hessians of clustered points at 2e-11, twenty times the FP64 mode's
+// error: orders above 31 keep the FP64 M2L.
 // ---------------------------------------------------------------------------
-constexpr int kSplitTailOrders = 14;
 
 // The tail images (i + j >= nt) of the 4 x 27 slot operators in real form,
 // T_ij = w2^i B_ij w1^j (w2 = 1/t, w1 = -1/t, t the slot offset), TF32
@@ -1046,7 +1050,6 @@ bool launch_split_triangle(const SegTable &sg, const int *boxes, const int *slot
         launch_dmma<MT_, KS_, NT>(sg, boxes, slots, bs, ndc, p, binom, mp, loc, ntiles, s); \
         return true;                                                                       \
     }
-    FMM_SPLIT_CASE(3, 6)
     FMM_SPLIT_CASE(4, 8)
     FMM_SPLIT_CASE(5, 10)
     FMM_SPLIT_CASE(6, 12)
@@ -1060,22 +1063,24 @@ struct SplitHold {
 };
 }  // namespace
 
+// 0: the order keeps the FP64 M2L
 int split_triangle_order(int p) {
     const char *e = getenv("FMM2D_B200_SPLIT_NT");
-    int nt = e ? atoi(e) : p + 1 - kSplitTailOrders;
-    // the supported triangles: 8, 12, 16, 20, 24
+    if (!e && p > 31) return 0;
+    int nt = e ? atoi(e) : (4 * (p - 13) + 2) / 3;
+    // the supported triangles: 8, 12, ..., 32
     if (nt < 8) nt = 8;
     nt = (nt + 3) / 4 * 4;
-    return nt > 24 ? 24 : nt;
+    return nt > 32 ? 0 : nt;
 }
 
 bool m2l_split_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp, double2 *loc,
                     cudaStream_t s) {
     const int L = T.nlevels, p = P.p, W = p + 1;
-    if (L < 2 || W < 12 || W > 48 || P.ndc > 128) return false;
+    if (L < 2 || W < 20 || W > 48 || P.ndc > 128) return false;
     const int KP = slot_gemm_kp(W);
     const int nt = split_triangle_order(p);
-    if (KP == 0 || nt >= 2 * W - 1) return false;
+    if (KP == 0 || nt == 0 || nt >= 2 * W - 1) return false;
     // planning first (nothing is launched when it fails)
     bool ok = false;
     const auto wp = m2l_cached<M2LWork>(P.m2l_cache, m2l_key(1, 8, 0), ok,
@@ -1102,6 +1107,8 @@ bool m2l_split_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp, do
         case 16: launched = launch_split_triangle<16>(sg, boxes, w.slots.get(), bs, P.ndc, p, binom, mp, loc, w.ntiles, s); break;
         case 20: launched = launch_split_triangle<20>(sg, boxes, w.slots.get(), bs, P.ndc, p, binom, mp, loc, w.ntiles, s); break;
         case 24: launched = launch_split_triangle<24>(sg, boxes, w.slots.get(), bs, P.ndc, p, binom, mp, loc, w.ntiles, s); break;
+        case 28: launched = launch_split_triangle<28>(sg, boxes, w.slots.get(), bs, P.ndc, p, binom, mp, loc, w.ntiles, s); break;
+        case 32: launched = launch_split_triangle<32>(sg, boxes, w.slots.get(), bs, P.ndc, p, binom, mp, loc, w.ntiles, s); break;
         default: break;
     }
     if (!launched) return false;
@@ -1134,6 +1141,7 @@ bool m2l_split_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp, do
         g.bimg = bimg;
         g.out = loc + (size_t)lo * stride;
         g.oscale = 1.0;
+        g.group = 27;
         if (!slot_gemm_tc_level(g, hp->spl, errp, s))
             throw FmmError(4, "split-precision M2L: unsupported tensor-core level shape");
     }

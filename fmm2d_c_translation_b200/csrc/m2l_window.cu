@@ -113,11 +113,6 @@ struct WinArgs {
     unsigned long long wait_ns;  // limit of every bounded wait of the roles
 };
 
-__device__ __forceinline__ void split_tf32(float v, float &hi, float &lo) {
-    hi = tc_tf32(v);
-    lo = tc_tf32(v - hi);
-}
-
 // Window values: hi = tf32(v) and lo = v - hi, the exact FP32 residual, so
 // that hi + lo gives back v for the rows summed on the CUDA cores (the MMA
 // reads lo at TF32 precision).
@@ -775,8 +770,7 @@ bool win_plan(const Tree &T, const CauchyProblem &P, int CH, cudaStream_t s, Win
         });
     }
     std::vector<int> hc(128);
-    FMM_CUDA(cudaMemcpyAsync(hc.data(), cnt.get(), 128 * sizeof(int), cudaMemcpyDeviceToHost, s));
-    FMM_CUDA(cudaStreamSynchronize(s));
+    read_small(hc.data(), cnt.get(), 128 * sizeof(int), s);
     // a level goes through the windows when its runs are at least 1/8 full
     int start = 0, open = -1;
     for (int l = 0; l <= L + 1 && l < 64; l++) {

@@ -1069,9 +1069,7 @@ bool build_by_keys(const double2 *d_src, int ns, const double2 *d_targ, int nt, 
             const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)ns + 255) / 256, kNumSM * 8));
             refine_count_kernel<<<blocks, 256, 0, s>>>(B.kvs, ns, ndiv, ds, nw, dc.get());
             FMM_CHECK_LAUNCH();
-            FMM_CUDA(cudaMemcpyAsync(kc.data() + 1, dc.get() + 1, 64 * sizeof(unsigned long long),
-                                     cudaMemcpyDeviceToHost, s));
-            FMM_CUDA(cudaStreamSynchronize(s));
+            read_small(kc.data() + 1, dc.get() + 1, 64 * sizeof(unsigned long long), s);
         }
         // a box of the deepest digit level still to be split: more digits
         if (ds < 64 && ds <= nlmax - 1 && kc[ds] > 0) return false;
@@ -1128,8 +1126,7 @@ bool build_by_keys(const double2 *d_src, int ns, const double2 *d_targ, int nt, 
     if (known && ilev > 0) {
         // every level's own count must equal the one the keys gave
         std::vector<int> h(ilev);
-        FMM_CUDA(cudaMemcpyAsync(h.data(), chk.get(), ilev * sizeof(int), cudaMemcpyDeviceToHost, s));
-        FMM_CUDA(cudaStreamSynchronize(s));
+        read_small(h.data(), chk.get(), ilev * sizeof(int), s);
         for (int l = 0; l < ilev; l++)
             if ((unsigned long long)h[l] != kc[l]) {
                 T.boxsize.resize(1);
@@ -1159,9 +1156,7 @@ void build_tree(const double2 *d_src, int ns, const double2 *d_targ, int nt,
     bbox_kernel<<<nblk, 256, 0, s>>>(d_src, ns, d_targ, nt, part.get());
     FMM_CHECK_LAUNCH();
     std::vector<double> hp(4 * nblk);
-    FMM_CUDA(cudaMemcpyAsync(hp.data(), part.get(), hp.size() * sizeof(double),
-                             cudaMemcpyDeviceToHost, s));
-    FMM_CUDA(cudaStreamSynchronize(s));
+    read_small(hp.data(), part.get(), hp.size() * sizeof(double), s);
     double xmin = hp[0], xmax = hp[1], ymin = hp[2], ymax = hp[3];
     for (int k = 1; k < nblk; k++) {
         xmin = std::min(xmin, hp[4 * k]);
