@@ -300,7 +300,41 @@ __global__ void __launch_bounds__(256) eval_far_points_kernel(
                 }
             }
         }
-        {
+        // the two channels of a pair side by side in the FP32 locals: one
+        // 16-byte load per coefficient for both Horner chains
+        bool paired = false;
+        if constexpr (MIXED && CH == 2) {
+            if (loc32 && (ndc & 1) == 0 && (c0 & 1) == 0) {
+                paired = true;
+                const double2 cb = centers[b];
+                const double rbi = 1.0 / bs[lb];
+                const R2 z = mk2<R2>((x.x - cb.x) * rbi, (x.y - cb.y) * rbi);
+                const R rinv = (R)rbi;
+                const int s4 = ndc >> 1;
+                const float4 *L4 = reinterpret_cast<const float4 *>(loc32 + (size_t)b * stride + c0);
+                float4 v = L4[(size_t)p * s4];
+                R2 a0[2] = {mk2<R2>(v.x, v.y), mk2<R2>(v.z, v.w)};
+                R2 a1[2] = {mk2<R2>(0.0, 0.0), mk2<R2>(0.0, 0.0)};
+                R2 a2[2] = {mk2<R2>(0.0, 0.0), mk2<R2>(0.0, 0.0)};
+                for (int m = p - 1; m >= 0; m--) {
+                    v = L4[(size_t)m * s4];
+                    const R2 c[2] = {mk2<R2>(v.x, v.y), mk2<R2>(v.z, v.w)};
+#pragma unroll
+                    for (int q = 0; q < 2; q++) {
+                        if (PGH >= 3) a2[q] = zadd(zmul(a2[q], z), a1[q]);
+                        if (PGH >= 2) a1[q] = zadd(zmul(a1[q], z), a0[q]);
+                        a0[q] = zadd(zmul(a0[q], z), c[q]);
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < 2; q++) {
+                    po[q] = zadd(po[q], a0[q]);
+                    if (PGH >= 2) gr[q] = zadd(gr[q], zscal(a1[q], rinv));
+                    if (PGH >= 3) he[q] = zadd(he[q], zscal(a2[q], (R)2 * rinv * rinv));
+                }
+            }
+        }
+        if (!paired) {
             const double2 cb = centers[b];
             const double rb = bs[lb];
             const R2 z = mk2<R2>((x.x - cb.x) / rb, (x.y - cb.y) / rb);
@@ -1526,6 +1560,90 @@ __global__ void __launch_bounds__(kPowWarps * 32) p2m_warp_kernel(
     }
 }
 
+// P2M of the mixed mode: the same scheme with the power series and its
+// sums in FP32 (the multipoles feed the FP32 / TF32 M2L, which reads them
+// rounded to FP32), from FP32 charges; the scaled offsets (x - c) / r and
+// d / r are formed in FP64 before the conversion.
+inline size_t pow32_warp_smem(int p, int CH) {
+    return (size_t)kPowWarps * kPowSrc * (p + 1 + 2 * CH) * sizeof(float2);
+}
+
+template <int CH>
+__global__ void __launch_bounds__(kPowWarps * 32) p2m_warp32_kernel(
+    int lo, int hi, int p, const int *__restrict__ nchild, const double2 *__restrict__ centers,
+    const int *__restrict__ level, const double *__restrict__ bs, const int2 *__restrict__ sse,
+    const double2 *__restrict__ src, const float2 *__restrict__ chg32,
+    const double2 *__restrict__ dip, int ifc, int ifd, int ndc, int c0,
+    double2 *__restrict__ mp) {
+    extern __shared__ float2 pow32_smem[];
+    const int P = p + 1, stride = P * ndc;
+    const int lane = lane_id(), wib = threadIdx.x >> 5;
+    float2 *sPw = pow32_smem + (size_t)wib * kPowSrc * (P + 2 * CH);
+    float2 *sSt = sPw + kPowSrc * P;
+    const float2 z0 = make_float2(0.f, 0.f);
+    for (int b = lo + warp_global(); b < hi; b += warp_count()) {
+        if (nchild[b] != 0) continue;
+        const int2 rg = sse[b];
+        if (rg.y <= rg.x) continue;
+        const double2 c = centers[b];
+        const double rinv = 1.0 / bs[level[b]];
+        float2 acc[2][CH];
+#pragma unroll
+        for (int h = 0; h < 2; h++)
+#pragma unroll
+            for (int q = 0; q < CH; q++) acc[h][q] = z0;
+        for (int j0 = rg.x; j0 < rg.y; j0 += kPowSrc) {
+            const int n = min(kPowSrc, rg.y - j0);
+            __syncwarp();
+            if (lane < n) {
+                const int j = j0 + lane;
+                const double2 x = src[j];
+                const float2 base = make_float2((float)((x.x - c.x) * rinv), (float)((x.y - c.y) * rinv));
+#pragma unroll
+                for (int q = 0; q < CH; q++) {
+                    sSt[lane * 2 * CH + q] = ifc ? chg32[(size_t)j * ndc + c0 + q] : z0;
+                    const double2 d = ifd ? dip[(size_t)j * ndc + c0 + q] : make_double2(0.0, 0.0);
+                    sSt[lane * 2 * CH + CH + q] = make_float2((float)(d.x * rinv), (float)(d.y * rinv));
+                }
+                float2 w = make_float2(1.f, 0.f);
+                for (int k = 0; k < P; k++) {
+                    sPw[lane * P + k] = w;
+                    w = zmul(w, base);
+                }
+            }
+            __syncwarp();
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int k = lane + 32 * h;
+                if (k >= P) break;
+                const float ik = k > 0 ? -1.f / (float)k : 0.f;
+                for (int s = 0; s < n; s++) {
+                    const float2 pk = sPw[s * P + k];
+                    const float2 pd = k > 0 ? sPw[s * P + k - 1] : z0;  // z^(k-1) for the dipole
+#pragma unroll
+                    for (int q = 0; q < CH; q++) {
+                        const float2 qv = sSt[s * 2 * CH + q], dv = sSt[s * 2 * CH + CH + q];
+                        if (k == 0)
+                            acc[h][q] = zadd(acc[h][q], qv);
+                        else
+                            zfma(acc[h][q], qv, zscal(pk, ik));
+                        zfma(acc[h][q], dv, pd);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int k = lane + 32 * h;
+            if (k >= P) break;
+#pragma unroll
+            for (int q = 0; q < CH; q++)
+                mp[(size_t)b * stride + (size_t)k * ndc + c0 + q] =
+                    make_double2((double)acc[h][q].x, (double)acc[h][q].y);
+        }
+    }
+}
+
 template <int CH>
 __global__ void __launch_bounds__(kPowWarps * 32) p2l_warp_kernel(
     int lo, int hi, int p, EvalCounts ec, const int *__restrict__ nlist4,
@@ -1586,7 +1704,14 @@ void upward_chunk(const Tree &T, const CauchyProblem &P, int c0,
     const bool warpk = p + 1 <= 40;
     if (L >= 2) {
         const int lo = T.lstart[2];
-        if (warpk) {
+        if (warpk && P.mixed && (P.charge32 || !P.ifcharge)) {
+            const size_t sm = pow32_warp_smem(p, CH);
+            raise_smem_limit(p2m_warp32_kernel<CH>, (int)sm);
+            p2m_warp32_kernel<CH><<<pow_grid(nb - lo), kPowWarps * 32, sm, s>>>(
+                lo, nb, p, T.nchild.get(), T.centers.get(), T.level.get(), bs,
+                T.srcse.get(), P.src, P.charge32, P.dipstr, P.ifcharge, P.ifdipole,
+                P.ndc, c0, mp);
+        } else if (warpk) {
             const size_t sm = pow_warp_smem(p, CH);
             raise_smem_limit(p2m_warp_kernel<CH>, (int)sm);
             p2m_warp_kernel<CH><<<pow_grid(nb - lo), kPowWarps * 32, sm, s>>>(

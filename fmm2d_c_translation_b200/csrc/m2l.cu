@@ -968,11 +968,12 @@ bool m2l_tensor_fp64(const Tree &T, const CauchyProblem &P, const double2 *mp,
 // accumulation over a tile's slots: the tail is small beside the result)
 // and is added on top.  The tail's error falls about 0.59x per order of NT
 // and eps about 0.47x per order of p, so NT grows faster than p:
-// NT = 4 (p - 13) / 3 (rounded up to a multiple of 4) holds gradients and
-// Hessians on clustered points within eps at 1e-9 (p = 28, NT = 20) and
-// 1e-10 (p = 31, NT = 24).  At 1e-12 (p = 37) even NT = 32 left the
-// Hessians of clustered points at 2e-11, twenty times the FP64 mode's
-// error: orders above 31 keep the FP64 M2L.
+// NT = 4 (p - 13) / 3 + 2 (rounded up to a multiple of 4) holds gradients
+// and Hessians on clustered points within eps of the FP64 mode at 1e-9
+// (p = 28, NT = 24) and 1e-10 (p = 31, NT = 28; 24 left Hessians 1.15e-10
+// off).  At 1e-12 (p = 37) even NT = 32 left the Hessians of clustered
+// points at 2e-11, twenty times the FP64 mode's error: orders above 31 keep
+// the FP64 M2L.
 // ---------------------------------------------------------------------------
 
 // The tail images (i + j >= nt) of the 4 x 27 slot operators in real form,
@@ -1067,7 +1068,7 @@ struct SplitHold {
 int split_triangle_order(int p) {
     const char *e = getenv("FMM2D_B200_SPLIT_NT");
     if (!e && p > 31) return 0;
-    int nt = e ? atoi(e) : (4 * (p - 13) + 2) / 3;
+    int nt = e ? atoi(e) : (4 * (p - 13) + 2) / 3 + 2;
     // the supported triangles: 8, 12, ..., 32
     if (nt < 8) nt = 8;
     nt = (nt + 3) / 4 * 4;

@@ -12,12 +12,13 @@
 // blocks are reused by the next ones without returning to the driver.
 //
 // Continuous batching: a worker that takes a small lfmm2d request also
-// takes the queued requests of the same kind (eps, precision, strengths,
-// output flags) that fit the budget, up to kBatchMax requests and
-// kBatchPoints points, and evaluates them together as one forest
-// (run_laplace_batch): one launch per level and pass for all of them.  Their
-// trees differ from the ones they would get alone, so their results agree
-// with the alone ones to the requested eps.  FMM2D_B200_SERVE_BATCH=0, read
+// takes the queued requests of the same kind (arithmetic -- mixed, FP64 or
+// split --, strengths, output flags) that fit the budget, up to kBatchMax
+// requests and kBatchPoints points, and evaluates them together as one
+// forest (run_laplace_batch) at the smallest eps among them: one launch per
+// level and pass for all of them.  Their trees (and, for the looser eps,
+// their orders) differ from the ones they would get alone, so their results
+// agree with the alone ones to the requested eps.  FMM2D_B200_SERVE_BATCH=0, read
 // when the server is made, turns batching off.
 //
 // The reference has no counterpart (its entry points are single calls).
@@ -85,8 +86,17 @@ bool batchable(const FmmCall &c) {
            (int64_t)c.ns + c.nt <= kBatchRequest;
 }
 
+// The arithmetic a call runs in: 2 mixed (explicit, or auto at eps >= 0.5e-6),
+// else its precision code (all-FP64 or split).
+int arith_class(const FmmCall &c) {
+    const bool mixed = c.precision == kPrecMixed || (c.precision == kPrecAuto && c.eps >= 0.5e-6);
+    return mixed ? kPrecMixed : (c.precision == kPrecAuto ? kPrecFP64 : c.precision);
+}
+
+// Requests of one arithmetic and output layout batch together; the batch
+// runs at the smallest eps among them, which meets every member's eps.
 bool same_kind(const FmmCall &a, const FmmCall &b) {
-    return a.eps == b.eps && a.precision == b.precision && a.ifcharge == b.ifcharge &&
+    return arith_class(a) == arith_class(b) && a.ifcharge == b.ifcharge &&
            a.ifdipole == b.ifdipole && a.ifpgh == b.ifpgh && (a.nt > 0) == (b.nt > 0) &&
            (a.nt == 0 || a.ifpghtarg == b.ifpghtarg);
 }
@@ -237,6 +247,7 @@ class Server {
         BatchCall b;
         b.kernel = c0.kernel;
         b.eps = c0.eps;
+        for (const Request *r : batch) b.eps = std::min(b.eps, r->call.eps);
         b.nprob = (int)n;
         b.ns = ns.data();
         b.nt = nt.data();
@@ -253,7 +264,8 @@ class Server {
         b.pottarg = o[3].data();
         b.gradtarg = o[4].data();
         b.hesstarg = o[5].data();
-        b.precision = c0.precision;
+        // (the class's arithmetic at the batch's eps)
+        b.precision = arith_class(c0) == kPrecMixed ? kPrecMixed : c0.precision;
         return run_laplace_batch(b);
     }
 

@@ -123,3 +123,31 @@ def test_batched_stream_matches_alone(fm, monkeypatch):
                 assert W.rel_err(keep[key], ref[key]) <= max(2 * eps, 1e-12), key
     assert srv.stats()["batched"] >= 2
     srv.close()
+
+
+@pytest.mark.gpu
+def test_batch_across_eps_of_one_arithmetic(fm, monkeypatch):
+    """Mixed-mode requests at eps 1e-3 and 1e-6 batch together and run at
+    1e-6; each result is within its own eps of its alone run."""
+    monkeypatch.delenv("FMM2D_B200_SERVE_BATCH", raising=False)
+    specs = [(800 + 97 * i, 1e-3 if i % 2 else 1e-6) for i in range(24)]
+    alone = []
+    for i, (n, eps) in enumerate(specs):
+        r, keep = _req(fm, "l", n, 900 + i, eps=eps)
+        srv1 = fm.Server(slots=1, hbm_budget=100e9)
+        t = srv1.submit(r, keep)
+        assert srv1.wait(t)[0] == 0
+        srv1.close()
+        alone.append((keep, eps))
+    srv = fm.Server(slots=1, hbm_budget=100e9)
+    tickets = []
+    for i, (n, eps) in enumerate(specs):
+        r, keep = _req(fm, "l", n, 900 + i, eps=eps)
+        tickets.append((srv.submit(r, keep), keep))
+    for (t, keep), (ref, eps) in zip(tickets, alone):
+        assert srv.wait(t)[0] == 0
+        for key in ref:
+            if key.startswith(("pot", "grad")):
+                assert W.rel_err(keep[key], ref[key]) <= 2 * eps, key
+    assert srv.stats()["batched"] >= 4
+    srv.close()
