@@ -101,7 +101,7 @@ struct WinArgs {
     int run0, nrun;
     const double *bs;  // box size per level
     int ndc, c0, p;
-    const float4 *H;   // [40][2 HALF] h_k(t), TF32 split: (re hi, re lo, im hi, im lo); h_0 = 0
+    const float *Bimg;  // [12 stages][3 shifts][hi | lo] the B operands in the operand layout
     const float *Bj;   // [HALF] b_j
     const double *Ai;  // [HALF] a_i = 1 / i!
     const float2 *Hf;  // [40][2 HALF] h_k(t) in FP32, with -log|t| at k = 0 (the rows
@@ -147,8 +147,7 @@ __global__ void __launch_bounds__(kWinThreads, 1) m2l_win_kernel(WinArgs A) {
     extern __shared__ __align__(1024) unsigned char win_smem[];
     float *sW = reinterpret_cast<float *>(win_smem);                 // [buf][hi, lo]
     float *sO = sW + 4 * WSZ;                                         // [buf][hi, lo]
-    float4 *sH = reinterpret_cast<float4 *>(sO + 4 * OSZ);            // [40][KH]
-    float2 *sHf = reinterpret_cast<float2 *>(sH + kWinOffsets * KH);  // [40][KH]
+    float2 *sHf = reinterpret_cast<float2 *>(sO + 4 * OSZ);           // [40][KH]
     double *sAi = reinterpret_cast<double *>(sHf + kWinOffsets * KH);  // [HALF]
     float *sBj = reinterpret_cast<float *>(sAi + HALF);               // [HALF]
     // barriers: 0-1 window full, 2-3 window free of MMAs, 4-5 window free
@@ -166,7 +165,7 @@ __global__ void __launch_bounds__(kWinThreads, 1) m2l_win_kernel(WinArgs A) {
             mbar_init(WBAR(0 + i), kWinWorkers);
             mbar_init(WBAR(2 + i), 1);
             mbar_init(WBAR(4 + i), 128);
-            mbar_init(WBAR(6 + i), kWinWorkers);
+            mbar_init(WBAR(6 + i), 1);  // (with the bulk copy's bytes)
             mbar_init(WBAR(8 + i), 1);
             mbar_init(WBAR(10 + i), 1);
             mbar_init(WBAR(12 + i), 128);
@@ -175,7 +174,6 @@ __global__ void __launch_bounds__(kWinThreads, 1) m2l_win_kernel(WinArgs A) {
         s_abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    for (int e = tid; e < kWinOffsets * KH; e += blockDim.x) sH[e] = A.H[e];
     for (int e = tid; e < kWinOffsets * KH; e += blockDim.x) sHf[e] = A.Hf[e];
     for (int e = tid; e < HALF; e += blockDim.x) {
         sAi[e] = A.Ai[e];
@@ -251,37 +249,6 @@ __global__ void __launch_bounds__(kWinThreads, 1) m2l_win_kernel(WinArgs A) {
                 }
             }
         };
-        // B operand of step (s, jj): the real form of the Hankel matrix
-        // h_{i+j}(t) of each child position's offset t, rows i >= 1 (zero
-        // outside list 2 and beyond the order)
-        auto gen_matrices = [&](int s, int jj, float *Ohi, float *Olo) {
-            constexpr int NTO = 4 * NQ * HALF;
-            for (int tau = wt; tau < NTO; tau += kWinWorkers) {
-                const int i = tau % HALF, jq = (tau / HALF) % NQ, c = tau / (HALF * NQ);
-                int dx, dy;
-                const bool in2 = win_slot(s, jj, c, dx, dy);
-                float4 h[4];
-#pragma unroll
-                for (int e = 0; e < 4; e++) h[e] = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (in2 && i >= 1 && i < P) {
-                    const float4 *hrow = sH + win_offset_index(dx, dy) * KH + i + 4 * jq;
-#pragma unroll
-                    for (int e = 0; e < 4; e++)
-                        if (4 * jq + e < P) h[e] = hrow[e];
-                }
-                const int nre = c * KP + i, nim = nre + HALF;
-                const int f1 = tc_fidx(nre, 4 * jq, NOP), f2 = tc_fidx(nre, HALF + 4 * jq, NOP);
-                const int f3 = tc_fidx(nim, 4 * jq, NOP), f4 = tc_fidx(nim, HALF + 4 * jq, NOP);
-                *reinterpret_cast<float4 *>(Ohi + f1) = make_float4(h[0].x, h[1].x, h[2].x, h[3].x);
-                *reinterpret_cast<float4 *>(Olo + f1) = make_float4(h[0].y, h[1].y, h[2].y, h[3].y);
-                *reinterpret_cast<float4 *>(Ohi + f2) = make_float4(-h[0].z, -h[1].z, -h[2].z, -h[3].z);
-                *reinterpret_cast<float4 *>(Olo + f2) = make_float4(-h[0].w, -h[1].w, -h[2].w, -h[3].w);
-                *reinterpret_cast<float4 *>(Ohi + f3) = make_float4(h[0].z, h[1].z, h[2].z, h[3].z);
-                *reinterpret_cast<float4 *>(Olo + f3) = make_float4(h[0].w, h[1].w, h[2].w, h[3].w);
-                *reinterpret_cast<float4 *>(Ohi + f4) = make_float4(h[0].x, h[1].x, h[2].x, h[3].x);
-                *reinterpret_cast<float4 *>(Olo + f4) = make_float4(h[0].y, h[1].y, h[2].y, h[3].y);
-            }
-        };
         int g = 0, u = 0;
         bool ok = true;
         if ((int)blockIdx.x < A.nrun) prefetch(A.run0 + blockIdx.x, 0);
@@ -301,26 +268,35 @@ __global__ void __launch_bounds__(kWinThreads, 1) m2l_win_kernel(WinArgs A) {
                 store_window(Whi, Wlo);
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 mbar_arrive(WBAR(0 + b));
-                for (int j = 0; j < 3; j++, u++) {
-                    const int ob = u & 1;
-                    if (u >= 2 && !mbar_wait_bounded(WBAR(8 + ob), (uint32_t)(((u >> 1) - 1) & 1),
-                                                     abort_flag, A.wait_ns)) {
-                        ok = false;
-                        break;
-                    }
-                    float *Ohi = sO + (2 * ob) * OSZ, *Olo = Ohi + OSZ;
-                    gen_matrices(s, j - 1, Ohi, Olo);
-                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                    mbar_arrive(WBAR(6 + ob));
-                    if (j == 0) {
-                        // the next stage's inputs, once the first matrices are out
-                        if (s < 11)
-                            prefetch(R, s + 1);
-                        else if (run + (int)gridDim.x < A.nrun)
-                            prefetch(R + gridDim.x, 0);
+                // the next stage's inputs
+                if (s < 11)
+                    prefetch(R, s + 1);
+                else if (run + (int)gridDim.x < A.nrun)
+                    prefetch(R + gridDim.x, 0);
+                // the stage's three B operands: bulk copies of the
+                // precomputed images, each into the matrix buffer the MMAs
+                // of two steps ago have released
+                if (wt == 0) {
+                    for (int j = 0; j < 3; j++, u++) {
+                        const int ob = u & 1;
+                        if (u >= 2 && !mbar_wait_bounded(WBAR(8 + ob), (uint32_t)(((u >> 1) - 1) & 1),
+                                                         abort_flag, A.wait_ns)) {
+                            ok = false;
+                            break;
+                        }
+                        mbar_arrive_expect_tx(WBAR(6 + ob), 2u * OSZ * 4u);
+                        bulk_g2s(smem_u32(sO + (2 * ob) * OSZ), A.Bimg + (size_t)(s * 3 + j) * 2 * OSZ,
+                                 2u * OSZ * 4u, WBAR(6 + ob));
                     }
                 }
             }
+        }
+        if (wt == 0) {
+            // the last bulk copies have landed before the block exits (the
+            // issuer has waited for them unless the block stopped early)
+            int never = 0;
+            for (int t = u - 2; t < u; t++)
+                if (t >= 0) mbar_wait_bounded(WBAR(6 + (t & 1)), (uint32_t)((t >> 1) & 1), &never, kWinWaitNs);
         }
         if (!ok) *abort_flag = 1;
     } else if (warp < kWinEpi0 + 4) {
@@ -524,16 +500,18 @@ __global__ void __launch_bounds__(kWinThreads, 1) m2l_win_kernel(WinArgs A) {
 template <int CH, int HALF>
 constexpr size_t win_smem_bytes() {
     return (size_t)(4 * kWinRows * 2 * HALF + 4 * 8 * HALF * 2 * HALF) * sizeof(float) +
-           (size_t)kWinOffsets * 2 * HALF * sizeof(float4) +
            (size_t)kWinOffsets * 2 * HALF * sizeof(float2) + (size_t)HALF * sizeof(double) +
            (size_t)HALF * sizeof(float);
 }
 
-// Tables of one (order, HALF): h_k(t) for the 40 offsets split into TF32
-// hi / lo, the same in FP32 with -log|t| at k = 0 (the leading rows over
-// the window values), b_j and a_i; cached per device.
+// Tables of one (order, HALF): the B operand of every (stage, shift) step
+// -- the real form of the Hankel matrices h_(i+j)(t) of the four child
+// positions' offsets, rows i >= 1 (zero outside list 2 and beyond the
+// order), TF32 hi then lo, in the operand layout --, h_k(t) in FP32 with
+// -log|t| at k = 0 (the leading rows over the window values), b_j and a_i;
+// cached per device.
 struct WinTables {
-    const float4 *H = nullptr;
+    const float *Bimg = nullptr;  // [12][3][hi | lo][4 * 2 HALF * 2 HALF]
     const float2 *Hf = nullptr;
     const float *Bj = nullptr;
     const double *Ai = nullptr;
@@ -599,21 +577,56 @@ WinTables win_tables(int p, int HALF, cudaStream_t s) {
         if (i >= 1) fi *= (double)i;
         Ai[i] = 1.0 / fi;
     }
+    // the B operands of the 36 steps (the layout the MMA reads: N = 4 KP
+    // rows -- child position c, then [Re outputs | Im outputs] --, K = KP)
+    const int KP = 2 * HALF, NOP = 4 * KP, NQ = HALF / 4, OSZ = NOP * KP;
+    std::vector<float> img((size_t)36 * 2 * OSZ, 0.f);
+    for (int st = 0; st < 12; st++)
+        for (int j = 0; j < 3; j++) {
+            float *Ohi = img.data() + (size_t)(st * 3 + j) * 2 * OSZ, *Olo = Ohi + OSZ;
+            for (int c = 0; c < 4; c++) {
+                int dx, dy;
+                const bool in2 = win_slot(st, j - 1, c, dx, dy);
+                for (int jq = 0; jq < NQ; jq++)
+                    for (int i = 0; i < HALF; i++) {
+                        float4 h[4];
+                        for (int e = 0; e < 4; e++) h[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+                        if (in2 && i >= 1 && i <= p) {
+                            const float4 *hrow = H.data() + (size_t)win_offset_index(dx, dy) * KH + i + 4 * jq;
+                            for (int e = 0; e < 4; e++)
+                                if (4 * jq + e <= p) h[e] = hrow[e];
+                        }
+                        const int nre = c * KP + i, nim = nre + HALF;
+                        const int f1 = tc_fidx(nre, 4 * jq, NOP), f2 = tc_fidx(nre, HALF + 4 * jq, NOP);
+                        const int f3 = tc_fidx(nim, 4 * jq, NOP), f4 = tc_fidx(nim, HALF + 4 * jq, NOP);
+                        for (int e = 0; e < 4; e++) {
+                            Ohi[f1 + e] = h[e].x;   // Re h
+                            Olo[f1 + e] = h[e].y;
+                            Ohi[f2 + e] = -h[e].z;  // -Im h
+                            Olo[f2 + e] = -h[e].w;
+                            Ohi[f3 + e] = h[e].z;   // Im h
+                            Olo[f3 + e] = h[e].w;
+                            Ohi[f4 + e] = h[e].x;   // Re h
+                            Olo[f4 + e] = h[e].y;
+                        }
+                    }
+            }
+        }
     WinTables t;
-    float4 *dH = nullptr;
+    float *dH = nullptr;
     float2 *dR = nullptr;
     float *dB = nullptr;
     double *dA = nullptr;
-    FMM_CUDA(cudaMalloc(&dH, H.size() * sizeof(float4)));
+    FMM_CUDA(cudaMalloc(&dH, img.size() * sizeof(float)));
     FMM_CUDA(cudaMalloc(&dR, Hf.size() * sizeof(float2)));
     FMM_CUDA(cudaMalloc(&dB, Bj.size() * sizeof(float)));
     FMM_CUDA(cudaMalloc(&dA, Ai.size() * sizeof(double)));
-    FMM_CUDA(cudaMemcpyAsync(dH, H.data(), H.size() * sizeof(float4), cudaMemcpyHostToDevice, s));
+    FMM_CUDA(cudaMemcpyAsync(dH, img.data(), img.size() * sizeof(float), cudaMemcpyHostToDevice, s));
     FMM_CUDA(cudaMemcpyAsync(dR, Hf.data(), Hf.size() * sizeof(float2), cudaMemcpyHostToDevice, s));
     FMM_CUDA(cudaMemcpyAsync(dB, Bj.data(), Bj.size() * sizeof(float), cudaMemcpyHostToDevice, s));
     FMM_CUDA(cudaMemcpyAsync(dA, Ai.data(), Ai.size() * sizeof(double), cudaMemcpyHostToDevice, s));
     FMM_CUDA(cudaStreamSynchronize(s));
-    t.H = dH;
+    t.Bimg = dH;
     t.Hf = dR;
     t.Bj = dB;
     t.Ai = dA;
@@ -815,7 +828,7 @@ void launch_win(const WinPlan &W, const WinTables &tb, const Tree &T, const Cauc
         a.ndc = P.ndc;
         a.c0 = c0;
         a.p = P.p;
-        a.H = tb.H;
+        a.Bimg = tb.Bimg;
         a.Bj = tb.Bj;
         a.Ai = tb.Ai;
         a.Hf = tb.Hf;
