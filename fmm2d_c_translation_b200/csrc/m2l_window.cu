@@ -113,6 +113,17 @@ struct WinArgs {
     unsigned long long wait_ns;  // limit of every bounded wait of the roles
 };
 
+// Packed FP32 FMA (two lanes per instruction): d = a * b + c per lane,
+// round to nearest like fmaf.
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+    const uint64_t ua = (uint64_t)__float_as_uint(a.x) | ((uint64_t)__float_as_uint(a.y) << 32);
+    const uint64_t ub = (uint64_t)__float_as_uint(b.x) | ((uint64_t)__float_as_uint(b.y) << 32);
+    const uint64_t uc = (uint64_t)__float_as_uint(c.x) | ((uint64_t)__float_as_uint(c.y) << 32);
+    uint64_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(ua), "l"(ub), "l"(uc));
+    return make_float2(__uint_as_float((uint32_t)d), __uint_as_float((uint32_t)(d >> 32)));
+}
+
 // Window values: hi = tf32(v) and lo = v - hi, the exact FP32 residual, so
 // that hi + lo gives back v for the rows summed on the CUDA cores (the MMA
 // reads lo at TF32 precision).
@@ -147,7 +158,8 @@ __global__ void __launch_bounds__(kWinThreads, 1) m2l_win_kernel(WinArgs A) {
     extern __shared__ __align__(1024) unsigned char win_smem[];
     float *sW = reinterpret_cast<float *>(win_smem);                 // [buf][hi, lo]
     float *sO = sW + 4 * WSZ;                                         // [buf][hi, lo]
-    float2 *sHf = reinterpret_cast<float2 *>(sO + 4 * OSZ);           // [40][KH]
+    // h_k(t) expanded for the packed FP32 pipe: (Re, Re, -Im, Im)
+    float4 *sHf = reinterpret_cast<float4 *>(sO + 4 * OSZ);           // [40][KH]
     double *sAi = reinterpret_cast<double *>(sHf + kWinOffsets * KH);  // [HALF]
     float *sBj = reinterpret_cast<float *>(sAi + HALF);               // [HALF]
     // barriers: 0-1 window full, 2-3 window free of MMAs, 4-5 window free
@@ -174,7 +186,10 @@ __global__ void __launch_bounds__(kWinThreads, 1) m2l_win_kernel(WinArgs A) {
         s_abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    for (int e = tid; e < kWinOffsets * KH; e += blockDim.x) sHf[e] = A.Hf[e];
+    for (int e = tid; e < kWinOffsets * KH; e += blockDim.x) {
+        const float2 t = A.Hf[e];
+        sHf[e] = make_float4(t.x, t.x, -t.y, t.y);
+    }
     for (int e = tid; e < HALF; e += blockDim.x) {
         sAi[e] = A.Ai[e];
         sBj[e] = A.Bj[e];
@@ -358,17 +373,28 @@ __global__ void __launch_bounds__(kWinThreads, 1) m2l_win_kernel(WinArgs A) {
                     for (int c = 0; c < 4; c++) {
                         if (!v[c]) continue;
                         // (window values beyond the order are zero)
-                        const float2 *hf = sHf + win_offset_index(dxs[c], dys[c]) * KH;
+                        // acc_i += h_(i+jp) W_jp for the NR rows at once: the
+                        // table entries h_jp .. h_(jp+NR-1) rotate through
+                        // registers, one load per jp; each complex update is
+                        // two packed FMAs, (Re, Im) += (-Im h, Im h) (Im W,
+                        // Re W) then += (Re h, Re h) (Re W, Im W) -- the same
+                        // operations in the same order as scalar FMAs
+                        const float4 *hf = sHf + win_offset_index(dxs[c], dys[c]) * KH;
+                        float4 w[NR];
 #pragma unroll
-                        for (int i = 0; i < NR; i++) {
-                            float ax = lr_[c][i].x, ay = lr_[c][i].y;
+                        for (int q = 0; q + 1 < NR; q++) w[q] = hf[q];
 #pragma unroll
-                            for (int jp = 0; jp < HALF; jp++) {
-                                const float2 t = hf[i + jp];
-                                ax = fmaf(t.x, mr[jp], fmaf(-t.y, mi[jp], ax));
-                                ay = fmaf(t.x, mi[jp], fmaf(t.y, mr[jp], ay));
+                        for (int jp = 0; jp < HALF; jp++) {
+                            w[NR - 1] = hf[jp + NR - 1];
+                            const float2 MI = make_float2(mi[jp], mr[jp]);
+                            const float2 MR = make_float2(mr[jp], mi[jp]);
+#pragma unroll
+                            for (int i = 0; i < NR; i++) {
+                                lr_[c][i] = fma2(make_float2(w[i].z, w[i].w), MI, lr_[c][i]);
+                                lr_[c][i] = fma2(make_float2(w[i].x, w[i].y), MR, lr_[c][i]);
                             }
-                            lr_[c][i] = make_float2(ax, ay);
+#pragma unroll
+                            for (int q = 0; q + 1 < NR; q++) w[q] = w[q + 1];
                         }
                         s0[c].x -= mr[0];  // M_0 = -W_0
                         s0[c].y -= mi[0];
@@ -500,7 +526,7 @@ __global__ void __launch_bounds__(kWinThreads, 1) m2l_win_kernel(WinArgs A) {
 template <int CH, int HALF>
 constexpr size_t win_smem_bytes() {
     return (size_t)(4 * kWinRows * 2 * HALF + 4 * 8 * HALF * 2 * HALF) * sizeof(float) +
-           (size_t)kWinOffsets * 2 * HALF * sizeof(float2) + (size_t)HALF * sizeof(double) +
+           (size_t)kWinOffsets * 2 * HALF * sizeof(float4) + (size_t)HALF * sizeof(double) +
            (size_t)HALF * sizeof(float);
 }
 
