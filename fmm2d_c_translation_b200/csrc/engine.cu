@@ -386,6 +386,14 @@ void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaS
                       double *upot, double *ugrad, double *uhess) {
         if (pgh <= 0 || n <= 0) return;
         const int gcomp = lap ? 2 : 1, hcomp = lap ? 3 : 1;
+        // Walked in input order through the inverse permutation: each point
+        // reads its outputs in tree order (whole 32-byte sectors) and the
+        // writes in the caller's layout are coalesced, instead of writing
+        // half sectors at random (measured on a B200: the scatters of
+        // 10^7 + 10^7 points with pot and grad took 1.13 ms against 1.55).
+        DevBuf<int> invb(n, s);
+        int *inv = invb.get();
+        for_each(n, s, [=] __device__(int64_t k) { inv[perm[k]] = (int)k; });
         if (real) {
             // rfmm2d.f:159-214: pot = Re pot1, grad = (Re g1, -Im g1),
             // hess = (Re h1, -Im h1, -Re h1), all real
@@ -399,8 +407,8 @@ void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaS
             if (pgh >= 3) oh.set(uhess, (size_t)nd * 3 * n, on_dev, s);
             const double2 *P0 = po.get(), *G0 = gr.get(), *H0 = he.get();
             double *up = op.ptr, *ug = og.ptr, *uh = oh.ptr;
-            for_each(n, s, [=] __device__(int64_t k) {
-                const int i = perm[k];
+            for_each(n, s, [=] __device__(int64_t i) {
+                const int k = inv[i];
                 for (int j = 0; j < nd; j++) {
                     const size_t a = (size_t)k * ndc + j;
                     up[(size_t)i * nd + j] = P0[a].x;
@@ -429,8 +437,8 @@ void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaS
         if (pgh >= 3) oh.set(uhess, (size_t)nd * hcomp * n, on_dev, s);
         const double2 *P0 = po.get(), *G0 = gr.get(), *H0 = he.get();
         double2 *up = op.ptr, *ug = og.ptr, *uh = oh.ptr;
-        for_each(n, s, [=] __device__(int64_t k) {
-            const int i = perm[k];
+        for_each(n, s, [=] __device__(int64_t i) {
+            const int k = inv[i];
             for (int j = 0; j < nd; j++) {
                 if (lap) {
                     // lfmm2d.f:168-225: pot = Re pot1(1) + i Re pot1(2),
