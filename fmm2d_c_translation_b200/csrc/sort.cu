@@ -8,10 +8,10 @@
 //
 // One pass per 8-bit digit: a per-tile histogram, a scan of the digit-major
 // histogram table, and a scatter in which every tile first ranks its items
-// stably into shared memory (each warp ranks a contiguous chunk with warp
-// match and a per-warp digit count, one block-wide step adds the counts of
-// the warps before) and then writes them out in digit order, so that
-// consecutive threads write consecutive addresses of the same digit run.
+// stably into shared memory (warp match for ties inside a warp, per-warp
+// counts across warps, a running per-digit count across rounds) and then
+// writes them out in digit order, so that consecutive threads write
+// consecutive addresses of the same digit run.
 #include "common.cuh"
 #include "sort.cuh"
 
@@ -40,14 +40,6 @@ __global__ void __launch_bounds__(kThreads) radix_hist_kernel(
     hist[threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
 }
 
-// Each warp ranks a contiguous chunk of kRounds * 32 items of the tile
-// (round r, lane l: item warp * kRounds * 32 + r * 32 + l), so the stable
-// order within the tile is (warp, round, lane): a warp counts its digits in
-// registers of the digit's leader lane as it goes (match_any ties within a
-// round, a per-warp digit count carried across rounds in shared memory that
-// only the warp touches), then one block-wide step turns the per-warp counts
-// into offsets and every item goes to its place in shared memory; the tile
-// is written out in digit order as before.
 __global__ void __launch_bounds__(kThreads) radix_scatter_kernel(
     const uint32_t *__restrict__ kin, const uint32_t *__restrict__ vin,
     uint32_t *__restrict__ kout, uint32_t *__restrict__ vout, int64_t n, int shift,
@@ -56,7 +48,8 @@ __global__ void __launch_bounds__(kThreads) radix_scatter_kernel(
     __shared__ uint32_t sv[kTile];
     __shared__ int lstart[kRadix];  // tile-local start of each digit
     __shared__ int gdelta[kRadix];  // global position - local position
-    __shared__ int wc[kWarps][kRadix];  // per-warp digit counts, then offsets
+    __shared__ int run[kRadix];
+    __shared__ int wc[kWarps][kRadix];
     __shared__ int wsum[kWarps];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     // exclusive scan of this tile's digit counts
@@ -68,62 +61,49 @@ __global__ void __launch_bounds__(kThreads) radix_scatter_kernel(
         if (lane >= d) incl += y;
     }
     if (lane == 31) wsum[warp] = incl;
-#pragma unroll
-    for (int w = 0; w < kWarps; w++) wc[w][tid] = 0;
     __syncthreads();
     int wpre = 0;
     for (int w = 0; w < warp; w++) wpre += wsum[w];
     const int excl = wpre + incl - h;
     lstart[tid] = excl;
     gdelta[tid] = offs[tid * nblocks + blockIdx.x] - excl;
+    run[tid] = 0;
     const unsigned lt_mask = (1u << lane) - 1u;
-    const int64_t wbase = (int64_t)blockIdx.x * kTile + (int64_t)warp * kRounds * 32;
-    // the warp's items, loaded up front (coalesced, all in flight at once)
+    const int64_t base = (int64_t)blockIdx.x * kTile;
+    // the tile's items, loaded up front (coalesced, all in flight at once)
     uint32_t kr[kRounds], vr[kRounds];
 #pragma unroll
     for (int r = 0; r < kRounds; r++) {
-        const int64_t idx = wbase + (int64_t)r * 32 + lane;
+        const int64_t idx = base + (int64_t)r * kThreads + tid;
         kr[r] = idx < n ? kin[idx] : 0u;
         vr[r] = idx < n ? vin[idx] : 0u;
     }
-    // rank of every item among the warp's items of the same digit
-    int rk[kRounds];
-    int *mine = wc[warp];
 #pragma unroll
     for (int r = 0; r < kRounds; r++) {
-        const int64_t idx = wbase + (int64_t)r * 32 + lane;
-        const int d = idx < n ? (int)((kr[r] >> shift) & 0xff) : -1;
+#pragma unroll
+        for (int w = 0; w < kWarps; w++) wc[w][tid] = 0;
+        __syncthreads();
+        const int64_t idx = base + (int64_t)r * kThreads + tid;
+        const bool valid = idx < n;
+        const uint32_t key = kr[r], val = vr[r];
+        const int d = valid ? (int)((key >> shift) & 0xff) : -1;
         const unsigned peers = __match_any_sync(0xffffffffu, d);
-        const int before = d >= 0 ? mine[d] : 0;  // (read by every peer before the leader adds)
-        rk[r] = before + __popc(peers & lt_mask);
-        __syncwarp();
-        if (d >= 0 && (peers & lt_mask) == 0) mine[d] = before + __popc(peers);
-        __syncwarp();
-    }
-    __syncthreads();
-    // per digit: the counts of the warps before, as offsets
-    {
-        int run = 0;
-#pragma unroll
-        for (int w = 0; w < kWarps; w++) {
-            const int c = wc[w][tid];
-            wc[w][tid] = run;
-            run += c;
+        const int rank = __popc(peers & lt_mask);
+        if (valid && rank == 0) wc[warp][d] = __popc(peers);
+        __syncthreads();
+        if (valid) {
+            int pos = lstart[d] + run[d] + rank;
+            for (int w = 0; w < warp; w++) pos += wc[w][d];
+            sk[pos] = key;
+            sv[pos] = val;
         }
-    }
-    __syncthreads();
+        __syncthreads();
+        int add = 0;
 #pragma unroll
-    for (int r = 0; r < kRounds; r++) {
-        const int64_t idx = wbase + (int64_t)r * 32 + lane;
-        if (idx < n) {
-            const int d = (int)((kr[r] >> shift) & 0xff);
-            const int pos = lstart[d] + wc[warp][d] + rk[r];
-            sk[pos] = kr[r];
-            sv[pos] = vr[r];
-        }
+        for (int w = 0; w < kWarps; w++) add += wc[w][tid];
+        run[tid] += add;
     }
     __syncthreads();
-    const int64_t base = (int64_t)blockIdx.x * kTile;
     const int cnt = n - base < kTile ? (int)(n - base) : kTile;
     for (int i = tid; i < cnt; i += kThreads) {
         const uint32_t key = sk[i];
