@@ -76,10 +76,10 @@ def make_inputs(ns, nt, seed):
 # on the bench command with --ns 2000000 --nt 2000000 (the summary with the
 # full command is kept in profiles/)
 TRAFFIC_2E6 = {
-    ("mixed", "m2l"): (247.4e6, "profiles/kernels_mixed_2e6_dram.md: m2l_win_kernel<2,20,4> "
-                                "101.5 MB read + 145.9 MB write at 2e6+2e6, scaled by points"),
-    ("mixed", "p2p"): (656.5e6, "profiles/kernels_mixed_2e6_dram.md: p2p_flat_kernel "
-                                "447.1 MB read + 209.4 MB write at 2e6+2e6, scaled by points"),
+    ("mixed", "m2l"): (249.3e6, "profiles/kernels_mixed_2e6_dram.md: m2l_win_kernel<2,20,4> "
+                                "103.9 MB read + 145.4 MB write at 2e6+2e6, scaled by points"),
+    ("mixed", "p2p"): (661.8e6, "profiles/kernels_mixed_2e6_dram.md: p2p_flat_kernel "
+                                "447.6 MB read + 214.2 MB write at 2e6+2e6, scaled by points"),
 }
 
 
