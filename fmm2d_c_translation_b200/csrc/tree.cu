@@ -534,14 +534,34 @@ struct Builder {
         // remaining step (subdivision, reorganisation, colleagues, the
         // flag++ pass) would leave it as it is.
         if (count_flags(1, 2) == 0) return;
-        // Subdivide flag and flag+ boxes of the original levels.
+        // Subdivide flag and flag+ boxes of the original levels.  Their
+        // flags are final, so the boxes to split on every level are counted
+        // at once (one synchronisation instead of one per level).
         std::vector<int> ts(L + 1, 0), te(L + 1, 0);
+        std::vector<int> nsplit(L + 1, 0);
+        if (L >= 3) {
+            DevBuf<int> cnt(L + 1, s);
+            cnt.zero(s);
+            int *cp = cnt.get();
+            const int *fl = iflag.get();
+            const int lo = T.lstart[1], n = T.lend[L - 2] - lo;
+            for_each(n, s, [=] __device__(int64_t i) {
+                const int b = lo + (int)i;
+                const int key = fl[b] > 0 ? lev[b] : -1;
+                const unsigned am = __activemask();
+                const unsigned peers = __match_any_sync(am, key);
+                if (key >= 0 && (int)(threadIdx.x & 31) == __ffs(peers) - 1)
+                    atomicAdd(&cp[key], __popc(peers));
+            });
+            read_small(nsplit.data(), cp, (L + 1) * sizeof(int), s);
+        }
         for (int l = 1; l <= L - 2; l++) {
             ts[l + 1] = T.nboxes;
             int *fl = iflag.get();
-            refine_range(
-                T.lstart[l], T.lend[l], l + 1, T.boxsize[l + 1],
-                [=] __device__(int b) { return fl[b] > 0; }, true);
+            if (nsplit[l] > 0)
+                refine_range(
+                    T.lstart[l], T.lend[l], l + 1, T.boxsize[l + 1],
+                    [=] __device__(int b) { return fl[b] > 0; }, true, nsplit[l]);
             te[l + 1] = T.nboxes;
         }
         reorg(ts, te);
@@ -585,14 +605,32 @@ struct Builder {
                 fl[b] = f;
             });
             ts[l + 1] = T.nboxes;
-            refine_range(
-                T.lstart[l], T.lend[l], l + 1, T.boxsize[l + 1],
-                [=] __device__(int b) { return fl[b] > 0; }, true);
+            // the boxes to split in the level and in its tail, counted
+            // together (their flags are final; the splits only append)
+            int hc[2] = {0, 0};
             {
+                DevBuf<int> c2(2, s);
+                c2.zero(s);
+                int *cp = c2.get();
+                for_each(n1 + n2, s, [=] __device__(int64_t i) {
+                    const int b = i < n1 ? lo + (int)i : tlo + (int)(i - n1);
+                    const int key = fl[b] > 0 ? (i < n1 ? 0 : 1) : -1;
+                    const unsigned am = __activemask();
+                    const unsigned peers = __match_any_sync(am, key);
+                    if (key >= 0 && (int)(threadIdx.x & 31) == __ffs(peers) - 1)
+                        atomicAdd(&cp[key], __popc(peers));
+                });
+                read_small(hc, cp, sizeof(hc), s);
+            }
+            if (hc[0] > 0)
+                refine_range(
+                    T.lstart[l], T.lend[l], l + 1, T.boxsize[l + 1],
+                    [=] __device__(int b) { return fl[b] > 0; }, true, hc[0]);
+            if (hc[1] > 0) {
                 int *fl2 = iflag.get();
                 refine_range(
                     tlo, tlo + n2, l + 1, T.boxsize[l + 1],
-                    [=] __device__(int b) { return fl2[b] > 0; }, true);
+                    [=] __device__(int b) { return fl2[b] > 0; }, true, hc[1]);
             }
             te[l + 1] = T.nboxes;
             // colleagues of the new boxes from their dad's (current) list
