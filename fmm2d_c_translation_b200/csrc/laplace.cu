@@ -1330,18 +1330,24 @@ __device__ __forceinline__ double2 child_offset(int cs) {
     return make_double2((cs & 1) ? 0.25 : -0.25, (cs & 2) ? 0.25 : -0.25);
 }
 
+// The boxes visited come from a BoxList (the level's boxes with evaluation
+// points, whose parents then have points too), or, with ids null, are all
+// boxes of [lo, hi) whose parent has points.
 template <int PMAX>
 __global__ void __launch_bounds__(128) l2l_pascal_kernel(
-    int lo, int hi, int p, EvalCounts ec, const int *__restrict__ parent,
+    int lo, int hi, int p, EvalCounts ec, const int *__restrict__ ids,
+    const int *__restrict__ off, const int *__restrict__ parent,
     const int *__restrict__ child, int ndc, int c0, int nch, double2 *__restrict__ loc,
     float2 *__restrict__ loc32) {
     const int stride = (p + 1) * ndc;
-    const int64_t total = (int64_t)(hi - lo) * nch;
+    const int k0 = ids ? off[lo] : 0;
+    const int64_t total = (int64_t)(ids ? off[hi] - k0 : hi - lo) * nch;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
          t += (int64_t)gridDim.x * blockDim.x) {
-        const int b = lo + (int)(t / nch), q = c0 + (int)(t % nch);
+        const int k = (int)(t / nch), q = c0 + (int)(t % nch);
+        const int b = ids ? ids[k0 + k] : lo + k;
         const int pb = parent[b];
-        if (ec.npts(pb) <= 0) continue;
+        if (!ids && ec.npts(pb) <= 0) continue;
         const double2 d = child_offset(child_pos(child, pb, b));
         const double2 *Lp = loc + (size_t)pb * stride + q;
         double2 e[PMAX];
@@ -1372,19 +1378,23 @@ __global__ void __launch_bounds__(128) l2l_pascal_kernel(
     }
 }
 
+// The parents visited come from a BoxList (the level's parents with
+// sources), or, with ids null, are all boxes of [lo, hi) with children.
 template <int PMAX>
 __global__ void __launch_bounds__(128) m2m_pascal_kernel(
-    int lo, int hi, int p, const int *__restrict__ nchild, const int *__restrict__ child,
+    int lo, int hi, int p, const int *__restrict__ ids, const int *__restrict__ off,
+    const int *__restrict__ nchild, const int *__restrict__ child,
     const int2 *__restrict__ sse, int ndc, int c0, int nch, double2 *__restrict__ mp) {
     const int stride = (p + 1) * ndc;
-    const int64_t total = (int64_t)(hi - lo) * nch * 4;
+    const int k0 = ids ? off[lo] : 0;
+    const int64_t total = (int64_t)(ids ? off[hi] - k0 : hi - lo) * nch * 4;
     // warp-uniform trip count: the lanes of a parent meet in the shuffles
     for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < total;
          base += (int64_t)gridDim.x * blockDim.x) {
         const int64_t t = base + threadIdx.x;
         const bool valid = t < total;
         const int64_t tt = valid ? t : 0;
-        const int b = lo + (int)(tt / (4 * nch));
+        const int b = ids ? ids[k0 + (int)(tt / (4 * nch))] : lo + (int)(tt / (4 * nch));
         const int q = c0 + (int)((tt / 4) % nch), cs = (int)(tt % 4);
         const bool par = valid && nchild[b] > 0;
         const double2 d = child_offset(cs);
@@ -1428,6 +1438,21 @@ __global__ void __launch_bounds__(128) m2m_pascal_kernel(
             if (par && cs == 0) mp[(size_t)b * stride + (size_t)i * ndc + q] = v;
         }
     }
+}
+
+// Boxes b of [0, nb) with pred(b), in box order: ids[off[b]] = b, off[nb]
+// the count (off is the exclusive scan of the predicate).
+template <class Pred>
+void box_list(int nb, Pred pred, DevBuf<int> &ids, DevBuf<int> &off, cudaStream_t s) {
+    DevBuf<int> f(std::max(nb, 1), s);
+    ids.alloc(std::max(nb, 1), s);
+    off.alloc(nb + 1, s);
+    int *fp = f.get(), *ip = ids.get(), *op = off.get();
+    for_each(nb, s, [=] __device__(int64_t i) { fp[i] = pred((int)i) ? 1 : 0; });
+    exclusive_scan_i32(fp, op, nb, op + nb, s);
+    for_each(nb, s, [=] __device__(int64_t i) {
+        if (fp[i]) ip[op[i]] = (int)i;
+    });
 }
 
 inline int pascal_grid(int64_t nthreads) {
@@ -1732,10 +1757,16 @@ void upward_chunk(const Tree &T, const CauchyProblem &P, int c0,
         const int64_t nt = (int64_t)(hi - lo) * CH * 4;
         if (p + 1 <= 20)
             m2m_pascal_kernel<20><<<pascal_grid(nt), 128, 0, s>>>(
-                lo, hi, p, T.nchild.get(), T.child.get(), T.srcse.get(), P.ndc, c0, CH, mp);
+                lo, hi, p, P.m2m_ids, P.m2m_off, T.nchild.get(), T.child.get(), T.srcse.get(),
+                P.ndc, c0, CH, mp);
+        else if (p + 1 <= 32)
+            m2m_pascal_kernel<32><<<pascal_grid(nt), 128, 0, s>>>(
+                lo, hi, p, P.m2m_ids, P.m2m_off, T.nchild.get(), T.child.get(), T.srcse.get(),
+                P.ndc, c0, CH, mp);
         else if (p + 1 <= 40)
             m2m_pascal_kernel<40><<<pascal_grid(nt), 128, 0, s>>>(
-                lo, hi, p, T.nchild.get(), T.child.get(), T.srcse.get(), P.ndc, c0, CH, mp);
+                lo, hi, p, P.m2m_ids, P.m2m_off, T.nchild.get(), T.child.get(), T.srcse.get(),
+                P.ndc, c0, CH, mp);
         else
             m2m_coef_kernel<CH><<<blocks(hi - lo), 256, 0, s>>>(
                 lo, hi, p, T.nchild.get(), T.child.get(), T.srcse.get(), A, P.ndc,
@@ -1805,10 +1836,16 @@ void downward_chunk(const Tree &T, const CauchyProblem &P, int c0,
         const int64_t nt = (int64_t)(hi - lo) * CH;
         if (p + 1 <= 20)
             l2l_pascal_kernel<20><<<pascal_grid(nt), 128, 0, s>>>(
-                lo, hi, p, ec, T.parent.get(), T.child.get(), P.ndc, c0, CH, loc, loc32);
+                lo, hi, p, ec, P.l2l_ids, P.l2l_off, T.parent.get(), T.child.get(), P.ndc, c0,
+                CH, loc, loc32);
+        else if (p + 1 <= 32)
+            l2l_pascal_kernel<32><<<pascal_grid(nt), 128, 0, s>>>(
+                lo, hi, p, ec, P.l2l_ids, P.l2l_off, T.parent.get(), T.child.get(), P.ndc, c0,
+                CH, loc, loc32);
         else if (p + 1 <= 40)
             l2l_pascal_kernel<40><<<pascal_grid(nt), 128, 0, s>>>(
-                lo, hi, p, ec, T.parent.get(), T.child.get(), P.ndc, c0, CH, loc, loc32);
+                lo, hi, p, ec, P.l2l_ids, P.l2l_off, T.parent.get(), T.child.get(), P.ndc, c0,
+                CH, loc, loc32);
         else
             l2l_coef_kernel<CH><<<blocks(hi - lo), 256, 0, s>>>(
                 lo, hi, p, ec, T.parent.get(), T.child.get(), A, P.ndc, c0, loc);
@@ -2004,6 +2041,21 @@ void cauchy_fmm(const Tree &T, const CauchyProblem &P0, cudaStream_t s) {
     const int nlow = T.nlevels >= 1 ? T.lend[1] : T.lend[0];
     FMM_CUDA(cudaMemsetAsync(loc.get(), 0,
                              (size_t)nlow * (P.p + 1) * P.ndc * sizeof(double2), s));
+    // the boxes the Pascal M2M and L2L visit (in adaptive trees most boxes
+    // of the deep levels are leaves or empty)
+    DevBuf<int> m2m_ids, m2m_off, l2l_ids, l2l_off;
+    if (T.nlevels >= 2 && P.p + 1 <= 40) {
+        const int *nchp = T.nchild.get();
+        const int2 *sse = T.srcse.get();
+        const EvalCounts ec{T.srcse.get(), T.trgse.get(), P.sset.pgh, P.tset.pgh};
+        box_list(T.nboxes, [=] __device__(int b) { return nchp[b] > 0 && count(sse, b) > 0; },
+                 m2m_ids, m2m_off, s);
+        box_list(T.nboxes, [=] __device__(int b) { return ec.npts(b) > 0; }, l2l_ids, l2l_off, s);
+        P.m2m_ids = m2m_ids.get();
+        P.m2m_off = m2m_off.get();
+        P.l2l_ids = l2l_ids.get();
+        P.l2l_off = l2l_off.get();
+    }
     prof_mark("fmm_setup", s);
     auto per_chunk = [&](auto f2, auto f1) {
         for (int c0 = 0; c0 < P.ndc; c0 += 2) {

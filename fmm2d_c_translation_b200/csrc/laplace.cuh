@@ -81,6 +81,11 @@ struct CauchyProblem {
     const float4 *trg_hl = nullptr;
     double *timeinfo = nullptr;       // 8 phase times (s), optional
     M2LCache *m2l_cache = nullptr;    // planning kept across evaluations (plans)
+    // boxes visited by the Pascal M2M (parents with sources) and L2L (boxes
+    // with evaluation points), in box order: level l's entries are
+    // ids[off[lstart[l]] .. off[lend[l]]) (set by cauchy_fmm)
+    const int *m2m_ids = nullptr, *m2m_off = nullptr;
+    const int *l2l_ids = nullptr, *l2l_off = nullptr;
 };
 
 // Runs steps 1-8 of cfmm2dmain (src/laplace/cfmm2d.f:442-1340) on the
