@@ -18,10 +18,11 @@ constexpr int kScanItems = 4;
 constexpr int kScanTile = kScanThreads * kScanItems;  // 1024 values per block
 
 // Block-local exclusive scan of one 1024-value tile; writes the tile total
-// to block_sums[blockIdx.x].
+// to block_sums[blockIdx.x], and, for a scan of one tile, to *total (when
+// not null).
 __global__ void scan_tile_kernel(const int *__restrict__ in,
                                  int *__restrict__ out, int64_t n,
-                                 int *__restrict__ block_sums) {
+                                 int *__restrict__ block_sums, int *__restrict__ total) {
     __shared__ int warp_tot[kScanThreads / 32];
     const int64_t base = (int64_t)blockIdx.x * kScanTile + threadIdx.x * kScanItems;
     int v[kScanItems];
@@ -50,7 +51,10 @@ __global__ void scan_tile_kernel(const int *__restrict__ in,
             if (lane >= d) wi += y;
         }
         if (lane < kScanThreads / 32) warp_tot[lane] = wi - w;  // exclusive
-        if (lane == kScanThreads / 32 - 1) block_sums[blockIdx.x] = wi;
+        if (lane == kScanThreads / 32 - 1) {
+            block_sums[blockIdx.x] = wi;
+            if (total && gridDim.x == 1) *total = wi;
+        }
     }
     __syncthreads();
     int run = warp_tot[warp] + incl - tsum;
@@ -72,26 +76,16 @@ __global__ void scan_add_kernel(int *__restrict__ out, int64_t n,
     }
 }
 
-__global__ void scan_total_kernel(const int *block_incl_last, int *total) {
-    *total = *block_incl_last;
-}
-
 // Exclusive scan; also leaves the inclusive grand total in *d_total_out
 // when requested.
 void scan_rec(const int *in, int *out, int64_t n, int *d_total,
               cudaStream_t s) {
     const int64_t nb = (n + kScanTile - 1) / kScanTile;
     DevBuf<int> sums(nb + 1, s);
-    scan_tile_kernel<<<(unsigned)nb, kScanThreads, 0, s>>>(in, out, n,
-                                                           sums.get());
+    scan_tile_kernel<<<(unsigned)nb, kScanThreads, 0, s>>>(in, out, n, sums.get(),
+                                                           nb == 1 ? d_total : nullptr);
     FMM_CHECK_LAUNCH();
-    if (nb == 1) {
-        if (d_total) {
-            scan_total_kernel<<<1, 1, 0, s>>>(sums.get(), d_total);
-            FMM_CHECK_LAUNCH();
-        }
-        return;
-    }
+    if (nb == 1) return;
     DevBuf<int> offs(nb, s);
     scan_rec(sums.get(), offs.get(), nb, d_total, s);
     scan_add_kernel<<<(unsigned)nb, kScanThreads, 0, s>>>(out, n, offs.get());

@@ -217,12 +217,16 @@ struct Builder {
     void set_child_ranges(int nb0, int nb1) {
         if (!ranges || nb1 <= nb0) return;
         const int *par = T.parent.get(), *lev = T.level.get();
-        int2 *R[2] = {rs.get(), rt.get()};
-        const KeyView K[2] = {kvs, kvt};
-        for (int set = 0; set < 2; set++) {
-            int2 *r = R[set];
-            const KeyView kv = K[set];
-            for_each(nb1 - nb0, s, [=] __device__(int64_t i) {
+        int2 *rs0 = rs.get(), *rt0 = rt.get();
+        const KeyView ks0 = kvs, kt0 = kvt;
+        const int64_t nn = nb1 - nb0;
+        // both point sets in one launch: items [0, nn) sources, [nn, 2 nn) targets
+        {
+            for_each(2 * nn, s, [=] __device__(int64_t ii) {
+                const bool tset = ii >= nn;
+                const int64_t i = tset ? ii - nn : ii;
+                int2 *r = tset ? rt0 : rs0;
+                const KeyView kv = tset ? kt0 : ks0;
                 const int kb = nb0 + (int)i, j = (int)(i & 3);
                 const int m = lev[kb];
                 const int2 pr = r[par[kb]];
@@ -312,6 +316,52 @@ struct Builder {
         T.nboxes += 4 * nref;
         set_child_ranges(nb0, T.nboxes);
         return nref;
+    }
+
+    // Splits the selected boxes among the items [0, n1 + n2) -- item i is
+    // box lo + i for i < n1, else tlo + (i - n1) -- given their selection
+    // flags fp, its exclusive scan op and the number selected, nref (exact:
+    // counted from the same flags).  Four children per selected box are
+    // appended in item order, which is the order of the reference's
+    // per-level calls (a level range before its tail).  A child's level and
+    // size follow from its parent's level (d_bsl: box size per level), so
+    // the items may span several levels in box order.  Children get flag 3
+    // under a flag-1 parent and 0 otherwise (tree_refine_boxes_flag); with
+    // set_flags false the flags are left alone (tree_refine_boxes).
+    void split_items(int lo, int n1, int tlo, int n2, const int *fp, const int *op, int nref,
+                     const double *d_bsl, bool set_flags = true) {
+        if (nref <= 0) return;
+        ensure(T.nboxes + 4 * nref);
+        const int nb0 = T.nboxes, cap = T.cap;
+        double2 *cen = T.centers.get();
+        int *lev = T.level.get(), *par = T.parent.get(), *nch = T.nchild.get();
+        int *chi = T.child.get(), *flg = iflag.get();
+        int *cs = cnt_s.get(), *ct = cnt_t.get();
+        for_each((int64_t)n1 + n2, s, [=] __device__(int64_t i) {
+            if (!fp[i]) return;
+            const int b = i < n1 ? lo + (int)i : tlo + (int)(i - n1);
+            const int base = nb0 + 4 * op[i];
+            if (base + 4 > cap) return;
+            const double2 c = cen[b];
+            const int nl = lev[b] + 1;
+            const double bs = d_bsl[nl];
+            const int cf = set_flags && flg[b] == 1 ? 3 : 0;
+            nch[b] = 4;
+            for (int j = 0; j < 4; j++) {
+                const int kb = base + j;
+                cen[kb] = child_center(c, bs, j);
+                par[kb] = b;
+                nch[kb] = 0;
+                lev[kb] = nl;
+                for (int l = 0; l < 4; l++) chi[4 * kb + l] = -1;
+                chi[4 * b + j] = kb;
+                if (set_flags) flg[kb] = cf;
+                if (cs) cs[kb] = 0;
+                if (ct) ct[kb] = 0;
+            }
+        });
+        T.nboxes += 4 * nref;
+        set_child_ranges(nb0, T.nboxes);
     }
 
     std::vector<double> host_dist(int kind) const {
@@ -534,35 +584,42 @@ struct Builder {
         // remaining step (subdivision, reorganisation, colleagues, the
         // flag++ pass) would leave it as it is.
         if (count_flags(1, 2) == 0) return;
-        // Subdivide flag and flag+ boxes of the original levels.  Their
-        // flags are final, so the boxes to split on every level are counted
-        // at once (one synchronisation instead of one per level).
+        // Subdivide flag and flag+ boxes of the original levels 1 .. L-2.
+        // Their flags are final and the children of every level are
+        // appended after those of the coarser levels, so all levels split
+        // in one pass over the boxes in box order; the per-level counts (one
+        // synchronisation) give each level's range of new boxes.
         std::vector<int> ts(L + 1, 0), te(L + 1, 0);
         std::vector<int> nsplit(L + 1, 0);
+        DevBuf<double> d_bsl(T.boxsize.size(), s);
+        FMM_CUDA(cudaMemcpyAsync(d_bsl.get(), T.boxsize.data(), T.boxsize.size() * sizeof(double),
+                                 cudaMemcpyHostToDevice, s));
         if (L >= 3) {
-            DevBuf<int> cnt(L + 1, s);
-            cnt.zero(s);
-            int *cp = cnt.get();
-            const int *fl = iflag.get();
             const int lo = T.lstart[1], n = T.lend[L - 2] - lo;
+            DevBuf<int> cnt(L + 1, s), f(std::max(n, 1), s), off(std::max(n, 1), s);
+            cnt.zero(s);
+            int *cp = cnt.get(), *fp = f.get();
+            const int *fl = iflag.get();
             for_each(n, s, [=] __device__(int64_t i) {
                 const int b = lo + (int)i;
-                const int key = fl[b] > 0 ? lev[b] : -1;
+                const bool hit = fl[b] > 0;
+                fp[i] = hit ? 1 : 0;
+                const int key = hit ? lev[b] : -1;
                 const unsigned am = __activemask();
                 const unsigned peers = __match_any_sync(am, key);
                 if (key >= 0 && (int)(threadIdx.x & 31) == __ffs(peers) - 1)
                     atomicAdd(&cp[key], __popc(peers));
             });
+            exclusive_scan_i32(fp, off.get(), n, nullptr, s);
             read_small(nsplit.data(), cp, (L + 1) * sizeof(int), s);
-        }
-        for (int l = 1; l <= L - 2; l++) {
-            ts[l + 1] = T.nboxes;
-            int *fl = iflag.get();
-            if (nsplit[l] > 0)
-                refine_range(
-                    T.lstart[l], T.lend[l], l + 1, T.boxsize[l + 1],
-                    [=] __device__(int b) { return fl[b] > 0; }, true, nsplit[l]);
-            te[l + 1] = T.nboxes;
+            int nb = T.nboxes, nref = 0;
+            for (int l = 1; l <= L - 2; l++) {
+                ts[l + 1] = nb;
+                nb += 4 * nsplit[l];
+                te[l + 1] = nb;
+                nref += nsplit[l];
+            }
+            split_items(lo, n, 0, 0, fp, off.get(), nref, d_bsl.get());
         }
         reorg(ts, te);
         computecoll(0, L);
@@ -587,9 +644,18 @@ struct Builder {
             const double dist = d3[l];
             const int lo = T.lstart[l], n1 = T.lend[l] - T.lstart[l];
             const int tlo = ts[l], n2 = te[l] - ts[l];
+            ts[l + 1] = T.nboxes;
+            // the selection (final flag > 0) of the level and its tail, in
+            // item order, scanned for the children's places; the count is
+            // the one synchronisation of the level
+            DevBuf<int> f(std::max(n1 + n2, 1), s), off(std::max(n1 + n2, 1), s), tot(1, s);
+            int *fp = f.get();
             for_each(n1 + n2, s, [=] __device__(int64_t i) {
                 const int b = i < n1 ? lo + (int)i : tlo + (int)(i - n1);
-                if (fl[b] != 3) return;
+                if (fl[b] != 3) {
+                    fp[i] = fl[b] > 0 ? 1 : 0;
+                    return;
+                }
                 int f = 0;
                 const double2 cb = cp[b];
                 for (int k = 0; k < nnb[b] && !f; k++) {
@@ -603,35 +669,14 @@ struct Builder {
                     }
                 }
                 fl[b] = f;
+                fp[i] = f;
             });
-            ts[l + 1] = T.nboxes;
-            // the boxes to split in the level and in its tail, counted
-            // together (their flags are final; the splits only append)
-            int hc[2] = {0, 0};
-            {
-                DevBuf<int> c2(2, s);
-                c2.zero(s);
-                int *cp = c2.get();
-                for_each(n1 + n2, s, [=] __device__(int64_t i) {
-                    const int b = i < n1 ? lo + (int)i : tlo + (int)(i - n1);
-                    const int key = fl[b] > 0 ? (i < n1 ? 0 : 1) : -1;
-                    const unsigned am = __activemask();
-                    const unsigned peers = __match_any_sync(am, key);
-                    if (key >= 0 && (int)(threadIdx.x & 31) == __ffs(peers) - 1)
-                        atomicAdd(&cp[key], __popc(peers));
-                });
-                read_small(hc, cp, sizeof(hc), s);
+            int nref = 0;
+            if (n1 + n2 > 0) {
+                exclusive_scan_i32(fp, off.get(), n1 + n2, tot.get(), s);
+                read_small(&nref, tot.get(), sizeof(int), s);
             }
-            if (hc[0] > 0)
-                refine_range(
-                    T.lstart[l], T.lend[l], l + 1, T.boxsize[l + 1],
-                    [=] __device__(int b) { return fl[b] > 0; }, true, hc[0]);
-            if (hc[1] > 0) {
-                int *fl2 = iflag.get();
-                refine_range(
-                    tlo, tlo + n2, l + 1, T.boxsize[l + 1],
-                    [=] __device__(int b) { return fl2[b] > 0; }, true, hc[1]);
-            }
+            split_items(lo, n1, tlo, n2, fp, off.get(), nref, d_bsl.get());
             te[l + 1] = T.nboxes;
             // colleagues of the new boxes from their dad's (current) list
             const int nlo = ts[l + 1], nn = te[l + 1] - ts[l + 1];
@@ -1068,10 +1113,16 @@ bool build_by_keys(const double2 *d_src, int ns, const double2 *d_targ, int nt, 
                              cudaMemcpyHostToDevice, s));
     KeyedPoints ks, kt;
     const int nroots = F ? F->nroots : 1;
+    // presized form: the targets are sorted once the source keys have shown
+    // that ds digits suffice (a deeper tree retries with more digits)
+    const bool known = !sync_levels && presized_refinement(F, idivflag);
+    auto sort_targets = [&]() {
+        key_sort(d_targ, nt, c0, d_bsl.get(), ds, kt, s, F ? F->tprob : nullptr, F ? F->pbits : 0);
+        B.kvt = kt.view();
+    };
     key_sort(d_src, ns, c0, d_bsl.get(), ds, ks, s, F ? F->sprob : nullptr, F ? F->pbits : 0);
-    key_sort(d_targ, nt, c0, d_bsl.get(), ds, kt, s, F ? F->tprob : nullptr, F ? F->pbits : 0);
     B.kvs = ks.view();
-    B.kvt = kt.view();
+    if (!known) sort_targets();
     B.ensure(std::max(1024, 4 * nroots));
     T.nboxes = nroots;
     T.lstart.push_back(0);
@@ -1095,7 +1146,6 @@ bool build_by_keys(const double2 *d_src, int ns, const double2 *d_targ, int nt, 
     }
     // known refinement counts per level (presized form): level 0 from the
     // source count, levels 1..ds from the keys, one synchronisation
-    const bool known = !sync_levels && presized_refinement(F, idivflag);
     std::vector<unsigned long long> kc(65, 0);
     DevBuf<int> chk(known ? nlmax + 1 : 0, s);
     if (known) {
@@ -1111,6 +1161,7 @@ bool build_by_keys(const double2 *d_src, int ns, const double2 *d_targ, int nt, 
         }
         // a box of the deepest digit level still to be split: more digits
         if (ds < 64 && ds <= nlmax - 1 && kc[ds] > 0) return false;
+        sort_targets();
         long long tot = nroots;
         for (int l = 0; l < std::min(ds, nlmax); l++) {
             if (kc[l] == 0) break;
