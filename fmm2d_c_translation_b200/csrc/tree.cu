@@ -1181,6 +1181,44 @@ bool build_by_keys(const double2 *d_src, int ns, const double2 *d_targ, int nt, 
         if (known && last) break;  // (no box of level ds is split: checked above)
         DevBuf<int> f(hi - lo, s);
         int *fp = f.get();
+        if (known) {
+            // the capacity holds every level's known count; the new boxes
+            // are set to defaults in the selection's own launch, so a known
+            // count above the device's leaves no box unset (the ones no
+            // parent fills hang under the root, and the count check after
+            // the last level rebuilds the tree)
+            const int nref = (int)kc[ilev], n = hi - lo;
+            if (nref == 0) break;
+            T.boxsize.push_back(T.boxsize[ilev] / 2);
+            const int nb0 = T.nboxes;
+            const int nset = std::max(n, 4 * nref);
+            DevBuf<int> off(n, s);
+            double2 *cen = T.centers.get();
+            int *lev = T.level.get(), *par = T.parent.get(), *nch = T.nchild.get(),
+                *chi = T.child.get();
+            const int newlevel = ilev + 1;
+            for_each(nset, s, [=] __device__(int64_t i) {
+                if (i < n) {
+                    const int b = lo + (int)i;
+                    const int nss = ra[b].y - ra[b].x, ntt = rb[b].y - rb[b].x;
+                    const int nn = dflag == 0 ? nss : (dflag == 1 ? ntt : (nss > ntt ? nss : ntt));
+                    fp[i] = nn > nd ? 1 : 0;
+                }
+                if (i < 4 * (int64_t)nref) {
+                    const int kb = nb0 + (int)i;
+                    cen[kb] = cen[0];
+                    par[kb] = 0;
+                    lev[kb] = newlevel;
+                    nch[kb] = 0;
+                    for (int l = 0; l < 4; l++) chi[4 * kb + l] = -1;
+                }
+            });
+            exclusive_scan_i32(fp, off.get(), n, chk.get() + ilev, s);
+            B.split_items(lo, n, 0, 0, fp, off.get(), nref, d_bsl.get(), false);
+            T.lstart.push_back(nb0);
+            T.lend.push_back(T.nboxes);
+            continue;
+        }
         int *nf = nflag.get();
         if (last) nflag.zero(s);
         for_each(hi - lo, s, [=] __device__(int64_t i) {
