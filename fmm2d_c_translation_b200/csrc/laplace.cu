@@ -262,12 +262,67 @@ __global__ void __launch_bounds__(256) eval_far_points_kernel(
 #pragma unroll
         for (int q = 0; q < CH; q++) po[q] = gr[q] = he[q] = mk2<R2>(0.0, 0.0);
         const int n3 = (lb >= 1 && lb <= nlevels - 1) ? nlist3[b] : 0;
+        // mixed mode with both channels of a pair side by side in the FP32
+        // multipoles: one 16-byte load per coefficient for both Horner
+        // chains, and 1/z from one FP32 reciprocal of |z|^2 (the FP64
+        // divisions of the general form cost most of this pass's
+        // instructions where leaves sit on two levels)
+        bool pair3 = false;
+        if constexpr (MIXED && CH == 2) pair3 = mp32 && (ndc & 1) == 0 && (c0 & 1) == 0;
         for (int e = 0; e < n3; e++) {
             const int jb = list3[kMaxList3 * b + e];
             if (sse[jb].y <= sse[jb].x) continue;  // no multipole
             const double2 cj = centers[jb];
             const double r = bs[level[jb]];
             const double zx = x.x - cj.x, zy = x.y - cj.y;
+            if constexpr (MIXED && CH == 2) {
+                if (pair3) {
+                    const R fx = (R)zx, fy = (R)zy, rf = (R)r;
+                    const R zzf = fx * fx + fy * fy;
+                    const R izz = Real<MIXED>::rcp(zzf);
+                    const R2 zi = mk2<R2>(fx * izz, -fy * izz);  // 1/z
+                    const R2 w = zscal(zi, rf);                   // r/z
+                    const R lz = (R)0.5 * Real<MIXED>::log_(zzf);
+                    const R rinv = Real<MIXED>::rcp(rf);
+                    const int s4 = ndc >> 1;
+                    const float4 *M4 = reinterpret_cast<const float4 *>(mp32 + (size_t)jb * stride + c0);
+                    float4 v = M4[(size_t)p * s4];
+                    R2 a0[2] = {mk2<R2>(v.x, v.y), mk2<R2>(v.z, v.w)};
+                    R2 a1[2] = {mk2<R2>(0.0, 0.0), mk2<R2>(0.0, 0.0)};
+                    R2 a2[2] = {mk2<R2>(0.0, 0.0), mk2<R2>(0.0, 0.0)};
+                    for (int m = p - 1; m >= 1; m--) {
+                        v = M4[(size_t)m * s4];
+                        const R2 c[2] = {mk2<R2>(v.x, v.y), mk2<R2>(v.z, v.w)};
+#pragma unroll
+                        for (int q = 0; q < 2; q++) {
+                            if (PGH >= 3) a2[q] = zadd(zmul(a2[q], w), a1[q]);
+                            if (PGH >= 2) a1[q] = zadd(zmul(a1[q], w), a0[q]);
+                            a0[q] = zadd(zmul(a0[q], w), c[q]);
+                        }
+                    }
+                    v = M4[0];
+                    const R2 m0[2] = {mk2<R2>(v.x, v.y), mk2<R2>(v.z, v.w)};
+#pragma unroll
+                    for (int q = 0; q < 2; q++) {
+                        if (PGH >= 3) a2[q] = zadd(zmul(a2[q], w), a1[q]);
+                        if (PGH >= 2) a1[q] = zadd(zmul(a1[q], w), a0[q]);
+                        a0[q] = zmul(a0[q], w);
+                        po[q] = zadd(po[q], zadd(zscal(m0[q], lz), a0[q]));
+                        if (PGH >= 2) {
+                            const R2 w2 = zmul(w, w);
+                            gr[q] = zadd(gr[q], zadd(zmul(m0[q], zi), zscal(zmul(a1[q], w2), -rinv)));
+                            if (PGH >= 3) {
+                                const R2 w3 = zmul(w2, w), w4 = zmul(w2, w2);
+                                R2 h = zscal(zmul(m0[q], zmul(zi, zi)), (R)-1);
+                                h = zadd(h, zscal(zmul(a2[q], w4), (R)2 * rinv * rinv));
+                                h = zadd(h, zscal(zmul(a1[q], w3), (R)2 * rinv * rinv));
+                                he[q] = zadd(he[q], h);
+                            }
+                        }
+                    }
+                    continue;
+                }
+            }
             const double zz = zx * zx + zy * zy;
             const R2 zi = mk2<R2>(zx / zz, -zy / zz);                 // 1/z
             const R2 w = mk2<R2>(r * zx / zz, -r * zy / zz);          // r/z
