@@ -240,17 +240,21 @@ void laplace_evaluate(const FmmCall &c, const LapGeometry &G, bool on_dev, cudaS
     {
         const int *perm = T.isrc.get();
         auto put = [=] __device__(double2 *o, float2 *o32, size_t a, double2 v) {
-            o[a] = v;
+            if (o) o[a] = v;
             if (o32) o32[a] = make_float2((float)v.x, (float)v.y);
         };
-        // one pass over the points for charges and dipoles together
+        // one pass over the points for charges and dipoles together; the
+        // mixed mode's passes read only the FP32 copies while the P2M and
+        // P2L run their warp-per-box forms (order <= 39), so the FP64
+        // copies are not made there
         const bool ifc = c.ifcharge, ifd = c.ifdipole;
+        const bool keep64 = !mixed || G.p + 1 > 40;
         if (ifc) {
-            chg_s.alloc((size_t)ns * ndc, s);
+            if (keep64) chg_s.alloc((size_t)ns * ndc, s);
             if (mixed) chg32.alloc((size_t)ns * ndc, s);
         }
         if (ifd) {
-            dip_s.alloc((size_t)ns * ndc, s);
+            if (keep64) dip_s.alloc((size_t)ns * ndc, s);
             if (mixed) dip32.alloc((size_t)ns * ndc, s);
         }
         const double2 *q = reinterpret_cast<const double2 *>(chg_in.ptr),

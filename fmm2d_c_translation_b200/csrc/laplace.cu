@@ -1533,13 +1533,18 @@ inline size_t pow_warp_smem(int p, int CH) {
                                 (size_t)kPowSrc * sizeof(double));
 }
 
-template <int CH, bool P2L>
+// Strengths as the passes read them: FP64, or the FP32 copies of the mixed
+// mode (widened on load).
+__device__ __forceinline__ double2 str_d2(double2 v) { return v; }
+__device__ __forceinline__ double2 str_d2(float2 v) { return make_double2(v.x, v.y); }
+
+template <int CH, bool P2L, class S>
 __device__ __forceinline__ void pow_warp_box(int b, int p, int lane, double2 *sPw, double2 *sSt,
                                              double *sLz, const double2 c, const double r,
                                              const int2 *rgs, int nrg,
                                              const double2 *__restrict__ src,
-                                             const double2 *__restrict__ chg,
-                                             const double2 *__restrict__ dip, int ifc, int ifd,
+                                             const S *__restrict__ chg,
+                                             const S *__restrict__ dip, int ifc, int ifd,
                                              int ndc, int c0, double2 (&acc)[2][CH]) {
     const int P = p + 1;
     for (int g = 0; g < nrg; g++) {
@@ -1559,18 +1564,20 @@ __device__ __forceinline__ void pow_warp_box(int b, int p, int lane, double2 *sP
                     sLz[lane] = 0.5 * log(z0.x * z0.x + z0.y * z0.y);
 #pragma unroll
                     for (int q = 0; q < CH; q++)
-                        dv[q] = ifd ? cscal(cmul(dip[(size_t)j * ndc + c0 + q], zi), -1.0)
+                        dv[q] = ifd ? cscal(cmul(str_d2(dip[(size_t)j * ndc + c0 + q]), zi), -1.0)
                                     : make_double2(0.0, 0.0);
                 } else {
                     base = make_double2((x.x - c.x) / r, (x.y - c.y) / r);
                     const double rinv = 1.0 / r;
 #pragma unroll
                     for (int q = 0; q < CH; q++)
-                        dv[q] = ifd ? cscal(dip[(size_t)j * ndc + c0 + q], rinv) : make_double2(0.0, 0.0);
+                        dv[q] = ifd ? cscal(str_d2(dip[(size_t)j * ndc + c0 + q]), rinv)
+                                    : make_double2(0.0, 0.0);
                 }
 #pragma unroll
                 for (int q = 0; q < CH; q++) {
-                    sSt[lane * 2 * CH + q] = ifc ? chg[(size_t)j * ndc + c0 + q] : make_double2(0.0, 0.0);
+                    sSt[lane * 2 * CH + q] =
+                        ifc ? str_d2(chg[(size_t)j * ndc + c0 + q]) : make_double2(0.0, 0.0);
                     sSt[lane * 2 * CH + CH + q] = dv[q];
                 }
                 double2 w = make_double2(1.0, 0.0);
@@ -1628,7 +1635,7 @@ __global__ void __launch_bounds__(kPowWarps * 32) p2m_warp_kernel(
         for (int h = 0; h < 2; h++)
 #pragma unroll
             for (int q = 0; q < CH; q++) acc[h][q] = make_double2(0.0, 0.0);
-        pow_warp_box<CH, false>(b, p, lane, sPw, sSt, sLz, centers[b], bs[level[b]], &rg, 1, src,
+        pow_warp_box<CH, false, double2>(b, p, lane, sPw, sSt, sLz, centers[b], bs[level[b]], &rg, 1, src,
                                 chg, dip, ifc, ifd, ndc, c0, acc);
 #pragma unroll
         for (int h = 0; h < 2; h++) {
@@ -1648,12 +1655,13 @@ inline size_t pow32_warp_smem(int p, int CH) {
     return (size_t)kPowWarps * kPowSrc * (p + 1 + 2 * CH) * sizeof(float2);
 }
 
-template <int CH>
+// S: the dipole strengths' type (FP64, or the mixed mode's FP32 copies).
+template <int CH, class S>
 __global__ void __launch_bounds__(kPowWarps * 32) p2m_warp32_kernel(
     int lo, int hi, int p, const int *__restrict__ nchild, const double2 *__restrict__ centers,
     const int *__restrict__ level, const double *__restrict__ bs, const int2 *__restrict__ sse,
     const double2 *__restrict__ src, const float2 *__restrict__ chg32,
-    const double2 *__restrict__ dip, int ifc, int ifd, int ndc, int c0,
+    const S *__restrict__ dip, int ifc, int ifd, int ndc, int c0,
     double2 *__restrict__ mp) {
     extern __shared__ float2 pow32_smem[];
     const int P = p + 1, stride = P * ndc;
@@ -1682,7 +1690,7 @@ __global__ void __launch_bounds__(kPowWarps * 32) p2m_warp32_kernel(
 #pragma unroll
                 for (int q = 0; q < CH; q++) {
                     sSt[lane * 2 * CH + q] = ifc ? chg32[(size_t)j * ndc + c0 + q] : z0;
-                    const double2 d = ifd ? dip[(size_t)j * ndc + c0 + q] : make_double2(0.0, 0.0);
+                    const double2 d = ifd ? str_d2(dip[(size_t)j * ndc + c0 + q]) : make_double2(0.0, 0.0);
                     sSt[lane * 2 * CH + CH + q] = make_float2((float)(d.x * rinv), (float)(d.y * rinv));
                 }
                 float2 w = make_float2(1.f, 0.f);
@@ -1724,13 +1732,14 @@ __global__ void __launch_bounds__(kPowWarps * 32) p2m_warp32_kernel(
     }
 }
 
-template <int CH>
+// S: the strengths' type (FP64, or the mixed mode's FP32 copies).
+template <int CH, class S>
 __global__ void __launch_bounds__(kPowWarps * 32) p2l_warp_kernel(
     int lo, int hi, int p, EvalCounts ec, const int *__restrict__ nlist4,
     const int *__restrict__ list4, const double2 *__restrict__ centers,
     const int *__restrict__ level, const double *__restrict__ bs,
-    const double2 *__restrict__ src, const double2 *__restrict__ chg,
-    const double2 *__restrict__ dip, int ifc, int ifd, int ndc, int c0,
+    const double2 *__restrict__ src, const S *__restrict__ chg,
+    const S *__restrict__ dip, int ifc, int ifd, int ndc, int c0,
     double2 *__restrict__ loc) {
     extern __shared__ double2 pow_smem[];
     const int P = p + 1, stride = P * ndc;
@@ -1749,8 +1758,8 @@ __global__ void __launch_bounds__(kPowWarps * 32) p2l_warp_kernel(
         for (int h = 0; h < 2; h++)
 #pragma unroll
             for (int q = 0; q < CH; q++) acc[h][q] = make_double2(0.0, 0.0);
-        pow_warp_box<CH, true>(b, p, lane, sPw, sSt, sLz, centers[b], bs[level[b]], rgs, n4, src,
-                               chg, dip, ifc, ifd, ndc, c0, acc);
+        pow_warp_box<CH, true, S>(b, p, lane, sPw, sSt, sLz, centers[b], bs[level[b]], rgs, n4,
+                                  src, chg, dip, ifc, ifd, ndc, c0, acc);
 #pragma unroll
         for (int h = 0; h < 2; h++) {
             const int k = lane + 32 * h;
@@ -1784,10 +1793,18 @@ void upward_chunk(const Tree &T, const CauchyProblem &P, int c0,
     const bool warpk = p + 1 <= 40;
     if (L >= 2) {
         const int lo = T.lstart[2];
-        if (warpk && P.mixed && (P.charge32 || !P.ifcharge)) {
+        if (warpk && P.mixed && (P.charge32 || !P.ifcharge) && (P.dipstr32 || !P.ifdipole)) {
+            // the FP32 copies of the strengths (the FP64 ones may be absent)
             const size_t sm = pow32_warp_smem(p, CH);
-            raise_smem_limit(p2m_warp32_kernel<CH>, (int)sm);
-            p2m_warp32_kernel<CH><<<pow_grid(nb - lo), kPowWarps * 32, sm, s>>>(
+            raise_smem_limit(p2m_warp32_kernel<CH, float2>, (int)sm);
+            p2m_warp32_kernel<CH, float2><<<pow_grid(nb - lo), kPowWarps * 32, sm, s>>>(
+                lo, nb, p, T.nchild.get(), T.centers.get(), T.level.get(), bs,
+                T.srcse.get(), P.src, P.charge32, P.dipstr32, P.ifcharge, P.ifdipole,
+                P.ndc, c0, mp);
+        } else if (warpk && P.mixed && (P.charge32 || !P.ifcharge)) {
+            const size_t sm = pow32_warp_smem(p, CH);
+            raise_smem_limit(p2m_warp32_kernel<CH, double2>, (int)sm);
+            p2m_warp32_kernel<CH, double2><<<pow_grid(nb - lo), kPowWarps * 32, sm, s>>>(
                 lo, nb, p, T.nchild.get(), T.centers.get(), T.level.get(), bs,
                 T.srcse.get(), P.src, P.charge32, P.dipstr, P.ifcharge, P.ifdipole,
                 P.ndc, c0, mp);
@@ -1869,10 +1886,18 @@ void downward_chunk(const Tree &T, const CauchyProblem &P, int c0,
     const bool warpk = p + 1 <= 40;
     if (L >= 2) {
         const int lo = T.lstart[2];
-        if (warpk) {
+        if (warpk && P.mixed && (P.charge32 || !P.ifcharge) && (P.dipstr32 || !P.ifdipole)) {
+            // the FP32 copies of the strengths (the FP64 ones may be absent)
             const size_t sm = pow_warp_smem(p, CH);
-            raise_smem_limit(p2l_warp_kernel<CH>, (int)sm);
-            p2l_warp_kernel<CH><<<pow_grid(nb - lo), kPowWarps * 32, sm, s>>>(
+            raise_smem_limit(p2l_warp_kernel<CH, float2>, (int)sm);
+            p2l_warp_kernel<CH, float2><<<pow_grid(nb - lo), kPowWarps * 32, sm, s>>>(
+                lo, nb, p, ec, T.nlist4.get(), T.list4.get(), T.centers.get(),
+                T.level.get(), bs, P.src, P.charge32, P.dipstr32, P.ifcharge,
+                P.ifdipole, P.ndc, c0, loc);
+        } else if (warpk) {
+            const size_t sm = pow_warp_smem(p, CH);
+            raise_smem_limit(p2l_warp_kernel<CH, double2>, (int)sm);
+            p2l_warp_kernel<CH, double2><<<pow_grid(nb - lo), kPowWarps * 32, sm, s>>>(
                 lo, nb, p, ec, T.nlist4.get(), T.list4.get(), T.centers.get(),
                 T.level.get(), bs, P.src, P.charge, P.dipstr, P.ifcharge,
                 P.ifdipole, P.ndc, c0, loc);
