@@ -1650,13 +1650,19 @@ __global__ void __launch_bounds__(kPowWarps * 32) p2m_warp_kernel(
 // P2M of the mixed mode: the same scheme with the power series and its
 // sums in FP32 (the multipoles feed the FP32 / TF32 M2L, which reads them
 // rounded to FP32), from FP32 charges; the scaled offsets (x - c) / r and
-// d / r are formed in FP64 before the conversion.
+// d / r are formed in FP64 before the conversion.  A chunk holds up to 32
+// sources (a leaf's sources in one chunk: every lane builds one source's
+// powers), a source's strengths are read back as 16-byte pairs, and with
+// real charges (LAPR: lfmm2d's channels, imaginary parts exactly 0) the
+// charge terms drop their zero halves (the same sums to the bit).
+constexpr int kPow32Src = 32;
+
 inline size_t pow32_warp_smem(int p, int CH) {
-    return (size_t)kPowWarps * kPowSrc * (p + 1 + 2 * CH) * sizeof(float2);
+    return (size_t)kPowWarps * kPow32Src * (p + 1 + 2 * CH) * sizeof(float2);
 }
 
 // S: the dipole strengths' type (FP64, or the mixed mode's FP32 copies).
-template <int CH, class S>
+template <int CH, class S, bool LAPR>
 __global__ void __launch_bounds__(kPowWarps * 32) p2m_warp32_kernel(
     int lo, int hi, int p, const int *__restrict__ nchild, const double2 *__restrict__ centers,
     const int *__restrict__ level, const double *__restrict__ bs, const int2 *__restrict__ sse,
@@ -1666,8 +1672,10 @@ __global__ void __launch_bounds__(kPowWarps * 32) p2m_warp32_kernel(
     extern __shared__ float2 pow32_smem[];
     const int P = p + 1, stride = P * ndc;
     const int lane = lane_id(), wib = threadIdx.x >> 5;
-    float2 *sPw = pow32_smem + (size_t)wib * kPowSrc * (P + 2 * CH);
-    float2 *sSt = sPw + kPowSrc * P;
+    float2 *sPw = pow32_smem + (size_t)wib * kPow32Src * (P + 2 * CH);
+    // strengths of source s: [q_0 .. q_CH-1, d_0 .. d_CH-1] at sSt + s * 2 CH
+    // (16-byte aligned: the power table holds kPow32Src * P float2)
+    float2 *sSt = sPw + kPow32Src * P;
     const float2 z0 = make_float2(0.f, 0.f);
     for (int b = lo + warp_global(); b < hi; b += warp_count()) {
         if (nchild[b] != 0) continue;
@@ -1680,8 +1688,8 @@ __global__ void __launch_bounds__(kPowWarps * 32) p2m_warp32_kernel(
         for (int h = 0; h < 2; h++)
 #pragma unroll
             for (int q = 0; q < CH; q++) acc[h][q] = z0;
-        for (int j0 = rg.x; j0 < rg.y; j0 += kPowSrc) {
-            const int n = min(kPowSrc, rg.y - j0);
+        for (int j0 = rg.x; j0 < rg.y; j0 += kPow32Src) {
+            const int n = min(kPow32Src, rg.y - j0);
             __syncwarp();
             if (lane < n) {
                 const int j = j0 + lane;
@@ -1708,14 +1716,33 @@ __global__ void __launch_bounds__(kPowWarps * 32) p2m_warp32_kernel(
                 for (int s = 0; s < n; s++) {
                     const float2 pk = sPw[s * P + k];
                     const float2 pd = k > 0 ? sPw[s * P + k - 1] : z0;  // z^(k-1) for the dipole
+                    float2 qv[CH], dv[CH];
+                    if constexpr (CH == 2) {
+                        const float4 *st4 = reinterpret_cast<const float4 *>(sSt + s * 4);
+                        const float4 a = st4[0], d4 = st4[1];
+                        qv[0] = make_float2(a.x, a.y);
+                        qv[1] = make_float2(a.z, a.w);
+                        dv[0] = make_float2(d4.x, d4.y);
+                        dv[1] = make_float2(d4.z, d4.w);
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < CH; q++) {
+                            qv[q] = sSt[s * 2 * CH + q];
+                            dv[q] = sSt[s * 2 * CH + CH + q];
+                        }
+                    }
+                    const float2 pks = zscal(pk, ik);
 #pragma unroll
                     for (int q = 0; q < CH; q++) {
-                        const float2 qv = sSt[s * 2 * CH + q], dv = sSt[s * 2 * CH + CH + q];
-                        if (k == 0)
-                            acc[h][q] = zadd(acc[h][q], qv);
-                        else
-                            zfma(acc[h][q], qv, zscal(pk, ik));
-                        zfma(acc[h][q], dv, pd);
+                        if (k == 0) {
+                            acc[h][q] = zadd(acc[h][q], qv[q]);
+                        } else if (LAPR) {
+                            acc[h][q].x = fmaf(qv[q].x, pks.x, acc[h][q].x);
+                            acc[h][q].y = fmaf(qv[q].x, pks.y, acc[h][q].y);
+                        } else {
+                            zfma(acc[h][q], qv[q], pks);
+                        }
+                        zfma(acc[h][q], dv[q], pd);
                     }
                 }
             }
@@ -1793,21 +1820,24 @@ void upward_chunk(const Tree &T, const CauchyProblem &P, int c0,
     const bool warpk = p + 1 <= 40;
     if (L >= 2) {
         const int lo = T.lstart[2];
-        if (warpk && P.mixed && (P.charge32 || !P.ifcharge) && (P.dipstr32 || !P.ifdipole)) {
-            // the FP32 copies of the strengths (the FP64 ones may be absent)
+        if (warpk && P.mixed && (P.charge32 || !P.ifcharge)) {
+            // FP32 dipoles when there are (the FP64 ones may be absent)
+            const bool d32 = P.dipstr32 || !P.ifdipole;
             const size_t sm = pow32_warp_smem(p, CH);
-            raise_smem_limit(p2m_warp32_kernel<CH, float2>, (int)sm);
-            p2m_warp32_kernel<CH, float2><<<pow_grid(nb - lo), kPowWarps * 32, sm, s>>>(
-                lo, nb, p, T.nchild.get(), T.centers.get(), T.level.get(), bs,
-                T.srcse.get(), P.src, P.charge32, P.dipstr32, P.ifcharge, P.ifdipole,
-                P.ndc, c0, mp);
-        } else if (warpk && P.mixed && (P.charge32 || !P.ifcharge)) {
-            const size_t sm = pow32_warp_smem(p, CH);
-            raise_smem_limit(p2m_warp32_kernel<CH, double2>, (int)sm);
-            p2m_warp32_kernel<CH, double2><<<pow_grid(nb - lo), kPowWarps * 32, sm, s>>>(
-                lo, nb, p, T.nchild.get(), T.centers.get(), T.level.get(), bs,
-                T.srcse.get(), P.src, P.charge32, P.dipstr, P.ifcharge, P.ifdipole,
-                P.ndc, c0, mp);
+            auto launch = [&](auto kern, const auto *dip) {
+                raise_smem_limit(kern, (int)sm);
+                kern<<<pow_grid(nb - lo), kPowWarps * 32, sm, s>>>(
+                    lo, nb, p, T.nchild.get(), T.centers.get(), T.level.get(), bs,
+                    T.srcse.get(), P.src, P.charge32, dip, P.ifcharge, P.ifdipole, P.ndc, c0, mp);
+            };
+            if (d32 && P.real_charge)
+                launch(p2m_warp32_kernel<CH, float2, true>, P.dipstr32);
+            else if (d32)
+                launch(p2m_warp32_kernel<CH, float2, false>, P.dipstr32);
+            else if (P.real_charge)
+                launch(p2m_warp32_kernel<CH, double2, true>, P.dipstr);
+            else
+                launch(p2m_warp32_kernel<CH, double2, false>, P.dipstr);
         } else if (warpk) {
             const size_t sm = pow_warp_smem(p, CH);
             raise_smem_limit(p2m_warp_kernel<CH>, (int)sm);
