@@ -1662,9 +1662,12 @@ inline size_t pow32_warp_smem(int p, int CH) {
 }
 
 // S: the dipole strengths' type (FP64, or the mixed mode's FP32 copies).
+// ids / off (optional): the leaves with sources in box order, entries
+// ids[off[lo] .. off[hi]) (only those are visited).
 template <int CH, class S, bool LAPR>
 __global__ void __launch_bounds__(kPowWarps * 32) p2m_warp32_kernel(
-    int lo, int hi, int p, const int *__restrict__ nchild, const double2 *__restrict__ centers,
+    int lo, int hi, const int *__restrict__ ids, const int *__restrict__ off, int p,
+    const int *__restrict__ nchild, const double2 *__restrict__ centers,
     const int *__restrict__ level, const double *__restrict__ bs, const int2 *__restrict__ sse,
     const double2 *__restrict__ src, const float2 *__restrict__ chg32,
     const S *__restrict__ dip, int ifc, int ifd, int ndc, int c0,
@@ -1677,8 +1680,10 @@ __global__ void __launch_bounds__(kPowWarps * 32) p2m_warp32_kernel(
     // (16-byte aligned: the power table holds kPow32Src * P float2)
     float2 *sSt = sPw + kPow32Src * P;
     const float2 z0 = make_float2(0.f, 0.f);
-    for (int b = lo + warp_global(); b < hi; b += warp_count()) {
-        if (nchild[b] != 0) continue;
+    const int k0 = ids ? off[lo] : lo, k1 = ids ? off[hi] : hi;
+    for (int kb = k0 + warp_global(); kb < k1; kb += warp_count()) {
+        const int b = ids ? ids[kb] : kb;
+        if (!ids && nchild[b] != 0) continue;
         const int2 rg = sse[b];
         if (rg.y <= rg.x) continue;
         const double2 c = centers[b];
@@ -1760,9 +1765,13 @@ __global__ void __launch_bounds__(kPowWarps * 32) p2m_warp32_kernel(
 }
 
 // S: the strengths' type (FP64, or the mixed mode's FP32 copies).
+// ids / off (optional): the boxes with list-4 entries and evaluation
+// points in box order, entries ids[off[lo] .. off[hi]) (only those are
+// visited).
 template <int CH, class S>
 __global__ void __launch_bounds__(kPowWarps * 32) p2l_warp_kernel(
-    int lo, int hi, int p, EvalCounts ec, const int *__restrict__ nlist4,
+    int lo, int hi, const int *__restrict__ ids, const int *__restrict__ off, int p,
+    EvalCounts ec, const int *__restrict__ nlist4,
     const int *__restrict__ list4, const double2 *__restrict__ centers,
     const int *__restrict__ level, const double *__restrict__ bs,
     const double2 *__restrict__ src, const S *__restrict__ chg,
@@ -1775,7 +1784,9 @@ __global__ void __launch_bounds__(kPowWarps * 32) p2l_warp_kernel(
     double2 *sSt = sPw + kPowSrc * P;
     double *sLz = reinterpret_cast<double *>(pow_smem + (size_t)kPowWarps * kPowSrc * (P + 2 * CH)) +
                   wib * kPowSrc;
-    for (int b = lo + warp_global(); b < hi; b += warp_count()) {
+    const int k0 = ids ? off[lo] : lo, k1 = ids ? off[hi] : hi;
+    for (int kb = k0 + warp_global(); kb < k1; kb += warp_count()) {
+        const int b = ids ? ids[kb] : kb;
         const int n4 = nlist4[b];
         if (n4 == 0 || ec.npts(b) <= 0) continue;
         int2 rgs[kMaxList4];
@@ -1827,7 +1838,7 @@ void upward_chunk(const Tree &T, const CauchyProblem &P, int c0,
             auto launch = [&](auto kern, const auto *dip) {
                 raise_smem_limit(kern, (int)sm);
                 kern<<<pow_grid(nb - lo), kPowWarps * 32, sm, s>>>(
-                    lo, nb, p, T.nchild.get(), T.centers.get(), T.level.get(), bs,
+                    lo, nb, P.p2m_ids, P.p2m_off, p, T.nchild.get(), T.centers.get(), T.level.get(), bs,
                     T.srcse.get(), P.src, P.charge32, dip, P.ifcharge, P.ifdipole, P.ndc, c0, mp);
             };
             if (d32 && P.real_charge)
@@ -1921,14 +1932,14 @@ void downward_chunk(const Tree &T, const CauchyProblem &P, int c0,
             const size_t sm = pow_warp_smem(p, CH);
             raise_smem_limit(p2l_warp_kernel<CH, float2>, (int)sm);
             p2l_warp_kernel<CH, float2><<<pow_grid(nb - lo), kPowWarps * 32, sm, s>>>(
-                lo, nb, p, ec, T.nlist4.get(), T.list4.get(), T.centers.get(),
+                lo, nb, P.p2l_ids, P.p2l_off, p, ec, T.nlist4.get(), T.list4.get(), T.centers.get(),
                 T.level.get(), bs, P.src, P.charge32, P.dipstr32, P.ifcharge,
                 P.ifdipole, P.ndc, c0, loc);
         } else if (warpk) {
             const size_t sm = pow_warp_smem(p, CH);
             raise_smem_limit(p2l_warp_kernel<CH, double2>, (int)sm);
             p2l_warp_kernel<CH, double2><<<pow_grid(nb - lo), kPowWarps * 32, sm, s>>>(
-                lo, nb, p, ec, T.nlist4.get(), T.list4.get(), T.centers.get(),
+                lo, nb, P.p2l_ids, P.p2l_off, p, ec, T.nlist4.get(), T.list4.get(), T.centers.get(),
                 T.level.get(), bs, P.src, P.charge, P.dipstr, P.ifcharge,
                 P.ifdipole, P.ndc, c0, loc);
         } else
@@ -2153,7 +2164,7 @@ void cauchy_fmm(const Tree &T, const CauchyProblem &P0, cudaStream_t s) {
                              (size_t)nlow * (P.p + 1) * P.ndc * sizeof(double2), s));
     // the boxes the Pascal M2M and L2L visit (in adaptive trees most boxes
     // of the deep levels are leaves or empty)
-    DevBuf<int> m2m_ids, m2m_off, l2l_ids, l2l_off;
+    DevBuf<int> m2m_ids, m2m_off, l2l_ids, l2l_off, p2m_ids, p2m_off, p2l_ids, p2l_off;
     if (T.nlevels >= 2 && P.p + 1 <= 40) {
         const int *nchp = T.nchild.get();
         const int2 *sse = T.srcse.get();
@@ -2161,6 +2172,17 @@ void cauchy_fmm(const Tree &T, const CauchyProblem &P0, cudaStream_t s) {
         box_list(T.nboxes, [=] __device__(int b) { return nchp[b] > 0 && count(sse, b) > 0; },
                  m2m_ids, m2m_off, s);
         box_list(T.nboxes, [=] __device__(int b) { return ec.npts(b) > 0; }, l2l_ids, l2l_off, s);
+        if (P.mixed) {
+            box_list(T.nboxes, [=] __device__(int b) { return nchp[b] == 0 && count(sse, b) > 0; },
+                     p2m_ids, p2m_off, s);
+            P.p2m_ids = p2m_ids.get();
+            P.p2m_off = p2m_off.get();
+        }
+        const int *n4p = T.nlist4.get();
+        box_list(T.nboxes, [=] __device__(int b) { return n4p[b] > 0 && ec.npts(b) > 0; },
+                 p2l_ids, p2l_off, s);
+        P.p2l_ids = p2l_ids.get();
+        P.p2l_off = p2l_off.get();
         P.m2m_ids = m2m_ids.get();
         P.m2m_off = m2m_off.get();
         P.l2l_ids = l2l_ids.get();

@@ -86,6 +86,10 @@ struct CauchyProblem {
     // ids[off[lstart[l]] .. off[lend[l]]) (set by cauchy_fmm)
     const int *m2m_ids = nullptr, *m2m_off = nullptr;
     const int *l2l_ids = nullptr, *l2l_off = nullptr;
+    // leaves with sources (the boxes the P2M visits), same form
+    const int *p2m_ids = nullptr, *p2m_off = nullptr;
+    // boxes with list-4 entries and evaluation points (the P2L), same form
+    const int *p2l_ids = nullptr, *p2l_off = nullptr;
 };
 
 // Runs steps 1-8 of cfmm2dmain (src/laplace/cfmm2d.f:442-1340) on the
