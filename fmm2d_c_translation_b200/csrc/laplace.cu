@@ -1391,16 +1391,15 @@ __device__ __forceinline__ double2 child_offset(int cs) {
 template <int PMAX>
 __global__ void __launch_bounds__(128) l2l_pascal_kernel(
     int lo, int hi, int p, EvalCounts ec, const int *__restrict__ ids,
-    const int *__restrict__ off, const int *__restrict__ parent,
+    const int *__restrict__ nids, const int *__restrict__ parent,
     const int *__restrict__ child, int ndc, int c0, int nch, double2 *__restrict__ loc,
     float2 *__restrict__ loc32) {
     const int stride = (p + 1) * ndc;
-    const int k0 = ids ? off[lo] : 0;
-    const int64_t total = (int64_t)(ids ? off[hi] - k0 : hi - lo) * nch;
+    const int64_t total = (int64_t)(ids ? *nids : hi - lo) * nch;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
          t += (int64_t)gridDim.x * blockDim.x) {
         const int k = (int)(t / nch), q = c0 + (int)(t % nch);
-        const int b = ids ? ids[k0 + k] : lo + k;
+        const int b = ids ? ids[k] : lo + k;
         const int pb = parent[b];
         if (!ids && ec.npts(pb) <= 0) continue;
         const double2 d = child_offset(child_pos(child, pb, b));
@@ -1437,19 +1436,18 @@ __global__ void __launch_bounds__(128) l2l_pascal_kernel(
 // sources), or, with ids null, are all boxes of [lo, hi) with children.
 template <int PMAX>
 __global__ void __launch_bounds__(128) m2m_pascal_kernel(
-    int lo, int hi, int p, const int *__restrict__ ids, const int *__restrict__ off,
+    int lo, int hi, int p, const int *__restrict__ ids, const int *__restrict__ nids,
     const int *__restrict__ nchild, const int *__restrict__ child,
     const int2 *__restrict__ sse, int ndc, int c0, int nch, double2 *__restrict__ mp) {
     const int stride = (p + 1) * ndc;
-    const int k0 = ids ? off[lo] : 0;
-    const int64_t total = (int64_t)(ids ? off[hi] - k0 : hi - lo) * nch * 4;
+    const int64_t total = (int64_t)(ids ? *nids : hi - lo) * nch * 4;
     // warp-uniform trip count: the lanes of a parent meet in the shuffles
     for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < total;
          base += (int64_t)gridDim.x * blockDim.x) {
         const int64_t t = base + threadIdx.x;
         const bool valid = t < total;
         const int64_t tt = valid ? t : 0;
-        const int b = ids ? ids[k0 + (int)(tt / (4 * nch))] : lo + (int)(tt / (4 * nch));
+        const int b = ids ? ids[(int)(tt / (4 * nch))] : lo + (int)(tt / (4 * nch));
         const int q = c0 + (int)((tt / 4) % nch), cs = (int)(tt % 4);
         const bool par = valid && nchild[b] > 0;
         const double2 d = child_offset(cs);
@@ -1495,18 +1493,57 @@ __global__ void __launch_bounds__(128) m2m_pascal_kernel(
     }
 }
 
-// Boxes b of [0, nb) with pred(b), in box order: ids[off[b]] = b, off[nb]
-// the count (off is the exclusive scan of the predicate).
-template <class Pred>
-void box_list(int nb, Pred pred, DevBuf<int> &ids, DevBuf<int> &off, cudaStream_t s) {
-    DevBuf<int> f(std::max(nb, 1), s);
-    ids.alloc(std::max(nb, 1), s);
-    off.alloc(nb + 1, s);
-    int *fp = f.get(), *ip = ids.get(), *op = off.get();
-    for_each(nb, s, [=] __device__(int64_t i) { fp[i] = pred((int)i) ? 1 : 0; });
-    exclusive_scan_i32(fp, op, nb, op + nb, s);
-    for_each(nb, s, [=] __device__(int64_t i) {
-        if (fp[i]) ip[op[i]] = (int)i;
+// The boxes the Pascal M2M and L2L, the FP32 P2M and the P2L visit, made in
+// one launch.  List i holds the boxes with bit i of sel(b): lists 0 and 1
+// (M2M, L2L) in one segment per level, level l's at ids[i][ls[l] ..
+// ls[l] + cnt[i][l]) (the level's box range bounds it), lists 2 and 3
+// (P2M, P2L) in one segment, ids[i][0 .. cnt[i][0]).  Slots come from
+// warp-aggregated atomic counters, so the order within a segment is not
+// box order; every visited box's work is independent of the others', so
+// the results do not depend on it.
+struct LevelStarts {
+    int v[kMaxLevels + 2];
+};
+struct BoxLists {
+    DevBuf<int> ids[4], cnt;
+    int L = 0;
+    // list i's entries and count for level l (lists 0, 1) or all (2, 3)
+    const int *seg(int i, const LevelStarts &ls, int l) const {
+        return ids[i].get() + (i < 2 ? ls.v[l] : 0);
+    }
+    const int *count(int i, int l) const { return cnt.get() + i * (L + 1) + (i < 2 ? l : 0); }
+};
+
+template <class Sel>
+void make_box_lists(const Tree &T, const LevelStarts &ls, Sel sel, BoxLists &B, cudaStream_t s) {
+    const int nb = T.nboxes, L = T.nlevels;
+    B.L = L;
+    for (int i = 0; i < 4; i++) B.ids[i].alloc(std::max(nb, 1), s);
+    B.cnt.alloc((size_t)4 * (L + 1), s);
+    B.cnt.zero(s);
+    int *i0 = B.ids[0].get(), *i1 = B.ids[1].get(), *i2 = B.ids[2].get(), *i3 = B.ids[3].get();
+    int *cn = B.cnt.get();
+    const int *lev = T.level.get();
+    for_each(nb, s, [=] __device__(int64_t t) {
+        const int b = (int)t, l = lev[b];
+        const unsigned m = sel(b);
+        const unsigned am = __activemask();
+        const int lane = (int)(threadIdx.x & 31);
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int key = ((m >> i) & 1u) ? (i < 2 ? l : 0) : -1;
+            const unsigned peers = __match_any_sync(am, key);
+            const int leader = __ffs(peers) - 1;
+            int base = 0;
+            if (key >= 0 && lane == leader)
+                base = atomicAdd(cn + i * (L + 1) + key, __popc(peers));
+            base = __shfl_sync(peers, base, leader);
+            if (key >= 0) {
+                int *ids = i == 0 ? i0 : (i == 1 ? i1 : (i == 2 ? i2 : i3));
+                const int rank = __popc(peers & ((1u << lane) - 1u));
+                ids[(i < 2 ? ls.v[l] : 0) + base + rank] = b;
+            }
+        }
     });
 }
 
@@ -1666,7 +1703,7 @@ inline size_t pow32_warp_smem(int p, int CH) {
 // ids[off[lo] .. off[hi]) (only those are visited).
 template <int CH, class S, bool LAPR>
 __global__ void __launch_bounds__(kPowWarps * 32) p2m_warp32_kernel(
-    int lo, int hi, const int *__restrict__ ids, const int *__restrict__ off, int p,
+    int lo, int hi, const int *__restrict__ ids, const int *__restrict__ nids, int p,
     const int *__restrict__ nchild, const double2 *__restrict__ centers,
     const int *__restrict__ level, const double *__restrict__ bs, const int2 *__restrict__ sse,
     const double2 *__restrict__ src, const float2 *__restrict__ chg32,
@@ -1680,7 +1717,7 @@ __global__ void __launch_bounds__(kPowWarps * 32) p2m_warp32_kernel(
     // (16-byte aligned: the power table holds kPow32Src * P float2)
     float2 *sSt = sPw + kPow32Src * P;
     const float2 z0 = make_float2(0.f, 0.f);
-    const int k0 = ids ? off[lo] : lo, k1 = ids ? off[hi] : hi;
+    const int k0 = ids ? 0 : lo, k1 = ids ? *nids : hi;
     for (int kb = k0 + warp_global(); kb < k1; kb += warp_count()) {
         const int b = ids ? ids[kb] : kb;
         if (!ids && nchild[b] != 0) continue;
@@ -1770,7 +1807,7 @@ __global__ void __launch_bounds__(kPowWarps * 32) p2m_warp32_kernel(
 // visited).
 template <int CH, class S>
 __global__ void __launch_bounds__(kPowWarps * 32) p2l_warp_kernel(
-    int lo, int hi, const int *__restrict__ ids, const int *__restrict__ off, int p,
+    int lo, int hi, const int *__restrict__ ids, const int *__restrict__ nids, int p,
     EvalCounts ec, const int *__restrict__ nlist4,
     const int *__restrict__ list4, const double2 *__restrict__ centers,
     const int *__restrict__ level, const double *__restrict__ bs,
@@ -1784,7 +1821,7 @@ __global__ void __launch_bounds__(kPowWarps * 32) p2l_warp_kernel(
     double2 *sSt = sPw + kPowSrc * P;
     double *sLz = reinterpret_cast<double *>(pow_smem + (size_t)kPowWarps * kPowSrc * (P + 2 * CH)) +
                   wib * kPowSrc;
-    const int k0 = ids ? off[lo] : lo, k1 = ids ? off[hi] : hi;
+    const int k0 = ids ? 0 : lo, k1 = ids ? *nids : hi;
     for (int kb = k0 + warp_global(); kb < k1; kb += warp_count()) {
         const int b = ids ? ids[kb] : kb;
         const int n4 = nlist4[b];
@@ -1838,7 +1875,7 @@ void upward_chunk(const Tree &T, const CauchyProblem &P, int c0,
             auto launch = [&](auto kern, const auto *dip) {
                 raise_smem_limit(kern, (int)sm);
                 kern<<<pow_grid(nb - lo), kPowWarps * 32, sm, s>>>(
-                    lo, nb, P.p2m_ids, P.p2m_off, p, T.nchild.get(), T.centers.get(), T.level.get(), bs,
+                    lo, nb, P.p2m_ids, P.p2m_cnt, p, T.nchild.get(), T.centers.get(), T.level.get(), bs,
                     T.srcse.get(), P.src, P.charge32, dip, P.ifcharge, P.ifdipole, P.ndc, c0, mp);
             };
             if (d32 && P.real_charge)
@@ -1868,17 +1905,19 @@ void upward_chunk(const Tree &T, const CauchyProblem &P, int c0,
     for (int l = L - 1; l >= 1; l--) {
         const int lo = T.lstart[l], hi = T.lend[l];
         const int64_t nt = (int64_t)(hi - lo) * CH * 4;
+        const int *ids = P.m2m_ids ? P.m2m_ids + lo : nullptr;
+        const int *nid = P.m2m_ids ? P.m2m_cnt + l : nullptr;
         if (p + 1 <= 20)
             m2m_pascal_kernel<20><<<pascal_grid(nt), 128, 0, s>>>(
-                lo, hi, p, P.m2m_ids, P.m2m_off, T.nchild.get(), T.child.get(), T.srcse.get(),
+                lo, hi, p, ids, nid, T.nchild.get(), T.child.get(), T.srcse.get(),
                 P.ndc, c0, CH, mp);
         else if (p + 1 <= 32)
             m2m_pascal_kernel<32><<<pascal_grid(nt), 128, 0, s>>>(
-                lo, hi, p, P.m2m_ids, P.m2m_off, T.nchild.get(), T.child.get(), T.srcse.get(),
+                lo, hi, p, ids, nid, T.nchild.get(), T.child.get(), T.srcse.get(),
                 P.ndc, c0, CH, mp);
         else if (p + 1 <= 40)
             m2m_pascal_kernel<40><<<pascal_grid(nt), 128, 0, s>>>(
-                lo, hi, p, P.m2m_ids, P.m2m_off, T.nchild.get(), T.child.get(), T.srcse.get(),
+                lo, hi, p, ids, nid, T.nchild.get(), T.child.get(), T.srcse.get(),
                 P.ndc, c0, CH, mp);
         else
             m2m_coef_kernel<CH><<<blocks(hi - lo), 256, 0, s>>>(
@@ -1932,14 +1971,14 @@ void downward_chunk(const Tree &T, const CauchyProblem &P, int c0,
             const size_t sm = pow_warp_smem(p, CH);
             raise_smem_limit(p2l_warp_kernel<CH, float2>, (int)sm);
             p2l_warp_kernel<CH, float2><<<pow_grid(nb - lo), kPowWarps * 32, sm, s>>>(
-                lo, nb, P.p2l_ids, P.p2l_off, p, ec, T.nlist4.get(), T.list4.get(), T.centers.get(),
+                lo, nb, P.p2l_ids, P.p2l_cnt, p, ec, T.nlist4.get(), T.list4.get(), T.centers.get(),
                 T.level.get(), bs, P.src, P.charge32, P.dipstr32, P.ifcharge,
                 P.ifdipole, P.ndc, c0, loc);
         } else if (warpk) {
             const size_t sm = pow_warp_smem(p, CH);
             raise_smem_limit(p2l_warp_kernel<CH, double2>, (int)sm);
             p2l_warp_kernel<CH, double2><<<pow_grid(nb - lo), kPowWarps * 32, sm, s>>>(
-                lo, nb, P.p2l_ids, P.p2l_off, p, ec, T.nlist4.get(), T.list4.get(), T.centers.get(),
+                lo, nb, P.p2l_ids, P.p2l_cnt, p, ec, T.nlist4.get(), T.list4.get(), T.centers.get(),
                 T.level.get(), bs, P.src, P.charge, P.dipstr, P.ifcharge,
                 P.ifdipole, P.ndc, c0, loc);
         } else
@@ -1955,17 +1994,19 @@ void downward_chunk(const Tree &T, const CauchyProblem &P, int c0,
     for (int l = 1; l <= L - 1; l++) {
         const int lo = T.lstart[l + 1], hi = T.lend[l + 1];
         const int64_t nt = (int64_t)(hi - lo) * CH;
+        const int *ids = P.l2l_ids ? P.l2l_ids + lo : nullptr;
+        const int *nid = P.l2l_ids ? P.l2l_cnt + l + 1 : nullptr;
         if (p + 1 <= 20)
             l2l_pascal_kernel<20><<<pascal_grid(nt), 128, 0, s>>>(
-                lo, hi, p, ec, P.l2l_ids, P.l2l_off, T.parent.get(), T.child.get(), P.ndc, c0,
+                lo, hi, p, ec, ids, nid, T.parent.get(), T.child.get(), P.ndc, c0,
                 CH, loc, loc32);
         else if (p + 1 <= 32)
             l2l_pascal_kernel<32><<<pascal_grid(nt), 128, 0, s>>>(
-                lo, hi, p, ec, P.l2l_ids, P.l2l_off, T.parent.get(), T.child.get(), P.ndc, c0,
+                lo, hi, p, ec, ids, nid, T.parent.get(), T.child.get(), P.ndc, c0,
                 CH, loc, loc32);
         else if (p + 1 <= 40)
             l2l_pascal_kernel<40><<<pascal_grid(nt), 128, 0, s>>>(
-                lo, hi, p, ec, P.l2l_ids, P.l2l_off, T.parent.get(), T.child.get(), P.ndc, c0,
+                lo, hi, p, ec, ids, nid, T.parent.get(), T.child.get(), P.ndc, c0,
                 CH, loc, loc32);
         else
             l2l_coef_kernel<CH><<<blocks(hi - lo), 256, 0, s>>>(
@@ -2164,29 +2205,29 @@ void cauchy_fmm(const Tree &T, const CauchyProblem &P0, cudaStream_t s) {
                              (size_t)nlow * (P.p + 1) * P.ndc * sizeof(double2), s));
     // the boxes the Pascal M2M and L2L visit (in adaptive trees most boxes
     // of the deep levels are leaves or empty)
-    DevBuf<int> m2m_ids, m2m_off, l2l_ids, l2l_off, p2m_ids, p2m_off, p2l_ids, p2l_off;
+    BoxLists lists;
     if (T.nlevels >= 2 && P.p + 1 <= 40) {
-        const int *nchp = T.nchild.get();
+        const int *nchp = T.nchild.get(), *n4p = T.nlist4.get();
         const int2 *sse = T.srcse.get();
         const EvalCounts ec{T.srcse.get(), T.trgse.get(), P.sset.pgh, P.tset.pgh};
-        box_list(T.nboxes, [=] __device__(int b) { return nchp[b] > 0 && count(sse, b) > 0; },
-                 m2m_ids, m2m_off, s);
-        box_list(T.nboxes, [=] __device__(int b) { return ec.npts(b) > 0; }, l2l_ids, l2l_off, s);
-        if (P.mixed) {
-            box_list(T.nboxes, [=] __device__(int b) { return nchp[b] == 0 && count(sse, b) > 0; },
-                     p2m_ids, p2m_off, s);
-            P.p2m_ids = p2m_ids.get();
-            P.p2m_off = p2m_off.get();
+        LevelStarts ls{};
+        for (int l = 0; l <= T.nlevels; l++) ls.v[l] = T.lstart[l];
+        const bool mixed = P.mixed;
+        make_box_lists(T, ls, [=] __device__(int b) -> unsigned {
+            const bool src = count(sse, b) > 0, pts = ec.npts(b) > 0, leaf = nchp[b] == 0;
+            return (!leaf && src ? 1u : 0u) | (pts ? 2u : 0u) | (mixed && leaf && src ? 4u : 0u) |
+                   (n4p[b] > 0 && pts ? 8u : 0u);
+        }, lists, s);
+        P.m2m_ids = lists.ids[0].get();
+        P.l2l_ids = lists.ids[1].get();
+        P.m2m_cnt = lists.count(0, 0);
+        P.l2l_cnt = lists.count(1, 0);
+        if (mixed) {
+            P.p2m_ids = lists.ids[2].get();
+            P.p2m_cnt = lists.count(2, 0);
         }
-        const int *n4p = T.nlist4.get();
-        box_list(T.nboxes, [=] __device__(int b) { return n4p[b] > 0 && ec.npts(b) > 0; },
-                 p2l_ids, p2l_off, s);
-        P.p2l_ids = p2l_ids.get();
-        P.p2l_off = p2l_off.get();
-        P.m2m_ids = m2m_ids.get();
-        P.m2m_off = m2m_off.get();
-        P.l2l_ids = l2l_ids.get();
-        P.l2l_off = l2l_off.get();
+        P.p2l_ids = lists.ids[3].get();
+        P.p2l_cnt = lists.count(3, 0);
     }
     prof_mark("fmm_setup", s);
     auto per_chunk = [&](auto f2, auto f1) {

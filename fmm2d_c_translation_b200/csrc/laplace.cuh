@@ -82,14 +82,14 @@ struct CauchyProblem {
     double *timeinfo = nullptr;       // 8 phase times (s), optional
     M2LCache *m2l_cache = nullptr;    // planning kept across evaluations (plans)
     // boxes visited by the Pascal M2M (parents with sources) and L2L (boxes
-    // with evaluation points), in box order: level l's entries are
-    // ids[off[lstart[l]] .. off[lend[l]]) (set by cauchy_fmm)
-    const int *m2m_ids = nullptr, *m2m_off = nullptr;
-    const int *l2l_ids = nullptr, *l2l_off = nullptr;
-    // leaves with sources (the boxes the P2M visits), same form
-    const int *p2m_ids = nullptr, *p2m_off = nullptr;
-    // boxes with list-4 entries and evaluation points (the P2L), same form
-    const int *p2l_ids = nullptr, *p2l_off = nullptr;
+    // with evaluation points): level l's at ids + lstart[l], cnt[l] of them;
+    // by the mixed mode's P2M (leaves with sources) and the P2L (boxes with
+    // list-4 entries and evaluation points): ids, *cnt of them (set by
+    // cauchy_fmm; the order within a level is arbitrary)
+    const int *m2m_ids = nullptr, *m2m_cnt = nullptr;
+    const int *l2l_ids = nullptr, *l2l_cnt = nullptr;
+    const int *p2m_ids = nullptr, *p2m_cnt = nullptr;
+    const int *p2l_ids = nullptr, *p2l_cnt = nullptr;
 };
 
 // Runs steps 1-8 of cfmm2dmain (src/laplace/cfmm2d.f:442-1340) on the
