@@ -1507,10 +1507,7 @@ struct LevelStarts {
 struct BoxLists {
     DevBuf<int> ids[4], cnt;
     int L = 0;
-    // list i's entries and count for level l (lists 0, 1) or all (2, 3)
-    const int *seg(int i, const LevelStarts &ls, int l) const {
-        return ids[i].get() + (i < 2 ? ls.v[l] : 0);
-    }
+    // list i's count for level l (lists 0, 1) or all (2, 3)
     const int *count(int i, int l) const { return cnt.get() + i * (L + 1) + (i < 2 ? l : 0); }
 };
 
